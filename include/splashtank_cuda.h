@@ -1,0 +1,235 @@
+/*
+ * splashtank_cuda.h - C ABI of the B200 FLIP water step (SplashTank's FlipSim) and the PBF solver.
+ *
+ * Plain C: pointers, sizes and POD structs only; no CUDA or torch types. One handle owns one CUDA
+ * stream and all device memory it needs. A handle is not thread-safe: call it from one host thread.
+ * Calls that only enqueue GPU work (st_flip_step) return before the GPU finishes; read calls
+ * (st_flip_read_*, st_flip_stats) synchronise the handle's stream.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the SplashTank repo).
+ */
+#ifndef SPLASHTANK_CUDA_H
+#define SPLASHTANK_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ST_ABI_VERSION 1u
+
+typedef enum st_status {
+  ST_OK = 0,
+  ST_NOT_READY = 1,     /* nothing to do: no particles (FlipSim.step returns early, src/flip/sim.js:181) */
+  ST_POOL_GREW = 2,     /* reserved: the tile pool grew (src/flip/sim.js:137-159) */
+  ST_OVERFLOW = 3,      /* a bounded list (whitewater ring, spawn list, cell bucket) was cut short */
+  ST_OOM = 4,           /* device allocation failed */
+  ST_BAD_ARG = 5,       /* null pointer, wrong struct size, out-of-range value */
+  ST_DEVICE_ERROR = 6,  /* a CUDA call failed; the message is in st_last_error() */
+  ST_TIMEOUT = 7,       /* a bounded device wait gave up */
+  ST_UNSUPPORTED = 8
+} st_status;
+
+/* Open faces of the box: particles leave through them (src/shared.js:229). */
+enum { ST_OPEN_X0 = 1, ST_OPEN_X1 = 2, ST_OPEN_Y0 = 4, ST_OPEN_Y1 = 8, ST_OPEN_Z0 = 16, ST_OPEN_Z1 = 32 };
+
+/* Step option switches: FlipSim.opt (src/flip/sim.js:49). */
+enum { ST_OPT_NO_FOAM = 1, ST_OPT_NO_CULL = 2, ST_OPT_FAST_AIR = 4 };
+
+typedef struct st_flip st_flip;
+
+/* new FlipSim(device, {d, maxN, size, open, ratio}) (src/flip/sim.js:47-58). */
+typedef struct st_flip_desc {
+  uint32_t size;        /* sizeof(st_flip_desc) */
+  double d;             /* particle spacing */
+  double ratio;         /* cell size over spacing; 0 means 2; clamped to [1.4, 4] */
+  double box[3];        /* box extent (W, H, D); zeros mean (3, 2.6, 3) */
+  uint32_t open;        /* ST_OPEN_* bits */
+  uint32_t max_n;       /* particle capacity (MAXN) */
+  uint32_t spray_cap;   /* whitewater points (FlipSim.setSprayCap, src/flip/sim.js:333); 0: off */
+  int32_t device;       /* CUDA device ordinal */
+} st_flip_desc;
+
+/* A collider's signed distance grid: the object passed as cols[k].sdf (src/shared.js:98, src/gpu.js:42-56).
+ * Grids are uploaded when the set of ids changes; data must stay valid only during the call. */
+typedef struct st_sdf {
+  uint32_t id;
+  uint32_t dims[3];
+  float origin[3];
+  float cell;
+  const float* data;    /* dims[0]*dims[1]*dims[2] floats, x fastest */
+} st_sdf;
+
+/* One collider record for a step: SceneRunner.step's colOf (src/shared.js:531-544). */
+typedef struct st_collider {
+  const st_sdf* sdf;
+  float pos[3];         /* x, y, z */
+  float R[9];           /* rotation, row major (eulerMat, src/shared.js:9-14) */
+  float vel[3];         /* vx, vy, vz */
+  float ang[3];         /* wx, wy, wz */
+} st_collider;
+
+/* Whitewater options: o.spr (src/flip/sim.js:203-205, 225). */
+typedef struct st_spray_opts {
+  float rate, min, life, mist, drag, mdrag;
+  float foam_life, rise, crest, impact;
+} st_spray_opts;
+
+/* The per-step options object o (src/flip/sim.js:185-230). Fill with st_step_opts_default first. */
+typedef struct st_step_opts {
+  uint32_t size;        /* sizeof(st_step_opts) */
+  float g;              /* gravity (o.g) */
+  float flip;           /* FLIP ratio (default 0.95) */
+  float comp;           /* density correction (default 6) */
+  float omega;          /* SOR factor; 0 picks min(1.9, 2/(1+sin(pi/max n))) */
+  float vmax;           /* speed limit; 0 means 14 */
+  float wind[3];
+  float drag;
+  float foam_tau;       /* default 1.2 */
+  float foam_sens;      /* default 1 */
+  float gust;
+  float tear;           /* sheet tearing threshold (particles per cell) */
+  float vs;             /* metres per scene unit (default 1) */
+  int32_t iters;        /* SOR iterations (red + black) */
+  uint32_t flags;       /* ST_OPT_* */
+  uint32_t ncols;       /* colliders (at most 32) */
+  const st_collider* cols;
+  int32_t spray_on;     /* o.spr present */
+  st_spray_opts spray;
+  int32_t nb_on;        /* o.nb.on: narrow band */
+  float nb_band;        /* o.nb.band (cells, at least 2) */
+} st_step_opts;
+
+/* Counters read back after a step: FlipSim.stats (src/flip/sim.js:160-168). */
+typedef struct st_stats {
+  uint32_t sc;          /* tiles (8^3 blocks) with storage */
+  uint32_t ovf;         /* tiles that did not fit (always 0: every tile has storage) */
+  uint32_t fluid;       /* fluid cells */
+  float vmax;           /* fastest particle speed seen by P2G */
+  uint32_t n;           /* particle slots in use (N) */
+  uint32_t live;        /* particles not parked dead */
+  uint32_t spray_used;  /* whitewater slots handed out (sctl[0]) */
+  uint32_t steps;       /* steps taken since create/clear */
+} st_stats;
+
+/* Dense debug export of the grid (FlipSim.dbgColumn/dbgRow, src/flip/sim.js:457-482), per cell of the
+ * tile box (tx*8) x (ty*8) x (tz*8), x fastest. Null pointers are skipped. Cells of tiles without storage
+ * read as the spare block does in the reference (cnt 0, ctype 0, pres 0). */
+typedef struct st_flip_grid {
+  uint8_t* tile_on;     /* tx*ty*tz */
+  int32_t* cnt;
+  uint32_t* ctype;
+  float* pres;
+  float* rhs;
+  float* vn;            /* 3 per cell: the cell's lower x, y, z faces (new velocity) */
+  float* vo;            /* 3 per cell: old velocity */
+  float* velg;          /* 3 per cell: kept grid velocity (narrow band) */
+} st_flip_grid;
+
+typedef struct st_flip_dims {
+  uint32_t nx, ny, nz, tx, ty, tz;
+  float h, x0, y0, z0, x1, y1, z1;
+} st_flip_dims;
+
+/* Per-stage device milliseconds of the last step (FlipSim.stepTimed, src/flip/sim.js:312-331). Stage
+ * names as in src/app/14-bench.js:17. */
+typedef struct st_stage_times {
+  float sort, blocks, clear, p2g, narrow_band, classify, norm_faces, divergence, pressure, project, g2p, spray, reseed, total;
+} st_stage_times;
+
+/* ---- FLIP ---- */
+
+/* Fill an options struct with the reference defaults (src/flip/sim.js:197-230). */
+void st_step_opts_default(st_step_opts* o);
+
+/* new FlipSim(device, opt) (src/flip/sim.js:47-105). */
+st_status st_flip_create(const st_flip_desc* desc, st_flip** out);
+/* FlipSim.destroy (src/flip/sim.js:496-501). */
+void st_flip_destroy(st_flip* s);
+/* FlipSim.clear (src/flip/sim.js:539-547, src/gpu.js:389). */
+st_status st_flip_clear(st_flip* s);
+/* FlipSim.setCap (src/gpu.js:388). */
+st_status st_flip_set_cap(st_flip* s, uint32_t cap);
+/* n calls of FlipSim.add(x,y,z,vx,vy,vz) then flushRun (src/gpu.js:390-408). pos3 and vel3 hold n xyz
+ * triples. *added receives how many were taken (the ring recycles slots when full). */
+st_status st_flip_add(st_flip* s, const float* pos3, const float* vel3, uint32_t n, uint32_t* added);
+/* FlipSim.step(dt, o) (src/flip/sim.js:179-241). Enqueues the step on the handle's stream. */
+st_status st_flip_step(st_flip* s, double dt, const st_step_opts* o);
+/* FlipSim.stepTimed (src/flip/sim.js:312-331): one step, returning device ms per stage. */
+st_status st_flip_step_timed(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t);
+/* FlipSim.readbackInto (src/flip/sim.js:439-455): particles in id order, 4 floats each.
+ * vel4 may be null. *n receives N; at most cap particles are written. */
+st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
+/* FlipSim.readSpray (src/flip/sim.js:423-437): whitewater slots handed out (positions with life in w,
+ * velocities with kind in w). */
+st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
+/* FlipSim.stats via readStats (src/flip/sim.js:160-168). Synchronises. */
+st_status st_flip_stats(st_flip* s, st_stats* out);
+/* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */
+st_status st_flip_read_grid(st_flip* s, const st_flip_grid* g);
+st_status st_flip_get_dims(st_flip* s, st_flip_dims* out);
+/* The particle state in storage order (the order after the last step's sort): pos4, vel4, ids.
+ * Pointers may be null. Together with st_flip_load_state this is the checkpoint of the particles. */
+st_status st_flip_save_state(st_flip* s, float* pos4, float* vel4, uint32_t* pid, uint32_t cap, uint32_t* n);
+/* Replace every particle (storage order, with ids); resets time-since-start to t and the seed counter. */
+st_status st_flip_load_state(st_flip* s, const float* pos4, const float* vel4, const uint32_t* pid, uint32_t n,
+                             double t, uint32_t seed);
+/* Narrow band start (nbSeed's sim.nbFills, src/shared.js:849-851): boxes as {x0,y0,z0,x1,y1,z1} and spheres as
+ * {x,y,z,r}; the next step initialises the depth field from them (nbInit = mode). */
+st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const float* spheres4, uint32_t nsph,
+                           uint32_t mode);
+/* The CUDA stream the handle enqueues on (a cudaStream_t), for events and graph capture by the caller. */
+void* st_flip_stream(st_flip* s);
+
+/* ---- PBF (GpuSim, src/gpu.js:357-428) ---- */
+
+typedef struct st_pbf st_pbf;
+
+typedef struct st_pbf_desc {
+  uint32_t size;        /* sizeof(st_pbf_desc) */
+  double d;             /* particle spacing; kernel radius h = 2.2 d */
+  double box[3];        /* zeros mean (3, 2.6, 3) */
+  uint32_t open;
+  uint32_t max_n;
+  int32_t device;
+  double eps_k;         /* 0 means 0.64 (src/shared.js:259) */
+  double wall_k;        /* 0 means 1.8 (src/shared.js:268) */
+} st_pbf_desc;
+
+/* Analytic collider of the native baker (native/splash.cpp:22): kind 0 sphere (r), kind 1 box (half
+ * extents, rotated by yaw about y). */
+typedef struct st_pbf_col {
+  int32_t kind;
+  float x, y, z, r, hx, hy, hz, yaw;
+} st_pbf_col;
+
+typedef struct st_pbf_opts {
+  uint32_t size;
+  float g;
+  float visc;
+  int32_t iters;
+  uint32_t ncols;
+  const st_pbf_col* cols;
+} st_pbf_opts;
+
+/* new FluidSim/GpuSim constants (src/shared.js:220-271, native/splash.cpp:50-71). */
+st_status st_pbf_create(const st_pbf_desc* desc, st_pbf** out);
+void st_pbf_destroy(st_pbf* s);
+/* Sim::add / fillBox (native/splash.cpp:78-89): n particles. */
+st_status st_pbf_add(st_pbf* s, const float* pos3, const float* vel3, uint32_t n, uint32_t* added);
+/* Sim::step (native/splash.cpp:212-247), GpuSim.step (src/gpu.js:409-428). */
+st_status st_pbf_step(st_pbf* s, double dt, const st_pbf_opts* o);
+/* positions (xyz, speed in w) and velocities in id order. */
+st_status st_pbf_read(st_pbf* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
+void* st_pbf_stream(st_pbf* s);
+
+/* ---- common ---- */
+uint32_t st_abi_version(void);
+/* Text of the last error on this thread (static storage). */
+const char* st_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

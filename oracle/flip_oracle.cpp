@@ -1,0 +1,1097 @@
+// flip_oracle.cpp - CPU restatement of SplashTank's FLIP step, used ONLY as the parity checker and as the
+// timed CPU baseline. It is test infrastructure: the product (splashtank_b200) never links or calls it.
+//
+// It restates the WGSL kernels of src/flip/wgsl-{core,blocks,solver,narrowband,whitewater}.js and the host
+// logic of src/flip/sim.js:179-310 kernel by kernel, in the reference's stage order, with the reference's
+// numerics (f32, fixed-point P2G at scale 65536, red-black SOR in place, 16-bit depth field).
+// Every function cites the reference file:line it follows.
+//
+// Parity status: the reference runs only as WGSL in a browser (WebGPU); it has no CPU FLIP code and its tests
+// hold no golden vectors for the step. This restatement is therefore "parity unpinned" against the reference
+// itself: it is pinned by reading, by the invariant tests in tests/ and by the golden fixtures it generated.
+//
+// Storage: a dense tile box ((tx*8) x (ty*8) x (tz*8) cells, 512 per tile, x fastest inside a tile) plus one
+// spare block at index ntiles, which plays the reference's spare slot 0: every read of a cell whose tile has
+// no storage lands there (wgsl-core.js:79-83). Order-dependent parts of the reference (atomic compaction) use
+// a canonical order here, the same the CUDA path uses:
+//   * particles are stored sorted by (cell key, id) each step, dead ones after them in their previous order;
+//   * narrow-band refill: deficit cells in ascending cell key, dead slots in ascending storage index;
+//   * whitewater emission: ring slots handed out in ascending storage index of the emitting particle.
+// Build with -ffp-contract=off (no FMA) so float results are bit-reproducible.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/splashtank_cuda.h"
+
+namespace {
+
+struct V3 { float x, y, z; };
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+inline V3 operator/(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float length(V3 a) { return sqrtf(dot(a, a)); }
+inline float fmin_(float a, float b) { return a < b ? a : b; }
+inline float fmax_(float a, float b) { return a > b ? a : b; }
+inline float clampf(float x, float lo, float hi) { return fmin_(fmax_(x, lo), hi); }
+inline V3 vmin(V3 a, V3 b) { return v3(fmin_(a.x, b.x), fmin_(a.y, b.y), fmin_(a.z, b.z)); }
+inline V3 vmax(V3 a, V3 b) { return v3(fmax_(a.x, b.x), fmax_(a.y, b.y), fmax_(a.z, b.z)); }
+inline V3 vclamp(V3 a, V3 lo, V3 hi) { return vmin(vmax(a, lo), hi); }
+inline V3 vfloor(V3 a) { return v3(floorf(a.x), floorf(a.y), floorf(a.z)); }
+inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline V3 vmix(V3 a, V3 b, float t) { return v3(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
+inline V3 cross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+inline float smoothstep(float e0, float e1, float x) { float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f); return t * t * (3.0f - 2.0f * t); }
+inline float comp(V3 a, int ax) { return ax == 0 ? a.x : (ax == 1 ? a.y : a.z); }
+inline void setc(V3& a, int ax, float v) { if (ax == 0) a.x = v; else if (ax == 1) a.y = v; else a.z = v; }
+inline float bitsf(int32_t i) { float f; memcpy(&f, &i, 4); return f; }
+inline int32_t fbits(float f) { int32_t i; memcpy(&i, &f, 4); return i; }
+// WGSL u32(f): truncation, saturating at 0 for negative values
+inline uint32_t u32f(float f) { return f <= 0.0f ? 0u : (uint32_t)f; }
+
+const float DEADY = -1.0e5f;
+const uint32_t NONE = 0xffffffffu;
+const float WWHOLD = 0.2f;
+
+// hash1 (wgsl-solver.js:181-184)
+inline float hash1(uint32_t n0) {
+  uint32_t x = n0; x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return (float)x * 2.3283064e-10f;
+}
+
+// The parameter block, f32 words as packed by sim.js:196-231 (wgsl-core.js:3-20).
+struct Params {
+  uint32_t n, nx, ny, nz, ncols, open, ncell;
+  float dt, h, ih, gravity, flip, rest, comp, omega;
+  float x0, y0, z0, vmax, margin, scale, x1, y1, z1;
+  float q0, q1, q2, q3, q4, q5, q6, q7, q8, q9, q10, q11, q12;
+  uint32_t lcap, tx, ty, tz, scap;
+  float sheetMin, sprRate, sprMin, sprLife, mistFrac, sprDrag, mistDrag, vs;
+  uint32_t smax, seed;
+  uint32_t nb; float band; uint32_t nbInit, nfill;
+  float wwFoamLife, wwRise, wwCrest, wwImpact;
+  float fills[16][4];
+};
+
+struct Oracle {
+  // fixed at create (sim.js:47-61)
+  double d, ratio, h, rest;
+  int nx, ny, nz, tx, ty, tz, ntiles;
+  double bx0, bx1, by0, by1, bz0, bz1;
+  uint32_t open, maxN, cap, N = 0, ring = 0, sprayCap;
+  bool recycle = true;
+  // particles in storage order: pos/vel 4 floats, id
+  std::vector<float> pos, vel;
+  std::vector<uint32_t> pid;
+  // tiles and cells ((ntiles + 1) * 512: spare block last)
+  std::vector<uint8_t> alloc, need;
+  std::vector<int32_t> cnt, accV, accW;   // acc: 3 per cell (x, y, z lower faces)
+  std::vector<uint32_t> ctype;
+  std::vector<float> pres, rhs, velG;
+  std::vector<uint32_t> active;           // tiles with storage, ascending
+  // colliders (packColliders, gpu.js:42-70): 32 floats each, sdf grids back to back
+  std::vector<float> cols, sdf;
+  uint32_t ncols = 0;
+  std::string sdfSig;
+  // whitewater (sim.js:71, 333-341)
+  std::vector<float> sPos, sVel, sAux;
+  uint32_t sctl0 = 0;
+  // narrow band state (sim.js:92, 120-126)
+  bool velGOn = false;
+  uint32_t nbInit = 0;
+  std::vector<float> fillsPacked;  // 8 floats per fill
+  // time and seed (sim.js:200, 207)
+  double tm = 0;
+  uint32_t seed = 0, steps = 0;
+  // stats
+  uint32_t st_sc = 0, st_fluid = 0, st_ovf = 0, spray_ovf = 0;
+  float st_vmax = 0;
+  Params P;
+  int nthreads = 1;
+
+  uint32_t spare() const { return (uint32_t)ntiles; }
+  // ---- addressing (wgsl-core.js:76-135) ----
+  uint32_t tileOf(int i, int j, int k) const { return (uint32_t)(i >> 3) + P.tx * ((uint32_t)(j >> 3) + P.ty * (uint32_t)(k >> 3)); }
+  uint32_t cellIdx(int i, int j, int k) const {
+    uint32_t t = tileOf(i, j, k);
+    uint32_t s = alloc[t] ? t : spare();
+    return s * 512u + (uint32_t)(i & 7) + 8u * ((uint32_t)(j & 7) + 8u * (uint32_t)(k & 7));
+  }
+  uint32_t faceIndex(int axis, int i, int j, int k) const {
+    int nx_ = (int)P.nx, ny_ = (int)P.ny, nz_ = (int)P.nz;
+    auto cl = [](int v, int lo, int hi) { return std::min(std::max(v, lo), hi); };
+    if (axis == 0) return cellIdx(cl(i, 0, nx_), cl(j, 0, ny_ - 1), cl(k, 0, nz_ - 1)) * 3u;
+    if (axis == 1) return cellIdx(cl(i, 0, nx_ - 1), cl(j, 0, ny_), cl(k, 0, nz_ - 1)) * 3u + 1u;
+    return cellIdx(cl(i, 0, nx_ - 1), cl(j, 0, ny_ - 1), cl(k, 0, nz_)) * 3u + 2u;
+  }
+  void tileCoord(uint32_t t, uint32_t local, int& i, int& j, int& k) const {
+    uint32_t tt = t / P.tx;
+    i = (int)((t % P.tx) * 8u + (local & 7u)); j = (int)((tt % P.ty) * 8u + ((local >> 3) & 7u)); k = (int)((tt / P.ty) * 8u + (local >> 6));
+  }
+  uint32_t ctypeOf(int i, int j, int k) const {
+    if (i < 0) return (P.open & 1u) ? 0u : 2u;
+    if (i >= (int)P.nx) return (P.open & 2u) ? 0u : 2u;
+    if (j < 0) return (P.open & 4u) ? 0u : 2u;
+    if (j >= (int)P.ny) return (P.open & 8u) ? 0u : 2u;
+    if (k < 0) return (P.open & 16u) ? 0u : 2u;
+    if (k >= (int)P.nz) return (P.open & 32u) ? 0u : 2u;
+    return ctype[cellIdx(i, j, k)] & 0xffu;
+  }
+  bool inDom(int i, int j, int k) const { return i >= 0 && j >= 0 && k >= 0 && i < (int)P.nx && j < (int)P.ny && k < (int)P.nz; }
+  V3 cellCenter(int i, int j, int k) const {
+    return v3(P.x0 + ((float)i + 0.5f) * P.h, P.y0 + ((float)j + 0.5f) * P.h, P.z0 + ((float)k + 0.5f) * P.h);
+  }
+  void particleCell(V3 p, int& ci, int& cj, int& ck) const {
+    V3 g = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih);
+    ci = std::min(std::max((int)g.x, 0), (int)P.nx - 1);
+    cj = std::min(std::max((int)g.y, 0), (int)P.ny - 1);
+    ck = std::min(std::max((int)g.z, 0), (int)P.nz - 1);
+  }
+  bool hasStorage(int i, int j, int k) const { return alloc[tileOf(i, j, k)] != 0; }
+  float gvR(uint32_t f) const { return bitsf(accV[f]); }
+  float gv0R(uint32_t f) const { return bitsf(accW[f]); }
+
+  // ---- colliders (gpu.js:6-38, wgsl-core.js:113-131) ----
+  const float* col(uint32_t k, int m) const { return &cols[(size_t)k * 32 + (size_t)m * 4]; }
+  void sdfEval(uint32_t k, V3 p, float& phi, V3& wn) const {
+    const float* a = col(k, 0); const float* b = col(k, 1);
+    V3 r0 = v3(col(k, 2)[0], col(k, 2)[1], col(k, 2)[2]);
+    V3 r1 = v3(col(k, 3)[0], col(k, 3)[1], col(k, 3)[2]);
+    V3 r2 = v3(col(k, 4)[0], col(k, 4)[1], col(k, 4)[2]);
+    V3 d_ = p - v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]);
+    V3 lp = v3(dot(r0, d_), dot(r1, d_), dot(r2, d_));
+    V3 g = (lp - v3(b[0], b[1], b[2])) / b[3];
+    V3 dims = v3(a[1], a[2], a[3]);
+    V3 gc = vclamp(g, v3(0, 0, 0), dims - v3(1.0001f, 1.0001f, 1.0001f));
+    V3 fl = vfloor(gc); V3 f = gc - fl;
+    uint32_t nx_ = u32f(a[1]), ny_ = u32f(a[2]);
+    uint32_t base = u32f(a[0]) + u32f(fl.x) + nx_ * (u32f(fl.y) + ny_ * u32f(fl.z));
+    uint32_t s = nx_ * ny_;
+    const float* sd = sdf.data();
+    float v000 = sd[base], v100 = sd[base + 1], v010 = sd[base + nx_], v110 = sd[base + nx_ + 1];
+    float v001 = sd[base + s], v101 = sd[base + s + 1], v011 = sd[base + s + nx_], v111 = sd[base + s + nx_ + 1];
+    float c00 = mixf(v000, v100, f.x), c10 = mixf(v010, v110, f.x), c01 = mixf(v001, v101, f.x), c11 = mixf(v011, v111, f.x);
+    float c0 = mixf(c00, c10, f.y), c1 = mixf(c01, c11, f.y);
+    phi = mixf(c0, c1, f.z);
+    V3 out = g - gc; V3 gl;
+    if (dot(out, out) > 0.0f) {
+      float l = length(out); phi += l * b[3]; gl = out / l;
+    } else {
+      gl = v3(mixf(mixf(v100 - v000, v110 - v010, f.y), mixf(v101 - v001, v111 - v011, f.y), f.z), mixf(c10 - c00, c11 - c01, f.z), c1 - c0);
+      float l = length(gl); gl = gl / fmax_(l, 1e-9f);
+    }
+    wn = r0 * gl.x + r1 * gl.y + r2 * gl.z;
+  }
+  V3 colSurfVel(uint32_t k, V3 p) const {
+    V3 c = v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]);
+    return v3(col(k, 6)[0], col(k, 6)[1], col(k, 6)[2]) + cross(v3(col(k, 7)[0], col(k, 7)[1], col(k, 7)[2]), p - c);
+  }
+  bool colNear(uint32_t k, V3 p) const {
+    if (P.q10 > 0.5f) return true;
+    const float* b = col(k, 1);
+    V3 d_ = p - v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]);
+    V3 lp = v3(dot(v3(col(k, 2)[0], col(k, 2)[1], col(k, 2)[2]), d_), dot(v3(col(k, 3)[0], col(k, 3)[1], col(k, 3)[2]), d_),
+               dot(v3(col(k, 4)[0], col(k, 4)[1], col(k, 4)[2]), d_));
+    V3 g = (lp - v3(b[0], b[1], b[2])) / b[3];
+    V3 dims = v3(col(k, 0)[1], col(k, 0)[2], col(k, 0)[3]);
+    float lo = -1.0f - P.q0 / b[3], hi = P.q0 / b[3];
+    return g.x > lo && g.y > lo && g.z > lo && g.x < dims.x + hi && g.y < dims.y + hi && g.z < dims.z + hi;
+  }
+  int colAt(V3 p) const {
+    for (uint32_t k = 0; k < P.ncols; k++) {
+      if (!colNear(k, p)) continue;
+      float phi; V3 wn; sdfEval(k, p, phi, wn);
+      if (phi < P.q0) return (int)k;
+    }
+    return -1;
+  }
+  int colAtCell(int i, int j, int k) const {
+    if (!inDom(i, j, k)) return -1;
+    return (int)((ctype[cellIdx(i, j, k)] >> 8) & 0xffu) - 1;
+  }
+
+  // ---- narrow band helpers (wgsl-core.js:160-200, 228-238) ----
+  uint32_t colBits(uint32_t c) const { return (ctype[c] >> 8) & 0xffu; }
+  float phiOf(uint32_t c) const { return 8.0f - (float)(ctype[c] >> 16) / 4096.0f; }
+  void phiPut(uint32_t c, float v) {
+    uint32_t q = (uint32_t)clampf(rintf((8.0f - v) * 4096.0f), 0.0f, 65535.0f);
+    ctype[c] = (ctype[c] & 0xffffu) | (q << 16);
+  }
+  V3 facePos(int i, int j, int k, int axis) const {
+    return v3(P.x0 + ((float)i + (axis == 0 ? 0.0f : 0.5f)) * P.h, P.y0 + ((float)j + (axis == 1 ? 0.0f : 0.5f)) * P.h,
+              P.z0 + ((float)k + (axis == 2 ? 0.0f : 0.5f)) * P.h);
+  }
+  float phiSample(V3 x) const {
+    V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
+    V3 gc = vclamp(g, v3(0, 0, 0), v3((float)P.nx - 1.001f, (float)P.ny - 1.001f, (float)P.nz - 1.001f));
+    V3 f0 = vfloor(gc); V3 fr = gc - f0; int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    float s = 0.0f, ws = 0.0f;
+    for (int c = 0; c < 8; c++) {
+      int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      uint32_t ci = cellIdx(i0 + dx, j0 + dy, k0 + dz);
+      if (colBits(ci) != 0u || w <= 0.0f) continue;
+      s += w * phiOf(ci); ws += w;
+    }
+    if (ws < 1.0e-4f) return 0.5f;
+    return s / ws;
+  }
+  float velGAxis(V3 x, int axis) const {
+    V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
+    if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+    V3 f0 = vfloor(g); V3 fr = g - f0; int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    float s = 0.0f;
+    for (int c = 0; c < 8; c++) {
+      int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      s += w * velG[faceIndex(axis, i0 + dx, j0 + dy, k0 + dz)];
+    }
+    return s;
+  }
+  V3 velGVec(V3 x) const { return v3(velGAxis(x, 0), velGAxis(x, 1), velGAxis(x, 2)); }
+  bool calmV(V3 v) const { return length(v) < 9.0f * P.h; }
+  float fillPhi(V3 x) const {
+    float dd = 1.0e9f;
+    for (uint32_t k = 0; k < P.nfill; k++) {
+      const float* A = P.fills[k * 2]; const float* B = P.fills[k * 2 + 1];
+      if (A[0] < 1.5f) {
+        V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(B[0], B[1], B[2]));
+        dd = fmin_(dd, length(vmax(q, v3(0, 0, 0))) + fmin_(fmax_(q.x, fmax_(q.y, q.z)), 0.0f));
+      } else {
+        dd = fmin_(dd, length(x - v3(A[1], A[2], A[3])) - B[0]);
+      }
+    }
+    return dd * P.ih;
+  }
+  // markAround (wgsl-core.js:239-246)
+  void markAround(int ci, int cj, int ck) {
+    int lox = std::max(ci - 2, 0) >> 3, loy = std::max(cj - 2, 0) >> 3, loz = std::max(ck - 2, 0) >> 3;
+    int hix = std::min(ci + 2, (int)P.tx * 8 - 1) >> 3, hiy = std::min(cj + 2, (int)P.ty * 8 - 1) >> 3, hiz = std::min(ck + 2, (int)P.tz * 8 - 1) >> 3;
+    for (int tk = loz; tk <= hiz; tk++) for (int tj = loy; tj <= hiy; tj++) for (int ti = lox; ti <= hix; ti++)
+      need[(uint32_t)ti + P.tx * ((uint32_t)tj + P.ty * (uint32_t)tk)] = 1;
+  }
+  V3 ppos(uint32_t i) const { return v3(pos[i * 4], pos[i * 4 + 1], pos[i * 4 + 2]); }
+  V3 pvel(uint32_t i) const { return v3(vel[i * 4], vel[i * 4 + 1], vel[i * 4 + 2]); }
+  template <class F> void forActive(F fn) {
+    const int64_t nc = (int64_t)active.size() * 512;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t t = 0; t < nc; t++) {
+      uint32_t tile = active[(size_t)(t >> 9)], local = (uint32_t)(t & 511);
+      int i, j, k; tileCoord(tile, local, i, j, k);
+      fn(tile * 512u + local, i, j, k);
+    }
+  }
+  template <class F> void forParticles(F fn) {
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t i = 0; i < (int64_t)P.n; i++) fn((uint32_t)i);
+  }
+
+  // ---- create (sim.js:47-98) ----
+  void create(const st_flip_desc* dsc) {
+    d = dsc->d;
+    double r = dsc->ratio != 0 ? dsc->ratio : 2.0;
+    ratio = std::max(1.4, std::min(4.0, r));
+    h = ratio * d; rest = ratio * ratio * ratio;
+    double sz[3] = {3, 2.6, 3};
+    if (dsc->box[0] > 0 && dsc->box[1] > 0 && dsc->box[2] > 0) { sz[0] = dsc->box[0]; sz[1] = dsc->box[1]; sz[2] = dsc->box[2]; }
+    nx = std::max(4, (int)std::floor(sz[0] / h + 0.5)); ny = std::max(4, (int)std::floor(sz[1] / h + 0.5)); nz = std::max(4, (int)std::floor(sz[2] / h + 0.5));
+    double W = nx * h, H = ny * h, D = nz * h;
+    bx0 = -W / 2; bx1 = W / 2; by0 = 0; by1 = H; bz0 = -D / 2; bz1 = D / 2;
+    open = dsc->open; maxN = dsc->max_n; cap = maxN; sprayCap = dsc->spray_cap;
+    tx = (nx + 1 + 7) / 8; ty = (ny + 1 + 7) / 8; tz = (nz + 1 + 7) / 8; ntiles = tx * ty * tz;
+    pos.assign((size_t)maxN * 4, 0.0f); vel.assign((size_t)maxN * 4, 0.0f); pid.resize(maxN);
+    for (uint32_t k = 0; k < maxN; k++) pid[k] = k;
+    size_t ncell = (size_t)(ntiles + 1) * 512;
+    alloc.assign(ntiles, 0); need.assign(ntiles, 0);
+    cnt.assign(ncell, 0); ctype.assign(ncell, 0); pres.assign(ncell, 0.0f); rhs.assign(ncell, 0.0f);
+    accV.assign(ncell * 3, 0); accW.assign(ncell * 3, 0); velG.assign(ncell * 3, 0.0f);
+    sPos.assign((size_t)std::max(sprayCap, 1u) * 4, 0.0f); sVel = sPos; sAux = sPos;
+    memset(&P, 0, sizeof(P));
+    P.tx = tx; P.ty = ty; P.tz = tz; P.nx = nx; P.ny = ny; P.nz = nz;
+  }
+  // FlipSim.clear (sim.js:539-547, gpu.js:389)
+  void clear() {
+    N = 0; ring = 0; tm = 0; nbInit = 1; fillsPacked.clear();
+    std::fill(sPos.begin(), sPos.end(), 0.0f); sctl0 = 0;
+    for (uint32_t k = 0; k < maxN; k++) pid[k] = k;
+    steps = 0;
+  }
+  // FlipSim.add (gpu.js:390-402)
+  bool add(float x, float y, float z, float vx, float vy, float vz) {
+    uint32_t i;
+    if (N < cap) i = N++;
+    else if (recycle) { i = ring++; if (ring >= cap) ring = 0; }
+    else return false;
+    pos[i * 4] = x; pos[i * 4 + 1] = y; pos[i * 4 + 2] = z;
+    pos[i * 4 + 3] = (float)std::sqrt((double)vx * vx + (double)vy * vy + (double)vz * vz);
+    vel[i * 4] = vx; vel[i * 4 + 1] = vy; vel[i * 4 + 2] = vz; vel[i * 4 + 3] = 0.0f;
+    return true;
+  }
+  // packColliders (gpu.js:42-70)
+  void packCols(const st_step_opts* o) {
+    uint32_t nc = std::min(o->ncols, 32u);
+    std::string sig; std::map<uint32_t, uint32_t> offs; uint32_t off = 0;
+    for (uint32_t k = 0; k < nc; k++) {
+      const st_sdf* sd = o->cols[k].sdf;
+      if (!offs.count(sd->id)) { offs[sd->id] = off; off += sd->dims[0] * sd->dims[1] * sd->dims[2]; sig += std::to_string(sd->id) + ","; }
+    }
+    if (sig != sdfSig) {
+      sdf.assign(std::max(off, 16u), 0.0f);
+      std::map<uint32_t, bool> seen;
+      for (uint32_t k = 0; k < nc; k++) {
+        const st_sdf* sd = o->cols[k].sdf;
+        if (seen[sd->id]) continue;
+        seen[sd->id] = true;
+        memcpy(&sdf[offs[sd->id]], sd->data, sizeof(float) * sd->dims[0] * sd->dims[1] * sd->dims[2]);
+      }
+      sdfSig = sig;
+    }
+    cols.assign((size_t)std::max(nc, 1u) * 32, 0.0f);
+    for (uint32_t k = 0; k < nc; k++) {
+      const st_collider& c = o->cols[k]; const st_sdf* sd = c.sdf; float* cf = &cols[k * 32];
+      cf[0] = (float)offs[sd->id]; cf[1] = (float)sd->dims[0]; cf[2] = (float)sd->dims[1]; cf[3] = (float)sd->dims[2];
+      cf[4] = sd->origin[0]; cf[5] = sd->origin[1]; cf[6] = sd->origin[2]; cf[7] = sd->cell;
+      cf[8] = c.R[0]; cf[9] = c.R[3]; cf[10] = c.R[6]; cf[11] = 0;
+      cf[12] = c.R[1]; cf[13] = c.R[4]; cf[14] = c.R[7]; cf[15] = 0;
+      cf[16] = c.R[2]; cf[17] = c.R[5]; cf[18] = c.R[8]; cf[19] = 0;
+      cf[20] = c.pos[0]; cf[21] = c.pos[1]; cf[22] = c.pos[2]; cf[23] = 0;
+      cf[24] = c.vel[0]; cf[25] = c.vel[1]; cf[26] = c.vel[2]; cf[27] = 0;
+      cf[28] = c.ang[0]; cf[29] = c.ang[1]; cf[30] = c.ang[2]; cf[31] = 0;
+    }
+    ncols = nc;
+  }
+  double omegaAuto() const { return std::min(1.9, 2.0 / (1.0 + std::sin(M_PI / std::max(nx, std::max(ny, nz))))); }
+
+  // ---- parameter block (sim.js:196-231) ----
+  void packParams(double dt, const st_step_opts* o, uint32_t init, bool nbOn, bool sprOn) {
+    P.n = N; P.nx = nx; P.ny = ny; P.nz = nz; P.ncols = ncols; P.open = open; P.ncell = (uint32_t)(nx * ny * nz);
+    P.dt = (float)dt; P.h = (float)h; P.ih = (float)(1.0 / h); P.gravity = o->g; P.flip = o->flip; P.rest = (float)rest; P.comp = o->comp;
+    P.omega = o->omega != 0.0f ? o->omega : (float)omegaAuto();
+    P.x0 = (float)bx0; P.y0 = (float)by0; P.z0 = (float)bz0; P.vmax = o->vmax != 0.0f ? o->vmax : 14.0f; P.margin = (float)(0.3 * d); P.scale = 65536.0f;
+    P.x1 = (float)bx1; P.y1 = (float)by1; P.z1 = (float)bz1; P.q0 = (float)(0.3 * h);
+    P.q1 = o->wind[0]; P.q2 = o->wind[1]; P.q3 = o->wind[2]; P.q4 = o->drag; P.q5 = o->foam_tau != 0.0f ? o->foam_tau : 1.2f;
+    P.q6 = o->foam_sens != 0.0f ? o->foam_sens : 1.0f; P.q7 = o->gust; P.q8 = (float)tm;
+    P.q9 = (o->flags & ST_OPT_NO_FOAM) ? 1.0f : 0.0f; P.q10 = (o->flags & ST_OPT_NO_CULL) ? 1.0f : 0.0f; P.q11 = 1.0f;
+    P.q12 = (o->flags & ST_OPT_FAST_AIR) ? 1.0f : 0.0f;
+    uint64_t pool = (uint64_t)(ntiles + 1) * 512;
+    P.lcap = velGOn ? (uint32_t)pool : (uint32_t)std::min<uint64_t>(pool, maxN);
+    P.tx = tx; P.ty = ty; P.tz = tz; P.scap = (uint32_t)(ntiles + 1);
+    const st_spray_opts& sp = o->spray;
+    P.sheetMin = o->tear; P.sprRate = sprOn ? sp.rate : 0.0f; P.sprMin = sprOn ? std::max(0.05f, sp.min) : 1.0f; P.sprLife = sprOn ? sp.life : 1.0f;
+    P.mistFrac = sprOn ? sp.mist : 0.0f; P.sprDrag = sprOn ? sp.drag : 1.0f; P.mistDrag = sprOn ? sp.mdrag : 4.0f; P.vs = o->vs != 0.0f ? o->vs : 1.0f;
+    P.smax = sprayCap; P.seed = seed;
+    P.nb = nbOn ? 1u : 0u; P.band = std::max(2.0f, o->nb_band != 0.0f ? o->nb_band : 3.0f); P.nbInit = init;
+    uint32_t nf = init ? (uint32_t)std::min<size_t>(fillsPacked.size() / 8, 8) : 0u; P.nfill = nf;
+    memset(P.fills, 0, sizeof(P.fills));
+    for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &fillsPacked[k * 8], 8 * sizeof(float));
+    P.wwFoamLife = sp.foam_life != 0.0f ? sp.foam_life : 3.0f; P.wwRise = sp.rise != 0.0f ? sp.rise : 0.3f;
+    P.wwCrest = sp.crest; P.wwImpact = sp.impact;
+  }
+
+  // ---- blocks (wgsl-blocks.js:5-55, wgsl-narrowband.js:6-18, sim.js:253-261) ----
+  void stageBlocks(bool nb, uint32_t init) {
+    std::fill(need.begin(), need.end(), 0);
+    for (uint32_t i = 0; i < P.n; i++) {              // tileMark
+      if (pos[i * 4 + 1] < DEADY) continue;
+      int ci, cj, ck; particleCell(ppos(i), ci, cj, ck); markAround(ci, cj, ck);
+    }
+    if (nb && init != 1) {                             // tileMarkPhi: last step's blocks holding water by depth
+      for (uint32_t tile : active) for (uint32_t local = 0; local < 512; local++) {
+        int i, j, k; tileCoord(tile, local, i, j, k);
+        if (!inDom(i, j, k) || phiOf(tile * 512 + local) >= 0.5f) continue;
+        markAround(i, j, k);
+      }
+    }
+    if (init) {                                        // tileMarkFill
+      for (uint32_t t = 0; t < (uint32_t)ntiles; t++) {
+        uint32_t tt = t / P.tx;
+        V3 tc = v3((float)(t % P.tx), (float)(tt % P.ty), (float)(tt / P.ty)) * 8.0f + v3(4.0f, 4.0f, 4.0f);
+        if (fillPhi(v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) need[t] = 1;
+      }
+    }
+    // tileFree + tileAlloc + initNew (a new block: pres 0, collider id per cell, depth bits 0, velG 0)
+    for (uint32_t t = 0; t < (uint32_t)ntiles; t++) {
+      if (!need[t] && alloc[t]) alloc[t] = 0;
+      else if (need[t] && !alloc[t]) {
+        alloc[t] = 1;
+        for (uint32_t local = 0; local < 512; local++) {
+          int i, j, k; tileCoord(t, local, i, j, k);
+          uint32_t c = t * 512 + local;
+          pres[c] = 0.0f;
+          ctype[c] = (uint32_t)(colAt(cellCenter(i, j, k)) + 1) << 8;
+          velG[c * 3] = 0.0f; velG[c * 3 + 1] = 0.0f; velG[c * 3 + 2] = 0.0f;
+        }
+      }
+    }
+    active.clear();
+    for (uint32_t t = 0; t < (uint32_t)ntiles; t++) if (alloc[t]) active.push_back(t);
+    st_sc = (uint32_t)active.size(); st_ovf = 0; st_vmax = 0.0f;
+    if (init) {                                         // phiInitAll (wgsl-narrowband.js:21-35)
+      forActive([&](uint32_t c, int i, int j, int k) {
+        float ph = clampf(fillPhi(cellCenter(i, j, k)), -7.9f, 7.9f);
+        if (ph < 0.0f) ph = fmin_(ph, -1.5f);
+        if (!inDom(i, j, k)) ph = 8.0f;
+        if (P.nbInit == 2u) ph = fmin_(ph, phiOf(c));
+        phiPut(c, ph);
+        if (P.nbInit == 1u) { velG[c * 3] = 0.0f; velG[c * 3 + 1] = 0.0f; velG[c * 3 + 2] = 0.0f; }
+      });
+    }
+  }
+  // clearSlots (wgsl-solver.js:6-15): blocks in use and the spare block
+  void stageClear() {
+    auto clr = [&](uint32_t c) { cnt[c] = 0; for (int a = 0; a < 3; a++) { accV[c * 3 + a] = 0; accW[c * 3 + a] = 0; } };
+    forActive([&](uint32_t c, int, int, int) { clr(c); });
+    for (uint32_t l = 0; l < 512; l++) { uint32_t c = spare() * 512 + l; clr(c); rhs[c] = 8.0f; }
+  }
+  // canonical storage order: live particles by (cell key, id), dead ones after them keeping their order
+  void stageSort() {
+    uint32_t n = P.n;
+    std::vector<uint64_t> key(n);
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; i++) {
+      order[i] = i;
+      if (pos[i * 4 + 1] < DEADY) { key[i] = ~0ull; continue; }
+      int ci, cj, ck; particleCell(ppos(i), ci, cj, ck);
+      key[i] = ((uint64_t)cellIdx(ci, cj, ck) << 32) | pid[i];
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    std::vector<float> np((size_t)n * 4), nv((size_t)n * 4); std::vector<uint32_t> nid(n);
+    for (uint32_t k = 0; k < n; k++) {
+      uint32_t s = order[k];
+      memcpy(&np[k * 4], &pos[s * 4], 16); memcpy(&nv[k * 4], &vel[s * 4], 16); nid[k] = pid[s];
+    }
+    memcpy(pos.data(), np.data(), (size_t)n * 16); memcpy(vel.data(), nv.data(), (size_t)n * 16);
+    memcpy(pid.data(), nid.data(), (size_t)n * 4);
+  }
+  // p2g (wgsl-solver.js:17-40)
+  void stageP2G() {
+    std::vector<float> vm(nthreads, 0.0f);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t ii = 0; ii < (int64_t)P.n; ii++) {
+      uint32_t i = (uint32_t)ii;
+      V3 p = ppos(i);
+      if (pos[i * 4 + 1] < DEADY) continue;
+      int ci, cj, ck; particleCell(p, ci, cj, ck);
+      if (!hasStorage(ci, cj, ck)) continue;
+      V3 v = pvel(i);
+#ifdef _OPENMP
+      int th = omp_get_thread_num();
+#else
+      int th = 0;
+#endif
+      vm[th] = fmax_(vm[th], length(v));
+      for (int axis = 0; axis < 3; axis++) {
+        V3 q = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+        if (axis == 0) { q.y -= 0.5f; q.z -= 0.5f; } else if (axis == 1) { q.x -= 0.5f; q.z -= 0.5f; } else { q.x -= 0.5f; q.y -= 0.5f; }
+        V3 f0 = vfloor(q); V3 fr = q - f0; int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+        float vc = comp(v, axis);
+        for (int c = 0; c < 8; c++) {
+          int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+          float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+          if (w <= 0.0f) continue;
+          uint32_t idx = faceIndex(axis, i0 + dx, j0 + dy, k0 + dz);
+          int32_t av = (int32_t)rintf(w * vc * P.scale), aw = (int32_t)rintf(w * P.scale);
+#pragma omp atomic
+          accV[idx] += av;
+#pragma omp atomic
+          accW[idx] += aw;
+        }
+      }
+      uint32_t cc = cellIdx(ci, cj, ck);
+#pragma omp atomic
+      cnt[cc] += 1;
+    }
+    for (float x : vm) st_vmax = fmax_(st_vmax, x);
+  }
+  // narrow band depth passes (wgsl-narrowband.js:38-68)
+  float jacNb(int i, int j, int k, float cur, bool fromRhs) const {
+    if (!inDom(i, j, k)) return 8.0f;
+    if (cur >= 0.0f) return cur;
+    float m = -8.0f;
+    for (int q = 0; q < 6; q++) {
+      int a = i, b = j, c = k;
+      if (q == 0) a -= 1; else if (q == 1) a += 1; else if (q == 2) b -= 1; else if (q == 3) b += 1; else if (q == 4) c -= 1; else c += 1;
+      if (!inDom(a, b, c)) continue;
+      uint32_t cq = cellIdx(a, b, c);
+      if (colBits(cq) != 0u) continue;
+      m = fmax_(m, fromRhs ? rhs[cq] : phiOf(cq));
+    }
+    return clampf(m - 1.0f, -7.9f, -0.5f);
+  }
+  void stageNarrowBand() {
+    forActive([&](uint32_t c, int i, int j, int k) {          // nbPhi
+      if (!inDom(i, j, k)) { rhs[c] = 8.0f; return; }
+      if (colBits(c) != 0u) { rhs[c] = 0.5f; return; }
+      V3 x = cellCenter(i, j, k);
+      float phA = phiSample(x - velGVec(x) * P.dt);
+      bool inside = cnt[c] > 0 || phA < -1.0f;
+      rhs[c] = inside ? clampf(phA, -7.9f, -0.5f) : clampf(phA, 0.5f, 7.9f);
+    });
+    auto jacA = [&]() { forActive([&](uint32_t c, int i, int j, int k) { phiPut(c, jacNb(i, j, k, rhs[c], true)); }); };
+    jacA();
+    forActive([&](uint32_t c, int i, int j, int k) { rhs[c] = jacNb(i, j, k, phiOf(c), false); });
+    jacA();
+  }
+  // collider bits (solidBuild, wgsl-solver.js:42-45) then classify (wgsl-solver.js:47-74)
+  void stageClassify() {
+    forActive([&](uint32_t c, int i, int j, int k) {
+      ctype[c] = (ctype[c] & 0xffff00ffu) | ((uint32_t)(colAt(cellCenter(i, j, k)) + 1) << 8);
+    });
+    forActive([&](uint32_t c, int i, int j, int k) {
+      uint32_t ty = 0;
+      uint32_t sb = ctype[c] & 0xffffff00u;
+      int32_t n = cnt[c];
+      V3 cx = cellCenter(i, j, k);
+      if (!inDom(i, j, k)) ty = 0;
+      else if ((sb & 0xff00u) != 0u) ty = 2;
+      else if (P.nb != 0u && phiOf(c) < -1.0f && (phiOf(c) < -P.band || calmV(velGVec(cx)))) ty = 1;
+      else if (n > 0) {
+        ty = 1;
+        if ((float)n < P.sheetMin) {
+          int32_t dth = (int32_t)ceilf(0.6f * P.rest); bool dense = false;
+          for (int q = 0; q < 6; q++) {
+            int a = i, b = j, cc = k;
+            if (q == 0) a -= 1; else if (q == 1) a += 1; else if (q == 2) b -= 1; else if (q == 3) b += 1; else if (q == 4) cc -= 1; else cc += 1;
+            if (!inDom(a, b, cc)) continue;
+            if (cnt[cellIdx(a, b, cc)] >= dth) dense = true;
+          }
+          if (!dense) ty = 0;
+        }
+      }
+      ctype[c] = ty | sb;
+      if (ty != 1u) pres[c] = 0.0f;
+    });
+    uint32_t fl = 0;
+    for (uint32_t t : active) for (uint32_t l = 0; l < 512; l++) if ((ctype[t * 512 + l] & 0xffu) == 1u) fl++;
+    st_fluid = fl;
+  }
+  // nbVel (wgsl-narrowband.js:71-85)
+  void stageNbVel() {
+    forActive([&](uint32_t c, int i, int j, int k) {
+      if (!inDom(i, j, k)) return;
+      if ((ctype[c] & 0xffu) != 1u) return;
+      for (int ax = 0; ax < 3; ax++) {
+        int a = i, b = j, cc = k;
+        if (ax == 0) a -= 1; else if (ax == 1) b -= 1; else cc -= 1;
+        if (!inDom(a, b, cc)) continue;
+        if ((ctype[cellIdx(a, b, cc)] & 0xffu) != 1u) continue;
+        uint32_t f = c * 3 + ax;
+        if (accW[f] > 0) continue;
+        V3 fp = facePos(i, j, k, ax);
+        float vc = velGAxis(fp - velGVec(fp) * P.dt, ax);
+        accV[f] = (int32_t)rintf(vc * P.scale); accW[f] = (int32_t)P.scale;
+      }
+    });
+  }
+  // normFaces / normBody (wgsl-solver.js:75-105)
+  void stageNormFaces() {
+    forActive([&](uint32_t c, int i, int j, int k) {
+      for (int axis = 0; axis < 3; axis++) {
+        uint32_t f = c * 3 + axis;
+        int li = i, lj = j, lk = k;
+        if (axis == 0) li -= 1; else if (axis == 1) lj -= 1; else lk -= 1;
+        uint32_t tl = ctypeOf(li, lj, lk), th = ctypeOf(i, j, k);
+        int32_t ws = accW[f], vs = accV[f];
+        float v = ws > 0 ? (float)vs / (float)std::max(ws, 1) : 0.0f;
+        float old = v;
+        if (axis == 1) v -= P.gravity * P.dt;
+        if (tl == 2u || th == 2u) {
+          float sv = 0.0f; int ci = -1;
+          if (tl == 2u) ci = colAtCell(li, lj, lk);
+          if (ci < 0 && th == 2u) ci = colAtCell(i, j, k);
+          V3 fp = facePos(i, j, k, axis);
+          if (ci >= 0) sv = comp(colSurfVel((uint32_t)ci, fp), axis);
+          v = sv; old = sv;
+        }
+        accW[f] = fbits(old); accV[f] = fbits(v);
+      }
+    });
+  }
+  // divergence (wgsl-solver.js:107-123)
+  void stageDivergence() {
+    forActive([&](uint32_t c, int i, int j, int k) {
+      if ((ctype[c] & 0xffu) != 1u) { rhs[c] = 0.0f; return; }
+      float div = (gvR(faceIndex(0, i + 1, j, k)) - gvR(faceIndex(0, i, j, k)) + gvR(faceIndex(1, i, j + 1, k)) - gvR(faceIndex(1, i, j, k)) +
+                   gvR(faceIndex(2, i, j, k + 1)) - gvR(faceIndex(2, i, j, k))) * P.ih;
+      bool interior = true;
+      if (ctypeOf(i - 1, j, k) == 0u || ctypeOf(i + 1, j, k) == 0u || ctypeOf(i, j - 1, k) == 0u || ctypeOf(i, j + 1, k) == 0u ||
+          ctypeOf(i, j, k - 1) == 0u || ctypeOf(i, j, k + 1) == 0u) interior = false;
+      float dens = (float)cnt[c] / P.rest - 1.0f;
+      float tgt = P.comp * (interior ? dens : fmax_(dens, 0.0f));
+      if (P.nb != 0u && phiOf(c) < -1.0f) tgt = 0.0f;
+      rhs[c] = (tgt - div) * P.h * P.h / P.dt;
+    });
+  }
+  // relax / rbRed / rbBlack (wgsl-solver.js:124-140, 162-164), iters x (red, black)
+  void stagePressure(int iters) {
+    for (int it = 0; it < iters; it++) for (uint32_t color = 0; color < 2; color++) {
+      forActive([&](uint32_t c, int i, int j, int k) {
+        if ((uint32_t)((i + j + k) & 1) != color) return;
+        if ((ctype[c] & 0xffu) != 1u) return;
+        float sum = 0.0f, nns = 0.0f;
+        for (int a = 0; a < 6; a++) {
+          int qi = i, qj = j, qk = k;
+          if (a == 0) qi -= 1; else if (a == 1) qi += 1; else if (a == 2) qj -= 1; else if (a == 3) qj += 1; else if (a == 4) qk -= 1; else qk += 1;
+          uint32_t ty = ctypeOf(qi, qj, qk);
+          if (ty == 2u) continue;
+          nns += 1.0f;
+          if (ty == 1u) sum += pres[cellIdx(qi, qj, qk)];
+        }
+        if (nns < 0.5f) { pres[c] = 0.0f; return; }
+        float pg = (rhs[c] + sum) / nns;
+        pres[c] = pres[c] + P.omega * (pg - pres[c]);
+      });
+    }
+  }
+  // project / projBody (wgsl-solver.js:165-180), then saveVel (wgsl-narrowband.js:88-91)
+  void stageProject(bool nb) {
+    forActive([&](uint32_t c, int i, int j, int k) {
+      for (int axis = 0; axis < 3; axis++) {
+        uint32_t f = c * 3 + axis;
+        int li = i, lj = j, lk = k;
+        if (axis == 0) li -= 1; else if (axis == 1) lj -= 1; else lk -= 1;
+        uint32_t tl = ctypeOf(li, lj, lk), th = ctypeOf(i, j, k);
+        if (tl == 2u || th == 2u) continue;
+        if (tl != 1u && th != 1u) continue;
+        float pl = 0.0f, ph = 0.0f;
+        if (tl == 1u) pl = pres[cellIdx(li, lj, lk)];
+        if (th == 1u) ph = pres[cellIdx(i, j, k)];
+        accV[f] = fbits(gvR(f) - P.dt * P.ih * (ph - pl));
+      }
+    });
+    if (nb) forActive([&](uint32_t c, int, int, int) { for (int a = 0; a < 3; a++) velG[c * 3 + a] = gvR(c * 3 + a); });
+  }
+  // sampleBoth (wgsl-core.js:138-154)
+  void sampleBoth(V3 p, V3& vn, V3& vo) const {
+    for (int axis = 0; axis < 3; axis++) {
+      V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+      if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+      V3 f0 = vfloor(g); V3 fr = g - f0; int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+      float sn = 0.0f, so = 0.0f;
+      for (int c = 0; c < 8; c++) {
+        int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+        float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+        uint32_t f = faceIndex(axis, i0 + dx, j0 + dy, k0 + dz);
+        sn += w * gvR(f); so += w * gv0R(f);
+      }
+      setc(vn, axis, sn); setc(vo, axis, so);
+    }
+  }
+  // collideP (wgsl-solver.js:185-197)
+  V3 collideP(V3 pin) const {
+    V3 p = pin; float m = P.margin;
+    for (uint32_t k = 0; k < P.ncols; k++) {
+      if (!colNear(k, p)) continue;
+      float phi; V3 wn; sdfEval(k, p, phi, wn);
+      if (phi < P.q0) p = p + wn * (P.q0 - phi);
+    }
+    float big = 1.0e9f;
+    V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
+    V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
+    return vclamp(p, lo, hi);
+  }
+  static float hsh3(V3 p) {
+    V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f); q = q - vfloor(q); q = q * 17.0f;
+    float r = q.x * q.y * q.z * (q.x + q.y + q.z);
+    return r - floorf(r);
+  }
+  static float vnz(V3 x) {    // value noise (wgsl-solver.js:202-207)
+    V3 i = vfloor(x); V3 fr = x - vfloor(x); V3 u = fr * fr * (v3(3, 3, 3) - fr * 2.0f);
+    float a = mixf(mixf(hsh3(i), hsh3(i + v3(1, 0, 0)), u.x), mixf(hsh3(i + v3(0, 1, 0)), hsh3(i + v3(1, 1, 0)), u.x), u.y);
+    float b = mixf(mixf(hsh3(i + v3(0, 0, 1)), hsh3(i + v3(1, 0, 1)), u.x), mixf(hsh3(i + v3(0, 1, 1)), hsh3(i + v3(1, 1, 1)), u.x), u.y);
+    return mixf(a, b, u.z);
+  }
+  // g2p (wgsl-solver.js:208-275)
+  void stageG2P() {
+    forParticles([&](uint32_t i) {
+      if (pos[i * 4 + 1] < DEADY) return;
+      V3 p = ppos(i); V3 v0 = pvel(i);
+      int fi, fj, fk; particleCell(p, fi, fj, fk);
+      V3 vn = v0 - v3(0.0f, P.gravity * P.dt, 0.0f); V3 vo = v0;
+      if (hasStorage(fi, fj, fk)) sampleBoth(p, vn, vo);
+      V3 v = vmix(vn, v0 + (vn - vo), P.flip);
+      V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+      int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+      float csum = 8.0f * P.rest;
+      bool fast = P.q12 > 0.5f;
+      if (P.q9 < 0.5f && fast) csum = 8.0f * (float)cnt[cellIdx(fi, fj, fk)];
+      else if (P.q9 < 0.5f) {
+        csum = 0.0f;
+        for (int dz = 0; dz <= 1; dz++) for (int dy = 0; dy <= 1; dy++) for (int dx = 0; dx <= 1; dx++) {
+          int a = std::min(std::max(bi + dx, 0), (int)P.nx - 1), b = std::min(std::max(bj + dy, 0), (int)P.ny - 1), c = std::min(std::max(bk + dz, 0), (int)P.nz - 1);
+          csum += (float)cnt[cellIdx(a, b, c)];
+        }
+      }
+      float rho = csum / (8.0f * P.rest);
+      float air = 1.0f - smoothstep(0.008f, 0.1f, rho);
+      float shield = smoothstep(0.1f, 0.65f, rho);
+      float exposure = 1.0f - 0.97f * shield;
+      float spd0 = length(v);
+      float sens = fmax_(P.q6, 0.05f);
+      float pacc = length(vn - vo) / P.dt;
+      float settle = smoothstep(0.1f, 0.5f, P.q8);
+      float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
+      float turb = clampf((length(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
+      float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
+      float tau = fmax_(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstep(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
+      float foam = vel[i * 4 + 3] * expf(-P.dt / tau);
+      foam = fmax_(foam, fmax_(spray * 0.9f, fmax_(impact, turb * 0.8f)));
+      V3 gust = v3(0, 0, 0);
+      if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
+        V3 gp = p * 0.55f; float tt = P.q8 * 0.6f;
+        gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1, 1, 1);
+      }
+      float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
+      V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
+      v = v + (airv - v) * (1.0f - expf(-kd * P.dt));
+      float sp = length(v);
+      if (sp > P.vmax) v = v * (P.vmax / sp);
+      V3 pt = p + v * P.dt;
+      V3 pc = collideP(pt);
+      V3 dsp = pc - pt;
+      if (dot(dsp, dsp) > 1.0e-12f) {
+        V3 nrm = dsp / length(dsp); float vd = dot(v, nrm);
+        if (vd < 0.0f) v = v - nrm * vd;
+      }
+      uint32_t o = P.open;
+      if (o != 0u && (((o & 1u) && pc.x < P.x0) || ((o & 2u) && pc.x > P.x1) || ((o & 4u) && pc.y < P.y0) ||
+                      ((o & 8u) && pc.y > P.y1) || ((o & 16u) && pc.z < P.z0) || ((o & 32u) && pc.z > P.z1))) {
+        pos[i * 4] = 0.0f; pos[i * 4 + 1] = -1.0e6f; pos[i * 4 + 2] = 0.0f; pos[i * 4 + 3] = 0.0f;
+        vel[i * 4] = 0.0f; vel[i * 4 + 1] = 0.0f; vel[i * 4 + 2] = 0.0f; vel[i * 4 + 3] = 0.0f;
+        return;
+      }
+      pos[i * 4] = pc.x; pos[i * 4 + 1] = pc.y; pos[i * 4 + 2] = pc.z;
+      pos[i * 4 + 3] = fmin_(length(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f);
+      vel[i * 4] = v.x; vel[i * 4 + 1] = v.y; vel[i * 4 + 2] = v.z; vel[i * 4 + 3] = foam;
+    });
+  }
+
+  // ---- whitewater (wgsl-whitewater.js:7-23, 92-180) ----
+  float wetCell(int i, int j, int k) const {
+    if (!inDom(i, j, k) || !hasStorage(i, j, k)) return 0.0f;
+    uint32_t ci = cellIdx(i, j, k);
+    if (P.nb != 0u && (ctype[ci] & 0xffu) == 1u && phiOf(ci) < -1.0f) return 1.0f;
+    return fmin_((float)cnt[ci] / P.rest, 1.0f);
+  }
+  float wetAt(V3 p) const {
+    V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
+    V3 f0 = vfloor(g); V3 fr = g - f0; int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    float s = 0.0f;
+    for (int c = 0; c < 8; c++) {
+      int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      if (w > 0.0f) s += w * wetCell(i0 + dx, j0 + dy, k0 + dz);
+    }
+    return s;
+  }
+  void stageSpray(bool emit) {
+    uint32_t m = std::min(sctl0, P.smax);
+    // wwSample
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t jj = 0; jj < (int64_t)m; jj++) {
+      uint32_t j = (uint32_t)jj;
+      if (sPos[j * 4 + 3] <= 0.0f) continue;
+      V3 p = v3(sPos[j * 4], sPos[j * 4 + 1], sPos[j * 4 + 2]); V3 vf = v3(0, 0, 0);
+      int ci, cj, ck; particleCell(p, ci, cj, ck);
+      if (hasStorage(ci, cj, ck)) { V3 vo; sampleBoth(p, vf, vo); }
+      sAux[j * 4] = vf.x; sAux[j * 4 + 1] = vf.y; sAux[j * 4 + 2] = vf.z; sAux[j * 4 + 3] = wetAt(p);
+    }
+    // sprayStep
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t jj = 0; jj < (int64_t)m; jj++) {
+      uint32_t j = (uint32_t)jj;
+      float life = sPos[j * 4 + 3];
+      if (life <= 0.0f) continue;
+      V3 v = v3(sVel[j * 4], sVel[j * 4 + 1], sVel[j * 4 + 2]); float kw = sVel[j * 4 + 3]; uint32_t kind = u32f(kw + 0.5f);
+      float tk = (kw - (float)kind) / 0.4f * WWHOLD; bool settled = tk >= WWHOLD * 0.999f; uint32_t k0 = kind;
+      float wet = sAux[j * 4 + 3]; V3 vf = v3(sAux[j * 4], sAux[j * 4 + 1], sAux[j * 4 + 2]);
+      uint32_t h0 = j * 2654435761u + P.seed * 974711u;
+      if (kind == 0u && v.y < vf.y && wet > 0.55f && tk > 0.05f) { kind = 2u; life = P.wwFoamLife * (0.6f + 0.8f * hash1(h0)); v = vf; }
+      else if (kind == 1u && wet > 0.55f) { life = 0.0f; }
+      else if (kind == 2u && wet > 0.97f && settled) { kind = 3u; }
+      else if (kind == 2u && wet < 0.04f && settled) { kind = 0u; life = fmin_(life, P.sprLife); }
+      else if (kind == 3u && wet < 0.6f && settled) { kind = 2u; life = fmax_(life, 0.5f * P.wwFoamLife); }
+      if (kind != k0) tk = 0.0f; else tk = fmin_(tk + P.dt, WWHOLD);
+      V3 p = v3(sPos[j * 4], sPos[j * 4 + 1], sPos[j * 4 + 2]);
+      if (kind <= 1u) {
+        bool mist = kind == 1u;
+        V3 gust = v3(0, 0, 0);
+        if (P.q7 > 0.0f) {
+          V3 gp = p * 0.55f * P.vs; float tt = P.q8 * 0.6f;
+          gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1, 1, 1);
+        }
+        V3 base = v3(P.q1, P.q2, P.q3);
+        V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
+        v.y -= P.gravity * P.dt;
+        v = v + (airv - v) * (1.0f - expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
+        life -= P.dt;
+      } else if (kind == 2u) {
+        float vy = vf.y + clampf((wet - 0.5f) * 4.0f, -1.0f, 1.0f) * P.h * 4.0f;
+        v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - expf(-10.0f * P.dt));
+        life -= P.dt;
+      } else {
+        v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - expf(-6.0f * P.dt));
+        life -= 0.3f * P.dt;
+      }
+      V3 np = p + v * P.dt;
+      if (np.x < P.x0 || np.x > P.x1 || np.y < P.y0 || np.y > P.y1 || np.z < P.z0 || np.z > P.z1) life = 0.0f;
+      else if (P.ncols > 0u && colAt(np) >= 0) life = 0.0f;
+      sPos[j * 4] = np.x; sPos[j * 4 + 1] = np.y; sPos[j * 4 + 2] = np.z; sPos[j * 4 + 3] = life;
+      sVel[j * 4] = v.x; sVel[j * 4 + 1] = v.y; sVel[j * 4 + 2] = v.z; sVel[j * 4 + 3] = (float)kind + 0.4f * tk / WWHOLD;
+    }
+    if (!emit) return;
+    // sprayEmit (wgsl-whitewater.js:101-133). Canonical order: particles by storage index, points by m; the ring
+    // counter advances once per point tried; a slot is taken only if it was not living before this pass.
+    if (P.smax == 0u || P.sprRate <= 0.0f) return;
+    std::vector<uint32_t> kcount(P.n, 0);
+    std::vector<float> rhov(P.n, 0.0f);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t ii = 0; ii < (int64_t)P.n; ii++) {
+      uint32_t i = (uint32_t)ii;
+      if (pos[i * 4 + 1] < DEADY) continue;
+      V3 q = ppos(i); V3 v = pvel(i); float foam = vel[i * 4 + 3]; float spd = length(v);
+      float fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
+      V3 bcf = vfloor((q - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+      int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+      float rho = 0.0f;
+      for (int dz = 0; dz <= 1; dz++) for (int dy = 0; dy <= 1; dy++) for (int dx = 0; dx <= 1; dx++) rho += wetCell(bi + dx, bj + dy, bk + dz);
+      rho = rho / 8.0f;
+      float crest = (1.0f - smoothstep(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
+      float churn = (1.0f - smoothstep(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstep(0.5f, 1.5f, spd * P.vs);
+      float e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstep(0.1f, 0.5f, P.q8);
+      if (e <= 0.0f) continue;
+      uint32_t h0 = pid[i] * 747796405u + P.seed * 2891336453u;
+      float kf = floorf(P.sprRate * e * P.dt + hash1(h0));
+      kcount[i] = std::min(u32f(kf), 4u); rhov[i] = rho;
+    }
+    uint64_t tried = 0; for (uint32_t i = 0; i < P.n; i++) tried += kcount[i];
+    if (tried > P.smax) spray_ovf++;
+    std::vector<float> lifeBefore(P.smax);
+    for (uint32_t j = 0; j < P.smax; j++) lifeBefore[j] = sPos[j * 4 + 3];
+    uint64_t run = 0;
+    for (uint32_t i = 0; i < P.n; i++) {
+      for (uint32_t mm = 0; mm < kcount[i]; mm++, run++) {
+        if (run >= P.smax) continue;   // more points tried in one step than the ring holds: the rest are dropped
+        uint32_t slot = (uint32_t)((sctl0 + run) % P.smax);
+        if (lifeBefore[slot] > 0.0f) continue;
+        V3 q = ppos(i); V3 v = pvel(i); float spd = length(v); float rho = rhov[i];
+        float fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
+        uint32_t h0 = pid[i] * 747796405u + P.seed * 2891336453u;
+        uint32_t hh = h0 ^ ((mm + 1u) * 0x9E3779B9u);
+        float z = hash1(hh + 1u) * 2.0f - 1.0f; float a = hash1(hh + 2u) * 6.2831853f; float s = sqrtf(fmax_(0.0f, 1.0f - z * z));
+        V3 dir = v3(s * cosf(a), s * sinf(a), z);
+        bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
+        bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
+        V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
+        float life = P.sprLife * (0.6f + 0.8f * hash1(hh + 5u)) * (mist ? 1.6f : 1.0f);
+        float kind = mist ? 1.0f : 0.0f;
+        if (under) { nv = v + dir * spd * 0.05f; life = P.wwFoamLife * (0.6f + 0.8f * hash1(hh + 5u)); kind = 3.0f; }
+        V3 np = q + nv * P.dt + dir * P.h * 0.3f * hash1(hh + 6u);
+        sPos[slot * 4] = np.x; sPos[slot * 4 + 1] = np.y; sPos[slot * 4 + 2] = np.z; sPos[slot * 4 + 3] = life;
+        sVel[slot * 4] = nv.x; sVel[slot * 4 + 1] = nv.y; sVel[slot * 4 + 2] = nv.z; sVel[slot * 4 + 3] = kind;
+      }
+    }
+    sctl0 = (uint32_t)(sctl0 + tried);
+  }
+
+  // ---- narrow band reseed (wgsl-narrowband.js:93-148) ----
+  void stageReseed() {
+    forParticles([&](uint32_t i) {                       // nbKill
+      if (pos[i * 4 + 1] < DEADY) return;
+      V3 q = ppos(i);
+      bool kill = false;
+      if (P.nb != 0u && calmV(pvel(i))) {
+        int ci, cj, ck; particleCell(q, ci, cj, ck);
+        if (hasStorage(ci, cj, ck) && phiOf(cellIdx(ci, cj, ck)) < -P.band) kill = true;
+      }
+      if (kill) { for (int a = 0; a < 4; a++) { pos[i * 4 + a] = 0.0f; vel[i * 4 + a] = 0.0f; } pos[i * 4 + 1] = -1.0e6f; }
+    });
+    std::vector<uint32_t> dead;                          // nbDead: ascending storage index
+    for (uint32_t i = 0; i < P.n; i++) if (pos[i * 4 + 1] < DEADY && dead.size() < P.lcap) dead.push_back(i);
+    struct Def { int i, j, k; uint32_t need; };
+    std::vector<Def> defs;                               // nbDeficit: ascending cell key
+    for (uint32_t tile : active) for (uint32_t local = 0; local < 512; local++) {
+      int i, j, k; tileCoord(tile, local, i, j, k); uint32_t c = tile * 512 + local;
+      if (!inDom(i, j, k) || colBits(c) != 0u) continue;
+      V3 cx = cellCenter(i, j, k); float ph = phiOf(c);
+      if ((ctype[c] & 0xffu) != 1u || ph > -1.0f || ph < -P.band) continue;
+      if (!calmV(velGVec(cx))) continue;
+      uint32_t n = (uint32_t)std::max(cnt[c], 0);
+      if ((float)n >= 0.55f * P.rest) continue;
+      uint32_t nd = std::min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
+      if (defs.size() >= P.lcap / 2u) continue;
+      defs.push_back({i, j, k, nd});
+    }
+    uint32_t avail = std::min((uint32_t)dead.size(), P.lcap);
+    uint32_t base = 0;
+    for (uint32_t e = 0; e < (uint32_t)defs.size(); e++) {   // nbSpawn
+      V3 cp = v3((float)defs[e].i, (float)defs[e].j, (float)defs[e].k);
+      for (uint32_t m = 0; m < defs[e].need; m++) {
+        uint32_t k = base + m; if (k >= avail) break;
+        uint32_t i = dead[k];
+        uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
+        V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
+        V3 v = velGVec(x);
+        pos[i * 4] = x.x; pos[i * 4 + 1] = x.y; pos[i * 4 + 2] = x.z; pos[i * 4 + 3] = fmin_(length(v), 63.0f);
+        vel[i * 4] = v.x; vel[i * 4 + 1] = v.y; vel[i * 4 + 2] = v.z; vel[i * 4 + 3] = 0.0f;
+      }
+      base += defs[e].need;
+    }
+  }
+
+  // ---- FlipSim.step (sim.js:179-241, stage list :245-310) ----
+  st_status step(double dt, const st_step_opts* o) {
+    if (N == 0) return ST_NOT_READY;
+    bool nbOn = o->nb_on != 0;
+    if (nbOn && !velGOn) velGOn = true;
+    uint32_t init = nbOn && nbInit ? nbInit : 0;
+    packCols(o);
+    bool sprOn = o->spray_on != 0 && sprayCap > 0;
+    seed = seed + 1u;
+    packParams(dt, o, init, nbOn, sprOn);
+    tm = tm + dt;
+    if (init) { nbInit = 0; fillsPacked.clear(); }
+    int iters = std::max(1, o->iters);
+    stageBlocks(nbOn, init);
+    stageClear();
+    stageSort();
+    stageP2G();
+    if (nbOn) stageNarrowBand();
+    stageClassify();
+    if (nbOn) stageNbVel();
+    stageNormFaces();
+    stageDivergence();
+    stagePressure(iters);
+    stageProject(nbOn);
+    stageG2P();
+    if (sprayCap > 0) stageSpray(sprOn);
+    if (nbOn) stageReseed();
+    steps++;
+    return ST_OK;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void oracle_step_opts_default(st_step_opts* o);
+
+st_status oracle_flip_create(const st_flip_desc* desc, void** out) {
+  if (!desc || !out || desc->size != sizeof(st_flip_desc) || desc->d <= 0 || desc->max_n == 0) return ST_BAD_ARG;
+  Oracle* s = new Oracle();
+  s->create(desc);
+  *out = s;
+  return ST_OK;
+}
+void oracle_flip_destroy(void* h) { delete (Oracle*)h; }
+void oracle_flip_set_threads(void* h, int n) { ((Oracle*)h)->nthreads = n < 1 ? 1 : n; }
+st_status oracle_flip_clear(void* h) { ((Oracle*)h)->clear(); return ST_OK; }
+st_status oracle_flip_set_cap(void* h, uint32_t c) {
+  Oracle* s = (Oracle*)h; s->cap = std::min(c, s->maxN); if (s->N > s->cap) s->N = s->cap; if (s->ring >= s->cap) s->ring = 0; return ST_OK;
+}
+st_status oracle_flip_add(void* h, const float* p3, const float* v3_, uint32_t n, uint32_t* added) {
+  Oracle* s = (Oracle*)h; uint32_t k = 0;
+  for (; k < n; k++) if (!s->add(p3[k * 3], p3[k * 3 + 1], p3[k * 3 + 2], v3_[k * 3], v3_[k * 3 + 1], v3_[k * 3 + 2])) break;
+  if (added) *added = k;
+  return ST_OK;
+}
+st_status oracle_flip_step(void* h, double dt, const st_step_opts* o) {
+  if (!o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
+  return ((Oracle*)h)->step(dt, o);
+}
+st_status oracle_flip_read_particles(void* h, float* pos4, float* vel4, uint32_t cap, uint32_t* n) {
+  Oracle* s = (Oracle*)h; if (n) *n = s->N;
+  for (uint32_t i = 0; i < s->N; i++) {
+    uint32_t id = s->pid[i]; if (id >= cap) continue;
+    if (pos4) memcpy(&pos4[(size_t)id * 4], &s->pos[(size_t)i * 4], 16);
+    if (vel4) memcpy(&vel4[(size_t)id * 4], &s->vel[(size_t)i * 4], 16);
+  }
+  return ST_OK;
+}
+st_status oracle_flip_read_spray(void* h, float* pos4, float* vel4, uint32_t cap, uint32_t* n) {
+  Oracle* s = (Oracle*)h; uint32_t m = std::max(1u, std::min(s->sprayCap, s->sctl0)); if (!s->sprayCap) m = 0;
+  if (n) *n = m;
+  for (uint32_t j = 0; j < m && j < cap; j++) {
+    if (pos4) memcpy(&pos4[j * 4], &s->sPos[j * 4], 16);
+    if (vel4) memcpy(&vel4[j * 4], &s->sVel[j * 4], 16);
+  }
+  return ST_OK;
+}
+st_status oracle_flip_stats(void* h, st_stats* o) {
+  Oracle* s = (Oracle*)h;
+  o->sc = s->st_sc; o->ovf = s->st_ovf; o->fluid = s->st_fluid; o->vmax = s->st_vmax; o->n = s->N;
+  uint32_t live = 0; for (uint32_t i = 0; i < s->N; i++) if (s->pos[i * 4 + 1] >= DEADY) live++;
+  o->live = live; o->spray_used = s->sctl0; o->steps = s->steps;
+  return ST_OK;
+}
+st_status oracle_flip_get_dims(void* h, st_flip_dims* o) {
+  Oracle* s = (Oracle*)h;
+  o->nx = s->nx; o->ny = s->ny; o->nz = s->nz; o->tx = s->tx; o->ty = s->ty; o->tz = s->tz;
+  o->h = (float)s->h; o->x0 = (float)s->bx0; o->y0 = (float)s->by0; o->z0 = (float)s->bz0; o->x1 = (float)s->bx1; o->y1 = (float)s->by1; o->z1 = (float)s->bz1;
+  return ST_OK;
+}
+st_status oracle_flip_read_grid(void* h, const st_flip_grid* g) {
+  Oracle* s = (Oracle*)h;
+  uint32_t NX = s->tx * 8, NY = s->ty * 8, NZ = s->tz * 8;
+  if (g->tile_on) for (int t = 0; t < s->ntiles; t++) g->tile_on[t] = s->alloc[t];
+  for (uint32_t k = 0; k < NZ; k++) for (uint32_t j = 0; j < NY; j++) for (uint32_t i = 0; i < NX; i++) {
+    size_t o = (size_t)i + NX * ((size_t)j + NY * k);
+    uint32_t c = s->cellIdx((int)i, (int)j, (int)k);
+    bool spare = (c >> 9) == s->spare();
+    if (g->cnt) g->cnt[o] = spare ? 0 : s->cnt[c];
+    if (g->ctype) g->ctype[o] = spare ? 0 : s->ctype[c];
+    if (g->pres) g->pres[o] = spare ? 0.0f : s->pres[c];
+    if (g->rhs) g->rhs[o] = spare ? 8.0f : s->rhs[c];
+    for (int a = 0; a < 3; a++) {
+      if (g->vn) g->vn[o * 3 + a] = spare ? 0.0f : bitsf(s->accV[c * 3 + a]);
+      if (g->vo) g->vo[o * 3 + a] = spare ? 0.0f : bitsf(s->accW[c * 3 + a]);
+      if (g->velg) g->velg[o * 3 + a] = spare ? 0.0f : s->velG[c * 3 + a];
+    }
+  }
+  return ST_OK;
+}
+st_status oracle_flip_save_state(void* h, float* pos4, float* vel4, uint32_t* pid, uint32_t cap, uint32_t* n) {
+  Oracle* s = (Oracle*)h; if (n) *n = s->N;
+  uint32_t m = std::min(cap, s->N);
+  if (pos4) memcpy(pos4, s->pos.data(), (size_t)m * 16);
+  if (vel4) memcpy(vel4, s->vel.data(), (size_t)m * 16);
+  if (pid) memcpy(pid, s->pid.data(), (size_t)m * 4);
+  return ST_OK;
+}
+st_status oracle_flip_load_state(void* h, const float* pos4, const float* vel4, const uint32_t* pid, uint32_t n, double t, uint32_t seed) {
+  Oracle* s = (Oracle*)h; if (n > s->maxN) return ST_BAD_ARG;
+  s->N = n; s->ring = 0;
+  memcpy(s->pos.data(), pos4, (size_t)n * 16); memcpy(s->vel.data(), vel4, (size_t)n * 16); memcpy(s->pid.data(), pid, (size_t)n * 4);
+  s->tm = t; s->seed = seed;
+  return ST_OK;
+}
+st_status oracle_flip_nb_fills(void* h, const float* boxes6, uint32_t nbox, const float* sph4, uint32_t nsph, uint32_t mode) {
+  Oracle* s = (Oracle*)h;
+  s->fillsPacked.clear();
+  for (uint32_t k = 0; k < nbox; k++) {
+    const float* b = &boxes6[k * 6];
+    float f[8] = {1, b[0], b[1], b[2], b[3], b[4], b[5], 0}; s->fillsPacked.insert(s->fillsPacked.end(), f, f + 8);
+  }
+  for (uint32_t k = 0; k < nsph; k++) {
+    const float* q = &sph4[k * 4];
+    float f[8] = {2, q[0], q[1], q[2], q[3], 0, 0, 0}; s->fillsPacked.insert(s->fillsPacked.end(), f, f + 8);
+  }
+  s->nbInit = mode ? mode : 1;
+  return ST_OK;
+}
+uint32_t oracle_flip_spray_overflow(void* h) { return ((Oracle*)h)->spray_ovf; }
+
+}  // extern "C"

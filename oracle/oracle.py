@@ -1,0 +1,48 @@
+"""Python handle on the CPU oracle (oracle/flip_oracle.cpp), for tests, smoke() and bench.py's CPU baseline only.
+
+OracleFlipSim has the same methods as splashtank_b200.flip.FlipSim because the oracle library exports the same
+C entry points under the prefix ``oracle_``.  The oracle is the checker, never the thing measured as the product.
+"""
+import ctypes as C
+import os
+import subprocess
+
+from splashtank_b200 import abi
+from splashtank_b200.flip import FlipSim
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_FUNCS = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE, os.path.join(HERE, "liboracle_flip.so"), os.path.join(HERE, "liboracle_pbf.so")], check=True)
+
+
+def funcs():
+    global _FUNCS
+    if _FUNCS is None:
+        path = os.path.join(HERE, "liboracle_flip.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        f = abi.bind(lib, "oracle_", abi.FLIP_FUNCS)
+        f["set_threads"] = lib.oracle_flip_set_threads
+        f["set_threads"].argtypes = [C.c_void_p, C.c_int]
+        f["set_threads"].restype = None
+        f["spray_overflow"] = lib.oracle_flip_spray_overflow
+        f["spray_overflow"].argtypes = [C.c_void_p]
+        f["spray_overflow"].restype = C.c_uint32
+        _FUNCS = f
+    return _FUNCS
+
+
+class OracleFlipSim(FlipSim):
+    def __init__(self, *a, threads=1, **k):
+        super().__init__(*a, _funcs=funcs(), **k)
+        self.set_threads(threads)
+
+    def set_threads(self, n):
+        self.f["set_threads"](self._h, int(n))
+
+    def stepTimed(self, dt, o):
+        raise NotImplementedError("the oracle has no stage timer")

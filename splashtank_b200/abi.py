@@ -1,0 +1,143 @@
+"""ctypes mirror of include/splashtank_cuda.h (the C ABI of the FLIP step and the PBF solver).
+
+Only plain data crosses the boundary: pointers, sizes and the POD structs below, so the same
+declarations bind any library that exports the header's functions (the CUDA library here; a
+Node N-API shim binds the same symbols).
+"""
+import ctypes as C
+
+ST_OK, ST_NOT_READY, ST_POOL_GREW, ST_OVERFLOW, ST_OOM, ST_BAD_ARG, ST_DEVICE_ERROR, ST_TIMEOUT, ST_UNSUPPORTED = range(9)
+STATUS_NAMES = ["OK", "NOT_READY", "POOL_GREW", "OVERFLOW", "OOM", "BAD_ARG", "DEVICE_ERROR", "TIMEOUT", "UNSUPPORTED"]
+ST_OPT_NO_FOAM, ST_OPT_NO_CULL, ST_OPT_FAST_AIR = 1, 2, 4
+
+f32p = C.POINTER(C.c_float)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+u8p = C.POINTER(C.c_uint8)
+
+
+class FlipDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("d", C.c_double), ("ratio", C.c_double), ("box", C.c_double * 3),
+                ("open", C.c_uint32), ("max_n", C.c_uint32), ("spray_cap", C.c_uint32), ("device", C.c_int32)]
+
+
+class Sdf(C.Structure):
+    _fields_ = [("id", C.c_uint32), ("dims", C.c_uint32 * 3), ("origin", C.c_float * 3), ("cell", C.c_float), ("data", f32p)]
+
+
+class Collider(C.Structure):
+    _fields_ = [("sdf", C.POINTER(Sdf)), ("pos", C.c_float * 3), ("R", C.c_float * 9), ("vel", C.c_float * 3), ("ang", C.c_float * 3)]
+
+
+class SprayOpts(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("rate", "min", "life", "mist", "drag", "mdrag", "foam_life", "rise", "crest", "impact")]
+
+
+class StepOpts(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("g", C.c_float), ("flip", C.c_float), ("comp", C.c_float), ("omega", C.c_float),
+                ("vmax", C.c_float), ("wind", C.c_float * 3), ("drag", C.c_float), ("foam_tau", C.c_float),
+                ("foam_sens", C.c_float), ("gust", C.c_float), ("tear", C.c_float), ("vs", C.c_float), ("iters", C.c_int32),
+                ("flags", C.c_uint32), ("ncols", C.c_uint32), ("cols", C.POINTER(Collider)), ("spray_on", C.c_int32),
+                ("spray", SprayOpts), ("nb_on", C.c_int32), ("nb_band", C.c_float)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("sc", C.c_uint32), ("ovf", C.c_uint32), ("fluid", C.c_uint32), ("vmax", C.c_float), ("n", C.c_uint32),
+                ("live", C.c_uint32), ("spray_used", C.c_uint32), ("steps", C.c_uint32)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("tile_on", u8p), ("cnt", i32p), ("ctype", u32p), ("pres", f32p), ("rhs", f32p), ("vn", f32p), ("vo", f32p), ("velg", f32p)]
+
+
+class Dims(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32), ("tx", C.c_uint32), ("ty", C.c_uint32), ("tz", C.c_uint32),
+                ("h", C.c_float), ("x0", C.c_float), ("y0", C.c_float), ("z0", C.c_float), ("x1", C.c_float), ("y1", C.c_float), ("z1", C.c_float)]
+
+
+STAGES = ("sort", "blocks", "clear", "p2g", "narrow_band", "classify", "norm_faces", "divergence", "pressure", "project", "g2p",
+          "spray", "reseed", "total")
+
+
+class StageTimes(C.Structure):
+    _fields_ = [(n, C.c_float) for n in STAGES]
+
+
+class PbfDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("d", C.c_double), ("box", C.c_double * 3), ("open", C.c_uint32), ("max_n", C.c_uint32),
+                ("device", C.c_int32), ("eps_k", C.c_double), ("wall_k", C.c_double)]
+
+
+class PbfCol(C.Structure):
+    _fields_ = [("kind", C.c_int32)] + [(n, C.c_float) for n in ("x", "y", "z", "r", "hx", "hy", "hz", "yaw")]
+
+
+class PbfOpts(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("g", C.c_float), ("visc", C.c_float), ("iters", C.c_int32), ("ncols", C.c_uint32),
+                ("cols", C.POINTER(PbfCol))]
+
+
+# (name, restype, argtypes) with the prefix left off; "h" stands for the opaque handle
+FLIP_FUNCS = [
+    ("flip_create", C.c_int, [C.POINTER(FlipDesc), C.POINTER(C.c_void_p)]),
+    ("flip_destroy", None, [C.c_void_p]),
+    ("flip_clear", C.c_int, [C.c_void_p]),
+    ("flip_set_cap", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("flip_add", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("flip_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepOpts)]),
+    ("flip_read_particles", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("flip_read_spray", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("flip_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("flip_read_grid", C.c_int, [C.c_void_p, C.POINTER(Grid)]),
+    ("flip_get_dims", C.c_int, [C.c_void_p, C.POINTER(Dims)]),
+    ("flip_save_state", C.c_int, [C.c_void_p, f32p, f32p, u32p, C.c_uint32, u32p]),
+    ("flip_load_state", C.c_int, [C.c_void_p, f32p, f32p, u32p, C.c_uint32, C.c_double, C.c_uint32]),
+    ("flip_nb_fills", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p, C.c_uint32, C.c_uint32]),
+]
+CUDA_ONLY_FUNCS = [
+    ("step_opts_default", None, [C.POINTER(StepOpts)]),
+    ("flip_step_timed", C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepOpts), C.POINTER(StageTimes)]),
+    ("flip_stream", C.c_void_p, [C.c_void_p]),
+    ("abi_version", C.c_uint32, []),
+    ("last_error", C.c_char_p, []),
+]
+PBF_FUNCS = [
+    ("pbf_create", C.c_int, [C.POINTER(PbfDesc), C.POINTER(C.c_void_p)]),
+    ("pbf_destroy", None, [C.c_void_p]),
+    ("pbf_add", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("pbf_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(PbfOpts)]),
+    ("pbf_read", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("pbf_stream", C.c_void_p, [C.c_void_p]),
+]
+
+
+def bind(lib, prefix, funcs):
+    """Set restype/argtypes of prefix+name for every entry; returns {name: function}."""
+    out = {}
+    for name, res, args in funcs:
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+        out[name] = fn
+    return out
+
+
+def default_opts():
+    """st_step_opts_default in Python (src/flip/sim.js:197-230 defaults)."""
+    o = StepOpts()
+    o.size = C.sizeof(StepOpts)
+    o.g = 9.81
+    o.flip = 0.95
+    o.comp = 6.0
+    o.omega = 0.0
+    o.vmax = 14.0
+    o.foam_tau = 1.2
+    o.foam_sens = 1.0
+    o.vs = 1.0
+    o.iters = 30
+    o.spray.foam_life = 3.0
+    o.spray.rise = 0.3
+    o.spray.crest = 1.0
+    o.spray.impact = 0.5
+    o.nb_band = 3.0
+    return o

@@ -1,0 +1,549 @@
+// capi.cu - the C ABI of include/splashtank_cuda.h for the FLIP step: handle, device memory, the parameter block
+// and the stage sequence of one step (FlipSim.step, src/flip/sim.js:179-310).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/splashtank_cuda.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace st;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+void set_err(const char* what, cudaError_t e) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) {                      \
+      set_err(#call, e_);                         \
+      return e_ == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR; \
+    }                                             \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+struct st_flip {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 148;
+  // geometry, fixed at create (src/flip/sim.js:47-61)
+  double d = 0, ratio = 2, h = 0, rest = 8;
+  int nx = 0, ny = 0, nz = 0, tx = 0, ty = 0, tz = 0;
+  uint32_t ntiles = 0, ncell = 0;
+  double bx0 = 0, bx1 = 0, by0 = 0, by1 = 0, bz0 = 0, bz1 = 0;
+  uint32_t open = 0, maxN = 0, cap = 0, N = 0, ring = 0, sprayCap = 0;
+  bool recycle = true;
+  // host-side step state
+  double tm = 0;
+  uint32_t seed = 0, steps = 0, stamp = 0, parity = 0;
+  bool velGOn = false;
+  uint32_t nbInit = 0;
+  std::vector<float> fills;
+  std::string sdfSig;
+  size_t sdfCap = 0;
+  FlipParams hp{};
+  // device memory
+  FlipParams* dP = nullptr;
+  Ctl* dCtl = nullptr;
+  Ctl* hCtl = nullptr;   // pinned
+  Part* part[2] = {nullptr, nullptr};
+  uint32_t* ids[2] = {nullptr, nullptr};
+  uint32_t *key = nullptr, *rank = nullptr, *srcIdx = nullptr, *spid = nullptr, *blkDead = nullptr;
+  uint32_t *need = nullptr, *blkTiles = nullptr, *active = nullptr, *tileSlot = nullptr, *dropped = nullptr;
+  uint32_t *tileCnt = nullptr, *tileAux = nullptr, *tileAux2 = nullptr;
+  uint8_t *on = nullptr, *tstate = nullptr;
+  int32_t* cnt[2] = {nullptr, nullptr};
+  uint32_t *cellOff = nullptr, *ctype = nullptr;
+  float *pres = nullptr, *rhs = nullptr, *vn = nullptr, *vo = nullptr, *velG = nullptr;
+  int32_t* acc = nullptr;
+  uint16_t* sorInfo = nullptr;
+  float4* cols = nullptr;
+  float* sdf = nullptr;
+  float4 *sPos = nullptr, *sVel = nullptr;
+  uint8_t* emitK = nullptr;
+  uint32_t *blkEmit = nullptr, *deadList = nullptr;
+  cudaEvent_t ev[16] = {};
+  int cur = 0;   // part[cur] holds this step's storage order
+
+  Bufs bufs() const {
+    Bufs B{};
+    B.P = dP; B.ctl = dCtl;
+    B.pa = part[cur]; B.pb = part[cur ^ 1]; B.ida = ids[cur]; B.idb = ids[cur ^ 1];
+    B.key = key; B.rank = rank; B.srcIdx = srcIdx; B.spid = spid; B.blkDead = blkDead;
+    B.need = need; B.on = on; B.tstate = tstate; B.blkTiles = blkTiles; B.active = active; B.prevActive = nullptr;
+    B.tileSlot = tileSlot; B.dropped = dropped; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2;
+    B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
+    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cols = cols; B.sdf = sdf;
+    B.sPos = sPos; B.sVel = sVel; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
+    B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
+    return B;
+  }
+  int tileGrid(int per_sm) const { return std::max(1, std::min<int>(sms * per_sm, (int)ntiles)); }
+};
+
+extern "C" {
+
+uint32_t st_abi_version(void) { return ST_ABI_VERSION; }
+const char* st_last_error(void) { return g_err; }
+
+void st_step_opts_default(st_step_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->size = sizeof(st_step_opts);
+  o->g = 9.81f; o->flip = 0.95f; o->comp = 6.0f; o->omega = 0.0f; o->vmax = 14.0f;
+  o->foam_tau = 1.2f; o->foam_sens = 1.0f; o->vs = 1.0f; o->iters = 30;
+  o->spray.foam_life = 3.0f; o->spray.rise = 0.3f; o->spray.crest = 1.0f; o->spray.impact = 0.5f;
+  o->nb_band = 3.0f;
+}
+
+void st_flip_destroy(st_flip* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  void* ptrs[] = {s->dP, s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
+                  s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->tileCnt, s->tileAux, s->tileAux2, s->on, s->tstate,
+                  s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo, s->cols,
+                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  if (s->hCtl) cudaFreeHost(s->hCtl);
+  for (auto& e : s->ev) if (e) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static st_status reset_ids(st_flip* s) {
+  for (int b = 0; b < 2; b++) launch_iota(s->ids[b], s->maxN, s->stream);
+  return ST_OK;
+}
+
+st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
+  if (!desc || !out || desc->size != sizeof(st_flip_desc) || !(desc->d > 0) || desc->max_n == 0) return ST_BAD_ARG;
+  st_flip* s = new st_flip();
+  *out = nullptr;
+  s->device = desc->device;
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) { set_err("cudaSetDevice", e); delete s; return ST_DEVICE_ERROR; }
+  cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
+  s->d = desc->d;
+  double r = desc->ratio != 0 ? desc->ratio : 2.0;
+  s->ratio = std::max(1.4, std::min(4.0, r));
+  s->h = s->ratio * s->d;
+  s->rest = s->ratio * s->ratio * s->ratio;
+  double sz[3] = {3, 2.6, 3};
+  if (desc->box[0] > 0 && desc->box[1] > 0 && desc->box[2] > 0) { sz[0] = desc->box[0]; sz[1] = desc->box[1]; sz[2] = desc->box[2]; }
+  // Math.round in the reference rounds halves up
+  s->nx = std::max(4, (int)std::floor(sz[0] / s->h + 0.5));
+  s->ny = std::max(4, (int)std::floor(sz[1] / s->h + 0.5));
+  s->nz = std::max(4, (int)std::floor(sz[2] / s->h + 0.5));
+  double W = s->nx * s->h, H = s->ny * s->h, D = s->nz * s->h;
+  s->bx0 = -W / 2; s->bx1 = W / 2; s->by0 = 0; s->by1 = H; s->bz0 = -D / 2; s->bz1 = D / 2;
+  s->tx = (s->nx + 1 + 7) / 8; s->ty = (s->ny + 1 + 7) / 8; s->tz = (s->nz + 1 + 7) / 8;
+  s->ntiles = (uint32_t)(s->tx * s->ty * s->tz);
+  s->ncell = s->ntiles * 512u;
+  s->open = desc->open; s->maxN = desc->max_n; s->cap = desc->max_n; s->sprayCap = desc->spray_cap;
+  const size_t M = s->maxN, T = s->ntiles, C = s->ncell, NB = (M + PBLK - 1) / PBLK;
+  st_status st = ST_OK;
+  auto A = [&](cudaError_t ee, const char* what) { if (ee != cudaSuccess && st == ST_OK) { set_err(what, ee); st = ee == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR; } };
+  A(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  A(dalloc(&s->dP, 1), "params"); A(dalloc(&s->dCtl, 1), "ctl"); A(cudaMallocHost((void**)&s->hCtl, sizeof(Ctl)), "ctl host");
+  for (int b = 0; b < 2; b++) { A(dalloc(&s->part[b], M), "particles"); A(dalloc(&s->ids[b], M), "ids"); A(dalloc(&s->cnt[b], C), "cnt"); }
+  A(dalloc(&s->key, M), "key"); A(dalloc(&s->rank, M), "rank"); A(dalloc(&s->srcIdx, M), "srcIdx"); A(dalloc(&s->spid, M), "spid");
+  A(dalloc(&s->blkDead, NB + 1), "blkDead"); A(dalloc(&s->blkEmit, NB + 1), "blkEmit"); A(dalloc(&s->emitK, M), "emitK");
+  A(dalloc(&s->deadList, M), "deadList");
+  A(dalloc(&s->need, T), "need"); A(dalloc(&s->on, T), "on"); A(dalloc(&s->tstate, T), "tstate"); A(dalloc(&s->blkTiles, (T + 1023) / 1024 + 1), "blkTiles");
+  A(dalloc(&s->active, T), "active"); A(dalloc(&s->tileSlot, T), "tileSlot"); A(dalloc(&s->dropped, T), "dropped");
+  A(dalloc(&s->tileCnt, T + 1), "tileCnt"); A(dalloc(&s->tileAux, T + 1), "tileAux"); A(dalloc(&s->tileAux2, T + 1), "tileAux2");
+  A(dalloc(&s->cellOff, C), "cellOff"); A(dalloc(&s->ctype, C), "ctype"); A(dalloc(&s->pres, C), "pres"); A(dalloc(&s->rhs, C), "rhs");
+  A(dalloc(&s->acc, 6 * C), "acc"); A(dalloc(&s->vn, 3 * C), "vn"); A(dalloc(&s->vo, 3 * C), "vo"); A(dalloc(&s->velG, 3 * C), "velG");
+  A(dalloc(&s->sorInfo, C), "sorInfo"); A(dalloc(&s->cols, 32 * 8), "cols"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
+  A(dalloc(&s->sPos, std::max<size_t>(s->sprayCap, 1)), "sPos"); A(dalloc(&s->sVel, std::max<size_t>(s->sprayCap, 1)), "sVel");
+  for (auto& ev : s->ev) A(cudaEventCreate(&ev), "event");
+  if (st != ST_OK) { st_flip_destroy(s); return st; }
+  // every tile starts in the state the reference's spare slot reads as
+  cudaStream_t q = s->stream;
+  A(cudaMemsetAsync(s->dCtl, 0, sizeof(Ctl), q), "memset");
+  for (int b = 0; b < 2; b++) { A(cudaMemsetAsync(s->part[b], 0, M * sizeof(Part), q), "memset"); A(cudaMemsetAsync(s->cnt[b], 0, C * 4, q), "memset"); }
+  A(cudaMemsetAsync(s->need, 0, T * 4, q), "memset"); A(cudaMemsetAsync(s->on, 0, T, q), "memset");
+  A(cudaMemsetAsync(s->ctype, 0, C * 4, q), "memset"); A(cudaMemsetAsync(s->pres, 0, C * 4, q), "memset");
+  A(cudaMemsetAsync(s->acc, 0, 6 * C * 4, q), "memset"); A(cudaMemsetAsync(s->vn, 0, 3 * C * 4, q), "memset");
+  A(cudaMemsetAsync(s->vo, 0, 3 * C * 4, q), "memset"); A(cudaMemsetAsync(s->velG, 0, 3 * C * 4, q), "memset");
+  A(cudaMemsetAsync(s->sorInfo, 0, C * 2, q), "memset");
+  A(cudaMemsetAsync(s->sPos, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
+  A(cudaMemsetAsync(s->sVel, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
+  launch_fill_f32(s->rhs, 8.0f, C, q);
+  reset_ids(s);
+  A(cudaStreamSynchronize(q), "create sync");
+  A(cudaGetLastError(), "create kernels");
+  if (st != ST_OK) { st_flip_destroy(s); return st; }
+  *out = s;
+  return ST_OK;
+}
+
+st_status st_flip_get_dims(st_flip* s, st_flip_dims* o) {
+  if (!s || !o) return ST_BAD_ARG;
+  o->nx = s->nx; o->ny = s->ny; o->nz = s->nz; o->tx = s->tx; o->ty = s->ty; o->tz = s->tz;
+  o->h = (float)s->h; o->x0 = (float)s->bx0; o->y0 = (float)s->by0; o->z0 = (float)s->bz0;
+  o->x1 = (float)s->bx1; o->y1 = (float)s->by1; o->z1 = (float)s->bz1;
+  return ST_OK;
+}
+
+void* st_flip_stream(st_flip* s) { return s ? (void*)s->stream : nullptr; }
+
+st_status st_flip_clear(st_flip* s) {
+  if (!s) return ST_BAD_ARG;
+  cudaSetDevice(s->device);
+  s->N = 0; s->ring = 0; s->tm = 0; s->nbInit = 1; s->fills.clear(); s->steps = 0;
+  if (s->sprayCap) {
+    CK(cudaMemsetAsync(s->sPos, 0, (size_t)s->sprayCap * 16, s->stream));
+    CK(cudaMemsetAsync(&s->dCtl->sctl0, 0, 4, s->stream));
+  }
+  reset_ids(s);
+  CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+st_status st_flip_set_cap(st_flip* s, uint32_t c) {
+  if (!s) return ST_BAD_ARG;
+  s->cap = std::min(c, s->maxN);
+  if (s->N > s->cap) s->N = s->cap;
+  if (s->ring >= s->cap) s->ring = 0;
+  return ST_OK;
+}
+
+// FlipSim.add for n particles (src/gpu.js:390-408): the speed goes in pos.w, foam 0. Slots past N take the next
+// ids; once the cap is reached the ring overwrites storage slots, keeping the id each slot holds.
+st_status st_flip_add(st_flip* s, const float* p3, const float* v3_, uint32_t n, uint32_t* added) {
+  if (!s || (n && (!p3 || !v3_))) return ST_BAD_ARG;
+  cudaSetDevice(s->device);
+  std::vector<Part> host(n);
+  std::vector<uint32_t> slot(n);
+  uint32_t k = 0;
+  for (; k < n; k++) {
+    uint32_t i;
+    if (s->N < s->cap) i = s->N++;
+    else if (s->recycle) { i = s->ring++; if (s->ring >= s->cap) s->ring = 0; }
+    else break;
+    float vx = v3_[k * 3], vy = v3_[k * 3 + 1], vz = v3_[k * 3 + 2];
+    host[k].p = make_float4(p3[k * 3], p3[k * 3 + 1], p3[k * 3 + 2], (float)std::sqrt((double)vx * vx + (double)vy * vy + (double)vz * vz));
+    host[k].v = make_float4(vx, vy, vz, 0.0f);
+    slot[k] = i;
+  }
+  // contiguous runs of slots go up in one copy each
+  uint32_t a = 0;
+  while (a < k) {
+    uint32_t b = a + 1;
+    while (b < k && slot[b] == slot[b - 1] + 1) b++;
+    CK(cudaMemcpyAsync(s->part[s->cur] + slot[a], host.data() + a, (size_t)(b - a) * sizeof(Part), cudaMemcpyHostToDevice, s->stream));
+    a = b;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  if (added) *added = k;
+  return ST_OK;
+}
+
+// packColliders (src/gpu.js:42-70): 32 floats per collider, SDF grids uploaded when the set of ids changes
+static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc) {
+  nc = std::min(o->ncols, 32u);
+  if (nc && !o->cols) return ST_BAD_ARG;
+  std::string sig;
+  std::map<uint32_t, uint32_t> offs;
+  uint32_t off = 0;
+  for (uint32_t k = 0; k < nc; k++) {
+    const st_sdf* sd = o->cols[k].sdf;
+    if (!sd || !sd->data) return ST_BAD_ARG;
+    if (!offs.count(sd->id)) { offs[sd->id] = off; off += sd->dims[0] * sd->dims[1] * sd->dims[2]; sig += std::to_string(sd->id) + ","; }
+  }
+  if (sig != s->sdfSig) {
+    if (off > s->sdfCap) {
+      CK(cudaStreamSynchronize(s->stream));
+      cudaFree(s->sdf);
+      s->sdfCap = (size_t)std::ceil(off * 1.3);
+      CK(dalloc(&s->sdf, s->sdfCap));
+    }
+    std::map<uint32_t, bool> seen;
+    for (uint32_t k = 0; k < nc; k++) {
+      const st_sdf* sd = o->cols[k].sdf;
+      if (seen[sd->id]) continue;
+      seen[sd->id] = true;
+      CK(cudaMemcpy(s->sdf + offs[sd->id], sd->data, sizeof(float) * sd->dims[0] * sd->dims[1] * sd->dims[2], cudaMemcpyHostToDevice));
+    }
+    s->sdfSig = sig;
+  }
+  if (nc) {
+    float cf[32 * 32];
+    for (uint32_t k = 0; k < nc; k++) {
+      const st_collider& c = o->cols[k];
+      const st_sdf* sd = c.sdf;
+      float* f = &cf[k * 32];
+      f[0] = (float)offs[sd->id]; f[1] = (float)sd->dims[0]; f[2] = (float)sd->dims[1]; f[3] = (float)sd->dims[2];
+      f[4] = sd->origin[0]; f[5] = sd->origin[1]; f[6] = sd->origin[2]; f[7] = sd->cell;
+      f[8] = c.R[0]; f[9] = c.R[3]; f[10] = c.R[6]; f[11] = 0;
+      f[12] = c.R[1]; f[13] = c.R[4]; f[14] = c.R[7]; f[15] = 0;
+      f[16] = c.R[2]; f[17] = c.R[5]; f[18] = c.R[8]; f[19] = 0;
+      f[20] = c.pos[0]; f[21] = c.pos[1]; f[22] = c.pos[2]; f[23] = 0;
+      f[24] = c.vel[0]; f[25] = c.vel[1]; f[26] = c.vel[2]; f[27] = 0;
+      f[28] = c.ang[0]; f[29] = c.ang[1]; f[30] = c.ang[2]; f[31] = 0;
+    }
+    CK(cudaMemcpyAsync(s->cols, cf, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  }
+  return ST_OK;
+}
+
+// the parameter block (src/flip/sim.js:196-231): host values in double, rounded once to f32
+static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t nc, uint32_t init, bool nbOn, bool sprOn) {
+  FlipParams& P = s->hp;
+  memset(&P, 0, sizeof(P));
+  P.n = s->N; P.nx = s->nx; P.ny = s->ny; P.nz = s->nz; P.ncols = nc; P.open = s->open;
+  P.tx = s->tx; P.ty = s->ty; P.tz = s->tz; P.ntiles = s->ntiles;
+  P.dt = (float)dt; P.h = (float)s->h; P.ih = (float)(1.0 / s->h); P.gravity = o->g; P.flip = o->flip; P.rest = (float)s->rest;
+  P.comp = o->comp;
+  double omAuto = std::min(1.9, 2.0 / (1.0 + std::sin(M_PI / std::max(s->nx, std::max(s->ny, s->nz)))));
+  P.omega = o->omega != 0.0f ? o->omega : (float)omAuto;
+  P.x0 = (float)s->bx0; P.y0 = (float)s->by0; P.z0 = (float)s->bz0; P.vmax = o->vmax != 0.0f ? o->vmax : 14.0f;
+  P.margin = (float)(0.3 * s->d); P.scale = 65536.0f; P.x1 = (float)s->bx1; P.y1 = (float)s->by1; P.z1 = (float)s->bz1;
+  P.q0 = (float)(0.3 * s->h); P.q1 = o->wind[0]; P.q2 = o->wind[1]; P.q3 = o->wind[2]; P.q4 = o->drag;
+  P.q5 = o->foam_tau != 0.0f ? o->foam_tau : 1.2f; P.q6 = o->foam_sens != 0.0f ? o->foam_sens : 1.0f; P.q7 = o->gust;
+  P.q8 = (float)s->tm; P.q9 = (o->flags & ST_OPT_NO_FOAM) ? 1.0f : 0.0f; P.q10 = (o->flags & ST_OPT_NO_CULL) ? 1.0f : 0.0f;
+  P.q12 = (o->flags & ST_OPT_FAST_AIR) ? 1.0f : 0.0f;
+  const st_spray_opts& sp = o->spray;
+  P.sheetMin = o->tear; P.sprRate = sprOn ? sp.rate : 0.0f; P.sprMin = sprOn ? std::max(0.05f, sp.min) : 1.0f;
+  P.sprLife = sprOn ? sp.life : 1.0f; P.mistFrac = sprOn ? sp.mist : 0.0f; P.sprDrag = sprOn ? sp.drag : 1.0f;
+  P.mistDrag = sprOn ? sp.mdrag : 4.0f; P.vs = o->vs != 0.0f ? o->vs : 1.0f;
+  P.smax = s->sprayCap; P.seed = s->seed; P.nb = nbOn ? 1u : 0u; P.nbInit = init; P.sprayOn = sprOn ? 1u : 0u;
+  uint64_t pool = (uint64_t)(s->ntiles + 1) * 512;
+  P.lcap = s->velGOn ? (uint32_t)std::min<uint64_t>(pool, 0xffffffffu) : (uint32_t)std::min<uint64_t>(pool, s->maxN);
+  P.stamp = s->stamp;
+  P.band = std::max(2.0f, o->nb_band != 0.0f ? o->nb_band : 3.0f);
+  P.wwFoamLife = sp.foam_life != 0.0f ? sp.foam_life : 3.0f; P.wwRise = sp.rise != 0.0f ? sp.rise : 0.3f;
+  P.wwCrest = sp.crest; P.wwImpact = sp.impact;
+  uint32_t nf = init ? (uint32_t)std::min<size_t>(s->fills.size() / 8, 8) : 0u;
+  P.nfill = nf;
+  for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &s->fills[k * 8], 8 * sizeof(float));
+}
+
+// one step; t (optional) receives device ms per stage
+static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
+  if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
+  if (s->N == 0) return ST_NOT_READY;
+  CK(cudaSetDevice(s->device));
+  const bool nbOn = o->nb_on != 0;
+  if (nbOn) s->velGOn = true;
+  const uint32_t init = nbOn && s->nbInit ? s->nbInit : 0;
+  uint32_t nc = 0;
+  st_status st = pack_colliders(s, o, nc);
+  if (st != ST_OK) return st;
+  const bool sprOn = o->spray_on != 0 && s->sprayCap > 0;
+  s->seed = s->seed + 1u;
+  s->stamp = s->stamp + 1u;
+  pack_params(s, dt, o, nc, init, nbOn, sprOn);
+  s->tm = s->tm + dt;
+  if (init) { s->nbInit = 0; s->fills.clear(); }
+  const int iters = std::max(1, o->iters);
+  cudaStream_t q = s->stream;
+  // this step's storage order goes into the other particle buffer; cell counts alternate buffers
+  s->cur ^= 1;
+  s->parity ^= 1;
+  CK(cudaMemcpyAsync(s->dP, &s->hp, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
+  // per-step counters: fluid, fastest speed, dropped tiles, emission
+  CK(cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q));   // fluid, vmaxBits (nActive is kept)
+  CK(cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q));
+  CK(cudaMemsetAsync(&s->dCtl->emitTried, 0, sizeof(uint32_t), q));
+  const Bufs B = s->bufs();
+  const int gT = s->tileGrid(8), gT4 = s->tileGrid(4);
+  auto mark = [&](int k) { if (t) cudaEventRecord(s->ev[k], q); };
+  mark(0);
+  // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
+  launch_count_mark(B, q);
+  if (nbOn && init != 1) launch_mark_phi(B, gT4, q);
+  if (init) launch_mark_fill(B, std::max(1, (int)std::min<uint32_t>((s->ntiles + 255) / 256, 4096)), q);
+  launch_tiles(B, s->ntiles, gT4, q);
+  if (init) launch_nb_init(B, gT4, q);
+  launch_scan_counts(B, q);
+  launch_scatter(B, q);
+  mark(1);
+  launch_p2g(B, gT, q);
+  mark(2);
+  if (nbOn) launch_nb_phi(B, gT4, q);
+  mark(3);
+  launch_classify(B, gT4, q);
+  if (nbOn) launch_nb_vel(B, gT4, q);
+  mark(4);
+  launch_norm_div(B, gT4, q);
+  mark(5);
+  launch_sor(B, gT, iters, q);
+  mark(6);
+  launch_project(B, gT4, q);
+  mark(7);
+  launch_g2p(B, s->N, q);
+  mark(8);
+  if (s->sprayCap > 0) launch_spray(B, s->sprayCap, sprOn, gT4, q);
+  mark(9);
+  if (nbOn) launch_nb_reseed(B, gT4, q);
+  mark(10);
+  CK(cudaGetLastError());
+  s->steps++;
+  if (t) {
+    CK(cudaEventSynchronize(s->ev[10]));
+    float ms[10];
+    for (int k = 0; k < 10; k++) cudaEventElapsedTime(&ms[k], s->ev[k], s->ev[k + 1]);
+    memset(t, 0, sizeof(*t));
+    t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
+    t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8]; t->reseed = ms[9];
+    cudaEventElapsedTime(&t->total, s->ev[0], s->ev[10]);
+  }
+  return ST_OK;
+}
+
+st_status st_flip_step(st_flip* s, double dt, const st_step_opts* o) { return do_step(s, dt, o, nullptr); }
+st_status st_flip_step_timed(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
+  if (!t) return ST_BAD_ARG;
+  return do_step(s, dt, o, t);
+}
+
+st_status st_flip_stats(st_flip* s, st_stats* out) {
+  if (!s || !out) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaMemcpyAsync(s->hCtl, s->dCtl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  out->sc = s->hCtl->nActive; out->ovf = 0; out->fluid = s->hCtl->fluid;
+  uint32_t vb = s->hCtl->vmaxBits; float vm; memcpy(&vm, &vb, 4); out->vmax = vm;
+  out->n = s->N; out->live = s->steps ? s->hCtl->nLive : s->N; out->spray_used = s->hCtl->sctl0; out->steps = s->steps;
+  return ST_OK;
+}
+
+// particles in id order: unsort on the device into the free particle buffer, then copy out
+st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n) {
+  if (!s || !pos4) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (n) *n = s->N;
+  uint32_t m = std::min(cap, s->N);
+  if (m == 0) return ST_OK;
+  float4* tmp = reinterpret_cast<float4*>(s->part[s->cur ^ 1]);   // 2 float4 per particle of room
+  launch_unsort(s->part[s->cur], s->ids[s->cur], s->N, tmp, vel4 ? tmp + s->N : nullptr, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(pos4, tmp, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
+  if (vel4) CK(cudaMemcpyAsync(vel4, tmp + s->N, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (!s->sprayCap) { if (n) *n = 0; return ST_OK; }
+  CK(cudaMemcpyAsync(s->hCtl, s->dCtl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  uint32_t m = std::max(1u, std::min(s->sprayCap, s->hCtl->sctl0));
+  if (n) *n = m;
+  uint32_t c = std::min(m, cap);
+  if (pos4 && c) CK(cudaMemcpyAsync(pos4, s->sPos, (size_t)c * 16, cudaMemcpyDeviceToHost, s->stream));
+  if (vel4 && c) CK(cudaMemcpyAsync(vel4, s->sVel, (size_t)c * 16, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+st_status st_flip_read_grid(st_flip* s, const st_flip_grid* g) {
+  if (!s || !g) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  const size_t C = s->ncell, T = s->ntiles;
+  std::vector<uint8_t> on(T);
+  std::vector<int32_t> cnt(C);
+  std::vector<uint32_t> ct(C);
+  std::vector<float> pr(C), rh(C), vn(3 * C), vo(3 * C), vg(3 * C);
+  cudaStream_t q = s->stream;
+  CK(cudaMemcpyAsync(on.data(), s->on, T, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(cnt.data(), s->cnt[s->parity], C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(ct.data(), s->ctype, C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(pr.data(), s->pres, C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(rh.data(), s->rhs, C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(vn.data(), s->vn, 3 * C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(vo.data(), s->vo, 3 * C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaMemcpyAsync(vg.data(), s->velG, 3 * C * 4, cudaMemcpyDeviceToHost, q));
+  CK(cudaStreamSynchronize(q));
+  const uint32_t NX = s->tx * 8, NY = s->ty * 8, NZ = s->tz * 8;
+  if (g->tile_on) memcpy(g->tile_on, on.data(), T);
+  for (uint32_t k = 0; k < NZ; k++)
+    for (uint32_t j = 0; j < NY; j++)
+      for (uint32_t i = 0; i < NX; i++) {
+        size_t o = (size_t)i + NX * ((size_t)j + NY * k);
+        uint32_t t = (i >> 3) + s->tx * ((j >> 3) + s->ty * (k >> 3));
+        size_t c = (size_t)t * 512 + (i & 7) + 8 * ((j & 7) + 8 * (k & 7));
+        bool live = on[t] != 0;
+        if (g->cnt) g->cnt[o] = live ? cnt[c] : 0;
+        if (g->ctype) g->ctype[o] = live ? ct[c] : 0;
+        if (g->pres) g->pres[o] = live ? pr[c] : 0.0f;
+        if (g->rhs) g->rhs[o] = live ? rh[c] : 8.0f;
+        for (int a = 0; a < 3; a++) {
+          if (g->vn) g->vn[o * 3 + a] = live ? vn[a * C + c] : 0.0f;
+          if (g->vo) g->vo[o * 3 + a] = live ? vo[a * C + c] : 0.0f;
+          if (g->velg) g->velg[o * 3 + a] = live ? vg[a * C + c] : 0.0f;
+        }
+      }
+  return ST_OK;
+}
+
+st_status st_flip_save_state(st_flip* s, float* pos4, float* vel4, uint32_t* pid, uint32_t cap, uint32_t* n) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (n) *n = s->N;
+  uint32_t m = std::min(cap, s->N);
+  if (m == 0) return ST_OK;
+  std::vector<Part> host(m);
+  CK(cudaMemcpyAsync(host.data(), s->part[s->cur], (size_t)m * sizeof(Part), cudaMemcpyDeviceToHost, s->stream));
+  if (pid) CK(cudaMemcpyAsync(pid, s->ids[s->cur], (size_t)m * 4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (uint32_t i = 0; i < m; i++) {
+    if (pos4) memcpy(&pos4[i * 4], &host[i].p, 16);
+    if (vel4) memcpy(&vel4[i * 4], &host[i].v, 16);
+  }
+  return ST_OK;
+}
+
+st_status st_flip_load_state(st_flip* s, const float* pos4, const float* vel4, const uint32_t* pid, uint32_t n, double t, uint32_t seed) {
+  if (!s || n > s->maxN || (n && (!pos4 || !vel4 || !pid))) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  std::vector<Part> host(n);
+  for (uint32_t i = 0; i < n; i++) { memcpy(&host[i].p, &pos4[i * 4], 16); memcpy(&host[i].v, &vel4[i * 4], 16); }
+  if (n) {
+    CK(cudaMemcpyAsync(s->part[s->cur], host.data(), (size_t)n * sizeof(Part), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->ids[s->cur], pid, (size_t)n * 4, cudaMemcpyHostToDevice, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->N = n; s->ring = 0; s->tm = t; s->seed = seed;
+  return ST_OK;
+}
+
+st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const float* sph4, uint32_t nsph, uint32_t mode) {
+  if (!s || (nbox && !boxes6) || (nsph && !sph4)) return ST_BAD_ARG;
+  s->fills.clear();
+  for (uint32_t k = 0; k < nbox; k++) {
+    const float* b = &boxes6[k * 6];
+    float f[8] = {1, b[0], b[1], b[2], b[3], b[4], b[5], 0};
+    s->fills.insert(s->fills.end(), f, f + 8);
+  }
+  for (uint32_t k = 0; k < nsph; k++) {
+    const float* q = &sph4[k * 4];
+    float f[8] = {2, q[0], q[1], q[2], q[3], 0, 0, 0};
+    s->fills.insert(s->fills.end(), f, f + 8);
+  }
+  s->nbInit = mode ? mode : 1;
+  return ST_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,278 @@
+// common.cuh - device-side data layout and helpers shared by the FLIP kernels.
+//
+// Grid storage is tile-indexed: tile t = ti + tx*(tj + ty*tk) owns cells t*512 + (i&7) + 8*((j&7) + 8*(k&7)).
+// The whole tile box of every workload fits in HBM, so every tile has a fixed home and no kernel needs the
+// reference's tile -> slot indirection (tmap, src/flip/wgsl-core.js:80-83). Tiles without storage in the
+// reference sense ("inactive") are kept in the state the reference's spare slot 0 reads as: cnt 0, type air,
+// pressure 0, rhs 8, velocities 0 (src/flip/wgsl-solver.js:6-15).
+//
+// All arithmetic follows the reference WGSL operation by operation (left-to-right sums, no fused multiply-add:
+// the library is built with -fmad=false) so that integer and discrete results are bit-identical to the oracle.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace st {
+
+constexpr float DEADY = -1.0e5f;
+constexpr uint32_t DEADKEY = 0xffffffffu;
+constexpr float WWHOLD = 0.2f;
+
+// The solver's parameter block (src/flip/wgsl-core.js:3-20, packed by src/flip/sim.js:196-231), resident in device
+// memory so that a captured launch sequence reads each step's values.
+struct FlipParams {
+  uint32_t n, nx, ny, nz, ncols, open, tx, ty, tz, ntiles;
+  float dt, h, ih, gravity, flip, rest, comp, omega;
+  float x0, y0, z0, vmax, margin, scale, x1, y1, z1;
+  float q0, q1, q2, q3, q4, q5, q6, q7, q8, q9, q10, q12;
+  float sheetMin, sprRate, sprMin, sprLife, mistFrac, sprDrag, mistDrag, vs;
+  uint32_t smax, seed, nb, nbInit, nfill, lcap, stamp, sprayOn;
+  float band, wwFoamLife, wwRise, wwCrest, wwImpact;
+  float fills[16][4];
+};
+
+// Device counters (the reference's ctl words, src/flip/wgsl-core.js:38-40, plus this design's own).
+struct Ctl {
+  uint32_t nActive;     // tiles with storage (ctl[4])
+  uint32_t fluid;       // fluid cells (ctl[0] + ctl[1])
+  uint32_t vmaxBits;    // fastest particle (ctl[6])
+  uint32_t nLive;       // live particles this step (sum of cell counts)
+  uint32_t nDropped;    // tiles that lost storage this step
+  uint32_t nDead;       // dead particle slots (narrow band refill list length)
+  uint32_t sctl0;       // whitewater slots handed out (sctl[0])
+  uint32_t sprayOvf;    // steps whose emission tried more points than the ring holds
+  uint32_t defCount;    // narrow band deficit cells
+  uint32_t defNeed;     // particles they ask for
+  uint32_t emitTried;   // whitewater points tried this step
+  uint32_t pad[5];
+};
+
+struct Part { float4 p, v; };   // one particle: position (w: speed + 64 x foam level), velocity (w: foam)
+
+// Pointers to every device buffer of one simulator.
+struct Bufs {
+  const FlipParams* P;
+  Ctl* ctl;
+  Part* pa;             // particles, storage order of this step (written by p2g)
+  Part* pb;             // particles, previous order (read by the sort)
+  uint32_t* ida;        // ids matching pa
+  uint32_t* idb;        // ids matching pb
+  uint32_t* key;        // per particle: cell key, DEADKEY when dead
+  uint32_t* rank;       // per particle: rank inside its cell (or dead rank inside its block)
+  uint32_t* srcIdx;     // per sorted position: index into pb
+  uint32_t* spid;       // per sorted position: id
+  uint32_t* blkDead;    // per particle block: dead count, then exclusive offsets
+  // tiles
+  uint32_t* need;       // stamp of the last step that marked the tile
+  uint8_t* on;          // tile has storage this step
+  uint8_t* tstate;      // bit0 had storage last step, bit1 has it now
+  uint32_t* blkTiles;   // per 1024-tile chunk: tiles with storage
+  uint32_t* active;     // tiles with storage, ascending
+  uint32_t* prevActive; // last step's list (narrow band marking)
+  uint32_t* tileSlot;   // tile -> position in active
+  uint32_t* dropped;    // tiles that lost storage this step
+  uint32_t* tileCnt;    // per active position: particles, then exclusive offsets (size ntiles + 1)
+  uint32_t* tileAux;    // per active position: scratch counts (deficit cells), then offsets
+  uint32_t* tileAux2;   // per active position: scratch sums (deficit need), then offsets
+  // cells (ncell = ntiles * 512)
+  int32_t* cnt;         // particles per cell, this step (two buffers alternate by step)
+  int32_t* cntOther;    // the other buffer: cleared during this step for the next one
+  uint32_t* cellOff;    // exclusive prefix of cnt inside the tile
+  uint32_t* ctype;      // bits 0-7 type, 8-15 collider + 1, 16-31 depth (src/flip/wgsl-core.js:33)
+  float* pres;
+  float* rhs;
+  int32_t* acc;         // 6 planes of ncell: summed v (x, y, z), summed weight (x, y, z), fixed point
+  float* vn;            // 3 planes: new face velocity
+  float* vo;            // 3 planes: old face velocity
+  float* velG;          // 3 planes: kept grid velocity (narrow band)
+  uint16_t* sorInfo;    // per fluid cell: bits 0-5 neighbour is fluid, bits 8-10 non-solid neighbours
+  // colliders
+  const float4* cols;   // 8 per collider (src/gpu.js:3-4)
+  const float* sdf;
+  // whitewater
+  float4* sPos;
+  float4* sVel;
+  uint8_t* emitK;       // per particle: points to emit
+  uint32_t* blkEmit;    // per particle block: points, then offsets
+  // narrow band refill
+  uint32_t* deadList;
+  uint32_t ncell;
+  uint32_t nblk;        // particle blocks of PBLK
+};
+
+constexpr int PBLK = 1024;     // particles per block in the order-defining passes (count, scatter, dead lists)
+
+// ---- small vector math: every operation spelled out so the order matches the oracle ----
+struct V3 { float x, y, z; };
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float len3(V3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ float fmn(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmx(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fmn(fmx(x, lo), hi); }
+__device__ __forceinline__ V3 vmin(V3 a, V3 b) { return v3(fmn(a.x, b.x), fmn(a.y, b.y), fmn(a.z, b.z)); }
+__device__ __forceinline__ V3 vmax(V3 a, V3 b) { return v3(fmx(a.x, b.x), fmx(a.y, b.y), fmx(a.z, b.z)); }
+__device__ __forceinline__ V3 vclamp(V3 a, V3 lo, V3 hi) { return vmin(vmax(a, lo), hi); }
+__device__ __forceinline__ V3 vfloor(V3 a) { return v3(floorf(a.x), floorf(a.y), floorf(a.z)); }
+__device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+__device__ __forceinline__ V3 vmix(V3 a, V3 b, float t) { return v3(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
+__device__ __forceinline__ V3 cross3(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+__device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
+  float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+__device__ __forceinline__ float comp3(V3 a, int ax) { return ax == 0 ? a.x : (ax == 1 ? a.y : a.z); }
+__device__ __forceinline__ uint32_t u32f(float f) { return f <= 0.0f ? 0u : (uint32_t)f; }
+__device__ __forceinline__ V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
+
+// hash1 (src/flip/wgsl-solver.js:181-184)
+__device__ __forceinline__ float hash1(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return (float)x * 2.3283064e-10f;
+}
+
+// ---- addressing ----
+__device__ __forceinline__ uint32_t tileOf(const FlipParams& P, int i, int j, int k) {
+  return (uint32_t)(i >> 3) + P.tx * ((uint32_t)(j >> 3) + P.ty * (uint32_t)(k >> 3));
+}
+__device__ __forceinline__ uint32_t cellIdx(const FlipParams& P, int i, int j, int k) {
+  return tileOf(P, i, j, k) * 512u + (uint32_t)(i & 7) + 8u * ((uint32_t)(j & 7) + 8u * (uint32_t)(k & 7));
+}
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// the cell holding face (axis, i, j, k) after the reference's clamping (src/flip/wgsl-core.js:84-89)
+__device__ __forceinline__ uint32_t faceCell(const FlipParams& P, int axis, int i, int j, int k) {
+  int nx = (int)P.nx, ny = (int)P.ny, nz = (int)P.nz;
+  if (axis == 0) return cellIdx(P, clampi(i, 0, nx), clampi(j, 0, ny - 1), clampi(k, 0, nz - 1));
+  if (axis == 1) return cellIdx(P, clampi(i, 0, nx - 1), clampi(j, 0, ny), clampi(k, 0, nz - 1));
+  return cellIdx(P, clampi(i, 0, nx - 1), clampi(j, 0, ny - 1), clampi(k, 0, nz));
+}
+__device__ __forceinline__ void tileCoord(const FlipParams& P, uint32_t t, uint32_t local, int& i, int& j, int& k) {
+  uint32_t tt = t / P.tx;
+  i = (int)((t % P.tx) * 8u + (local & 7u));
+  j = (int)((tt % P.ty) * 8u + ((local >> 3) & 7u));
+  k = (int)((tt / P.ty) * 8u + (local >> 6));
+}
+__device__ __forceinline__ bool inDom(const FlipParams& P, int i, int j, int k) {
+  return i >= 0 && j >= 0 && k >= 0 && i < (int)P.nx && j < (int)P.ny && k < (int)P.nz;
+}
+// ctypeOf (src/flip/wgsl-core.js:104-112)
+__device__ __forceinline__ uint32_t ctypeOf(const FlipParams& P, const uint32_t* __restrict__ ctype, int i, int j, int k) {
+  if (i < 0) return (P.open & 1u) ? 0u : 2u;
+  if (i >= (int)P.nx) return (P.open & 2u) ? 0u : 2u;
+  if (j < 0) return (P.open & 4u) ? 0u : 2u;
+  if (j >= (int)P.ny) return (P.open & 8u) ? 0u : 2u;
+  if (k < 0) return (P.open & 16u) ? 0u : 2u;
+  if (k >= (int)P.nz) return (P.open & 32u) ? 0u : 2u;
+  return ctype[cellIdx(P, i, j, k)] & 0xffu;
+}
+__device__ __forceinline__ V3 cellCenter(const FlipParams& P, int i, int j, int k) {
+  return v3(P.x0 + ((float)i + 0.5f) * P.h, P.y0 + ((float)j + 0.5f) * P.h, P.z0 + ((float)k + 0.5f) * P.h);
+}
+__device__ __forceinline__ void particleCell(const FlipParams& P, V3 p, int& ci, int& cj, int& ck) {
+  V3 g = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih);
+  ci = clampi((int)g.x, 0, (int)P.nx - 1);
+  cj = clampi((int)g.y, 0, (int)P.ny - 1);
+  ck = clampi((int)g.z, 0, (int)P.nz - 1);
+}
+__device__ __forceinline__ V3 facePos(const FlipParams& P, int i, int j, int k, int axis) {
+  return v3(P.x0 + ((float)i + (axis == 0 ? 0.0f : 0.5f)) * P.h, P.y0 + ((float)j + (axis == 1 ? 0.0f : 0.5f)) * P.h,
+            P.z0 + ((float)k + (axis == 2 ? 0.0f : 0.5f)) * P.h);
+}
+__device__ __forceinline__ float phiOfBits(uint32_t ct) { return 8.0f - (float)(ct >> 16) / 4096.0f; }
+__device__ __forceinline__ uint32_t phiPutBits(uint32_t ct, float v) {
+  uint32_t q = (uint32_t)clampf(rintf((8.0f - v) * 4096.0f), 0.0f, 65535.0f);
+  return (ct & 0xffffu) | (q << 16);
+}
+
+// ---- colliders (src/gpu.js:6-38, src/flip/wgsl-core.js:113-126) ----
+__device__ __forceinline__ void sdfEval(const float4* __restrict__ cols, const float* __restrict__ sdf, uint32_t k, V3 p,
+                                        float& phi, V3& wn) {
+  float4 a = cols[k * 8], b = cols[k * 8 + 1];
+  V3 r0 = xyz(cols[k * 8 + 2]), r1 = xyz(cols[k * 8 + 3]), r2 = xyz(cols[k * 8 + 4]);
+  V3 d = p - xyz(cols[k * 8 + 5]);
+  V3 lp = v3(dot3(r0, d), dot3(r1, d), dot3(r2, d));
+  V3 g = v3((lp.x - b.x) / b.w, (lp.y - b.y) / b.w, (lp.z - b.z) / b.w);
+  V3 dims = v3(a.y, a.z, a.w);
+  V3 gc = vclamp(g, v3(0.0f, 0.0f, 0.0f), dims - v3(1.0001f, 1.0001f, 1.0001f));
+  V3 fl = vfloor(gc);
+  V3 f = gc - fl;
+  uint32_t nx = u32f(a.y), ny = u32f(a.z);
+  uint32_t base = u32f(a.x) + u32f(fl.x) + nx * (u32f(fl.y) + ny * u32f(fl.z));
+  uint32_t s = nx * ny;
+  float v000 = sdf[base], v100 = sdf[base + 1], v010 = sdf[base + nx], v110 = sdf[base + nx + 1];
+  float v001 = sdf[base + s], v101 = sdf[base + s + 1], v011 = sdf[base + s + nx], v111 = sdf[base + s + nx + 1];
+  float c00 = mixf(v000, v100, f.x), c10 = mixf(v010, v110, f.x), c01 = mixf(v001, v101, f.x), c11 = mixf(v011, v111, f.x);
+  float c0 = mixf(c00, c10, f.y), c1 = mixf(c01, c11, f.y);
+  phi = mixf(c0, c1, f.z);
+  V3 out = g - gc;
+  V3 gl;
+  if (dot3(out, out) > 0.0f) {
+    float l = len3(out);
+    phi += l * b.w;
+    gl = out / l;
+  } else {
+    gl = v3(mixf(mixf(v100 - v000, v110 - v010, f.y), mixf(v101 - v001, v111 - v011, f.y), f.z), mixf(c10 - c00, c11 - c01, f.z), c1 - c0);
+    float l = len3(gl);
+    gl = gl / fmx(l, 1e-9f);
+  }
+  wn = r0 * gl.x + r1 * gl.y + r2 * gl.z;
+}
+__device__ __forceinline__ V3 colSurfVel(const float4* __restrict__ cols, uint32_t k, V3 p) {
+  V3 c = xyz(cols[k * 8 + 5]);
+  return xyz(cols[k * 8 + 6]) + cross3(xyz(cols[k * 8 + 7]), p - c);
+}
+__device__ __forceinline__ bool colNear(const FlipParams& P, const float4* __restrict__ cols, uint32_t k, V3 p) {
+  if (P.q10 > 0.5f) return true;
+  float4 b = cols[k * 8 + 1];
+  V3 d = p - xyz(cols[k * 8 + 5]);
+  V3 lp = v3(dot3(xyz(cols[k * 8 + 2]), d), dot3(xyz(cols[k * 8 + 3]), d), dot3(xyz(cols[k * 8 + 4]), d));
+  V3 g = v3((lp.x - b.x) / b.w, (lp.y - b.y) / b.w, (lp.z - b.z) / b.w);
+  float4 a = cols[k * 8];
+  float lo = -1.0f - P.q0 / b.w, hi = P.q0 / b.w;
+  return g.x > lo && g.y > lo && g.z > lo && g.x < a.y + hi && g.y < a.z + hi && g.z < a.w + hi;
+}
+__device__ __forceinline__ int colAt(const FlipParams& P, const float4* __restrict__ cols, const float* __restrict__ sdf, V3 p) {
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    if (!colNear(P, cols, k, p)) continue;
+    float phi; V3 wn;
+    sdfEval(cols, sdf, k, p, phi, wn);
+    if (phi < P.q0) return (int)k;
+  }
+  return -1;
+}
+
+// ---- block-wide scans (blockDim.x a multiple of 32, at most 1024) ----
+__device__ __forceinline__ uint32_t warpInclusive(uint32_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t n = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += n;
+  }
+  return v;
+}
+// exclusive prefix of v over the block; *total gets the block sum. smem must hold 33 words. Ends with a barrier.
+__device__ __forceinline__ uint32_t blockExclusive(uint32_t v, uint32_t* smem, uint32_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t inc = warpInclusive(v);
+  if (lane == 31) smem[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < nw ? smem[lane] : 0u;
+    uint32_t si = warpInclusive(s);
+    if (lane < nw) smem[lane] = si - s;
+    if (lane == nw - 1) smem[32] = si;
+  }
+  __syncthreads();
+  uint32_t r = smem[w] + inc - v;
+  if (total) *total = smem[32];
+  __syncthreads();
+  return r;
+}
+
+}  // namespace st

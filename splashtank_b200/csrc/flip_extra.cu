@@ -1,0 +1,490 @@
+// flip_extra.cu - narrow band (src/flip/wgsl-narrowband.js) and whitewater (src/flip/wgsl-whitewater.js) kernels.
+//
+// Where the reference compacts with atomics in arbitrary order (nbDead, nbDeficit, nbSpawn, sprayEmit), these
+// kernels use a fixed order built from block scans: dead slots in ascending storage index, deficit cells in
+// ascending cell key, whitewater ring slots in ascending storage index of the emitting particle.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace st {
+
+__device__ __forceinline__ void loadParamsX(FlipParams& s, const FlipParams* g) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(FlipParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ float velGAxisX(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x, int axis) {
+  V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
+  if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+  const V3 f0 = vfloor(g), fr = g - f0;
+  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  float s = 0.0f;
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    s += w * velG[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
+  }
+  return s;
+}
+__device__ __forceinline__ V3 velGVecX(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
+  return v3(velGAxisX(P, velG, nc, x, 0), velGAxisX(P, velG, nc, x, 1), velGAxisX(P, velG, nc, x, 2));
+}
+__device__ __forceinline__ float fillPhiX(const FlipParams& P, V3 x) {
+  float d = 1.0e9f;
+  for (uint32_t k = 0; k < P.nfill; k++) {
+    const float* A = P.fills[k * 2];
+    const float* Bq = P.fills[k * 2 + 1];
+    if (A[0] < 1.5f) {
+      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
+      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
+    } else {
+      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
+    }
+  }
+  return d * P.ih;
+}
+
+// ---- phiInitAll (wgsl-narrowband.js:20-35) ----
+__global__ void __launch_bounds__(512) k_nb_init(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    float ph = clampf(fillPhiX(P, cellCenter(P, i, j, k)), -7.9f, 7.9f);
+    if (ph < 0.0f) ph = fmn(ph, -1.5f);
+    if (!inDom(P, i, j, k)) ph = 8.0f;
+    const uint32_t ct = B.ctype[c];
+    if (P.nbInit == 2u) ph = fmn(ph, phiOfBits(ct));
+    B.ctype[c] = phiPutBits(ct, ph);
+    if (P.nbInit == 1u) { B.velG[c] = 0.0f; B.velG[nc + c] = 0.0f; B.velG[2 * nc + c] = 0.0f; }
+  }
+}
+
+// ---- depth passes: nbPhi (wgsl-narrowband.js:38-49), jacNb / nbJacA / nbJacB (:50-68) ----
+__device__ __forceinline__ float phiSampleX(const FlipParams& P, const uint32_t* __restrict__ ctype, V3 x) {
+  const V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
+  const V3 gc = vclamp(g, v3(0.0f, 0.0f, 0.0f), v3((float)P.nx - 1.001f, (float)P.ny - 1.001f, (float)P.nz - 1.001f));
+  const V3 f0 = vfloor(gc), fr = gc - f0;
+  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  float s = 0.0f, ws = 0.0f;
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    const uint32_t ct = ctype[cellIdx(P, i0 + dx, j0 + dy, k0 + dz)];
+    if (((ct >> 8) & 0xffu) != 0u || w <= 0.0f) continue;
+    s += w * phiOfBits(ct);
+    ws += w;
+  }
+  if (ws < 1.0e-4f) return 0.5f;
+  return s / ws;
+}
+__global__ void __launch_bounds__(512) k_nb_phi(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    if (!inDom(P, i, j, k)) { B.rhs[c] = 8.0f; continue; }
+    if (((B.ctype[c] >> 8) & 0xffu) != 0u) { B.rhs[c] = 0.5f; continue; }
+    const V3 x = cellCenter(P, i, j, k);
+    const float phA = phiSampleX(P, B.ctype, x - velGVecX(P, B.velG, nc, x) * P.dt);
+    const bool inside = B.cnt[c] > 0 || phA < -1.0f;
+    B.rhs[c] = inside ? clampf(phA, -7.9f, -0.5f) : clampf(phA, 0.5f, 7.9f);
+  }
+}
+__device__ __forceinline__ float jacNb(const FlipParams& P, const Bufs& B, int i, int j, int k, float cur, bool fromRhs) {
+  if (!inDom(P, i, j, k)) return 8.0f;
+  if (cur >= 0.0f) return cur;
+  float m = -8.0f;
+  for (int q = 0; q < 6; q++) {
+    int a = i, b = j, c = k;
+    if (q == 0) a -= 1; else if (q == 1) a += 1; else if (q == 2) b -= 1; else if (q == 3) b += 1; else if (q == 4) c -= 1; else c += 1;
+    if (!inDom(P, a, b, c)) continue;
+    const uint32_t cq = cellIdx(P, a, b, c);
+    const uint32_t ct = B.ctype[cq];
+    if (((ct >> 8) & 0xffu) != 0u) continue;
+    m = fmx(m, fromRhs ? B.rhs[cq] : phiOfBits(ct));
+  }
+  return clampf(m - 1.0f, -7.9f, -0.5f);
+}
+// pass A: depth (ctype bits) from rhs; pass B: rhs from depth
+__global__ void __launch_bounds__(512) k_nb_jac(Bufs B, int passA) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    if (passA) {
+      const float v = jacNb(P, B, i, j, k, B.rhs[c], true);
+      B.ctype[c] = phiPutBits(B.ctype[c], v);
+    } else {
+      B.rhs[c] = jacNb(P, B, i, j, k, phiOfBits(B.ctype[c]), false);
+    }
+  }
+}
+
+// ---- nbVel (wgsl-narrowband.js:70-85): water faces with no particle weight take the carried grid velocity ----
+__global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    if (!inDom(P, i, j, k) || (B.ctype[c] & 0xffu) != 1u) continue;
+    for (int ax = 0; ax < 3; ax++) {
+      int li = i, lj = j, lk = k;
+      if (ax == 0) li -= 1; else if (ax == 1) lj -= 1; else lk -= 1;
+      if (!inDom(P, li, lj, lk)) continue;
+      if ((B.ctype[cellIdx(P, li, lj, lk)] & 0xffu) != 1u) continue;
+      if (B.acc[(3 + ax) * nc + c] > 0) continue;
+      const V3 fp = facePos(P, i, j, k, ax);
+      const float vc = velGAxisX(P, B.velG, nc, fp - velGVecX(P, B.velG, nc, fp) * P.dt, ax);
+      B.acc[ax * nc + c] = (int32_t)rintf(vc * P.scale);
+      B.acc[(3 + ax) * nc + c] = (int32_t)P.scale;
+    }
+  }
+}
+
+// ---- refill: nbKill (wgsl-narrowband.js:93-102), nbDead (:106-110), nbDeficit (:112-130), nbSpawn (:134-148) ----
+__global__ void __launch_bounds__(PBLK) k_nb_kill(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  bool dead = false;
+  if (i < P.n) {
+    Part q = B.pa[i];
+    dead = q.p.y < DEADY;
+    if (!dead && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
+      int ci, cj, ck;
+      particleCell(P, xyz(q.p), ci, cj, ck);
+      const uint32_t cc = cellIdx(P, ci, cj, ck);
+      if (B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band) {
+        q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+        q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        B.pa[i] = q;
+        dead = true;
+      }
+    }
+  }
+  const uint32_t nd = __syncthreads_count(dead);
+  if (threadIdx.x == 0) B.blkDead[blockIdx.x] = nd;
+}
+__device__ void scanOneX(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
+  uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
+  uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
+  uint32_t s = 0;
+  for (uint32_t x = beg; x < end; x++) s += arr[x];
+  uint32_t tot;
+  uint32_t run = blockExclusive(s, sm, &tot);
+  for (uint32_t x = beg; x < end; x++) { uint32_t v = arr[x]; arr[x] = run; run += v; }
+  if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
+}
+// which: 0 dead blocks, 1 deficit (cells and need per tile), 2 emission blocks
+__global__ void __launch_bounds__(1024) k_scan_x(Bufs B, int which) {
+  __shared__ uint32_t sm[33];
+  if (which == 0) scanOneX(B.blkDead, B.nblk, &B.ctl->nDead, sm);
+  else if (which == 1) {
+    if (blockIdx.x == 0) scanOneX(B.tileAux, B.ctl->nActive, &B.ctl->defCount, sm);
+    else scanOneX(B.tileAux2, B.ctl->nActive, &B.ctl->defNeed, sm);
+  } else scanOneX(B.blkEmit, B.nblk, &B.ctl->emitTried, sm);
+}
+__global__ void __launch_bounds__(PBLK) k_dead_list(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParamsX(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  const bool dead = i < P.n && B.pa[i].p.y < DEADY;
+  const uint32_t r = blockExclusive(dead ? 1u : 0u, sm, nullptr);
+  const uint32_t k = B.blkDead[blockIdx.x] + r;
+  if (dead && k < P.lcap) B.deadList[k] = i;
+}
+// the deficit test of one cell; returns the particles it asks for (0: none)
+__device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs& B, uint32_t c, int i, int j, int k) {
+  if (!inDom(P, i, j, k)) return 0;
+  const uint32_t ct = B.ctype[c];
+  if (((ct >> 8) & 0xffu) != 0u) return 0;
+  const float ph = phiOfBits(ct);
+  if ((ct & 0xffu) != 1u || ph > -1.0f || ph < -P.band) return 0;
+  if (!(len3(velGVecX(P, B.velG, B.ncell, cellCenter(P, i, j, k))) < 9.0f * P.h)) return 0;
+  const uint32_t n = (uint32_t)max(B.cnt[c], 0);
+  if ((float)n >= 0.55f * P.rest) return 0;
+  return min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
+}
+__global__ void __launch_bounds__(512) k_def_count(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    const uint32_t nd = deficitNeed(P, B, c, i, j, k);
+    uint32_t cells, needs;
+    blockExclusive(nd ? 1u : 0u, sm, &cells);
+    blockExclusive(nd, sm, &needs);
+    if (threadIdx.x == 0) { B.tileAux[a] = cells; B.tileAux2[a] = needs; }
+  }
+}
+__global__ void __launch_bounds__(512) k_spawn(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParamsX(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  const uint32_t avail = min(B.ctl->nDead, P.lcap);
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    const uint32_t nd = deficitNeed(P, B, c, i, j, k);
+    const uint32_t e = B.tileAux[a] + blockExclusive(nd ? 1u : 0u, sm, nullptr);
+    const uint32_t base = B.tileAux2[a] + blockExclusive(nd, sm, nullptr);
+    if (!nd || e >= P.lcap / 2u) continue;
+    const V3 cp = v3((float)i, (float)j, (float)k);
+    for (uint32_t m = 0; m < nd; m++) {
+      const uint32_t kk = base + m;
+      if (kk >= avail) break;
+      const uint32_t pi = B.deadList[kk];
+      const uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
+      const V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
+      const V3 v = velGVecX(P, B.velG, nc, x);
+      Part q;
+      q.p = make_float4(x.x, x.y, x.z, fmn(len3(v), 63.0f));
+      q.v = make_float4(v.x, v.y, v.z, 0.0f);
+      B.pa[pi] = q;
+    }
+  }
+}
+
+// ---- whitewater: wetCell / wetAt (wgsl-whitewater.js:7-23) ----
+__device__ __forceinline__ float wetCell(const FlipParams& P, const Bufs& B, int i, int j, int k) {
+  if (!inDom(P, i, j, k)) return 0.0f;
+  const uint32_t ci = cellIdx(P, i, j, k);
+  if (!B.on[ci >> 9]) return 0.0f;
+  const uint32_t ct = B.ctype[ci];
+  if (P.nb != 0u && (ct & 0xffu) == 1u && phiOfBits(ct) < -1.0f) return 1.0f;
+  return fmn((float)B.cnt[ci] / P.rest, 1.0f);
+}
+__device__ __forceinline__ float wetAt(const FlipParams& P, const Bufs& B, V3 p) {
+  const V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
+  const V3 f0 = vfloor(g), fr = g - f0;
+  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  float s = 0.0f;
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    if (w > 0.0f) s += w * wetCell(P, B, i0 + dx, j0 + dy, k0 + dz);
+  }
+  return s;
+}
+__device__ __forceinline__ float hsh3X(V3 p) {
+  V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f);
+  q = q - vfloor(q);
+  q = q * 17.0f;
+  const float r = q.x * q.y * q.z * (q.x + q.y + q.z);
+  return r - floorf(r);
+}
+__device__ __forceinline__ float vnzX(V3 x) {
+  const V3 i = vfloor(x), fr = x - vfloor(x);
+  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
+  const float a = mixf(mixf(hsh3X(i), hsh3X(i + v3(1, 0, 0)), u.x), mixf(hsh3X(i + v3(0, 1, 0)), hsh3X(i + v3(1, 1, 0)), u.x), u.y);
+  const float b = mixf(mixf(hsh3X(i + v3(0, 0, 1)), hsh3X(i + v3(1, 0, 1)), u.x), mixf(hsh3X(i + v3(0, 1, 1)), hsh3X(i + v3(1, 1, 1)), u.x), u.y);
+  return mixf(a, b, u.z);
+}
+// wwSample (wgsl-whitewater.js:91-98) fused with sprayStep (:134-179): each point reads only its own sample
+__global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t m = min(B.ctl->sctl0, P.smax), nc = B.ncell;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    float4 sp = B.sPos[j];
+    if (sp.w <= 0.0f) continue;
+    const V3 p = xyz(sp);
+    // sample: water velocity (vn) and wetness
+    V3 vf = v3(0.0f, 0.0f, 0.0f);
+    int ci, cj, ck;
+    particleCell(P, p, ci, cj, ck);
+    if (B.on[tileOf(P, ci, cj, ck)]) {
+      float r[3];
+      for (int axis = 0; axis < 3; axis++) {
+        V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+        if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+        const V3 f0 = vfloor(g), fr = g - f0;
+        const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+        float sn = 0.0f;
+        for (int c = 0; c < 8; c++) {
+          const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+          const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+          sn += w * B.vn[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
+        }
+        r[axis] = sn;
+      }
+      vf = v3(r[0], r[1], r[2]);
+    }
+    const float wet = wetAt(P, B, p);
+    // step
+    float4 sv = B.sVel[j];
+    V3 v = xyz(sv);
+    const float kw = sv.w;
+    uint32_t kind = u32f(kw + 0.5f);
+    float tk = (kw - (float)kind) / 0.4f * WWHOLD;
+    const bool settled = tk >= WWHOLD * 0.999f;
+    const uint32_t k0 = kind;
+    float life = sp.w;
+    const uint32_t h0 = j * 2654435761u + P.seed * 974711u;
+    if (kind == 0u && v.y < vf.y && wet > 0.55f && tk > 0.05f) { kind = 2u; life = P.wwFoamLife * (0.6f + 0.8f * hash1(h0)); v = vf; }
+    else if (kind == 1u && wet > 0.55f) { life = 0.0f; }
+    else if (kind == 2u && wet > 0.97f && settled) { kind = 3u; }
+    else if (kind == 2u && wet < 0.04f && settled) { kind = 0u; life = fmn(life, P.sprLife); }
+    else if (kind == 3u && wet < 0.6f && settled) { kind = 2u; life = fmx(life, 0.5f * P.wwFoamLife); }
+    if (kind != k0) tk = 0.0f; else tk = fmn(tk + P.dt, WWHOLD);
+    if (kind <= 1u) {
+      const bool mist = kind == 1u;
+      V3 gust = v3(0.0f, 0.0f, 0.0f);
+      if (P.q7 > 0.0f) {
+        const V3 gp = p * 0.55f * P.vs;
+        const float tt = P.q8 * 0.6f;
+        gust = v3(vnzX(gp + v3(tt, 0.0f, 0.0f)), vnzX(gp + v3(17.3f, tt, 4.1f)), vnzX(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
+      }
+      const V3 base = v3(P.q1, P.q2, P.q3);
+      const V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
+      v.y -= P.gravity * P.dt;
+      v = v + (airv - v) * (1.0f - expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
+      life -= P.dt;
+    } else if (kind == 2u) {
+      const float vy = vf.y + clampf((wet - 0.5f) * 4.0f, -1.0f, 1.0f) * P.h * 4.0f;
+      v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - expf(-10.0f * P.dt));
+      life -= P.dt;
+    } else {
+      v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - expf(-6.0f * P.dt));
+      life -= 0.3f * P.dt;
+    }
+    const V3 np = p + v * P.dt;
+    if (np.x < P.x0 || np.x > P.x1 || np.y < P.y0 || np.y > P.y1 || np.z < P.z0 || np.z > P.z1) life = 0.0f;
+    else if (P.ncols > 0u && colAt(P, B.cols, B.sdf, np) >= 0) life = 0.0f;
+    B.sPos[j] = make_float4(np.x, np.y, np.z, life);
+    B.sVel[j] = make_float4(v.x, v.y, v.z, (float)kind + 0.4f * tk / WWHOLD);
+  }
+}
+// sprayEmit (wgsl-whitewater.js:99-133), part 1: how many points each water particle throws off
+__device__ __forceinline__ void emitTerms(const FlipParams& P, const Bufs& B, const Part& q, float& rho, float& fast, float& e) {
+  const V3 p = xyz(q.p), v = xyz(q.v);
+  const float foam = q.v.w, spd = len3(v);
+  fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
+  const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+  rho = 0.0f;
+  for (int dz = 0; dz <= 1; dz++)
+    for (int dy = 0; dy <= 1; dy++)
+      for (int dx = 0; dx <= 1; dx++) rho += wetCell(P, B, bi + dx, bj + dy, bk + dz);
+  rho = rho / 8.0f;
+  const float crest = (1.0f - smoothstepf(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
+  const float churn = (1.0f - smoothstepf(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstepf(0.5f, 1.5f, spd * P.vs);
+  e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstepf(0.1f, 0.5f, P.q8);
+}
+__global__ void __launch_bounds__(PBLK) k_emit_count(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  uint32_t kc = 0;
+  if (i < P.n && P.smax != 0u && P.sprRate > 0.0f) {
+    const Part q = B.pa[i];
+    if (q.p.y >= DEADY) {
+      float rho, fast, e;
+      emitTerms(P, B, q, rho, fast, e);
+      if (e > 0.0f) {
+        const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
+        kc = min(u32f(floorf(P.sprRate * e * P.dt + hash1(h0))), 4u);
+      }
+    }
+  }
+  if (i < P.n) B.emitK[i] = (uint8_t)kc;
+  __shared__ uint32_t sm[33];
+  uint32_t tot;
+  blockExclusive(kc, sm, &tot);
+  if (threadIdx.x == 0) B.blkEmit[blockIdx.x] = tot;
+}
+// part 2: the points, into ring slots (sctl[0] + run) % smax that are not alive
+__global__ void __launch_bounds__(PBLK) k_emit_write(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParamsX(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  const uint32_t kc = i < P.n ? B.emitK[i] : 0u;
+  const uint32_t run0 = B.blkEmit[blockIdx.x] + blockExclusive(kc, sm, nullptr);
+  if (!kc) return;
+  const uint32_t s0 = B.ctl->sctl0;
+  const Part q = B.pa[i];
+  float rho, fast, e;
+  emitTerms(P, B, q, rho, fast, e);
+  const V3 qp = xyz(q.p), v = xyz(q.v);
+  const float spd = len3(v);
+  const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
+  for (uint32_t mm = 0; mm < kc; mm++) {
+    const uint32_t run = run0 + mm;
+    if (run >= P.smax) break;   // more points tried in one step than the ring holds: the rest are dropped
+    const uint32_t slot = (uint32_t)(((uint64_t)s0 + run) % P.smax);
+    if (B.sPos[slot].w > 0.0f) continue;   // never replace a living point
+    const uint32_t hh = h0 ^ ((mm + 1u) * 0x9E3779B9u);
+    const float z = hash1(hh + 1u) * 2.0f - 1.0f;
+    const float an = hash1(hh + 2u) * 6.2831853f;
+    const float s = sqrtf(fmx(0.0f, 1.0f - z * z));
+    const V3 dir = v3(s * cosf(an), s * sinf(an), z);
+    const bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
+    const bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
+    V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
+    float life = P.sprLife * (0.6f + 0.8f * hash1(hh + 5u)) * (mist ? 1.6f : 1.0f);
+    float kind = mist ? 1.0f : 0.0f;
+    if (under) { nv = v + dir * spd * 0.05f; life = P.wwFoamLife * (0.6f + 0.8f * hash1(hh + 5u)); kind = 3.0f; }
+    const V3 np = qp + nv * P.dt + dir * P.h * 0.3f * hash1(hh + 6u);
+    B.sPos[slot] = make_float4(np.x, np.y, np.z, life);
+    B.sVel[slot] = make_float4(nv.x, nv.y, nv.z, kind);
+  }
+}
+__global__ void k_emit_done(Bufs B) {
+  const FlipParams* P = B.P;
+  const uint32_t tried = B.ctl->emitTried;
+  if (tried > P->smax) B.ctl->sprayOvf += 1u;
+  B.ctl->sctl0 = B.ctl->sctl0 + tried;
+}
+
+// ---- launchers ----
+void launch_nb_init(const Bufs& B, int grid, cudaStream_t s) { k_nb_init<<<grid, 512, 0, s>>>(B); }
+void launch_nb_phi(const Bufs& B, int grid, cudaStream_t s) {
+  k_nb_phi<<<grid, 512, 0, s>>>(B);
+  k_nb_jac<<<grid, 512, 0, s>>>(B, 1);
+  k_nb_jac<<<grid, 512, 0, s>>>(B, 0);
+  k_nb_jac<<<grid, 512, 0, s>>>(B, 1);
+}
+void launch_nb_vel(const Bufs& B, int grid, cudaStream_t s) { k_nb_vel<<<grid, 512, 0, s>>>(B); }
+void launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
+  if (!B.nblk) return;
+  k_nb_kill<<<B.nblk, PBLK, 0, s>>>(B);
+  k_scan_x<<<1, 1024, 0, s>>>(B, 0);
+  k_dead_list<<<B.nblk, PBLK, 0, s>>>(B);
+  k_def_count<<<grid, 512, 0, s>>>(B);
+  k_scan_x<<<2, 1024, 0, s>>>(B, 1);
+  k_spawn<<<grid, 512, 0, s>>>(B);
+}
+void launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s) {
+  if (!smax) return;
+  k_ww_step<<<grid, 256, 0, s>>>(B);
+  if (!emit || !B.nblk) return;
+  k_emit_count<<<B.nblk, PBLK, 0, s>>>(B);
+  k_scan_x<<<1, 1024, 0, s>>>(B, 2);
+  k_emit_write<<<B.nblk, PBLK, 0, s>>>(B);
+  k_emit_done<<<1, 1, 0, s>>>(B);
+}
+
+}  // namespace st

@@ -1,0 +1,644 @@
+// flip_kernels.cu - the FLIP step on B200: tile activation, particle sort, P2G, classify, normalise + divergence,
+// red-black SOR, projection and G2P. Narrow band and whitewater kernels are in flip_extra.cu.
+//
+// Every kernel is either one thread per particle (storage order) or one CTA per tile with storage, striding over
+// device-side counts, so a step needs no host round trip. Citations name the WGSL kernel each one restates.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace st {
+
+__device__ __forceinline__ void loadParams(FlipParams& s, const FlipParams* g) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(FlipParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+// markAround (wgsl-core.js:239-246): every tile within two cells of cell (ci, cj, ck) gets this step's stamp.
+__device__ __forceinline__ void markAround(const FlipParams& P, uint32_t* __restrict__ need, int ci, int cj, int ck) {
+  int lox = max(ci - 2, 0) >> 3, loy = max(cj - 2, 0) >> 3, loz = max(ck - 2, 0) >> 3;
+  int hix = min(ci + 2, (int)P.tx * 8 - 1) >> 3, hiy = min(cj + 2, (int)P.ty * 8 - 1) >> 3, hiz = min(ck + 2, (int)P.tz * 8 - 1) >> 3;
+  for (int tk = loz; tk <= hiz; tk++)
+    for (int tj = loy; tj <= hiy; tj++)
+      for (int ti = lox; ti <= hix; ti++) {
+        uint32_t t = (uint32_t)ti + P.tx * ((uint32_t)tj + P.ty * (uint32_t)tk);
+        if (need[t] != P.stamp) need[t] = P.stamp;
+      }
+}
+
+// ---- 1. tileMark + count per cell (wgsl-blocks.js:10-14, the cell count of wgsl-solver.js:39) ----
+// One pass over the particles in storage order: mark tiles near live particles, count particles per cell with
+// warp-aggregated atomics (the returned base gives each particle a rank in its cell), count dead slots per block,
+// and the fastest speed (ctl[6], wgsl-solver.js:24).
+__global__ void __launch_bounds__(PBLK) k_count_mark(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  uint32_t key = DEADKEY;
+  bool live = false, dead = false;
+  float sp = 0.0f;
+  if (i < P.n) {
+    Part q = B.pb[i];
+    if (q.p.y < DEADY) dead = true;
+    else {
+      live = true;
+      int ci, cj, ck;
+      particleCell(P, xyz(q.p), ci, cj, ck);
+      key = cellIdx(P, ci, cj, ck);
+      markAround(P, B.need, ci, cj, ck);
+      sp = len3(xyz(q.v));
+    }
+    B.key[i] = key;
+  }
+  uint32_t peers = __match_any_sync(0xffffffffu, key);
+  int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (live && lane == leader) base = (uint32_t)atomicAdd(&B.cnt[key], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (live) B.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
+  // fastest speed: lengths are non-negative, so their bit patterns order like the floats
+  float m = sp;
+  for (int o = 16; o > 0; o >>= 1) m = fmx(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0 && m > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(m));
+  uint32_t nd = __syncthreads_count(dead);
+  if (threadIdx.x == 0) B.blkDead[blockIdx.x] = nd;
+}
+
+// tileMarkPhi (wgsl-narrowband.js:6-10): last step's tiles that hold water by depth keep storage.
+__global__ void __launch_bounds__(512) k_mark_phi(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive;   // still last step's count: read before the new list is built
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    if (inDom(P, i, j, k) && phiOfBits(B.ctype[c]) < 0.5f) markAround(P, B.need, i, j, k);
+  }
+}
+
+// fillPhi (wgsl-core.js:228-238) for box and sphere fills
+__device__ __forceinline__ float fillPhi(const FlipParams& P, V3 x) {
+  float d = 1.0e9f;
+  for (uint32_t k = 0; k < P.nfill; k++) {
+    const float* A = P.fills[k * 2];
+    const float* Bq = P.fills[k * 2 + 1];
+    if (A[0] < 1.5f) {
+      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
+      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
+    } else {
+      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
+    }
+  }
+  return d * P.ih;
+}
+
+// tileMarkFill (wgsl-narrowband.js:12-18): on a restart every tile the starting water reaches
+__global__ void k_mark_fill(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntiles; t += gridDim.x * blockDim.x) {
+    uint32_t tt = t / P.tx;
+    V3 tc = v3((float)(t % P.tx), (float)(tt % P.ty), (float)(tt / P.ty)) * 8.0f + v3(4.0f, 4.0f, 4.0f);
+    if (fillPhi(P, v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) B.need[t] = P.stamp;
+  }
+}
+
+// ---- 2. which tiles keep, get or lose storage (tileFree / tileAlloc / slotListBuild, wgsl-blocks.js:16-53) ----
+// Chunks of 1024 tiles: flags and per-chunk counts; tiles that lose storage go on the dropped list.
+__global__ void __launch_bounds__(1024) k_tile_flags(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  uint32_t t = blockIdx.x * 1024u + threadIdx.x;
+  bool now = false;
+  if (t < P.ntiles) {
+    uint8_t was = B.on[t];
+    now = B.need[t] == P.stamp;
+    B.on[t] = now ? 1 : 0;
+    B.tstate[t] = (uint8_t)((was ? 1 : 0) | (now ? 2 : 0));
+    if (was && !now) B.dropped[atomicAdd(&B.ctl->nDropped, 1u)] = t;
+  }
+  uint32_t c = __syncthreads_count(now);
+  if (threadIdx.x == 0) B.blkTiles[blockIdx.x] = c;
+}
+// The list of tiles with storage in ascending tile order, and each tile's position in it.
+__global__ void __launch_bounds__(1024) k_tile_list(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParams(P, B.P);
+  uint32_t part = 0;
+  for (uint32_t b = threadIdx.x; b < blockIdx.x; b += 1024) part += B.blkTiles[b];
+  uint32_t off;
+  blockExclusive(part, sm, &off);
+  uint32_t t = blockIdx.x * 1024u + threadIdx.x;
+  bool now = t < P.ntiles && B.on[t];
+  uint32_t tot;
+  uint32_t r = blockExclusive(now ? 1u : 0u, sm, &tot);
+  if (now) { B.active[off + r] = t; B.tileSlot[t] = off + r; }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) B.ctl->nActive = off + tot;
+}
+
+// ---- 3. new tiles (initNew, wgsl-blocks.js:37-47), tiles leaving storage, and per-tile counts ----
+// Active tiles: a new one starts with pressure 0, air, its collider per cell and no kept velocity.
+// Each active tile also gets the exclusive prefix of its cell counts and its particle total.
+// Dropped tiles go back to the state the reference's spare slot reads as.
+__global__ void __launch_bounds__(512) k_tile_prep(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nD = B.ctl->nDropped, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA + nD; a += gridDim.x) {
+    if (a < nA) {
+      uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+      if (B.tstate[t] == 2) {
+        int i, j, k;
+        tileCoord(P, t, threadIdx.x, i, j, k);
+        B.pres[c] = 0.0f;
+        B.ctype[c] = (uint32_t)(colAt(P, B.cols, B.sdf, cellCenter(P, i, j, k)) + 1) << 8;   // depth bits 0: air
+        B.velG[c] = 0.0f; B.velG[nc + c] = 0.0f; B.velG[2 * nc + c] = 0.0f;
+      }
+      uint32_t tot;
+      uint32_t ex = blockExclusive((uint32_t)B.cnt[c], sm, &tot);
+      B.cellOff[c] = ex;
+      if (threadIdx.x == 0) B.tileCnt[a] = tot;
+    } else {
+      uint32_t t = B.dropped[a - nA], c = t * 512u + threadIdx.x;
+      B.cnt[c] = 0; B.cntOther[c] = 0; B.ctype[c] = 0u; B.pres[c] = 0.0f; B.rhs[c] = 8.0f; B.sorInfo[c] = 0;
+      for (int p = 0; p < 6; p++) B.acc[p * nc + c] = 0;
+      for (int p = 0; p < 3; p++) { B.vn[p * nc + c] = 0.0f; B.vo[p * nc + c] = 0.0f; B.velG[p * nc + c] = 0.0f; }
+    }
+  }
+}
+
+// Exclusive scan of up to a few hundred thousand counts by one CTA; block 0 scans the per-tile particle counts
+// (total = live particles), block 1 the per-block dead counts. arr[n] receives the total.
+__device__ void scanOne(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
+  uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
+  uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
+  uint32_t s = 0;
+  for (uint32_t x = beg; x < end; x++) s += arr[x];
+  uint32_t tot;
+  uint32_t run = blockExclusive(s, sm, &tot);
+  for (uint32_t x = beg; x < end; x++) { uint32_t v = arr[x]; arr[x] = run; run += v; }
+  if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
+}
+__global__ void __launch_bounds__(1024) k_scan_counts(Bufs B) {
+  __shared__ uint32_t sm[33];
+  if (blockIdx.x == 0) scanOne(B.tileCnt, B.ctl->nActive, &B.ctl->nLive, sm);
+  else scanOne(B.blkDead, B.nblk, nullptr, sm);
+}
+
+// ---- 4. scatter: sorted position of every particle ----
+// Live: (tile offset + cell offset + rank from the atomic count); the order inside a cell is fixed to ascending id by
+// p2g. Dead: after all live ones, in storage order (a block scan keeps it stable); they are moved here directly.
+__global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParams(P, B.P);
+  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
+  uint32_t k = i < P.n ? B.key[i] : 0u;
+  bool dead = i < P.n && k == DEADKEY;
+  uint32_t r = blockExclusive(dead ? 1u : 0u, sm, nullptr);
+  if (i >= P.n) return;
+  if (!dead) {
+    uint32_t a = B.tileSlot[k >> 9];
+    uint32_t pos = B.tileCnt[a] + B.cellOff[k] + B.rank[i];
+    B.srcIdx[pos] = i;
+    B.spid[pos] = B.idb[i];
+  } else {
+    uint32_t pos = B.ctl->nLive + B.blkDead[blockIdx.x] + r;
+    B.pa[pos] = B.pb[i];
+    B.ida[pos] = B.idb[i];
+  }
+}
+
+// ---- 5. p2g (wgsl-solver.js:17-40) ----
+// One CTA per tile with storage. Its particles (a contiguous sorted segment) are gathered from the previous order,
+// written to their final place (ascending id inside each cell) and splatted into a 10^3-cell shared-memory window
+// (the tile plus one cell around it) in the reference's fixed point: i32(round(w * v * 65536)) and i32(round(w * 65536)).
+// Integer sums do not depend on order, so the window is flushed to HBM with plain atomic adds.
+constexpr int P2G_T = 256;
+__global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ int32_t win[6][1000];
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a];
+    const uint32_t tt = t / P.tx;
+    const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
+    for (int r = threadIdx.x; r < 6000; r += P2G_T) (&win[0][0])[r] = 0;
+    __syncthreads();
+    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
+    for (uint32_t base = s0; base < s1; base += P2G_T) {
+      // lanes of a warp take particles 8 apart, so they fall in different cells and their shared atomics rarely collide
+      const uint32_t s = base + (uint32_t)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
+      if (s >= s1) continue;
+      const uint32_t src = B.srcIdx[s], myid = B.spid[s];
+      const Part q = B.pb[src];
+      const V3 p = xyz(q.p), v = xyz(q.v);
+      int ci, cj, ck;
+      particleCell(P, p, ci, cj, ck);
+      const uint32_t key = cellIdx(P, ci, cj, ck);
+      const uint32_t cs = s0 + B.cellOff[key], ce = cs + (uint32_t)B.cnt[key];
+      uint32_t rk = 0;
+      for (uint32_t u = cs; u < ce; u++) rk += B.spid[u] < myid ? 1u : 0u;
+      B.pa[cs + rk] = q;
+      B.ida[cs + rk] = myid;
+      for (int axis = 0; axis < 3; axis++) {
+        V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+        if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+        const V3 f0 = vfloor(g), fr = g - f0;
+        const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+        const float vc = comp3(v, axis);
+        for (int c = 0; c < 8; c++) {
+          const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+          const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+          if (w <= 0.0f) continue;
+          int fi = i0 + dx, fj = j0 + dy, fk = k0 + dz;   // the face's cell, clamped as faceIndex does
+          if (axis == 0) { fi = clampi(fi, 0, (int)P.nx); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz - 1); }
+          else if (axis == 1) { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny); fk = clampi(fk, 0, (int)P.nz - 1); }
+          else { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz); }
+          const int widx = (fi - ox + 1) + 10 * ((fj - oy + 1) + 10 * (fk - oz + 1));
+          atomicAdd(&win[axis][widx], (int32_t)rintf(w * vc * P.scale));
+          atomicAdd(&win[3 + axis][widx], (int32_t)rintf(w * P.scale));
+        }
+      }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < 1000; r += P2G_T) {
+      const int gi = ox + (r % 10) - 1, gj = oy + (r / 10) % 10 - 1, gk = oz + r / 100 - 1;
+      if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)P.tx * 8 || gj >= (int)P.ty * 8 || gk >= (int)P.tz * 8) continue;
+      const uint32_t c = cellIdx(P, gi, gj, gk);
+      for (int pl = 0; pl < 6; pl++) {
+        const int32_t v = win[pl][r];
+        if (v != 0) atomicAdd(&B.acc[pl * nc + c], v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- 6. collider bits (solidBuild, wgsl-solver.js:42-45) + classify (wgsl-solver.js:47-74) ----
+__device__ __forceinline__ V3 velGVecAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x);
+__global__ void __launch_bounds__(512) k_classify(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    const V3 cx = cellCenter(P, i, j, k);
+    uint32_t ct = B.ctype[c];
+    ct = (ct & 0xffff00ffu) | ((uint32_t)(colAt(P, B.cols, B.sdf, cx) + 1) << 8);
+    const uint32_t sb = ct & 0xffffff00u;
+    const int32_t n = B.cnt[c];
+    uint32_t ty = 0;
+    if (!inDom(P, i, j, k)) ty = 0;
+    else if ((sb & 0xff00u) != 0u) ty = 2;
+    else if (P.nb != 0u && phiOfBits(ct) < -1.0f &&
+             (phiOfBits(ct) < -P.band || len3(velGVecAt(P, B.velG, nc, cx)) < 9.0f * P.h)) ty = 1;
+    else if (n > 0) {
+      ty = 1;
+      if ((float)n < P.sheetMin) {
+        const int32_t dth = (int32_t)ceilf(0.6f * P.rest);
+        bool dense = false;
+        for (int q = 0; q < 6; q++) {
+          int qi = i, qj = j, qk = k;
+          if (q == 0) qi -= 1; else if (q == 1) qi += 1; else if (q == 2) qj -= 1; else if (q == 3) qj += 1; else if (q == 4) qk -= 1; else qk += 1;
+          if (!inDom(P, qi, qj, qk)) continue;
+          if (B.cnt[cellIdx(P, qi, qj, qk)] >= dth) dense = true;
+        }
+        if (!dense) ty = 0;
+      }
+    }
+    B.ctype[c] = ty | sb;
+    if (ty != 1u) B.pres[c] = 0.0f;
+    const uint32_t nf = __syncthreads_count(ty == 1u);
+    if (threadIdx.x == 0 && nf) atomicAdd(&B.ctl->fluid, nf);
+  }
+}
+
+// ---- 7. normFaces (wgsl-solver.js:75-105) fused with divergence (wgsl-solver.js:107-123) ----
+// normBody: the face velocity from the fixed-point sums, gravity on y faces, collider or wall velocity on solid faces.
+__device__ __forceinline__ int colAtCell(const FlipParams& P, const uint32_t* __restrict__ ctype, int i, int j, int k) {
+  if (!inDom(P, i, j, k)) return -1;
+  return (int)((ctype[cellIdx(P, i, j, k)] >> 8) & 0xffu) - 1;
+}
+__device__ __forceinline__ void normBody(const FlipParams& P, const Bufs& B, int axis, int i, int j, int k, uint32_t c, float& vOut, float& oldOut) {
+  int li = i, lj = j, lk = k;
+  if (axis == 0) li -= 1; else if (axis == 1) lj -= 1; else lk -= 1;
+  const uint32_t tl = ctypeOf(P, B.ctype, li, lj, lk), th = ctypeOf(P, B.ctype, i, j, k);
+  const int32_t ws = B.acc[(3 + axis) * B.ncell + c], vs = B.acc[axis * B.ncell + c];
+  float v = ws > 0 ? (float)vs / (float)max(ws, 1) : 0.0f;
+  float old = v;
+  if (axis == 1) v -= P.gravity * P.dt;
+  if (tl == 2u || th == 2u) {
+    float sv = 0.0f;
+    int ci = -1;
+    if (tl == 2u) ci = colAtCell(P, B.ctype, li, lj, lk);
+    if (ci < 0 && th == 2u) ci = colAtCell(P, B.ctype, i, j, k);
+    if (ci >= 0) sv = comp3(colSurfVel(B.cols, (uint32_t)ci, facePos(P, i, j, k, axis)), axis);
+    v = sv;
+    old = sv;
+  }
+  vOut = v;
+  oldOut = old;
+}
+__global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ float svn[3][512];
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    for (int axis = 0; axis < 3; axis++) {
+      float v, old;
+      normBody(P, B, axis, i, j, k, c, v, old);
+      B.vn[axis * nc + c] = v;
+      B.vo[axis * nc + c] = old;
+      svn[axis][threadIdx.x] = v;
+    }
+    __syncthreads();
+    const uint32_t ct = B.ctype[c];
+    if ((ct & 0xffu) != 1u) {
+      B.rhs[c] = 0.0f;
+      B.sorInfo[c] = 0;
+    } else {
+      float d, o2;
+      float vxp, vyp, vzp;
+      if (lx < 7) vxp = svn[0][threadIdx.x + 1]; else { normBody(P, B, 0, i + 1, j, k, cellIdx(P, i + 1, j, k), d, o2); vxp = d; }
+      if (ly < 7) vyp = svn[1][threadIdx.x + 8]; else { normBody(P, B, 1, i, j + 1, k, cellIdx(P, i, j + 1, k), d, o2); vyp = d; }
+      if (lz < 7) vzp = svn[2][threadIdx.x + 64]; else { normBody(P, B, 2, i, j, k + 1, cellIdx(P, i, j, k + 1), d, o2); vzp = d; }
+      const float div = (vxp - svn[0][threadIdx.x] + vyp - svn[1][threadIdx.x] + vzp - svn[2][threadIdx.x]) * P.ih;
+      bool interior = true;
+      uint32_t mask = 0, nns = 0;
+      for (int q = 0; q < 6; q++) {
+        int qi = i, qj = j, qk = k;
+        if (q == 0) qi -= 1; else if (q == 1) qi += 1; else if (q == 2) qj -= 1; else if (q == 3) qj += 1; else if (q == 4) qk -= 1; else qk += 1;
+        const uint32_t ty = ctypeOf(P, B.ctype, qi, qj, qk);
+        if (ty == 0u) interior = false;
+        if (ty != 2u) nns++;
+        if (ty == 1u) mask |= 1u << q;
+      }
+      const float dens = (float)B.cnt[c] / P.rest - 1.0f;
+      float tgt = P.comp * (interior ? dens : fmx(dens, 0.0f));
+      if (P.nb != 0u && phiOfBits(ct) < -1.0f) tgt = 0.0f;
+      B.rhs[c] = (tgt - div) * P.h * P.h / P.dt;
+      B.sorInfo[c] = (uint16_t)(0x8000u | (nns << 8) | mask);
+    }
+    __syncthreads();
+  }
+}
+
+// ---- 8. red-black SOR (relax, wgsl-solver.js:124-140; rbRed/rbBlack :162-164) ----
+// One CTA per tile, one thread per cell of the colour. sorInfo holds the neighbour types found after classify.
+__global__ void __launch_bounds__(256) k_sor(Bufs B, uint32_t color) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive;
+  const int lz = threadIdx.x >> 5, ly = (threadIdx.x >> 2) & 7;
+  const int lx = 2 * (threadIdx.x & 3) + (int)((ly + lz + color) & 1);
+  const uint32_t local = (uint32_t)(lx + 8 * (ly + 8 * lz));
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + local;
+    const uint32_t info = B.sorInfo[c];
+    if (!(info & 0x8000u)) continue;
+    const uint32_t nns = (info >> 8) & 7u;
+    if (nns == 0u) { B.pres[c] = 0.0f; continue; }
+    int i, j, k;
+    tileCoord(P, t, local, i, j, k);
+    float sum = 0.0f;
+    if (info & 1u) sum += B.pres[cellIdx(P, i - 1, j, k)];
+    if (info & 2u) sum += B.pres[cellIdx(P, i + 1, j, k)];
+    if (info & 4u) sum += B.pres[cellIdx(P, i, j - 1, k)];
+    if (info & 8u) sum += B.pres[cellIdx(P, i, j + 1, k)];
+    if (info & 16u) sum += B.pres[cellIdx(P, i, j, k - 1)];
+    if (info & 32u) sum += B.pres[cellIdx(P, i, j, k + 1)];
+    const float pg = (B.rhs[c] + sum) / (float)nns;
+    const float p0 = B.pres[c];
+    B.pres[c] = p0 + P.omega * (pg - p0);
+  }
+}
+
+// ---- 9. project (wgsl-solver.js:165-180) + saveVel (wgsl-narrowband.js:88-91) ----
+// Also clears this step's fixed-point sums and the other cell-count buffer, ready for the next step.
+__global__ void __launch_bounds__(512) k_project(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
+    int i, j, k;
+    tileCoord(P, t, threadIdx.x, i, j, k);
+    const uint32_t th = ctypeOf(P, B.ctype, i, j, k);
+    for (int axis = 0; axis < 3; axis++) {
+      int li = i, lj = j, lk = k;
+      if (axis == 0) li -= 1; else if (axis == 1) lj -= 1; else lk -= 1;
+      const uint32_t tl = ctypeOf(P, B.ctype, li, lj, lk);
+      float vnew = B.vn[axis * nc + c];
+      if (!(tl == 2u || th == 2u) && (tl == 1u || th == 1u)) {
+        float pl = 0.0f, ph = 0.0f;
+        if (tl == 1u) pl = B.pres[cellIdx(P, li, lj, lk)];
+        if (th == 1u) ph = B.pres[c];
+        vnew = vnew - P.dt * P.ih * (ph - pl);
+        B.vn[axis * nc + c] = vnew;
+      }
+      if (P.nb) B.velG[axis * nc + c] = vnew;
+    }
+    for (int pl = 0; pl < 6; pl++) B.acc[pl * nc + c] = 0;
+    B.cntOther[c] = 0;
+  }
+}
+
+// ---- 10. g2p (wgsl-solver.js:208-275) with sampleBoth (wgsl-core.js:138-154) and collideP (wgsl-solver.js:185-197) ----
+__device__ __forceinline__ void sampleBoth(const FlipParams& P, const Bufs& B, V3 p, V3& vn, V3& vo) {
+  const uint32_t nc = B.ncell;
+  float rn[3], ro[3];
+  for (int axis = 0; axis < 3; axis++) {
+    V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+    if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+    const V3 f0 = vfloor(g), fr = g - f0;
+    const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    float sn = 0.0f, so = 0.0f;
+    for (int c = 0; c < 8; c++) {
+      const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      const uint32_t f = faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz);
+      sn += w * B.vn[axis * nc + f];
+      so += w * B.vo[axis * nc + f];
+    }
+    rn[axis] = sn;
+    ro[axis] = so;
+  }
+  vn = v3(rn[0], rn[1], rn[2]);
+  vo = v3(ro[0], ro[1], ro[2]);
+}
+__device__ __forceinline__ V3 collideP(const FlipParams& P, const Bufs& B, V3 pin) {
+  V3 p = pin;
+  const float m = P.margin;
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    if (!colNear(P, B.cols, k, p)) continue;
+    float phi; V3 wn;
+    sdfEval(B.cols, B.sdf, k, p, phi, wn);
+    if (phi < P.q0) p = p + wn * (P.q0 - phi);
+  }
+  const float big = 1.0e9f;
+  const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
+  const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
+  return vclamp(p, lo, hi);
+}
+__device__ __forceinline__ float hsh3(V3 p) {
+  V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f);
+  q = q - vfloor(q);
+  q = q * 17.0f;
+  const float r = q.x * q.y * q.z * (q.x + q.y + q.z);
+  return r - floorf(r);
+}
+__device__ float vnz(V3 x) {   // value noise (wgsl-solver.js:202-207)
+  const V3 i = vfloor(x), fr = x - vfloor(x);
+  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
+  const float a = mixf(mixf(hsh3(i), hsh3(i + v3(1, 0, 0)), u.x), mixf(hsh3(i + v3(0, 1, 0)), hsh3(i + v3(1, 1, 0)), u.x), u.y);
+  const float b = mixf(mixf(hsh3(i + v3(0, 0, 1)), hsh3(i + v3(1, 0, 1)), u.x), mixf(hsh3(i + v3(0, 1, 1)), hsh3(i + v3(1, 1, 1)), u.x), u.y);
+  return mixf(a, b, u.z);
+}
+__global__ void __launch_bounds__(256) k_g2p(Bufs B) {
+  __shared__ FlipParams P;
+  loadParams(P, B.P);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
+    Part q = B.pa[i];
+    if (q.p.y < DEADY) continue;
+    const V3 p = xyz(q.p), v0 = xyz(q.v);
+    int fi, fj, fk;
+    particleCell(P, p, fi, fj, fk);
+    V3 vn = v0 - v3(0.0f, P.gravity * P.dt, 0.0f), vo = v0;
+    if (B.on[tileOf(P, fi, fj, fk)]) sampleBoth(P, B, p, vn, vo);
+    V3 v = vmix(vn, v0 + (vn - vo), P.flip);
+    const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+    const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+    float csum = 8.0f * P.rest;
+    const bool fast = P.q12 > 0.5f;
+    if (P.q9 < 0.5f && fast) csum = 8.0f * (float)B.cnt[cellIdx(P, fi, fj, fk)];
+    else if (P.q9 < 0.5f) {
+      csum = 0.0f;
+      for (int dz = 0; dz <= 1; dz++)
+        for (int dy = 0; dy <= 1; dy++)
+          for (int dx = 0; dx <= 1; dx++)
+            csum += (float)B.cnt[cellIdx(P, clampi(bi + dx, 0, (int)P.nx - 1), clampi(bj + dy, 0, (int)P.ny - 1), clampi(bk + dz, 0, (int)P.nz - 1))];
+    }
+    const float rho = csum / (8.0f * P.rest);
+    const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
+    const float shield = smoothstepf(0.1f, 0.65f, rho);
+    const float exposure = 1.0f - 0.97f * shield;
+    const float spd0 = len3(v);
+    const float sens = fmx(P.q6, 0.05f);
+    const float pacc = len3(vn - vo) / P.dt;
+    const float settle = smoothstepf(0.1f, 0.5f, P.q8);
+    const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
+    const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
+    const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
+    const float tau = fmx(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
+    float foam = q.v.w * expf(-P.dt / tau);
+    foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
+    V3 gust = v3(0.0f, 0.0f, 0.0f);
+    if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
+      const V3 gp = p * 0.55f;
+      const float tt = P.q8 * 0.6f;
+      gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
+    }
+    const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
+    const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
+    v = v + (airv - v) * (1.0f - expf(-kd * P.dt));
+    const float sp = len3(v);
+    if (sp > P.vmax) v = v * (P.vmax / sp);
+    const V3 pt = p + v * P.dt;
+    const V3 pc = collideP(P, B, pt);
+    const V3 dsp = pc - pt;
+    if (dot3(dsp, dsp) > 1.0e-12f) {
+      const V3 nrm = dsp / len3(dsp);
+      const float vd = dot3(v, nrm);
+      if (vd < 0.0f) v = v - nrm * vd;
+    }
+    const uint32_t o = P.open;
+    if (o != 0u && (((o & 1u) && pc.x < P.x0) || ((o & 2u) && pc.x > P.x1) || ((o & 4u) && pc.y < P.y0) ||
+                    ((o & 8u) && pc.y > P.y1) || ((o & 16u) && pc.z < P.z0) || ((o & 32u) && pc.z > P.z1))) {
+      q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+      q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+      q.p = make_float4(pc.x, pc.y, pc.z, fmn(len3(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f));
+      q.v = make_float4(v.x, v.y, v.z, foam);
+    }
+    B.pa[i] = q;
+  }
+}
+
+// ---- velG sampling (velGAxis, wgsl-core.js:185-197), used by classify and the narrow band ----
+__device__ __forceinline__ float velGAxisAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x, int axis) {
+  V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
+  if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+  const V3 f0 = vfloor(g), fr = g - f0;
+  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  float s = 0.0f;
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    s += w * velG[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
+  }
+  return s;
+}
+__device__ __forceinline__ V3 velGVecAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
+  return v3(velGAxisAt(P, velG, nc, x, 0), velGAxisAt(P, velG, nc, x, 1), velGAxisAt(P, velG, nc, x, 2));
+}
+
+// unsort for readback (wgsl-blocks.js:97-99): id order into dst (pos and vel)
+__global__ void k_unsort(const Part* __restrict__ src, const uint32_t* __restrict__ ids, uint32_t n, float4* __restrict__ pos, float4* __restrict__ vel) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t id = ids[i];
+    if (id >= n) continue;
+    const Part q = src[i];
+    pos[id] = q.p;
+    if (vel) vel[id] = q.v;
+  }
+}
+
+// the state an inactive tile holds (the reference's spare slot): rhs 8, everything else 0
+__global__ void k_fill_f32(float* p, float v, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_iota(uint32_t* p, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
+// ---- launchers ----
+void launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<B.nblk, PBLK, 0, s>>>(B); }
+void launch_mark_phi(const Bufs& B, int grid, cudaStream_t s) { k_mark_phi<<<grid, 512, 0, s>>>(B); }
+void launch_mark_fill(const Bufs& B, int grid, cudaStream_t s) { k_mark_fill<<<grid, 256, 0, s>>>(B); }
+void launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
+  uint32_t nb = (ntiles + 1023) / 1024;
+  k_tile_flags<<<nb, 1024, 0, s>>>(B);
+  k_tile_list<<<nb, 1024, 0, s>>>(B);
+  k_tile_prep<<<grid, 512, 0, s>>>(B);
+}
+void launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); }
+void launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, PBLK, 0, s>>>(B); }
+void launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); }
+void launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); }
+void launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); }
+void launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s) {
+  for (int it = 0; it < iters; it++) { k_sor<<<grid, 256, 0, s>>>(B, 0u); k_sor<<<grid, 256, 0, s>>>(B, 1u); }
+}
+void launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); }
+void launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s) { if (n) k_g2p<<<(n + 255) / 256, 256, 0, s>>>(B); }
+void launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {
+  if (n) k_unsort<<<(n + 255) / 256, 256, 0, s>>>(src, ids, n, pos, vel);
+}
+void launch_fill_f32(float* p, float v, size_t n, cudaStream_t s) { if (n) k_fill_f32<<<1024, 256, 0, s>>>(p, v, n); }
+void launch_iota(uint32_t* p, uint32_t n, cudaStream_t s) { if (n) k_iota<<<1024, 256, 0, s>>>(p, n); }
+
+}  // namespace st

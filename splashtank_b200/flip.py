@@ -1,0 +1,345 @@
+"""FlipSim: the reference simulator's per-step API (src/flip/sim.js FlipSim) over the C ABI.
+
+Method and field names follow the JavaScript class so callers (a scene runner, a bake loop, tests) read the
+same: ``step(dt, o)``, ``add``, ``fillBox``, ``fillSphere``, ``readbackInto``, ``readSpray``, ``clear``,
+``setCap``, ``stepTimed``, ``activeCells``, ``stats``, ``N``, ``MAXN``, ``h``, ``b``.  The options object
+``o`` is a dict with the reference's keys (g, iters, flip, comp, omega, vmax, wind, drag, foamTau, foamSens,
+gust, tear, vs, cols, spr, nb).
+
+The compute runs in libsplashtank_cuda.so (hand-written sm_100a kernels).  There is no CPU fallback: if the
+library or a GPU is missing, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB = None
+_FUNCS = None
+
+
+def lib_path():
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsplashtank_cuda.so")
+
+
+def load_library():
+    """Load the CUDA library (raises OSError when it has not been built)."""
+    global _LIB, _FUNCS
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise OSError("splashtank_b200: %s is missing; build it with `python -m splashtank_b200.build`" % path)
+        lib = C.CDLL(path)
+        funcs = abi.bind(lib, "st_", abi.FLIP_FUNCS + abi.CUDA_ONLY_FUNCS)
+        _LIB, _FUNCS = lib, funcs
+    return _LIB, _FUNCS
+
+
+class StError(RuntimeError):
+    pass
+
+
+def _f32(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(abi.f32p)
+
+
+class _ColliderPack:
+    """Keeps the ctypes collider records and SDF blobs alive for one call."""
+
+    def __init__(self, cols):
+        self.sdfs, self.keep = {}, []
+        n = len(cols)
+        self.arr = (abi.Collider * max(n, 1))()
+        for k, c in enumerate(cols):
+            sd = c["sdf"]
+            sid = int(sd["id"])
+            if sid not in self.sdfs:
+                data = np.ascontiguousarray(sd["data"], dtype=np.float32)
+                s = abi.Sdf()
+                s.id = sid
+                s.dims[:] = [int(x) for x in sd["dims"]]
+                s.origin[:] = [float(x) for x in sd["origin"]]
+                s.cell = float(sd["cell"])
+                s.data = data.ctypes.data_as(abi.f32p)
+                self.keep.append(data)
+                self.sdfs[sid] = s
+            r = self.arr[k]
+            r.sdf = C.pointer(self.sdfs[sid])
+            r.pos[:] = [float(c.get("x", 0)), float(c.get("y", 0)), float(c.get("z", 0))]
+            r.R[:] = [float(x) for x in c.get("R", (1, 0, 0, 0, 1, 0, 0, 0, 1))]
+            r.vel[:] = [float(c.get("vx", 0)), float(c.get("vy", 0)), float(c.get("vz", 0))]
+            r.ang[:] = [float(c.get("wx", 0)), float(c.get("wy", 0)), float(c.get("wz", 0))]
+        self.n = n
+
+
+def make_opts(o, opt=None, default=None):
+    """The options object o (src/flip/sim.js:185-230) as an st_step_opts; returns (opts, keepalive)."""
+    s = default if default is not None else abi.default_opts()
+    opt = opt or {}
+    s.g = float(o.get("g", 9.81))
+    s.iters = int(opt.get("iters") or o.get("iters", 30))
+    for key, field in (("flip", "flip"), ("comp", "comp"), ("omega", "omega"), ("vmax", "vmax"), ("drag", "drag"),
+                       ("foamTau", "foam_tau"), ("foamSens", "foam_sens"), ("gust", "gust"), ("tear", "tear"), ("vs", "vs")):
+        if o.get(key) is not None:
+            setattr(s, field, float(o[key]))
+    w = o.get("wind") or (0, 0, 0)
+    s.wind[:] = [float(x) for x in w]
+    flags = 0
+    if opt.get("noFoam"):
+        flags |= abi.ST_OPT_NO_FOAM
+    if opt.get("noCull"):
+        flags |= abi.ST_OPT_NO_CULL
+    if opt.get("fastAir"):
+        flags |= abi.ST_OPT_FAST_AIR
+    s.flags = flags
+    cols = _ColliderPack(o.get("cols") or [])
+    s.ncols = cols.n
+    s.cols = C.cast(cols.arr, C.POINTER(abi.Collider))
+    sp = o.get("spr")
+    s.spray_on = 1 if sp else 0
+    if sp:
+        for key in ("rate", "min", "life", "mist", "drag", "mdrag"):
+            setattr(s.spray, key, float(sp.get(key, 0)))
+        ww = sp.get("ww") or {}
+        s.spray.foam_life = float(ww.get("foamLife") or 3.0)
+        s.spray.rise = float(ww.get("rise") or 0.3)
+        s.spray.crest = float(ww["crest"]) if ww.get("crest") is not None else 1.0
+        s.spray.impact = float(ww["impact"]) if ww.get("impact") is not None else 0.5
+    nb = o.get("nb")
+    s.nb_on = 1 if (nb and nb.get("on")) else 0
+    s.nb_band = float(max(2.0, (nb or {}).get("band") or 3.0))
+    return s, cols
+
+
+class FlipSim:
+    """The FLIP water solver on a sparse MAC grid of 8^3 tiles (src/flip/sim.js:46)."""
+
+    _prefix = "st_"
+
+    def __init__(self, d, maxN, size=None, open=0, ratio=2.0, spray_cap=0, device=0, _funcs=None):
+        self.f = _funcs if _funcs is not None else load_library()[1]
+        desc = abi.FlipDesc()
+        desc.size = C.sizeof(abi.FlipDesc)
+        desc.d = float(d)
+        desc.ratio = float(ratio or 2.0)
+        sz = size or (3.0, 2.6, 3.0)
+        desc.box[:] = [float(x) for x in sz]
+        desc.open = int(open)
+        desc.max_n = int(maxN)
+        desc.spray_cap = int(spray_cap)
+        desc.device = int(device)
+        h = C.c_void_p()
+        self._check(self.f["flip_create"](C.byref(desc), C.byref(h)), "create")
+        self._h = h
+        dims = abi.Dims()
+        self.f["flip_get_dims"](self._h, C.byref(dims))
+        self.d = float(d)
+        self.ratio = max(1.4, min(4.0, float(ratio or 2.0)))
+        self.h = float(dims.h)
+        self.rest = self.ratio ** 3
+        self.nx, self.ny, self.nz = dims.nx, dims.ny, dims.nz
+        self.tx, self.ty, self.tz = dims.tx, dims.ty, dims.tz
+        self.ntiles = self.tx * self.ty * self.tz
+        self.ncell = self.nx * self.ny * self.nz
+        self.b = dict(x0=dims.x0, y0=dims.y0, z0=dims.z0, x1=dims.x1, y1=dims.y1, z1=dims.z1)
+        self.size = [self.nx * self.h, self.ny * self.h, self.nz * self.h]
+        self.open = int(open)
+        self.MAXN = int(maxN)
+        self.cap = int(maxN)
+        self.sprayCap = int(spray_cap)
+        self.opt = {"noFoam": False, "noCull": False, "fastAir": False, "iters": 0}
+        self.stats = None
+        self.lastMs = 0.0
+        self._pend_p, self._pend_v = [], []
+        self._n_host = 0
+
+    def _check(self, st, what):
+        if st not in (abi.ST_OK, abi.ST_NOT_READY):
+            msg = ""
+            if "last_error" in self.f:
+                e = self.f["last_error"]()
+                msg = e.decode() if e else ""
+            raise StError("%s failed: %s %s" % (what, abi.STATUS_NAMES[st] if st < len(abi.STATUS_NAMES) else st, msg))
+        return st
+
+    @property
+    def N(self):
+        self.flushRun()
+        s = abi.Stats()
+        self._check(self.f["flip_stats"](self._h, C.byref(s)), "stats")
+        return s.n
+
+    def setCap(self, c):
+        self.flushRun()
+        self.cap = min(int(c), self.MAXN)
+        self._check(self.f["flip_set_cap"](self._h, self.cap), "setCap")
+
+    def clear(self):
+        self._pend_p, self._pend_v = [], []
+        self._check(self.f["flip_clear"](self._h), "clear")
+
+    def add(self, x, y, z, vx, vy, vz):
+        """FlipSim.add (src/gpu.js:390-402); buffered until flushRun."""
+        self._pend_p.append((x, y, z))
+        self._pend_v.append((vx, vy, vz))
+        return True
+
+    def add_many(self, pos3, vel3=None):
+        """Many add() calls at once; returns how many were taken."""
+        self.flushRun()
+        p = np.ascontiguousarray(pos3, dtype=np.float32).reshape(-1, 3)
+        v = np.zeros_like(p) if vel3 is None else np.ascontiguousarray(vel3, dtype=np.float32).reshape(-1, 3)
+        got = C.c_uint32()
+        self._check(self.f["flip_add"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), len(p), C.byref(got)), "add")
+        return got.value
+
+    def flushRun(self):
+        if not self._pend_p:
+            return
+        p, v = self._pend_p, self._pend_v
+        self._pend_p, self._pend_v = [], []
+        self.add_many(np.array(p, np.float32), np.array(v, np.float32))
+
+    def fillBox(self, x0, x1, y0, y1, z0, z1, rng=None):
+        """FluidSim.fillBox (src/shared.js:285-291) with a seeded jitter source."""
+        rng = rng or np.random.default_rng(0)
+        d = self.d
+        j = 0.01 * d / 0.12
+        ys = np.arange(y0 + d / 2, y1, d)
+        xs = np.arange(x0 + d / 2, x1, d)
+        zs = np.arange(z0 + d / 2, z1, d)
+        Y, X, Z = np.meshgrid(ys, xs, zs, indexing="ij")
+        p = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+        p = p + (rng.random(p.shape) - 0.5) * j
+        return self.add_many(p)
+
+    def fillSphere(self, cx, cy, cz, R, vx=0, vy=0, vz=0, rng=None):
+        """FluidSim.fillSphere (src/shared.js:292-297) with a seeded jitter source."""
+        rng = rng or np.random.default_rng(0)
+        d = self.d
+        j = 0.01 * d / 0.12
+        r = np.arange(-R, R + 1e-12, d)
+        Y, X, Z = np.meshgrid(r, r, r, indexing="ij")
+        m = X ** 2 + Y ** 2 + Z ** 2 <= R * R
+        p = np.stack([X[m] + cx, Y[m] + cy, Z[m] + cz], 1)
+        p = p + (rng.random(p.shape) - 0.5) * j
+        v = np.tile(np.array([vx, vy, vz], np.float32), (len(p), 1))
+        return self.add_many(p, v)
+
+    def step(self, dt, o):
+        """FlipSim.step (src/flip/sim.js:179-241); returns the number of colliders used."""
+        self.flushRun()
+        s, keep = make_opts(o, self.opt)
+        st = self.f["flip_step"](self._h, float(dt), C.byref(s))
+        self._check(st, "step")
+        del keep
+        return min(len(o.get("cols") or []), 32)
+
+    def stepTimed(self, dt, o):
+        """FlipSim.stepTimed (src/flip/sim.js:312-331): device ms per stage."""
+        self.flushRun()
+        s, keep = make_opts(o, self.opt)
+        t = abi.StageTimes()
+        self._check(self.f["flip_step_timed"](self._h, float(dt), C.byref(s), C.byref(t)), "stepTimed")
+        del keep
+        return {n: getattr(t, n) for n in abi.STAGES}
+
+    def readStats(self):
+        s = abi.Stats()
+        self._check(self.f["flip_stats"](self._h, C.byref(s)), "stats")
+        self.stats = dict(sc=s.sc, ovf=s.ovf, fluid=s.fluid, vmax=s.vmax, n=s.n, live=s.live, spray_used=s.spray_used, steps=s.steps)
+        return self.stats
+
+    def activeCells(self):
+        return self.readStats()["fluid"]
+
+    def readbackInto(self, dst=None, vel=None):
+        """Particles in id order (src/flip/sim.js:439-455); returns (n, pos4[, vel4])."""
+        self.flushRun()
+        n = self.N
+        if dst is None:
+            dst = np.zeros((max(n, 1), 4), np.float32)
+        pv = None if vel is None else vel.ctypes.data_as(abi.f32p)
+        got = C.c_uint32()
+        self._check(self.f["flip_read_particles"](self._h, dst.ctypes.data_as(abi.f32p), pv, dst.size // 4, C.byref(got)), "readback")
+        return got.value
+
+    def particles(self):
+        n = self.N
+        p = np.zeros((n, 4), np.float32)
+        v = np.zeros((n, 4), np.float32)
+        got = C.c_uint32()
+        self._check(self.f["flip_read_particles"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), n, C.byref(got)), "readback")
+        return p, v
+
+    def readSpray(self):
+        """FlipSim.readSpray (src/flip/sim.js:423-437)."""
+        if not self.sprayCap:
+            return None
+        p = np.zeros((self.sprayCap, 4), np.float32)
+        v = np.zeros((self.sprayCap, 4), np.float32)
+        n = C.c_uint32()
+        self._check(self.f["flip_read_spray"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.sprayCap, C.byref(n)), "readSpray")
+        return dict(n=n.value, p=p[: n.value], v=v[: n.value])
+
+    def grid(self):
+        """Every cell of the tile box: tile_on, cnt, ctype, pres, rhs, vn, vo, velg (dense numpy arrays)."""
+        NX, NY, NZ = self.tx * 8, self.ty * 8, self.tz * 8
+        nc = NX * NY * NZ
+        out = dict(tile_on=np.zeros(self.ntiles, np.uint8), cnt=np.zeros(nc, np.int32), ctype=np.zeros(nc, np.uint32),
+                   pres=np.zeros(nc, np.float32), rhs=np.zeros(nc, np.float32), vn=np.zeros(nc * 3, np.float32),
+                   vo=np.zeros(nc * 3, np.float32), velg=np.zeros(nc * 3, np.float32))
+        g = abi.Grid()
+        g.tile_on = out["tile_on"].ctypes.data_as(abi.u8p)
+        g.cnt = out["cnt"].ctypes.data_as(abi.i32p)
+        g.ctype = out["ctype"].ctypes.data_as(abi.u32p)
+        for k in ("pres", "rhs", "vn", "vo", "velg"):
+            setattr(g, k, out[k].ctypes.data_as(abi.f32p))
+        self._check(self.f["flip_read_grid"](self._h, C.byref(g)), "read_grid")
+        shp = (NZ, NY, NX)
+        for k in ("cnt", "ctype", "pres", "rhs"):
+            out[k] = out[k].reshape(shp)
+        for k in ("vn", "vo", "velg"):
+            out[k] = out[k].reshape(shp + (3,))
+        return out
+
+    def save_state(self):
+        """(pos4, vel4, pid) in storage order."""
+        n = self.N
+        p = np.zeros((n, 4), np.float32)
+        v = np.zeros((n, 4), np.float32)
+        i = np.zeros(n, np.uint32)
+        got = C.c_uint32()
+        self._check(self.f["flip_save_state"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p),
+                                              i.ctypes.data_as(abi.u32p), n, C.byref(got)), "save_state")
+        return p, v, i
+
+    def load_state(self, pos4, vel4, pid, t=0.0, seed=0):
+        p = np.ascontiguousarray(pos4, np.float32).reshape(-1, 4)
+        v = np.ascontiguousarray(vel4, np.float32).reshape(-1, 4)
+        i = np.ascontiguousarray(pid, np.uint32).reshape(-1)
+        self._check(self.f["flip_load_state"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p),
+                                              i.ctypes.data_as(abi.u32p), len(p), float(t), int(seed)), "load_state")
+
+    def nb_fills(self, boxes=(), spheres=(), mode=1):
+        """Starting water of the narrow band (sim.nbFills written by nbSeed, src/shared.js:849-851)."""
+        b = np.ascontiguousarray(np.array(boxes, np.float32).reshape(-1, 6))
+        s = np.ascontiguousarray(np.array(spheres, np.float32).reshape(-1, 4))
+        self._check(self.f["flip_nb_fills"](self._h, b.ctypes.data_as(abi.f32p), len(b), s.ctypes.data_as(abi.f32p), len(s), int(mode)), "nb_fills")
+
+    def stream(self):
+        return self.f["flip_stream"](self._h)
+
+    def destroy(self):
+        if getattr(self, "_h", None):
+            self.f["flip_destroy"](self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
