@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FLIP step: particle-steps/s on the full-feature 256^3 wave tank (one JSON line).
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload wave_tank_256|dam_break_64]
+
+One process per GPU (torchrun for N > 1, NCCL only for the barrier and the max/sum of the numbers). The FLIP step of
+one tank does not shard, so N GPUs run N independent replica tanks (weak scaling) and value is the total over them.
+Timing: W untimed steps, then K steps bracketed by a barrier and a device synchronise, CUDA events on the library's own
+stream, the max over ranks. The working set (particles about 1.4 GB, grid about 0.6 GB) is larger than the 126 MB L2,
+so no flush is needed between steps. --impl reference times the CPU restatement of the reference step (the oracle; the
+reference's own step exists only as WGSL for a browser) on the host cores, on a bounded sample of the same scene.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="wave_tank_256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=40)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- workloads
+def workload(name):
+    from splashtank_b200 import scenes
+    if name.startswith("wave_tank"):
+        n = int(name.rsplit("_", 1)[1])
+        return scenes.WaveTank(n)
+    if name.startswith("dam_break"):
+        n = int(name.rsplit("_", 1)[1])
+        sc = scenes.dam_break(n)
+
+        class Dam:
+            pass
+        w = Dam()
+        w.__dict__.update(sc)
+        w.states = lambda t: []
+        w.spray_cap = 0
+        w.opts = sc["opts"]
+
+        def make(cls, **kw):
+            s = cls(sc["d"], len(sc["pos"]), size=sc["size"], ratio=sc["ratio"], **kw)
+            s.add_many(sc["pos"], sc["vel"])
+            return s
+        w.make = make
+        return w
+    raise SystemExit("unknown workload " + name)
+
+
+def config_of(name, w, n_live):
+    cfg = {"workload": name, "particles": int(n_live), "dt": w.dt, "steps_per_run": getattr(w, "steps", None),
+           "l2": "working set larger than L2 (126 MB): no flush", "parallelism": "replicas"}
+    if name.startswith("wave_tank"):
+        cfg.update(grid=[w.n] * 3, tile="8^3", sor_iters=w.opts["iters"], narrow_band="full depth (band 1e4)",
+                   colliders="piston box 0.5 Hz amp 0.05 + sphere r 0.1 on a linear path", whitewater_cap=w.spray_cap,
+                   pbf="not in this step")
+    return cfg
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, dev):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- algorithmic bytes per stage
+def stage_bytes(stage, n, cells, fluid, iters):
+    """Algorithmic HBM bytes of one launch of the stage's main kernel, and launches per step.
+    n live particles, cells = 512 x tiles with storage, fluid = fluid cells. Per unit: a particle is 32 B (pos, vel),
+    a cell's face data 24 B (three faces, two numbers each), cell count 4 B, pressure/rhs 4 B each, SOR info 2 B."""
+    if stage == "g2p":        # read particle and write it back; read vn, vo of every face once, cell counts once
+        return n * 64 + cells * (24 + 4), 1
+    if stage == "p2g":        # read particle (and its id) from the old order, write it in sorted order; splat into face sums
+        return n * 72 + cells * 24, 1
+    if stage == "pressure":   # one colour sweep: own sorInfo, rhs, p read and p written; the other colour's p read once
+        return fluid * (2 + 4 + 4 + 4) // 2 + fluid * 4 // 2, 2 * iters
+    if stage == "blocks":     # read particle, write key and rank; sort scatter reads them, writes source index and id
+        return n * (32 + 8 + 8 + 8), 1
+    if stage == "norm_faces":  # read face sums, write vn and vo; read types, counts; write rhs and SOR info
+        return cells * (24 + 24 + 4 + 4 + 4 + 2), 1
+    if stage == "classify":
+        return cells * (4 + 4 + 4 + 4), 1
+    if stage == "project":    # vn read and written, p and types read, sums and other count buffer cleared
+        return cells * (12 + 12 + 4 + 4 + 24 + 4), 1
+    if stage == "narrow_band":
+        return cells * (4 + 4 + 12) * 4, 4
+    if stage == "reseed":
+        return n * (32 + 4), 1
+    if stage == "spray":
+        return n * 32, 1
+    return None, 1
+
+
+def roofline(stage_ms, nsteps, n, cells, fluid, iters, peak, peak_src):
+    dom = max((k for k in stage_ms if k != "total"), key=lambda k: stage_ms[k])
+    b, launches = stage_bytes(dom, n, cells, fluid, iters)
+    if not b or stage_ms[dom] <= 0:
+        return None
+    per_launch_ms = stage_ms[dom] / (nsteps * launches)
+    achieved = b / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            t = json.load(open(tf))
+            ent = t.get(dom)
+            if ent and ent.get("particles"):
+                traffic = ent["bytes_per_launch"] * (n / ent["particles"])
+        except Exception:
+            traffic = None
+    return {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": traffic,
+            "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per_launch_ms, 5),
+            "stage_share": round(stage_ms[dom] / stage_ms["total"], 4)}
+
+
+def measured_peak():
+    try:
+        p = json.load(open(PEAKS))
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM, "fallback 6.65 TB/s"
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle)
+def cpu_sample(name, steps_cap=None, budget_s=20.0, threads=None):
+    """Time the CPU restatement (all host threads) on a bounded sample: the same scene at 96^3 (wave tank) or 64^3."""
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.scene import SceneRunner
+    sample = "wave_tank_96" if name.startswith("wave_tank") else name
+    w = workload(sample)
+    th = threads or os.cpu_count() or 1
+    sim = w.make(OracleFlipSim, threads=th)
+    run = SceneRunner(sim)
+    t, k, t0 = 0.0, 0, time.perf_counter()
+    live = None
+    while True:
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+        k += 1
+        if live is None:
+            live = sim.readStats()["live"]
+        el = time.perf_counter() - t0
+        if (steps_cap and k >= steps_cap) or el > budget_s:
+            break
+    live = sim.readStats()["live"]
+    return {"value": live * k / el, "unit": "particle-steps/s", "cores": th, "kind": "port",
+            "sample": "%s (%d particles), %d steps, oracle with %d OpenMP threads" % (sample, live, k, th)}, el
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.scene import SceneRunner
+    sample = "wave_tank_96" if a.workload.startswith("wave_tank") else a.workload
+    w = workload(sample)
+    th = os.cpu_count() or 1
+    sim = w.make(OracleFlipSim, threads=th)
+    run = SceneRunner(sim)
+    t = 0.0
+    for _ in range(a.warmup):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    el = time.perf_counter() - t0
+    live = sim.readStats()["live"]
+    v = live * a.steps / el
+    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config_of(a.workload, workload_meta(a.workload), live),
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": th, "kind": "port",
+                             "sample": "%s (%d particles) per step, oracle with %d OpenMP threads: the reference's FLIP step runs only "
+                                       "as WGSL in a browser (no graphics stack here), so its CPU restatement stands in" % (sample, live, th)},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_meta(name):
+    class M:
+        pass
+    m = M()
+    if name.startswith("wave_tank"):
+        from splashtank_b200 import scenes
+        m.n = int(name.rsplit("_", 1)[1])
+        m.dt = 1.0 / 240.0
+        m.steps = 200
+        m.opts = dict(iters=30)
+        m.spray_cap = 4_000_000
+    else:
+        m.dt = 1.0 / 240.0
+        m.steps = 100
+    return m
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    w = workload(a.workload)
+    sim = w.make(FlipSim, device=local)
+    run = SceneRunner(sim)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    t = 0.0
+
+    def step():
+        nonlocal t
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    st0 = sim.readStats()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-timed region
+    sim.set_timing(True)
+    clocks = Clocks(local)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    stages, nrec = sim.read_timing()
+    sim.set_timing(False)
+    st1 = sim.readStats()
+    live = st1["live"]
+    launches = st1["launches"] - st0["launches"]
+    ms_max, live_sum = ms, live
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+        tl = torch.tensor([float(live)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tl)
+        live_sum = int(tl.item())
+    value = live_sum * a.steps / (ms_max * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers: every step the options and collider records go up from pinned
+    # host memory and the step's counters come back (readStats); every 4th step (a 60 Hz frame at dt 1/240) all particle
+    # positions come back into a pinned host buffer, as a bake does
+    n_all = st1["n"]
+    host = torch.empty((max(n_all, 1), 4), dtype=torch.float32, pin_memory=True).numpy()
+    nc = len(w.states(0.0))
+    h2d = 496 + nc * 128   # the 496-byte parameter block and 128 bytes per collider record, per step
+    d2h = 64 + (16 * n_all) / 4.0
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for k in range(a.e2e_steps):
+        step()
+        sim.readStats()
+        if k % 4 == 3:
+            sim.readbackInto(host)
+    f1.record(stream)
+    f1.synchronize()
+    barrier()
+    ems = f0.elapsed_time(f1)
+    if dist:
+        tt = torch.tensor([ems], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt.item())
+    e2e_value = live_sum * a.e2e_steps / (ems * 1e-3)
+
+    if rank == 0:
+        peak, src = measured_peak()
+        cells = st1["sc"] * 512
+        rl = roofline(stages, nrec, live, cells, st1["fluid"], w.opts.get("iters", 30), peak, src)
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jitter, 8 particles per cell)",
+                "config": config_of(a.workload, w, live), "gpu_launches": int(launches),
+                "stage_ms_per_step": {k: round(v / max(nrec, 1), 4) for k, v in stages.items()},
+                "clocks": clk, "roofline": rl,
+                "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                        "steps": a.e2e_steps, "readback": "counters every step, all particle positions every 4th step"}}
+        if world == 1 and not a.no_cpu_baseline:
+            del sim
+            cb, _ = cpu_sample(a.workload)
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -108,9 +108,11 @@ typedef struct st_stats {
   uint32_t fluid;       /* fluid cells */
   float vmax;           /* fastest particle speed seen by P2G */
   uint32_t n;           /* particle slots in use (N) */
-  uint32_t live;        /* particles not parked dead */
+  uint32_t live;        /* particles alive when the last step sorted them (N before the first step) */
   uint32_t spray_used;  /* whitewater slots handed out (sctl[0]) */
   uint32_t steps;       /* steps taken since create/clear */
+  uint32_t spray_overflow; /* steps whose whitewater emission tried more points than the ring holds */
+  uint64_t launches;    /* CUDA kernels launched by steps since create */
 } st_stats;
 
 /* Dense debug export of the grid (FlipSim.dbgColumn/dbgRow, src/flip/sim.js:457-482), per cell of the
@@ -158,6 +160,11 @@ st_status st_flip_add(st_flip* s, const float* pos3, const float* vel3, uint32_t
 st_status st_flip_step(st_flip* s, double dt, const st_step_opts* o);
 /* FlipSim.stepTimed (src/flip/sim.js:312-331): one step, returning device ms per stage. */
 st_status st_flip_step_timed(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t);
+/* Stage timing without stalls (the per-stage numbers of src/app/14-bench.js, measured in place): while on, every step
+ * records its stage boundaries as CUDA events; st_flip_read_timing waits for them and returns the summed stage times
+ * of the steps recorded since timing was turned on or last read (at most the last 256). */
+st_status st_flip_set_timing(st_flip* s, int on);
+st_status st_flip_read_timing(st_flip* s, st_stage_times* sum, uint32_t* nsteps);
 /* FlipSim.readbackInto (src/flip/sim.js:439-455): particles in id order, 4 floats each.
  * vel4 may be null. *n receives N; at most cap particles are written. */
 st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);

@@ -30,6 +30,7 @@
 #endif
 
 #include "../include/splashtank_cuda.h"
+#include "../include/st_math.h"
 
 namespace {
 
@@ -116,7 +117,7 @@ struct Oracle {
   double tm = 0;
   uint32_t seed = 0, steps = 0;
   // stats
-  uint32_t st_sc = 0, st_fluid = 0, st_ovf = 0, spray_ovf = 0;
+  uint32_t st_sc = 0, st_fluid = 0, st_ovf = 0, spray_ovf = 0, st_live = 0;
   float st_vmax = 0;
   Params P;
   int nthreads = 1;
@@ -467,6 +468,8 @@ struct Oracle {
       key[i] = ((uint64_t)cellIdx(ci, cj, ck) << 32) | pid[i];
     }
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    st_live = 0;
+    for (uint32_t i = 0; i < n; i++) if (key[i] != ~0ull) st_live++;
     std::vector<float> np((size_t)n * 4), nv((size_t)n * 4); std::vector<uint32_t> nid(n);
     for (uint32_t k = 0; k < n; k++) {
       uint32_t s = order[k];
@@ -746,7 +749,7 @@ struct Oracle {
       float turb = clampf((length(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
       float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
       float tau = fmax_(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstep(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
-      float foam = vel[i * 4 + 3] * expf(-P.dt / tau);
+      float foam = vel[i * 4 + 3] * st_expf(-P.dt / tau);
       foam = fmax_(foam, fmax_(spray * 0.9f, fmax_(impact, turb * 0.8f)));
       V3 gust = v3(0, 0, 0);
       if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
@@ -755,7 +758,7 @@ struct Oracle {
       }
       float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
       V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
-      v = v + (airv - v) * (1.0f - expf(-kd * P.dt));
+      v = v + (airv - v) * (1.0f - st_expf(-kd * P.dt));
       float sp = length(v);
       if (sp > P.vmax) v = v * (P.vmax / sp);
       V3 pt = p + v * P.dt;
@@ -835,14 +838,14 @@ struct Oracle {
         V3 base = v3(P.q1, P.q2, P.q3);
         V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
         v.y -= P.gravity * P.dt;
-        v = v + (airv - v) * (1.0f - expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
+        v = v + (airv - v) * (1.0f - st_expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
         life -= P.dt;
       } else if (kind == 2u) {
         float vy = vf.y + clampf((wet - 0.5f) * 4.0f, -1.0f, 1.0f) * P.h * 4.0f;
-        v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - expf(-10.0f * P.dt));
+        v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - st_expf(-10.0f * P.dt));
         life -= P.dt;
       } else {
-        v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - expf(-6.0f * P.dt));
+        v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - st_expf(-6.0f * P.dt));
         life -= 0.3f * P.dt;
       }
       V3 np = p + v * P.dt;
@@ -891,7 +894,8 @@ struct Oracle {
         uint32_t h0 = pid[i] * 747796405u + P.seed * 2891336453u;
         uint32_t hh = h0 ^ ((mm + 1u) * 0x9E3779B9u);
         float z = hash1(hh + 1u) * 2.0f - 1.0f; float a = hash1(hh + 2u) * 6.2831853f; float s = sqrtf(fmax_(0.0f, 1.0f - z * z));
-        V3 dir = v3(s * cosf(a), s * sinf(a), z);
+        float sa, ca; st_sincosf(a, &sa, &ca);
+        V3 dir = v3(s * ca, s * sa, z);
         bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
         bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
         V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
@@ -1033,8 +1037,8 @@ st_status oracle_flip_read_spray(void* h, float* pos4, float* vel4, uint32_t cap
 st_status oracle_flip_stats(void* h, st_stats* o) {
   Oracle* s = (Oracle*)h;
   o->sc = s->st_sc; o->ovf = s->st_ovf; o->fluid = s->st_fluid; o->vmax = s->st_vmax; o->n = s->N;
-  uint32_t live = 0; for (uint32_t i = 0; i < s->N; i++) if (s->pos[i * 4 + 1] >= DEADY) live++;
-  o->live = live; o->spray_used = s->sctl0; o->steps = s->steps;
+  // particles alive at the start of the last step's sort (all slots before the first step)
+  o->live = s->steps ? s->st_live : s->N; o->spray_used = s->sctl0; o->steps = s->steps; o->spray_overflow = s->spray_ovf; o->launches = 0;
   return ST_OK;
 }
 st_status oracle_flip_get_dims(void* h, st_flip_dims* o) {

@@ -43,7 +43,8 @@ class StepOpts(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("sc", C.c_uint32), ("ovf", C.c_uint32), ("fluid", C.c_uint32), ("vmax", C.c_float), ("n", C.c_uint32),
-                ("live", C.c_uint32), ("spray_used", C.c_uint32), ("steps", C.c_uint32)]
+                ("live", C.c_uint32), ("spray_used", C.c_uint32), ("steps", C.c_uint32), ("spray_overflow", C.c_uint32),
+                ("launches", C.c_uint64)]
 
 
 class Grid(C.Structure):
@@ -98,6 +99,8 @@ CUDA_ONLY_FUNCS = [
     ("step_opts_default", None, [C.POINTER(StepOpts)]),
     ("flip_step_timed", C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepOpts), C.POINTER(StageTimes)]),
     ("flip_stream", C.c_void_p, [C.c_void_p]),
+    ("flip_set_timing", C.c_int, [C.c_void_p, C.c_int]),
+    ("flip_read_timing", C.c_int, [C.c_void_p, C.POINTER(StageTimes), u32p]),
     ("abi_version", C.c_uint32, []),
     ("last_error", C.c_char_p, []),
 ]

@@ -58,10 +58,22 @@ struct st_flip {
   std::string sdfSig;
   size_t sdfCap = 0;
   FlipParams hp{};
+  // per-step uploads (parameter block + collider records) come from a ring of pinned host blocks, so the copies are
+  // asynchronous and a block is rewritten only after the copy that read it has run
+  static constexpr int RING = 16;
+  struct Upload { FlipParams P; float cols[32 * 32]; };
+  Upload* ring_h = nullptr;
+  cudaEvent_t ring_ev[RING] = {};
+  int ring_i = 0;
+  // stage timing without stalls: each step records its stage events into a ring; st_flip_read_timing sums them
+  static constexpr int TSLOTS = 256, TEV = 11;
+  bool timing = false;
+  cudaEvent_t tev[TSLOTS][TEV] = {};
+  uint32_t tcount = 0;
   // device memory
-  FlipParams* dP = nullptr;
   Ctl* dCtl = nullptr;
   Ctl* hCtl = nullptr;   // pinned
+  Upload* dUp = nullptr;
   Part* part[2] = {nullptr, nullptr};
   uint32_t* ids[2] = {nullptr, nullptr};
   uint32_t *key = nullptr, *rank = nullptr, *srcIdx = nullptr, *spid = nullptr, *blkDead = nullptr;
@@ -73,23 +85,23 @@ struct st_flip {
   float *pres = nullptr, *rhs = nullptr, *vn = nullptr, *vo = nullptr, *velG = nullptr;
   int32_t* acc = nullptr;
   uint16_t* sorInfo = nullptr;
-  float4* cols = nullptr;
   float* sdf = nullptr;
   float4 *sPos = nullptr, *sVel = nullptr;
   uint8_t* emitK = nullptr;
   uint32_t *blkEmit = nullptr, *deadList = nullptr;
   cudaEvent_t ev[16] = {};
   int cur = 0;   // part[cur] holds this step's storage order
+  uint64_t launches = 0;   // kernels launched by steps since create
 
   Bufs bufs() const {
     Bufs B{};
-    B.P = dP; B.ctl = dCtl;
+    B.P = &dUp->P; B.ctl = dCtl;
     B.pa = part[cur]; B.pb = part[cur ^ 1]; B.ida = ids[cur]; B.idb = ids[cur ^ 1];
     B.key = key; B.rank = rank; B.srcIdx = srcIdx; B.spid = spid; B.blkDead = blkDead;
     B.need = need; B.on = on; B.tstate = tstate; B.blkTiles = blkTiles; B.active = active; B.prevActive = nullptr;
     B.tileSlot = tileSlot; B.dropped = dropped; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
-    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cols = cols; B.sdf = sdf;
+    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
     B.sPos = sPos; B.sVel = sVel; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
@@ -116,12 +128,16 @@ void st_flip_destroy(st_flip* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  void* ptrs[] = {s->dP, s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
+  void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->tileCnt, s->tileAux, s->tileAux2, s->on, s->tstate,
-                  s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo, s->cols,
+                  s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
                   s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
+  if (s->ring_h) cudaFreeHost(s->ring_h);
+  if (s->dUp) cudaFree(s->dUp);
+  for (auto& e : s->ring_ev) if (e) cudaEventDestroy(e);
+  for (auto& row : s->tev) for (auto& e : row) if (e) cudaEventDestroy(e);
   for (auto& e : s->ev) if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -161,7 +177,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   st_status st = ST_OK;
   auto A = [&](cudaError_t ee, const char* what) { if (ee != cudaSuccess && st == ST_OK) { set_err(what, ee); st = ee == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR; } };
   A(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
-  A(dalloc(&s->dP, 1), "params"); A(dalloc(&s->dCtl, 1), "ctl"); A(cudaMallocHost((void**)&s->hCtl, sizeof(Ctl)), "ctl host");
+  A(dalloc(&s->dCtl, 1), "ctl"); A(cudaMallocHost((void**)&s->hCtl, sizeof(Ctl)), "ctl host");
   for (int b = 0; b < 2; b++) { A(dalloc(&s->part[b], M), "particles"); A(dalloc(&s->ids[b], M), "ids"); A(dalloc(&s->cnt[b], C), "cnt"); }
   A(dalloc(&s->key, M), "key"); A(dalloc(&s->rank, M), "rank"); A(dalloc(&s->srcIdx, M), "srcIdx"); A(dalloc(&s->spid, M), "spid");
   A(dalloc(&s->blkDead, NB + 1), "blkDead"); A(dalloc(&s->blkEmit, NB + 1), "blkEmit"); A(dalloc(&s->emitK, M), "emitK");
@@ -171,13 +187,16 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(dalloc(&s->tileCnt, T + 1), "tileCnt"); A(dalloc(&s->tileAux, T + 1), "tileAux"); A(dalloc(&s->tileAux2, T + 1), "tileAux2");
   A(dalloc(&s->cellOff, C), "cellOff"); A(dalloc(&s->ctype, C), "ctype"); A(dalloc(&s->pres, C), "pres"); A(dalloc(&s->rhs, C), "rhs");
   A(dalloc(&s->acc, 6 * C), "acc"); A(dalloc(&s->vn, 3 * C), "vn"); A(dalloc(&s->vo, 3 * C), "vo"); A(dalloc(&s->velG, 3 * C), "velG");
-  A(dalloc(&s->sorInfo, C), "sorInfo"); A(dalloc(&s->cols, 32 * 8), "cols"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
+  A(dalloc(&s->sorInfo, C), "sorInfo"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
   A(dalloc(&s->sPos, std::max<size_t>(s->sprayCap, 1)), "sPos"); A(dalloc(&s->sVel, std::max<size_t>(s->sprayCap, 1)), "sVel");
   for (auto& ev : s->ev) A(cudaEventCreate(&ev), "event");
+  A(cudaMallocHost((void**)&s->ring_h, sizeof(st_flip::Upload) * st_flip::RING), "upload ring"); A(dalloc(&s->dUp, 1), "upload");
+  for (auto& ev : s->ring_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "ring event");
   if (st != ST_OK) { st_flip_destroy(s); return st; }
   // every tile starts in the state the reference's spare slot reads as
   cudaStream_t q = s->stream;
   A(cudaMemsetAsync(s->dCtl, 0, sizeof(Ctl), q), "memset");
+  A(cudaMemsetAsync(s->dUp, 0, sizeof(st_flip::Upload), q), "memset");
   for (int b = 0; b < 2; b++) { A(cudaMemsetAsync(s->part[b], 0, M * sizeof(Part), q), "memset"); A(cudaMemsetAsync(s->cnt[b], 0, C * 4, q), "memset"); }
   A(cudaMemsetAsync(s->need, 0, T * 4, q), "memset"); A(cudaMemsetAsync(s->on, 0, T, q), "memset");
   A(cudaMemsetAsync(s->ctype, 0, C * 4, q), "memset"); A(cudaMemsetAsync(s->pres, 0, C * 4, q), "memset");
@@ -258,7 +277,7 @@ st_status st_flip_add(st_flip* s, const float* p3, const float* v3_, uint32_t n,
 }
 
 // packColliders (src/gpu.js:42-70): 32 floats per collider, SDF grids uploaded when the set of ids changes
-static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc) {
+static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc, float* cf) {
   nc = std::min(o->ncols, 32u);
   if (nc && !o->cols) return ST_BAD_ARG;
   std::string sig;
@@ -286,7 +305,6 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc)
     s->sdfSig = sig;
   }
   if (nc) {
-    float cf[32 * 32];
     for (uint32_t k = 0; k < nc; k++) {
       const st_collider& c = o->cols[k];
       const st_sdf* sd = c.sdf;
@@ -300,7 +318,6 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc)
       f[24] = c.vel[0]; f[25] = c.vel[1]; f[26] = c.vel[2]; f[27] = 0;
       f[28] = c.ang[0]; f[29] = c.ang[1]; f[30] = c.ang[2]; f[31] = 0;
     }
-    CK(cudaMemcpyAsync(s->cols, cf, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, s->stream));
   }
   return ST_OK;
 }
@@ -337,6 +354,7 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
   for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &s->fills[k * 8], 8 * sizeof(float));
 }
 
+static void stage_fill(st_stage_times* t, const float* ms, float total);
 // one step; t (optional) receives device ms per stage
 static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
   if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
@@ -345,8 +363,13 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   const bool nbOn = o->nb_on != 0;
   if (nbOn) s->velGOn = true;
   const uint32_t init = nbOn && s->nbInit ? s->nbInit : 0;
+  // the next pinned upload block: wait for the copy that last read it
+  st_flip::Upload* up = &s->ring_h[s->ring_i];
+  cudaEvent_t upEv = s->ring_ev[s->ring_i];
+  s->ring_i = (s->ring_i + 1) % st_flip::RING;
+  CK(cudaEventSynchronize(upEv));
   uint32_t nc = 0;
-  st_status st = pack_colliders(s, o, nc);
+  st_status st = pack_colliders(s, o, nc, up->cols);
   if (st != ST_OK) return st;
   const bool sprOn = o->spray_on != 0 && s->sprayCap > 0;
   s->seed = s->seed + 1u;
@@ -359,58 +382,104 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   // this step's storage order goes into the other particle buffer; cell counts alternate buffers
   s->cur ^= 1;
   s->parity ^= 1;
-  CK(cudaMemcpyAsync(s->dP, &s->hp, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
+  up->P = s->hp;
+  CK(cudaMemcpyAsync(&s->dUp->P, &up->P, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
+  if (nc) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
+  CK(cudaEventRecord(upEv, q));
   // per-step counters: fluid, fastest speed, dropped tiles, emission
   CK(cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q));   // fluid, vmaxBits (nActive is kept)
   CK(cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q));
   CK(cudaMemsetAsync(&s->dCtl->emitTried, 0, sizeof(uint32_t), q));
   const Bufs B = s->bufs();
   const int gT = s->tileGrid(8), gT4 = s->tileGrid(4);
-  auto mark = [&](int k) { if (t) cudaEventRecord(s->ev[k], q); };
+  cudaEvent_t* tslot = nullptr;
+  if (s->timing) {
+    if (s->tcount >= (uint32_t)st_flip::TSLOTS) { CK(cudaEventSynchronize(s->tev[(s->tcount) % st_flip::TSLOTS][10])); }
+    tslot = s->tev[s->tcount % st_flip::TSLOTS];
+  }
+  auto mark = [&](int k) {
+    if (t) cudaEventRecord(s->ev[k], q);
+    if (tslot) cudaEventRecord(tslot[k], q);
+  };
   mark(0);
   // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
-  launch_count_mark(B, q);
-  if (nbOn && init != 1) launch_mark_phi(B, gT4, q);
-  if (init) launch_mark_fill(B, std::max(1, (int)std::min<uint32_t>((s->ntiles + 255) / 256, 4096)), q);
-  launch_tiles(B, s->ntiles, gT4, q);
-  if (init) launch_nb_init(B, gT4, q);
-  launch_scan_counts(B, q);
-  launch_scatter(B, q);
+  int nl = 0;
+  nl += launch_count_mark(B, q);
+  if (nbOn && init != 1) nl += launch_mark_phi(B, gT4, q);
+  if (init) nl += launch_mark_fill(B, std::max(1, (int)std::min<uint32_t>((s->ntiles + 255) / 256, 4096)), q);
+  nl += launch_tiles(B, s->ntiles, gT4, q);
+  if (init) nl += launch_nb_init(B, gT4, q);
+  nl += launch_scan_counts(B, q);
+  nl += launch_scatter(B, q);
   mark(1);
-  launch_p2g(B, gT, q);
+  nl += launch_p2g(B, gT, q);
   mark(2);
-  if (nbOn) launch_nb_phi(B, gT4, q);
+  if (nbOn) nl += launch_nb_phi(B, gT4, q);
   mark(3);
-  launch_classify(B, gT4, q);
-  if (nbOn) launch_nb_vel(B, gT4, q);
+  nl += launch_classify(B, gT4, q);
+  if (nbOn) nl += launch_nb_vel(B, gT4, q);
   mark(4);
-  launch_norm_div(B, gT4, q);
+  nl += launch_norm_div(B, gT4, q);
   mark(5);
-  launch_sor(B, gT, iters, q);
+  nl += launch_sor(B, gT, iters, q);
   mark(6);
-  launch_project(B, gT4, q);
+  nl += launch_project(B, gT4, q);
   mark(7);
-  launch_g2p(B, s->N, q);
+  nl += launch_g2p(B, s->N, q);
   mark(8);
-  if (s->sprayCap > 0) launch_spray(B, s->sprayCap, sprOn, gT4, q);
+  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, gT4, q);
   mark(9);
-  if (nbOn) launch_nb_reseed(B, gT4, q);
+  if (nbOn) nl += launch_nb_reseed(B, gT4, q);
   mark(10);
+  s->launches += (uint64_t)nl;
   CK(cudaGetLastError());
   s->steps++;
+  if (tslot) s->tcount++;
   if (t) {
     CK(cudaEventSynchronize(s->ev[10]));
     float ms[10];
     for (int k = 0; k < 10; k++) cudaEventElapsedTime(&ms[k], s->ev[k], s->ev[k + 1]);
-    memset(t, 0, sizeof(*t));
-    t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
-    t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8]; t->reseed = ms[9];
-    cudaEventElapsedTime(&t->total, s->ev[0], s->ev[10]);
+    float tot = 0.0f;
+    cudaEventElapsedTime(&tot, s->ev[0], s->ev[10]);
+    stage_fill(t, ms, tot);
   }
   return ST_OK;
 }
 
 st_status st_flip_step(st_flip* s, double dt, const st_step_opts* o) { return do_step(s, dt, o, nullptr); }
+
+static void stage_fill(st_stage_times* t, const float* ms, float total) {
+  t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
+  t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8];
+  t->reseed = ms[9]; t->total = total;
+}
+st_status st_flip_set_timing(st_flip* s, int on) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (on && !s->tev[0][0])
+    for (auto& row : s->tev) for (auto& e : row) CK(cudaEventCreate(&e));
+  s->timing = on != 0;
+  s->tcount = 0;
+  return ST_OK;
+}
+// sum of the stage times of the steps recorded since st_flip_set_timing (at most the last 256)
+st_status st_flip_read_timing(st_flip* s, st_stage_times* sum, uint32_t* nsteps) {
+  if (!s || !sum) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  memset(sum, 0, sizeof(*sum));
+  uint32_t n = std::min<uint32_t>(s->tcount, st_flip::TSLOTS);
+  if (n) CK(cudaStreamSynchronize(s->stream));
+  float acc[10] = {0}, tot = 0.0f;
+  for (uint32_t k = 0; k < n; k++) {
+    cudaEvent_t* e = s->tev[(s->tcount - 1 - k) % st_flip::TSLOTS];
+    for (int j = 0; j < 10; j++) { float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[j], e[j + 1])); acc[j] += ms; }
+    float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[0], e[10])); tot += ms;
+  }
+  stage_fill(sum, acc, tot);
+  if (nsteps) *nsteps = n;
+  s->tcount = 0;
+  return ST_OK;
+}
 st_status st_flip_step_timed(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
   if (!t) return ST_BAD_ARG;
   return do_step(s, dt, o, t);
@@ -424,6 +493,7 @@ st_status st_flip_stats(st_flip* s, st_stats* out) {
   out->sc = s->hCtl->nActive; out->ovf = 0; out->fluid = s->hCtl->fluid;
   uint32_t vb = s->hCtl->vmaxBits; float vm; memcpy(&vm, &vb, 4); out->vmax = vm;
   out->n = s->N; out->live = s->steps ? s->hCtl->nLive : s->N; out->spray_used = s->hCtl->sctl0; out->steps = s->steps;
+  out->launches = s->launches; out->spray_overflow = s->hCtl->sprayOvf;
   return ST_OK;
 }
 

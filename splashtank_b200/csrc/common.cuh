@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/st_math.h"
+
 namespace st {
 
 constexpr float DEADY = -1.0e5f;

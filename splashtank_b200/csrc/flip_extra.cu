@@ -360,14 +360,14 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
       const V3 base = v3(P.q1, P.q2, P.q3);
       const V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
       v.y -= P.gravity * P.dt;
-      v = v + (airv - v) * (1.0f - expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
+      v = v + (airv - v) * (1.0f - st_expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
       life -= P.dt;
     } else if (kind == 2u) {
       const float vy = vf.y + clampf((wet - 0.5f) * 4.0f, -1.0f, 1.0f) * P.h * 4.0f;
-      v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - expf(-10.0f * P.dt));
+      v = vmix(v, v3(vf.x, vy, vf.z), 1.0f - st_expf(-10.0f * P.dt));
       life -= P.dt;
     } else {
-      v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - expf(-6.0f * P.dt));
+      v = vmix(v, vf + v3(0.0f, P.wwRise, 0.0f), 1.0f - st_expf(-6.0f * P.dt));
       life -= 0.3f * P.dt;
     }
     const V3 np = p + v * P.dt;
@@ -440,7 +440,9 @@ __global__ void __launch_bounds__(PBLK) k_emit_write(Bufs B) {
     const float z = hash1(hh + 1u) * 2.0f - 1.0f;
     const float an = hash1(hh + 2u) * 6.2831853f;
     const float s = sqrtf(fmx(0.0f, 1.0f - z * z));
-    const V3 dir = v3(s * cosf(an), s * sinf(an), z);
+    float sa, ca;
+    st_sincosf(an, &sa, &ca);
+    const V3 dir = v3(s * ca, s * sa, z);
     const bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
     const bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
     V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
@@ -459,32 +461,35 @@ __global__ void k_emit_done(Bufs B) {
   B.ctl->sctl0 = B.ctl->sctl0 + tried;
 }
 
-// ---- launchers ----
-void launch_nb_init(const Bufs& B, int grid, cudaStream_t s) { k_nb_init<<<grid, 512, 0, s>>>(B); }
-void launch_nb_phi(const Bufs& B, int grid, cudaStream_t s) {
+// ---- launchers: each returns how many kernels it launched ----
+int launch_nb_init(const Bufs& B, int grid, cudaStream_t s) { k_nb_init<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s) {
   k_nb_phi<<<grid, 512, 0, s>>>(B);
   k_nb_jac<<<grid, 512, 0, s>>>(B, 1);
   k_nb_jac<<<grid, 512, 0, s>>>(B, 0);
   k_nb_jac<<<grid, 512, 0, s>>>(B, 1);
+  return 4;
 }
-void launch_nb_vel(const Bufs& B, int grid, cudaStream_t s) { k_nb_vel<<<grid, 512, 0, s>>>(B); }
-void launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
-  if (!B.nblk) return;
+int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s) { k_nb_vel<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
+  if (!B.nblk) return 0;
   k_nb_kill<<<B.nblk, PBLK, 0, s>>>(B);
   k_scan_x<<<1, 1024, 0, s>>>(B, 0);
   k_dead_list<<<B.nblk, PBLK, 0, s>>>(B);
   k_def_count<<<grid, 512, 0, s>>>(B);
   k_scan_x<<<2, 1024, 0, s>>>(B, 1);
   k_spawn<<<grid, 512, 0, s>>>(B);
+  return 6;
 }
-void launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s) {
-  if (!smax) return;
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s) {
+  if (!smax) return 0;
   k_ww_step<<<grid, 256, 0, s>>>(B);
-  if (!emit || !B.nblk) return;
+  if (!emit || !B.nblk) return 1;
   k_emit_count<<<B.nblk, PBLK, 0, s>>>(B);
   k_scan_x<<<1, 1024, 0, s>>>(B, 2);
   k_emit_write<<<B.nblk, PBLK, 0, s>>>(B);
   k_emit_done<<<1, 1, 0, s>>>(B);
+  return 5;
 }
 
 }  // namespace st

@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(256) k_g2p(Bufs B) {
     const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
     const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
     const float tau = fmx(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
-    float foam = q.v.w * expf(-P.dt / tau);
+    float foam = q.v.w * st_expf(-P.dt / tau);
     foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
     V3 gust = v3(0.0f, 0.0f, 0.0f);
     if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(256) k_g2p(Bufs B) {
     }
     const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
     const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
-    v = v + (airv - v) * (1.0f - expf(-kd * P.dt));
+    v = v + (airv - v) * (1.0f - st_expf(-kd * P.dt));
     const float sp = len3(v);
     if (sp > P.vmax) v = v * (P.vmax / sp);
     const V3 pt = p + v * P.dt;
@@ -615,30 +615,46 @@ __global__ void k_iota(uint32_t* p, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
 }
 
-// ---- launchers ----
-void launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<B.nblk, PBLK, 0, s>>>(B); }
-void launch_mark_phi(const Bufs& B, int grid, cudaStream_t s) { k_mark_phi<<<grid, 512, 0, s>>>(B); }
-void launch_mark_fill(const Bufs& B, int grid, cudaStream_t s) { k_mark_fill<<<grid, 256, 0, s>>>(B); }
-void launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
+// ---- launchers: each returns how many kernels it launched ----
+int launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<B.nblk, PBLK, 0, s>>>(B); return 1; }
+int launch_mark_phi(const Bufs& B, int grid, cudaStream_t s) { k_mark_phi<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_mark_fill(const Bufs& B, int grid, cudaStream_t s) { k_mark_fill<<<grid, 256, 0, s>>>(B); return 1; }
+int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
   uint32_t nb = (ntiles + 1023) / 1024;
   k_tile_flags<<<nb, 1024, 0, s>>>(B);
   k_tile_list<<<nb, 1024, 0, s>>>(B);
   k_tile_prep<<<grid, 512, 0, s>>>(B);
+  return 3;
 }
-void launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); }
-void launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, PBLK, 0, s>>>(B); }
-void launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); }
-void launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); }
-void launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); }
-void launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s) {
+int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
+int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, PBLK, 0, s>>>(B); return 1; }
+int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
+int launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s) {
   for (int it = 0; it < iters; it++) { k_sor<<<grid, 256, 0, s>>>(B, 0u); k_sor<<<grid, 256, 0, s>>>(B, 1u); }
+  return 2 * iters;
 }
-void launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); }
-void launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s) { if (n) k_g2p<<<(n + 255) / 256, 256, 0, s>>>(B); }
-void launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {
-  if (n) k_unsort<<<(n + 255) / 256, 256, 0, s>>>(src, ids, n, pos, vel);
+int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s) {
+  if (!n) return 0;
+  k_g2p<<<(n + 255) / 256, 256, 0, s>>>(B);
+  return 1;
 }
-void launch_fill_f32(float* p, float v, size_t n, cudaStream_t s) { if (n) k_fill_f32<<<1024, 256, 0, s>>>(p, v, n); }
-void launch_iota(uint32_t* p, uint32_t n, cudaStream_t s) { if (n) k_iota<<<1024, 256, 0, s>>>(p, n); }
+int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {
+  if (!n) return 0;
+  k_unsort<<<(n + 255) / 256, 256, 0, s>>>(src, ids, n, pos, vel);
+  return 1;
+}
+int launch_fill_f32(float* p, float v, size_t n, cudaStream_t s) {
+  if (!n) return 0;
+  k_fill_f32<<<1024, 256, 0, s>>>(p, v, n);
+  return 1;
+}
+int launch_iota(uint32_t* p, uint32_t n, cudaStream_t s) {
+  if (!n) return 0;
+  k_iota<<<1024, 256, 0, s>>>(p, n);
+  return 1;
+}
 
 }  // namespace st

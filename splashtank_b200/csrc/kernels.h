@@ -3,26 +3,26 @@
 #include "common.cuh"
 
 namespace st {
-void launch_count_mark(const Bufs& B, cudaStream_t s);
-void launch_mark_phi(const Bufs& B, int grid, cudaStream_t s);
-void launch_mark_fill(const Bufs& B, int grid, cudaStream_t s);
-void launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s);
-void launch_scan_counts(const Bufs& B, cudaStream_t s);
-void launch_scatter(const Bufs& B, cudaStream_t s);
-void launch_p2g(const Bufs& B, int grid, cudaStream_t s);
-void launch_classify(const Bufs& B, int grid, cudaStream_t s);
-void launch_norm_div(const Bufs& B, int grid, cudaStream_t s);
-void launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s);
-void launch_project(const Bufs& B, int grid, cudaStream_t s);
-void launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s);
-void launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);
-void launch_fill_f32(float* p, float v, size_t n, cudaStream_t s);
-void launch_iota(uint32_t* p, uint32_t n, cudaStream_t s);
+int launch_count_mark(const Bufs& B, cudaStream_t s);
+int launch_mark_phi(const Bufs& B, int grid, cudaStream_t s);
+int launch_mark_fill(const Bufs& B, int grid, cudaStream_t s);
+int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s);
+int launch_scan_counts(const Bufs& B, cudaStream_t s);
+int launch_scatter(const Bufs& B, cudaStream_t s);
+int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
+int launch_classify(const Bufs& B, int grid, cudaStream_t s);
+int launch_norm_div(const Bufs& B, int grid, cudaStream_t s);
+int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s);
+int launch_project(const Bufs& B, int grid, cudaStream_t s);
+int launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s);
+int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);
+int launch_fill_f32(float* p, float v, size_t n, cudaStream_t s);
+int launch_iota(uint32_t* p, uint32_t n, cudaStream_t s);
 // narrow band (flip_extra.cu)
-void launch_nb_init(const Bufs& B, int grid, cudaStream_t s);
-void launch_nb_phi(const Bufs& B, int grid, cudaStream_t s);
-void launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
-void launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
+int launch_nb_init(const Bufs& B, int grid, cudaStream_t s);
+int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s);
+int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
+int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 // whitewater (flip_extra.cu)
-void launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s);
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s);
 }  // namespace st

@@ -247,10 +247,22 @@ class FlipSim:
         del keep
         return {n: getattr(t, n) for n in abi.STAGES}
 
+    def set_timing(self, on=True):
+        """Record per-stage device times of every step without stalling (st_flip_set_timing)."""
+        self._check(self.f["flip_set_timing"](self._h, 1 if on else 0), "set_timing")
+
+    def read_timing(self):
+        """Summed stage ms of the steps recorded since set_timing/read_timing, and how many steps that is."""
+        t = abi.StageTimes()
+        n = C.c_uint32()
+        self._check(self.f["flip_read_timing"](self._h, C.byref(t), C.byref(n)), "read_timing")
+        return {k: getattr(t, k) for k in abi.STAGES}, n.value
+
     def readStats(self):
         s = abi.Stats()
         self._check(self.f["flip_stats"](self._h, C.byref(s)), "stats")
-        self.stats = dict(sc=s.sc, ovf=s.ovf, fluid=s.fluid, vmax=s.vmax, n=s.n, live=s.live, spray_used=s.spray_used, steps=s.steps)
+        self.stats = dict(sc=s.sc, ovf=s.ovf, fluid=s.fluid, vmax=s.vmax, n=s.n, live=s.live, spray_used=s.spray_used, steps=s.steps,
+                          spray_overflow=s.spray_overflow, launches=s.launches)
         return self.stats
 
     def activeCells(self):

@@ -7,21 +7,26 @@ ratio 2), each uniformly jittered inside its sub-cell from a seeded numpy genera
 Coordinates: a workload stated on [0, W] x [0, H] x [0, D] maps to the reference box [-W/2, W/2] x [0, H] x [-D/2, D/2]
 (src/flip/sim.js:53) by x_ref = x - W/2, z_ref = z - D/2.
 """
+import math
+
 import numpy as np
 
 
-def seed_cells(cells_ijk, h, rng, x0, y0, z0):
-    """8 jittered particles per cell: one per 2 x 2 x 2 sub-cell. cells_ijk is (n, 3) int; returns (8n, 3) float32."""
+def seed_cells(cells_ijk, h, rng, x0, y0, z0, chunk=1 << 20):
+    """8 jittered particles per cell: one per 2 x 2 x 2 sub-cell. cells_ijk is (n, 3) int; returns (8n, 3) float32.
+    Cells are processed in chunks so a 256^3 tank (about 40M particles) needs little temporary memory."""
     d = h / 2.0
     sub = np.array([[sx, sy, sz] for sz in (0, 1) for sy in (0, 1) for sx in (0, 1)], np.float64)   # x fastest
-    base = cells_ijk.astype(np.float64)[:, None, :] * h + sub[None, :, :] * d
-    u = rng.random(base.shape)
-    p = base + u * d
-    p = p.reshape(-1, 3)
-    p[:, 0] += x0
-    p[:, 1] += y0
-    p[:, 2] += z0
-    return p.astype(np.float32)
+    out = np.empty((len(cells_ijk) * 8, 3), np.float32)
+    for a in range(0, len(cells_ijk), chunk):
+        c = cells_ijk[a:a + chunk]
+        base = c.astype(np.float64)[:, None, :] * h + sub[None, :, :] * d
+        p = (base + rng.random(base.shape) * d).reshape(-1, 3)
+        p[:, 0] += x0
+        p[:, 1] += y0
+        p[:, 2] += z0
+        out[a * 8:(a + len(c)) * 8] = p
+    return out
 
 
 def box_cells(n_xyz, pred):
@@ -42,3 +47,66 @@ def dam_break(n=64, seed=1234, fx=0.4, fy=0.6):
     pos = seed_cells(cells, h, rng, -0.5, 0.0, -0.5)
     return dict(d=h / 2.0, ratio=2.0, size=(1.0, 1.0, 1.0), open=0, pos=pos, vel=np.zeros_like(pos), dt=1.0 / 240.0,
                 opts=dict(g=9.81, flip=0.97, iters=50, omega=1.7, comp=6.0, vmax=14.0), steps=100, name="dam_break_%d" % n)
+
+
+# the app's whitewater and solver settings (simPar, src/app/01-draw.js:55-63, defaults src/app/00-state.js:8-15)
+APP_SPRAY = dict(rate=24.0, min=2.5, life=1.2, mist=0.3, drag=1.0, mdrag=5.0, ww=dict(foamLife=3.0, rise=0.4, crest=1.0, impact=0.25))
+
+
+class WaveTank:
+    """Full-feature wave tank on an n^3 grid over the unit box (256^3 is the benchmark workload).
+
+    Water fills the lower 30% (cell centres below y = 0.3) in front of a piston; 8 particles per cell, seeded jitter.
+    Piston: a box collider whose front face moves as xf(t) = -0.44 + 0.05 sin(2 pi 0.5 t) (0.5 Hz, amplitude 0.05);
+    the block reaches past the -x wall, so no water is trapped behind it. Sphere: r = 0.1 on a linear keyframed path from
+    y = 0.55 down through the surface to y = 0.12 over the 200 steps. Narrow band on at full depth (band 1e4: particles
+    all the way down, depth field and kept grid velocity maintained, refill of thin calm cells); whitewater with the app's
+    settings except an emission speed threshold of 0.25 m/s so the slow piston waves throw off points; air drag 0.3 with
+    gusts, sheet tearing below 2 particles, 30 SOR iterations, dt = 1/240.
+    """
+
+    def __init__(self, n=256, seed=7, spray_cap=4_000_000, band=1e4, steps=200):
+        self.n = n
+        self.h = 1.0 / n
+        self.d = self.h / 2.0
+        self.dt = 1.0 / 240.0
+        self.steps = steps
+        self.spray_cap = spray_cap
+        self.band = band
+        self.xf0 = -0.44
+        rng = np.random.default_rng(seed)
+        h = self.h
+        cells = box_cells((n, n, n), lambda ci, cj, ck: (cj * h < 0.3) & (ci * h - 0.5 > self.xf0 + 0.5 * h))
+        self.pos = seed_cells(cells, h, rng, -0.5, 0.0, -0.5)
+        self.vel = np.zeros_like(self.pos)
+        from .scene import box_sdf, sphere_sdf
+        self.piston_sdf = box_sdf(0.1, 0.35, 0.53, 0.01, sid=1)
+        self.sphere_sdf = sphere_sdf(0.1, 0.01, sid=2)
+        T = steps * self.dt
+        self.sphere_keys = [dict(t=0.0, x=0.15, y=0.55, z=0.0), dict(t=T, x=0.15, y=0.12, z=0.0)]
+        self.opts = dict(g=9.81, flip=0.95, comp=6.0, iters=30, vmax=50.0, drag=0.3, gust=1.0, foamSens=1.0, foamTau=1.2,
+                         tear=2.0, vs=1.0, colMax=100.0, spr=dict(APP_SPRAY, min=0.25), nb=dict(on=True, band=band))
+        self.fill_box = (self.xf0, -1e4, -1e4, 1e4, 0.3, 1e4)   # x0, y0, z0, x1, y1, z1 (faces on walls pushed out)
+
+    def states(self, t):
+        from .scene import key_pose
+        xf = self.xf0 + 0.05 * math.sin(2 * math.pi * 0.5 * t)
+        s = key_pose(self.sphere_keys, t, smooth=False)
+        return [dict(id=1, sdf=self.piston_sdf, x=xf - 0.1, y=0.3, z=0.0),
+                dict(id=2, sdf=self.sphere_sdf, x=s["x"], y=s["y"], z=s["z"])]
+
+    def spare(self):
+        """Parked slots the narrow band refills from (nbSeed keeps ceil(0.35 * seeded) + 4000, src/shared.js:846-848, sized
+        for a thin band). At full depth almost no cell runs short, so this tank keeps 2% + 4000."""
+        return int(math.ceil(0.02 * len(self.pos))) + 4000
+
+    def make(self, cls, **kw):
+        """A simulator (FlipSim or a class with the same constructor) loaded with this tank."""
+        spare = self.spare()
+        sim = cls(self.d, len(self.pos) + spare, size=(1.0, 1.0, 1.0), ratio=2.0, spray_cap=self.spray_cap, **kw)
+        sim.add_many(self.pos, self.vel)
+        park = np.zeros((spare, 3), np.float32)
+        park[:, 1] = -1.0e6
+        sim.add_many(park)
+        sim.nb_fills(boxes=[self.fill_box], mode=1)
+        return sim
