@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--workload", default="wave_tank_256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     return ap.parse_args()
 
 
@@ -327,6 +328,8 @@ def main():
     nc = len(w.states(0.0))
     h2d = 496 + nc * 128   # the 496-byte parameter block and 128 bytes per collider record, per step
     d2h = 64 + (16 * n_all) / 4.0
+    if a.no_e2e:
+        a.e2e_steps = 0
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
@@ -343,7 +346,7 @@ def main():
         tt = torch.tensor([ems], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ems = float(tt.item())
-    e2e_value = live_sum * a.e2e_steps / (ems * 1e-3)
+    e2e_value = live_sum * a.e2e_steps / (ems * 1e-3) if a.e2e_steps else None
 
     if rank == 0:
         peak, src = measured_peak()

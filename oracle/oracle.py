@@ -46,3 +46,41 @@ class OracleFlipSim(FlipSim):
 
     def stepTimed(self, dt, o):
         raise NotImplementedError("the oracle has no stage timer")
+
+
+_PBF = None
+
+
+def pbf_funcs():
+    global _PBF
+    if _PBF is None:
+        path = os.path.join(HERE, "liboracle_pbf.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        f = abi.bind(lib, "oracle_", abi.PBF_FUNCS[:5])
+        f["set_threads"] = lib.oracle_pbf_set_threads
+        f["set_threads"].argtypes = [C.c_void_p, C.c_int]
+        f["set_threads"].restype = None
+        f["fill_box"] = lib.oracle_pbf_fill_box
+        f["fill_box"].argtypes = [C.c_void_p] + [C.c_float] * 6
+        f["fill_box"].restype = C.c_uint32
+        _PBF = f
+    return _PBF
+
+
+from splashtank_b200.pbf import PbfSim  # noqa: E402
+
+
+class OraclePbfSim(PbfSim):
+    """The CPU restatement of native/splash.cpp's Sim behind PbfSim's methods."""
+
+    def __init__(self, *a, threads=1, **k):
+        super().__init__(*a, _funcs=pbf_funcs(), **k)
+        self.f["set_threads"](self._h, int(threads))
+
+    def fill_box_baker(self, x0, x1, y0, y1, z0, z1):
+        """The baker's own fillBox (native/splash.cpp:85-89): lattice plus jitter from mt19937 seeded 12345."""
+        n = self.f["fill_box"](self._h, x0, x1, y0, y1, z0, z1)
+        self.n += n
+        return n

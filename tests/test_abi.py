@@ -63,9 +63,11 @@ int main(void) {
 
 
 def test_product_path_has_no_cpu_fallback():
-    """The product package never imports the oracle; without the library it raises instead of computing on the CPU."""
+    """The product package never imports or loads the oracle; without the CUDA library it raises instead of computing."""
     import splashtank_b200
     pkg = os.path.dirname(splashtank_b200.__file__)
     for fn in os.listdir(pkg):
         if fn.endswith(".py"):
-            assert "oracle" not in re.sub(r"#.*", "", open(os.path.join(pkg, fn)).read()).replace("oracle-free", ""), fn
+            src = open(os.path.join(pkg, fn)).read()
+            assert not re.search(r"^\s*(from|import)\s+oracle", src, flags=re.M), fn
+            assert "liboracle" not in src, fn
