@@ -77,14 +77,16 @@ struct st_flip {
   Part* part[2] = {nullptr, nullptr};
   uint32_t* ids[2] = {nullptr, nullptr};
   uint32_t *key = nullptr, *rank = nullptr, *srcIdx = nullptr, *spid = nullptr, *blkDead = nullptr;
-  uint32_t *need = nullptr, *blkTiles = nullptr, *active = nullptr, *tileSlot = nullptr, *dropped = nullptr;
-  uint32_t *tileCnt = nullptr, *tileAux = nullptr, *tileAux2 = nullptr;
+  uint32_t *need = nullptr, *blkTiles = nullptr, *active = nullptr, *tileSlot = nullptr, *dropped = nullptr, *fluidTiles = nullptr;
+  uint32_t *tileCnt = nullptr, *tileAux = nullptr, *tileAux2 = nullptr, *tileEmit = nullptr, *tileDead = nullptr;
+  uint8_t* deadF = nullptr;
   uint8_t *on = nullptr, *tstate = nullptr;
   int32_t* cnt[2] = {nullptr, nullptr};
   uint32_t *cellOff = nullptr, *ctype = nullptr;
   float *pres = nullptr, *rhs = nullptr, *vn = nullptr, *vo = nullptr, *velG = nullptr;
   int32_t* acc = nullptr;
   uint16_t* sorInfo = nullptr;
+  float* wet = nullptr;
   float* sdf = nullptr;
   float4 *sPos = nullptr, *sVel = nullptr;
   uint8_t* emitK = nullptr;
@@ -92,6 +94,9 @@ struct st_flip {
   cudaEvent_t ev[16] = {};
   int cur = 0;   // part[cur] holds this step's storage order
   uint64_t launches = 0;   // kernels launched by steps since create
+  struct Graph { uint64_t key = 0; cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t evnode[11] = {}; int launches = 0; };
+  std::vector<Graph> graphs;
+  bool use_graphs = true;
 
   Bufs bufs() const {
     Bufs B{};
@@ -99,7 +104,7 @@ struct st_flip {
     B.pa = part[cur]; B.pb = part[cur ^ 1]; B.ida = ids[cur]; B.idb = ids[cur ^ 1];
     B.key = key; B.rank = rank; B.srcIdx = srcIdx; B.spid = spid; B.blkDead = blkDead;
     B.need = need; B.on = on; B.tstate = tstate; B.blkTiles = blkTiles; B.active = active; B.prevActive = nullptr;
-    B.tileSlot = tileSlot; B.dropped = dropped; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2;
+    B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
     B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
     B.sPos = sPos; B.sVel = sVel; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
@@ -108,6 +113,8 @@ struct st_flip {
   }
   int tileGrid(int per_sm) const { return std::max(1, std::min<int>(sms * per_sm, (int)ntiles)); }
 };
+
+static void drop_graphs(st_flip* s);
 
 extern "C" {
 
@@ -128,8 +135,9 @@ void st_flip_destroy(st_flip* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
-                  s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->tileCnt, s->tileAux, s->tileAux2, s->on, s->tstate,
+                  s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
                   s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -183,8 +191,9 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(dalloc(&s->blkDead, NB + 1), "blkDead"); A(dalloc(&s->blkEmit, NB + 1), "blkEmit"); A(dalloc(&s->emitK, M), "emitK");
   A(dalloc(&s->deadList, M), "deadList");
   A(dalloc(&s->need, T), "need"); A(dalloc(&s->on, T), "on"); A(dalloc(&s->tstate, T), "tstate"); A(dalloc(&s->blkTiles, (T + 1023) / 1024 + 1), "blkTiles");
-  A(dalloc(&s->active, T), "active"); A(dalloc(&s->tileSlot, T), "tileSlot"); A(dalloc(&s->dropped, T), "dropped");
+  A(dalloc(&s->active, T), "active"); A(dalloc(&s->fluidTiles, T), "fluidTiles"); A(dalloc(&s->wet, C), "wet"); A(dalloc(&s->tileSlot, T), "tileSlot"); A(dalloc(&s->dropped, T), "dropped");
   A(dalloc(&s->tileCnt, T + 1), "tileCnt"); A(dalloc(&s->tileAux, T + 1), "tileAux"); A(dalloc(&s->tileAux2, T + 1), "tileAux2");
+  A(dalloc(&s->tileEmit, T + 1), "tileEmit"); A(dalloc(&s->tileDead, T + 1), "tileDead"); A(dalloc(&s->deadF, M), "deadF");
   A(dalloc(&s->cellOff, C), "cellOff"); A(dalloc(&s->ctype, C), "ctype"); A(dalloc(&s->pres, C), "pres"); A(dalloc(&s->rhs, C), "rhs");
   A(dalloc(&s->acc, 6 * C), "acc"); A(dalloc(&s->vn, 3 * C), "vn"); A(dalloc(&s->vo, 3 * C), "vo"); A(dalloc(&s->velG, 3 * C), "velG");
   A(dalloc(&s->sorInfo, C), "sorInfo"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
@@ -203,6 +212,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(cudaMemsetAsync(s->acc, 0, 6 * C * 4, q), "memset"); A(cudaMemsetAsync(s->vn, 0, 3 * C * 4, q), "memset");
   A(cudaMemsetAsync(s->vo, 0, 3 * C * 4, q), "memset"); A(cudaMemsetAsync(s->velG, 0, 3 * C * 4, q), "memset");
   A(cudaMemsetAsync(s->sorInfo, 0, C * 2, q), "memset");
+  A(cudaMemsetAsync(s->wet, 0, C * 4, q), "memset");
   A(cudaMemsetAsync(s->sPos, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
   A(cudaMemsetAsync(s->sVel, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
   launch_fill_f32(s->rhs, 8.0f, C, q);
@@ -291,6 +301,7 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc,
   if (sig != s->sdfSig) {
     if (off > s->sdfCap) {
       CK(cudaStreamSynchronize(s->stream));
+      drop_graphs(s);   // captured steps hold the old grid pointer
       cudaFree(s->sdf);
       s->sdfCap = (size_t)std::ceil(off * 1.3);
       CK(dalloc(&s->sdf, s->sdfCap));
@@ -354,7 +365,117 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
   for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &s->fills[k * 8], 8 * sizeof(float));
 }
 
-static void stage_fill(st_stage_times* t, const float* ms, float total);
+}  // extern "C"
+
+static void stage_fill(st_stage_times* t, const float* ms, float total) {
+  t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
+  t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8];
+  t->reseed = ms[9]; t->total = total;
+}
+
+// The device work of one step after the uploads: counters reset, then the stages in the reference's order
+// (src/flip/sim.js:253-309). mark(k) is called at the 11 stage boundaries. Returns the kernels launched.
+template <class Mark>
+static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, bool sprOn, int iters, Mark mark) {
+  cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q);        // fluid, vmaxBits, nLive (nActive is kept)
+  cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q);
+  cudaMemsetAsync(&s->dCtl->emitTried, 0, 2 * sizeof(uint32_t), q);     // emitTried, nFluidTiles
+  const int gT = s->tileGrid(8), gT4 = s->tileGrid(4);
+  int nl = 0;
+  mark(0);
+  // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
+  nl += launch_count_mark(B, q);
+  if (nbOn && init != 1) nl += launch_mark_phi(B, gT4, q);
+  if (init) nl += launch_mark_fill(B, std::max(1, (int)std::min<uint32_t>((s->ntiles + 255) / 256, 4096)), q);
+  nl += launch_tiles(B, s->ntiles, gT4, q);
+  if (init) nl += launch_nb_init(B, gT4, q);
+  nl += launch_scan_counts(B, q);
+  nl += launch_scatter(B, q);
+  mark(1);
+  nl += launch_p2g(B, gT, q);
+  mark(2);
+  if (nbOn) nl += launch_nb_phi(B, gT4, q);
+  mark(3);
+  nl += launch_classify(B, gT4, q);
+  if (nbOn) nl += launch_nb_vel(B, gT4, q);
+  mark(4);
+  nl += launch_norm_div(B, gT4, q);
+  mark(5);
+  nl += launch_sor(B, gT, iters, q);
+  mark(6);
+  nl += launch_project(B, gT4, q);
+  mark(7);
+  nl += launch_g2p(B, gT, q);
+  mark(8);
+  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, gT4, q);
+  mark(9);
+  if (nbOn) nl += launch_nb_reseed(B, gT4, q);
+  mark(10);
+  return nl;
+}
+
+// A step's kernels as a CUDA graph, keyed by everything that changes what is launched: the particle buffer parity,
+// the particle count (grid sizes), SOR iterations, narrow band, whitewater emission and stage timing. Stage markers are
+// external event-record nodes, pointed at the timing ring's events before each launch.
+static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, bool timing) {
+  return (uint64_t)s->cur | ((uint64_t)s->parity << 1) | ((uint64_t)nbOn << 2) | ((uint64_t)sprOn << 3) | ((uint64_t)timing << 4) |
+         ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24);
+}
+static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, bool timing, st_flip::Graph** out) {
+  const uint64_t key = graph_key(s, nbOn, sprOn, iters, timing);
+  for (auto& g : s->graphs) if (g.exec && g.key == key) { *out = &g; return ST_OK; }
+  if (s->graphs.size() >= 8) {   // a small cache: drop the oldest
+    if (s->graphs.front().exec) cudaGraphExecDestroy(s->graphs.front().exec);
+    if (s->graphs.front().graph) cudaGraphDestroy(s->graphs.front().graph);
+    s->graphs.erase(s->graphs.begin());
+  }
+  cudaStream_t q = s->stream;
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(q, cudaStreamCaptureModeThreadLocal));
+  int nl = enqueue_step(s, B, q, nbOn, 0, sprOn, iters, [&](int k) {
+    if (timing) cudaEventRecordWithFlags(s->tev[0][k], q, cudaEventRecordExternal);
+  });
+  cudaError_t e = cudaStreamEndCapture(q, &graph);
+  if (e != cudaSuccess) { set_err("graph capture", e); return ST_DEVICE_ERROR; }
+  st_flip::Graph g;
+  g.key = key;
+  g.launches = nl;
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (e == cudaSuccess && timing) {
+    size_t n = 0;
+    cudaGraphGetNodes(graph, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    cudaGraphGetNodes(graph, nodes.data(), &n);
+    int found = 0;
+    for (size_t k = 0; k < n && found < st_flip::TEV; k++) {
+      cudaGraphNodeType ty;
+      cudaGraphNodeGetType(nodes[k], &ty);
+      if (ty != cudaGraphNodeTypeEventRecord) continue;
+      cudaEvent_t ev;
+      cudaGraphEventRecordNodeGetEvent(nodes[k], &ev);
+      for (int j = 0; j < st_flip::TEV; j++) if (ev == s->tev[0][j]) { g.evnode[j] = nodes[k]; found++; }
+    }
+    if (found != st_flip::TEV) e = cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) {
+    set_err("graph instantiate", e);
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    cudaGraphDestroy(graph);
+    return ST_DEVICE_ERROR;
+  }
+  g.graph = graph;   // kept: its event-record node handles are updated before each launch
+  s->graphs.push_back(g);
+  *out = &s->graphs.back();
+  return ST_OK;
+}
+static void drop_graphs(st_flip* s) {
+  for (auto& g : s->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  s->graphs.clear();
+}
+
 // one step; t (optional) receives device ms per stage
 static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
   if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
@@ -386,51 +507,27 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   CK(cudaMemcpyAsync(&s->dUp->P, &up->P, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
   if (nc) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
   CK(cudaEventRecord(upEv, q));
-  // per-step counters: fluid, fastest speed, dropped tiles, emission
-  CK(cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q));   // fluid, vmaxBits (nActive is kept)
-  CK(cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q));
-  CK(cudaMemsetAsync(&s->dCtl->emitTried, 0, sizeof(uint32_t), q));
   const Bufs B = s->bufs();
-  const int gT = s->tileGrid(8), gT4 = s->tileGrid(4);
   cudaEvent_t* tslot = nullptr;
   if (s->timing) {
-    if (s->tcount >= (uint32_t)st_flip::TSLOTS) { CK(cudaEventSynchronize(s->tev[(s->tcount) % st_flip::TSLOTS][10])); }
+    if (s->tcount >= (uint32_t)st_flip::TSLOTS) CK(cudaEventSynchronize(s->tev[s->tcount % st_flip::TSLOTS][10]));
     tslot = s->tev[s->tcount % st_flip::TSLOTS];
   }
-  auto mark = [&](int k) {
-    if (t) cudaEventRecord(s->ev[k], q);
-    if (tslot) cudaEventRecord(tslot[k], q);
-  };
-  mark(0);
-  // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
   int nl = 0;
-  nl += launch_count_mark(B, q);
-  if (nbOn && init != 1) nl += launch_mark_phi(B, gT4, q);
-  if (init) nl += launch_mark_fill(B, std::max(1, (int)std::min<uint32_t>((s->ntiles + 255) / 256, 4096)), q);
-  nl += launch_tiles(B, s->ntiles, gT4, q);
-  if (init) nl += launch_nb_init(B, gT4, q);
-  nl += launch_scan_counts(B, q);
-  nl += launch_scatter(B, q);
-  mark(1);
-  nl += launch_p2g(B, gT, q);
-  mark(2);
-  if (nbOn) nl += launch_nb_phi(B, gT4, q);
-  mark(3);
-  nl += launch_classify(B, gT4, q);
-  if (nbOn) nl += launch_nb_vel(B, gT4, q);
-  mark(4);
-  nl += launch_norm_div(B, gT4, q);
-  mark(5);
-  nl += launch_sor(B, gT, iters, q);
-  mark(6);
-  nl += launch_project(B, gT4, q);
-  mark(7);
-  nl += launch_g2p(B, s->N, q);
-  mark(8);
-  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, gT4, q);
-  mark(9);
-  if (nbOn) nl += launch_nb_reseed(B, gT4, q);
-  mark(10);
+  if (s->use_graphs && !t && !init) {
+    st_flip::Graph* g = nullptr;
+    st = get_graph(s, B, nbOn, sprOn, iters, tslot != nullptr, &g);
+    if (st != ST_OK) return st;
+    if (tslot)
+      for (int k = 0; k < st_flip::TEV; k++) CK(cudaGraphExecEventRecordNodeSetEvent(g->exec, g->evnode[k], tslot[k]));
+    CK(cudaGraphLaunch(g->exec, q));
+    nl = g->launches;
+  } else {
+    nl = enqueue_step(s, B, q, nbOn, init, sprOn, iters, [&](int k) {
+      if (t) cudaEventRecord(s->ev[k], q);
+      if (tslot) cudaEventRecord(tslot[k], q);
+    });
+  }
   s->launches += (uint64_t)nl;
   CK(cudaGetLastError());
   s->steps++;
@@ -446,13 +543,10 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   return ST_OK;
 }
 
+extern "C" {
+
 st_status st_flip_step(st_flip* s, double dt, const st_step_opts* o) { return do_step(s, dt, o, nullptr); }
 
-static void stage_fill(st_stage_times* t, const float* ms, float total) {
-  t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
-  t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8];
-  t->reseed = ms[9]; t->total = total;
-}
 st_status st_flip_set_timing(st_flip* s, int on) {
   if (!s) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));

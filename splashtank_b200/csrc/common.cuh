@@ -46,7 +46,9 @@ struct Ctl {
   uint32_t defCount;    // narrow band deficit cells
   uint32_t defNeed;     // particles they ask for
   uint32_t emitTried;   // whitewater points tried this step
-  uint32_t pad[5];
+  uint32_t nFluidTiles; // tiles holding at least one fluid cell
+  uint32_t nKilled;     // particles g2p killed this step (open faces, narrow band trim)
+  uint32_t pad[3];
 };
 
 struct Part { float4 p, v; };   // one particle: position (w: speed + 64 x foam level), velocity (w: foam)
@@ -73,6 +75,7 @@ struct Bufs {
   uint32_t* prevActive; // last step's list (narrow band marking)
   uint32_t* tileSlot;   // tile -> position in active
   uint32_t* dropped;    // tiles that lost storage this step
+  uint32_t* fluidTiles; // tiles holding fluid this step (any order)
   uint32_t* tileCnt;    // per active position: particles, then exclusive offsets (size ntiles + 1)
   uint32_t* tileAux;    // per active position: scratch counts (deficit cells), then offsets
   uint32_t* tileAux2;   // per active position: scratch sums (deficit need), then offsets
@@ -88,6 +91,7 @@ struct Bufs {
   float* vo;            // 3 planes: old face velocity
   float* velG;          // 3 planes: kept grid velocity (narrow band)
   uint16_t* sorInfo;    // per fluid cell: bits 0-5 neighbour is fluid, bits 8-10 non-solid neighbours
+  float* wet;           // per cell: how much water (wetCell, src/flip/wgsl-whitewater.js:7-12), 0 outside the domain
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)
   const float* sdf;
@@ -96,8 +100,11 @@ struct Bufs {
   float4* sVel;
   uint8_t* emitK;       // per particle: points to emit
   uint32_t* blkEmit;    // per particle block: points, then offsets
+  uint8_t* deadF;       // per particle: killed by g2p this step (narrow band runs)
+  uint32_t* tileEmit;   // per active position: whitewater points its particles throw off, then offsets
+  uint32_t* tileDead;   // per active position: particles killed in it, then offsets
   // narrow band refill
-  uint32_t* deadList;
+  uint32_t* deadList;   // this step's killed particles in storage order
   uint32_t ncell;
   uint32_t nblk;        // particle blocks of PBLK
 };
@@ -246,6 +253,28 @@ __device__ __forceinline__ int colAt(const FlipParams& P, const float4* __restri
     if (phi < P.q0) return (int)k;
   }
   return -1;
+}
+
+// ---- whitewater emission terms (sprayEmit, src/flip/wgsl-whitewater.js:101-117), shared by g2p and the emit pass ----
+constexpr uint8_t EMIT_KILL = 0x80;   // emitK flag: the narrow band trims this particle once its points are written
+__device__ __forceinline__ float wetCellAt(const FlipParams& P, const float* __restrict__ wet, int i, int j, int k) {
+  if (!inDom(P, i, j, k)) return 0.0f;
+  return wet[cellIdx(P, i, j, k)];
+}
+__device__ __forceinline__ void emitTerms(const FlipParams& P, const float* __restrict__ wet, float4 qp, float4 qv, float& rho, float& fast, float& e) {
+  const V3 p = xyz(qp), v = xyz(qv);
+  const float foam = qv.w, spd = len3(v);
+  fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
+  const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+  rho = 0.0f;
+  for (int dz = 0; dz <= 1; dz++)
+    for (int dy = 0; dy <= 1; dy++)
+      for (int dx = 0; dx <= 1; dx++) rho += wetCellAt(P, wet, bi + dx, bj + dy, bk + dz);
+  rho = rho / 8.0f;
+  const float crest = (1.0f - smoothstepf(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
+  const float churn = (1.0f - smoothstepf(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstepf(0.5f, 1.5f, spd * P.vs);
+  e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstepf(0.1f, 0.5f, P.q8);
 }
 
 // ---- block-wide scans (blockDim.x a multiple of 32, at most 1024) ----

@@ -156,30 +156,7 @@ __global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
   }
 }
 
-// ---- refill: nbKill (wgsl-narrowband.js:93-102), nbDead (:106-110), nbDeficit (:112-130), nbSpawn (:134-148) ----
-__global__ void __launch_bounds__(PBLK) k_nb_kill(Bufs B) {
-  __shared__ FlipParams P;
-  loadParamsX(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
-  bool dead = false;
-  if (i < P.n) {
-    Part q = B.pa[i];
-    dead = q.p.y < DEADY;
-    if (!dead && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
-      int ci, cj, ck;
-      particleCell(P, xyz(q.p), ci, cj, ck);
-      const uint32_t cc = cellIdx(P, ci, cj, ck);
-      if (B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band) {
-        q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
-        q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        B.pa[i] = q;
-        dead = true;
-      }
-    }
-  }
-  const uint32_t nd = __syncthreads_count(dead);
-  if (threadIdx.x == 0) B.blkDead[blockIdx.x] = nd;
-}
+// ---- refill: nbDead (wgsl-narrowband.js:106-110), nbDeficit (:112-130), nbSpawn (:134-148); nbKill is in g2p ----
 __device__ void scanOneX(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
   uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
   uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
@@ -190,24 +167,39 @@ __device__ void scanOneX(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* s
   for (uint32_t x = beg; x < end; x++) { uint32_t v = arr[x]; arr[x] = run; run += v; }
   if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
 }
-// which: 0 dead blocks, 1 deficit (cells and need per tile), 2 emission blocks
+// which: 0 particles killed per tile, 1 deficit (cells and need per tile), 2 whitewater points per tile
 __global__ void __launch_bounds__(1024) k_scan_x(Bufs B, int which) {
   __shared__ uint32_t sm[33];
-  if (which == 0) scanOneX(B.blkDead, B.nblk, &B.ctl->nDead, sm);
+  const uint32_t nA = B.ctl->nActive;
+  if (which == 0) scanOneX(B.tileDead, nA, &B.ctl->nKilled, sm);
   else if (which == 1) {
-    if (blockIdx.x == 0) scanOneX(B.tileAux, B.ctl->nActive, &B.ctl->defCount, sm);
-    else scanOneX(B.tileAux2, B.ctl->nActive, &B.ctl->defNeed, sm);
-  } else scanOneX(B.blkEmit, B.nblk, &B.ctl->emitTried, sm);
+    if (blockIdx.x == 0) scanOneX(B.tileAux, nA, &B.ctl->defCount, sm);
+    else scanOneX(B.tileAux2, nA, &B.ctl->defNeed, sm);
+  } else scanOneX(B.tileEmit, nA, &B.ctl->emitTried, sm);
 }
-__global__ void __launch_bounds__(PBLK) k_dead_list(Bufs B) {
+// the dead slots, in ascending storage index: this step's kills inside the tiles' segments (listed here), then the slots
+// that were already dead when the step sorted them ([nLive, N), no list needed)
+__global__ void __launch_bounds__(512) k_killed_list(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
   loadParamsX(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
-  const bool dead = i < P.n && B.pa[i].p.y < DEADY;
-  const uint32_t r = blockExclusive(dead ? 1u : 0u, sm, nullptr);
-  const uint32_t k = B.blkDead[blockIdx.x] + r;
-  if (dead && k < P.lcap) B.deadList[k] = i;
+  const uint32_t nA = B.ctl->nActive;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    if (B.tileDead[a + 1] == B.tileDead[a]) continue;   // uniform per block: no kills in this tile
+    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
+    uint32_t base = B.tileDead[a];
+    for (uint32_t c0 = s0; c0 < s1; c0 += blockDim.x) {
+      const uint32_t i = c0 + threadIdx.x;
+      const bool d = i < s1 && B.deadF[i];
+      uint32_t tot;
+      const uint32_t r = blockExclusive(d ? 1u : 0u, sm, &tot);
+      if (d && base + r < P.lcap) B.deadList[base + r] = i;
+      base += tot;
+    }
+  }
+}
+__device__ __forceinline__ uint32_t deadSlot(const Bufs& B, uint32_t k, uint32_t nKilled, uint32_t nLive) {
+  return k < nKilled ? B.deadList[k] : nLive + (k - nKilled);
 }
 // the deficit test of one cell; returns the particles it asks for (0: none)
 __device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs& B, uint32_t c, int i, int j, int k) {
@@ -242,7 +234,8 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
   __shared__ uint32_t sm[33];
   loadParamsX(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
-  const uint32_t avail = min(B.ctl->nDead, P.lcap);
+  const uint32_t nKilled = B.ctl->nKilled, nLive = B.ctl->nLive;
+  const uint32_t avail = min(nKilled + (P.n - nLive), P.lcap);
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
@@ -255,7 +248,7 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
     for (uint32_t m = 0; m < nd; m++) {
       const uint32_t kk = base + m;
       if (kk >= avail) break;
-      const uint32_t pi = B.deadList[kk];
+      const uint32_t pi = deadSlot(B, kk, nKilled, nLive);
       const uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
       const V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
       const V3 v = velGVecX(P, B.velG, nc, x);
@@ -268,14 +261,8 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
 }
 
 // ---- whitewater: wetCell / wetAt (wgsl-whitewater.js:7-23) ----
-__device__ __forceinline__ float wetCell(const FlipParams& P, const Bufs& B, int i, int j, int k) {
-  if (!inDom(P, i, j, k)) return 0.0f;
-  const uint32_t ci = cellIdx(P, i, j, k);
-  if (!B.on[ci >> 9]) return 0.0f;
-  const uint32_t ct = B.ctype[ci];
-  if (P.nb != 0u && (ct & 0xffu) == 1u && phiOfBits(ct) < -1.0f) return 1.0f;
-  return fmn((float)B.cnt[ci] / P.rest, 1.0f);
-}
+// the per-cell values are computed once a step by the divergence pass (0 for tiles without storage)
+__device__ __forceinline__ float wetCell(const FlipParams& P, const Bufs& B, int i, int j, int k) { return wetCellAt(P, B.wet, i, j, k); }
 __device__ __forceinline__ float wetAt(const FlipParams& P, const Bufs& B, V3 p) {
   const V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
   const V3 f0 = vfloor(g), fr = g - f0;
@@ -377,81 +364,59 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
     B.sVel[j] = make_float4(v.x, v.y, v.z, (float)kind + 0.4f * tk / WWHOLD);
   }
 }
-// sprayEmit (wgsl-whitewater.js:99-133), part 1: how many points each water particle throws off
-__device__ __forceinline__ void emitTerms(const FlipParams& P, const Bufs& B, const Part& q, float& rho, float& fast, float& e) {
-  const V3 p = xyz(q.p), v = xyz(q.v);
-  const float foam = q.v.w, spd = len3(v);
-  fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
-  const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
-  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
-  rho = 0.0f;
-  for (int dz = 0; dz <= 1; dz++)
-    for (int dy = 0; dy <= 1; dy++)
-      for (int dx = 0; dx <= 1; dx++) rho += wetCell(P, B, bi + dx, bj + dy, bk + dz);
-  rho = rho / 8.0f;
-  const float crest = (1.0f - smoothstepf(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
-  const float churn = (1.0f - smoothstepf(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstepf(0.5f, 1.5f, spd * P.vs);
-  e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstepf(0.1f, 0.5f, P.q8);
-}
-__global__ void __launch_bounds__(PBLK) k_emit_count(Bufs B) {
+// sprayEmit (wgsl-whitewater.js:99-133): g2p counted each particle's points (emitK) and their sum per tile; here the
+// points go into ring slots (sctl[0] + run) % smax that are not alive, run counting in storage order
+__global__ void __launch_bounds__(256) k_emit_write(Bufs B) {
   __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
   loadParamsX(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
-  uint32_t kc = 0;
-  if (i < P.n && P.smax != 0u && P.sprRate > 0.0f) {
-    const Part q = B.pa[i];
-    if (q.p.y >= DEADY) {
+  const uint32_t nA = B.ctl->nActive, s0ring = B.ctl->sctl0;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    if (B.tileEmit[a + 1] == B.tileEmit[a]) continue;   // uniform per block: nothing thrown off in this tile
+    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
+    uint32_t base = B.tileEmit[a];
+    for (uint32_t c0 = s0; c0 < s1; c0 += blockDim.x) {
+      const uint32_t i = c0 + threadIdx.x;
+      const uint32_t ek = i < s1 ? B.emitK[i] : 0u;
+      const uint32_t kc = ek & 7u;
+      uint32_t tot;
+      const uint32_t run0 = base + blockExclusive(kc, sm, &tot);
+      base += tot;
+      if (!kc) continue;
+      Part q = B.pa[i];
       float rho, fast, e;
-      emitTerms(P, B, q, rho, fast, e);
-      if (e > 0.0f) {
-        const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
-        kc = min(u32f(floorf(P.sprRate * e * P.dt + hash1(h0))), 4u);
+      emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
+      const V3 qp = xyz(q.p), v = xyz(q.v);
+      const float spd = len3(v);
+      const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
+      for (uint32_t mm = 0; mm < kc; mm++) {
+        const uint32_t run = run0 + mm;
+        if (run >= P.smax) break;   // more points tried in one step than the ring holds: the rest are dropped
+        const uint32_t slot = (uint32_t)(((uint64_t)s0ring + run) % P.smax);
+        if (B.sPos[slot].w > 0.0f) continue;   // never replace a living point
+        const uint32_t hh = h0 ^ ((mm + 1u) * 0x9E3779B9u);
+        const float z = hash1(hh + 1u) * 2.0f - 1.0f;
+        const float an = hash1(hh + 2u) * 6.2831853f;
+        const float s = sqrtf(fmx(0.0f, 1.0f - z * z));
+        float sa, ca;
+        st_sincosf(an, &sa, &ca);
+        const V3 dir = v3(s * ca, s * sa, z);
+        const bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
+        const bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
+        V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
+        float life = P.sprLife * (0.6f + 0.8f * hash1(hh + 5u)) * (mist ? 1.6f : 1.0f);
+        float kind = mist ? 1.0f : 0.0f;
+        if (under) { nv = v + dir * spd * 0.05f; life = P.wwFoamLife * (0.6f + 0.8f * hash1(hh + 5u)); kind = 3.0f; }
+        const V3 np = qp + nv * P.dt + dir * P.h * 0.3f * hash1(hh + 6u);
+        B.sPos[slot] = make_float4(np.x, np.y, np.z, life);
+        B.sVel[slot] = make_float4(nv.x, nv.y, nv.z, kind);
+      }
+      if (ek & EMIT_KILL) {   // the narrow band trim g2p held back until the points were written
+        q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+        q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        B.pa[i] = q;
       }
     }
-  }
-  if (i < P.n) B.emitK[i] = (uint8_t)kc;
-  __shared__ uint32_t sm[33];
-  uint32_t tot;
-  blockExclusive(kc, sm, &tot);
-  if (threadIdx.x == 0) B.blkEmit[blockIdx.x] = tot;
-}
-// part 2: the points, into ring slots (sctl[0] + run) % smax that are not alive
-__global__ void __launch_bounds__(PBLK) k_emit_write(Bufs B) {
-  __shared__ FlipParams P;
-  __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
-  const uint32_t kc = i < P.n ? B.emitK[i] : 0u;
-  const uint32_t run0 = B.blkEmit[blockIdx.x] + blockExclusive(kc, sm, nullptr);
-  if (!kc) return;
-  const uint32_t s0 = B.ctl->sctl0;
-  const Part q = B.pa[i];
-  float rho, fast, e;
-  emitTerms(P, B, q, rho, fast, e);
-  const V3 qp = xyz(q.p), v = xyz(q.v);
-  const float spd = len3(v);
-  const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
-  for (uint32_t mm = 0; mm < kc; mm++) {
-    const uint32_t run = run0 + mm;
-    if (run >= P.smax) break;   // more points tried in one step than the ring holds: the rest are dropped
-    const uint32_t slot = (uint32_t)(((uint64_t)s0 + run) % P.smax);
-    if (B.sPos[slot].w > 0.0f) continue;   // never replace a living point
-    const uint32_t hh = h0 ^ ((mm + 1u) * 0x9E3779B9u);
-    const float z = hash1(hh + 1u) * 2.0f - 1.0f;
-    const float an = hash1(hh + 2u) * 6.2831853f;
-    const float s = sqrtf(fmx(0.0f, 1.0f - z * z));
-    float sa, ca;
-    st_sincosf(an, &sa, &ca);
-    const V3 dir = v3(s * ca, s * sa, z);
-    const bool under = rho > 0.7f && hash1(hh + 7u) < 0.7f;
-    const bool mist = !under && hash1(hh + 3u) < P.mistFrac * fast;
-    V3 nv = v * (0.9f + 0.2f * hash1(hh + 4u)) + dir * spd * (mist ? 0.2f : 0.06f);
-    float life = P.sprLife * (0.6f + 0.8f * hash1(hh + 5u)) * (mist ? 1.6f : 1.0f);
-    float kind = mist ? 1.0f : 0.0f;
-    if (under) { nv = v + dir * spd * 0.05f; life = P.wwFoamLife * (0.6f + 0.8f * hash1(hh + 5u)); kind = 3.0f; }
-    const V3 np = qp + nv * P.dt + dir * P.h * 0.3f * hash1(hh + 6u);
-    B.sPos[slot] = make_float4(np.x, np.y, np.z, life);
-    B.sVel[slot] = make_float4(nv.x, nv.y, nv.z, kind);
   }
 }
 __global__ void k_emit_done(Bufs B) {
@@ -472,24 +437,21 @@ int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s) {
 }
 int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s) { k_nb_vel<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
-  if (!B.nblk) return 0;
-  k_nb_kill<<<B.nblk, PBLK, 0, s>>>(B);
   k_scan_x<<<1, 1024, 0, s>>>(B, 0);
-  k_dead_list<<<B.nblk, PBLK, 0, s>>>(B);
+  k_killed_list<<<grid, 512, 0, s>>>(B);
   k_def_count<<<grid, 512, 0, s>>>(B);
   k_scan_x<<<2, 1024, 0, s>>>(B, 1);
   k_spawn<<<grid, 512, 0, s>>>(B);
-  return 6;
+  return 5;
 }
 int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s) {
   if (!smax) return 0;
   k_ww_step<<<grid, 256, 0, s>>>(B);
-  if (!emit || !B.nblk) return 1;
-  k_emit_count<<<B.nblk, PBLK, 0, s>>>(B);
+  if (!emit) return 1;
   k_scan_x<<<1, 1024, 0, s>>>(B, 2);
-  k_emit_write<<<B.nblk, PBLK, 0, s>>>(B);
+  k_emit_write<<<grid, 256, 0, s>>>(B);
   k_emit_done<<<1, 1, 0, s>>>(B);
-  return 5;
+  return 4;
 }
 
 }  // namespace st

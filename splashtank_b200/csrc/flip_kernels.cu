@@ -58,12 +58,20 @@ __global__ void __launch_bounds__(PBLK) k_count_mark(Bufs B) {
   if (live && lane == leader) base = (uint32_t)atomicAdd(&B.cnt[key], __popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (live) B.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
-  // fastest speed: lengths are non-negative, so their bit patterns order like the floats
+  // fastest speed: lengths are non-negative, so their bit patterns order like the floats; one atomic per block
+  __shared__ float wmax[PBLK / 32];
   float m = sp;
   for (int o = 16; o > 0; o >>= 1) m = fmx(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0 && m > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(m));
+  if (lane == 0) wmax[threadIdx.x >> 5] = m;
   uint32_t nd = __syncthreads_count(dead);
-  if (threadIdx.x == 0) B.blkDead[blockIdx.x] = nd;
+  if (threadIdx.x < 32) {
+    float b = wmax[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) b = fmx(b, __shfl_xor_sync(0xffffffffu, b, o));
+    if (threadIdx.x == 0) {
+      B.blkDead[blockIdx.x] = nd;
+      if (b > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(b));
+    }
+  }
 }
 
 // tileMarkPhi (wgsl-narrowband.js:6-10): last step's tiles that hold water by depth keep storage.
@@ -165,7 +173,7 @@ __global__ void __launch_bounds__(512) k_tile_prep(Bufs B) {
       if (threadIdx.x == 0) B.tileCnt[a] = tot;
     } else {
       uint32_t t = B.dropped[a - nA], c = t * 512u + threadIdx.x;
-      B.cnt[c] = 0; B.cntOther[c] = 0; B.ctype[c] = 0u; B.pres[c] = 0.0f; B.rhs[c] = 8.0f; B.sorInfo[c] = 0;
+      B.cnt[c] = 0; B.cntOther[c] = 0; B.ctype[c] = 0u; B.pres[c] = 0.0f; B.rhs[c] = 8.0f; B.sorInfo[c] = 0; B.wet[c] = 0.0f;
       for (int p = 0; p < 6; p++) B.acc[p * nc + c] = 0;
       for (int p = 0; p < 3; p++) { B.vn[p * nc + c] = 0.0f; B.vo[p * nc + c] = 0.0f; B.velG[p * nc + c] = 0.0f; }
     }
@@ -318,7 +326,10 @@ __global__ void __launch_bounds__(512) k_classify(Bufs B) {
     B.ctype[c] = ty | sb;
     if (ty != 1u) B.pres[c] = 0.0f;
     const uint32_t nf = __syncthreads_count(ty == 1u);
-    if (threadIdx.x == 0 && nf) atomicAdd(&B.ctl->fluid, nf);
+    if (threadIdx.x == 0 && nf) {
+      atomicAdd(&B.ctl->fluid, nf);
+      B.fluidTiles[atomicAdd(&B.ctl->nFluidTiles, 1u)] = t;   // the pressure sweeps visit only these (order free)
+    }
   }
 }
 
@@ -367,6 +378,11 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
     }
     __syncthreads();
     const uint32_t ct = B.ctype[c];
+    {   // wetCell (wgsl-whitewater.js:7-12): types, depth and counts are final for this step from here on
+      float wv = 0.0f;
+      if (inDom(P, i, j, k)) wv = (P.nb != 0u && (ct & 0xffu) == 1u && phiOfBits(ct) < -1.0f) ? 1.0f : fmn((float)B.cnt[c] / P.rest, 1.0f);
+      B.wet[c] = wv;
+    }
     if ((ct & 0xffu) != 1u) {
       B.rhs[c] = 0.0f;
       B.sorInfo[c] = 0;
@@ -398,31 +414,42 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
 }
 
 // ---- 8. red-black SOR (relax, wgsl-solver.js:124-140; rbRed/rbBlack :162-164) ----
-// One CTA per tile, one thread per cell of the colour. sorInfo holds the neighbour types found after classify.
+// One CTA per tile holding fluid, one thread per cell of the colour. sorInfo (from classify's types) says which
+// neighbours are fluid and how many are not solid. All eight loads of a cell are issued together from addresses that
+// are always valid (a missing neighbour reads the cell itself); the sum then adds only the fluid neighbours, in the
+// reference's order, so the arithmetic is unchanged.
 __global__ void __launch_bounds__(256) k_sor(Bufs B, uint32_t color) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
-  const uint32_t nA = B.ctl->nActive;
+  const uint32_t nT = B.ctl->nFluidTiles;
   const int lz = threadIdx.x >> 5, ly = (threadIdx.x >> 2) & 7;
   const int lx = 2 * (threadIdx.x & 3) + (int)((ly + lz + color) & 1);
   const uint32_t local = (uint32_t)(lx + 8 * (ly + 8 * lz));
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
-    const uint32_t t = B.active[a], c = t * 512u + local;
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t t = B.fluidTiles[a], c = t * 512u + local;
+    const uint32_t tt = t / P.tx, ti = t % P.tx, tj = tt % P.ty, tk = tt / P.ty;
+    // neighbour cells: inside the tile by offset, across a tile face into the neighbouring tile
+    const uint32_t cxm = lx > 0 ? c - 1u : (ti > 0 ? c - 512u + 7u : c);
+    const uint32_t cxp = lx < 7 ? c + 1u : (ti + 1 < P.tx ? c + 512u - 7u : c);
+    const uint32_t cym = ly > 0 ? c - 8u : (tj > 0 ? c - 512u * P.tx + 56u : c);
+    const uint32_t cyp = ly < 7 ? c + 8u : (tj + 1 < P.ty ? c + 512u * P.tx - 56u : c);
+    const uint32_t cell_z = 512u * P.tx * P.ty;
+    const uint32_t czm = lz > 0 ? c - 64u : (tk > 0 ? c - cell_z + 448u : c);
+    const uint32_t czp = lz < 7 ? c + 64u : (tk + 1 < P.tz ? c + cell_z - 448u : c);
     const uint32_t info = B.sorInfo[c];
+    const float p0 = B.pres[c], r0 = B.rhs[c];
+    const float pxm = B.pres[cxm], pxp = B.pres[cxp], pym = B.pres[cym], pyp = B.pres[cyp], pzm = B.pres[czm], pzp = B.pres[czp];
     if (!(info & 0x8000u)) continue;
     const uint32_t nns = (info >> 8) & 7u;
     if (nns == 0u) { B.pres[c] = 0.0f; continue; }
-    int i, j, k;
-    tileCoord(P, t, local, i, j, k);
     float sum = 0.0f;
-    if (info & 1u) sum += B.pres[cellIdx(P, i - 1, j, k)];
-    if (info & 2u) sum += B.pres[cellIdx(P, i + 1, j, k)];
-    if (info & 4u) sum += B.pres[cellIdx(P, i, j - 1, k)];
-    if (info & 8u) sum += B.pres[cellIdx(P, i, j + 1, k)];
-    if (info & 16u) sum += B.pres[cellIdx(P, i, j, k - 1)];
-    if (info & 32u) sum += B.pres[cellIdx(P, i, j, k + 1)];
-    const float pg = (B.rhs[c] + sum) / (float)nns;
-    const float p0 = B.pres[c];
+    if (info & 1u) sum += pxm;
+    if (info & 2u) sum += pxp;
+    if (info & 4u) sum += pym;
+    if (info & 8u) sum += pyp;
+    if (info & 16u) sum += pzm;
+    if (info & 32u) sum += pzp;
+    const float pg = (r0 + sum) / (float)nns;
     B.pres[c] = p0 + P.omega * (pg - p0);
   }
 }
@@ -508,73 +535,222 @@ __device__ float vnz(V3 x) {   // value noise (wgsl-solver.js:202-207)
   const float b = mixf(mixf(hsh3(i + v3(0, 0, 1)), hsh3(i + v3(1, 0, 1)), u.x), mixf(hsh3(i + v3(0, 1, 1)), hsh3(i + v3(1, 1, 1)), u.x), u.y);
   return mixf(a, b, u.z);
 }
-__global__ void __launch_bounds__(256) k_g2p(Bufs B) {
+// The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
+struct G2PWin {
+  const float* vn;   // [3][1000]
+  const float* vo;
+  const int32_t* cnt;
+  int ox, oy, oz;
+  __device__ __forceinline__ int idx(int i, int j, int k) const { return (i - ox + 1) + 10 * ((j - oy + 1) + 10 * (k - oz + 1)); }
+};
+__device__ __forceinline__ void sampleWin(const FlipParams& P, const G2PWin& W, V3 p, V3& vn, V3& vo) {
+  float rn[3], ro[3];
+  for (int axis = 0; axis < 3; axis++) {
+    V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+    if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+    const V3 f0 = vfloor(g), fr = g - f0;
+    const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    // the clamped corner cells of faceIndex (wgsl-core.js:84-89): two candidates per axis
+    const int hx = axis == 0 ? (int)P.nx : (int)P.nx - 1, hy = axis == 1 ? (int)P.ny : (int)P.ny - 1, hz = axis == 2 ? (int)P.nz : (int)P.nz - 1;
+    const int xa = clampi(i0, 0, hx), xb = clampi(i0 + 1, 0, hx);
+    const int ya = clampi(j0, 0, hy), yb = clampi(j0 + 1, 0, hy);
+    const int za = clampi(k0, 0, hz), zb = clampi(k0 + 1, 0, hz);
+    const float* wn = W.vn + axis * 1000;
+    const float* wo = W.vo + axis * 1000;
+    float sn = 0.0f, so = 0.0f;
+    for (int c = 0; c < 8; c++) {
+      const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      const int f = W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za);
+      sn += w * wn[f];
+      so += w * wo[f];
+    }
+    rn[axis] = sn;
+    ro[axis] = so;
+  }
+  vn = v3(rn[0], rn[1], rn[2]);
+  vo = v3(ro[0], ro[1], ro[2]);
+}
+// The gust noise's hash lattice has spacing 1 in units of p * 0.55, so a whole tank spans only a few lattice points.
+// Each CTA hashes them once into a table (the same hsh3 on the same integer-valued inputs, so the values are identical);
+// points outside the table are hashed directly.
+constexpr int GT_MAX = 512;
+struct GustTab {
+  float v[3][GT_MAX];
+  int lo[3][3], n[3][3];
+  bool on;
+};
+__device__ __forceinline__ float vnzTab(const GustTab& T, int which, V3 x) {
+  const V3 i = vfloor(x), fr = x - vfloor(x);
+  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
+  const int ix = (int)i.x - T.lo[which][0], iy = (int)i.y - T.lo[which][1], iz = (int)i.z - T.lo[which][2];
+  const int nx = T.n[which][0], ny = T.n[which][1], nz = T.n[which][2];
+  if (!T.on || ix < 0 || iy < 0 || iz < 0 || ix + 1 >= nx || iy + 1 >= ny || iz + 1 >= nz) return vnz(x);
+  const float* t = T.v[which];
+  const int b = ix + nx * (iy + ny * iz), sy = nx, sz = nx * ny;
+  const float a = mixf(mixf(t[b], t[b + 1], u.x), mixf(t[b + sy], t[b + sy + 1], u.x), u.y);
+  const float c = mixf(mixf(t[b + sz], t[b + sz + 1], u.x), mixf(t[b + sz + sy], t[b + sz + sy + 1], u.x), u.y);
+  return mixf(a, c, u.z);
+}
+__device__ void buildGust(const FlipParams& P, GustTab& T) {
+  const float tt = P.q8 * 0.6f;
+  const float off[3][3] = {{tt, 0.0f, 0.0f}, {17.3f, tt, 4.1f}, {5.7f, 9.2f, tt}};
+  const float lo3[3] = {P.x0, P.y0, P.z0}, hi3[3] = {P.x1, P.y1, P.z1};
+  if (threadIdx.x == 0) {
+    bool ok = P.q7 > 0.0f && P.q4 > 0.0f;
+    for (int w = 0; w < 3; w++) {
+      int cells = 1;
+      for (int a = 0; a < 3; a++) {
+        const int l = (int)floorf(lo3[a] * 0.55f + off[w][a]) - 1, h = (int)floorf(hi3[a] * 0.55f + off[w][a]) + 2;
+        T.lo[w][a] = l;
+        T.n[w][a] = h - l + 1;
+        cells *= T.n[w][a];
+      }
+      if (cells > GT_MAX) ok = false;
+    }
+    T.on = ok;
+  }
+  __syncthreads();
+  if (!T.on) return;
+  for (int w = 0; w < 3; w++) {
+    const int nx = T.n[w][0], ny = T.n[w][1], nz = T.n[w][2];
+    for (int r = threadIdx.x; r < nx * ny * nz; r += blockDim.x) {
+      const int ix = r % nx, iy = (r / nx) % ny, iz = r / (nx * ny);
+      T.v[w][r] = hsh3(v3((float)(ix + T.lo[w][0]), (float)(iy + T.lo[w][1]), (float)(iz + T.lo[w][2])));
+    }
+  }
+  __syncthreads();
+}
+__device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, Part& q) {
+  const V3 p = xyz(q.p), v0 = xyz(q.v);
+  int fi, fj, fk;
+  particleCell(P, p, fi, fj, fk);
+  V3 vn, vo;
+  sampleWin(P, W, p, vn, vo);    // the particle's own tile has storage: it marked it this step
+  V3 v = vmix(vn, v0 + (vn - vo), P.flip);
+  const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+  float csum = 8.0f * P.rest;
+  const bool fast = P.q12 > 0.5f;
+  if (P.q9 < 0.5f && fast) csum = 8.0f * (float)W.cnt[W.idx(fi, fj, fk)];
+  else if (P.q9 < 0.5f) {
+    csum = 0.0f;
+    const int xa = clampi(bi, 0, (int)P.nx - 1), xb = clampi(bi + 1, 0, (int)P.nx - 1);
+    const int ya = clampi(bj, 0, (int)P.ny - 1), yb = clampi(bj + 1, 0, (int)P.ny - 1);
+    const int za = clampi(bk, 0, (int)P.nz - 1), zb = clampi(bk + 1, 0, (int)P.nz - 1);
+    for (int dz = 0; dz <= 1; dz++)
+      for (int dy = 0; dy <= 1; dy++)
+        for (int dx = 0; dx <= 1; dx++) csum += (float)W.cnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
+  }
+  const float rho = csum / (8.0f * P.rest);
+  const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
+  const float shield = smoothstepf(0.1f, 0.65f, rho);
+  const float exposure = 1.0f - 0.97f * shield;
+  const float spd0 = len3(v);
+  const float sens = fmx(P.q6, 0.05f);
+  const float pacc = len3(vn - vo) / P.dt;
+  const float settle = smoothstepf(0.1f, 0.5f, P.q8);
+  const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
+  const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
+  const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
+  const float tau = fmx(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
+  float foam = q.v.w * st_expf(-P.dt / tau);
+  foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
+  V3 gust = v3(0.0f, 0.0f, 0.0f);
+  if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
+    const V3 gp = p * 0.55f;
+    const float tt = P.q8 * 0.6f;
+    gust = v3(vnzTab(T, 0, gp + v3(tt, 0.0f, 0.0f)), vnzTab(T, 1, gp + v3(17.3f, tt, 4.1f)), vnzTab(T, 2, gp + v3(5.7f, 9.2f, tt))) * 2.0f -
+           v3(1.0f, 1.0f, 1.0f);
+  }
+  const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
+  const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
+  v = v + (airv - v) * (1.0f - st_expf(-kd * P.dt));
+  const float sp = len3(v);
+  if (sp > P.vmax) v = v * (P.vmax / sp);
+  const V3 pt = p + v * P.dt;
+  const V3 pc = collideP(P, B, pt);
+  const V3 dsp = pc - pt;
+  if (dot3(dsp, dsp) > 1.0e-12f) {
+    const V3 nrm = dsp / len3(dsp);
+    const float vd = dot3(v, nrm);
+    if (vd < 0.0f) v = v - nrm * vd;
+  }
+  const uint32_t o = P.open;
+  if (o != 0u && (((o & 1u) && pc.x < P.x0) || ((o & 2u) && pc.x > P.x1) || ((o & 4u) && pc.y < P.y0) ||
+                  ((o & 8u) && pc.y > P.y1) || ((o & 16u) && pc.z < P.z0) || ((o & 32u) && pc.z > P.z1))) {
+    q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+    q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  } else {
+    q.p = make_float4(pc.x, pc.y, pc.z, fmn(len3(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f));
+    q.v = make_float4(v.x, v.y, v.z, foam);
+  }
+}
+// One CTA per tile with storage: the tile's particles are one contiguous sorted segment, and every face and count they
+// sample lies in the 10^3-cell window (the tile plus one cell around it), staged once in shared memory.
+constexpr int G2P_T = 256;
+__global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   __shared__ FlipParams P;
+  __shared__ float wvn[3 * 1000], wvo[3 * 1000];
+  __shared__ int32_t wcnt[1000];
+  __shared__ GustTab gtab;
+  __shared__ uint32_t sm[33];
   loadParams(P, B.P);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x) {
-    Part q = B.pa[i];
-    if (q.p.y < DEADY) continue;
-    const V3 p = xyz(q.p), v0 = xyz(q.v);
-    int fi, fj, fk;
-    particleCell(P, p, fi, fj, fk);
-    V3 vn = v0 - v3(0.0f, P.gravity * P.dt, 0.0f), vo = v0;
-    if (B.on[tileOf(P, fi, fj, fk)]) sampleBoth(P, B, p, vn, vo);
-    V3 v = vmix(vn, v0 + (vn - vo), P.flip);
-    const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
-    const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
-    float csum = 8.0f * P.rest;
-    const bool fast = P.q12 > 0.5f;
-    if (P.q9 < 0.5f && fast) csum = 8.0f * (float)B.cnt[cellIdx(P, fi, fj, fk)];
-    else if (P.q9 < 0.5f) {
-      csum = 0.0f;
-      for (int dz = 0; dz <= 1; dz++)
-        for (int dy = 0; dy <= 1; dy++)
-          for (int dx = 0; dx <= 1; dx++)
-            csum += (float)B.cnt[cellIdx(P, clampi(bi + dx, 0, (int)P.nx - 1), clampi(bj + dy, 0, (int)P.ny - 1), clampi(bk + dz, 0, (int)P.nz - 1))];
+  buildGust(P, gtab);
+  const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
+  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    const uint32_t t = B.active[a], tt = t / P.tx;
+    G2PWin W{wvn, wvo, wcnt, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    for (int r = threadIdx.x; r < 1000; r += G2P_T) {
+      const int gi = W.ox + r % 10 - 1, gj = W.oy + (r / 10) % 10 - 1, gk = W.oz + r / 100 - 1;
+      if (gi < 0 || gj < 0 || gk < 0 || gi >= NX || gj >= NY || gk >= NZ) continue;   // never sampled: clamping keeps indices >= 0
+      const uint32_t c = cellIdx(P, gi, gj, gk);
+      for (int ax = 0; ax < 3; ax++) { wvn[ax * 1000 + r] = B.vn[ax * nc + c]; wvo[ax * 1000 + r] = B.vo[ax * nc + c]; }
+      wcnt[r] = B.cnt[c];
     }
-    const float rho = csum / (8.0f * P.rest);
-    const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
-    const float shield = smoothstepf(0.1f, 0.65f, rho);
-    const float exposure = 1.0f - 0.97f * shield;
-    const float spd0 = len3(v);
-    const float sens = fmx(P.q6, 0.05f);
-    const float pacc = len3(vn - vo) / P.dt;
-    const float settle = smoothstepf(0.1f, 0.5f, P.q8);
-    const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
-    const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
-    const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
-    const float tau = fmx(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
-    float foam = q.v.w * st_expf(-P.dt / tau);
-    foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
-    V3 gust = v3(0.0f, 0.0f, 0.0f);
-    if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
-      const V3 gp = p * 0.55f;
-      const float tt = P.q8 * 0.6f;
-      gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
+    __syncthreads();
+    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
+    uint32_t emitSum = 0, deadSum = 0;
+    for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
+      Part q = B.pa[i];
+      g2pOne(P, B, W, gtab, q);
+      // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
+      // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
+      const bool gone = q.p.y < DEADY;
+      uint32_t kc = 0;
+      if (!gone && P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f) {
+        float rho, fast, e;
+        emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
+        if (e > 0.0f) {
+          const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
+          kc = min(u32f(floorf(P.sprRate * e * P.dt + hash1(h0))), 4u);
+        }
+      }
+      bool kill = false;
+      if (!gone && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
+        int ci, cj, ck;
+        particleCell(P, xyz(q.p), ci, cj, ck);
+        const uint32_t cc = cellIdx(P, ci, cj, ck);
+        kill = B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band;
+      }
+      if (kill && kc == 0) {
+        q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+        q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      }
+      B.pa[i] = q;
+      if (P.sprayOn != 0u) B.emitK[i] = (uint8_t)(kc | (kill && kc ? EMIT_KILL : 0u));
+      if (P.nb != 0u) B.deadF[i] = (gone || kill) ? 1 : 0;
+      emitSum += kc;
+      deadSum += (gone || kill) ? 1u : 0u;
     }
-    const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
-    const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
-    v = v + (airv - v) * (1.0f - st_expf(-kd * P.dt));
-    const float sp = len3(v);
-    if (sp > P.vmax) v = v * (P.vmax / sp);
-    const V3 pt = p + v * P.dt;
-    const V3 pc = collideP(P, B, pt);
-    const V3 dsp = pc - pt;
-    if (dot3(dsp, dsp) > 1.0e-12f) {
-      const V3 nrm = dsp / len3(dsp);
-      const float vd = dot3(v, nrm);
-      if (vd < 0.0f) v = v - nrm * vd;
+    if (P.sprayOn != 0u || P.nb != 0u) {
+      uint32_t te, td;
+      blockExclusive(emitSum, sm, &te);
+      blockExclusive(deadSum, sm, &td);
+      if (threadIdx.x == 0) { B.tileEmit[a] = te; B.tileDead[a] = td; }
     }
-    const uint32_t o = P.open;
-    if (o != 0u && (((o & 1u) && pc.x < P.x0) || ((o & 2u) && pc.x > P.x1) || ((o & 4u) && pc.y < P.y0) ||
-                    ((o & 8u) && pc.y > P.y1) || ((o & 16u) && pc.z < P.z0) || ((o & 32u) && pc.z > P.z1))) {
-      q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
-      q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    } else {
-      q.p = make_float4(pc.x, pc.y, pc.z, fmn(len3(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f));
-      q.v = make_float4(v.x, v.y, v.z, foam);
-    }
-    B.pa[i] = q;
+    __syncthreads();
   }
 }
 
@@ -636,9 +812,8 @@ int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s) {
   return 2 * iters;
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
-int launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s) {
-  if (!n) return 0;
-  k_g2p<<<(n + 255) / 256, 256, 0, s>>>(B);
+int launch_g2p(const Bufs& B, int grid, cudaStream_t s) {
+  k_g2p<<<grid, G2P_T, 0, s>>>(B);
   return 1;
 }
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {

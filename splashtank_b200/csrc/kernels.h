@@ -14,7 +14,7 @@ int launch_classify(const Bufs& B, int grid, cudaStream_t s);
 int launch_norm_div(const Bufs& B, int grid, cudaStream_t s);
 int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s);
 int launch_project(const Bufs& B, int grid, cudaStream_t s);
-int launch_g2p(const Bufs& B, uint32_t n, cudaStream_t s);
+int launch_g2p(const Bufs& B, int grid, cudaStream_t s);
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);
 int launch_fill_f32(float* p, float v, size_t n, cudaStream_t s);
 int launch_iota(uint32_t* p, uint32_t n, cudaStream_t s);
