@@ -40,7 +40,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=40)
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    return ap.parse_args()
+    ap.add_argument("--tol", type=float, default=1e-6, help="pressure workloads: relative residual to reach")
+    ap.add_argument("--omega", type=float, default=1.9, help="pressure workloads: SOR factor")
+    ap.add_argument("--inner", type=int, default=100, help="pressure workloads: FP32 iterations per refinement")
+    ap.add_argument("--ref-sweeps", type=int, default=1500, help="pressure workloads, reference arm: iterations the CPU time is scaled to")
+    a = ap.parse_args()
+    if a.workload.startswith("pressure_") and "--steps" not in sys.argv:
+        a.steps, a.warmup = 5, 3
+    return a
 
 
 # ---------------------------------------------------------------- workloads
@@ -253,9 +260,152 @@ def workload_meta(name):
     return m
 
 
+# ---------------------------------------------------------------- pressure solve precision study
+def pressure_scene(name):
+    from splashtank_b200 import scenes
+    n = int(name.rsplit("_", 1)[1])
+    ty, rhs = scenes.splash_blobs(n)
+    return n, ty, rhs
+
+
+def pressure_config(name, n, ty, nt, a):
+    return {"workload": name, "grid": [n] * 3, "tile": "8^3", "active_tiles": nt, "active_tile_frac": round(nt / (n // 8) ** 3, 4),
+            "fluid_cells": int((ty == 1).sum()), "tol": a.tol, "omega": a.omega, "inner_sweeps": a.inner,
+            "scene": "seeded Gaussian blobs above 0.5 (120 blobs, sigma 0.025-0.07 of the box), solid walls; rhs = divergence of a "
+                     "seeded uniform(-1,1) face field", "l2": "working set (FP32 p, rhs about 250 MB at 512^3) larger than L2: no flush",
+            "parallelism": "replicas"}
+
+
+def run_pressure(a):
+    """ms per pressure solve to rel residual tol: FP32 SOR inside FP64 refinement (the value), plain FP32 SOR and FP64 SOR
+    beside it, each solution's error against an FP64 SOR solve to 1e-11 (the FP64 operator and its CG solution are checked
+    against the oracle in the tests)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    from splashtank_b200.poisson import REFINE, SOR32, SOR64, PoissonSolver
+    n, ty, rhs = pressure_scene(a.workload)
+    s = PoissonSolver((n, n, n), device=local)
+    t0 = time.perf_counter()
+    s.set(ty, rhs)
+    nt, nf = s.stats()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ro = dict(tol=a.tol, omega=a.omega, inner_sweeps=a.inner, max_sweeps=200000)
+    for _ in range(a.warmup):
+        s.solve(REFINE, **ro)
+    clocks = Clocks(local)
+    barrier()
+    res = [s.solve(REFINE, **ro) for _ in range(a.steps)]
+    barrier()
+    clk = clocks.stop()
+    ms = sum(r["ms"] for r in res)
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per = ms / a.steps
+    r_ref = res[-1]
+    x_ref32 = s.read()
+    # plain FP32 SOR to the same tolerance (residual checked as often as the refinement checks it), then FP64 SOR
+    r32 = s.solve(SOR32, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000))
+    x32 = s.read()
+    r64 = s.solve(SOR64, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000))
+    x64 = s.read()
+    rgold = s.solve(SOR64, tol=1e-11, omega=a.omega, check_every=50, max_sweeps=400000)
+    gold = s.read()
+    gn, gmax = float(np.linalg.norm(gold)), float(np.abs(gold).max())
+
+    def err(x):
+        d = x - gold
+        return {"rel_l2": float(np.linalg.norm(d)) / gn, "max_abs_over_max": float(np.abs(d).max()) / gmax}
+    # roofline of the FP32 sweep kernel (one colour per launch): per launch every cell of the active tiles reads its 2-byte
+    # info word in its own colour half, and every fluid cell of the colour reads rhs and p, writes p, and one fluid cell
+    # of the other colour is read (4 B): cells/2 * 2 + fluid/2 * 16 bytes
+    it = 200
+    sms = s.sweeps32(a.omega, it)
+    per_launch = sms / (2 * it)
+    b = nt * 512 + nf * 8
+    peak, src = measured_peak()
+    achieved = b / (per_launch * 1e-3) / 1e9
+    rl = {"kernel": "k_ps_sor32", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+          "peak_source": src, "traffic": None, "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per_launch, 5)}
+    # end to end through the C ABI with host buffers: upload (types, rhs), solve, read back
+    e0 = time.perf_counter()
+    s.set(ty, rhs)
+    re = s.solve(REFINE, **ro)
+    s.read()
+    e_ms = (time.perf_counter() - e0) * 1e3
+    if rank == 0:
+        line = {"metric": "pressure ms/solve to 1e-6 rel residual (FP32 SOR in FP64 refinement)", "value": ms_per, "unit": "ms",
+                "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_per, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 sweeps, f64 residual/correction", "data": "synthetic (seeded)",
+                "config": pressure_config(a.workload, n, ty, nt, a), "gpu_launches": int(r_ref["sweeps"] * 2 + r_ref["refinements"] * 4 + 2),
+                "refine": {"ms": ms_per, "sweeps": r_ref["sweeps"], "refinements": r_ref["refinements"], "rel_residual": r_ref["rel_residual"],
+                           "error_vs_fp64": err(x_ref32)},
+                "fp32_sor": {"ms": r32["ms"], "sweeps": r32["sweeps"], "rel_residual": r32["rel_residual"], "converged": r32["converged"],
+                             "error_vs_fp64": err(x32)},
+                "fp64_sor": {"ms": r64["ms"], "sweeps": r64["sweeps"], "rel_residual": r64["rel_residual"], "converged": r64["converged"],
+                             "error_vs_fp64": err(x64)},
+                "fp64_reference": {"method": "FP64 SOR to 1e-11", "sweeps": rgold["sweeps"], "rel_residual": rgold["rel_residual"], "ms": rgold["ms"]},
+                "clocks": clk, "roofline": rl,
+                "e2e": {"value": e_ms, "unit": "ms", "h2d_bytes_per_step": int(ty.nbytes + rhs.nbytes), "d2h_bytes_per_step": int(gold.nbytes),
+                        "note": "wall clock of set (host builds the tile index) + solve + read through the C ABI"}}
+        if world == 1 and not a.no_cpu_baseline:
+            line["cpu_baseline"] = pressure_cpu(ty, rhs, n, a, r_ref["sweeps"])
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def pressure_cpu(ty, rhs, n, a, sweeps, budget_sweeps=6):
+    """The oracle's FP32 SOR sweeps (all host threads) on the same system, a few sweeps timed and scaled to the sweep
+    count the refined solve needs."""
+    from oracle.oracle import OraclePoisson
+    th = os.cpu_count() or 1
+    o = OraclePoisson((n, n, n), threads=th)
+    o.set(ty, rhs)
+    o.sweeps32(a.omega, 1)
+    t0 = time.perf_counter()
+    o.sweeps32(a.omega, budget_sweeps)
+    el = time.perf_counter() - t0
+    v = el * 1e3 / budget_sweeps * sweeps
+    return {"value": v, "unit": "ms", "cores": th, "kind": "port",
+            "sample": "%d FP32 SOR iterations of the oracle on the %d^3 system timed (%.1f s), scaled to the %d iterations of the "
+                      "refined solve" % (budget_sweeps, n, el, sweeps)}
+
+
+def run_pressure_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n, ty, rhs = pressure_scene(a.workload)
+    cb = pressure_cpu(ty, rhs, n, a, a.ref_sweeps)
+    line = {"metric": "pressure ms/solve to 1e-6 rel residual (FP32 SOR in FP64 refinement)", "value": cb["value"], "unit": "ms",
+            "impl": "reference", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["value"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": a.workload, "grid": [n] * 3, "tol": a.tol, "omega": a.omega},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- our arm
 def main():
     a = parse()
+    if a.workload.startswith("pressure_"):
+        return run_pressure_reference(a) if a.impl == "reference" else run_pressure(a)
     if a.impl == "reference":
         return run_reference(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -231,6 +231,47 @@ st_status st_pbf_step(st_pbf* s, double dt, const st_pbf_opts* o);
 st_status st_pbf_read(st_pbf* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
 void* st_pbf_stream(st_pbf* s);
 
+/* ---- the pressure projection's solve on its own: precision study ---- */
+
+/* The linear system of the reference's pressure solve (relax, src/flip/wgsl-solver.js:124-140): for a fluid cell,
+ * nns p - sum(fluid neighbours p) = rhs, with air neighbours at p = 0 and solid (walls, unless open) left out. */
+typedef struct st_poisson st_poisson;
+typedef struct st_poisson_desc {
+  uint32_t size;        /* sizeof(st_poisson_desc) */
+  uint32_t n[3];        /* cells per axis */
+  uint32_t open;        /* ST_OPEN_* bits: box faces that are air instead of wall */
+  int32_t device;
+} st_poisson_desc;
+enum { ST_SOLVE_SOR32 = 0, ST_SOLVE_REFINE = 1, ST_SOLVE_SOR64 = 2 };
+typedef struct st_poisson_opts {
+  uint32_t size;        /* sizeof(st_poisson_opts) */
+  int32_t mode;         /* ST_SOLVE_*: FP32 red-black SOR; FP32 SOR inside FP64 residual/correction refinement; FP64 SOR */
+  double tol;           /* stop at ||b - A x|| / ||b|| <= tol (measured in FP64) */
+  float omega;          /* SOR factor */
+  int32_t max_sweeps;   /* red + black iterations, all refinements together */
+  int32_t inner_sweeps; /* iterations per refinement (mode 1) */
+  int32_t check_every;  /* iterations between residual checks (modes 0 and 2) */
+} st_poisson_opts;
+typedef struct st_poisson_result {
+  double rel_residual;
+  int32_t sweeps;
+  int32_t refinements;
+  int32_t converged;
+  float ms;             /* device time of the solve */
+} st_poisson_result;
+st_status st_poisson_create(const st_poisson_desc* d, st_poisson** out);
+void st_poisson_destroy(st_poisson* s);
+/* dense cell types (0 air, 1 fluid, 2 solid) and right-hand side, n[0] x n[1] x n[2], x fastest */
+st_status st_poisson_set(st_poisson* s, const uint8_t* type, const double* rhs);
+/* solve from zero */
+st_status st_poisson_solve(st_poisson* s, const st_poisson_opts* o, st_poisson_result* res);
+/* iters FP32 red-black SOR iterations from zero on (float) rhs; the result is readable with st_poisson_read.
+ * ms (optional): device time of the sweeps alone. */
+st_status st_poisson_sweeps32(st_poisson* s, float omega, int32_t iters, float* ms);
+/* the current solution in FP64, dense, x fastest */
+st_status st_poisson_read(st_poisson* s, double* p);
+void* st_poisson_stream(st_poisson* s);
+
 /* ---- common ---- */
 uint32_t st_abi_version(void);
 /* Text of the last error on this thread (static storage). */

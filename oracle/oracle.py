@@ -7,6 +7,8 @@ import ctypes as C
 import os
 import subprocess
 
+import numpy as np
+
 from splashtank_b200 import abi
 from splashtank_b200.flip import FlipSim
 
@@ -15,7 +17,8 @@ _FUNCS = None
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", HERE, os.path.join(HERE, "liboracle_flip.so"), os.path.join(HERE, "liboracle_pbf.so")], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, os.path.join(HERE, "liboracle_flip.so"), os.path.join(HERE, "liboracle_pbf.so"),
+                    os.path.join(HERE, "liboracle_poisson.so")], check=True)
 
 
 def funcs():
@@ -84,3 +87,51 @@ class OraclePbfSim(PbfSim):
         n = self.f["fill_box"](self._h, x0, x1, y0, y1, z0, z1)
         self.n += n
         return n
+
+
+class OraclePoisson:
+    """FP32 SOR sweeps, FP64 residual norms (the kernels' summation order) and the all-FP64 CG reference solve."""
+
+    def __init__(self, n, open=0, threads=8):
+        lib = C.CDLL(os.path.join(HERE, "liboracle_poisson.so")) if os.path.exists(os.path.join(HERE, "liboracle_poisson.so")) else None
+        if lib is None:
+            build()
+            lib = C.CDLL(os.path.join(HERE, "liboracle_poisson.so"))
+        dp = C.POINTER(C.c_double)
+        lib.oracle_poisson_create.restype = C.c_void_p
+        lib.oracle_poisson_create.argtypes = [C.c_uint32] * 4 + [C.c_int]
+        lib.oracle_poisson_destroy.argtypes = [C.c_void_p]
+        lib.oracle_poisson_set.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), dp]
+        lib.oracle_poisson_sweeps32.argtypes = [C.c_void_p, C.c_float, C.c_int, dp]
+        lib.oracle_poisson_rel_residual.restype = C.c_double
+        lib.oracle_poisson_rel_residual.argtypes = [C.c_void_p, dp, dp, dp]
+        lib.oracle_poisson_cg.restype = C.c_int
+        lib.oracle_poisson_cg.argtypes = [C.c_void_p, C.c_double, C.c_int, dp]
+        self.lib = lib
+        self.n = tuple(int(x) for x in n)
+        self.h = lib.oracle_poisson_create(self.n[0], self.n[1], self.n[2], int(open), int(threads))
+
+    def set(self, cell_type, rhs):
+        self._t = np.ascontiguousarray(cell_type, np.uint8)
+        self._b = np.ascontiguousarray(rhs, np.float64)
+        self.lib.oracle_poisson_set(self.h, self._t.ctypes.data_as(C.POINTER(C.c_uint8)), self._b.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def sweeps32(self, omega, iters):
+        out = np.zeros(self.n[::-1], np.float64)
+        self.lib.oracle_poisson_sweeps32(self.h, float(omega), int(iters), out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def rel_residual(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        return self.lib.oracle_poisson_rel_residual(self.h, x.ctypes.data_as(C.POINTER(C.c_double)), None, None)
+
+    def cg(self, tol=1e-12, maxit=100000):
+        out = np.zeros(self.n[::-1], np.float64)
+        it = self.lib.oracle_poisson_cg(self.h, float(tol), int(maxit), out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out, it
+
+    def __del__(self):
+        try:
+            self.lib.oracle_poisson_destroy(self.h)
+        except Exception:
+            pass

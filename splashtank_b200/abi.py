@@ -78,6 +78,20 @@ class PbfOpts(C.Structure):
                 ("cols", C.POINTER(PbfCol))]
 
 
+class PoissonDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("n", C.c_uint32 * 3), ("open", C.c_uint32), ("device", C.c_int32)]
+
+
+class PoissonOpts(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("mode", C.c_int32), ("tol", C.c_double), ("omega", C.c_float), ("max_sweeps", C.c_int32),
+                ("inner_sweeps", C.c_int32), ("check_every", C.c_int32)]
+
+
+class PoissonResult(C.Structure):
+    _fields_ = [("rel_residual", C.c_double), ("sweeps", C.c_int32), ("refinements", C.c_int32), ("converged", C.c_int32),
+                ("ms", C.c_float)]
+
+
 # (name, restype, argtypes) with the prefix left off; "h" stands for the opaque handle
 FLIP_FUNCS = [
     ("flip_create", C.c_int, [C.POINTER(FlipDesc), C.POINTER(C.c_void_p)]),
@@ -103,6 +117,14 @@ CUDA_ONLY_FUNCS = [
     ("flip_read_timing", C.c_int, [C.c_void_p, C.POINTER(StageTimes), u32p]),
     ("abi_version", C.c_uint32, []),
     ("last_error", C.c_char_p, []),
+]
+POISSON_FUNCS = [
+    ("poisson_create", C.c_int, [C.POINTER(PoissonDesc), C.POINTER(C.c_void_p)]),
+    ("poisson_destroy", None, [C.c_void_p]),
+    ("poisson_set", C.c_int, [C.c_void_p, u8p, C.POINTER(C.c_double)]),
+    ("poisson_solve", C.c_int, [C.c_void_p, C.POINTER(PoissonOpts), C.POINTER(PoissonResult)]),
+    ("poisson_sweeps32", C.c_int, [C.c_void_p, C.c_float, C.c_int32, C.POINTER(C.c_float)]),
+    ("poisson_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
 ]
 PBF_FUNCS = [
     ("pbf_create", C.c_int, [C.POINTER(PbfDesc), C.POINTER(C.c_void_p)]),

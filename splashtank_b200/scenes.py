@@ -110,3 +110,38 @@ class WaveTank:
         sim.add_many(park)
         sim.nb_fills(boxes=[self.fill_box], mode=1)
         return sim
+
+
+def splash_blobs(n=512, seed=11, blobs=None, sigma=(0.025, 0.07), level=0.5):
+    """Pressure-solve workload: fluid where a sum of seeded Gaussian blobs exceeds level (splash-shaped, merged), inside
+    solid walls; rhs is the divergence of a seeded random face-velocity field on the fluid cells. Returns (type, rhs) as
+    (n, n, n) arrays indexed [k][j][i]: uint8 0 air / 1 fluid, float64. About 20% of the 8^3 tiles hold fluid."""
+    rng = np.random.default_rng(seed)
+    k_blobs = blobs if blobs is not None else 120
+    c = rng.uniform(0.12, 0.88, (k_blobs, 3))
+    s = rng.uniform(sigma[0], sigma[1], k_blobs)
+    f = np.zeros((n, n, n), np.float32)
+    h = 1.0 / n
+    for (cx, cy, cz), sg in zip(c, s):
+        r = 2.6 * sg
+        lo = [max(0, int((q - r) / h)) for q in (cx, cy, cz)]
+        hi = [min(n, int((q + r) / h) + 1) for q in (cx, cy, cz)]
+        xs = ((np.arange(lo[0], hi[0]) + 0.5) * h - cx).astype(np.float32)
+        ys = ((np.arange(lo[1], hi[1]) + 0.5) * h - cy).astype(np.float32)
+        zs = ((np.arange(lo[2], hi[2]) + 0.5) * h - cz).astype(np.float32)
+        inv = np.float32(-0.5 / (sg * sg))
+        g = np.exp(zs[:, None, None] ** 2 * inv) * np.exp(ys[None, :, None] ** 2 * inv) * np.exp(xs[None, None, :] ** 2 * inv)
+        f[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += g
+    cell_type = (f > level).astype(np.uint8)
+    del f
+    rhs = np.zeros((n, n, n), np.float64)
+    slab = 32
+    for z0 in range(0, n, slab):
+        z1 = min(n, z0 + slab)
+        r2 = np.random.default_rng([seed, z0])
+        u = r2.uniform(-1, 1, (z1 - z0, n, n + 1))
+        v = r2.uniform(-1, 1, (z1 - z0, n + 1, n))
+        w = r2.uniform(-1, 1, (z1 - z0 + 1, n, n))
+        rhs[z0:z1] = (u[:, :, 1:] - u[:, :, :-1]) + (v[:, 1:, :] - v[:, :-1, :]) + (w[1:] - w[:-1])
+    rhs[cell_type != 1] = 0.0
+    return cell_type, rhs
