@@ -38,6 +38,8 @@ cudaError_t dalloc(T** p, size_t count) {
 
 }  // namespace
 
+void st::set_error_text(const char* text) { snprintf(g_err, sizeof(g_err), "%s", text); }
+
 struct st_flip {
   int device = 0;
   cudaStream_t stream = nullptr;

@@ -16,6 +16,9 @@
 
 namespace st {
 
+// the text st_last_error() returns on this thread (capi.cu)
+void set_error_text(const char* text);
+
 constexpr float DEADY = -1.0e5f;
 constexpr uint32_t DEADKEY = 0xffffffffu;
 constexpr float WWHOLD = 0.2f;

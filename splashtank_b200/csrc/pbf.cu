@@ -328,7 +328,7 @@ struct st_pbf {
   do {                                                                                        \
     cudaError_t e_ = (call);                                                                  \
     if (e_ != cudaSuccess) {                                                                  \
-      snprintf(g_perr, sizeof(g_perr), "%s: %s", #call, cudaGetErrorString(e_));              \
+      snprintf(g_perr, sizeof(g_perr), "%s: %s", #call, cudaGetErrorString(e_)); st::set_error_text(g_perr);              \
       return e_ == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR;                      \
     }                                                                                         \
   } while (0)
@@ -394,7 +394,7 @@ st_status st_pbf_create(const st_pbf_desc* ds, st_pbf** out) {
   if (e == cudaSuccess) e = cudaMemsetAsync(s->BG, 0, M * 12, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
-    snprintf(g_perr, sizeof(g_perr), "create: %s", cudaGetErrorString(e));
+    snprintf(g_perr, sizeof(g_perr), "create: %s", cudaGetErrorString(e)); st::set_error_text(g_perr);
     st_pbf_destroy(s);
     return e == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR;
   }

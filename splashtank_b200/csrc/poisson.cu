@@ -180,7 +180,7 @@ struct st_poisson {
   do {                                                                                      \
     cudaError_t e_ = (call);                                                                \
     if (e_ != cudaSuccess) {                                                                \
-      snprintf(g_serr, sizeof(g_serr), "%s: %s", #call, cudaGetErrorString(e_));            \
+      snprintf(g_serr, sizeof(g_serr), "%s: %s", #call, cudaGetErrorString(e_)); st::set_error_text(g_serr);            \
       return e_ == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR;                    \
     }                                                                                       \
   } while (0)
@@ -221,7 +221,7 @@ st_status st_poisson_create(const st_poisson_desc* d, st_poisson** out) {
   if (e == cudaSuccess) e = cudaMemsetAsync(s->x64, 0, s->ncell * 8, s->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
-    snprintf(g_serr, sizeof(g_serr), "create: %s", cudaGetErrorString(e));
+    snprintf(g_serr, sizeof(g_serr), "create: %s", cudaGetErrorString(e)); st::set_error_text(g_serr);
     st_poisson_destroy(s);
     return e == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR;
   }

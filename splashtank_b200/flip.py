@@ -41,6 +41,15 @@ class StError(RuntimeError):
     pass
 
 
+def status_error(what, st):
+    """StError for a failed call: the status name and the library's last error text on this thread."""
+    e = load_library()[1].get("last_error")
+    t = e() if e else None
+    msg = t.decode() if t else ""
+    name = abi.STATUS_NAMES[st] if 0 <= st < len(abi.STATUS_NAMES) else str(st)
+    return StError(("%s failed: %s %s" % (what, name, msg)).rstrip())
+
+
 def _f32(a, n=None):
     a = np.ascontiguousarray(a, dtype=np.float32)
     return a, a.ctypes.data_as(abi.f32p)

@@ -9,7 +9,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from .flip import StError, load_library
+from .flip import load_library, status_error
 
 _PBF = None
 
@@ -47,7 +47,7 @@ class PbfSim:
         h = C.c_void_p()
         st = self.f["pbf_create"](C.byref(desc), C.byref(h))
         if st != abi.ST_OK:
-            raise StError("pbf create failed: %s" % abi.STATUS_NAMES[st])
+            raise status_error("pbf create", st)
         self._h = h
         self.d = float(d)
         self.h = 2.2 * self.d
@@ -66,7 +66,7 @@ class PbfSim:
         got = C.c_uint32()
         st = self.f["pbf_add"](self._h, p.ctypes.data_as(abi.f32p), None if v is None else v.ctypes.data_as(abi.f32p), len(p), C.byref(got))
         if st != abi.ST_OK:
-            raise StError("pbf add failed: %s" % abi.STATUS_NAMES[st])
+            raise status_error("pbf add", st)
         self.n += got.value
         return got.value
 
@@ -96,7 +96,7 @@ class PbfSim:
         op.cols = C.cast(arr, C.POINTER(abi.PbfCol))
         st = self.f["pbf_step"](self._h, float(dt), C.byref(op))
         if st not in (abi.ST_OK, abi.ST_NOT_READY):
-            raise StError("pbf step failed: %s" % abi.STATUS_NAMES[st])
+            raise status_error("pbf step", st)
 
     def particles(self):
         p = np.zeros((max(self.n, 1), 4), np.float32)
@@ -104,7 +104,7 @@ class PbfSim:
         got = C.c_uint32()
         st = self.f["pbf_read"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.n, C.byref(got))
         if st != abi.ST_OK:
-            raise StError("pbf read failed: %s" % abi.STATUS_NAMES[st])
+            raise status_error("pbf read", st)
         return p[: got.value], v[: got.value]
 
     def readbackInto(self, dst):

@@ -5,7 +5,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi
-from .flip import StError, load_library
+from .flip import load_library, status_error
 
 SOR32, REFINE, SOR64 = 0, 1, 2
 _F = None
@@ -33,7 +33,7 @@ class PoissonSolver:
 
     def _check(self, st, what):
         if st != abi.ST_OK:
-            raise StError("poisson %s failed: %s" % (what, abi.STATUS_NAMES[st]))
+            raise status_error("poisson " + what, st)
 
     def set(self, cell_type, rhs):
         """cell_type: uint8 (nz, ny, nx) 0 air / 1 fluid / 2 solid; rhs: float64 same shape."""
