@@ -272,6 +272,37 @@ st_status st_poisson_sweeps32(st_poisson* s, float omega, int32_t iters, float* 
 st_status st_poisson_read(st_poisson* s, double* p);
 void* st_poisson_stream(st_poisson* s);
 
+/* ---- pressure residual that allocates nothing (no reference counterpart: the reference measures no residual) ----
+ * ||b - A x|| / ||b|| of the pressure system above, in FP64, on arrays the caller owns on the device, in the tile-major
+ * layout (tile t = ti + tx (tj + ty tk) with tx = ceil(n[0]/8) ..., cell t*512 + lx + 8 (ly + 8 lz)). For callers that
+ * cannot allocate device memory at the call: a process whose free device memory is held by another allocator (a
+ * caching allocator such as PyTorch's reserves it, so a cudaMalloc here can fail although the caller has room), or a
+ * stepping loop that must not take the device-wide synchronisation that cudaMalloc/cudaFree can imply.
+ * It calls no cudaMalloc/cudaFree and no allocating library routine. Its scratch is a fixed device array inside the
+ * library, one per device: 2 x ST_NOALLOC_MAX_TILES + 4 doubles (1 MiB), holding per-tile partial sums.
+ *  - n_tiles above ST_NOALLOC_MAX_TILES is rejected with ST_BAD_ARG and a message in st_last_error().
+ *  - The first call on each device, made with that device current, looks up the scratch address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture on the device.
+ *  - The scratch's error word must start at zero: each call clears it on `stream` before its kernels. The partial sums
+ *    need no clearing; each call writes every one it reads.
+ *  - Calls on one device share the scratch: calls that overlap in time (on other streams or host threads) race and
+ *    return wrong numbers. Serialise them.
+ * Runs on the current device, on `stream` (NULL: the default stream), and waits for that stream before returning. A
+ * tile index outside the box returns ST_BAD_ARG (nothing outside the arrays is read). */
+#define ST_NOALLOC_MAX_TILES 65536u
+typedef struct st_poisson_system {
+  uint32_t size;         /* sizeof(st_poisson_system) */
+  uint32_t n[3];         /* cells per axis */
+  uint32_t n_tiles;      /* tiles holding fluid (at most ST_NOALLOC_MAX_TILES) */
+  const uint32_t* tiles; /* device: the n_tiles tiles holding fluid, ascending */
+  const uint16_t* info;  /* device, tx*ty*tz*512 words: 0x8000 fluid | non-solid neighbours << 8 | fluid-neighbour bits
+                            (-x, +x, -y, +y, -z, +z), 0 for other cells */
+  const double* b;       /* device, tx*ty*tz*512: right-hand side on fluid cells */
+} st_poisson_system;
+/* x: device, tx*ty*tz*512 FP64 values. rel = ||r|| / ||b|| (0 when b = 0); r2, b2 (optional) = ||r||^2, ||b||^2. */
+st_status st_poisson_residual_noalloc(const st_poisson_system* sys, const double* x, void* stream, double* rel, double* r2,
+                                      double* b2);
+
 /* ---- common ---- */
 uint32_t st_abi_version(void);
 /* Text of the last error on this thread (static storage). */

@@ -92,6 +92,13 @@ class PoissonResult(C.Structure):
                 ("ms", C.c_float)]
 
 
+class PoissonSystem(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("n", C.c_uint32 * 3), ("n_tiles", C.c_uint32), ("tiles", C.c_void_p), ("info", C.c_void_p),
+                ("b", C.c_void_p)]
+
+
+NOALLOC_MAX_TILES = 65536
+
 # (name, restype, argtypes) with the prefix left off; "h" stands for the opaque handle
 FLIP_FUNCS = [
     ("flip_create", C.c_int, [C.POINTER(FlipDesc), C.POINTER(C.c_void_p)]),
@@ -125,6 +132,10 @@ POISSON_FUNCS = [
     ("poisson_solve", C.c_int, [C.c_void_p, C.POINTER(PoissonOpts), C.POINTER(PoissonResult)]),
     ("poisson_sweeps32", C.c_int, [C.c_void_p, C.c_float, C.c_int32, C.POINTER(C.c_float)]),
     ("poisson_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+]
+NOALLOC_FUNCS = [
+    ("poisson_residual_noalloc", C.c_int, [C.POINTER(PoissonSystem), C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 ]
 PBF_FUNCS = [
     ("pbf_create", C.c_int, [C.POINTER(PbfDesc), C.POINTER(C.c_void_p)]),

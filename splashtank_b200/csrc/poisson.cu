@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/splashtank_cuda.h"
@@ -413,3 +414,143 @@ st_status st_poisson_read(st_poisson* s, double* p) {
 void* st_poisson_stream(st_poisson* s) { return s ? (void*)s->stream : nullptr; }
 
 }  // extern "C"
+
+// ---- residual norm without allocation (st_poisson_residual_noalloc) ----
+// Its scratch is this fixed array: per-tile partial sums of r^2 and b^2, the two totals and an error word. One copy
+// per device; the host looks its address up once per device.
+namespace {
+
+constexpr uint32_t kNoAllocTiles = ST_NOALLOC_MAX_TILES;
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocTiles + 4];
+
+// r = b - A x in FP64 summed per tile (the same arithmetic and tree as k_ps_resid), without storing r; a tile index
+// outside the box sets the error word and its partials to zero instead of reading
+__global__ void __launch_bounds__(512) k_ps_resid_norm(PGeo G, const uint32_t* __restrict__ tiles, uint32_t nT, uint32_t nTiles,
+                                                       const uint16_t* __restrict__ info, const double* __restrict__ x,
+                                                       const double* __restrict__ b, double* __restrict__ tileR2,
+                                                       double* __restrict__ tileB2, unsigned long long* __restrict__ bad) {
+  __shared__ double sr[512], sb[512];
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t t = tiles[a];
+    double rv = 0.0, bv = 0.0;
+    if (t < nTiles) {
+      const uint32_t c = t * 512u + threadIdx.x;
+      uint32_t nb[6];
+      neighbours(G, t, threadIdx.x, nb);
+      const uint32_t in = info[c];
+      if (in & 0x8000u) {
+        const uint32_t nns = (in >> 8) & 7u;
+        double s = 0.0;
+        for (int q = 0; q < 6; q++) if (in & (1u << q)) s += x[nb[q]];
+        bv = b[c];
+        rv = bv - ((double)nns * x[c] - s);
+      }
+    } else if (threadIdx.x == 0) {
+      atomicExch(bad, 1ull);
+    }
+    sr[threadIdx.x] = rv * rv;
+    sb[threadIdx.x] = bv * bv;
+    __syncthreads();
+    for (int w = 256; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) { sr[threadIdx.x] += sr[threadIdx.x + w]; sb[threadIdx.x] += sb[threadIdx.x + w]; }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) { tileR2[a] = sr[0]; tileB2[a] = sb[0]; }
+    __syncthreads();
+  }
+}
+
+struct NoAllocDev {
+  double* scratch = nullptr;
+  int sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDev g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+void noalloc_err(const char* text) { st::set_error_text(text); }
+
+}  // namespace
+
+extern "C" st_status st_poisson_residual_noalloc(const st_poisson_system* sys, const double* x, void* stream, double* rel,
+                                                double* r2, double* b2) {
+  char msg[256];
+  if (!sys || !rel || sys->size != sizeof(st_poisson_system) || !sys->n[0] || !sys->n[1] || !sys->n[2]) {
+    noalloc_err("st_poisson_residual_noalloc: null argument, wrong st_poisson_system.size or an empty box");
+    return ST_BAD_ARG;
+  }
+  const uint64_t tx = (sys->n[0] + 7) / 8, ty = (sys->n[1] + 7) / 8, tz = (sys->n[2] + 7) / 8, nTiles = tx * ty * tz;
+  if (nTiles * 512u > 0xffffffffull) {
+    noalloc_err("st_poisson_residual_noalloc: box too large for 32-bit cell indices");
+    return ST_BAD_ARG;
+  }
+  if (sys->n_tiles > kNoAllocTiles) {
+    snprintf(msg, sizeof(msg), "st_poisson_residual_noalloc: n_tiles %u exceeds the fixed scratch of %u tiles", sys->n_tiles, kNoAllocTiles);
+    noalloc_err(msg);
+    return ST_BAD_ARG;
+  }
+  if (sys->n_tiles && (!sys->tiles || !sys->info || !sys->b || !x)) {
+    noalloc_err("st_poisson_residual_noalloc: null device array");
+    return ST_BAD_ARG;
+  }
+  *rel = 0.0;
+  if (r2) *r2 = 0.0;
+  if (b2) *b2 = 0.0;
+  if (!sys->n_tiles) return ST_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    snprintf(msg, sizeof(msg), "st_poisson_residual_noalloc: current device %d: %s", dev, cudaGetErrorString(e));
+    noalloc_err(msg);
+    return ST_DEVICE_ERROR;
+  }
+  NoAllocDev d;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_dev[dev].scratch) {   // first call on this device: look the scratch up with the device current
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      int sms = 0;
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) {
+        snprintf(msg, sizeof(msg), "st_poisson_residual_noalloc: scratch lookup on device %d: %s", dev, cudaGetErrorString(e));
+        noalloc_err(msg);
+        return ST_DEVICE_ERROR;
+      }
+      g_noalloc_dev[dev].scratch = (double*)p;
+      g_noalloc_dev[dev].sms = sms;
+    }
+    d = g_noalloc_dev[dev];
+  }
+  double* tileR2 = d.scratch;
+  double* tileB2 = d.scratch + kNoAllocTiles;
+  double* tot = d.scratch + 2 * kNoAllocTiles;                                      // [0] r^2, [1] b^2
+  unsigned long long* bad = (unsigned long long*)(d.scratch + 2 * kNoAllocTiles + 2);  // must start at zero
+  cudaStream_t q = (cudaStream_t)stream;
+  const PGeo G{sys->n[0], sys->n[1], sys->n[2], (uint32_t)tx, (uint32_t)ty, (uint32_t)tz};
+  const int grid = std::max(1, std::min<int>(d.sms * 4, (int)sys->n_tiles));
+  double h[3] = {0.0, 0.0, 0.0};
+  e = cudaMemsetAsync(bad, 0, sizeof(unsigned long long), q);
+  if (e == cudaSuccess) {
+    k_ps_resid_norm<<<grid, 512, 0, q>>>(G, sys->tiles, sys->n_tiles, (uint32_t)nTiles, sys->info, x, sys->b, tileR2, tileB2, bad);
+    k_ps_norms<<<1, 1024, 0, q>>>(tileR2, tileB2, sys->n_tiles, tot);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, tot, 3 * sizeof(double), cudaMemcpyDeviceToHost, q);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(q);
+  if (e != cudaSuccess) {
+    snprintf(msg, sizeof(msg), "st_poisson_residual_noalloc: %s", cudaGetErrorString(e));
+    noalloc_err(msg);
+    return ST_DEVICE_ERROR;
+  }
+  unsigned long long badv = 0;
+  memcpy(&badv, &h[2], sizeof(badv));
+  if (badv) {
+    noalloc_err("st_poisson_residual_noalloc: a tile index is outside the box");
+    return ST_BAD_ARG;
+  }
+  *rel = h[1] > 0.0 ? std::sqrt(h[0]) / std::sqrt(h[1]) : 0.0;
+  if (r2) *r2 = h[0];
+  if (b2) *b2 = h[1];
+  return ST_OK;
+}

@@ -9,6 +9,7 @@ from .flip import load_library, status_error
 
 SOR32, REFINE, SOR64 = 0, 1, 2
 _F = None
+_NA = None
 
 
 def funcs():
@@ -78,3 +79,69 @@ class PoissonSolver:
             self.destroy()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- the system in the tile-major layout, on the host
+def _tile_index(n):
+    """Tile-major index of every cell of a dense (nz, ny, nx) box: t * 512 + lx + 8 (ly + 8 lz)."""
+    nx, ny, nz = n
+    tx, ty = (nx + 7) // 8, (ny + 7) // 8
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    t = (i >> 3) + tx * ((j >> 3) + ty * (k >> 3))
+    return (t * 512 + (i & 7) + 8 * ((j & 7) + 8 * (k & 7))).astype(np.int64)
+
+
+def n_cells(n):
+    return ((n[0] + 7) // 8) * ((n[1] + 7) // 8) * ((n[2] + 7) // 8) * 512
+
+
+def to_tile_major(dense):
+    """A dense (nz, ny, nx) field in the tile-major layout (zeros in the cells past the box)."""
+    n = dense.shape[::-1]
+    out = np.zeros(n_cells(n), dense.dtype)
+    out[_tile_index(n).ravel()] = dense.ravel()
+    return out
+
+
+def tile_system(cell_type, rhs, open=0):
+    """(tiles, info, b) of st_poisson_system built on the host, as st_poisson_set builds them: tiles holding fluid
+    ascending; info = 0x8000 | non-solid neighbours << 8 | fluid-neighbour bits (-x, +x, -y, +y, -z, +z), the box's
+    outside solid unless its face is open (ST_OPEN_* bits); b = rhs on fluid cells."""
+    t = np.ascontiguousarray(cell_type, np.uint8)
+    nz, ny, nx = t.shape
+    fluid = t == 1
+    pad = np.full((nz + 2, ny + 2, nx + 2), 2, np.uint8)
+    pad[1:-1, 1:-1, 1:-1] = t
+    for bit, sl in ((1, np.s_[1:-1, 1:-1, 0]), (2, np.s_[1:-1, 1:-1, -1]), (4, np.s_[1:-1, 0, 1:-1]), (8, np.s_[1:-1, -1, 1:-1]),
+                    (16, np.s_[0, 1:-1, 1:-1]), (32, np.s_[-1, 1:-1, 1:-1])):
+        if open & bit:
+            pad[sl] = 0
+    nbs = [pad[1:-1, 1:-1, :-2], pad[1:-1, 1:-1, 2:], pad[1:-1, :-2, 1:-1], pad[1:-1, 2:, 1:-1], pad[:-2, 1:-1, 1:-1], pad[2:, 1:-1, 1:-1]]
+    mask = np.zeros(t.shape, np.uint16)
+    nns = np.zeros(t.shape, np.uint16)
+    for a, q in enumerate(nbs):
+        mask |= (q == 1).astype(np.uint16) << a
+        nns += (q != 2).astype(np.uint16)
+    info = np.where(fluid, 0x8000 | (nns << 8) | mask, 0).astype(np.uint16)
+    b = np.where(fluid, np.asarray(rhs, np.float64), 0.0)
+    idx = _tile_index((nx, ny, nz))
+    tiles = np.unique(idx[fluid] >> 9).astype(np.uint32)
+    return tiles, to_tile_major(info), to_tile_major(b)
+
+
+def residual_noalloc(n, tiles, info, b, x, stream=0):
+    """st_poisson_residual_noalloc on device arrays (anything with data_ptr(), e.g. torch CUDA tensors: tiles uint32
+    (int32 storage), info uint16 (int16 storage), b and x float64 in the tile-major layout). Returns (rel, r2, b2)."""
+    global _NA
+    if _NA is None:
+        _NA = abi.bind(load_library()[0], "st_", abi.NOALLOC_FUNCS)
+    s = abi.PoissonSystem()
+    s.size = C.sizeof(abi.PoissonSystem)
+    s.n[:] = [int(v) for v in n]
+    s.n_tiles = int(tiles.numel())
+    s.tiles, s.info, s.b = tiles.data_ptr(), info.data_ptr(), b.data_ptr()
+    rel, r2, b2 = C.c_double(), C.c_double(), C.c_double()
+    st = _NA["poisson_residual_noalloc"](C.byref(s), C.c_void_p(x.data_ptr()), C.c_void_p(int(stream)), C.byref(rel), C.byref(r2), C.byref(b2))
+    if st != abi.ST_OK:
+        raise status_error("poisson residual_noalloc", st)
+    return rel.value, r2.value, b2.value
