@@ -264,7 +264,9 @@ __device__ __forceinline__ float wetCellAt(const FlipParams& P, const float* __r
   if (!inDom(P, i, j, k)) return 0.0f;
   return wet[cellIdx(P, i, j, k)];
 }
-__device__ __forceinline__ void emitTerms(const FlipParams& P, const float* __restrict__ wet, float4 qp, float4 qv, float& rho, float& fast, float& e) {
+// wetAt(i, j, k) gives wetCellAt for the eight cells around the particle (from HBM, or a staged window)
+template <class WetAt>
+__device__ __forceinline__ void emitTermsT(const FlipParams& P, const WetAt& wetAt, float4 qp, float4 qv, float& rho, float& fast, float& e) {
   const V3 p = xyz(qp), v = xyz(qv);
   const float foam = qv.w, spd = len3(v);
   fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
@@ -273,11 +275,19 @@ __device__ __forceinline__ void emitTerms(const FlipParams& P, const float* __re
   rho = 0.0f;
   for (int dz = 0; dz <= 1; dz++)
     for (int dy = 0; dy <= 1; dy++)
-      for (int dx = 0; dx <= 1; dx++) rho += wetCellAt(P, wet, bi + dx, bj + dy, bk + dz);
+      for (int dx = 0; dx <= 1; dx++) rho += wetAt(bi + dx, bj + dy, bk + dz);
   rho = rho / 8.0f;
   const float crest = (1.0f - smoothstepf(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
   const float churn = (1.0f - smoothstepf(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstepf(0.5f, 1.5f, spd * P.vs);
   e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstepf(0.1f, 0.5f, P.q8);
+}
+struct WetGlobal {
+  const FlipParams& P;
+  const float* __restrict__ wet;
+  __device__ __forceinline__ float operator()(int i, int j, int k) const { return wetCellAt(P, wet, i, j, k); }
+};
+__device__ __forceinline__ void emitTerms(const FlipParams& P, const float* __restrict__ wet, float4 qp, float4 qv, float& rho, float& fast, float& e) {
+  emitTermsT(P, WetGlobal{P, wet}, qp, qv, rho, fast, e);
 }
 
 // ---- block-wide scans (blockDim.x a multiple of 32, at most 1024) ----

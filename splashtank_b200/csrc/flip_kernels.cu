@@ -39,15 +39,14 @@ __global__ void __launch_bounds__(PBLK) k_count_mark(Bufs B) {
   uint32_t key = DEADKEY;
   bool live = false, dead = false;
   float sp = 0.0f;
+  int ci = 0, cj = 0, ck = 0;
   if (i < P.n) {
     Part q = B.pb[i];
     if (q.p.y < DEADY) dead = true;
     else {
       live = true;
-      int ci, cj, ck;
       particleCell(P, xyz(q.p), ci, cj, ck);
       key = cellIdx(P, ci, cj, ck);
-      markAround(P, B.need, ci, cj, ck);
       sp = len3(xyz(q.v));
     }
     B.key[i] = key;
@@ -55,6 +54,8 @@ __global__ void __launch_bounds__(PBLK) k_count_mark(Bufs B) {
   uint32_t peers = __match_any_sync(0xffffffffu, key);
   int leader = __ffs(peers) - 1;
   uint32_t base = 0;
+  // lanes in one cell mark the same tiles: the group's first lane marks for all of them
+  if (live && lane == leader) markAround(P, B.need, ci, cj, ck);
   if (live && lane == leader) base = (uint32_t)atomicAdd(&B.cnt[key], __popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (live) B.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
@@ -418,6 +419,8 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
 // neighbours are fluid and how many are not solid. All eight loads of a cell are issued together from addresses that
 // are always valid (a missing neighbour reads the cell itself); the sum then adds only the fluid neighbours, in the
 // reference's order, so the arithmetic is unchanged.
+// One colour over the fluid tiles a = first, first + stride, ...; pressures are read at L2 (__ldcg) so that the
+// persistent launch below sees other CTAs' writes after its grid barrier.
 __global__ void __launch_bounds__(256) k_sor(Bufs B, uint32_t color) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
@@ -507,6 +510,57 @@ __device__ __forceinline__ void sampleBoth(const FlipParams& P, const Bufs& B, V
   vn = v3(rn[0], rn[1], rn[2]);
   vo = v3(ro[0], ro[1], ro[2]);
 }
+// Cheap tests that only skip colliders colNear (src/flip/wgsl-core.js:113-126) rejects, so collideP's result is
+// unchanged. s: a world-space sphere around the near box (xyz centre, w radius^2; w = +inf when the rows are not a
+// rotation): in exact arithmetic colNear(p) puts the local point inside the box centre cL +- half extents h, so
+// |p - (pos + R^T cL)| < |h|. lo/hi: the near box in local coordinates, before colNear's division by the voxel size.
+// Both carry slack (1% and one voxel) that covers rounding. on = 0 when colNear always holds.
+struct ColPre {
+  float4 s, r0, r1, r2, pos, lo, hi;
+  int on;
+};
+__device__ ColPre colPre(const FlipParams& P, const float4* __restrict__ cols, uint32_t k) {
+  ColPre X;
+  const float4 a = cols[k * 8], b = cols[k * 8 + 1];
+  X.r0 = cols[k * 8 + 2]; X.r1 = cols[k * 8 + 3]; X.r2 = cols[k * 8 + 4]; X.pos = cols[k * 8 + 5];
+  const V3 r0 = xyz(X.r0), r1 = xyz(X.r1), r2 = xyz(X.r2), pos = xyz(X.pos);
+  const float tol = 1.0e-4f, hw = b.w, m = fabsf(P.q0);
+  X.on = (P.q10 > 0.5f || !(hw > 0.0f)) ? 0 : 1;
+  const bool rot = fabsf(dot3(r0, r0) - 1.0f) < tol && fabsf(dot3(r1, r1) - 1.0f) < tol && fabsf(dot3(r2, r2) - 1.0f) < tol &&
+                   fabsf(dot3(r0, r1)) < tol && fabsf(dot3(r0, r2)) < tol && fabsf(dot3(r1, r2)) < tol;
+  const float sl = 0.01f * hw + hw;
+  X.lo = make_float4(b.x - hw - m - sl, b.y - hw - m - sl, b.z - hw - m - sl, 0.0f);
+  X.hi = make_float4(b.x + a.y * hw + m + sl, b.y + a.z * hw + m + sl, b.z + a.w * hw + m + sl, 0.0f);
+  const V3 cL = v3(b.x + (a.y - 1.0f) * 0.5f * hw, b.y + (a.z - 1.0f) * 0.5f * hw, b.z + (a.w - 1.0f) * 0.5f * hw);
+  const V3 h = v3((a.y + 1.0f) * 0.5f * hw + m, (a.z + 1.0f) * 0.5f * hw + m, (a.w + 1.0f) * 0.5f * hw + m);
+  const V3 c = pos + r0 * cL.x + r1 * cL.y + r2 * cL.z;
+  const float rad = len3(h) * 1.01f + hw;
+  X.s = (X.on && rot) ? make_float4(c.x, c.y, c.z, rad * rad) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0x7f800000));
+  return X;
+}
+// collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first
+__device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, const ColPre* pre, V3 pin) {
+  V3 p = pin;
+  const float m = P.margin;
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    const ColPre& X = pre[k];
+    const V3 d0 = p - xyz(X.s);
+    if (dot3(d0, d0) > X.s.w) continue;
+    if (X.on) {
+      const V3 d = p - xyz(X.pos);
+      const V3 lp = v3(dot3(xyz(X.r0), d), dot3(xyz(X.r1), d), dot3(xyz(X.r2), d));
+      if (lp.x < X.lo.x || lp.y < X.lo.y || lp.z < X.lo.z || lp.x > X.hi.x || lp.y > X.hi.y || lp.z > X.hi.z) continue;
+    }
+    if (!colNear(P, B.cols, k, p)) continue;
+    float phi; V3 wn;
+    sdfEval(B.cols, B.sdf, k, p, phi, wn);
+    if (phi < P.q0) p = p + wn * (P.q0 - phi);
+  }
+  const float big = 1.0e9f;
+  const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
+  const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
+  return vclamp(p, lo, hi);
+}
 __device__ __forceinline__ V3 collideP(const FlipParams& P, const Bufs& B, V3 pin) {
   V3 p = pin;
   const float m = P.margin;
@@ -540,8 +594,18 @@ struct G2PWin {
   const float* vn;   // [3][1000]
   const float* vo;
   const int32_t* cnt;
+  const float* wet;      // wetCellAt of each window cell (0 outside the domain)
+  const uint8_t* kill;   // the narrow band's trim test of each window cell
+  const ColPre* cpre;    // collider pre-tests (colPre)
   int ox, oy, oz;
   __device__ __forceinline__ int idx(int i, int j, int k) const { return (i - ox + 1) + 10 * ((j - oy + 1) + 10 * (k - oz + 1)); }
+  __device__ __forceinline__ bool has(int i, int j, int k) const {
+    return (unsigned)(i - ox + 1) < 10u && (unsigned)(j - oy + 1) < 10u && (unsigned)(k - oz + 1) < 10u;
+  }
+};
+struct WetWin {
+  const G2PWin& W;
+  __device__ __forceinline__ float operator()(int i, int j, int k) const { return W.wet[W.idx(i, j, k)]; }
 };
 __device__ __forceinline__ void sampleWin(const FlipParams& P, const G2PWin& W, V3 p, V3& vn, V3& vo) {
   float rn[3], ro[3];
@@ -669,7 +733,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const float sp = len3(v);
   if (sp > P.vmax) v = v * (P.vmax / sp);
   const V3 pt = p + v * P.dt;
-  const V3 pc = collideP(P, B, pt);
+  const V3 pc = collidePB(P, B, W.cpre, pt);
   const V3 dsp = pc - pt;
   if (dot3(dsp, dsp) > 1.0e-12f) {
     const V3 nrm = dsp / len3(dsp);
@@ -693,21 +757,32 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float wvn[3 * 1000], wvo[3 * 1000];
   __shared__ int32_t wcnt[1000];
+  __shared__ float wwet[1000];
+  __shared__ uint8_t wkill[1000];
+  __shared__ ColPre cpre[32];
   __shared__ GustTab gtab;
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
-  buildGust(P, gtab);
+  if (threadIdx.x < P.ncols) cpre[threadIdx.x] = colPre(P, B.cols, threadIdx.x);
+  buildGust(P, gtab);   // its barriers also publish cpre
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wvn, wvo, wcnt, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wvn, wvo, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
       const int gi = W.ox + r % 10 - 1, gj = W.oy + (r / 10) % 10 - 1, gk = W.oz + r / 100 - 1;
-      if (gi < 0 || gj < 0 || gk < 0 || gi >= NX || gj >= NY || gk >= NZ) continue;   // never sampled: clamping keeps indices >= 0
+      if (gi < 0 || gj < 0 || gk < 0 || gi >= NX || gj >= NY || gk >= NZ) {   // faces here are never sampled (clamped)
+        wwet[r] = 0.0f;
+        wkill[r] = 0;
+        continue;
+      }
       const uint32_t c = cellIdx(P, gi, gj, gk);
       for (int ax = 0; ax < 3; ax++) { wvn[ax * 1000 + r] = B.vn[ax * nc + c]; wvo[ax * 1000 + r] = B.vo[ax * nc + c]; }
       wcnt[r] = B.cnt[c];
+      if (needWet) wwet[r] = inDom(P, gi, gj, gk) ? B.wet[c] : 0.0f;
+      if (needKill) wkill[r] = (B.on[c >> 9] && phiOfBits(B.ctype[c]) < -P.band) ? 1 : 0;
     }
     __syncthreads();
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
@@ -719,9 +794,13 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
       const bool gone = q.p.y < DEADY;
       uint32_t kc = 0;
-      if (!gone && P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f) {
+      if (!gone && needWet) {
         float rho, fast, e;
-        emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
+        // the eight cells around the moved particle: from the window when it holds them
+        const V3 bcf = vfloor((xyz(q.p) - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
+        const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+        if (W.has(bi, bj, bk) && W.has(bi + 1, bj + 1, bk + 1)) emitTermsT(P, WetWin{W}, q.p, q.v, rho, fast, e);
+        else emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
         if (e > 0.0f) {
           const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
           kc = min(u32f(floorf(P.sprRate * e * P.dt + hash1(h0))), 4u);
@@ -731,8 +810,11 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
       if (!gone && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
         int ci, cj, ck;
         particleCell(P, xyz(q.p), ci, cj, ck);
-        const uint32_t cc = cellIdx(P, ci, cj, ck);
-        kill = B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band;
+        if (W.has(ci, cj, ck)) kill = W.kill[W.idx(ci, cj, ck)] != 0;
+        else {
+          const uint32_t cc = cellIdx(P, ci, cj, ck);
+          kill = B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band;
+        }
       }
       if (kill && kc == 0) {
         q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
