@@ -156,6 +156,9 @@ __device__ __forceinline__ uint32_t cellIdx(const FlipParams& P, int i, int j, i
   return tileOf(P, i, j, k) * 512u + (uint32_t)(i & 7) + 8u * ((uint32_t)(j & 7) + 8u * (uint32_t)(k & 7));
 }
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// a floored grid coordinate as an index, held in [-2, 2^24] so that index + 1 cannot overflow for huge or infinite
+// positions (the conversion saturates); in-range values are unchanged
+__device__ __forceinline__ int gidx(float f) { return clampi((int)f, -2, 1 << 24); }
 // the cell holding face (axis, i, j, k) after the reference's clamping (src/flip/wgsl-core.js:84-89)
 __device__ __forceinline__ uint32_t faceCell(const FlipParams& P, int axis, int i, int j, int k) {
   int nx = (int)P.nx, ny = (int)P.ny, nz = (int)P.nz;
@@ -271,7 +274,7 @@ __device__ __forceinline__ void emitTermsT(const FlipParams& P, const WetAt& wet
   const float foam = qv.w, spd = len3(v);
   fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
   const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
-  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+  const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
   rho = 0.0f;
   for (int dz = 0; dz <= 1; dz++)
     for (int dy = 0; dy <= 1; dy++)

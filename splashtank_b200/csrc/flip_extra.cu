@@ -19,7 +19,7 @@ __device__ __forceinline__ float velGAxisX(const FlipParams& P, const float* __r
   V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
   if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
   const V3 f0 = vfloor(g), fr = g - f0;
-  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
   float s = 0.0f;
   for (int c = 0; c < 8; c++) {
     const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
@@ -70,7 +70,7 @@ __device__ __forceinline__ float phiSampleX(const FlipParams& P, const uint32_t*
   const V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
   const V3 gc = vclamp(g, v3(0.0f, 0.0f, 0.0f), v3((float)P.nx - 1.001f, (float)P.ny - 1.001f, (float)P.nz - 1.001f));
   const V3 f0 = vfloor(gc), fr = gc - f0;
-  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
   float s = 0.0f, ws = 0.0f;
   for (int c = 0; c < 8; c++) {
     const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
@@ -266,7 +266,7 @@ __device__ __forceinline__ float wetCell(const FlipParams& P, const Bufs& B, int
 __device__ __forceinline__ float wetAt(const FlipParams& P, const Bufs& B, V3 p) {
   const V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f);
   const V3 f0 = vfloor(g), fr = g - f0;
-  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
   float s = 0.0f;
   for (int c = 0; c < 8; c++) {
     const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
         V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
         if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
         const V3 f0 = vfloor(g), fr = g - f0;
-        const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+        const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
         float sn = 0.0f;
         for (int c = 0; c < 8; c++) {
           const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;

@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
         V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
         if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
         const V3 f0 = vfloor(g), fr = g - f0;
-        const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+        const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
         const float vc = comp3(v, axis);
         for (int c = 0; c < 8; c++) {
           const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
@@ -495,7 +495,7 @@ __device__ __forceinline__ void sampleBoth(const FlipParams& P, const Bufs& B, V
     V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
     if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
     const V3 f0 = vfloor(g), fr = g - f0;
-    const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
     float sn = 0.0f, so = 0.0f;
     for (int c = 0; c < 8; c++) {
       const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
@@ -613,7 +613,7 @@ __device__ __forceinline__ void sampleWin(const FlipParams& P, const G2PWin& W, 
     V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
     if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
     const V3 f0 = vfloor(g), fr = g - f0;
-    const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+    const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
     // the clamped corner cells of faceIndex (wgsl-core.js:84-89): two candidates per axis
     const int hx = axis == 0 ? (int)P.nx : (int)P.nx - 1, hy = axis == 1 ? (int)P.ny : (int)P.ny - 1, hz = axis == 2 ? (int)P.nz : (int)P.nz - 1;
     const int xa = clampi(i0, 0, hx), xb = clampi(i0 + 1, 0, hx);
@@ -693,7 +693,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   sampleWin(P, W, p, vn, vo);    // the particle's own tile has storage: it marked it this step
   V3 v = vmix(vn, v0 + (vn - vo), P.flip);
   const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
-  const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+  const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
   float csum = 8.0f * P.rest;
   const bool fast = P.q12 > 0.5f;
   if (P.q9 < 0.5f && fast) csum = 8.0f * (float)W.cnt[W.idx(fi, fj, fk)];
@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
         float rho, fast, e;
         // the eight cells around the moved particle: from the window when it holds them
         const V3 bcf = vfloor((xyz(q.p) - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
-        const int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
+        const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
         if (W.has(bi, bj, bk) && W.has(bi + 1, bj + 1, bk + 1)) emitTermsT(P, WetWin{W}, q.p, q.v, rho, fast, e);
         else emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
         if (e > 0.0f) {
@@ -841,7 +841,7 @@ __device__ __forceinline__ float velGAxisAt(const FlipParams& P, const float* __
   V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
   if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
   const V3 f0 = vfloor(g), fr = g - f0;
-  const int i0 = (int)f0.x, j0 = (int)f0.y, k0 = (int)f0.z;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
   float s = 0.0f;
   for (int c = 0; c < 8; c++) {
     const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
