@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the B200 FLIP step: particle-steps/s on the full-feature 256^3 wave tank (one JSON line).
 
-python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload wave_tank_256|dam_break_64]
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--workload wave_tank_256|dam_break_64|pressure_512|batch_64]
 
 One process per GPU (torchrun for N > 1, NCCL only for the barrier and the max/sum of the numbers). The FLIP step of
 one tank does not shard, so N GPUs run N independent replica tanks (weak scaling) and value is the total over them.
@@ -44,9 +45,12 @@ def parse():
     ap.add_argument("--omega", type=float, default=1.9, help="pressure workloads: SOR factor")
     ap.add_argument("--inner", type=int, default=100, help="pressure workloads: FP32 iterations per refinement")
     ap.add_argument("--ref-sweeps", type=int, default=1500, help="pressure workloads, reference arm: iterations the CPU time is scaled to")
+    ap.add_argument("--no-autotune", action="store_true", help="batch workloads: default launch shapes")
     a = ap.parse_args()
     if a.workload.startswith("pressure_") and "--steps" not in sys.argv:
         a.steps, a.warmup = 5, 3
+    if a.workload.startswith("batch_") and "--steps" not in sys.argv:
+        a.steps = 100
     return a
 
 
@@ -401,11 +405,186 @@ def run_pressure_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- many tanks per step
+def batch_bytes(stats, iters):
+    """Algorithmic HBM bytes of one step of every tank (the stage_bytes figures of the main stages, summed)."""
+    tot = 0
+    for live, tiles, fluid in stats:
+        cells = tiles * 512
+        for st in ("blocks", "p2g", "norm_faces", "classify", "project", "g2p"):
+            b, _ = stage_bytes(st, live, cells, fluid, iters)
+            tot += b
+        b, launches = stage_bytes("pressure", live, cells, fluid, iters)
+        tot += b * launches
+    return tot
+
+
+def run_batch(a):
+    """64 tanks of uneven size stepped together: value = particle-steps/s over all tanks with the step graphs of all of
+    a rank's tanks in one graph launch and launch shapes from the autotuner; the same tanks launched one after another
+    are timed beside it. Ranks take disjoint sets of tanks (LPT on cells + particles); no collective in the step."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    from splashtank_b200 import scenes
+    from splashtank_b200.batch import TankBatch, autotune, lpt_partition
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    count = int(a.workload.rsplit("_", 1)[1])
+    spec = scenes.BatchTanks(count=count)
+    mine = lpt_partition([spec.cost(k) for k in range(count)], world)[rank]
+    made = [spec.make(k, FlipSim, device=local) for k in mine]
+    sims = [m[0] for m in made]
+    runners = [SceneRunner(s) for s in sims]
+    batch = TankBatch(sims, "graph")
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+
+    def step():
+        batch.step(spec.dt, [spec.step_opts(k, s, r) for k, s, r in zip(mine, sims, runners)])
+
+    def timer(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        return float(t.item())
+
+    for _ in range(2):
+        step()
+    # autotune the launch shape per size class (thirds of this rank's tanks by cells)
+    order = sorted(range(len(mine)), key=lambda i: spec.cost(mine[i]))
+    third = max(1, len(order) // 3)
+    classes = [order[:third], order[third:2 * third], order[2 * third:]]
+    choice, trials = autotune(batch, sims, classes, step, timer) if not a.no_autotune else ([(8, 4, 8)] * 3, {})
+    for _ in range(a.warmup):
+        step()
+    barrier()
+    l0 = batch.launches()
+    clocks = Clocks(local)
+    barrier()
+    ms = timer(lambda: [step() for _ in range(a.steps)])
+    barrier()
+    clk = clocks.stop()
+    launches = batch.launches() - l0
+    stats = [s.readStats() for s in sims]
+    live = sum(st["live"] for st in stats)
+    ms_max = max_over_ranks(ms)
+    live_all = sum_over_ranks(live)
+    value = live_all * a.steps / (ms_max * 1e-3)
+    # the same tanks, one step graph after another on one stream
+    batch.set_mode("sequential")
+    for _ in range(2):
+        step()
+    barrier()
+    ms_seq = max_over_ranks(timer(lambda: [step() for _ in range(a.steps)]))
+    batch.set_mode("graph")
+    # end to end: every step the options and collider records go up and every tank's counters come back
+    barrier()
+    e_steps = max(1, a.e2e_steps // 4)
+    ems = max_over_ranks(timer(lambda: [(step(), [s.readStats() for s in sims]) for _ in range(e_steps)]))
+    if rank == 0:
+        peak, src = measured_peak()
+        iters = spec.opts["iters"]
+        b = batch_bytes([(st["live"], st["sc"], st["fluid"]) for st in stats], iters)
+        per_step_ms = ms / a.steps
+        achieved = b / (per_step_ms * 1e-3) / 1e9
+        ntanks = len(mine)
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded tanks, 8 particles per cell)",
+                "config": {"workload": a.workload, "tanks": count, "tanks_rank0": ntanks, "particles": int(live_all),
+                           "edges": "uniform from %s per axis, cell 1/64" % (scenes.TANK_EDGES,), "fill": "20-60%",
+                           "collider": "one static SDF sphere per tank", "sor_iters": iters, "dt": spec.dt,
+                           "mode": "one graph launch per step (tank step graphs as parallel branches)",
+                           "launch_shape_per_class": choice, "parallelism": "tanks split over ranks (LPT)",
+                           "l2": "working set larger than L2: no flush"},
+                "gpu_launches": int(launches),
+                "sequential": {"ms_per_step": ms_seq / a.steps, "value": live_all * a.steps / (ms_seq * 1e-3),
+                               "mode": "the same step graphs launched one after another on one stream"},
+                "autotune_ms": {"%d:%s" % (k, "x".join(map(str, c))): round(v, 3) for (k, c), v in trials.items()},
+                "clocks": clk,
+                "roofline": {"kernel": "whole batch step (all kernels of all tanks)", "bound": "hbm", "achieved": round(achieved, 1),
+                             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": src, "traffic": None,
+                             "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per_step_ms, 4)},
+                "e2e": {"value": live_all * e_steps / (ems * 1e-3), "unit": "particle-steps/s",
+                        "h2d_bytes_per_step": int(ntanks * (496 + 128)), "d2h_bytes_per_step": int(ntanks * 64), "steps": e_steps,
+                        "readback": "every tank's counters every step"}}
+        if world == 1 and not a.no_cpu_baseline:
+            line["cpu_baseline"] = batch_cpu(spec)
+        print(json.dumps(line), flush=True)
+    batch.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def batch_cpu(spec, budget_s=15.0):
+    """The oracle (all host threads) stepping the smallest tanks of the set one after another, a bounded sample."""
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.scene import SceneRunner
+    th = os.cpu_count() or 1
+    order = sorted(range(len(spec.tanks)), key=lambda k: spec.cost(k))[:4]
+    sims = [spec.make(k, OracleFlipSim, threads=th)[0] for k in order]
+    runners = [SceneRunner(s) for s in sims]
+    n, steps, t0 = 0, 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s:
+        for k, s, r in zip(order, sims, runners):
+            s.step(spec.dt, spec.step_opts(k, s, r))
+        steps += 1
+    el = time.perf_counter() - t0
+    n = sum(s.readStats()["live"] for s in sims)
+    return {"value": n * steps / el, "unit": "particle-steps/s", "cores": th, "kind": "port",
+            "sample": "the 4 smallest tanks (%d particles), %d steps each, oracle with %d OpenMP threads" % (n, steps, th)}
+
+
+def run_batch_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from splashtank_b200 import scenes
+    spec = scenes.BatchTanks(count=int(a.workload.rsplit("_", 1)[1]))
+    cb = batch_cpu(spec, budget_s=min(60.0, 5.0 * max(1, a.steps)))
+    line = {"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s", "impl": "reference", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded tanks)", "config": {"workload": a.workload}, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- our arm
 def main():
     a = parse()
     if a.workload.startswith("pressure_"):
         return run_pressure_reference(a) if a.impl == "reference" else run_pressure(a)
+    if a.workload.startswith("batch_"):
+        return run_batch_reference(a) if a.impl == "reference" else run_batch(a)
     if a.impl == "reference":
         return run_reference(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))

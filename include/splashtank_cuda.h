@@ -272,6 +272,32 @@ st_status st_poisson_sweeps32(st_poisson* s, float omega, int32_t iters, float* 
 st_status st_poisson_read(st_poisson* s, double* p);
 void* st_poisson_stream(st_poisson* s);
 
+/* ---- launch shape of a tank's kernels (no reference counterpart: WebGPU picks no grid sizes) ----
+ * CTAs per SM of the per-tile kernels: heavy (p2g, g2p; default 8), light (classify, normalise, project, narrow band;
+ * default 4) and the pressure sweeps (default 8), each capped at the tile count. Results do not depend on them; an
+ * autotuner picks them for many tanks sharing one GPU. */
+st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light_ctas_per_sm, int32_t sor_ctas_per_sm);
+
+/* ---- many independent tanks stepped together (no reference counterpart; the reference steps one tank) ----
+ * The tanks are st_flip handles on one device, created and owned by the caller. st_batch_step does each tank's
+ * st_flip_step (same options, same result) and runs all their step graphs either as parallel branches of one CUDA
+ * graph launch (ST_BATCH_GRAPH) or one after another on the batch stream (ST_BATCH_SEQUENTIAL). The batch's work is
+ * ordered after each tank's earlier work and before its later work. */
+typedef struct st_batch st_batch;
+enum { ST_BATCH_GRAPH = 0, ST_BATCH_SEQUENTIAL = 1 };
+typedef struct st_batch_desc {
+  uint32_t size;   /* sizeof(st_batch_desc) */
+  int32_t mode;    /* ST_BATCH_* */
+} st_batch_desc;
+st_status st_batch_create(const st_batch_desc* d, st_flip* const* tanks, uint32_t n, st_batch** out);
+void st_batch_destroy(st_batch* b);
+/* opts[i]: the options of tank i (its colliders included) */
+st_status st_batch_step(st_batch* b, double dt, const st_step_opts* const* opts);
+st_status st_batch_set_mode(st_batch* b, int32_t mode);
+void* st_batch_stream(st_batch* b);
+/* kernels launched by batch steps so far */
+uint64_t st_batch_launches(st_batch* b);
+
 /* ---- pressure residual that allocates nothing (no reference counterpart: the reference measures no residual) ----
  * ||b - A x|| / ||b|| of the pressure system above, in FP64, on arrays the caller owns on the device, in the tile-major
  * layout (tile t = ti + tx (tj + ty tk) with tx = ceil(n[0]/8) ..., cell t*512 + lx + 8 (ly + 8 lz)). For callers that

@@ -117,6 +117,7 @@ FLIP_FUNCS = [
     ("flip_nb_fills", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p, C.c_uint32, C.c_uint32]),
 ]
 CUDA_ONLY_FUNCS = [
+    ("flip_set_launch", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     ("step_opts_default", None, [C.POINTER(StepOpts)]),
     ("flip_step_timed", C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepOpts), C.POINTER(StageTimes)]),
     ("flip_stream", C.c_void_p, [C.c_void_p]),
@@ -132,6 +133,19 @@ POISSON_FUNCS = [
     ("poisson_solve", C.c_int, [C.c_void_p, C.POINTER(PoissonOpts), C.POINTER(PoissonResult)]),
     ("poisson_sweeps32", C.c_int, [C.c_void_p, C.c_float, C.c_int32, C.POINTER(C.c_float)]),
     ("poisson_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+]
+class BatchDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("mode", C.c_int32)]
+
+
+ST_BATCH_GRAPH, ST_BATCH_SEQUENTIAL = 0, 1
+BATCH_FUNCS = [
+    ("batch_create", C.c_int, [C.POINTER(BatchDesc), C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]),
+    ("batch_destroy", None, [C.c_void_p]),
+    ("batch_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.POINTER(StepOpts))]),
+    ("batch_set_mode", C.c_int, [C.c_void_p, C.c_int32]),
+    ("batch_stream", C.c_void_p, [C.c_void_p]),
+    ("batch_launches", C.c_uint64, [C.c_void_p]),
 ]
 NOALLOC_FUNCS = [
     ("poisson_residual_noalloc", C.c_int, [C.POINTER(PoissonSystem), C.c_void_p, C.c_void_p, C.POINTER(C.c_double),

@@ -99,6 +99,9 @@ struct st_flip {
   struct Graph { uint64_t key = 0; cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t evnode[11] = {}; int launches = 0; };
   std::vector<Graph> graphs;
   bool use_graphs = true;
+  // CTAs per SM of the per-tile kernels (heavy: p2g, g2p; light: the rest) and of the pressure sweeps
+  int gridT = 8, gridT4 = 4, gridSor = 8;
+  uint64_t gen = 0;   // bumped whenever the captured steps are dropped (their buffers or launch shapes changed)
 
   Bufs bufs() const {
     Bufs B{};
@@ -382,7 +385,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q);        // fluid, vmaxBits, nLive (nActive is kept)
   cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q);
   cudaMemsetAsync(&s->dCtl->emitTried, 0, 2 * sizeof(uint32_t), q);     // emitTried, nFluidTiles
-  const int gT = s->tileGrid(8), gT4 = s->tileGrid(4);
+  const int gT = s->tileGrid(s->gridT), gT4 = s->tileGrid(s->gridT4);
   int nl = 0;
   mark(0);
   // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
@@ -403,7 +406,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(4);
   nl += launch_norm_div(B, gT4, q);
   mark(5);
-  nl += launch_sor(B, gT, iters, q);
+  nl += launch_sor(B, s->tileGrid(s->gridSor), iters, q);
   mark(6);
   nl += launch_project(B, gT4, q);
   mark(7);
@@ -476,13 +479,12 @@ static void drop_graphs(st_flip* s) {
     if (g.graph) cudaGraphDestroy(g.graph);
   }
   s->graphs.clear();
+  s->gen++;
 }
 
-// one step; t (optional) receives device ms per stage
-static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
-  if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
-  if (s->N == 0) return ST_NOT_READY;
-  CK(cudaSetDevice(s->device));
+// The host half of a step: parameter block, collider records and counters, with the uploads enqueued on q.
+struct StepPrep { bool nbOn = false, sprOn = false; uint32_t init = 0; int iters = 1; };
+static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cudaStream_t q, StepPrep* pr) {
   const bool nbOn = o->nb_on != 0;
   if (nbOn) s->velGOn = true;
   const uint32_t init = nbOn && s->nbInit ? s->nbInit : 0;
@@ -501,7 +503,6 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   s->tm = s->tm + dt;
   if (init) { s->nbInit = 0; s->fills.clear(); }
   const int iters = std::max(1, o->iters);
-  cudaStream_t q = s->stream;
   // this step's storage order goes into the other particle buffer; cell counts alternate buffers
   s->cur ^= 1;
   s->parity ^= 1;
@@ -509,6 +510,22 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   CK(cudaMemcpyAsync(&s->dUp->P, &up->P, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
   if (nc) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
   CK(cudaEventRecord(upEv, q));
+  pr->nbOn = nbOn; pr->sprOn = sprOn; pr->init = init; pr->iters = iters;
+  return ST_OK;
+}
+
+// one step; t (optional) receives device ms per stage
+static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
+  if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
+  if (s->N == 0) return ST_NOT_READY;
+  CK(cudaSetDevice(s->device));
+  cudaStream_t q = s->stream;
+  StepPrep pr;
+  st_status st = prepare_step(s, dt, o, q, &pr);
+  if (st != ST_OK) return st;
+  const bool nbOn = pr.nbOn, sprOn = pr.sprOn;
+  const uint32_t init = pr.init;
+  const int iters = pr.iters;
   const Bufs B = s->bufs();
   cudaEvent_t* tslot = nullptr;
   if (s->timing) {
@@ -709,6 +726,176 @@ st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const
     s->fills.insert(s->fills.end(), f, f + 8);
   }
   s->nbInit = mode ? mode : 1;
+  return ST_OK;
+}
+
+
+st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light_ctas_per_sm, int32_t sor_ctas_per_sm) {
+  if (!s || tile_ctas_per_sm < 1 || light_ctas_per_sm < 1 || sor_ctas_per_sm < 1 || tile_ctas_per_sm > 64 ||
+      light_ctas_per_sm > 64 || sor_ctas_per_sm > 64)
+    return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (s->gridT == tile_ctas_per_sm && s->gridT4 == light_ctas_per_sm && s->gridSor == sor_ctas_per_sm) return ST_OK;
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  s->gridT = tile_ctas_per_sm; s->gridT4 = light_ctas_per_sm; s->gridSor = sor_ctas_per_sm;
+  return ST_OK;
+}
+
+}  // extern "C"
+
+// ---- many tanks per step (st_batch_*) ----
+// Each tank keeps its own buffers and its captured step graph. A batch step does the host half of every tank's step
+// (uploads on the batch stream), then runs the tanks' step graphs either as the parallel branches of one CUDA graph
+// (ST_BATCH_GRAPH: one launch; independent tanks run concurrently and fill the GPU together) or one after another on
+// the batch stream (ST_BATCH_SEQUENTIAL). Both orders give every tank the same result as st_flip_step.
+struct st_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int mode = ST_BATCH_GRAPH;
+  std::vector<st_flip*> tanks;
+  std::vector<cudaEvent_t> tankEv;
+  cudaEvent_t evOut = nullptr;
+  struct Combined {
+    std::vector<uint64_t> key;   // per tank: step graph key and generation
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<Combined> cache;
+  uint64_t launches = 0, graph_launches = 0;
+};
+
+static void batch_drop(st_batch* b) {
+  for (auto& c : b->cache) {
+    if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+  }
+  b->cache.clear();
+}
+
+extern "C" {
+
+void st_batch_destroy(st_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop(b);
+  for (auto e : b->tankEv) if (e) cudaEventDestroy(e);
+  if (b->evOut) cudaEventDestroy(b->evOut);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+st_status st_batch_create(const st_batch_desc* d, st_flip* const* tanks, uint32_t n, st_batch** out) {
+  if (!d || !out || d->size != sizeof(st_batch_desc) || !tanks || !n || (d->mode != ST_BATCH_GRAPH && d->mode != ST_BATCH_SEQUENTIAL))
+    return ST_BAD_ARG;
+  *out = nullptr;
+  for (uint32_t i = 0; i < n; i++)
+    if (!tanks[i] || tanks[i]->device != tanks[0]->device) return ST_BAD_ARG;
+  st_batch* b = new st_batch();
+  b->device = tanks[0]->device;
+  b->mode = d->mode;
+  b->tanks.assign(tanks, tanks + n);
+  b->tankEv.assign(n, nullptr);
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evOut, cudaEventDisableTiming);
+  for (uint32_t i = 0; i < n && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&b->tankEv[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    set_err("batch create", e);
+    st_batch_destroy(b);
+    return ST_DEVICE_ERROR;
+  }
+  *out = b;
+  return ST_OK;
+}
+
+st_status st_batch_set_mode(st_batch* b, int32_t mode) {
+  if (!b || (mode != ST_BATCH_GRAPH && mode != ST_BATCH_SEQUENTIAL)) return ST_BAD_ARG;
+  b->mode = mode;
+  return ST_OK;
+}
+
+void* st_batch_stream(st_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+uint64_t st_batch_launches(st_batch* b) { return b ? b->launches : 0; }
+
+st_status st_batch_step(st_batch* b, double dt, const st_step_opts* const* opts) {
+  if (!b || !opts) return ST_BAD_ARG;
+  const size_t n = b->tanks.size();
+  for (size_t i = 0; i < n; i++)
+    if (!opts[i] || opts[i]->size != sizeof(st_step_opts)) return ST_BAD_ARG;
+  CK(cudaSetDevice(b->device));
+  cudaStream_t q = b->stream;
+  // after whatever each tank's own stream still has queued (adds, reads)
+  for (size_t i = 0; i < n; i++) {
+    CK(cudaEventRecord(b->tankEv[i], b->tanks[i]->stream));
+    CK(cudaStreamWaitEvent(q, b->tankEv[i], 0));
+  }
+  std::vector<cudaGraph_t> kids;
+  std::vector<uint64_t> key;
+  for (size_t i = 0; i < n; i++) {
+    st_flip* s = b->tanks[i];
+    if (s->N == 0) continue;
+    StepPrep pr;
+    st_status st = prepare_step(s, dt, opts[i], q, &pr);
+    if (st != ST_OK) return st;
+    const Bufs B = s->bufs();
+    int nl = 0;
+    if (pr.init || !s->use_graphs) {
+      nl = enqueue_step(s, B, q, pr.nbOn, pr.init, pr.sprOn, pr.iters, [](int) {});
+    } else {
+      st_flip::Graph* g = nullptr;
+      st = get_graph(s, B, pr.nbOn, pr.sprOn, pr.iters, false, &g);
+      if (st != ST_OK) return st;
+      nl = g->launches;
+      if (b->mode == ST_BATCH_SEQUENTIAL) {
+        CK(cudaGraphLaunch(g->exec, q));
+        b->graph_launches++;
+      } else {
+        kids.push_back(g->graph);
+        key.push_back(g->key);
+        key.push_back(s->gen);
+        key.push_back((uint64_t)i);
+      }
+    }
+    s->launches += (uint64_t)nl;
+    b->launches += (uint64_t)nl;
+    s->steps++;
+  }
+  if (!kids.empty()) {
+    st_batch::Combined* c = nullptr;
+    for (auto& x : b->cache) if (x.key == key) c = &x;
+    if (!c) {
+      if (b->cache.size() >= 4) {
+        if (b->cache.front().exec) cudaGraphExecDestroy(b->cache.front().exec);
+        if (b->cache.front().graph) cudaGraphDestroy(b->cache.front().graph);
+        b->cache.erase(b->cache.begin());
+      }
+      st_batch::Combined nc;
+      nc.key = key;
+      cudaError_t e = cudaGraphCreate(&nc.graph, 0);
+      for (size_t k = 0; k < kids.size() && e == cudaSuccess; k++) {
+        cudaGraphNode_t node;
+        e = cudaGraphAddChildGraphNode(&node, nc.graph, nullptr, 0, kids[k]);
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&nc.exec, nc.graph, 0);
+      if (e != cudaSuccess) {
+        set_err("batch graph", e);
+        if (nc.exec) cudaGraphExecDestroy(nc.exec);
+        if (nc.graph) cudaGraphDestroy(nc.graph);
+        return ST_DEVICE_ERROR;
+      }
+      b->cache.push_back(nc);
+      c = &b->cache.back();
+    }
+    CK(cudaGraphLaunch(c->exec, q));
+    b->graph_launches++;
+  }
+  CK(cudaGetLastError());
+  // each tank's later work (reads, the next single step) waits for this batch step
+  CK(cudaEventRecord(b->evOut, q));
+  for (size_t i = 0; i < n; i++) CK(cudaStreamWaitEvent(b->tanks[i]->stream, b->evOut, 0));
   return ST_OK;
 }
 

@@ -228,32 +228,44 @@ __global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
 // written to their final place (ascending id inside each cell) and splatted into a 10^3-cell shared-memory window
 // (the tile plus one cell around it) in the reference's fixed point: i32(round(w * v * 65536)) and i32(round(w * 65536)).
 // Integer sums do not depend on order, so the window is flushed to HBM with plain atomic adds.
+// The tile's ids (when at most P2G_IDS), cell offsets and counts are staged in shared memory first: the in-cell rank
+// (ids below this particle's in its cell) then reads shared memory instead of issuing a global load per neighbour.
 constexpr int P2G_T = 256;
+constexpr uint32_t P2G_IDS = 4608;
 __global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
   __shared__ FlipParams P;
   __shared__ int32_t win[6][1000];
+  __shared__ uint32_t sid[P2G_IDS];
+  __shared__ uint32_t soff[512];
+  __shared__ int32_t scnt[512];
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a];
     const uint32_t tt = t / P.tx;
     const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
-    for (int r = threadIdx.x; r < 6000; r += P2G_T) (&win[0][0])[r] = 0;
-    __syncthreads();
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
+    const bool staged = s1 - s0 <= P2G_IDS;
+    for (int r = threadIdx.x; r < 6000; r += P2G_T) (&win[0][0])[r] = 0;
+    if (staged) for (uint32_t u = s0 + threadIdx.x; u < s1; u += P2G_T) sid[u - s0] = B.spid[u];
+    for (int r = threadIdx.x; r < 512; r += P2G_T) { soff[r] = B.cellOff[t * 512u + r]; scnt[r] = B.cnt[t * 512u + r]; }
+    __syncthreads();
     for (uint32_t base = s0; base < s1; base += P2G_T) {
       // lanes of a warp take particles 8 apart, so they fall in different cells and their shared atomics rarely collide
       const uint32_t s = base + (uint32_t)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
       if (s >= s1) continue;
-      const uint32_t src = B.srcIdx[s], myid = B.spid[s];
+      const uint32_t src = B.srcIdx[s], myid = staged ? sid[s - s0] : B.spid[s];
       const Part q = B.pb[src];
       const V3 p = xyz(q.p), v = xyz(q.v);
       int ci, cj, ck;
       particleCell(P, p, ci, cj, ck);
-      const uint32_t key = cellIdx(P, ci, cj, ck);
-      const uint32_t cs = s0 + B.cellOff[key], ce = cs + (uint32_t)B.cnt[key];
+      const uint32_t key = cellIdx(P, ci, cj, ck), lk = key - t * 512u;
+      uint32_t cs, ce;
+      if (lk < 512u) { cs = s0 + soff[lk]; ce = cs + (uint32_t)scnt[lk]; }
+      else { cs = s0 + B.cellOff[key]; ce = cs + (uint32_t)B.cnt[key]; }
       uint32_t rk = 0;
-      for (uint32_t u = cs; u < ce; u++) rk += B.spid[u] < myid ? 1u : 0u;
+      if (staged && cs >= s0 && ce <= s1) { for (uint32_t u = cs - s0; u < ce - s0; u++) rk += sid[u] < myid ? 1u : 0u; }
+      else { for (uint32_t u = cs; u < ce; u++) rk += B.spid[u] < myid ? 1u : 0u; }
       B.pa[cs + rk] = q;
       B.ida[cs + rk] = myid;
       for (int axis = 0; axis < 3; axis++) {

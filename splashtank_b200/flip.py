@@ -256,6 +256,11 @@ class FlipSim:
         del keep
         return {n: getattr(t, n) for n in abi.STAGES}
 
+    def set_launch(self, tile_ctas_per_sm, light_ctas_per_sm, sor_ctas_per_sm):
+        """CTAs per SM of the heavy per-tile kernels, the light ones and the pressure sweeps (st_flip_set_launch)."""
+        self._check(self.f["flip_set_launch"](self._h, int(tile_ctas_per_sm), int(light_ctas_per_sm), int(sor_ctas_per_sm)),
+                    "set_launch")
+
     def set_timing(self, on=True):
         """Record per-stage device times of every step without stalling (st_flip_set_timing)."""
         self._check(self.f["flip_set_timing"](self._h, 1 if on else 0), "set_timing")
