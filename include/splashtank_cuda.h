@@ -182,6 +182,14 @@ st_status st_flip_save_state(st_flip* s, float* pos4, float* vel4, uint32_t* pid
 /* Replace every particle (storage order, with ids); resets time-since-start to t and the seed counter. */
 st_status st_flip_load_state(st_flip* s, const float* pos4, const float* vel4, const uint32_t* pid, uint32_t n,
                              double t, uint32_t seed);
+/* Full checkpoint (no reference counterpart: the reference's cache stores frames, not solver state): everything a step
+ * reads before it writes (particles in storage order, pressure warm start, cell types with the narrow band's depth,
+ * kept grid velocity, both count buffers, tile flags and list, face velocities, the whitewater ring, the device
+ * counters) and the host step state (time, seed, stamps, buffer parity). Restoring it into a handle created with the
+ * same desc continues bit-identically. save: with buf null, *size receives the bytes needed; a smaller cap returns
+ * ST_OVERFLOW. load: collider distance grids are uploaded again by the next step. */
+st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size);
+st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size);
 /* Narrow band start (nbSeed's sim.nbFills, src/shared.js:849-851): boxes as {x0,y0,z0,x1,y1,z1} and spheres as
  * {x,y,z,r}; the next step initialises the depth field from them (nbInit = mode). */
 st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const float* spheres4, uint32_t nsph,

@@ -117,6 +117,8 @@ FLIP_FUNCS = [
     ("flip_nb_fills", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p, C.c_uint32, C.c_uint32]),
 ]
 CUDA_ONLY_FUNCS = [
+    ("flip_save_full", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("flip_load_full", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     ("flip_set_launch", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     ("step_opts_default", None, [C.POINTER(StepOpts)]),
     ("flip_step_timed", C.c_int, [C.c_void_p, C.c_double, C.POINTER(StepOpts), C.POINTER(StageTimes)]),

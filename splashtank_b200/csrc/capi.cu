@@ -730,6 +730,83 @@ st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const
 }
 
 
+// ---- full checkpoint: every buffer a step reads before it writes, plus the host step state ----
+struct FullHdr {
+  uint32_t magic, version, nx, ny, nz, ntiles, ncell, maxN, sprayCap;
+  uint32_t N, cap, ring, seed, steps, stamp, parity, cur, velGOn, nbInit, nfills, pad;
+  double tm;
+};
+static constexpr uint32_t FULL_MAGIC = 0x53544650u;   // "PFTS"
+static void full_parts(st_flip* s, std::vector<std::pair<void*, size_t>>& v) {
+  const size_t C = s->ncell, T = s->ntiles, SC = std::max<size_t>(s->sprayCap, 1), N = s->N;
+  v = {{s->dCtl, sizeof(Ctl)}, {s->part[s->cur], N * sizeof(Part)}, {s->ids[s->cur], N * 4}, {s->need, T * 4}, {s->on, T},
+       {s->tstate, T}, {s->active, T * 4}, {s->cnt[0], C * 4}, {s->cnt[1], C * 4}, {s->ctype, C * 4}, {s->pres, C * 4},
+       {s->rhs, C * 4}, {s->acc, 6 * C * 4}, {s->vn, 3 * C * 4}, {s->vo, 3 * C * 4}, {s->velG, 3 * C * 4}, {s->sorInfo, C * 2},
+       {s->wet, C * 4}, {s->sPos, SC * 16}, {s->sVel, SC * 16}};
+}
+
+st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size) {
+  if (!s || !size) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  std::vector<std::pair<void*, size_t>> parts;
+  full_parts(s, parts);
+  uint64_t need = sizeof(FullHdr) + s->fills.size() * sizeof(float);
+  for (auto& p : parts) need += p.second;
+  *size = need;
+  if (!buf) return ST_OK;
+  if (cap < need) return ST_OVERFLOW;
+  FullHdr h{};
+  h.magic = FULL_MAGIC; h.version = 1; h.nx = (uint32_t)s->nx; h.ny = (uint32_t)s->ny; h.nz = (uint32_t)s->nz; h.ntiles = s->ntiles;
+  h.ncell = s->ncell; h.maxN = s->maxN; h.sprayCap = s->sprayCap; h.N = s->N; h.cap = s->cap; h.ring = s->ring; h.seed = s->seed;
+  h.steps = s->steps; h.stamp = s->stamp; h.parity = s->parity; h.cur = (uint32_t)s->cur; h.velGOn = s->velGOn ? 1u : 0u;
+  h.nbInit = s->nbInit; h.nfills = (uint32_t)s->fills.size(); h.tm = s->tm;
+  char* out = static_cast<char*>(buf);
+  memcpy(out, &h, sizeof(h));
+  out += sizeof(h);
+  if (!s->fills.empty()) { memcpy(out, s->fills.data(), s->fills.size() * sizeof(float)); out += s->fills.size() * sizeof(float); }
+  for (auto& p : parts) {
+    if (p.second) CK(cudaMemcpyAsync(out, p.first, p.second, cudaMemcpyDeviceToHost, s->stream));
+    out += p.second;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
+  if (!s || !buf || size < sizeof(FullHdr)) return ST_BAD_ARG;
+  FullHdr h;
+  memcpy(&h, buf, sizeof(h));
+  if (h.magic != FULL_MAGIC || h.version != 1 || h.nx != (uint32_t)s->nx || h.ny != (uint32_t)s->ny || h.nz != (uint32_t)s->nz ||
+      h.ntiles != s->ntiles || h.ncell != s->ncell || h.maxN != s->maxN || h.sprayCap != s->sprayCap || h.N > s->maxN || h.cur > 1 ||
+      h.parity > 1) {
+    snprintf(g_err, sizeof(g_err), "load_full: the checkpoint is not of a simulator with this geometry and capacity");
+    return ST_BAD_ARG;
+  }
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  s->N = h.N; s->cap = h.cap; s->ring = h.ring; s->seed = h.seed; s->steps = h.steps; s->stamp = h.stamp; s->parity = h.parity;
+  s->cur = (int)h.cur; s->velGOn = h.velGOn != 0; s->nbInit = h.nbInit; s->tm = h.tm;
+  std::vector<std::pair<void*, size_t>> parts;
+  full_parts(s, parts);
+  uint64_t need = sizeof(FullHdr) + (uint64_t)h.nfills * sizeof(float);
+  for (auto& p : parts) need += p.second;
+  if (size < need) {
+    snprintf(g_err, sizeof(g_err), "load_full: %llu bytes given, %llu needed", (unsigned long long)size, (unsigned long long)need);
+    return ST_BAD_ARG;
+  }
+  const char* in = static_cast<const char*>(buf) + sizeof(FullHdr);
+  s->fills.assign(reinterpret_cast<const float*>(in), reinterpret_cast<const float*>(in) + h.nfills);
+  in += (size_t)h.nfills * sizeof(float);
+  for (auto& p : parts) {
+    if (p.second) CK(cudaMemcpyAsync(p.first, in, p.second, cudaMemcpyHostToDevice, s->stream));
+    in += p.second;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  s->sdfSig.clear();   // the next step uploads its colliders' distance grids again
+  return ST_OK;
+}
+
 st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light_ctas_per_sm, int32_t sor_ctas_per_sm) {
   if (!s || tile_ctas_per_sm < 1 || light_ctas_per_sm < 1 || sor_ctas_per_sm < 1 || tile_ctas_per_sm > 64 ||
       light_ctas_per_sm > 64 || sor_ctas_per_sm > 64)

@@ -256,6 +256,20 @@ class FlipSim:
         del keep
         return {n: getattr(t, n) for n in abi.STAGES}
 
+    def save_full(self):
+        """The full checkpoint (st_flip_save_full) as bytes."""
+        self.flushRun()
+        n = C.c_uint64()
+        self._check(self.f["flip_save_full"](self._h, None, 0, C.byref(n)), "save_full")
+        buf = C.create_string_buffer(n.value)
+        self._check(self.f["flip_save_full"](self._h, buf, n.value, C.byref(n)), "save_full")
+        return buf.raw
+
+    def load_full(self, blob):
+        """Restore a full checkpoint made by a simulator with the same geometry and capacity."""
+        self._pend_p, self._pend_v = [], []
+        self._check(self.f["flip_load_full"](self._h, blob, len(blob)), "load_full")
+
     def set_launch(self, tile_ctas_per_sm, light_ctas_per_sm, sor_ctas_per_sm):
         """CTAs per SM of the heavy per-tile kernels, the light ones and the pressure sweeps (st_flip_set_launch)."""
         self._check(self.f["flip_set_launch"](self._h, int(tile_ctas_per_sm), int(light_ctas_per_sm), int(sor_ctas_per_sm)),
