@@ -88,6 +88,9 @@ struct st_flip {
   float *pres = nullptr, *rhs = nullptr, *vn = nullptr, *vo = nullptr, *velG = nullptr;
   int32_t* acc = nullptr;
   uint16_t* sorInfo = nullptr;
+  float *cp = nullptr, *crhs = nullptr;
+  uint16_t* cinfo = nullptr;
+  uint32_t *nbs = nullptr, *slotOf = nullptr;
   float* wet = nullptr;
   float* sdf = nullptr;
   float4 *sPos = nullptr, *sVel = nullptr;
@@ -111,7 +114,7 @@ struct st_flip {
     B.need = need; B.on = on; B.tstate = tstate; B.blkTiles = blkTiles; B.active = active; B.prevActive = nullptr;
     B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
-    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
+    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
     B.sPos = sPos; B.sVel = sVel; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
@@ -144,7 +147,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList};
+                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -201,7 +204,9 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(dalloc(&s->tileEmit, T + 1), "tileEmit"); A(dalloc(&s->tileDead, T + 1), "tileDead"); A(dalloc(&s->deadF, M), "deadF");
   A(dalloc(&s->cellOff, C), "cellOff"); A(dalloc(&s->ctype, C), "ctype"); A(dalloc(&s->pres, C), "pres"); A(dalloc(&s->rhs, C), "rhs");
   A(dalloc(&s->acc, 6 * C), "acc"); A(dalloc(&s->vn, 3 * C), "vn"); A(dalloc(&s->vo, 3 * C), "vo"); A(dalloc(&s->velG, 3 * C), "velG");
-  A(dalloc(&s->sorInfo, C), "sorInfo"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
+  A(dalloc(&s->sorInfo, C), "sorInfo");
+  A(dalloc(&s->cp, C), "sweep p"); A(dalloc(&s->crhs, C), "sweep rhs"); A(dalloc(&s->cinfo, C), "sweep info");
+  A(dalloc(&s->nbs, 6 * T), "sweep neighbours"); A(dalloc(&s->slotOf, T), "sweep slots"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
   A(dalloc(&s->sPos, std::max<size_t>(s->sprayCap, 1)), "sPos"); A(dalloc(&s->sVel, std::max<size_t>(s->sprayCap, 1)), "sVel");
   for (auto& ev : s->ev) A(cudaEventCreate(&ev), "event");
   A(cudaMallocHost((void**)&s->ring_h, sizeof(st_flip::Upload) * st_flip::RING), "upload ring"); A(dalloc(&s->dUp, 1), "upload");
@@ -217,6 +222,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(cudaMemsetAsync(s->acc, 0, 6 * C * 4, q), "memset"); A(cudaMemsetAsync(s->vn, 0, 3 * C * 4, q), "memset");
   A(cudaMemsetAsync(s->vo, 0, 3 * C * 4, q), "memset"); A(cudaMemsetAsync(s->velG, 0, 3 * C * 4, q), "memset");
   A(cudaMemsetAsync(s->sorInfo, 0, C * 2, q), "memset");
+  A(cudaMemsetAsync(s->slotOf, 0xff, T * 4, q), "memset");
   A(cudaMemsetAsync(s->wet, 0, C * 4, q), "memset");
   A(cudaMemsetAsync(s->sPos, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
   A(cudaMemsetAsync(s->sVel, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
@@ -406,7 +412,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(4);
   nl += launch_norm_div(B, gT4, q);
   mark(5);
-  nl += launch_sor(B, s->tileGrid(s->gridSor), iters, q);
+  nl += launch_sor_compact(B, s->tileGrid(s->gridSor), gT4, iters, q);
   mark(6);
   nl += launch_project(B, gT4, q);
   mark(7);

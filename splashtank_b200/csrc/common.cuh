@@ -94,6 +94,13 @@ struct Bufs {
   float* vo;            // 3 planes: old face velocity
   float* velG;          // 3 planes: kept grid velocity (narrow band)
   uint16_t* sorInfo;    // per fluid cell: bits 0-5 neighbour is fluid, bits 8-10 non-solid neighbours
+  // the pressure sweeps' compact copy: per fluid tile (position a in fluidTiles) 512 values, red cells then black
+  // ones, each half ordered (lx / 2) + 4 (ly + 8 lz); nbs: the positions of its 6 face neighbours (own when none)
+  float* cp;
+  float* crhs;
+  uint16_t* cinfo;
+  uint32_t* nbs;
+  uint32_t* slotOf;     // per tile: position in fluidTiles, or 0xffffffff
   float* wet;           // per cell: how much water (wetCell, src/flip/wgsl-whitewater.js:7-12), 0 outside the domain
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)

@@ -431,32 +431,64 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
 // neighbours are fluid and how many are not solid. All eight loads of a cell are issued together from addresses that
 // are always valid (a missing neighbour reads the cell itself); the sum then adds only the fluid neighbours, in the
 // reference's order, so the arithmetic is unchanged.
-// One colour over the fluid tiles a = first, first + stride, ...; pressures are read at L2 (__ldcg) so that the
-// persistent launch below sees other CTAs' writes after its grid barrier.
-__global__ void __launch_bounds__(256) k_sor(Bufs B, uint32_t color) {
+// The sweeps run on a compact copy of the fluid tiles: per tile its red cells then its black ones, each half ordered
+// (lx / 2) + 4 (ly + 8 lz). A warp's cells and each of its six neighbour loads are then contiguous runs of the other
+// colour's half (a face neighbour across the tile boundary comes from the neighbour tile's copy), instead of touching
+// whole 32-byte sectors of neighbour tiles for one value each. Same arithmetic, same order per cell.
+__global__ void k_sor_slots(Bufs B) {
+  const uint32_t nT = B.ctl->nFluidTiles;
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nT; a += gridDim.x * blockDim.x) B.slotOf[B.fluidTiles[a]] = a;
+}
+__device__ __forceinline__ uint32_t splitIdx(uint32_t local) {
+  const uint32_t lx = local & 7u, ly = (local >> 3) & 7u, lz = local >> 6;
+  return ((lx + ly + lz) & 1u) * 256u + (lx >> 1) + 4u * (ly + 8u * lz);
+}
+__global__ void __launch_bounds__(512) k_sor_pack(Bufs B) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
   const uint32_t nT = B.ctl->nFluidTiles;
-  const int lz = threadIdx.x >> 5, ly = (threadIdx.x >> 2) & 7;
-  const int lx = 2 * (threadIdx.x & 3) + (int)((ly + lz + color) & 1);
-  const uint32_t local = (uint32_t)(lx + 8 * (ly + 8 * lz));
   for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t t = B.fluidTiles[a], c = t * 512u + local;
-    const uint32_t tt = t / P.tx, ti = t % P.tx, tj = tt % P.ty, tk = tt / P.ty;
-    // neighbour cells: inside the tile by offset, across a tile face into the neighbouring tile
-    const uint32_t cxm = lx > 0 ? c - 1u : (ti > 0 ? c - 512u + 7u : c);
-    const uint32_t cxp = lx < 7 ? c + 1u : (ti + 1 < P.tx ? c + 512u - 7u : c);
-    const uint32_t cym = ly > 0 ? c - 8u : (tj > 0 ? c - 512u * P.tx + 56u : c);
-    const uint32_t cyp = ly < 7 ? c + 8u : (tj + 1 < P.ty ? c + 512u * P.tx - 56u : c);
-    const uint32_t cell_z = 512u * P.tx * P.ty;
-    const uint32_t czm = lz > 0 ? c - 64u : (tk > 0 ? c - cell_z + 448u : c);
-    const uint32_t czp = lz < 7 ? c + 64u : (tk + 1 < P.tz ? c + cell_z - 448u : c);
-    const uint32_t info = B.sorInfo[c];
-    const float p0 = B.pres[c], r0 = B.rhs[c];
-    const float pxm = B.pres[cxm], pxp = B.pres[cxp], pym = B.pres[cym], pyp = B.pres[cyp], pzm = B.pres[czm], pzp = B.pres[czp];
+    const uint32_t t = B.fluidTiles[a], c = t * 512u + threadIdx.x, d = a * 512u + splitIdx(threadIdx.x);
+    B.cp[d] = B.pres[c];
+    B.crhs[d] = B.rhs[c];
+    B.cinfo[d] = B.sorInfo[c];
+    if (threadIdx.x < 6) {
+      const uint32_t tt = t / P.tx, ti = t % P.tx, tj = tt % P.ty, tk = tt / P.ty;
+      const int dir = threadIdx.x;
+      uint32_t n = 0xffffffffu;
+      if (dir == 0 && ti > 0) n = t - 1u;
+      if (dir == 1 && ti + 1 < P.tx) n = t + 1u;
+      if (dir == 2 && tj > 0) n = t - P.tx;
+      if (dir == 3 && tj + 1 < P.ty) n = t + P.tx;
+      if (dir == 4 && tk > 0) n = t - P.tx * P.ty;
+      if (dir == 5 && tk + 1 < P.tz) n = t + P.tx * P.ty;
+      const uint32_t sl = n != 0xffffffffu ? B.slotOf[n] : 0xffffffffu;
+      B.nbs[a * 6u + dir] = sl != 0xffffffffu ? sl : a;   // no fluid there: never summed, so any valid cell will do
+    }
+  }
+}
+__global__ void __launch_bounds__(256) k_sor_c(Bufs B, uint32_t color) {
+  const uint32_t nT = B.ctl->nFluidTiles;
+  const float omega = B.P->omega;
+  const uint32_t j = threadIdx.x, lz = j >> 5, ly = (j >> 2) & 7u;
+  const uint32_t lx = 2u * (j & 3u) + ((ly + lz + color) & 1u), row = j & ~3u;
+  const uint32_t own = color * 256u + j, oth = (color ^ 1u) * 256u;
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t* nb = B.nbs + a * 6u;
+    const uint32_t base = a * 512u + oth;
+    const uint32_t ixm = lx > 0 ? base + row + ((lx - 1u) >> 1) : nb[0] * 512u + oth + row + 3u;
+    const uint32_t ixp = lx < 7 ? base + row + ((lx + 1u) >> 1) : nb[1] * 512u + oth + row;
+    const uint32_t iym = ly > 0 ? base + j - 4u : nb[2] * 512u + oth + j + 28u;
+    const uint32_t iyp = ly < 7 ? base + j + 4u : nb[3] * 512u + oth + j - 28u;
+    const uint32_t izm = lz > 0 ? base + j - 32u : nb[4] * 512u + oth + j + 224u;
+    const uint32_t izp = lz < 7 ? base + j + 32u : nb[5] * 512u + oth + j - 224u;
+    const uint32_t c = a * 512u + own;
+    const uint32_t info = B.cinfo[c];
+    const float p0 = B.cp[c], r0 = B.crhs[c];
+    const float pxm = B.cp[ixm], pxp = B.cp[ixp], pym = B.cp[iym], pyp = B.cp[iyp], pzm = B.cp[izm], pzp = B.cp[izp];
     if (!(info & 0x8000u)) continue;
     const uint32_t nns = (info >> 8) & 7u;
-    if (nns == 0u) { B.pres[c] = 0.0f; continue; }
+    if (nns == 0u) { B.cp[c] = 0.0f; continue; }
     float sum = 0.0f;
     if (info & 1u) sum += pxm;
     if (info & 2u) sum += pxp;
@@ -465,7 +497,16 @@ __global__ void __launch_bounds__(256) k_sor(Bufs B, uint32_t color) {
     if (info & 16u) sum += pzm;
     if (info & 32u) sum += pzp;
     const float pg = (r0 + sum) / (float)nns;
-    B.pres[c] = p0 + P.omega * (pg - p0);
+    B.cp[c] = p0 + omega * (pg - p0);
+  }
+}
+// back into the grid; the slot map goes back to empty for the next step
+__global__ void __launch_bounds__(512) k_sor_unpack(Bufs B) {
+  const uint32_t nT = B.ctl->nFluidTiles;
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t t = B.fluidTiles[a];
+    B.pres[t * 512u + threadIdx.x] = B.cp[a * 512u + splitIdx(threadIdx.x)];
+    if (threadIdx.x == 0) B.slotOf[t] = 0xffffffffu;
   }
 }
 
@@ -901,9 +942,12 @@ int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, PBLK, 0,
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
 int launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); return 1; }
-int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s) {
-  for (int it = 0; it < iters; it++) { k_sor<<<grid, 256, 0, s>>>(B, 0u); k_sor<<<grid, 256, 0, s>>>(B, 1u); }
-  return 2 * iters;
+int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s) {
+  k_sor_slots<<<64, 256, 0, s>>>(B);
+  k_sor_pack<<<grid4, 512, 0, s>>>(B);
+  for (int it = 0; it < iters; it++) { k_sor_c<<<grid, 256, 0, s>>>(B, 0u); k_sor_c<<<grid, 256, 0, s>>>(B, 1u); }
+  k_sor_unpack<<<grid4, 512, 0, s>>>(B);
+  return 2 * iters + 3;
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_g2p(const Bufs& B, int grid, cudaStream_t s) {

@@ -12,7 +12,7 @@ int launch_scatter(const Bufs& B, cudaStream_t s);
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
 int launch_classify(const Bufs& B, int grid, cudaStream_t s);
 int launch_norm_div(const Bufs& B, int grid, cudaStream_t s);
-int launch_sor(const Bufs& B, int grid, int iters, cudaStream_t s);
+int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s);
 int launch_project(const Bufs& B, int grid, cudaStream_t s);
 int launch_g2p(const Bufs& B, int grid, cudaStream_t s);
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);

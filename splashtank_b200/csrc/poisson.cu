@@ -7,8 +7,11 @@
 // Refinement: x (FP64) = 0, r = b; repeat: e = FP32 SOR sweeps on A e = (float) r from e = 0, x += e, r = b - A x in FP64,
 // until ||r|| / ||b|| <= tol. Only the residual and the correction use FP64.
 //
-// Layout: the tile-major layout of the FLIP grid (8^3 tiles, cell t*512 + local); only tiles holding fluid are visited.
-// Norms are summed per tile in cell order, then over tiles in tile order by one CTA, so they are reproducible.
+// Layout: only the 8^3 tiles holding fluid are stored, in ascending tile order (slot a); a slot holds its tile's red
+// cells then its black ones, each half ordered (lx / 2) + 4 (ly + 8 lz), and nbs gives the slots of its 6 face
+// neighbours (its own slot when a neighbour holds no fluid: such values are never summed). A sweep's loads are then
+// contiguous per warp. Norms are summed per tile over the cells in (lx, ly, lz) order by a fixed tree, then over tiles
+// in tile order by one CTA, so they are reproducible.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -23,6 +26,7 @@ namespace {
 
 struct PGeo { uint32_t nx, ny, nz, tx, ty, tz; };
 
+// standard tile-major neighbours (used by the residual on caller arrays below)
 __device__ __forceinline__ void neighbours(const PGeo& G, uint32_t t, uint32_t local, uint32_t* nb) {
   const uint32_t c = t * 512u + local;
   const int lx = local & 7, ly = (local >> 3) & 7, lz = local >> 6;
@@ -36,89 +40,87 @@ __device__ __forceinline__ void neighbours(const PGeo& G, uint32_t t, uint32_t l
   nb[5] = lz < 7 ? c + 64u : (tk + 1 < G.tz ? c + slab - 448u : c);
 }
 
-// one colour sweep in FP32 (same arithmetic as the FLIP step's k_sor)
-__global__ void __launch_bounds__(256) k_ps_sor32(PGeo G, const uint32_t* __restrict__ tiles, uint32_t nT, const uint16_t* __restrict__ info,
-                                                  float* __restrict__ p, const float* __restrict__ rhs, float omega, uint32_t color) {
-  const int lz = threadIdx.x >> 5, ly = (threadIdx.x >> 2) & 7;
-  const int lx = 2 * (threadIdx.x & 3) + (int)((ly + lz + color) & 1);
-  const uint32_t local = (uint32_t)(lx + 8 * (ly + 8 * lz));
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t t = tiles[a], c = t * 512u + local;
-    uint32_t nb[6];
-    neighbours(G, t, local, nb);
-    const uint32_t in = info[c];
-    const float p0 = p[c], r0 = rhs[c];
-    const float q0 = p[nb[0]], q1 = p[nb[1]], q2 = p[nb[2]], q3 = p[nb[3]], q4 = p[nb[4]], q5 = p[nb[5]];
-    if (!(in & 0x8000u)) continue;
-    const uint32_t nns = (in >> 8) & 7u;
-    if (nns == 0u) { p[c] = 0.0f; continue; }
-    float sum = 0.0f;
-    if (in & 1u) sum += q0;
-    if (in & 2u) sum += q1;
-    if (in & 4u) sum += q2;
-    if (in & 8u) sum += q3;
-    if (in & 16u) sum += q4;
-    if (in & 32u) sum += q5;
-    const float pg = (r0 + sum) / (float)nns;
-    p[c] = p0 + omega * (pg - p0);
-  }
+// position of local cell l inside its slot
+__host__ __device__ __forceinline__ uint32_t splitIdx(uint32_t l) {
+  const uint32_t lx = l & 7u, ly = (l >> 3) & 7u, lz = l >> 6;
+  return ((lx + ly + lz) & 1u) * 256u + (lx >> 1) + 4u * (ly + 8u * lz);
 }
-// one colour sweep in FP64
-__global__ void __launch_bounds__(256) k_ps_sor64(PGeo G, const uint32_t* __restrict__ tiles, uint32_t nT, const uint16_t* __restrict__ info,
-                                                  double* __restrict__ p, const double* __restrict__ rhs, double omega, uint32_t color) {
-  const int lz = threadIdx.x >> 5, ly = (threadIdx.x >> 2) & 7;
-  const int lx = 2 * (threadIdx.x & 3) + (int)((ly + lz + color) & 1);
-  const uint32_t local = (uint32_t)(lx + 8 * (ly + 8 * lz));
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t t = tiles[a], c = t * 512u + local;
-    uint32_t nb[6];
-    neighbours(G, t, local, nb);
-    const uint32_t in = info[c];
-    const double p0 = p[c], r0 = rhs[c];
-    const double q0 = p[nb[0]], q1 = p[nb[1]], q2 = p[nb[2]], q3 = p[nb[3]], q4 = p[nb[4]], q5 = p[nb[5]];
-    if (!(in & 0x8000u)) continue;
-    const uint32_t nns = (in >> 8) & 7u;
-    if (nns == 0u) { p[c] = 0.0; continue; }
-    double sum = 0.0;
-    if (in & 1u) sum += q0;
-    if (in & 2u) sum += q1;
-    if (in & 4u) sum += q2;
-    if (in & 8u) sum += q3;
-    if (in & 16u) sum += q4;
-    if (in & 32u) sum += q5;
-    const double pg = (r0 + sum) / (double)nns;
-    p[c] = p0 + omega * (pg - p0);
+// compact index of the face neighbour of local cell l of slot a in direction dir (-x, +x, -y, +y, -z, +z)
+__device__ __forceinline__ uint32_t nbIdx(const uint32_t* __restrict__ nbs, uint32_t a, uint32_t l, int dir) {
+  const uint32_t lx = l & 7u, ly = (l >> 3) & 7u, lz = l >> 6;
+  uint32_t sl = a, nl = l;
+  switch (dir) {
+    case 0: if (lx > 0) nl = l - 1u; else { sl = nbs[a * 6u]; nl = l + 7u; } break;
+    case 1: if (lx < 7) nl = l + 1u; else { sl = nbs[a * 6u + 1u]; nl = l - 7u; } break;
+    case 2: if (ly > 0) nl = l - 8u; else { sl = nbs[a * 6u + 2u]; nl = l + 56u; } break;
+    case 3: if (ly < 7) nl = l + 8u; else { sl = nbs[a * 6u + 3u]; nl = l - 56u; } break;
+    case 4: if (lz > 0) nl = l - 64u; else { sl = nbs[a * 6u + 4u]; nl = l + 448u; } break;
+    default: if (lz < 7) nl = l + 64u; else { sl = nbs[a * 6u + 5u]; nl = l - 448u; } break;
   }
+  return sl * 512u + splitIdx(nl);
 }
-// r = b - A x in FP64 for x in FP64 (x64) or FP32 (x32); per-tile sums of r^2 in cell order (and b^2 when asked)
+
+// one colour sweep (thread j: the colour's cell (lx / 2) + 4 (ly + 8 lz) = j), same arithmetic as the FLIP step's
 template <class T>
-__global__ void __launch_bounds__(512) k_ps_resid(PGeo G, const uint32_t* __restrict__ tiles, uint32_t nT, const uint16_t* __restrict__ info,
+__global__ void __launch_bounds__(256) k_ps_sor(uint32_t nT, const uint32_t* __restrict__ nbs, const uint16_t* __restrict__ info,
+                                                T* __restrict__ p, const T* __restrict__ rhs, T omega, uint32_t color) {
+  const uint32_t j = threadIdx.x, lz = j >> 5, ly = (j >> 2) & 7u;
+  const uint32_t lx = 2u * (j & 3u) + ((ly + lz + color) & 1u), row = j & ~3u;
+  const uint32_t own = color * 256u + j, oth = (color ^ 1u) * 256u;
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t* nb = nbs + a * 6u;
+    const uint32_t base = a * 512u + oth;
+    const uint32_t ixm = lx > 0 ? base + row + ((lx - 1u) >> 1) : nb[0] * 512u + oth + row + 3u;
+    const uint32_t ixp = lx < 7 ? base + row + ((lx + 1u) >> 1) : nb[1] * 512u + oth + row;
+    const uint32_t iym = ly > 0 ? base + j - 4u : nb[2] * 512u + oth + j + 28u;
+    const uint32_t iyp = ly < 7 ? base + j + 4u : nb[3] * 512u + oth + j - 28u;
+    const uint32_t izm = lz > 0 ? base + j - 32u : nb[4] * 512u + oth + j + 224u;
+    const uint32_t izp = lz < 7 ? base + j + 32u : nb[5] * 512u + oth + j - 224u;
+    const uint32_t c = a * 512u + own;
+    const uint32_t in = info[c];
+    const T p0 = p[c], r0 = rhs[c];
+    const T q0 = p[ixm], q1 = p[ixp], q2 = p[iym], q3 = p[iyp], q4 = p[izm], q5 = p[izp];
+    if (!(in & 0x8000u)) continue;
+    const uint32_t nns = (in >> 8) & 7u;
+    if (nns == 0u) { p[c] = (T)0; continue; }
+    T sum = (T)0;
+    if (in & 1u) sum += q0;
+    if (in & 2u) sum += q1;
+    if (in & 4u) sum += q2;
+    if (in & 8u) sum += q3;
+    if (in & 16u) sum += q4;
+    if (in & 32u) sum += q5;
+    const T pg = (r0 + sum) / (T)nns;
+    p[c] = p0 + omega * (pg - p0);
+  }
+}
+// r = b - A x in FP64 for x in FP64 or FP32; per-tile sums of r^2 (and b^2 when asked) over the cells in local order
+template <class T>
+__global__ void __launch_bounds__(512) k_ps_resid(uint32_t nT, const uint32_t* __restrict__ nbs, const uint16_t* __restrict__ info,
                                                   const T* __restrict__ x, const double* __restrict__ b, double* __restrict__ r,
                                                   double* __restrict__ tileR2, double* __restrict__ tileB2) {
   __shared__ double sr[512], sb[512];
   for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t t = tiles[a], c = t * 512u + threadIdx.x;
-    uint32_t nb[6];
-    neighbours(G, t, threadIdx.x, nb);
+    const uint32_t l = threadIdx.x, c = a * 512u + splitIdx(l);
     const uint32_t in = info[c];
     double rv = 0.0, bv = 0.0;
     if (in & 0x8000u) {
       const uint32_t nns = (in >> 8) & 7u;
       double s = 0.0;
-      for (int q = 0; q < 6; q++) if (in & (1u << q)) s += (double)x[nb[q]];
+      for (int q = 0; q < 6; q++) if (in & (1u << q)) s += (double)x[nbIdx(nbs, a, l, q)];
       bv = b[c];
       rv = bv - ((double)nns * (double)x[c] - s);
     }
     r[c] = rv;
-    sr[threadIdx.x] = rv * rv;
-    sb[threadIdx.x] = bv * bv;
+    sr[l] = rv * rv;
+    sb[l] = bv * bv;
     __syncthreads();
     // fixed-order tree over the tile's 512 cells
     for (int w = 256; w > 0; w >>= 1) {
-      if ((int)threadIdx.x < w) { sr[threadIdx.x] += sr[threadIdx.x + w]; sb[threadIdx.x] += sb[threadIdx.x + w]; }
+      if ((int)l < w) { sr[l] += sr[l + w]; sb[l] += sb[l + w]; }
       __syncthreads();
     }
-    if (threadIdx.x == 0) { tileR2[a] = sr[0]; if (tileB2) tileB2[a] = sb[0]; }
+    if (l == 0) { tileR2[a] = sr[0]; if (tileB2) tileB2[a] = sb[0]; }
     __syncthreads();
   }
 }
@@ -137,25 +139,18 @@ __global__ void __launch_bounds__(1024) k_ps_norms(const double* __restrict__ ti
   }
   if (threadIdx.x == 0) { out[0] = s1[0]; out[1] = s2[0]; }
 }
-// refinement helpers: inner right-hand side and zero start; correction x += e
-__global__ void k_ps_inner(const uint32_t* __restrict__ tiles, uint32_t nT, const double* __restrict__ r, float* __restrict__ rhs32, float* __restrict__ e) {
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t c = tiles[a] * 512u + threadIdx.x;
-    rhs32[c] = (float)r[c];
-    e[c] = 0.0f;
+// refinement helpers over all stored cells: inner right-hand side and zero start; correction x += e; FP32 -> FP64 copy
+__global__ void k_ps_inner(size_t n, const double* __restrict__ r, float* __restrict__ rhs32, float* __restrict__ e) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    rhs32[i] = (float)r[i];
+    e[i] = 0.0f;
   }
 }
-__global__ void k_ps_correct(const uint32_t* __restrict__ tiles, uint32_t nT, const float* __restrict__ e, double* __restrict__ x) {
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t c = tiles[a] * 512u + threadIdx.x;
-    x[c] = x[c] + (double)e[c];
-  }
+__global__ void k_ps_correct(size_t n, const float* __restrict__ e, double* __restrict__ x) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = x[i] + (double)e[i];
 }
-__global__ void k_ps_copy(const uint32_t* __restrict__ tiles, uint32_t nT, const float* __restrict__ p32, double* __restrict__ x) {
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t c = tiles[a] * 512u + threadIdx.x;
-    x[c] = (double)p32[c];
-  }
+__global__ void k_ps_copy(size_t n, const float* __restrict__ p32, double* __restrict__ x) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = (double)p32[i];
 }
 
 thread_local char g_serr[256] = "";
@@ -167,14 +162,14 @@ struct st_poisson {
   cudaStream_t stream = nullptr;
   int sms = 148;
   PGeo G{};
-  uint32_t open = 0, nT = 0;
-  size_t ncell = 0;
-  uint32_t* tiles = nullptr;
+  uint32_t open = 0, nT = 0, capT = 0;
+  std::vector<uint32_t> tiles;   // host copy: tile of each slot
+  uint32_t* nbs = nullptr;
   uint16_t* info = nullptr;
   float *p32 = nullptr, *rhs32 = nullptr;
   double *x64 = nullptr, *b64 = nullptr, *r64 = nullptr, *tileR2 = nullptr, *tileB2 = nullptr, *norms = nullptr;
-  double bnorm2 = 0.0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  size_t cells() const { return (size_t)nT * 512; }
 };
 
 #define SK(call)                                                                            \
@@ -186,14 +181,21 @@ struct st_poisson {
     }                                                                                       \
   } while (0)
 
+static void poisson_free(st_poisson* s) {
+  void* ptrs[] = {s->nbs, s->info, s->p32, s->rhs32, s->x64, s->b64, s->r64, s->tileR2, s->tileB2};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  s->nbs = nullptr; s->info = nullptr; s->p32 = s->rhs32 = nullptr; s->x64 = s->b64 = s->r64 = s->tileR2 = s->tileB2 = nullptr;
+  s->capT = 0;
+}
+
 extern "C" {
 
 void st_poisson_destroy(st_poisson* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  void* ptrs[] = {s->tiles, s->info, s->p32, s->rhs32, s->x64, s->b64, s->r64, s->tileR2, s->tileB2, s->norms};
-  for (void* p : ptrs) if (p) cudaFree(p);
+  poisson_free(s);
+  if (s->norms) cudaFree(s->norms);
   if (s->e0) cudaEventDestroy(s->e0);
   if (s->e1) cudaEventDestroy(s->e1);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -209,18 +211,10 @@ st_status st_poisson_create(const st_poisson_desc* d, st_poisson** out) {
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
   s->G = PGeo{d->n[0], d->n[1], d->n[2], (d->n[0] + 7) / 8, (d->n[1] + 7) / 8, (d->n[2] + 7) / 8};
   s->open = d->open;
-  const size_t T = (size_t)s->G.tx * s->G.ty * s->G.tz;
-  s->ncell = T * 512;
   cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-  auto A = [&](void** p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(b, 16)); };
-  A((void**)&s->tiles, T * 4); A((void**)&s->info, s->ncell * 2); A((void**)&s->p32, s->ncell * 4); A((void**)&s->rhs32, s->ncell * 4);
-  A((void**)&s->x64, s->ncell * 8); A((void**)&s->b64, s->ncell * 8); A((void**)&s->r64, s->ncell * 8);
-  A((void**)&s->tileR2, T * 8); A((void**)&s->tileB2, T * 8); A((void**)&s->norms, 16);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&s->norms, 4 * sizeof(double));
   if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
   if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->p32, 0, s->ncell * 4, s->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->x64, 0, s->ncell * 8, s->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
     snprintf(g_serr, sizeof(g_serr), "create: %s", cudaGetErrorString(e)); st::set_error_text(g_serr);
     st_poisson_destroy(s);
@@ -236,9 +230,6 @@ st_status st_poisson_set(st_poisson* s, const uint8_t* type, const double* rhs) 
   SK(cudaSetDevice(s->device));
   const PGeo& G = s->G;
   const size_t T = (size_t)G.tx * G.ty * G.tz;
-  std::vector<uint16_t> info(s->ncell, 0);
-  std::vector<double> b(s->ncell, 0.0);
-  std::vector<uint8_t> tileOn(T, 0);
   auto ty = [&](long i, long j, long k) -> int {   // ctypeOf (src/flip/wgsl-core.js:104-112)
     if (i < 0) return (s->open & 1u) ? 0 : 2;
     if (i >= (long)G.nx) return (s->open & 2u) ? 0 : 2;
@@ -248,33 +239,67 @@ st_status st_poisson_set(st_poisson* s, const uint8_t* type, const double* rhs) 
     if (k >= (long)G.nz) return (s->open & 32u) ? 0 : 2;
     return type[(size_t)i + G.nx * ((size_t)j + (size_t)G.ny * k)];
   };
+  // the tiles holding fluid, ascending, and each one's slot
+  std::vector<uint32_t> slot(T, 0xffffffffu);
   for (long k = 0; k < (long)G.nz; k++)
     for (long j = 0; j < (long)G.ny; j++)
-      for (long i = 0; i < (long)G.nx; i++) {
-        const size_t o = (size_t)i + G.nx * ((size_t)j + (size_t)G.ny * k);
-        if (type[o] != 1) continue;
-        const size_t t = (size_t)(i >> 3) + G.tx * ((size_t)(j >> 3) + (size_t)G.ty * (k >> 3));
-        const size_t c = t * 512 + (i & 7) + 8 * ((j & 7) + 8 * (k & 7));
-        const long q[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
-        uint32_t mask = 0, nns = 0;
-        for (int a = 0; a < 6; a++) {
-          const int tq = ty(q[a][0], q[a][1], q[a][2]);
-          if (tq != 2) nns++;
-          if (tq == 1) mask |= 1u << a;
-        }
-        info[c] = (uint16_t)(0x8000u | (nns << 8) | mask);
-        b[c] = rhs[o];
-        tileOn[t] = 1;
+      for (long i = 0; i < (long)G.nx; i++)
+        if (type[(size_t)i + G.nx * ((size_t)j + (size_t)G.ny * k)] == 1)
+          slot[(size_t)(i >> 3) + G.tx * ((size_t)(j >> 3) + (size_t)G.ty * (k >> 3))] = 0;
+  s->tiles.clear();
+  for (size_t t = 0; t < T; t++) if (slot[t] == 0) { slot[t] = (uint32_t)s->tiles.size(); s->tiles.push_back((uint32_t)t); }
+  const uint32_t nT = (uint32_t)s->tiles.size();
+  const size_t n = (size_t)nT * 512;
+  std::vector<uint16_t> info(n, 0);
+  std::vector<double> b(n, 0.0);
+  std::vector<uint32_t> nbs((size_t)nT * 6);
+  for (uint32_t a = 0; a < nT; a++) {
+    const uint32_t t = s->tiles[a], tt = t / G.tx, ti = t % G.tx, tj = tt % G.ty, tk = tt / G.ty;
+    const long nt[6] = {ti > 0 ? (long)t - 1 : -1, ti + 1 < G.tx ? (long)t + 1 : -1, tj > 0 ? (long)(t - G.tx) : -1,
+                        tj + 1 < G.ty ? (long)(t + G.tx) : -1, tk > 0 ? (long)(t - G.tx * G.ty) : -1,
+                        tk + 1 < G.tz ? (long)(t + G.tx * G.ty) : -1};
+    for (int d = 0; d < 6; d++) nbs[(size_t)a * 6 + d] = (nt[d] >= 0 && slot[nt[d]] != 0xffffffffu) ? slot[nt[d]] : a;
+    for (uint32_t l = 0; l < 512; l++) {
+      const long i = (long)ti * 8 + (l & 7), j = (long)tj * 8 + ((l >> 3) & 7), k = (long)tk * 8 + (l >> 6);
+      if (i >= (long)G.nx || j >= (long)G.ny || k >= (long)G.nz) continue;
+      const size_t o = (size_t)i + G.nx * ((size_t)j + (size_t)G.ny * k);
+      if (type[o] != 1) continue;
+      const long q[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+      uint32_t mask = 0, nns = 0;
+      for (int d = 0; d < 6; d++) {
+        const int tq = ty(q[d][0], q[d][1], q[d][2]);
+        if (tq != 2) nns++;
+        if (tq == 1) mask |= 1u << d;
       }
-  std::vector<uint32_t> tiles;
-  for (size_t t = 0; t < T; t++) if (tileOn[t]) tiles.push_back((uint32_t)t);
-  s->nT = (uint32_t)tiles.size();
+      const size_t c = (size_t)a * 512 + splitIdx(l);
+      info[c] = (uint16_t)(0x8000u | (nns << 8) | mask);
+      b[c] = rhs[o];
+    }
+  }
+  if (nT > s->capT) {
+    SK(cudaStreamSynchronize(s->stream));
+    poisson_free(s);
+    const size_t m = (size_t)std::max(nT, 1u) * 512;
+    SK(cudaMalloc((void**)&s->nbs, (size_t)std::max(nT, 1u) * 6 * 4));
+    SK(cudaMalloc((void**)&s->info, m * 2));
+    SK(cudaMalloc((void**)&s->p32, m * 4));
+    SK(cudaMalloc((void**)&s->rhs32, m * 4));
+    SK(cudaMalloc((void**)&s->x64, m * 8));
+    SK(cudaMalloc((void**)&s->b64, m * 8));
+    SK(cudaMalloc((void**)&s->r64, m * 8));
+    SK(cudaMalloc((void**)&s->tileR2, (size_t)std::max(nT, 1u) * 8));
+    SK(cudaMalloc((void**)&s->tileB2, (size_t)std::max(nT, 1u) * 8));
+    s->capT = std::max(nT, 1u);
+  }
+  s->nT = nT;
   cudaStream_t q = s->stream;
-  SK(cudaMemcpyAsync(s->info, info.data(), s->ncell * 2, cudaMemcpyHostToDevice, q));
-  SK(cudaMemcpyAsync(s->b64, b.data(), s->ncell * 8, cudaMemcpyHostToDevice, q));
-  SK(cudaMemcpyAsync(s->tiles, tiles.data(), std::max<size_t>(tiles.size(), 1) * 4, cudaMemcpyHostToDevice, q));
-  SK(cudaMemsetAsync(s->p32, 0, s->ncell * 4, q));
-  SK(cudaMemsetAsync(s->x64, 0, s->ncell * 8, q));
+  if (nT) {
+    SK(cudaMemcpyAsync(s->info, info.data(), n * 2, cudaMemcpyHostToDevice, q));
+    SK(cudaMemcpyAsync(s->b64, b.data(), n * 8, cudaMemcpyHostToDevice, q));
+    SK(cudaMemcpyAsync(s->nbs, nbs.data(), (size_t)nT * 6 * 4, cudaMemcpyHostToDevice, q));
+    SK(cudaMemsetAsync(s->p32, 0, n * 4, q));
+    SK(cudaMemsetAsync(s->x64, 0, n * 8, q));
+  }
   SK(cudaStreamSynchronize(q));
   return ST_OK;
 }
@@ -290,6 +315,13 @@ static st_status norms(st_poisson* s, bool withB, double* r2, double* b2) {
   return ST_OK;
 }
 
+static void sweeps32(st_poisson* s, int grid, float om, int iters) {
+  for (int k = 0; k < iters; k++) {
+    k_ps_sor<float><<<grid, 256, 0, s->stream>>>(s->nT, s->nbs, s->info, s->p32, s->rhs32, om, 0u);
+    k_ps_sor<float><<<grid, 256, 0, s->stream>>>(s->nT, s->nbs, s->info, s->p32, s->rhs32, om, 1u);
+  }
+}
+
 // Solve from zero. mode 0: FP32 SOR (the residual is measured in FP64 every check_every iterations);
 // 1: FP32 SOR inside FP64 refinement (inner_sweeps iterations per refinement); 2: FP64 SOR.
 st_status st_poisson_solve(st_poisson* s, const st_poisson_opts* o, st_poisson_result* res) {
@@ -298,46 +330,45 @@ st_status st_poisson_solve(st_poisson* s, const st_poisson_opts* o, st_poisson_r
   memset(res, 0, sizeof(*res));
   if (!s->nT) { res->converged = 1; return ST_OK; }
   cudaStream_t q = s->stream;
+  const size_t n = s->cells();
   const int grid = std::max(1, std::min<int>(s->sms * 8, (int)s->nT)), grid4 = std::max(1, std::min<int>(s->sms * 4, (int)s->nT));
+  const int gridE = s->sms * 8;
   const int check = std::max(1, o->check_every), maxIt = std::max(1, o->max_sweeps);
   const float om = o->omega;
-  SK(cudaMemsetAsync(s->p32, 0, s->ncell * 4, q));
-  SK(cudaMemsetAsync(s->x64, 0, s->ncell * 8, q));
+  SK(cudaMemsetAsync(s->p32, 0, n * 4, q));
+  SK(cudaMemsetAsync(s->x64, 0, n * 8, q));
   // ||b|| once, from the residual of x = 0
-  k_ps_resid<double><<<grid4, 512, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->x64, s->b64, s->r64, s->tileR2, s->tileB2);
+  k_ps_resid<double><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, s->r64, s->tileR2, s->tileB2);
   double r2 = 0, b2 = 0;
   st_status st = norms(s, true, &r2, &b2);
   if (st != ST_OK) return st;
-  s->bnorm2 = b2;
   const double bn = std::sqrt(b2);
   if (bn == 0.0) { res->converged = 1; return ST_OK; }
   SK(cudaEventRecord(s->e0, q));
   int it = 0, ref = 0;
   double rel = 1.0;
   if (o->mode == 0) {
-    k_ps_inner<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->b64, s->rhs32, s->p32);
+    k_ps_inner<<<gridE, 256, 0, q>>>(n, s->b64, s->rhs32, s->p32);
     while (it < maxIt) {
-      for (int k = 0; k < check && it < maxIt; k++, it++) {
-        k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, om, 0u);
-        k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, om, 1u);
-      }
-      k_ps_resid<float><<<grid4, 512, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->b64, s->r64, s->tileR2, nullptr);
+      const int k = std::min(check, maxIt - it);
+      sweeps32(s, grid, om, k);
+      it += k;
+      k_ps_resid<float><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->p32, s->b64, s->r64, s->tileR2, nullptr);
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
       rel = std::sqrt(r2) / bn;
       if (rel <= o->tol) break;
     }
-    k_ps_copy<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->p32, s->x64);
+    k_ps_copy<<<gridE, 256, 0, q>>>(n, s->p32, s->x64);
   } else if (o->mode == 1) {
     const int inner = std::max(1, o->inner_sweeps);
     while (it < maxIt) {
-      k_ps_inner<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->r64, s->rhs32, s->p32);
-      for (int k = 0; k < inner && it < maxIt; k++, it++) {
-        k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, om, 0u);
-        k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, om, 1u);
-      }
-      k_ps_correct<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->p32, s->x64);
-      k_ps_resid<double><<<grid4, 512, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
+      k_ps_inner<<<gridE, 256, 0, q>>>(n, s->r64, s->rhs32, s->p32);
+      const int k = std::min(inner, maxIt - it);
+      sweeps32(s, grid, om, k);
+      it += k;
+      k_ps_correct<<<gridE, 256, 0, q>>>(n, s->p32, s->x64);
+      k_ps_resid<double><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
       ref++;
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
@@ -347,10 +378,10 @@ st_status st_poisson_solve(st_poisson* s, const st_poisson_opts* o, st_poisson_r
   } else if (o->mode == 2) {
     while (it < maxIt) {
       for (int k = 0; k < check && it < maxIt; k++, it++) {
-        k_ps_sor64<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->x64, s->b64, (double)om, 0u);
-        k_ps_sor64<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->x64, s->b64, (double)om, 1u);
+        k_ps_sor<double><<<grid, 256, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, (double)om, 0u);
+        k_ps_sor<double><<<grid, 256, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, (double)om, 1u);
       }
-      k_ps_resid<double><<<grid4, 512, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
+      k_ps_resid<double><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
       rel = std::sqrt(r2) / bn;
@@ -379,35 +410,37 @@ st_status st_poisson_sweeps32(st_poisson* s, float omega, int32_t iters, float* 
   if (ms) *ms = 0.0f;
   if (!s->nT) return ST_OK;
   cudaStream_t q = s->stream;
-  const int grid = std::max(1, std::min<int>(s->sms * 8, (int)s->nT)), grid4 = std::max(1, std::min<int>(s->sms * 4, (int)s->nT));
-  k_ps_inner<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->b64, s->rhs32, s->p32);
+  const size_t n = s->cells();
+  const int grid = std::max(1, std::min<int>(s->sms * 8, (int)s->nT)), gridE = s->sms * 8;
+  k_ps_inner<<<gridE, 256, 0, q>>>(n, s->b64, s->rhs32, s->p32);
   SK(cudaEventRecord(s->e0, q));
-  for (int k = 0; k < iters; k++) {
-    k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, omega, 0u);
-    k_ps_sor32<<<grid, 256, 0, q>>>(s->G, s->tiles, s->nT, s->info, s->p32, s->rhs32, omega, 1u);
-  }
+  sweeps32(s, grid, omega, iters);
   SK(cudaEventRecord(s->e1, q));
-  k_ps_copy<<<grid4, 512, 0, q>>>(s->tiles, s->nT, s->p32, s->x64);
+  k_ps_copy<<<gridE, 256, 0, q>>>(n, s->p32, s->x64);
   SK(cudaStreamSynchronize(q));
   SK(cudaGetLastError());
   if (ms) SK(cudaEventElapsedTime(ms, s->e0, s->e1));
   return ST_OK;
 }
 
-// the solution (FP64, dense, x fastest) and the relative residual of a given dense FP64 field
+// the solution (FP64, dense, x fastest; 0 outside the tiles holding fluid)
 st_status st_poisson_read(st_poisson* s, double* p) {
   if (!s || !p) return ST_BAD_ARG;
   SK(cudaSetDevice(s->device));
   const PGeo& G = s->G;
-  std::vector<double> x(s->ncell);
-  SK(cudaMemcpyAsync(x.data(), s->x64, s->ncell * 8, cudaMemcpyDeviceToHost, s->stream));
+  memset(p, 0, sizeof(double) * (size_t)G.nx * G.ny * G.nz);
+  if (!s->nT) return ST_OK;
+  std::vector<double> x(s->cells());
+  SK(cudaMemcpyAsync(x.data(), s->x64, s->cells() * 8, cudaMemcpyDeviceToHost, s->stream));
   SK(cudaStreamSynchronize(s->stream));
-  for (size_t k = 0; k < G.nz; k++)
-    for (size_t j = 0; j < G.ny; j++)
-      for (size_t i = 0; i < G.nx; i++) {
-        const size_t t = (i >> 3) + G.tx * ((j >> 3) + (size_t)G.ty * (k >> 3));
-        p[i + G.nx * (j + (size_t)G.ny * k)] = x[t * 512 + (i & 7) + 8 * ((j & 7) + 8 * (k & 7))];
-      }
+  for (uint32_t a = 0; a < s->nT; a++) {
+    const uint32_t t = s->tiles[a], tt = t / G.tx, ti = t % G.tx, tj = tt % G.ty, tk = tt / G.ty;
+    for (uint32_t l = 0; l < 512; l++) {
+      const size_t i = (size_t)ti * 8 + (l & 7), j = (size_t)tj * 8 + ((l >> 3) & 7), k = (size_t)tk * 8 + (l >> 6);
+      if (i >= G.nx || j >= G.ny || k >= G.nz) continue;
+      p[i + G.nx * (j + (size_t)G.ny * k)] = x[(size_t)a * 512 + splitIdx(l)];
+    }
+  }
   return ST_OK;
 }
 
