@@ -51,6 +51,8 @@ def parse():
         a.steps, a.warmup = 5, 3
     if a.workload.startswith("batch_") and "--steps" not in sys.argv:
         a.steps = 100
+    if a.workload.startswith("diff_") and "--steps" not in sys.argv:
+        a.steps, a.warmup = 3, 1
     return a
 
 
@@ -578,6 +580,73 @@ def run_batch_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- differentiable rollout
+def run_diff(a):
+    """Gradient of the 32-step differentiable rollout (forward with checkpoints, recompute, adjoint) in FP32: value =
+    particle-steps/s of the whole gradient evaluation; beside it the forward alone, and the gradient's error against
+    the FP64 adjoint and against FP64 central differences (eps 1e-3) on six parameters."""
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    from splashtank_b200 import scenes
+    n = int(a.workload.rsplit("_", 1)[1])
+    d = scenes.DiffDam(n=n)
+    p0 = d.params
+    s32 = d.make(device=local)
+    stream = torch.cuda.ExternalStream(s32.stream(), device=local)
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    for _ in range(a.warmup):
+        s32.forward(p0)
+        s32.backward()
+    clocks = Clocks(local)
+    ms_grad = timed(lambda: (s32.forward(p0), s32.backward()), a.steps)
+    clk = clocks.stop()
+    ms_fwd = timed(lambda: s32.forward(p0), a.steps)
+    mem, cg = s32.stats()
+    loss32 = s32.forward(p0)
+    g32 = s32.backward()
+    s32.destroy()
+    s64 = d.make(fp64=True, device=local)
+    loss64 = s64.forward(p0)
+    g64 = s64.backward()
+    idx = [6, 7, 8, 15, 24, 25]
+    fd = []
+    for i in idx:
+        e = np.zeros(27)
+        e[i] = 1e-3
+        fd.append((s64.forward(p0 + e, record=False) - s64.forward(p0 - e, record=False)) / 2e-3)
+    fd = np.array(fd)
+    s64.destroy()
+    ps = d.pos.shape[0] * d.steps
+    if rank == 0:
+        line = {"metric": "gradient particle-steps/s (forward + adjoint)", "value": ps / (ms_grad * 1e-3), "unit": "particle-steps/s",
+                "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_grad, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (f64 reference)", "data": "synthetic (seeded)",
+                "config": {"workload": a.workload, "grid": [n] * 3, "particles": int(d.pos.shape[0]), "rollout_steps": d.steps,
+                           "checkpoint_every": d.ckpt, "params": "8 collider keyframes (xyz) + initial velocity",
+                           "collider": "analytic box, half extents 0.06 x 0.12 x 0.25", "note": "ms_per_step: one whole gradient (rollout)"},
+                "forward_ms": ms_fwd, "gradient_ms": ms_grad, "device_bytes": int(mem), "cg_iterations_last": int(cg),
+                "loss_f32": loss32, "loss_f64": loss64,
+                "grad_check": {"f32_vs_f64_adjoint_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+                               "f64_adjoint_vs_fd_max_rel": float(np.max(np.abs(g64[idx] - fd)) / max(np.max(np.abs(fd)), 1e-300)),
+                               "params_checked": idx, "fd_eps": 1e-3},
+                "clocks": clk, "roofline": None, "gpu_launches": None,
+                "e2e": {"value": ps / (ms_grad * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": 27 * 8, "d2h_bytes_per_step": 27 * 8,
+                        "note": "parameters up and gradient back through the C ABI are inside the timed calls"},
+                "cpu_baseline": None, "cpu_baseline_note": "the reference has no gradient; no CPU adjoint exists to time"}
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- our arm
 def main():
     a = parse()
@@ -585,6 +654,11 @@ def main():
         return run_pressure_reference(a) if a.impl == "reference" else run_pressure(a)
     if a.workload.startswith("batch_"):
         return run_batch_reference(a) if a.impl == "reference" else run_batch(a)
+    if a.workload.startswith("diff_"):
+        if a.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no differentiable rollout"}), flush=True)
+            return None
+        return run_diff(a)
     if a.impl == "reference":
         return run_reference(a)
     world = int(os.environ.get("WORLD_SIZE", "1"))

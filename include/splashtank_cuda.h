@@ -306,6 +306,40 @@ void* st_batch_stream(st_batch* b);
 /* kernels launched by batch steps so far */
 uint64_t st_batch_launches(st_batch* b);
 
+/* ---- differentiable rollout and its adjoint (no reference counterpart: the reference has no gradients) ----
+ * A FLIP rollout on a dense n^3 MAC grid over the unit box (P2G, gravity, collider and wall face velocities, pressure
+ * projection by preconditioned conjugate gradients, FLIP/PIC G2P, advection, analytic box collider push-out, wall
+ * clamp) whose loss is sum over cells of (splatted particle density - target)^2. Parameters (27 doubles): the box
+ * collider's centre at 8 keyframes spread evenly over the rollout (xyz each, linear in between), then the initial
+ * fluid velocity. A recording forward pass fixes the discrete decisions (cell types, faces with mass, collider and
+ * wall contacts, the piece of the box's distance field each particle is on); st_diff_backward returns the exact gradient of the rollout with those decisions held, by a
+ * hand-written adjoint with checkpoint-and-recompute every ckpt_every steps; a frozen forward pass (record 0)
+ * evaluates that same function for finite differences. fp64 selects double precision throughout. */
+typedef struct st_diff st_diff;
+typedef struct st_diff_desc {
+  uint32_t size;          /* sizeof(st_diff_desc) */
+  uint32_t n;             /* cells per axis (cell size 1/n) */
+  uint32_t steps;
+  uint32_t ckpt_every;    /* particle checkpoint interval of the reverse pass */
+  int32_t fp64;
+  int32_t device;
+  float dt, flip, g;      /* time step, FLIP ratio, gravity */
+  float q0;               /* collider push-out distance */
+  float margin;           /* particles stay in [margin, 1 - margin] */
+  float box_half[3];      /* collider half extents */
+  uint32_t cg_maxit;
+  float cg_tol;           /* relative residual of the pressure solves */
+} st_diff_desc;
+/* pos3: initial particle positions; target: n^3 densities, x fastest */
+st_status st_diff_create(const st_diff_desc* d, const float* pos3, uint32_t np, const float* target, st_diff** out);
+void st_diff_destroy(st_diff* s);
+st_status st_diff_forward(st_diff* s, const double* params, int32_t record, double* loss);
+/* gradient of the loss at the parameters of the last recording forward pass */
+st_status st_diff_backward(st_diff* s, double* grad);
+/* device bytes held; conjugate-gradient iterations of the last forward or backward call */
+st_status st_diff_stats(st_diff* s, uint64_t* device_bytes, int32_t* cg_iters);
+void* st_diff_stream(st_diff* s);
+
 /* ---- pressure residual that allocates nothing (no reference counterpart: the reference measures no residual) ----
  * ||b - A x|| / ||b|| of the pressure system above, in FP64, on arrays the caller owns on the device, in the tile-major
  * layout (tile t = ti + tx (tj + ty tk) with tx = ceil(n[0]/8) ..., cell t*512 + lx + 8 (ly + 8 lz)). For callers that

@@ -149,6 +149,20 @@ BATCH_FUNCS = [
     ("batch_stream", C.c_void_p, [C.c_void_p]),
     ("batch_launches", C.c_uint64, [C.c_void_p]),
 ]
+class DiffDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("n", C.c_uint32), ("steps", C.c_uint32), ("ckpt_every", C.c_uint32), ("fp64", C.c_int32),
+                ("device", C.c_int32), ("dt", C.c_float), ("flip", C.c_float), ("g", C.c_float), ("q0", C.c_float), ("margin", C.c_float),
+                ("box_half", C.c_float * 3), ("cg_maxit", C.c_uint32), ("cg_tol", C.c_float)]
+
+
+DIFF_FUNCS = [
+    ("diff_create", C.c_int, [C.POINTER(DiffDesc), f32p, C.c_uint32, f32p, C.POINTER(C.c_void_p)]),
+    ("diff_destroy", None, [C.c_void_p]),
+    ("diff_forward", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double)]),
+    ("diff_backward", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("diff_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
+    ("diff_stream", C.c_void_p, [C.c_void_p]),
+]
 NOALLOC_FUNCS = [
     ("poisson_residual_noalloc", C.c_int, [C.POINTER(PoissonSystem), C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]),

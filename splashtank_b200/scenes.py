@@ -209,3 +209,41 @@ class BatchTanks:
         o = dict(self.opts)
         o["cols"] = runner.colliders(self.dt, st, 20.0)
         return o
+
+
+def splat_density(pos, n):
+    """Cell-centred trilinear density of particles on an n^3 grid over the unit box (x fastest), corners clamped."""
+    g = pos.astype(np.float64) * n - 0.5
+    f0 = np.floor(g)
+    fr = g - f0
+    i0 = f0.astype(np.int64)
+    rho = np.zeros(n ** 3, np.float64)
+    for c in range(8):
+        o = np.array([(c >> d) & 1 for d in range(3)])
+        ii = np.clip(i0 + o, 0, n - 1)
+        w = np.prod(np.where(o == 1, fr, 1.0 - fr), axis=1)
+        rho += np.bincount(ii[:, 0] + n * (ii[:, 1] + n * ii[:, 2]), weights=w, minlength=n ** 3)
+    return rho.astype(np.float32)
+
+
+class DiffDam:
+    """Differentiation workload: n^3 dam break on the unit box (water where x < 0.4, y < 0.6, 8 particles per cell,
+    seeded jitter) with a moving box collider (half extents 0.06 x 0.12 x 0.25) whose centre follows 8 keyframes from
+    (0.75, 0.3, 0.5) towards the water; loss against a seeded target density: the starting water moved by a seeded
+    offset. Parameters: the keyframes (24) then the initial fluid velocity (3)."""
+
+    def __init__(self, n=128, seed=21, steps=32, ckpt=8, fx=0.4, fy=0.6):
+        self.n, self.steps, self.ckpt = n, steps, ckpt
+        h = 1.0 / n
+        rng = np.random.default_rng(seed)
+        cells = box_cells((n, n, n), lambda ci, cj, ck: (ci * h < fx) & (cj * h < fy))
+        self.pos = seed_cells(cells, h, rng, 0.0, 0.0, 0.0)
+        keys = np.array([[0.75 - 0.04 * k, 0.3, 0.5] for k in range(8)], np.float64)
+        self.params = np.concatenate([keys.ravel(), [0.2, 0.0, 0.0]])
+        off = np.array([rng.uniform(0.02, 0.08), -rng.uniform(0.0, 0.05), rng.uniform(-0.03, 0.03)])
+        moved = np.clip(self.pos + off.astype(np.float32), 0.5 * h, 1 - 0.5 * h)
+        self.target = splat_density(moved, n)
+
+    def make(self, **kw):
+        from .diff import DiffRollout
+        return DiffRollout(self.n, self.pos, self.target, self.steps, ckpt_every=self.ckpt, **kw)
