@@ -28,6 +28,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
+NCU_TRAFFIC = {"g2p": {"bytes": 180489216 + 100843520, "particles": 4669521},
+               "p2g": {"bytes": 209696000 + 137505280, "particles": 4669521}}
 FALLBACK_HBM = 6650.0
 
 
@@ -167,16 +170,9 @@ def roofline(stage_ms, nsteps, n, cells, fluid, iters, peak, peak_src):
         return None
     per_launch_ms = stage_ms[dom] / (nsteps * launches)
     achieved = b / (per_launch_ms * 1e-3) / 1e9
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        try:
-            t = json.load(open(tf))
-            ent = t.get(dom)
-            if ent and ent.get("particles"):
-                traffic = ent["bytes_per_launch"] * (n / ent["particles"])
-        except Exception:
-            traffic = None
+    # DRAM bytes of one launch from an ncu capture of a smaller tank, scaled by particles (traffic grows with them)
+    ent = NCU_TRAFFIC.get(dom)
+    traffic = int(ent["bytes"] * n / ent["particles"]) if ent else None
     return {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": traffic,
             "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per_launch_ms, 5),
