@@ -280,6 +280,26 @@ st_status st_poisson_sweeps32(st_poisson* s, float omega, int32_t iters, float* 
 st_status st_poisson_read(st_poisson* s, double* p);
 void* st_poisson_stream(st_poisson* s);
 
+/* ---- frames and bake measurements ----
+ * The particles as a cache frame (packFrameBuf, src/gpu.js:525-560; format of writeCacheParts, src/shared.js:688-705),
+ * packed on the device in id order: pos 3 x uint16 per point across the box, spd one byte (16ths of speed x vs, at most
+ * 191, 255 = gone), fm one byte (white-water level x 17). *n: points in the frame (the last live id + 1); *any_foam:
+ * whether any point has white water (the frame stores fm only then). Arrays need room for cap points; at most
+ * min(cap, n) are written. vs: metres per scene unit (the bake's scale; 0 means 1). */
+st_status st_flip_read_frame(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap, uint32_t* n,
+                             int32_t* any_foam);
+/* bakeDiag (src/flip/bake.js:60-83) of the current particles, on the device: the same counts; sums agree to rounding. */
+typedef struct st_bake_diag {
+  uint32_t alive, gone, non_finite, outside_box, at_speed_limit, foamy;
+  double mean_speed, max_speed, mean_foam;
+  double center[3];
+  int32_t has_bbox;
+  double bbox[6];       /* x0, y0, z0, x1, y1, z1 of the live points */
+  uint32_t height_hist[16];
+} st_bake_diag;
+/* vcap: the step's speed limit (o.vmax; 0 means 14) */
+st_status st_flip_bake_diag(st_flip* s, float vcap, st_bake_diag* out);
+
 /* ---- launch shape of a tank's kernels (no reference counterpart: WebGPU picks no grid sizes) ----
  * CTAs per SM of the per-tile kernels: heavy (p2g, g2p; default 8), light (classify, normalise, project, narrow band;
  * default 4) and the pressure sweeps (default 8), each capped at the tile count. Results do not depend on them; an

@@ -116,7 +116,16 @@ FLIP_FUNCS = [
     ("flip_load_state", C.c_int, [C.c_void_p, f32p, f32p, u32p, C.c_uint32, C.c_double, C.c_uint32]),
     ("flip_nb_fills", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p, C.c_uint32, C.c_uint32]),
 ]
+class BakeDiag(C.Structure):
+    _fields_ = [("alive", C.c_uint32), ("gone", C.c_uint32), ("non_finite", C.c_uint32), ("outside_box", C.c_uint32),
+                ("at_speed_limit", C.c_uint32), ("foamy", C.c_uint32), ("mean_speed", C.c_double), ("max_speed", C.c_double),
+                ("mean_foam", C.c_double), ("center", C.c_double * 3), ("has_bbox", C.c_int32), ("bbox", C.c_double * 6),
+                ("height_hist", C.c_uint32 * 16)]
+
+
 CUDA_ONLY_FUNCS = [
+    ("flip_read_frame", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, u8p, C.c_uint32, u32p, C.POINTER(C.c_int32)]),
+    ("flip_bake_diag", C.c_int, [C.c_void_p, C.c_float, C.POINTER(BakeDiag)]),
     ("flip_save_full", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("flip_load_full", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     ("flip_set_launch", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),

@@ -91,6 +91,8 @@ struct st_flip {
   float *cp = nullptr, *crhs = nullptr;
   uint16_t* cinfo = nullptr;
   uint32_t *nbs = nullptr, *slotOf = nullptr;
+  uint8_t* frame = nullptr;   // packed frame (allocated by the first st_flip_read_frame)
+  DiagAcc* diag = nullptr;
   float* wet = nullptr;
   float* sdf = nullptr;
   float4 *sPos = nullptr, *sVel = nullptr;
@@ -147,7 +149,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf};
+                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -629,6 +631,78 @@ st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t 
   CK(cudaMemcpyAsync(pos4, tmp, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
   if (vel4) CK(cudaMemcpyAsync(vel4, tmp + s->N, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+st_status st_flip_read_frame(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap, uint32_t* n,
+                             int32_t* any_foam) {
+  if (!s || !n) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  *n = 0;
+  if (any_foam) *any_foam = 0;
+  if (s->N == 0) return ST_OK;
+  if (!s->frame) {   // packed frame: 6 + 1 + 1 bytes per slot, plus 2 counters
+    CK(cudaMalloc((void**)&s->frame, (size_t)s->maxN * 8 + 16));
+  }
+  uint32_t* meta = reinterpret_cast<uint32_t*>(s->frame);
+  uint16_t* p16 = reinterpret_cast<uint16_t*>(s->frame + 16);
+  uint8_t* sp = s->frame + 16 + (size_t)s->maxN * 6;
+  uint8_t* f8 = sp + s->maxN;
+  float4* tmp = reinterpret_cast<float4*>(s->part[s->cur ^ 1]);
+  launch_unsort(s->part[s->cur], s->ids[s->cur], s->N, tmp, nullptr, s->stream);
+  FrameBox F{s->bx0, s->by0, s->bz0, 65535.0 / (s->bx1 - s->bx0), 65535.0 / (s->by1 - s->by0), 65535.0 / (s->bz1 - s->bz0),
+             16.0 * (vs != 0.0f ? (double)vs : 1.0)};
+  CK(cudaMemsetAsync(meta, 0, 8, s->stream));
+  launch_pack_frame(tmp, s->N, F, p16, sp, f8, meta, s->stream);
+  CK(cudaGetLastError());
+  uint32_t h[2];
+  CK(cudaMemcpyAsync(h, meta, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *n = h[0];
+  if (any_foam) *any_foam = (int32_t)h[1];
+  const uint32_t m = std::min(cap, h[0]);
+  if (m) {
+    if (pos) CK(cudaMemcpyAsync(pos, p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->stream));
+    if (spd) CK(cudaMemcpyAsync(spd, sp, m, cudaMemcpyDeviceToHost, s->stream));
+    if (fm && h[1]) CK(cudaMemcpyAsync(fm, f8, m, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return ST_OK;
+}
+
+st_status st_flip_bake_diag(st_flip* s, float vcap, st_bake_diag* out) {
+  if (!s || !out) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  memset(out, 0, sizeof(*out));
+  if (!s->diag) CK(cudaMalloc((void**)&s->diag, sizeof(DiagAcc)));
+  DiagAcc h{};
+  for (int k = 0; k < 3; k++) { h.mn[k] = ~0ull; h.mx[k] = 0; }
+  CK(cudaMemcpyAsync(s->diag, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
+  const double vc = vcap != 0.0f ? (double)vcap : 14.0;
+  DiagBox D{s->bx0, s->by0, s->bz0, s->bx1, s->by1, s->bz1, (s->by1 - s->by0) / 16.0, std::min(vc, 63.0) * 0.98};
+  launch_bake_diag(s->part[s->cur], s->N, D, s->diag, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&h, s->diag, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const uint32_t alive = h.count[0];
+  const double a = std::max<double>(alive, 1.0);
+  auto dbl = [](unsigned long long k) {   // back from the ordered integer
+    const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double d;
+    memcpy(&d, &u, 8);
+    return d;
+  };
+  out->alive = alive; out->non_finite = h.count[1]; out->gone = s->N - alive - h.count[1];
+  out->outside_box = h.count[2]; out->at_speed_limit = h.count[3]; out->foamy = h.count[4];
+  out->mean_speed = h.sum[3] / a;
+  double smax;
+  memcpy(&smax, &h.smax, 8);
+  out->max_speed = smax;
+  out->mean_foam = h.sum[4] / a / 15.0;
+  for (int k = 0; k < 3; k++) out->center[k] = h.sum[k] / a;
+  out->has_bbox = alive ? 1 : 0;
+  if (alive) for (int k = 0; k < 3; k++) { out->bbox[k] = dbl(h.mn[k]); out->bbox[3 + k] = dbl(h.mx[k]); }
+  for (int k = 0; k < 16; k++) out->height_hist[k] = h.hist[k];
   return ST_OK;
 }
 

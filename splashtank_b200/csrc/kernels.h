@@ -25,4 +25,17 @@ int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 // whitewater (flip_extra.cu)
 int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s);
+// frames and bake measurements (frames.cu)
+struct FrameBox { double x0, y0, z0, kx, ky, kz, ks; };
+struct DiagBox { double x0, y0, z0, x1, y1, z1, hy, cap; };
+struct DiagAcc {
+  uint32_t count[5];            // alive, non-finite, outside the box, at the speed limit, foamy
+  uint32_t hist[16];            // heights
+  double sum[5];                // x, y, z, speed, foam level
+  unsigned long long smax;      // fastest speed (bits of a non-negative double)
+  unsigned long long mn[3], mx[3];   // bounding box (doubles as ordered integers)
+};
+int launch_pack_frame(const float4* pos4, uint32_t n, const FrameBox& F, uint16_t* pos16, uint8_t* spd, uint8_t* fm, uint32_t* meta,
+                      cudaStream_t s);
+int launch_bake_diag(const Part* pa, uint32_t n, const DiagBox& D, DiagAcc* acc, cudaStream_t s);
 }  // namespace st

@@ -256,6 +256,31 @@ class FlipSim:
         del keep
         return {n: getattr(t, n) for n in abi.STAGES}
 
+    def read_frame(self, vs=1.0, out=None):
+        """The particles as a cache frame (packFrameBuf, src/gpu.js:525-560), packed on the device: dict n, pos
+        (n, 3) uint16, spd (n,) uint8 and fm (n,) uint8 or None when no point has white water. out: optional
+        (pos, spd, fm) arrays with room for MAXN points (e.g. views of pinned host memory) to read into."""
+        self.flushRun()
+        cap = max(self.MAXN, 1)
+        if out is None:
+            pos, spd, fm = np.zeros((cap, 3), np.uint16), np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        else:
+            pos, spd, fm = out
+            cap = min(cap, len(spd), len(fm), pos.size // 3)
+        n, foam = C.c_uint32(), C.c_int32()
+        self._check(self.f["flip_read_frame"](self._h, float(vs), pos.ctypes.data_as(C.POINTER(C.c_uint16)), spd.ctypes.data_as(abi.u8p),
+                                              fm.ctypes.data_as(abi.u8p), cap, C.byref(n), C.byref(foam)), "read_frame")
+        m = n.value
+        return dict(n=m, pos=pos[:m], spd=spd[:m], fm=fm[:m] if foam.value else None)
+
+    def bake_diag(self, vcap=14.0):
+        """bakeDiag (src/flip/bake.js:60-83) computed on the device, with the reference's keys."""
+        d = abi.BakeDiag()
+        self._check(self.f["flip_bake_diag"](self._h, float(vcap or 0.0), C.byref(d)), "bake_diag")
+        return dict(alive=d.alive, gone=d.gone, nonFinite=d.non_finite, outsideBox=d.outside_box, atWaterSpeedLimit=d.at_speed_limit,
+                    meanSpeed=d.mean_speed, maxSpeed=d.max_speed, meanFoam=d.mean_foam, foamyPoints=d.foamy, center=list(d.center),
+                    bbox=list(d.bbox) if d.has_bbox else None, heightHist=list(d.height_hist))
+
     def save_full(self):
         """The full checkpoint (st_flip_save_full) as bytes."""
         self.flushRun()
