@@ -276,7 +276,8 @@ __device__ __forceinline__ float wetCellAt(const FlipParams& P, const float* __r
 }
 // wetAt(i, j, k) gives wetCellAt for the eight cells around the particle (from HBM, or a staged window)
 template <class WetAt>
-__device__ __forceinline__ void emitTermsT(const FlipParams& P, const WetAt& wetAt, float4 qp, float4 qv, float& rho, float& fast, float& e) {
+__device__ __forceinline__ void emitTermsT(const FlipParams& P, const WetAt& wetAt, float4 qp, float4 qv, float& rho, float& fast, float& e,
+                                           float settle) {
   const V3 p = xyz(qp), v = xyz(qv);
   const float foam = qv.w, spd = len3(v);
   fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
@@ -289,7 +290,7 @@ __device__ __forceinline__ void emitTermsT(const FlipParams& P, const WetAt& wet
   rho = rho / 8.0f;
   const float crest = (1.0f - smoothstepf(0.3f, 0.75f, rho)) * fast * (0.3f + 0.7f * foam);
   const float churn = (1.0f - smoothstepf(0.8f, 1.0f, rho)) * clampf((foam - 0.55f) / 0.45f, 0.0f, 1.0f) * smoothstepf(0.5f, 1.5f, spd * P.vs);
-  e = (P.wwCrest * crest + P.wwImpact * churn) * smoothstepf(0.1f, 0.5f, P.q8);
+  e = (P.wwCrest * crest + P.wwImpact * churn) * settle;
 }
 struct WetGlobal {
   const FlipParams& P;
@@ -297,7 +298,7 @@ struct WetGlobal {
   __device__ __forceinline__ float operator()(int i, int j, int k) const { return wetCellAt(P, wet, i, j, k); }
 };
 __device__ __forceinline__ void emitTerms(const FlipParams& P, const float* __restrict__ wet, float4 qp, float4 qv, float& rho, float& fast, float& e) {
-  emitTermsT(P, WetGlobal{P, wet}, qp, qv, rho, fast, e);
+  emitTermsT(P, WetGlobal{P, wet}, qp, qv, rho, fast, e, smoothstepf(0.1f, 0.5f, P.q8));
 }
 
 // ---- block-wide scans (blockDim.x a multiple of 32, at most 1024) ----

@@ -31,47 +31,69 @@ __device__ __forceinline__ void markAround(const FlipParams& P, uint32_t* __rest
 // One pass over the particles in storage order: mark tiles near live particles, count particles per cell with
 // warp-aggregated atomics (the returned base gives each particle a rank in its cell), count dead slots per block,
 // and the fastest speed (ctl[6], wgsl-solver.js:24).
-__global__ void __launch_bounds__(PBLK) k_count_mark(Bufs B) {
+// A CTA takes CM_U consecutive blocks of PBLK particles and keeps all of them in flight (loads, then the atomics, then
+// the tile marks), so the latency of the dependent steps overlaps across blocks; dead slots are still counted per block.
+constexpr int CM_U = 4;
+__global__ void __launch_bounds__(PBLK, 1) k_count_mark(Bufs B) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  uint32_t key = DEADKEY;
-  bool live = false, dead = false;
+  Part q[CM_U];
+  uint32_t key[CM_U], idx[CM_U], peers[CM_U], base[CM_U];
+  bool live[CM_U], dead[CM_U];
+  int ci[CM_U], cj[CM_U], ck[CM_U];
   float sp = 0.0f;
-  int ci = 0, cj = 0, ck = 0;
-  if (i < P.n) {
-    Part q = B.pb[i];
-    if (q.p.y < DEADY) dead = true;
-    else {
-      live = true;
-      particleCell(P, xyz(q.p), ci, cj, ck);
-      key = cellIdx(P, ci, cj, ck);
-      sp = len3(xyz(q.v));
-    }
-    B.key[i] = key;
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    idx[u] = (blockIdx.x * CM_U + u) * PBLK + threadIdx.x;
+    if (idx[u] < P.n) q[u] = B.pb[idx[u]];
   }
-  uint32_t peers = __match_any_sync(0xffffffffu, key);
-  int leader = __ffs(peers) - 1;
-  uint32_t base = 0;
-  // lanes in one cell mark the same tiles: the group's first lane marks for all of them
-  if (live && lane == leader) markAround(P, B.need, ci, cj, ck);
-  if (live && lane == leader) base = (uint32_t)atomicAdd(&B.cnt[key], __popc(peers));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (live) B.rank[i] = base + __popc(peers & ((1u << lane) - 1u));
-  // fastest speed: lengths are non-negative, so their bit patterns order like the floats; one atomic per block
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    key[u] = DEADKEY;
+    live[u] = dead[u] = false;
+    ci[u] = cj[u] = ck[u] = 0;
+    if (idx[u] < P.n) {
+      if (q[u].p.y < DEADY) dead[u] = true;
+      else {
+        live[u] = true;
+        particleCell(P, xyz(q[u].p), ci[u], cj[u], ck[u]);
+        key[u] = cellIdx(P, ci[u], cj[u], ck[u]);
+        sp = fmx(sp, len3(xyz(q[u].v)));
+      }
+      B.key[idx[u]] = key[u];
+    }
+    peers[u] = __match_any_sync(0xffffffffu, key[u]);
+  }
+  // the group's first lane counts for all of them, and marks the tiles (lanes in one cell mark the same tiles)
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    base[u] = 0;
+    if (live[u] && lane == __ffs(peers[u]) - 1) base[u] = (uint32_t)atomicAdd(&B.cnt[key[u]], __popc(peers[u]));
+  }
+#pragma unroll
+  for (int u = 0; u < CM_U; u++)
+    if (live[u] && lane == __ffs(peers[u]) - 1) markAround(P, B.need, ci[u], cj[u], ck[u]);
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
+    if (live[u]) B.rank[idx[u]] = b + __popc(peers[u] & ((1u << lane) - 1u));
+  }
+  // fastest speed: lengths are non-negative, so their bit patterns order like the floats; one atomic per CTA
   __shared__ float wmax[PBLK / 32];
   float m = sp;
   for (int o = 16; o > 0; o >>= 1) m = fmx(m, __shfl_xor_sync(0xffffffffu, m, o));
   if (lane == 0) wmax[threadIdx.x >> 5] = m;
-  uint32_t nd = __syncthreads_count(dead);
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    const uint32_t nd = __syncthreads_count(dead[u]);
+    const uint32_t blk = blockIdx.x * CM_U + u;
+    if (threadIdx.x == 0 && blk < B.nblk) B.blkDead[blk] = nd;
+  }
   if (threadIdx.x < 32) {
     float b = wmax[threadIdx.x];
     for (int o = 16; o > 0; o >>= 1) b = fmx(b, __shfl_xor_sync(0xffffffffu, b, o));
-    if (threadIdx.x == 0) {
-      B.blkDead[blockIdx.x] = nd;
-      if (b > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(b));
-    }
+    if (threadIdx.x == 0 && b > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(b));
   }
 }
 
@@ -206,20 +228,35 @@ __global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
-  const uint32_t i = blockIdx.x * PBLK + threadIdx.x;
-  uint32_t k = i < P.n ? B.key[i] : 0u;
-  bool dead = i < P.n && k == DEADKEY;
-  uint32_t r = blockExclusive(dead ? 1u : 0u, sm, nullptr);
-  if (i >= P.n) return;
-  if (!dead) {
-    uint32_t a = B.tileSlot[k >> 9];
-    uint32_t pos = B.tileCnt[a] + B.cellOff[k] + B.rank[i];
-    B.srcIdx[pos] = i;
-    B.spid[pos] = B.idb[i];
-  } else {
-    uint32_t pos = B.ctl->nLive + B.blkDead[blockIdx.x] + r;
-    B.pa[pos] = B.pb[i];
-    B.ida[pos] = B.idb[i];
+  uint32_t idx[CM_U], k[CM_U], r[CM_U], rk[CM_U], id[CM_U], a[CM_U], off[CM_U];
+  bool dead[CM_U];
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    idx[u] = (blockIdx.x * CM_U + u) * PBLK + threadIdx.x;
+    k[u] = idx[u] < P.n ? B.key[idx[u]] : 0u;
+  }
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    dead[u] = idx[u] < P.n && k[u] == DEADKEY;
+    if (idx[u] < P.n) {
+      id[u] = B.idb[idx[u]];
+      if (!dead[u]) { a[u] = B.tileSlot[k[u] >> 9]; off[u] = B.cellOff[k[u]]; rk[u] = B.rank[idx[u]]; }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) r[u] = blockExclusive(dead[u] ? 1u : 0u, sm, nullptr);
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) {
+    if (idx[u] >= P.n) continue;
+    if (!dead[u]) {
+      const uint32_t pos = B.tileCnt[a[u]] + off[u] + rk[u];
+      B.srcIdx[pos] = idx[u];
+      B.spid[pos] = id[u];
+    } else {
+      const uint32_t pos = B.ctl->nLive + B.blkDead[blockIdx.x * CM_U + u] + r[u];
+      B.pa[pos] = B.pb[idx[u]];
+      B.ida[pos] = id[u];
+    }
   }
 }
 
@@ -738,7 +775,14 @@ __device__ void buildGust(const FlipParams& P, GustTab& T) {
   }
   __syncthreads();
 }
-__device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, Part& q) {
+// values of the particle update that depend only on the parameters, computed once per thread
+struct G2PUni {
+  float sens, settle, tau0, tt;
+};
+__device__ __forceinline__ G2PUni g2pUni(const FlipParams& P) {
+  return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f};
+}
+__device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q) {
   const V3 p = xyz(q.p), v0 = xyz(q.v);
   int fi, fj, fk;
   particleCell(P, p, fi, fj, fk);
@@ -764,19 +808,19 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const float shield = smoothstepf(0.1f, 0.65f, rho);
   const float exposure = 1.0f - 0.97f * shield;
   const float spd0 = len3(v);
-  const float sens = fmx(P.q6, 0.05f);
+  const float sens = U.sens;
   const float pacc = len3(vn - vo) / P.dt;
-  const float settle = smoothstepf(0.1f, 0.5f, P.q8);
+  const float settle = U.settle;
   const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
   const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
   const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
-  const float tau = fmx(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
+  const float tau = U.tau0 * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
   float foam = q.v.w * st_expf(-P.dt / tau);
   foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
   V3 gust = v3(0.0f, 0.0f, 0.0f);
   if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
     const V3 gp = p * 0.55f;
-    const float tt = P.q8 * 0.6f;
+    const float tt = U.tt;
     gust = v3(vnzTab(T, 0, gp + v3(tt, 0.0f, 0.0f)), vnzTab(T, 1, gp + v3(17.3f, tt, 4.1f)), vnzTab(T, 2, gp + v3(5.7f, 9.2f, tt))) * 2.0f -
            v3(1.0f, 1.0f, 1.0f);
   }
@@ -824,6 +868,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
     const uint32_t t = B.active[a], tt = t / P.tx;
     G2PWin W{wvn, wvo, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
+    const G2PUni U = g2pUni(P);
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
       const int gi = W.ox + r % 10 - 1, gj = W.oy + (r / 10) % 10 - 1, gk = W.oz + r / 100 - 1;
       if (gi < 0 || gj < 0 || gk < 0 || gi >= NX || gj >= NY || gk >= NZ) {   // faces here are never sampled (clamped)
@@ -842,7 +887,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
     uint32_t emitSum = 0, deadSum = 0;
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
       Part q = B.pa[i];
-      g2pOne(P, B, W, gtab, q);
+      g2pOne(P, B, W, gtab, U, q);
       // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
       const bool gone = q.p.y < DEADY;
@@ -852,7 +897,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
         // the eight cells around the moved particle: from the window when it holds them
         const V3 bcf = vfloor((xyz(q.p) - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
         const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
-        if (W.has(bi, bj, bk) && W.has(bi + 1, bj + 1, bk + 1)) emitTermsT(P, WetWin{W}, q.p, q.v, rho, fast, e);
+        if (W.has(bi, bj, bk) && W.has(bi + 1, bj + 1, bk + 1)) emitTermsT(P, WetWin{W}, q.p, q.v, rho, fast, e, U.settle);
         else emitTerms(P, B.wet, q.p, q.v, rho, fast, e);
         if (e > 0.0f) {
           const uint32_t h0 = B.ida[i] * 747796405u + P.seed * 2891336453u;
@@ -927,7 +972,7 @@ __global__ void k_iota(uint32_t* p, uint32_t n) {
 }
 
 // ---- launchers: each returns how many kernels it launched ----
-int launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<B.nblk, PBLK, 0, s>>>(B); return 1; }
+int launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<(B.nblk + CM_U - 1) / CM_U, PBLK, 0, s>>>(B); return 1; }
 int launch_mark_phi(const Bufs& B, int grid, cudaStream_t s) { k_mark_phi<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_mark_fill(const Bufs& B, int grid, cudaStream_t s) { k_mark_fill<<<grid, 256, 0, s>>>(B); return 1; }
 int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
@@ -938,7 +983,7 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
   return 3;
 }
 int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
-int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, PBLK, 0, s>>>(B); return 1; }
+int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<(B.nblk + CM_U - 1) / CM_U, PBLK, 0, s>>>(B); return 1; }
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
 int launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); return 1; }
