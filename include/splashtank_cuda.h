@@ -99,6 +99,10 @@ typedef struct st_step_opts {
   st_spray_opts spray;
   int32_t nb_on;        /* o.nb.on: narrow band */
   float nb_band;        /* o.nb.band (cells, at least 2) */
+  int32_t air_on;       /* o.air.on: air field dragged by water and spray, moving the whitewater (needs spray_on) */
+  float air_couple;     /* o.air.couple */
+  float air_decay;      /* o.air.decay */
+  float air_blur;       /* o.air.blur (default 0.35) */
 } st_step_opts;
 
 /* Counters read back after a step: FlipSim.stats (src/flip/sim.js:160-168). */
@@ -171,6 +175,10 @@ st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t 
 /* FlipSim.readSpray (src/flip/sim.js:423-437): whitewater slots handed out (positions with life in w,
  * velocities with kind in w). */
 st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
+/* The air field (src/flip/wgsl-whitewater.js:24-89, grid made by airAlloc, src/flip/sim.js:342-350): air velocity at
+ * each air-cell centre, x fastest, 4 floats per cell (w 0). dims3 receives the air grid's cells per axis (0 0 0 when
+ * the handle has no whitewater pool, which the air field needs); at most cap cells are written. */
+st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims3);
 /* FlipSim.stats via readStats (src/flip/sim.js:160-168). Synchronises. */
 st_status st_flip_stats(st_flip* s, st_stats* out);
 /* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */

@@ -61,6 +61,15 @@ inline float bitsf(int32_t i) { float f; memcpy(&f, &i, 4); return f; }
 inline int32_t fbits(float f) { int32_t i; memcpy(&i, &f, 4); return i; }
 // WGSL u32(f): truncation, saturating at 0 for negative values
 inline uint32_t u32f(float f) { return f <= 0.0f ? 0u : (uint32_t)f; }
+// WGSL i32(f): truncation, saturating at the ends of the range; NaN gives 0
+inline int32_t i32f(float f) {
+  if (!(f == f)) return 0;
+  if (f >= 2147483648.0f) return 2147483647;
+  if (f <= -2147483648.0f) return (int32_t)0x80000000u;
+  return (int32_t)f;
+}
+// a floored coordinate as an index, held in [-2, 2^24] so that index + 1 cannot overflow (in-range values unchanged)
+inline int i32idx(float f) { return std::min(std::max(i32f(f), -2), 1 << 24); }
 
 const float DEADY = -1.0e5f;
 const uint32_t NONE = 0xffffffffu;
@@ -83,6 +92,7 @@ struct Params {
   uint32_t smax, seed;
   uint32_t nb; float band; uint32_t nbInit, nfill;
   float wwFoamLife, wwRise, wwCrest, wwImpact;
+  uint32_t airOn, aNx, aNy, aNz; float airCouple, airDecay, airH, airBlur;   // words 72-76, 82
   float fills[16][4];
 };
 
@@ -109,6 +119,11 @@ struct Oracle {
   // whitewater (sim.js:71, 333-341)
   std::vector<float> sPos, sVel, sAux;
   uint32_t sctl0 = 0;
+  // air field (sim.js:342-350): 4 floats per air cell (air, air2), 4 fixed-point sums (airAcc)
+  std::vector<float> air, air2;
+  std::vector<int32_t> airAcc;
+  uint32_t aNx = 0, aNy = 0, aNz = 0, airCells = 0;
+  double airH = 1.0;
   // narrow band state (sim.js:92, 120-126)
   bool velGOn = false;
   uint32_t nbInit = 0;
@@ -319,6 +334,13 @@ struct Oracle {
     cnt.assign(ncell, 0); ctype.assign(ncell, 0); pres.assign(ncell, 0.0f); rhs.assign(ncell, 0.0f);
     accV.assign(ncell * 3, 0); accW.assign(ncell * 3, 0); velG.assign(ncell * 3, 0.0f);
     sPos.assign((size_t)std::max(sprayCap, 1u) * 4, 0.0f); sVel = sPos; sAux = sPos;
+    if (sprayCap) {   // airAlloc (sim.js:343-350), made up front: it stays zero until the air field is first on
+      int r = std::max(2, (int)std::ceil(std::cbrt((double)nx * ny * nz / 260000.0)));
+      airH = h * r;
+      aNx = (uint32_t)((nx + r - 1) / r + 1); aNy = (uint32_t)((ny + r - 1) / r + 1); aNz = (uint32_t)((nz + r - 1) / r + 1);
+      airCells = aNx * aNy * aNz;
+      air.assign((size_t)airCells * 4, 0.0f); air2 = air; airAcc.assign((size_t)airCells * 4, 0);
+    }
     memset(&P, 0, sizeof(P));
     P.tx = tx; P.ty = ty; P.tz = tz; P.nx = nx; P.ny = ny; P.nz = nz;
   }
@@ -326,6 +348,7 @@ struct Oracle {
   void clear() {
     N = 0; ring = 0; tm = 0; nbInit = 1; fillsPacked.clear();
     std::fill(sPos.begin(), sPos.end(), 0.0f); sctl0 = 0;
+    std::fill(air.begin(), air.end(), 0.0f);
     for (uint32_t k = 0; k < maxN; k++) pid[k] = k;
     steps = 0;
   }
@@ -399,6 +422,10 @@ struct Oracle {
     for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &fillsPacked[k * 8], 8 * sizeof(float));
     P.wwFoamLife = sp.foam_life != 0.0f ? sp.foam_life : 3.0f; P.wwRise = sp.rise != 0.0f ? sp.rise : 0.3f;
     P.wwCrest = sp.crest; P.wwImpact = sp.impact;
+    bool airo = sprOn && o->air_on != 0 && airCells != 0;   // sim.js:222-229
+    P.airOn = airo ? 1u : 0u; P.airCouple = airo ? o->air_couple : 0.0f; P.airDecay = airo ? o->air_decay : 0.0f;
+    P.airH = airCells ? (float)airH : 1.0f; P.airBlur = airo ? o->air_blur : 0.0f;
+    P.aNx = airCells ? aNx : 1u; P.aNy = airCells ? aNy : 1u; P.aNz = airCells ? aNz : 1u;
   }
 
   // ---- blocks (wgsl-blocks.js:5-55, wgsl-narrowband.js:6-18, sim.js:253-261) ----
@@ -799,7 +826,77 @@ struct Oracle {
     }
     return s;
   }
+  // ---- air field (wgsl-whitewater.js:24-89) ----
+  uint32_t airIdx(int x, int y, int z) const {   // :25-28
+    int qx = std::min(std::max(x, 0), (int)P.aNx - 1), qy = std::min(std::max(y, 0), (int)P.aNy - 1), qz = std::min(std::max(z, 0), (int)P.aNz - 1);
+    return (uint32_t)qx + P.aNx * ((uint32_t)qy + P.aNy * (uint32_t)qz);
+  }
+  V3 airV(uint32_t c) const { return v3(air[c * 4], air[c * 4 + 1], air[c * 4 + 2]); }
+  V3 airAt(V3 p) const {   // :30-40
+    V3 g = (p - v3(P.x0, P.y0, P.z0)) / P.airH - v3(0.5f, 0.5f, 0.5f);
+    V3 f0 = vfloor(g); V3 fr = g - f0; int i0 = i32idx(f0.x), j0 = i32idx(f0.y), k0 = i32idx(f0.z);
+    V3 s = v3(0, 0, 0);
+    for (int c = 0; c < 8; c++) {
+      int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      s = s + airV(airIdx(i0 + dx, j0 + dy, k0 + dz)) * w;
+    }
+    return s;
+  }
+  void airPush(V3 p, V3 v, float w) {   // :41-45 (integer sums: any order gives the same result)
+    V3 g = vfloor((p - v3(P.x0, P.y0, P.z0)) / P.airH);
+    uint32_t c = airIdx(i32idx(g.x), i32idx(g.y), i32idx(g.z)) * 4u;
+    uint32_t q[4] = {(uint32_t)i32f(v.x * w * 256.0f), (uint32_t)i32f(v.y * w * 256.0f), (uint32_t)i32f(v.z * w * 256.0f), (uint32_t)i32f(w * 256.0f)};
+    for (int a = 0; a < 4; a++) {
+      uint32_t* t = reinterpret_cast<uint32_t*>(&airAcc[c + a]);
+#pragma omp atomic
+      *t += q[a];
+    }
+  }
+  void stageAir() {
+    std::fill(airAcc.begin(), airAcc.end(), 0);                                   // airClear
+    forParticles([&](uint32_t i) {                                                // airSplatW (:51-57)
+      if (pos[i * 4 + 1] < DEADY) return;
+      V3 p = ppos(i);
+      int ci, cj, ck; particleCell(p, ci, cj, ck);
+      if (hasStorage(ci, cj, ck) && (float)cnt[cellIdx(ci, cj, ck)] > 0.85f * P.rest) return;
+      airPush(p, pvel(i), 1.0f);
+    });
+    uint32_t m = std::min(sctl0, P.smax);                                         // airSplatS (:59-64), over the slots handed out
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t jj = 0; jj < (int64_t)m; jj++) {
+      uint32_t j = (uint32_t)jj;
+      if (sPos[j * 4 + 3] <= 0.0f || sVel[j * 4 + 3] > 1.5f) continue;
+      airPush(v3(sPos[j * 4], sPos[j * 4 + 1], sPos[j * 4 + 2]), v3(sVel[j * 4], sVel[j * 4 + 1], sVel[j * 4 + 2]), 0.25f);
+    }
+    uint32_t na = P.aNx * P.aNy * P.aNz;                                          // airUpdate (:67-86)
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t cc = 0; cc < (int64_t)na; cc++) {
+      uint32_t c = (uint32_t)cc;
+      int ci = (int)(c % P.aNx), cj = (int)((c / P.aNx) % P.aNy), ck = (int)(c / (P.aNx * P.aNy));
+      V3 a = airV(c);
+      V3 nb = (airV(airIdx(ci + 1, cj, ck)) + airV(airIdx(ci - 1, cj, ck)) + airV(airIdx(ci, cj + 1, ck)) + airV(airIdx(ci, cj - 1, ck)) +
+               airV(airIdx(ci, cj, ck + 1)) + airV(airIdx(ci, cj, ck - 1))) / 6.0f;
+      a = vmix(a, nb, P.airBlur);
+      float w = (float)airAcc[c * 4 + 3] / 256.0f;
+      if (w > 0.0f) {
+        V3 vt = v3((float)airAcc[c * 4], (float)airAcc[c * 4 + 1], (float)airAcc[c * 4 + 2]) / (w * 256.0f);
+        a = vmix(a, vt, 1.0f - st_expf(-P.airCouple * fmin_(w, 8.0f) * P.dt));
+      }
+      V3 x = v3(P.x0, P.y0, P.z0) + (v3((float)ci, (float)cj, (float)ck) + v3(0.5f, 0.5f, 0.5f)) * P.airH;
+      for (uint32_t k = 0; k < P.ncols; k++) {
+        if (!colNear(k, x)) continue;
+        float phi; V3 wn; sdfEval(k, x, phi, wn);
+        if (phi < 0.6f * P.airH) { a = colSurfVel(k, x); break; }
+      }
+      a = vmix(a, v3(P.q1, P.q2, P.q3), 1.0f - st_expf(-P.airDecay * P.dt));
+      air2[c * 4] = a.x; air2[c * 4 + 1] = a.y; air2[c * 4 + 2] = a.z; air2[c * 4 + 3] = 0.0f;
+    }
+    std::copy(air2.begin(), air2.begin() + (size_t)na * 4, air.begin());        // airCopy
+  }
+
   void stageSpray(bool emit) {
+    if (P.airOn != 0u) stageAir();   // the air field first, so the whitewater moves with this step's air (sim.js:297-301)
     uint32_t m = std::min(sctl0, P.smax);
     // wwSample
 #pragma omp parallel for schedule(static) num_threads(nthreads)
@@ -835,7 +932,7 @@ struct Oracle {
           V3 gp = p * 0.55f * P.vs; float tt = P.q8 * 0.6f;
           gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1, 1, 1);
         }
-        V3 base = v3(P.q1, P.q2, P.q3);
+        V3 base = P.airOn != 0u ? airAt(p) : v3(P.q1, P.q2, P.q3);
         V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
         v.y -= P.gravity * P.dt;
         v = v + (airv - v) * (1.0f - st_expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
@@ -1032,6 +1129,13 @@ st_status oracle_flip_read_spray(void* h, float* pos4, float* vel4, uint32_t cap
     if (pos4) memcpy(&pos4[j * 4], &s->sPos[j * 4], 16);
     if (vel4) memcpy(&vel4[j * 4], &s->sVel[j * 4], 16);
   }
+  return ST_OK;
+}
+st_status oracle_flip_read_air(void* h, float* vel4, uint32_t cap, uint32_t* dims3) {
+  Oracle* s = (Oracle*)h;
+  if (dims3) { dims3[0] = s->aNx; dims3[1] = s->aNy; dims3[2] = s->aNz; }
+  uint32_t m = std::min(cap, s->airCells);
+  if (vel4 && m) memcpy(vel4, s->air.data(), (size_t)m * 16);
   return ST_OK;
 }
 st_status oracle_flip_stats(void* h, st_stats* o) {

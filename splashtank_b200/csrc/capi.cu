@@ -96,6 +96,11 @@ struct st_flip {
   float* wet = nullptr;
   float* sdf = nullptr;
   float4 *sPos = nullptr, *sVel = nullptr;
+  // air field (src/flip/sim.js:342-350): cells r solver cells wide, r = max(2, ceil(cbrt(cells / 260000)))
+  float4 *air = nullptr, *air2 = nullptr;
+  int32_t* airAcc = nullptr;
+  uint32_t aNx = 0, aNy = 0, aNz = 0, airCells = 0;
+  double airH = 1.0;
   uint8_t* emitK = nullptr;
   uint32_t *blkEmit = nullptr, *deadList = nullptr;
   cudaEvent_t ev[16] = {};
@@ -117,7 +122,7 @@ struct st_flip {
     B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
     B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
-    B.sPos = sPos; B.sVel = sVel; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
+    B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
   }
@@ -139,6 +144,7 @@ void st_step_opts_default(st_step_opts* o) {
   o->foam_tau = 1.2f; o->foam_sens = 1.0f; o->vs = 1.0f; o->iters = 30;
   o->spray.foam_life = 3.0f; o->spray.rise = 0.3f; o->spray.crest = 1.0f; o->spray.impact = 0.5f;
   o->nb_band = 3.0f;
+  o->air_blur = 0.35f;
 }
 
 void st_flip_destroy(st_flip* s) {
@@ -149,7 +155,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
+                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -210,6 +216,14 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(dalloc(&s->cp, C), "sweep p"); A(dalloc(&s->crhs, C), "sweep rhs"); A(dalloc(&s->cinfo, C), "sweep info");
   A(dalloc(&s->nbs, 6 * T), "sweep neighbours"); A(dalloc(&s->slotOf, T), "sweep slots"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
   A(dalloc(&s->sPos, std::max<size_t>(s->sprayCap, 1)), "sPos"); A(dalloc(&s->sVel, std::max<size_t>(s->sprayCap, 1)), "sVel");
+  if (s->sprayCap) {   // the air field exists only with whitewater: it is stepped in the whitewater stage
+    const double cells = (double)s->nx * (double)s->ny * (double)s->nz;
+    const int r = std::max(2, (int)std::ceil(std::cbrt(cells / 260000.0)));
+    s->airH = s->h * r;
+    s->aNx = (uint32_t)((s->nx + r - 1) / r + 1); s->aNy = (uint32_t)((s->ny + r - 1) / r + 1); s->aNz = (uint32_t)((s->nz + r - 1) / r + 1);
+    s->airCells = s->aNx * s->aNy * s->aNz;
+    A(dalloc(&s->air, s->airCells), "air"); A(dalloc(&s->air2, s->airCells), "air2"); A(dalloc(&s->airAcc, 4 * (size_t)s->airCells), "air acc");
+  }
   for (auto& ev : s->ev) A(cudaEventCreate(&ev), "event");
   A(cudaMallocHost((void**)&s->ring_h, sizeof(st_flip::Upload) * st_flip::RING), "upload ring"); A(dalloc(&s->dUp, 1), "upload");
   for (auto& ev : s->ring_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "ring event");
@@ -228,6 +242,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(cudaMemsetAsync(s->wet, 0, C * 4, q), "memset");
   A(cudaMemsetAsync(s->sPos, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
   A(cudaMemsetAsync(s->sVel, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
+  if (s->airCells) { A(cudaMemsetAsync(s->air, 0, (size_t)s->airCells * 16, q), "memset"); A(cudaMemsetAsync(s->air2, 0, (size_t)s->airCells * 16, q), "memset"); }
   launch_fill_f32(s->rhs, 8.0f, C, q);
   reset_ids(s);
   A(cudaStreamSynchronize(q), "create sync");
@@ -255,6 +270,7 @@ st_status st_flip_clear(st_flip* s) {
     CK(cudaMemsetAsync(s->sPos, 0, (size_t)s->sprayCap * 16, s->stream));
     CK(cudaMemsetAsync(&s->dCtl->sctl0, 0, 4, s->stream));
   }
+  if (s->airCells) CK(cudaMemsetAsync(s->air, 0, (size_t)s->airCells * 16, s->stream));
   reset_ids(s);
   CK(cudaStreamSynchronize(s->stream));
   return ST_OK;
@@ -373,6 +389,11 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
   P.band = std::max(2.0f, o->nb_band != 0.0f ? o->nb_band : 3.0f);
   P.wwFoamLife = sp.foam_life != 0.0f ? sp.foam_life : 3.0f; P.wwRise = sp.rise != 0.0f ? sp.rise : 0.3f;
   P.wwCrest = sp.crest; P.wwImpact = sp.impact;
+  // air field (words 72-76, 82): on only with whitewater on this step
+  const bool airOn = sprOn && o->air_on != 0 && s->airCells != 0;
+  P.airOn = airOn ? 1u : 0u; P.airCouple = airOn ? o->air_couple : 0.0f; P.airDecay = airOn ? o->air_decay : 0.0f;
+  P.airH = s->airCells ? (float)s->airH : 1.0f; P.airBlur = airOn ? o->air_blur : 0.0f;
+  P.aNx = s->airCells ? s->aNx : 1u; P.aNy = s->airCells ? s->aNy : 1u; P.aNz = s->airCells ? s->aNz : 1u;
   uint32_t nf = init ? (uint32_t)std::min<size_t>(s->fills.size() / 8, 8) : 0u;
   P.nfill = nf;
   for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &s->fills[k * 8], 8 * sizeof(float));
@@ -420,7 +441,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(7);
   nl += launch_g2p(B, gT, q);
   mark(8);
-  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, gT4, q);
+  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, gT4, q);
   mark(9);
   if (nbOn) nl += launch_nb_reseed(B, gT4, q);
   mark(10);
@@ -428,10 +449,11 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
 }
 
 // A step's kernels as a CUDA graph, keyed by everything that changes what is launched: the particle buffer parity,
-// the particle count (grid sizes), SOR iterations, narrow band, whitewater emission and stage timing. Stage markers are
+// the particle count (grid sizes), SOR iterations, narrow band, whitewater emission, the air field and stage timing. Stage markers are
 // external event-record nodes, pointed at the timing ring's events before each launch.
 static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, bool timing) {
   return (uint64_t)s->cur | ((uint64_t)s->parity << 1) | ((uint64_t)nbOn << 2) | ((uint64_t)sprOn << 3) | ((uint64_t)timing << 4) |
+         ((uint64_t)(s->hp.airOn != 0) << 5) |
          ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24);
 }
 static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, bool timing, st_flip::Graph** out) {
@@ -721,6 +743,18 @@ st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap,
   return ST_OK;
 }
 
+st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims3) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (dims3) { dims3[0] = s->aNx; dims3[1] = s->aNy; dims3[2] = s->aNz; }
+  const uint32_t m = std::min(cap, s->airCells);
+  if (vel4 && m) {
+    CK(cudaMemcpyAsync(vel4, s->air, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return ST_OK;
+}
+
 st_status st_flip_read_grid(st_flip* s, const st_flip_grid* g) {
   if (!s || !g) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));
@@ -817,12 +851,14 @@ struct FullHdr {
   double tm;
 };
 static constexpr uint32_t FULL_MAGIC = 0x53544650u;   // "PFTS"
+static constexpr uint32_t FULL_VERSION = 2;           // 2: the air field follows the whitewater pools
 static void full_parts(st_flip* s, std::vector<std::pair<void*, size_t>>& v) {
   const size_t C = s->ncell, T = s->ntiles, SC = std::max<size_t>(s->sprayCap, 1), N = s->N;
   v = {{s->dCtl, sizeof(Ctl)}, {s->part[s->cur], N * sizeof(Part)}, {s->ids[s->cur], N * 4}, {s->need, T * 4}, {s->on, T},
        {s->tstate, T}, {s->active, T * 4}, {s->cnt[0], C * 4}, {s->cnt[1], C * 4}, {s->ctype, C * 4}, {s->pres, C * 4},
        {s->rhs, C * 4}, {s->acc, 6 * C * 4}, {s->vn, 3 * C * 4}, {s->vo, 3 * C * 4}, {s->velG, 3 * C * 4}, {s->sorInfo, C * 2},
        {s->wet, C * 4}, {s->sPos, SC * 16}, {s->sVel, SC * 16}};
+  if (s->airCells) v.push_back({s->air, (size_t)s->airCells * 16});
 }
 
 st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size) {
@@ -836,7 +872,7 @@ st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size)
   if (!buf) return ST_OK;
   if (cap < need) return ST_OVERFLOW;
   FullHdr h{};
-  h.magic = FULL_MAGIC; h.version = 1; h.nx = (uint32_t)s->nx; h.ny = (uint32_t)s->ny; h.nz = (uint32_t)s->nz; h.ntiles = s->ntiles;
+  h.magic = FULL_MAGIC; h.version = FULL_VERSION; h.nx = (uint32_t)s->nx; h.ny = (uint32_t)s->ny; h.nz = (uint32_t)s->nz; h.ntiles = s->ntiles;
   h.ncell = s->ncell; h.maxN = s->maxN; h.sprayCap = s->sprayCap; h.N = s->N; h.cap = s->cap; h.ring = s->ring; h.seed = s->seed;
   h.steps = s->steps; h.stamp = s->stamp; h.parity = s->parity; h.cur = (uint32_t)s->cur; h.velGOn = s->velGOn ? 1u : 0u;
   h.nbInit = s->nbInit; h.nfills = (uint32_t)s->fills.size(); h.tm = s->tm;
@@ -856,7 +892,7 @@ st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
   if (!s || !buf || size < sizeof(FullHdr)) return ST_BAD_ARG;
   FullHdr h;
   memcpy(&h, buf, sizeof(h));
-  if (h.magic != FULL_MAGIC || h.version != 1 || h.nx != (uint32_t)s->nx || h.ny != (uint32_t)s->ny || h.nz != (uint32_t)s->nz ||
+  if (h.magic != FULL_MAGIC || h.version != FULL_VERSION || h.nx != (uint32_t)s->nx || h.ny != (uint32_t)s->ny || h.nz != (uint32_t)s->nz ||
       h.ntiles != s->ntiles || h.ncell != s->ncell || h.maxN != s->maxN || h.sprayCap != s->sprayCap || h.N > s->maxN || h.cur > 1 ||
       h.parity > 1) {
     snprintf(g_err, sizeof(g_err), "load_full: the checkpoint is not of a simulator with this geometry and capacity");

@@ -33,6 +33,8 @@ struct FlipParams {
   float sheetMin, sprRate, sprMin, sprLife, mistFrac, sprDrag, mistDrag, vs;
   uint32_t smax, seed, nb, nbInit, nfill, lcap, stamp, sprayOn;
   float band, wwFoamLife, wwRise, wwCrest, wwImpact;
+  uint32_t airOn, aNx, aNy, aNz;          // air field (words 72-83 of the reference's block)
+  float airCouple, airDecay, airH, airBlur;
   float fills[16][4];
 };
 
@@ -102,6 +104,10 @@ struct Bufs {
   uint32_t* nbs;
   uint32_t* slotOf;     // per tile: position in fluidTiles, or 0xffffffff
   float* wet;           // per cell: how much water (wetCell, src/flip/wgsl-whitewater.js:7-12), 0 outside the domain
+  // air field (src/flip/wgsl-whitewater.js:24-89): velocity at air-cell centres, its next value, fixed-point pushes
+  float4* air;
+  float4* air2;
+  int32_t* airAcc;      // 4 per air cell: sum of v w 256 (x, y, z) and of w 256
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)
   const float* sdf;

@@ -3,6 +3,8 @@
 // Where the reference compacts with atomics in arbitrary order (nbDead, nbDeficit, nbSpawn, sprayEmit), these
 // kernels use a fixed order built from block scans: dead slots in ascending storage index, deficit cells in
 // ascending cell key, whitewater ring slots in ascending storage index of the emitting particle.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -289,6 +291,134 @@ __device__ __forceinline__ float vnzX(V3 x) {
   const float b = mixf(mixf(hsh3X(i + v3(0, 0, 1)), hsh3X(i + v3(1, 0, 1)), u.x), mixf(hsh3X(i + v3(0, 1, 1)), hsh3X(i + v3(1, 1, 1)), u.x), u.y);
   return mixf(a, b, u.z);
 }
+// ---- air field (wgsl-whitewater.js:24-89): a coarse grid of air velocity at cell centres (cells P.airH wide from the
+// box's low corner) that water near the surface and flying spray drag along; spray and mist drift with it ----
+// WGSL i32(f32): truncation towards zero, saturating at the ends of the range; NaN gives 0
+__device__ __forceinline__ int32_t i32f(float f) {
+  if (!(f == f)) return 0;
+  if (f >= 2147483648.0f) return 2147483647;
+  if (f <= -2147483648.0f) return (int32_t)0x80000000u;
+  return (int32_t)f;
+}
+__device__ __forceinline__ uint32_t airIdx(const FlipParams& P, int x, int y, int z) {   // airIdx (:25-28)
+  const int qx = clampi(x, 0, (int)P.aNx - 1), qy = clampi(y, 0, (int)P.aNy - 1), qz = clampi(z, 0, (int)P.aNz - 1);
+  return (uint32_t)qx + P.aNx * ((uint32_t)qy + P.aNy * (uint32_t)qz);
+}
+__device__ __forceinline__ V3 airAt(const FlipParams& P, const float4* __restrict__ air, V3 p) {   // airAt (:30-40)
+  const V3 g = (p - v3(P.x0, P.y0, P.z0)) / P.airH - v3(0.5f, 0.5f, 0.5f);
+  const V3 f0 = vfloor(g), fr = g - f0;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
+  V3 s = v3(0.0f, 0.0f, 0.0f);
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    s = s + xyz(__ldg(&air[airIdx(P, i0 + dx, j0 + dy, k0 + dz)])) * w;
+  }
+  return s;
+}
+// airPush (:41-45) for a warp at once: the lanes that push into the same air cell add their fixed-point values first
+// (integer sums, so the result does not depend on the order), and one lane per cell does the atomics
+__device__ __forceinline__ void airPushWarp(const FlipParams& P, int32_t* __restrict__ acc, bool valid, V3 p, V3 v, float w) {
+  uint32_t key = 0xffffffffu, q0 = 0, q1 = 0, q2 = 0, q3 = 0;
+  if (valid) {
+    const V3 g = vfloor((p - v3(P.x0, P.y0, P.z0)) / P.airH);
+    key = airIdx(P, gidx(g.x), gidx(g.y), gidx(g.z));
+    q0 = (uint32_t)i32f(v.x * w * 256.0f);
+    q1 = (uint32_t)i32f(v.y * w * 256.0f);
+    q2 = (uint32_t)i32f(v.z * w * 256.0f);
+    q3 = (uint32_t)i32f(w * 256.0f);
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t pend = __ballot_sync(0xffffffffu, valid);
+  while (pend) {
+    const int lead = __ffs(pend) - 1;
+    const uint32_t k = __shfl_sync(0xffffffffu, key, lead);
+    const bool mine = valid && key == k;
+    const uint32_t grp = __ballot_sync(0xffffffffu, mine);
+    const uint32_t s0 = __reduce_add_sync(0xffffffffu, mine ? q0 : 0u), s1 = __reduce_add_sync(0xffffffffu, mine ? q1 : 0u);
+    const uint32_t s2 = __reduce_add_sync(0xffffffffu, mine ? q2 : 0u), s3 = __reduce_add_sync(0xffffffffu, mine ? q3 : 0u);
+    if (lane == (uint32_t)lead) {
+      uint32_t* a = reinterpret_cast<uint32_t*>(acc) + 4ull * k;
+      atomicAdd(a, s0); atomicAdd(a + 1, s1); atomicAdd(a + 2, s2); atomicAdd(a + 3, s3);
+    }
+    pend &= ~grp;
+  }
+}
+// airSplatW (:51-57) over the live particles, then airSplatS (:59-64) over the whitewater slots handed out, in one
+// launch. g2p held back the narrow band trim of particles that throw off no points (their kill belongs to the
+// reseed stage, after the air has felt them); they are removed here once pushed.
+__global__ void __launch_bounds__(256) k_air_splat(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nL = B.ctl->nLive, m = min(B.ctl->sctl0, P.smax), tot = nL + m;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < tot; i0 += stride) {
+    const uint32_t i = i0 + (threadIdx.x & 31u);
+    bool valid = false;
+    V3 p = v3(0.0f, 0.0f, 0.0f), v = p;
+    float w = 1.0f;
+    if (i < nL) {
+      const Part q = B.pa[i];
+      p = xyz(q.p);
+      v = xyz(q.v);
+      valid = !(q.p.y < DEADY);
+      if (valid) {
+        int ci, cj, ck;
+        particleCell(P, p, ci, cj, ck);
+        if (B.on[tileOf(P, ci, cj, ck)] && (float)B.cnt[cellIdx(P, ci, cj, ck)] > 0.85f * P.rest) valid = false;
+        const uint8_t ek = B.emitK[i];
+        if ((ek & EMIT_KILL) && (ek & 7u) == 0u) {
+          Part d;
+          d.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+          d.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          B.pa[i] = d;
+        }
+      }
+    } else if (i < tot) {
+      const uint32_t j = i - nL;
+      const float4 sp = B.sPos[j], sv = B.sVel[j];
+      p = xyz(sp);
+      v = xyz(sv);
+      w = 0.25f;
+      valid = !(sp.w <= 0.0f) && !(sv.w > 1.5f);
+    }
+    airPushWarp(P, B.airAcc, valid, p, v, w);
+  }
+}
+// airUpdate (:67-86): blur towards the six neighbours, pull towards what pushed the cell, take the velocity of an
+// object the cell is inside, settle back to the wind
+__global__ void __launch_bounds__(256) k_air_update(Bufs B) {
+  __shared__ FlipParams P;
+  loadParamsX(P, B.P);
+  const uint32_t nax = P.aNx, nay = P.aNy, na = nax * nay * P.aNz;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < na; c += gridDim.x * blockDim.x) {
+    const int ci = (int)(c % nax), cj = (int)((c / nax) % nay), ck = (int)(c / (nax * nay));
+    V3 a = xyz(B.air[c]);
+    const V3 nb = (xyz(B.air[airIdx(P, ci + 1, cj, ck)]) + xyz(B.air[airIdx(P, ci - 1, cj, ck)]) + xyz(B.air[airIdx(P, ci, cj + 1, ck)]) +
+                   xyz(B.air[airIdx(P, ci, cj - 1, ck)]) + xyz(B.air[airIdx(P, ci, cj, ck + 1)]) + xyz(B.air[airIdx(P, ci, cj, ck - 1)])) / 6.0f;
+    a = vmix(a, nb, P.airBlur);
+    const int4 ac = reinterpret_cast<const int4*>(B.airAcc)[c];
+    const float w = (float)ac.w / 256.0f;
+    if (w > 0.0f) {
+      const V3 vt = v3((float)ac.x, (float)ac.y, (float)ac.z) / (w * 256.0f);
+      a = vmix(a, vt, 1.0f - st_expf(-P.airCouple * fmn(w, 8.0f) * P.dt));
+    }
+    const V3 x = v3(P.x0, P.y0, P.z0) + (v3((float)ci, (float)cj, (float)ck) + v3(0.5f, 0.5f, 0.5f)) * P.airH;
+    for (uint32_t k = 0; k < P.ncols; k++) {
+      if (!colNear(P, B.cols, k, x)) continue;
+      float phi;
+      V3 wn;
+      sdfEval(B.cols, B.sdf, k, x, phi, wn);
+      if (phi < 0.6f * P.airH) { a = colSurfVel(B.cols, k, x); break; }
+    }
+    a = vmix(a, v3(P.q1, P.q2, P.q3), 1.0f - st_expf(-P.airDecay * P.dt));
+    B.air2[c] = make_float4(a.x, a.y, a.z, 0.0f);
+  }
+}
+__global__ void __launch_bounds__(256) k_air_copy(Bufs B, uint32_t na) {   // airCopy (:88)
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < na; c += gridDim.x * blockDim.x) B.air[c] = B.air2[c];
+}
+
 // wwSample (wgsl-whitewater.js:91-98) fused with sprayStep (:134-179): each point reads only its own sample
 __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
   __shared__ FlipParams P;
@@ -344,7 +474,7 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
         const float tt = P.q8 * 0.6f;
         gust = v3(vnzX(gp + v3(tt, 0.0f, 0.0f)), vnzX(gp + v3(17.3f, tt, 4.1f)), vnzX(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
       }
-      const V3 base = v3(P.q1, P.q2, P.q3);
+      const V3 base = P.airOn != 0u ? airAt(P, B.air, p) : v3(P.q1, P.q2, P.q3);
       const V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);
       v.y -= P.gravity * P.dt;
       v = v + (airv - v) * (1.0f - st_expf(-(mist ? P.mistDrag : P.sprDrag) * P.dt));
@@ -444,14 +574,23 @@ int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
   k_spawn<<<grid, 512, 0, s>>>(B);
   return 5;
 }
-int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s) {
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, int grid, cudaStream_t s) {
   if (!smax) return 0;
+  int nl = 0;
+  if (airCells) {   // the air field first, so the whitewater moves with this step's air (src/flip/sim.js:297-301)
+    cudaMemsetAsync(B.airAcc, 0, (size_t)airCells * 16, s);
+    k_air_splat<<<grid * 2, 256, 0, s>>>(B);
+    const int ga = (int)std::min<uint32_t>((airCells + 255) / 256, 148u * 8u);
+    k_air_update<<<ga, 256, 0, s>>>(B);
+    k_air_copy<<<ga, 256, 0, s>>>(B, airCells);
+    nl += 3;
+  }
   k_ww_step<<<grid, 256, 0, s>>>(B);
-  if (!emit) return 1;
+  if (!emit) return nl + 1;
   k_scan_x<<<1, 1024, 0, s>>>(B, 2);
   k_emit_write<<<grid, 256, 0, s>>>(B);
   k_emit_done<<<1, 1, 0, s>>>(B);
-  return 4;
+  return nl + 4;
 }
 
 }  // namespace st

@@ -914,12 +914,15 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
           kill = B.on[cc >> 9] && phiOfBits(B.ctype[cc]) < -P.band;
         }
       }
-      if (kill && kc == 0) {
+      // the trim waits for the points this particle throws off (written by the emit pass) and, with the air field
+      // on, for the air splat, which still sees the particle (the reference trims in the reseed stage)
+      const bool holdKill = kc != 0 || P.airOn != 0u;
+      if (kill && !holdKill) {
         q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
         q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       }
       B.pa[i] = q;
-      if (P.sprayOn != 0u) B.emitK[i] = (uint8_t)(kc | (kill && kc ? EMIT_KILL : 0u));
+      if (P.sprayOn != 0u) B.emitK[i] = (uint8_t)(kc | (kill && holdKill ? EMIT_KILL : 0u));
       if (P.nb != 0u) B.deadF[i] = (gone || kill) ? 1 : 0;
       emitSum += kc;
       deadSum += (gone || kill) ? 1u : 0u;

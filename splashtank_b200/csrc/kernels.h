@@ -24,7 +24,8 @@ int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 // whitewater (flip_extra.cu)
-int launch_spray(const Bufs& B, uint32_t smax, bool emit, int grid, cudaStream_t s);
+// airCells: air-field cells to step first (0 when the air field is off this step)
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, int grid, cudaStream_t s);
 // frames and bake measurements (frames.cu)
 struct FrameBox { double x0, y0, z0, kx, ky, kz, ks; };
 struct DiagBox { double x0, y0, z0, x1, y1, z1, hy, cap; };

@@ -120,6 +120,11 @@ def make_opts(o, opt=None, default=None):
     nb = o.get("nb")
     s.nb_on = 1 if (nb and nb.get("on")) else 0
     s.nb_band = float(max(2.0, (nb or {}).get("band") or 3.0))
+    air = o.get("air")
+    s.air_on = 1 if (air and air.get("on")) else 0
+    s.air_couple = float((air or {}).get("couple", 0.0))
+    s.air_decay = float((air or {}).get("decay", 0.0))
+    s.air_blur = float((air or {}).get("blur", 0.35))
     return s, cols
 
 
@@ -349,6 +354,17 @@ class FlipSim:
         n = C.c_uint32()
         self._check(self.f["flip_read_spray"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.sprayCap, C.byref(n)), "readSpray")
         return dict(n=n.value, p=p[: n.value], v=v[: n.value])
+
+    def read_air(self):
+        """The air field: (nz, ny, nx, 3) float32 air velocity at the air-cell centres, or None without a whitewater pool."""
+        dims = (C.c_uint32 * 3)()
+        self._check(self.f["flip_read_air"](self._h, None, 0, dims), "readAir")
+        nx, ny, nz = dims[0], dims[1], dims[2]
+        if not nx:
+            return None
+        a = np.zeros((nz * ny * nx, 4), np.float32)
+        self._check(self.f["flip_read_air"](self._h, a.ctypes.data_as(abi.f32p), nx * ny * nz, dims), "readAir")
+        return a[:, :3].reshape(nz, ny, nx, 3)
 
     def grid(self):
         """Every cell of the tile box: tile_on, cnt, ctype, pres, rhs, vn, vo, velg (dense numpy arrays)."""

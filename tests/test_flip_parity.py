@@ -45,6 +45,8 @@ def assert_same_state(g, o, spray=False):
     if spray:
         x, y = g.readSpray(), o.readSpray()
         assert x["n"] == y["n"] and same(x["p"], y["p"]) and same(x["v"], y["v"]), "whitewater"
+        a, b = g.read_air(), o.read_air()
+        assert (a is None) == (b is None) and (a is None or same(a, b)), "air field"
 
 
 def dam_pair(n, **kw):
@@ -122,6 +124,32 @@ def test_wave_tank_band3_trims_and_refills():
     _run_tank(w, (g, o), 30)
     st = g.readStats()
     assert st["live"] < len(w.pos)     # the deep water was trimmed to the band
+    assert_same_state(g, o, spray=True)
+
+
+@pytest.mark.parametrize("spray_cap", [30000, 4000])
+def test_air_field_with_whitewater(spray_cap):
+    """Whitewater of every kind with the air field on: water thrown at the wall from t = 0.6 s (emission at full
+    strength), gusts, narrow band of 3 cells (the trim of particles the air splat still sees), 40 steps. With the
+    smaller pool the ring wraps several times. The air field, the pool and the particles agree bit for bit."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    sc = scenes.dam_break(32)
+    sc["vel"] = np.tile(np.array([[2.5, 0.5, 0.0]], np.float32), (len(sc["pos"]), 1))
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY, min=0.5), air=dict(on=True, couple=3.0, decay=0.6), gust=1.0,
+                nb=dict(on=True, band=3.0))
+    g, o = make_pair(sc, spray_cap=spray_cap)
+    for s in (g, o):
+        p, v, i = s.save_state()
+        s.load_state(p, v, i, t=0.6, seed=0)
+    for _ in range(40):
+        for s in (g, o):
+            s.step(sc["dt"], opts)
+    sp = g.readSpray()
+    kinds = np.bincount(np.round(sp["v"][sp["p"][:, 3] > 0, 3]).astype(int), minlength=4)
+    assert np.all(kinds > 0), kinds                      # spray, mist, foam and bubbles all present
+    assert g.readStats()["live"] < len(sc["pos"])          # the narrow band trimmed
+    assert np.abs(g.read_air()).max() > 0.5
     assert_same_state(g, o, spray=True)
 
 

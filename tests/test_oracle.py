@@ -130,6 +130,38 @@ def test_narrow_band_full_depth_keeps_particles():
     assert (phi[deep] < 0.5).mean() > 0.9                     # water cells carry a negative depth
 
 
+def test_air_field_settles_to_the_wind():
+    """With no coupling, every air cell relaxes towards the wind by 1 - exp(-decay dt) a step (airUpdate,
+    src/flip/wgsl-whitewater.js:67-86); a uniform field stays uniform under the blur. The grid is airAlloc's
+    (src/flip/sim.js:343-350): r = 2 solver cells at 16^3, so 8 + 1 cells per axis."""
+    s, sc = dam(16, spray_cap=100)
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY), wind=(1.0, 0.0, -0.5), air=dict(on=True, couple=0.0, decay=0.6))
+    assert s.read_air().shape == (9, 9, 9, 3) and not s.read_air().any()
+    steps = 12
+    for _ in range(steps):
+        s.step(sc["dt"], opts)
+    a = s.read_air().reshape(-1, 3)
+    left = np.exp(-0.6 * sc["dt"]) ** steps
+    np.testing.assert_allclose(a, np.tile([1.0 - left, 0.0, -0.5 * (1.0 - left)], (len(a), 1)), rtol=1e-4, atol=1e-6)
+    s.step(sc["dt"], dict(opts, air=None))   # off: the field is kept as it is
+    np.testing.assert_array_equal(s.read_air().reshape(-1, 3), a)
+    s.clear()
+    assert not s.read_air().any()
+
+
+def test_air_field_follows_the_water():
+    """Coupled to moving water, the air near the surface picks up the water's direction."""
+    s, sc = dam(16, spray_cap=100)
+    s2 = OracleFlipSim(sc["d"], len(sc["pos"]), size=sc["size"], ratio=sc["ratio"], threads=4, spray_cap=100)
+    vel = np.tile(np.array([[1.5, 0.0, 0.0]], np.float32), (len(sc["pos"]), 1))
+    s2.add_many(sc["pos"], vel)
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY), air=dict(on=True, couple=3.0, decay=0.6))
+    for _ in range(10):
+        s2.step(sc["dt"], opts)
+    a = s2.read_air()
+    assert a[..., 0].max() > 0.1 and a[..., 0].sum() > 0 and np.all(np.isfinite(a))
+
+
 @pytest.mark.parametrize("name", ["dam_break_16_s10", "wave_tank_24_s8"])
 def test_golden_fixture(name):
     """The oracle still produces the committed fixtures (tests/golden/make_golden.py) bit for bit."""
