@@ -103,6 +103,9 @@ typedef struct st_step_opts {
   float air_couple;     /* o.air.couple */
   float air_decay;      /* o.air.decay */
   float air_blur;       /* o.air.blur (default 0.35) */
+  int32_t drip_on;      /* o.drip.on: wet colliders drip after they leave the water (needs spray_on) */
+  float drip_rate;      /* o.drip.rate: drops a second from a fully wet surface sample */
+  float drip_dry;       /* o.drip.dry: seconds a surface stays wet out of the water */
 } st_step_opts;
 
 /* Counters read back after a step: FlipSim.stats (src/flip/sim.js:160-168). */
@@ -179,6 +182,10 @@ st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap,
  * each air-cell centre, x fastest, 4 floats per cell (w 0). dims3 receives the air grid's cells per axis (0 0 0 when
  * the handle has no whitewater pool, which the air field needs); at most cap cells are written. */
 st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims3);
+/* The drip samples (dripSamples, src/flip/bake.js:19-40; bDrip, src/flip/sim.js:352-363): 8 floats each, the
+ * position on the collider in its own frame, the collider number, the normal in its own frame and the wetness (1 in
+ * water, falling to 0 over o.drip.dry seconds out of it). *n receives the count; at most cap are written. */
+st_status st_flip_read_drips(st_flip* s, float* out8, uint32_t cap, uint32_t* n);
 /* FlipSim.stats via readStats (src/flip/sim.js:160-168). Synchronises. */
 st_status st_flip_stats(st_flip* s, st_stats* out);
 /* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */

@@ -93,6 +93,7 @@ struct Params {
   uint32_t nb; float band; uint32_t nbInit, nfill;
   float wwFoamLife, wwRise, wwCrest, wwImpact;
   uint32_t airOn, aNx, aNy, aNz; float airCouple, airDecay, airH, airBlur;   // words 72-76, 82
+  uint32_t ndrip; float dripRate, dripDry;                                    // words 79-81
   float fills[16][4];
 };
 
@@ -124,6 +125,10 @@ struct Oracle {
   std::vector<int32_t> airAcc;
   uint32_t aNx = 0, aNy = 0, aNz = 0, airCells = 0;
   double airH = 1.0;
+  // drip samples (sim.js:352-363): 8 floats each (local position, collider, local normal, wetness)
+  std::vector<float> drip;
+  uint32_t ndrip = 0;
+  std::string dripSig;
   // narrow band state (sim.js:92, 120-126)
   bool velGOn = false;
   uint32_t nbInit = 0;
@@ -349,6 +354,7 @@ struct Oracle {
     N = 0; ring = 0; tm = 0; nbInit = 1; fillsPacked.clear();
     std::fill(sPos.begin(), sPos.end(), 0.0f); sctl0 = 0;
     std::fill(air.begin(), air.end(), 0.0f);
+    dripSig.clear();   // drip samples come back dry
     for (uint32_t k = 0; k < maxN; k++) pid[k] = k;
     steps = 0;
   }
@@ -426,6 +432,47 @@ struct Oracle {
     P.airOn = airo ? 1u : 0u; P.airCouple = airo ? o->air_couple : 0.0f; P.airDecay = airo ? o->air_decay : 0.0f;
     P.airH = airCells ? (float)airH : 1.0f; P.airBlur = airo ? o->air_blur : 0.0f;
     P.aNx = airCells ? aNx : 1u; P.aNy = airCells ? aNy : 1u; P.aNz = airCells ? aNz : 1u;
+    bool dr = sprOn && o->drip_on != 0;
+    P.ndrip = dr ? ndrip : 0u; P.dripRate = dr ? o->drip_rate : 0.0f; P.dripDry = dr ? o->drip_dry : 1.0f;
+  }
+
+  // ---- drip samples (dripSamples, bake.js:19-40, in JavaScript doubles; dripUpdate, sim.js:352-363) ----
+  static double jsRound(double x) { double r = std::floor(x); return x - r >= 0.5 ? r + 1.0 : r; }
+  void dripSamplesOf(const st_sdf* sd, uint32_t k, std::vector<float>& out) const {
+    int sx = (int)sd->dims[0], sy = (int)sd->dims[1], sz = (int)sd->dims[2];
+    double c = sd->cell;
+    auto D = [&](int i, int j, int q) { return (double)sd->data[(size_t)i + (size_t)sx * ((size_t)j + (size_t)sy * (size_t)q)]; };
+    auto at = [&](int i, int j, int q) { return D(std::min(sx - 1, std::max(0, i)), std::min(sy - 1, std::max(0, j)), std::min(sz - 1, std::max(0, q))); };
+    std::vector<double> pts;
+    for (int q = 1; q < sz - 1; q++) for (int j = 1; j < sy - 1; j++) for (int i = 1; i < sx - 1; i++) {
+      double v = D(i, j, q);
+      if (std::fabs(v) > 0.6 * c) continue;
+      double gx = at(i + 1, j, q) - at(i - 1, j, q), gy = at(i, j + 1, q) - at(i, j - 1, q), gz = at(i, j, q + 1) - at(i, j, q - 1);
+      double gl = std::sqrt(gx * gx + gy * gy + gz * gz);   // Math.hypot
+      if (gl < 1e-9) continue;
+      gx /= gl; gy /= gl; gz /= gl;
+      double rec[6] = {(double)sd->origin[0] + i * c - gx * v, (double)sd->origin[1] + j * c - gy * v, (double)sd->origin[2] + q * c - gz * v, gx, gy, gz};
+      pts.insert(pts.end(), rec, rec + 6);
+    }
+    double nsurf = (double)(pts.size() / 6);
+    double want = std::max(100.0, std::min(6000.0, jsRound(nsurf * c * c / (h * h))));
+    double step = std::max(1.0, nsurf / want);
+    double seedv = 7.0 + (double)(int32_t)sd->id;
+    auto rnd = [&]() { seedv = std::fmod(seedv * 16807.0, 2147483647.0); return seedv / 2147483647.0; };
+    for (double t = rnd() * step; t < nsurf; t += step) {
+      size_t i = (size_t)std::floor(t) * 6;
+      float rec[8] = {(float)pts[i], (float)pts[i + 1], (float)pts[i + 2], (float)k, (float)pts[i + 3], (float)pts[i + 4], (float)pts[i + 5], 0.0f};
+      out.insert(out.end(), rec, rec + 8);
+    }
+  }
+  void dripUpdate(const st_step_opts* o, uint32_t nc) {
+    std::string sig;
+    for (uint32_t k = 0; k < nc; k++) sig += std::to_string(o->cols[k].sdf->id) + ",";
+    if (sig == dripSig) return;
+    dripSig = sig;
+    drip.clear();
+    for (uint32_t k = 0; k < nc; k++) dripSamplesOf(o->cols[k].sdf, k, drip);
+    ndrip = (uint32_t)(drip.size() / 8);
   }
 
   // ---- blocks (wgsl-blocks.js:5-55, wgsl-narrowband.js:6-18, sim.js:253-261) ----
@@ -951,7 +998,43 @@ struct Oracle {
       sPos[j * 4] = np.x; sPos[j * 4 + 1] = np.y; sPos[j * 4 + 2] = np.z; sPos[j * 4 + 3] = life;
       sVel[j * 4] = v.x; sVel[j * 4 + 1] = v.y; sVel[j * 4 + 2] = v.z; sVel[j * 4 + 3] = (float)kind + 0.4f * tk / WWHOLD;
     }
-    if (!emit) return;
+    if (emit) stageEmit();
+    if (P.ndrip) stageDrip();
+  }
+
+  // dripStep (wgsl-whitewater.js:254-278). Canonical order: samples ascending; the ring counter advances once per drop;
+  // drops beyond smax in one pass are not written.
+  void stageDrip() {
+    uint32_t run = 0;
+    for (uint32_t s = 0; s < P.ndrip; s++) {
+      float* a = &drip[(size_t)s * 8]; float* b = a + 4;
+      uint32_t k = u32f(a[3]); if (k >= P.ncols) continue;
+      V3 r0 = v3(col(k, 2)[0], col(k, 2)[1], col(k, 2)[2]), r1 = v3(col(k, 3)[0], col(k, 3)[1], col(k, 3)[2]), r2 = v3(col(k, 4)[0], col(k, 4)[1], col(k, 4)[2]);
+      V3 wp = v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]) + r0 * a[0] + r1 * a[1] + r2 * a[2];
+      V3 wr = r0 * b[0] + r1 * b[1] + r2 * b[2];
+      V3 wn = wr / length(wr);
+      V3 probe = wp + wn * P.h * 0.75f;
+      float here = wetAt(probe);
+      if (here > 0.4f) { b[3] = 1.0f; continue; }
+      float wetness = fmax_(0.0f, b[3] - P.dt / fmax_(P.dripDry, 0.05f));
+      b[3] = wetness;
+      if (wetness <= 0.0f || here > 0.1f || P.smax == 0u || P.dripRate <= 0.0f) continue;
+      float down = clampf(-wn.y, 0.0f, 1.0f);
+      float rate = P.dripRate * wetness * wetness * (0.15f + 0.85f * down);
+      uint32_t h0 = s * 747796405u + P.seed * 2891336453u + 17u;
+      if (hash1(h0) >= rate * P.dt) continue;
+      uint32_t r = run++;
+      if (r >= P.smax) continue;
+      uint32_t slot = (uint32_t)(((uint64_t)sctl0 + r) % P.smax);
+      if (sPos[slot * 4 + 3] > 0.0f) continue;
+      V3 nv = colSurfVel(k, wp) + wn * P.h * 2.0f * hash1(h0 + 1u);
+      sPos[slot * 4] = probe.x; sPos[slot * 4 + 1] = probe.y; sPos[slot * 4 + 2] = probe.z; sPos[slot * 4 + 3] = P.sprLife * 2.0f;
+      sVel[slot * 4] = nv.x; sVel[slot * 4 + 1] = nv.y; sVel[slot * 4 + 2] = nv.z; sVel[slot * 4 + 3] = 0.0f;
+    }
+    sctl0 = sctl0 + run;
+  }
+
+  void stageEmit() {
     // sprayEmit (wgsl-whitewater.js:101-133). Canonical order: particles by storage index, points by m; the ring
     // counter advances once per point tried; a slot is taken only if it was not living before this pass.
     if (P.smax == 0u || P.sprRate <= 0.0f) return;
@@ -1060,6 +1143,7 @@ struct Oracle {
     uint32_t init = nbOn && nbInit ? nbInit : 0;
     packCols(o);
     bool sprOn = o->spray_on != 0 && sprayCap > 0;
+    if (sprOn && o->drip_on != 0) dripUpdate(o, ncols);
     seed = seed + 1u;
     packParams(dt, o, init, nbOn, sprOn);
     tm = tm + dt;
@@ -1136,6 +1220,13 @@ st_status oracle_flip_read_air(void* h, float* vel4, uint32_t cap, uint32_t* dim
   if (dims3) { dims3[0] = s->aNx; dims3[1] = s->aNy; dims3[2] = s->aNz; }
   uint32_t m = std::min(cap, s->airCells);
   if (vel4 && m) memcpy(vel4, s->air.data(), (size_t)m * 16);
+  return ST_OK;
+}
+st_status oracle_flip_read_drips(void* h, float* out8, uint32_t cap, uint32_t* n) {
+  Oracle* s = (Oracle*)h;
+  if (n) *n = s->ndrip;
+  uint32_t m = std::min(cap, s->ndrip);
+  if (out8 && m) memcpy(out8, s->drip.data(), (size_t)m * 32);
   return ST_OK;
 }
 st_status oracle_flip_stats(void* h, st_stats* o) {

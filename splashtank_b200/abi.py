@@ -38,7 +38,8 @@ class StepOpts(C.Structure):
                 ("vmax", C.c_float), ("wind", C.c_float * 3), ("drag", C.c_float), ("foam_tau", C.c_float),
                 ("foam_sens", C.c_float), ("gust", C.c_float), ("tear", C.c_float), ("vs", C.c_float), ("iters", C.c_int32),
                 ("flags", C.c_uint32), ("ncols", C.c_uint32), ("cols", C.POINTER(Collider)), ("spray_on", C.c_int32),
-                ("spray", SprayOpts), ("nb_on", C.c_int32), ("nb_band", C.c_float), ("air_on", C.c_int32), ("air_couple", C.c_float), ("air_decay", C.c_float), ("air_blur", C.c_float)]
+                ("spray", SprayOpts), ("nb_on", C.c_int32), ("nb_band", C.c_float), ("air_on", C.c_int32), ("air_couple", C.c_float), ("air_decay", C.c_float), ("air_blur", C.c_float),
+                ("drip_on", C.c_int32), ("drip_rate", C.c_float), ("drip_dry", C.c_float)]
 
 
 class Stats(C.Structure):
@@ -110,6 +111,7 @@ FLIP_FUNCS = [
     ("flip_read_particles", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
     ("flip_read_spray", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
     ("flip_read_air", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
+    ("flip_read_drips", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
     ("flip_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("flip_read_grid", C.c_int, [C.c_void_p, C.POINTER(Grid)]),
     ("flip_get_dims", C.c_int, [C.c_void_p, C.POINTER(Dims)]),

@@ -8,11 +8,11 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["capi.cu", "flip_kernels.cu", "flip_extra.cu", "pbf.cu", "poisson.cu", "diff.cu", "frames.cu"]
+SRC = ["capi.cu", "flip_kernels.cu", "flip_extra.cu", "pbf.cu", "poisson.cu", "diff.cu", "frames.cu", "drips.cpp"]
 OUT = os.path.join(HERE, "libsplashtank_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
-         "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-O3"]
+         "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-Xptxas", "-O3"]
 
 
 def sources():

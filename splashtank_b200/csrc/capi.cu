@@ -63,7 +63,7 @@ struct st_flip {
   // per-step uploads (parameter block + collider records) come from a ring of pinned host blocks, so the copies are
   // asynchronous and a block is rewritten only after the copy that read it has run
   static constexpr int RING = 16;
-  struct Upload { FlipParams P; float cols[32 * 32]; };
+  struct Upload { FlipParams P; alignas(16) float cols[32 * 32]; };   // cols are read as float4
   Upload* ring_h = nullptr;
   cudaEvent_t ring_ev[RING] = {};
   int ring_i = 0;
@@ -101,6 +101,12 @@ struct st_flip {
   int32_t* airAcc = nullptr;
   uint32_t aNx = 0, aNy = 0, aNz = 0, airCells = 0;
   double airH = 1.0;
+  // drip samples on the colliders (dripUpdate, src/flip/sim.js:352-363): 2 float4 each, rebuilt (dry) when the
+  // colliders' distance grids change
+  float4* drip = nullptr;
+  uint32_t ndrip = 0, dripCap = 0;
+  std::string dripSig;
+  std::map<uint32_t, std::vector<float>> dripCache;   // per grid id: its samples (collider number 0)
   uint8_t* emitK = nullptr;
   uint32_t *blkEmit = nullptr, *deadList = nullptr;
   cudaEvent_t ev[16] = {};
@@ -122,7 +128,7 @@ struct st_flip {
     B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
     B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
-    B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
+    B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.drip = drip; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
   }
@@ -145,6 +151,7 @@ void st_step_opts_default(st_step_opts* o) {
   o->spray.foam_life = 3.0f; o->spray.rise = 0.3f; o->spray.crest = 1.0f; o->spray.impact = 0.5f;
   o->nb_band = 3.0f;
   o->air_blur = 0.35f;
+  o->drip_dry = 1.0f;
 }
 
 void st_flip_destroy(st_flip* s) {
@@ -155,7 +162,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
+                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->drip, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -271,6 +278,7 @@ st_status st_flip_clear(st_flip* s) {
     CK(cudaMemsetAsync(&s->dCtl->sctl0, 0, 4, s->stream));
   }
   if (s->airCells) CK(cudaMemsetAsync(s->air, 0, (size_t)s->airCells * 16, s->stream));
+  s->dripSig.clear();   // drip samples come back dry
   reset_ids(s);
   CK(cudaStreamSynchronize(s->stream));
   return ST_OK;
@@ -316,7 +324,7 @@ st_status st_flip_add(st_flip* s, const float* p3, const float* v3_, uint32_t n,
 }
 
 // packColliders (src/gpu.js:42-70): 32 floats per collider, SDF grids uploaded when the set of ids changes
-static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc, float* cf) {
+static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc, float* cf, cudaStream_t q) {
   nc = std::min(o->ncols, 32u);
   if (nc && !o->cols) return ST_BAD_ARG;
   std::string sig;
@@ -329,7 +337,7 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc,
   }
   if (sig != s->sdfSig) {
     if (off > s->sdfCap) {
-      CK(cudaStreamSynchronize(s->stream));
+      CK(cudaStreamSynchronize(q));
       drop_graphs(s);   // captured steps hold the old grid pointer
       cudaFree(s->sdf);
       s->sdfCap = (size_t)std::ceil(off * 1.3);
@@ -340,8 +348,9 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc,
       const st_sdf* sd = o->cols[k].sdf;
       if (seen[sd->id]) continue;
       seen[sd->id] = true;
-      CK(cudaMemcpy(s->sdf + offs[sd->id], sd->data, sizeof(float) * sd->dims[0] * sd->dims[1] * sd->dims[2], cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(s->sdf + offs[sd->id], sd->data, sizeof(float) * sd->dims[0] * sd->dims[1] * sd->dims[2], cudaMemcpyHostToDevice, q));
     }
+    CK(cudaStreamSynchronize(q));   // in stream order after the steps that read the old grids; data is the caller's
     s->sdfSig = sig;
   }
   if (nc) {
@@ -359,6 +368,45 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc,
       f[28] = c.ang[0]; f[29] = c.ang[1]; f[30] = c.ang[2]; f[31] = 0;
     }
   }
+  return ST_OK;
+}
+
+// dripUpdate (src/flip/sim.js:352-363): the samples of every collider's distance grid, rebuilt when the grids of the
+// colliders (in collider order) change; a rebuilt set starts dry
+static st_status drip_update(st_flip* s, const st_step_opts* o, uint32_t nc, cudaStream_t q) {
+  std::string sig;
+  for (uint32_t k = 0; k < nc; k++) sig += std::to_string(o->cols[k].sdf->id) + ",";
+  if (sig == s->dripSig) return ST_OK;
+  std::vector<float> all;
+  for (uint32_t k = 0; k < nc; k++) {
+    const st_sdf* sd = o->cols[k].sdf;
+    auto it = s->dripCache.find(sd->id);
+    if (it == s->dripCache.end()) {
+      std::vector<float> v;
+      drip_samples(sd, s->h, 0, v);
+      if (s->dripCache.size() >= 32) s->dripCache.erase(s->dripCache.begin());
+      it = s->dripCache.emplace(sd->id, std::move(v)).first;
+    }
+    const size_t at = all.size();
+    all.insert(all.end(), it->second.begin(), it->second.end());
+    for (size_t i = at + 3; i < all.size(); i += 8) all[i] = (float)k;
+  }
+  const uint32_t n = (uint32_t)(all.size() / 8);
+  if (n > s->dripCap) {
+    CK(cudaStreamSynchronize(q));
+    drop_graphs(s);   // captured steps hold the old buffer
+    if (s->drip) cudaFree(s->drip);
+    s->drip = nullptr;
+    s->dripCap = 0;
+    CK(dalloc(&s->drip, 2 * (size_t)n));
+    s->dripCap = n;
+  }
+  if (n) {
+    CK(cudaMemcpyAsync(s->drip, all.data(), all.size() * sizeof(float), cudaMemcpyHostToDevice, q));
+    CK(cudaStreamSynchronize(q));
+  }
+  s->ndrip = n;
+  s->dripSig = sig;
   return ST_OK;
 }
 
@@ -394,6 +442,9 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
   P.airOn = airOn ? 1u : 0u; P.airCouple = airOn ? o->air_couple : 0.0f; P.airDecay = airOn ? o->air_decay : 0.0f;
   P.airH = s->airCells ? (float)s->airH : 1.0f; P.airBlur = airOn ? o->air_blur : 0.0f;
   P.aNx = s->airCells ? s->aNx : 1u; P.aNy = s->airCells ? s->aNy : 1u; P.aNz = s->airCells ? s->aNz : 1u;
+  // drips (words 79-81): on only with whitewater on this step
+  const bool drOn = sprOn && o->drip_on != 0;
+  P.ndrip = drOn ? s->ndrip : 0u; P.dripRate = drOn ? o->drip_rate : 0.0f; P.dripDry = drOn ? o->drip_dry : 1.0f;
   uint32_t nf = init ? (uint32_t)std::min<size_t>(s->fills.size() / 8, 8) : 0u;
   P.nfill = nf;
   for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &s->fills[k * 8], 8 * sizeof(float));
@@ -441,7 +492,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(7);
   nl += launch_g2p(B, gT, q);
   mark(8);
-  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, gT4, q);
+  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, s->hp.ndrip != 0, gT4, q);
   mark(9);
   if (nbOn) nl += launch_nb_reseed(B, gT4, q);
   mark(10);
@@ -453,7 +504,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
 // external event-record nodes, pointed at the timing ring's events before each launch.
 static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, bool timing) {
   return (uint64_t)s->cur | ((uint64_t)s->parity << 1) | ((uint64_t)nbOn << 2) | ((uint64_t)sprOn << 3) | ((uint64_t)timing << 4) |
-         ((uint64_t)(s->hp.airOn != 0) << 5) |
+         ((uint64_t)(s->hp.airOn != 0) << 5) | ((uint64_t)(s->hp.ndrip != 0) << 6) |
          ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24);
 }
 static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, bool timing, st_flip::Graph** out) {
@@ -524,9 +575,13 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   s->ring_i = (s->ring_i + 1) % st_flip::RING;
   CK(cudaEventSynchronize(upEv));
   uint32_t nc = 0;
-  st_status st = pack_colliders(s, o, nc, up->cols);
+  st_status st = pack_colliders(s, o, nc, up->cols, q);
   if (st != ST_OK) return st;
   const bool sprOn = o->spray_on != 0 && s->sprayCap > 0;
+  if (sprOn && o->drip_on) {
+    st = drip_update(s, o, nc, q);
+    if (st != ST_OK) return st;
+  }
   s->seed = s->seed + 1u;
   s->stamp = s->stamp + 1u;
   pack_params(s, dt, o, nc, init, nbOn, sprOn);
@@ -755,6 +810,18 @@ st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims
   return ST_OK;
 }
 
+st_status st_flip_read_drips(st_flip* s, float* out8, uint32_t cap, uint32_t* n) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (n) *n = s->ndrip;
+  const uint32_t m = std::min(cap, s->ndrip);
+  if (out8 && m) {
+    CK(cudaMemcpyAsync(out8, s->drip, (size_t)m * 32, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return ST_OK;
+}
+
 st_status st_flip_read_grid(st_flip* s, const st_flip_grid* g) {
   if (!s || !g) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));
@@ -847,11 +914,11 @@ st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const
 // ---- full checkpoint: every buffer a step reads before it writes, plus the host step state ----
 struct FullHdr {
   uint32_t magic, version, nx, ny, nz, ntiles, ncell, maxN, sprayCap;
-  uint32_t N, cap, ring, seed, steps, stamp, parity, cur, velGOn, nbInit, nfills, pad;
+  uint32_t N, cap, ring, seed, steps, stamp, parity, cur, velGOn, nbInit, nfills, ndrip, nsig, pad[2];
   double tm;
 };
 static constexpr uint32_t FULL_MAGIC = 0x53544650u;   // "PFTS"
-static constexpr uint32_t FULL_VERSION = 2;           // 2: the air field follows the whitewater pools
+static constexpr uint32_t FULL_VERSION = 3;           // 3: the air field and the drip samples follow the whitewater pools
 static void full_parts(st_flip* s, std::vector<std::pair<void*, size_t>>& v) {
   const size_t C = s->ncell, T = s->ntiles, SC = std::max<size_t>(s->sprayCap, 1), N = s->N;
   v = {{s->dCtl, sizeof(Ctl)}, {s->part[s->cur], N * sizeof(Part)}, {s->ids[s->cur], N * 4}, {s->need, T * 4}, {s->on, T},
@@ -859,14 +926,16 @@ static void full_parts(st_flip* s, std::vector<std::pair<void*, size_t>>& v) {
        {s->rhs, C * 4}, {s->acc, 6 * C * 4}, {s->vn, 3 * C * 4}, {s->vo, 3 * C * 4}, {s->velG, 3 * C * 4}, {s->sorInfo, C * 2},
        {s->wet, C * 4}, {s->sPos, SC * 16}, {s->sVel, SC * 16}};
   if (s->airCells) v.push_back({s->air, (size_t)s->airCells * 16});
+  if (s->ndrip) v.push_back({s->drip, (size_t)s->ndrip * 32});
 }
+static size_t pad4(size_t n) { return (n + 3) & ~(size_t)3; }
 
 st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size) {
   if (!s || !size) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));
   std::vector<std::pair<void*, size_t>> parts;
   full_parts(s, parts);
-  uint64_t need = sizeof(FullHdr) + s->fills.size() * sizeof(float);
+  uint64_t need = sizeof(FullHdr) + s->fills.size() * sizeof(float) + pad4(s->dripSig.size());
   for (auto& p : parts) need += p.second;
   *size = need;
   if (!buf) return ST_OK;
@@ -876,10 +945,14 @@ st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size)
   h.ncell = s->ncell; h.maxN = s->maxN; h.sprayCap = s->sprayCap; h.N = s->N; h.cap = s->cap; h.ring = s->ring; h.seed = s->seed;
   h.steps = s->steps; h.stamp = s->stamp; h.parity = s->parity; h.cur = (uint32_t)s->cur; h.velGOn = s->velGOn ? 1u : 0u;
   h.nbInit = s->nbInit; h.nfills = (uint32_t)s->fills.size(); h.tm = s->tm;
+  h.ndrip = s->ndrip; h.nsig = (uint32_t)s->dripSig.size();
   char* out = static_cast<char*>(buf);
   memcpy(out, &h, sizeof(h));
   out += sizeof(h);
   if (!s->fills.empty()) { memcpy(out, s->fills.data(), s->fills.size() * sizeof(float)); out += s->fills.size() * sizeof(float); }
+  memset(out, 0, pad4(s->dripSig.size()));
+  memcpy(out, s->dripSig.data(), s->dripSig.size());
+  out += pad4(s->dripSig.size());
   for (auto& p : parts) {
     if (p.second) CK(cudaMemcpyAsync(out, p.first, p.second, cudaMemcpyDeviceToHost, s->stream));
     out += p.second;
@@ -902,9 +975,18 @@ st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
   CK(cudaStreamSynchronize(s->stream));
   s->N = h.N; s->cap = h.cap; s->ring = h.ring; s->seed = h.seed; s->steps = h.steps; s->stamp = h.stamp; s->parity = h.parity;
   s->cur = (int)h.cur; s->velGOn = h.velGOn != 0; s->nbInit = h.nbInit; s->tm = h.tm;
+  if (h.ndrip > s->dripCap) {
+    drop_graphs(s);
+    if (s->drip) cudaFree(s->drip);
+    s->drip = nullptr;
+    s->dripCap = 0;
+    CK(dalloc(&s->drip, 2 * (size_t)h.ndrip));
+    s->dripCap = h.ndrip;
+  }
+  s->ndrip = h.ndrip;
   std::vector<std::pair<void*, size_t>> parts;
   full_parts(s, parts);
-  uint64_t need = sizeof(FullHdr) + (uint64_t)h.nfills * sizeof(float);
+  uint64_t need = sizeof(FullHdr) + (uint64_t)h.nfills * sizeof(float) + pad4(h.nsig);
   for (auto& p : parts) need += p.second;
   if (size < need) {
     snprintf(g_err, sizeof(g_err), "load_full: %llu bytes given, %llu needed", (unsigned long long)size, (unsigned long long)need);
@@ -913,6 +995,8 @@ st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
   const char* in = static_cast<const char*>(buf) + sizeof(FullHdr);
   s->fills.assign(reinterpret_cast<const float*>(in), reinterpret_cast<const float*>(in) + h.nfills);
   in += (size_t)h.nfills * sizeof(float);
+  s->dripSig.assign(in, h.nsig);
+  in += pad4(h.nsig);
   for (auto& p : parts) {
     if (p.second) CK(cudaMemcpyAsync(p.first, in, p.second, cudaMemcpyHostToDevice, s->stream));
     in += p.second;

@@ -35,8 +35,13 @@ struct FlipParams {
   float band, wwFoamLife, wwRise, wwCrest, wwImpact;
   uint32_t airOn, aNx, aNy, aNz;          // air field (words 72-83 of the reference's block)
   float airCouple, airDecay, airH, airBlur;
+  uint32_t ndrip;                         // drips (words 79-81)
+  float dripRate, dripDry;
+  uint32_t padW;
   float fills[16][4];
 };
+// the collider records follow the block in the upload buffer and are read as float4
+static_assert(sizeof(FlipParams) % 16 == 0, "FlipParams must keep 16-byte multiples");
 
 // Device counters (the reference's ctl words, src/flip/wgsl-core.js:38-40, plus this design's own).
 struct Ctl {
@@ -108,6 +113,7 @@ struct Bufs {
   float4* air;
   float4* air2;
   int32_t* airAcc;      // 4 per air cell: sum of v w 256 (x, y, z) and of w 256
+  float4* drip;         // 2 per drip sample (dripSamples, src/flip/bake.js:19-40): local position + collider, local normal + wetness
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)
   const float* sdf;

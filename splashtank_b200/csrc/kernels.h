@@ -1,5 +1,8 @@
 // kernels.h - host-side launchers of the FLIP and PBF kernels (defined next to the kernels they launch).
 #pragma once
+#include <vector>
+
+#include "../../include/splashtank_cuda.h"
 #include "common.cuh"
 
 namespace st {
@@ -24,8 +27,10 @@ int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 // whitewater (flip_extra.cu)
-// airCells: air-field cells to step first (0 when the air field is off this step)
-int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, int grid, cudaStream_t s);
+// airCells: air-field cells to step first (0 when the air field is off this step); drip: step the drip samples last
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, bool drip, int grid, cudaStream_t s);
+// drip samples of one collider's distance grid (drips.cpp), appended to out: 8 floats each
+void drip_samples(const st_sdf* sdf, double h, uint32_t k, std::vector<float>& out);
 // frames and bake measurements (frames.cu)
 struct FrameBox { double x0, y0, z0, kx, ky, kz, ks; };
 struct DiagBox { double x0, y0, z0, x1, y1, z1, hy, cap; };

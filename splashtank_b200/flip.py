@@ -125,6 +125,10 @@ def make_opts(o, opt=None, default=None):
     s.air_couple = float((air or {}).get("couple", 0.0))
     s.air_decay = float((air or {}).get("decay", 0.0))
     s.air_blur = float((air or {}).get("blur", 0.35))
+    drip = o.get("drip")
+    s.drip_on = 1 if (drip and drip.get("on")) else 0
+    s.drip_rate = float((drip or {}).get("rate", 0.0))
+    s.drip_dry = float((drip or {}).get("dry", 1.0))
     return s, cols
 
 
@@ -365,6 +369,15 @@ class FlipSim:
         a = np.zeros((nz * ny * nx, 4), np.float32)
         self._check(self.f["flip_read_air"](self._h, a.ctypes.data_as(abi.f32p), nx * ny * nz, dims), "readAir")
         return a[:, :3].reshape(nz, ny, nx, 3)
+
+    def read_drips(self):
+        """The drip samples: (n, 8) float32 rows of local position, collider number, local normal, wetness."""
+        n = C.c_uint32()
+        self._check(self.f["flip_read_drips"](self._h, None, 0, C.byref(n)), "readDrips")
+        a = np.zeros((n.value, 8), np.float32)
+        if n.value:
+            self._check(self.f["flip_read_drips"](self._h, a.ctypes.data_as(abi.f32p), n.value, C.byref(n)), "readDrips")
+        return a
 
     def grid(self):
         """Every cell of the tile box: tile_on, cnt, ctype, pres, rhs, vn, vo, velg (dense numpy arrays)."""

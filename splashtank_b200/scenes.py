@@ -63,7 +63,8 @@ class WaveTank:
     all the way down, depth field and kept grid velocity maintained, refill of thin calm cells); whitewater with the app's
     settings except an emission speed threshold of 0.25 m/s so the slow piston waves throw off points; the air field on
     with the app's coupling 3 and decay 0.6 (src/app/00-state.js:9, so spray and mist drift with the air the water and
-    spray drag along); air drag 0.3 with gusts, sheet tearing below 2 particles, 30 SOR iterations, dt = 1/240.
+    spray drag along); drips on with the app's rate 2 and drying time 3 s (the colliders drip after they leave the
+    water); air drag 0.3 with gusts, sheet tearing below 2 particles, 30 SOR iterations, dt = 1/240.
     """
 
     def __init__(self, n=256, seed=7, spray_cap=4_000_000, band=1e4, steps=200):
@@ -87,7 +88,7 @@ class WaveTank:
         self.sphere_keys = [dict(t=0.0, x=0.15, y=0.55, z=0.0), dict(t=T, x=0.15, y=0.12, z=0.0)]
         self.opts = dict(g=9.81, flip=0.95, comp=6.0, iters=30, vmax=50.0, drag=0.3, gust=1.0, foamSens=1.0, foamTau=1.2,
                          tear=2.0, vs=1.0, colMax=100.0, spr=dict(APP_SPRAY, min=0.25), nb=dict(on=True, band=band),
-                         air=dict(on=True, couple=3.0, decay=0.6))
+                         air=dict(on=True, couple=3.0, decay=0.6), drip=dict(on=True, rate=2.0, dry=3.0))
         self.fill_box = (self.xf0, -1e4, -1e4, 1e4, 0.3, 1e4)   # x0, y0, z0, x1, y1, z1 (faces on walls pushed out)
 
     def states(self, t):

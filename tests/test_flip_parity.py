@@ -153,6 +153,29 @@ def test_air_field_with_whitewater(spray_cap):
     assert_same_state(g, o, spray=True)
 
 
+def test_drips_from_a_rising_sphere():
+    """A sphere lifted out of the water drips (no other emission): drip samples, their wetness, the drops in the
+    whitewater pool, the air field they push and the water agree bit for bit after 60 steps."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    from splashtank_b200.scene import SceneRunner, sphere_sdf
+    sc = scenes.dam_break(32)
+    sdf = sphere_sdf(0.1, 0.01, sid=5)
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY, rate=0.0), air=dict(on=True, couple=3.0, decay=0.6),
+                drip=dict(on=True, rate=20.0, dry=3.0))
+    g, o = make_pair(sc, spray_cap=20000)
+    runs, t = [SceneRunner(s) for s in (g, o)], 0.0
+    for _ in range(60):
+        t += sc["dt"]
+        st = [dict(id=1, sdf=sdf, x=-0.3, y=0.3 + min(1.0, t / 0.15) * 0.55, z=0.0)]
+        for r in runs:
+            r.step(sc["dt"], st, opts)
+    assert g.readStats()["spray_used"] >= 20
+    da, db = g.read_drips(), o.read_drips()
+    assert len(da) > 0 and same(da, db), "drip samples"
+    assert_same_state(g, o, spray=True)
+
+
 def test_particle_state_round_trip():
     """save_state -> load_state -> save_state returns the same particles, ids and storage order."""
     from splashtank_b200 import scenes

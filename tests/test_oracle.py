@@ -162,6 +162,47 @@ def test_air_field_follows_the_water():
     assert a[..., 0].max() > 0.1 and a[..., 0].sum() > 0 and np.all(np.isfinite(a))
 
 
+def _drip_run(steps, y_of_t, dry=3.0, rate=20.0):
+    from splashtank_b200.scene import sphere_sdf
+    s, sc = dam(16, spray_cap=2000)
+    sdf = sphere_sdf(0.1, 0.01, sid=5)
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY, rate=0.0), drip=dict(on=True, rate=rate, dry=dry))
+    r, t = SceneRunner(s), 0.0
+    for _ in range(steps):
+        t += sc["dt"]
+        r.step(sc["dt"], [dict(id=1, sdf=sdf, x=-0.3, y=y_of_t(t), z=0.0)], opts)
+    return s, sc
+
+
+def test_drip_samples_lie_on_the_surface():
+    """dripSamples (src/flip/bake.js:19-40): points of the distance grid near the surface moved onto it along the
+    gradient, about one per solver cell of surface (4 pi r^2 / h^2 = 32 at h = 1/16, so the floor of 100 applies)."""
+    s, _ = _drip_run(1, lambda t: 0.8)
+    d = s.read_drips()
+    assert len(d) == 100
+    p, n = d[:, 0:3].astype(np.float64), d[:, 4:7].astype(np.float64)
+    assert np.all(d[:, 3] == 0)                                          # collider number
+    np.testing.assert_allclose(np.linalg.norm(p, axis=1), 0.1, atol=2e-3)   # on the sphere
+    np.testing.assert_allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-5)
+    assert np.min(np.sum(n * p, axis=1) / np.linalg.norm(p, axis=1)) > 0.99   # normals point out
+    assert np.all(d[:, 7] == 0)                                          # out of the water from the start: dry
+
+
+def test_drips_wet_in_water_then_dry_out():
+    """A sphere held in the water is wet (1); lifted out, its wetness falls by dt / dry a step (dripStep,
+    src/flip/wgsl-whitewater.js:254-278) and it lets go of drops, which fly as spray with twice the spray life."""
+    s, sc = _drip_run(8, lambda t: 0.3)
+    assert np.all(s.read_drips()[:, 7] == 1.0)                           # in the water everywhere
+    s2, sc = _drip_run(8 + 30, lambda t: 0.3 if t < 8.5 * sc["dt"] else 0.9)
+    w = s2.read_drips()[:, 7]
+    assert np.all(w < 1.0) and np.all(w > 1.0 - 31 * sc["dt"] / 3.0)
+    np.testing.assert_allclose(w.max(), 1.0 - 30 * sc["dt"] / 3.0, atol=1e-4)
+    st, sp = s2.readStats(), s2.readSpray()
+    assert st["spray_used"] > 0
+    alive = sp["p"][:, 3] > 0
+    assert np.all(sp["v"][alive, 3] < 0.5)                               # spray kind (the fraction is time held)
+
+
 @pytest.mark.parametrize("name", ["dam_break_16_s10", "wave_tank_24_s8"])
 def test_golden_fixture(name):
     """The oracle still produces the committed fixtures (tests/golden/make_golden.py) bit for bit."""
