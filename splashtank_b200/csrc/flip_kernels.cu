@@ -892,7 +892,10 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
       const bool gone = q.p.y < DEADY;
       uint32_t kc = 0;
-      if (!gone && needWet) {
+      // e is 0 (or NaN) unless the particle is fast enough for crest (speed over sprMin) or churn (over 0.5): the
+      // common slow particle skips the eight wetness reads (kc stays 0 either way)
+      const float xs = len3(xyz(q.v)) * P.vs;
+      if (!gone && needWet && U.settle != 0.0f && (xs - P.sprMin > 0.0f || xs > 0.5f)) {
         float rho, fast, e;
         // the eight cells around the moved particle: from the window when it holds them
         const V3 bcf = vfloor((xyz(q.p) - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
