@@ -681,8 +681,7 @@ __device__ float vnz(V3 x) {   // value noise (wgsl-solver.js:202-207)
 }
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
-  const float* vn;   // [3][1000]
-  const float* vo;
+  const float2* v;   // [3][1000]: (vn, vo) of each face, one 64-bit load per corner
   const int32_t* cnt;
   const float* wet;      // wetCellAt of each window cell (0 outside the domain)
   const uint8_t* kill;   // the narrow band's trim test of each window cell
@@ -709,15 +708,15 @@ __device__ __forceinline__ void sampleWin(const FlipParams& P, const G2PWin& W, 
     const int xa = clampi(i0, 0, hx), xb = clampi(i0 + 1, 0, hx);
     const int ya = clampi(j0, 0, hy), yb = clampi(j0 + 1, 0, hy);
     const int za = clampi(k0, 0, hz), zb = clampi(k0 + 1, 0, hz);
-    const float* wn = W.vn + axis * 1000;
-    const float* wo = W.vo + axis * 1000;
+    const float2* wv = W.v + axis * 1000;
     float sn = 0.0f, so = 0.0f;
     for (int c = 0; c < 8; c++) {
       const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
       const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
       const int f = W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za);
-      sn += w * wn[f];
-      so += w * wo[f];
+      const float2 fv = wv[f];
+      sn += w * fv.x;
+      so += w * fv.y;
     }
     rn[axis] = sn;
     ro[axis] = so;
@@ -852,7 +851,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
 constexpr int G2P_T = 256;
 __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   __shared__ FlipParams P;
-  __shared__ float wvn[3 * 1000], wvo[3 * 1000];
+  __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
@@ -866,7 +865,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wvn, wvo, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wv, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
     const G2PUni U = g2pUni(P);
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
@@ -877,7 +876,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
         continue;
       }
       const uint32_t c = cellIdx(P, gi, gj, gk);
-      for (int ax = 0; ax < 3; ax++) { wvn[ax * 1000 + r] = B.vn[ax * nc + c]; wvo[ax * 1000 + r] = B.vo[ax * nc + c]; }
+      for (int ax = 0; ax < 3; ax++) wv[ax * 1000 + r] = make_float2(B.vn[ax * nc + c], B.vo[ax * nc + c]);
       wcnt[r] = B.cnt[c];
       if (needWet) wwet[r] = inDom(P, gi, gj, gk) ? B.wet[c] : 0.0f;
       if (needKill) wkill[r] = (B.on[c >> 9] && phiOfBits(B.ctype[c]) < -P.band) ? 1 : 0;
