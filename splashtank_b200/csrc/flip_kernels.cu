@@ -682,6 +682,7 @@ __device__ float vnz(V3 x) {   // value noise (wgsl-solver.js:202-207)
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
   const float2* v;   // [3][1000]: (vn, vo) of each face, one 64-bit load per corner
+  const float* csum;     // [9][9][9]: g2p's summed counts of the 2 x 2 x 2 cells from (ox - 1, oy - 1, oz - 1) + (x, y, z)
   const int32_t* cnt;
   const float* wet;      // wetCellAt of each window cell (0 outside the domain)
   const uint8_t* kill;   // the narrow band's trim test of each window cell
@@ -727,9 +728,9 @@ __device__ __forceinline__ void sampleWin(const FlipParams& P, const G2PWin& W, 
 // The gust noise's hash lattice has spacing 1 in units of p * 0.55, so a whole tank spans only a few lattice points.
 // Each CTA hashes them once into a table (the same hsh3 on the same integer-valued inputs, so the values are identical);
 // points outside the table are hashed directly.
-constexpr int GT_MAX = 512;
+constexpr int GT_MAX = 256;   // lattice points per noise: 6^3 covers boxes up to about 3.5 m a side
 struct GustTab {
-  float v[3][GT_MAX];
+  float2 v[3][GT_MAX];   // (hash at a lattice point, hash at the next point along x): one 64-bit load per pair
   int lo[3][3], n[3][3];
   bool on;
 };
@@ -739,10 +740,11 @@ __device__ __forceinline__ float vnzTab(const GustTab& T, int which, V3 x) {
   const int ix = (int)i.x - T.lo[which][0], iy = (int)i.y - T.lo[which][1], iz = (int)i.z - T.lo[which][2];
   const int nx = T.n[which][0], ny = T.n[which][1], nz = T.n[which][2];
   if (!T.on || ix < 0 || iy < 0 || iz < 0 || ix + 1 >= nx || iy + 1 >= ny || iz + 1 >= nz) return vnz(x);
-  const float* t = T.v[which];
+  const float2* t = T.v[which];
   const int b = ix + nx * (iy + ny * iz), sy = nx, sz = nx * ny;
-  const float a = mixf(mixf(t[b], t[b + 1], u.x), mixf(t[b + sy], t[b + sy + 1], u.x), u.y);
-  const float c = mixf(mixf(t[b + sz], t[b + sz + 1], u.x), mixf(t[b + sz + sy], t[b + sz + sy + 1], u.x), u.y);
+  const float2 t0 = t[b], t1 = t[b + sy], t2 = t[b + sz], t3 = t[b + sz + sy];
+  const float a = mixf(mixf(t0.x, t0.y, u.x), mixf(t1.x, t1.y, u.x), u.y);
+  const float c = mixf(mixf(t2.x, t2.y, u.x), mixf(t3.x, t3.y, u.x), u.y);
   return mixf(a, c, u.z);
 }
 __device__ void buildGust(const FlipParams& P, GustTab& T) {
@@ -769,7 +771,8 @@ __device__ void buildGust(const FlipParams& P, GustTab& T) {
     const int nx = T.n[w][0], ny = T.n[w][1], nz = T.n[w][2];
     for (int r = threadIdx.x; r < nx * ny * nz; r += blockDim.x) {
       const int ix = r % nx, iy = (r / nx) % ny, iz = r / (nx * ny);
-      T.v[w][r] = hsh3(v3((float)(ix + T.lo[w][0]), (float)(iy + T.lo[w][1]), (float)(iz + T.lo[w][2])));
+      const V3 x = v3((float)(ix + T.lo[w][0]), (float)(iy + T.lo[w][1]), (float)(iz + T.lo[w][2]));
+      T.v[w][r] = make_float2(hsh3(x), hsh3(v3((float)(ix + 1 + T.lo[w][0]), x.y, x.z)));
     }
   }
   __syncthreads();
@@ -794,13 +797,11 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const bool fast = P.q12 > 0.5f;
   if (P.q9 < 0.5f && fast) csum = 8.0f * (float)W.cnt[W.idx(fi, fj, fk)];
   else if (P.q9 < 0.5f) {
-    csum = 0.0f;
-    const int xa = clampi(bi, 0, (int)P.nx - 1), xb = clampi(bi + 1, 0, (int)P.nx - 1);
-    const int ya = clampi(bj, 0, (int)P.ny - 1), yb = clampi(bj + 1, 0, (int)P.ny - 1);
-    const int za = clampi(bk, 0, (int)P.nz - 1), zb = clampi(bk + 1, 0, (int)P.nz - 1);
-    for (int dz = 0; dz <= 1; dz++)
-      for (int dy = 0; dy <= 1; dy++)
-        for (int dx = 0; dx <= 1; dx++) csum += (float)W.cnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
+    // the sum depends on the corner only through its clamp into [-1, n - 1], which the tile's particles keep within
+    // the staged 9^3 block (the outer clamp only keeps the shared-memory index in bounds)
+    const int x = clampi(clampi(bi, -1, (int)P.nx - 1) - (W.ox - 1), 0, 8), y = clampi(clampi(bj, -1, (int)P.ny - 1) - (W.oy - 1), 0, 8);
+    const int z = clampi(clampi(bk, -1, (int)P.nz - 1) - (W.oz - 1), 0, 8);
+    csum = W.csum[x + 9 * (y + 9 * z)];
   }
   const float rho = csum / (8.0f * P.rest);
   const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
@@ -853,6 +854,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
+  __shared__ float wcsum[729];
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
   __shared__ ColPre cpre[32];
@@ -865,7 +867,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wv, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wv, wcsum, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
     const G2PUni U = g2pUni(P);
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
@@ -882,6 +884,22 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
       if (needKill) wkill[r] = (B.on[c >> 9] && phiOfBits(B.ctype[c]) < -P.band) ? 1 : 0;
     }
     __syncthreads();
+    // the local density's count sums (g2p's foam terms, wgsl-solver.js:222-229) of every corner a particle of this tile
+    // can have: integer-valued floats, so the sum is exact in any order
+    if (P.q9 < 0.5f && !(P.q12 > 0.5f)) {
+      for (int r = threadIdx.x; r < 729; r += G2P_T) {
+        const int bi = W.ox - 1 + r % 9, bj = W.oy - 1 + (r / 9) % 9, bk = W.oz - 1 + r / 81;
+        const int xa = clampi(bi, 0, (int)P.nx - 1), xb = clampi(bi + 1, 0, (int)P.nx - 1);
+        const int ya = clampi(bj, 0, (int)P.ny - 1), yb = clampi(bj + 1, 0, (int)P.ny - 1);
+        const int za = clampi(bk, 0, (int)P.nz - 1), zb = clampi(bk + 1, 0, (int)P.nz - 1);
+        float cs = 0.0f;
+        for (int dz = 0; dz <= 1; dz++)
+          for (int dy = 0; dy <= 1; dy++)
+            for (int dx = 0; dx <= 1; dx++) cs += (float)wcnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
+        wcsum[r] = cs;
+      }
+      __syncthreads();
+    }
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
     uint32_t emitSum = 0, deadSum = 0;
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
