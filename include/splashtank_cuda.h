@@ -178,6 +178,37 @@ st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t 
 /* FlipSim.readSpray (src/flip/sim.js:423-437): whitewater slots handed out (positions with life in w,
  * velocities with kind in w). */
 st_status st_flip_read_spray(st_flip* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
+/* The live view (FlipSim.dispPack + pump, src/flip/sim.js:381-404, 506-525; kernels subsample, sprayDisp, deepPick and
+ * packDisp, src/flip/wgsl-solver.js:141-147, src/flip/wgsl-whitewater.js:196-297): a sample of the water (the first
+ * n_water particles of the storage order, or every stride-th one when there are more than 300,000 or when whitewater
+ * or deep water is shown), up to 200,000 whitewater points (every stride-th slot handed out, the living ones) and, with
+ * the deep look on, up to 200,000 deep-water points, packed in packLayout's 32-bit words: word 0 whitewater points,
+ * word 1 deep points, 2 zero words, then the parts at the offsets below (positions 3 x uint16 across the box, water
+ * speed and white-water bytes, whitewater codes, deep speed bytes). The reference's order of the compacted
+ * whitewater and deep points is that of its atomics; here it is ascending slot and tile-major cell. With words null
+ * only the layout is filled; a smaller cap_words returns ST_OVERFLOW. */
+typedef struct st_live_layout {
+  uint32_t size;        /* sizeof(st_live_layout) */
+  uint32_t n_water, n_spray, n_deep;   /* capacities of the parts, in points */
+  uint32_t from_pos;    /* 1: the water part is the first n_water particles; 0: every stride-th */
+  uint32_t o_wp, o_ws, o_wf, o_sp, o_sk, o_dp, o_ds;   /* word offsets: water positions, speeds, white water; whitewater
+                                                          positions, codes; deep positions, speeds */
+  uint32_t words;       /* words in all */
+} st_live_layout;
+st_status st_flip_pack_live(st_flip* s, float vs, uint32_t* words, uint64_t cap_words, st_live_layout* layout);
+/* FlipSim.setDeepLook (src/flip/sim.js:406): show the narrow band's deep water (fluid cells with no particles). */
+st_status st_flip_set_deep_look(st_flip* s, int on);
+/* readDeep + packDeep (src/flip/sim.js:408-421, src/gpu.js:512-524): the deep-water points of the last step for a
+ * frame (deep look on and the narrow band on in that step; else *n = 0): positions 3 x uint16 across the box and speed
+ * bytes (16ths of the speed times vs, at most 191). Above 200,000 deep cells a fixed hashed sample is kept, sized from
+ * the previous call's count. *n receives the count; at most cap are written (ST_OVERFLOW when more). */
+st_status st_flip_read_deep(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint32_t cap, uint32_t* n);
+/* packSprayFrame (src/flip/bake.js:43-58): the whitewater part of a frame. Of the slots handed out, every step-th
+ * (step = max(1, ceil(alive / max_points))) that is alive, in slot order: positions 3 x uint16 across the box and the
+ * 32-bit codes of packSprayJS (foam_life 0 means 3). *n receives the points, *alive the living slots; at most cap are
+ * written (ST_OVERFLOW when more). */
+st_status st_flip_read_spray_frame(st_flip* s, uint32_t max_points, float foam_life, uint16_t* pos, uint32_t* pk, uint32_t cap,
+                                   uint32_t* n, uint32_t* alive);
 /* The air field (src/flip/wgsl-whitewater.js:24-89, grid made by airAlloc, src/flip/sim.js:342-350): air velocity at
  * each air-cell centre, x fastest, 4 floats per cell (w 0). dims3 receives the air grid's cells per axis (0 0 0 when
  * the handle has no whitewater pool, which the air field needs); at most cap cells are written. */

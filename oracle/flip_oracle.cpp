@@ -136,6 +136,10 @@ struct Oracle {
   // time and seed (sim.js:200, 207)
   double tm = 0;
   uint32_t seed = 0, steps = 0;
+  // the live view's state (sim.js:80, 184, 406): deep look, the last step's particle count and narrow band, and
+  // how many deep cells the previous deep pass saw (ctl[12])
+  bool deepOn = false, lastNb = false;
+  uint32_t lastN = 0, deepPrev = 0;
   // stats
   uint32_t st_sc = 0, st_fluid = 0, st_ovf = 0, spray_ovf = 0, st_live = 0;
   float st_vmax = 0;
@@ -1135,6 +1139,27 @@ struct Oracle {
     }
   }
 
+  // ---- deepClear + deepPick + deepFin (wgsl-whitewater.js:282-297): fluid cells with no particles, as points at their
+  // centres (x, y, z, 4096 + speed), in ascending tile then cell order; above DEEPMAX cells seen by the previous pass, a
+  // fixed hashed sample ----
+  std::vector<float> deepPass() {
+    const uint32_t DEEPMAX = 200000u;
+    std::vector<float> out;
+    uint32_t seen = 0, picked = 0;
+    for (uint32_t tile : active) for (uint32_t local = 0; local < 512; local++) {
+      int i, j, k; tileCoord(tile, local, i, j, k); uint32_t c = tile * 512u + local;
+      if (!inDom(i, j, k) || (ctype[c] & 0xffu) != 1u || cnt[c] > 0) continue;
+      seen++;
+      if (deepPrev > DEEPMAX && hash1(c * 2654435761u + 7u) * (float)deepPrev >= (float)DEEPMAX) continue;
+      if (picked++ >= DEEPMAX) continue;
+      V3 x = cellCenter(i, j, k);
+      float rec[4] = {x.x, x.y, x.z, 4096.0f + fmin_(length(velGVec(x)), 63.0f)};
+      out.insert(out.end(), rec, rec + 4);
+    }
+    deepPrev = seen;
+    return out;
+  }
+
   // ---- FlipSim.step (sim.js:179-241, stage list :245-310) ----
   st_status step(double dt, const st_step_opts* o) {
     if (N == 0) return ST_NOT_READY;
@@ -1144,6 +1169,7 @@ struct Oracle {
     packCols(o);
     bool sprOn = o->spray_on != 0 && sprayCap > 0;
     if (sprOn && o->drip_on != 0) dripUpdate(o, ncols);
+    lastN = N; lastNb = nbOn;
     seed = seed + 1u;
     packParams(dt, o, init, nbOn, sprOn);
     tm = tm + dt;
@@ -1227,6 +1253,19 @@ st_status oracle_flip_read_drips(void* h, float* out8, uint32_t cap, uint32_t* n
   if (n) *n = s->ndrip;
   uint32_t m = std::min(cap, s->ndrip);
   if (out8 && m) memcpy(out8, s->drip.data(), (size_t)m * 32);
+  return ST_OK;
+}
+st_status oracle_flip_set_deep_look(void* h, int on) { ((Oracle*)h)->deepOn = on != 0; return ST_OK; }
+// one deep pass when the deep look applies (deep look on, narrow band and kept velocities on at the last step), as
+// float4 points; *n receives the count (0 when it does not apply)
+st_status oracle_flip_deep_points(void* h, float* out4, uint32_t cap, uint32_t* n) {
+  Oracle* s = (Oracle*)h;
+  if (n) *n = 0;
+  if (!(s->deepOn && s->lastNb && s->velGOn && s->lastN)) return ST_OK;
+  std::vector<float> d = s->deepPass();
+  uint32_t m = (uint32_t)(d.size() / 4);
+  if (n) *n = m;
+  if (out4) memcpy(out4, d.data(), (size_t)std::min(m, cap) * 16);
   return ST_OK;
 }
 st_status oracle_flip_stats(void* h, st_stats* o) {

@@ -35,6 +35,9 @@ def funcs():
         f["spray_overflow"] = lib.oracle_flip_spray_overflow
         f["spray_overflow"].argtypes = [C.c_void_p]
         f["spray_overflow"].restype = C.c_uint32
+        f["deep_points"] = lib.oracle_flip_deep_points
+        f["deep_points"].argtypes = [C.c_void_p, abi.f32p, C.c_uint32, abi.u32p]
+        f["deep_points"].restype = C.c_int
         _FUNCS = f
     return _FUNCS
 
@@ -49,6 +52,14 @@ class OracleFlipSim(FlipSim):
 
     def stepTimed(self, dt, o):
         raise NotImplementedError("the oracle has no stage timer")
+
+    def deep_points(self):
+        """One deep pass (deepClear + deepPick + deepFin): (n, 4) float32 points x, y, z, 4096 + speed, or None when the
+        deep look does not apply."""
+        n = C.c_uint32()
+        out = np.zeros((200000, 4), np.float32)   # a pass writes at most 200,000 points
+        self.f["deep_points"](self._h, out.ctypes.data_as(abi.f32p), len(out), C.byref(n))
+        return out[:n.value].copy() if n.value else None
 
 
 _PBF = None

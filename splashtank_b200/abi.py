@@ -112,6 +112,7 @@ FLIP_FUNCS = [
     ("flip_read_spray", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
     ("flip_read_air", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
     ("flip_read_drips", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
+    ("flip_set_deep_look", C.c_int, [C.c_void_p, C.c_int]),
     ("flip_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("flip_read_grid", C.c_int, [C.c_void_p, C.POINTER(Grid)]),
     ("flip_get_dims", C.c_int, [C.c_void_p, C.POINTER(Dims)]),
@@ -126,7 +127,16 @@ class BakeDiag(C.Structure):
                 ("height_hist", C.c_uint32 * 16)]
 
 
+class LiveLayout(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("n_water", C.c_uint32), ("n_spray", C.c_uint32), ("n_deep", C.c_uint32), ("from_pos", C.c_uint32),
+                ("o_wp", C.c_uint32), ("o_ws", C.c_uint32), ("o_wf", C.c_uint32), ("o_sp", C.c_uint32), ("o_sk", C.c_uint32),
+                ("o_dp", C.c_uint32), ("o_ds", C.c_uint32), ("words", C.c_uint32)]
+
+
 CUDA_ONLY_FUNCS = [
+    ("flip_pack_live", C.c_int, [C.c_void_p, C.c_float, u32p, C.c_uint64, C.POINTER(LiveLayout)]),
+    ("flip_read_deep", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, C.c_uint32, u32p]),
+    ("flip_read_spray_frame", C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_uint16), u32p, C.c_uint32, u32p, u32p]),
     ("flip_read_frame", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, u8p, C.c_uint32, u32p, C.POINTER(C.c_int32)]),
     ("flip_bake_diag", C.c_int, [C.c_void_p, C.c_float, C.POINTER(BakeDiag)]),
     ("flip_save_full", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),

@@ -109,6 +109,17 @@ struct st_flip {
   std::map<uint32_t, std::vector<float>> dripCache;   // per grid id: its samples (collider number 0)
   uint8_t* emitK = nullptr;
   uint32_t *blkEmit = nullptr, *deadList = nullptr;
+  // the live view and a frame's whitewater / deep-water parts (allocated by their first call)
+  static constexpr uint32_t DISP_MAX = 300000, SPRAY_DISP_MAX = 200000, DEEP_MAX = 200000;
+  bool deepOn = false, lastNb = false;
+  uint32_t lastN = 0, stride = 1, deepPrev = 0;
+  float4* deepBuf = nullptr;       // DEEP_MAX deep-water points of the last pass
+  uint32_t* viewScratch = nullptr; // per-block or per-tile counts, then 2 counters
+  size_t viewScratchN = 0;
+  uint32_t* liveOut = nullptr;     // the packed live view
+  size_t liveWords = 0;
+  uint8_t* framePart = nullptr;    // packed whitewater or deep-water points of a frame
+  size_t framePartBytes = 0;
   cudaEvent_t ev[16] = {};
   int cur = 0;   // part[cur] holds this step's storage order
   uint64_t launches = 0;   // kernels launched by steps since create
@@ -162,7 +173,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->drip, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
+                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->drip, s->deepBuf, s->viewScratch, s->liveOut, s->framePart, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -586,6 +597,10 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   s->stamp = s->stamp + 1u;
   pack_params(s, dt, o, nc, init, nbOn, sprOn);
   s->tm = s->tm + dt;
+  // the live view's water sample (src/flip/sim.js:184): every stride-th particle, at most about DISP_MAX
+  s->stride = std::max<uint32_t>(1u, (uint32_t)((s->N + st_flip::DISP_MAX - 1) / st_flip::DISP_MAX));
+  s->lastN = s->N;
+  s->lastNb = nbOn;
   if (init) { s->nbInit = 0; s->fills.clear(); }
   const int iters = std::max(1, o->iters);
   // this step's storage order goes into the other particle buffer; cell counts alternate buffers
@@ -708,6 +723,140 @@ st_status st_flip_read_particles(st_flip* s, float* pos4, float* vel4, uint32_t 
   CK(cudaMemcpyAsync(pos4, tmp, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
   if (vel4) CK(cudaMemcpyAsync(vel4, tmp + s->N, (size_t)m * 16, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  return ST_OK;
+}
+
+// ---- the live view and a frame's whitewater / deep-water parts (live.cu) ----
+}  // extern "C"
+template <class T>
+static cudaError_t grow(T** p, size_t& have, size_t need) {   // a device buffer of at least need elements
+  if (need <= have && *p) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  have = 0;
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(need, 1) * sizeof(T));
+  if (e == cudaSuccess) have = need;
+  return e;
+}
+extern "C" {
+static FrameBox frame_box(const st_flip* s, float vs) {
+  return FrameBox{s->bx0, s->by0, s->bz0, 65535.0 / (s->bx1 - s->bx0), 65535.0 / (s->by1 - s->by0), 65535.0 / (s->bz1 - s->bz0),
+                  16.0 * (vs != 0.0f ? (double)vs : 1.0)};
+}
+static bool deep_ready(const st_flip* s) { return s->deepOn && s->lastNb && s->velGOn && s->lastN; }
+// deepClear + deepPick + deepFin (src/flip/wgsl-whitewater.js:282-297): the deep points into deepBuf; returns how many
+static st_status deep_pass(st_flip* s, uint32_t* n) {
+  if (!s->deepBuf) CK(cudaMalloc((void**)&s->deepBuf, (size_t)st_flip::DEEP_MAX * sizeof(float4)));
+  CK(grow(&s->viewScratch, s->viewScratchN, std::max<size_t>(s->ntiles, 1) + 2));
+  uint32_t* counts = s->viewScratch + std::max<size_t>(s->ntiles, 1);
+  const Bufs B = s->bufs();
+  launch_deep(B, s->deepPrev, s->ntiles, s->tileGrid(s->gridT4), s->viewScratch, counts, s->deepBuf, s->stream);
+  uint32_t h[2];
+  CK(cudaMemcpyAsync(h, counts, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  s->deepPrev = h[0];
+  *n = std::min(h[1], st_flip::DEEP_MAX);
+  return ST_OK;
+}
+
+st_status st_flip_set_deep_look(st_flip* s, int on) {
+  if (!s) return ST_BAD_ARG;
+  s->deepOn = on != 0;
+  return ST_OK;
+}
+
+st_status st_flip_read_deep(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint32_t cap, uint32_t* n) {
+  if (!s || !n) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  *n = 0;
+  if (!deep_ready(s)) return ST_OK;
+  uint32_t nd = 0;
+  st_status st = deep_pass(s, &nd);
+  if (st != ST_OK) return st;
+  *n = nd;
+  const uint32_t m = std::min(nd, cap);
+  if (!m) return nd ? ST_OVERFLOW : ST_OK;
+  CK(grow(&s->framePart, s->framePartBytes, (size_t)st_flip::DEEP_MAX * 7));
+  uint16_t* p16 = reinterpret_cast<uint16_t*>(s->framePart);
+  uint8_t* s8 = s->framePart + (size_t)st_flip::DEEP_MAX * 6;
+  launch_pack_deep(s->deepBuf, nd, frame_box(s, vs), p16, s8, s->stream);
+  if (pos) CK(cudaMemcpyAsync(pos, p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->stream));
+  if (spd) CK(cudaMemcpyAsync(spd, s8, m, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  return m < nd ? ST_OVERFLOW : ST_OK;
+}
+
+st_status st_flip_read_spray_frame(st_flip* s, uint32_t max_points, float foam_life, uint16_t* pos, uint32_t* pk, uint32_t cap,
+                                   uint32_t* n, uint32_t* alive) {
+  if (!s || !n) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  *n = 0;
+  if (alive) *alive = 0;
+  if (!s->sprayCap) return ST_OK;
+  uint32_t used = 0;
+  CK(cudaMemcpyAsync(&used, &s->dCtl->sctl0, 4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  const uint32_t nslots = std::max(1u, std::min(s->sprayCap, used));
+  const double fl = (foam_life == foam_life && foam_life != 0.0f) ? (double)foam_life : 3.0;   // foamLife || 3
+  CK(grow(&s->viewScratch, s->viewScratchN, std::max<size_t>((nslots + 255) / 256, s->ntiles) + 2));
+  uint32_t* counts = s->viewScratch + (s->viewScratchN - 2);
+  const size_t codesAt = ((size_t)s->sprayCap * 6 + 15) & ~(size_t)15;   // the codes start 16-byte aligned
+  CK(grow(&s->framePart, s->framePartBytes, std::max<size_t>(codesAt + (size_t)s->sprayCap * 4, (size_t)st_flip::DEEP_MAX * 7)));
+  uint16_t* p16 = reinterpret_cast<uint16_t*>(s->framePart);
+  uint32_t* k32 = reinterpret_cast<uint32_t*>(s->framePart + codesAt);
+  launch_spray_frame(s->sPos, s->sVel, nslots, max_points, frame_box(s, 1.0f), fl, s->viewScratch, p16, k32, counts, s->stream);
+  uint32_t h[2];
+  CK(cudaMemcpyAsync(h, counts, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  if (alive) *alive = h[0];
+  *n = h[1];
+  const uint32_t m = std::min(h[1], cap);
+  if (m && pos) CK(cudaMemcpyAsync(pos, p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->stream));
+  if (m && pk) CK(cudaMemcpyAsync(pk, k32, (size_t)m * 4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return m < h[1] ? ST_OVERFLOW : ST_OK;
+}
+
+// packLayout (src/flip/sim.js:371-376)
+static void live_layout(uint32_t nW, uint32_t nS, uint32_t nD, st_live_layout* L) {
+  const uint32_t gW = (nW + 3) / 4, gS = (nS + 3) / 4, gD = (nD + 3) / 4;
+  L->n_water = nW; L->n_spray = nS; L->n_deep = nD;
+  L->o_wp = 4; L->o_ws = L->o_wp + gW * 6; L->o_wf = L->o_ws + gW; L->o_sp = L->o_wf + gW; L->o_sk = L->o_sp + gS * 6;
+  L->o_dp = L->o_sk + gS * 4; L->o_ds = L->o_dp + gD * 6; L->words = L->o_ds + gD;
+}
+
+st_status st_flip_pack_live(st_flip* s, float vs, uint32_t* words, uint64_t cap_words, st_live_layout* L) {
+  if (!s || !L || L->size != sizeof(st_live_layout)) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  const uint32_t sdMax = std::min(s->sprayCap, st_flip::SPRAY_DISP_MAX);
+  const bool spr = sdMax > 0 && s->lastN, deep = deep_ready(s);
+  const bool fromPos = !spr && !deep && (s->stride <= 1 || !s->lastN);
+  const uint32_t nW = fromPos ? std::min(std::min(s->N, st_flip::DISP_MAX + 1), s->maxN) : (s->lastN + s->stride - 1) / s->stride;
+  live_layout(nW, spr ? sdMax : 0, deep ? st_flip::DEEP_MAX : 0, L);
+  L->from_pos = fromPos ? 1u : 0u;
+  if (!words) return ST_OK;
+  if (cap_words < L->words) return ST_OVERFLOW;
+  uint32_t nDeep = 0;
+  if (deep) {
+    st_status st = deep_pass(s, &nDeep);
+    if (st != ST_OK) return st;
+  }
+  CK(grow(&s->liveOut, s->liveWords, L->words));
+  CK(grow(&s->viewScratch, s->viewScratchN, std::max<size_t>((sdMax + 255) / 256, s->ntiles) + 2));
+  CK(cudaMemsetAsync(s->liveOut, 0, (size_t)L->words * 4, s->stream));
+  if (L->n_deep) CK(cudaMemsetAsync(s->liveOut + L->o_ds, 0xff, (size_t)(L->words - L->o_ds) * 4, s->stream));   // speed 255: no point
+  LiveBox K{(float)s->bx0, (float)s->by0, (float)s->bz0, (float)(65535.0 / (s->bx1 - s->bx0)), (float)(65535.0 / (s->by1 - s->by0)),
+            (float)(65535.0 / (s->bz1 - s->bz0)), vs != 0.0f ? vs : 1.0f, s->sprayCap, L->n_spray,
+            L->o_wp, L->o_ws, L->o_wf, L->o_sp, L->o_sk, L->o_dp, L->o_ds};
+  const Bufs B = s->bufs();
+  launch_live(B, K, nW, fromPos ? 1u : s->stride, spr ? sdMax : 0u, s->hp.wwFoamLife, s->deepBuf, nDeep, s->viewScratch, s->liveOut, s->stream);
+  CK(cudaMemcpyAsync(words, s->liveOut, (size_t)L->words * 4, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  words[1] = nDeep;   // header: whitewater points (written by the device), deep points, two zero words
   return ST_OK;
 }
 

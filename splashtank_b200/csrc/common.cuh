@@ -133,6 +133,14 @@ struct Bufs {
 
 constexpr int PBLK = 1024;     // particles per block in the order-defining passes (count, scatter, dead lists)
 
+// the parameter block into a CTA's shared copy (every thread of the CTA calls it; it ends with a barrier)
+__device__ __forceinline__ void loadParams(FlipParams& s, const FlipParams* g) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(FlipParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
 // ---- small vector math: every operation spelled out so the order matches the oracle ----
 struct V3 { float x, y, z; };
 __device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
@@ -221,6 +229,24 @@ __device__ __forceinline__ float phiOfBits(uint32_t ct) { return 8.0f - (float)(
 __device__ __forceinline__ uint32_t phiPutBits(uint32_t ct, float v) {
   uint32_t q = (uint32_t)clampf(rintf((8.0f - v) * 4096.0f), 0.0f, 65535.0f);
   return (ct & 0xffffu) | (q << 16);
+}
+
+// ---- velGAxis (src/flip/wgsl-core.js:185-197): the kept grid velocity (narrow band), trilinear on the MAC faces ----
+__device__ __forceinline__ float velGAxis(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x, int axis) {
+  V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
+  if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+  const V3 f0 = vfloor(g), fr = g - f0;
+  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
+  float s = 0.0f;
+  for (int c = 0; c < 8; c++) {
+    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+    s += w * velG[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
+  }
+  return s;
+}
+__device__ __forceinline__ V3 velGVec(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
+  return v3(velGAxis(P, velG, nc, x, 0), velGAxis(P, velG, nc, x, 1), velGAxis(P, velG, nc, x, 2));
 }
 
 // ---- colliders (src/gpu.js:6-38, src/flip/wgsl-core.js:113-126) ----

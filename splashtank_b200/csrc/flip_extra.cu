@@ -10,29 +10,6 @@
 
 namespace st {
 
-__device__ __forceinline__ void loadParamsX(FlipParams& s, const FlipParams* g) {
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
-  for (int i = threadIdx.x; i < (int)(sizeof(FlipParams) / 4); i += blockDim.x) dst[i] = src[i];
-  __syncthreads();
-}
-
-__device__ __forceinline__ float velGAxisX(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x, int axis) {
-  V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
-  if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
-  const V3 f0 = vfloor(g), fr = g - f0;
-  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
-  float s = 0.0f;
-  for (int c = 0; c < 8; c++) {
-    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
-    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
-    s += w * velG[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
-  }
-  return s;
-}
-__device__ __forceinline__ V3 velGVecX(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
-  return v3(velGAxisX(P, velG, nc, x, 0), velGAxisX(P, velG, nc, x, 1), velGAxisX(P, velG, nc, x, 2));
-}
 __device__ __forceinline__ float fillPhiX(const FlipParams& P, V3 x) {
   float d = 1.0e9f;
   for (uint32_t k = 0; k < P.nfill; k++) {
@@ -51,7 +28,7 @@ __device__ __forceinline__ float fillPhiX(const FlipParams& P, V3 x) {
 // ---- phiInitAll (wgsl-narrowband.js:20-35) ----
 __global__ void __launch_bounds__(512) k_nb_init(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
@@ -87,7 +64,7 @@ __device__ __forceinline__ float phiSampleX(const FlipParams& P, const uint32_t*
 }
 __global__ void __launch_bounds__(512) k_nb_phi(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
@@ -96,7 +73,7 @@ __global__ void __launch_bounds__(512) k_nb_phi(Bufs B) {
     if (!inDom(P, i, j, k)) { B.rhs[c] = 8.0f; continue; }
     if (((B.ctype[c] >> 8) & 0xffu) != 0u) { B.rhs[c] = 0.5f; continue; }
     const V3 x = cellCenter(P, i, j, k);
-    const float phA = phiSampleX(P, B.ctype, x - velGVecX(P, B.velG, nc, x) * P.dt);
+    const float phA = phiSampleX(P, B.ctype, x - velGVec(P, B.velG, nc, x) * P.dt);
     const bool inside = B.cnt[c] > 0 || phA < -1.0f;
     B.rhs[c] = inside ? clampf(phA, -7.9f, -0.5f) : clampf(phA, 0.5f, 7.9f);
   }
@@ -119,7 +96,7 @@ __device__ __forceinline__ float jacNb(const FlipParams& P, const Bufs& B, int i
 // pass A: depth (ctype bits) from rhs; pass B: rhs from depth
 __global__ void __launch_bounds__(512) k_nb_jac(Bufs B, int passA) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
@@ -137,7 +114,7 @@ __global__ void __launch_bounds__(512) k_nb_jac(Bufs B, int passA) {
 // ---- nbVel (wgsl-narrowband.js:70-85): water faces with no particle weight take the carried grid velocity ----
 __global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
@@ -151,7 +128,7 @@ __global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
       if ((B.ctype[cellIdx(P, li, lj, lk)] & 0xffu) != 1u) continue;
       if (B.acc[(3 + ax) * nc + c] > 0) continue;
       const V3 fp = facePos(P, i, j, k, ax);
-      const float vc = velGAxisX(P, B.velG, nc, fp - velGVecX(P, B.velG, nc, fp) * P.dt, ax);
+      const float vc = velGAxis(P, B.velG, nc, fp - velGVec(P, B.velG, nc, fp) * P.dt, ax);
       B.acc[ax * nc + c] = (int32_t)rintf(vc * P.scale);
       B.acc[(3 + ax) * nc + c] = (int32_t)P.scale;
     }
@@ -184,7 +161,7 @@ __global__ void __launch_bounds__(1024) k_scan_x(Bufs B, int which) {
 __global__ void __launch_bounds__(512) k_killed_list(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     if (B.tileDead[a + 1] == B.tileDead[a]) continue;   // uniform per block: no kills in this tile
@@ -210,7 +187,7 @@ __device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs&
   if (((ct >> 8) & 0xffu) != 0u) return 0;
   const float ph = phiOfBits(ct);
   if ((ct & 0xffu) != 1u || ph > -1.0f || ph < -P.band) return 0;
-  if (!(len3(velGVecX(P, B.velG, B.ncell, cellCenter(P, i, j, k))) < 9.0f * P.h)) return 0;
+  if (!(len3(velGVec(P, B.velG, B.ncell, cellCenter(P, i, j, k))) < 9.0f * P.h)) return 0;
   const uint32_t n = (uint32_t)max(B.cnt[c], 0);
   if ((float)n >= 0.55f * P.rest) return 0;
   return min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
@@ -218,7 +195,7 @@ __device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs&
 __global__ void __launch_bounds__(512) k_def_count(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
@@ -234,7 +211,7 @@ __global__ void __launch_bounds__(512) k_def_count(Bufs B) {
 __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const uint32_t nKilled = B.ctl->nKilled, nLive = B.ctl->nLive;
   const uint32_t avail = min(nKilled + (P.n - nLive), P.lcap);
@@ -253,7 +230,7 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
       const uint32_t pi = deadSlot(B, kk, nKilled, nLive);
       const uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
       const V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
-      const V3 v = velGVecX(P, B.velG, nc, x);
+      const V3 v = velGVec(P, B.velG, nc, x);
       Part q;
       q.p = make_float4(x.x, x.y, x.z, fmn(len3(v), 63.0f));
       q.v = make_float4(v.x, v.y, v.z, 0.0f);
@@ -349,7 +326,7 @@ __device__ __forceinline__ void airPushWarp(const FlipParams& P, int32_t* __rest
 // reseed stage, after the air has felt them); they are removed here once pushed.
 __global__ void __launch_bounds__(256) k_air_splat(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nL = B.ctl->nLive, m = min(B.ctl->sctl0, P.smax), tot = nL + m;
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < tot; i0 += stride) {
@@ -389,7 +366,7 @@ __global__ void __launch_bounds__(256) k_air_splat(Bufs B) {
 // object the cell is inside, settle back to the wind
 __global__ void __launch_bounds__(256) k_air_update(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nax = P.aNx, nay = P.aNy, na = nax * nay * P.aNz;
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < na; c += gridDim.x * blockDim.x) {
     const int ci = (int)(c % nax), cj = (int)((c / nax) % nay), ck = (int)(c / (nax * nay));
@@ -422,7 +399,7 @@ __global__ void __launch_bounds__(256) k_air_copy(Bufs B, uint32_t na) {   // ai
 // wwSample (wgsl-whitewater.js:91-98) fused with sprayStep (:134-179): each point reads only its own sample
 __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
   __shared__ FlipParams P;
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t m = min(B.ctl->sctl0, P.smax), nc = B.ncell;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
     float4 sp = B.sPos[j];
@@ -499,7 +476,7 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
 __global__ void __launch_bounds__(256) k_emit_write(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, s0ring = B.ctl->sctl0;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     if (B.tileEmit[a + 1] == B.tileEmit[a]) continue;   // uniform per block: nothing thrown off in this tile
@@ -562,7 +539,7 @@ __global__ void k_emit_done(Bufs B) {
 __global__ void __launch_bounds__(1024) k_drip(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
-  loadParamsX(P, B.P);
+  loadParams(P, B.P);
   const uint32_t nd = P.ndrip, s0ring = B.ctl->sctl0;
   uint32_t base = 0;
   for (uint32_t c0 = 0; c0 < nd; c0 += blockDim.x) {

@@ -8,13 +8,6 @@
 
 namespace st {
 
-__device__ __forceinline__ void loadParams(FlipParams& s, const FlipParams* g) {
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
-  for (int i = threadIdx.x; i < (int)(sizeof(FlipParams) / 4); i += blockDim.x) dst[i] = src[i];
-  __syncthreads();
-}
-
 // markAround (wgsl-core.js:239-246): every tile within two cells of cell (ci, cj, ck) gets this step's stamp.
 __device__ __forceinline__ void markAround(const FlipParams& P, uint32_t* __restrict__ need, int ci, int cj, int ck) {
   int lox = max(ci - 2, 0) >> 3, loy = max(cj - 2, 0) >> 3, loz = max(ck - 2, 0) >> 3;
@@ -340,7 +333,6 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
 }
 
 // ---- 6. collider bits (solidBuild, wgsl-solver.js:42-45) + classify (wgsl-solver.js:47-74) ----
-__device__ __forceinline__ V3 velGVecAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x);
 __global__ void __launch_bounds__(512) k_classify(Bufs B) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
@@ -358,7 +350,7 @@ __global__ void __launch_bounds__(512) k_classify(Bufs B) {
     if (!inDom(P, i, j, k)) ty = 0;
     else if ((sb & 0xff00u) != 0u) ty = 2;
     else if (P.nb != 0u && phiOfBits(ct) < -1.0f &&
-             (phiOfBits(ct) < -P.band || len3(velGVecAt(P, B.velG, nc, cx)) < 9.0f * P.h)) ty = 1;
+             (phiOfBits(ct) < -P.band || len3(velGVec(P, B.velG, nc, cx)) < 9.0f * P.h)) ty = 1;
     else if (n > 0) {
       ty = 1;
       if ((float)n < P.sheetMin) {
@@ -955,24 +947,6 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
     }
     __syncthreads();
   }
-}
-
-// ---- velG sampling (velGAxis, wgsl-core.js:185-197), used by classify and the narrow band ----
-__device__ __forceinline__ float velGAxisAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x, int axis) {
-  V3 g = (x - v3(P.x0, P.y0, P.z0)) * P.ih;
-  if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
-  const V3 f0 = vfloor(g), fr = g - f0;
-  const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
-  float s = 0.0f;
-  for (int c = 0; c < 8; c++) {
-    const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
-    const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
-    s += w * velG[axis * nc + faceCell(P, axis, i0 + dx, j0 + dy, k0 + dz)];
-  }
-  return s;
-}
-__device__ __forceinline__ V3 velGVecAt(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
-  return v3(velGAxisAt(P, velG, nc, x, 0), velGAxisAt(P, velG, nc, x, 1), velGAxisAt(P, velG, nc, x, 2));
 }
 
 // unsort for readback (wgsl-blocks.js:97-99): id order into dst (pos and vel)

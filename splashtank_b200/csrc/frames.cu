@@ -7,22 +7,10 @@
 // (Math.round is round-half-up, a Uint8Array store truncates), so the bytes are identical, and only 8 bytes per point
 // cross PCIe instead of 16.
 #include "common.cuh"
+#include "jsnum.cuh"
 #include "kernels.h"
 
 namespace st {
-
-__device__ __forceinline__ uint16_t q16(double v, double lo, double k) {   // Math.max(0, Math.min(65535, Math.round(...)))
-  const double x = (v - lo) * k;
-  double r = floor(x);
-  if (x - r >= 0.5) r += 1.0;   // Math.round: the nearest integer, halves up (exact: x - floor(x) has no rounding)
-  return (uint16_t)(r < 0.0 ? 0.0 : (r > 65535.0 ? 65535.0 : r));
-}
-__device__ __forceinline__ uint8_t toU8(double s) {   // a Uint8Array store: ToUint8 (truncate, then modulo 256)
-  if (!(s == s) || isinf(s)) return 0;
-  const double t = trunc(s);
-  const long long m = (long long)fmod(t, 256.0);
-  return (uint8_t)(m < 0 ? m + 256 : m);
-}
 
 // meta[0]: last water point + 1 (atomicMax of index + 1), meta[1]: any white water
 __global__ void k_pack_frame(const float4* __restrict__ pos4, uint32_t n, FrameBox F, uint16_t* __restrict__ pos16,

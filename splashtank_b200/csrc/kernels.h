@@ -44,4 +44,16 @@ struct DiagAcc {
 int launch_pack_frame(const float4* pos4, uint32_t n, const FrameBox& F, uint16_t* pos16, uint8_t* spd, uint8_t* fm, uint32_t* meta,
                       cudaStream_t s);
 int launch_bake_diag(const Part* pa, uint32_t n, const DiagBox& D, DiagAcc* acc, cudaStream_t s);
+// the live view and a frame's whitewater and deep-water parts (live.cu)
+struct LiveBox {
+  float x0, y0, z0, kx, ky, kz, vs;            // the box and the speed scale, f32 as the shader has them
+  uint32_t smax, nS;                           // whitewater slots; whitewater points the view holds
+  uint32_t oWp, oWs, oWf, oSp, oSk, oDp, oDs;  // word offsets of the parts (packLayout)
+};
+int launch_spray_frame(const float4* sPos, const float4* sVel, uint32_t nslots, uint32_t maxPoints, const FrameBox& F, double foamLife,
+                       uint32_t* scratch, uint16_t* pos16, uint32_t* pk, uint32_t* counts, cudaStream_t s);
+int launch_deep(const Bufs& B, uint32_t prev, uint32_t nActiveMax, int grid, uint32_t* tcount, uint32_t* counts, float4* out, cudaStream_t s);
+int launch_pack_deep(const float4* dp, uint32_t n, const FrameBox& F, uint16_t* pos16, uint8_t* spd, cudaStream_t s);
+int launch_live(const Bufs& B, const LiveBox& K, uint32_t nW, uint32_t stride, uint32_t sdMax, float foamLife, const float4* deep, uint32_t nDeep,
+                uint32_t* scratch, uint32_t* out, cudaStream_t s);
 }  // namespace st

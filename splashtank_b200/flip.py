@@ -359,6 +359,46 @@ class FlipSim:
         self._check(self.f["flip_read_spray"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.sprayCap, C.byref(n)), "readSpray")
         return dict(n=n.value, p=p[: n.value], v=v[: n.value])
 
+    def setDeepLook(self, on):
+        """FlipSim.setDeepLook (src/flip/sim.js:406): show the narrow band's deep water as points."""
+        self._check(self.f["flip_set_deep_look"](self._h, 1 if on else 0), "setDeepLook")
+
+    def read_deep(self, vs=1.0):
+        """readDeep + packDeep (src/flip/sim.js:408-421, src/gpu.js:512-524) on the device: the frame's deep-water part,
+        dict n, pos (n, 3) uint16 and spd (n,) uint8, or None when the deep look does not apply."""
+        self.flushRun()
+        cap = 200000
+        pos, spd = np.zeros((cap, 3), np.uint16), np.zeros(cap, np.uint8)
+        n = C.c_uint32()
+        self._check(self.f["flip_read_deep"](self._h, float(vs), pos.ctypes.data_as(C.POINTER(C.c_uint16)), spd.ctypes.data_as(abi.u8p), cap,
+                                             C.byref(n)), "readDeep")
+        m = n.value
+        return dict(n=m, pos=pos[:m], spd=spd[:m]) if m else None
+
+    def read_spray_frame(self, cap=200000, foam_life=3.0):
+        """packSprayFrame (src/flip/bake.js:43-58) on the device: the frame's whitewater part, dict n, pos (n, 3) uint16,
+        pk (n,) uint32 and alive, or None without a whitewater pool."""
+        if not self.sprayCap:
+            return None
+        self.flushRun()
+        room = self.sprayCap
+        pos, pk = np.zeros((room, 3), np.uint16), np.zeros(room, np.uint32)
+        n, alive = C.c_uint32(), C.c_uint32()
+        self._check(self.f["flip_read_spray_frame"](self._h, int(cap), float(foam_life), pos.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                                    pk.ctypes.data_as(abi.u32p), room, C.byref(n), C.byref(alive)), "readSprayFrame")
+        m = n.value
+        return dict(n=m, pos=pos[:m], pk=pk[:m], alive=alive.value)
+
+    def pack_live(self, vs=1.0):
+        """FlipSim.dispPack (src/flip/sim.js:381-404) on the device: (words, layout) of the packed live view."""
+        self.flushRun()
+        L = abi.LiveLayout()
+        L.size = C.sizeof(abi.LiveLayout)
+        self._check(self.f["flip_pack_live"](self._h, float(vs), None, 0, C.byref(L)), "packLive")
+        words = np.zeros(max(L.words, 1), np.uint32)
+        self._check(self.f["flip_pack_live"](self._h, float(vs), words.ctypes.data_as(abi.u32p), len(words), C.byref(L)), "packLive")
+        return words[:L.words], {k: getattr(L, k) for k, _ in abi.LiveLayout._fields_ if k != "size"}
+
     def read_air(self):
         """The air field: (nz, ny, nx, 3) float32 air velocity at the air-cell centres, or None without a whitewater pool."""
         dims = (C.c_uint32 * 3)()

@@ -50,8 +50,8 @@ def test_struct_sizes_match_the_header():
 int main(void) {
   printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(st_flip_desc), sizeof(st_step_opts), sizeof(st_collider), sizeof(st_sdf),
          sizeof(st_stats), sizeof(st_flip_grid), sizeof(st_stage_times), sizeof(st_pbf_desc), sizeof(st_pbf_opts));
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(st_poisson_desc), sizeof(st_poisson_opts), sizeof(st_poisson_result), sizeof(st_poisson_system),
-         sizeof(st_batch_desc), sizeof(st_diff_desc));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(st_poisson_desc), sizeof(st_poisson_opts), sizeof(st_poisson_result), sizeof(st_poisson_system),
+         sizeof(st_batch_desc), sizeof(st_diff_desc), sizeof(st_live_layout));
   return 0;
 }
 '''
@@ -62,7 +62,8 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(x) for x in (abi.FlipDesc, abi.StepOpts, abi.Collider, abi.Sdf, abi.Stats, abi.Grid, abi.StageTimes, abi.PbfDesc, abi.PbfOpts,
-                                  abi.PoissonDesc, abi.PoissonOpts, abi.PoissonResult, abi.PoissonSystem, abi.BatchDesc, abi.DiffDesc)]
+                                  abi.PoissonDesc, abi.PoissonOpts, abi.PoissonResult, abi.PoissonSystem, abi.BatchDesc, abi.DiffDesc,
+                                  abi.LiveLayout)]
     assert got == want
 
 

@@ -87,3 +87,122 @@ def test_bake_loop_writes_a_cache():
     buf = bake.write_cache([f for f, _ in frames], dict(d=tank.d, fps=60, ids=[1, 2], engine="flip"))
     meta, back = bake.parse_cache(buf)
     assert len(back) == 5 and back[-1]["n"] == frames[-1][0]["n"] and np.array_equal(back[-1]["pos"], frames[-1][0]["pos"])
+
+
+def test_spray_codes_follow_the_javascript_arithmetic():
+    """packSprayJS (src/flip/bake.js:4-15), worked by hand: speed in quarter units from bit 21, kind bits, octahedral
+    direction (Math.round: 511.5 rounds up to 512) or the foam's life left."""
+    from oracle.frames import pack_spray_js
+    v = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, -2.0], [0.0, 3.0, 0.0]])
+    got = pack_spray_js(v, np.array([0.0, 0.0, 1.0, 2.0]), np.array([0.5, 0.5, 0.5, 0.25]))
+    want = [0x80000000 | (1023 << 10) | 512,                       # at rest: straight up
+            0x80000000 | (4 << 21) | (512 << 10) | 1023,            # +x at speed 1
+            0x80000000 | (8 << 21) | 0x40000000 | (1023 << 10) | 1023,   # mist falling -z: folded octahedron
+            0x80000000 | (12 << 21) | 0x20000000 | 256]             # foam with a quarter of its life left (255.75 -> 256)
+    assert [int(x) for x in got] == want
+
+
+def test_deep_points_pack_like_pack_deep():
+    from oracle.frames import pack_deep
+    box = (-0.5, 0.0, -0.5, 0.5, 1.0, 0.5)
+    d = pack_deep(np.array([[0.0, 0.5, 0.0, 4096.0 + 2.5], [0.0, -1e6, 0.0, 0.0], [0.5, 1.0, -0.5, 4096.0 + 63.0]], np.float32), box, 1.0)
+    assert d["n"] == 2                                         # the gone point is left out
+    assert tuple(d["pos"][0]) == (32768, 32768, 32768) and d["spd"][0] == 40
+    assert tuple(d["pos"][1]) == (65535, 65535, 0) and d["spd"][1] == 191
+
+
+def _spray_scene():
+    from flip_compare import make_pair
+    sc = scenes.dam_break(32)
+    sc["vel"] = np.tile(np.array([[2.5, 0.5, 0.0]], np.float32), (len(sc["pos"]), 1))
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY, min=0.5), gust=1.0, nb=dict(on=True, band=3.0))
+    g, o = make_pair(sc, spray_cap=30000)
+    for s in (g, o):
+        p, v, i = s.save_state()
+        s.load_state(p, v, i, t=0.6, seed=0)
+    for _ in range(30):
+        for s in (g, o):
+            s.step(sc["dt"], opts)
+    return g, o
+
+
+@pytest.mark.gpu
+def test_device_spray_frame_matches_pack_spray_frame():
+    """The frame's whitewater part packed on the device equals packSprayFrame of the pool read back, with every
+    living slot (cap above the living count) and with a sampling step (cap 500)."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from oracle.frames import pack_spray_frame
+    g, _ = _spray_scene()
+    b = g.b
+    box = (b["x0"], b["y0"], b["z0"], b["x1"], b["y1"], b["z1"])
+    sd = g.readSpray()
+    for cap in (200000, 500):
+        got = g.read_spray_frame(cap, 3.0)
+        want = pack_spray_frame(sd["p"], sd["v"], sd["n"], box, cap, 3.0)
+        assert got["alive"] == want["alive"] > 500 and got["n"] == want["n"] > 0
+        assert np.array_equal(got["pos"], want["pos"]) and np.array_equal(got["pk"], want["pk"])
+    kinds = (g.read_spray_frame()["pk"] >> 29) & 3
+    assert len(set(kinds.tolist())) == 4                      # spray, foam, mist and bubble codes all present
+
+
+@pytest.mark.gpu
+def test_device_deep_points_and_live_view_match_the_oracle():
+    """Narrow band of 3 cells on a 96^3 tank (2.05M particle slots: the live view samples every 7th), deep look on:
+    the deep water points and the packed live view equal the oracle's. About 240k deep cells: the first pass keeps the
+    first 200,000, later passes a hashed sample sized by the previous count."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from oracle.frames import pack_deep, pack_live
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    w = scenes.WaveTank(96, spray_cap=50000, band=3.0)
+    g, o = w.make(FlipSim), w.make(OracleFlipSim, threads=8)
+    for s in (g, o):
+        s.setDeepLook(True)
+    runs, t = [SceneRunner(s) for s in (g, o)], 0.0
+    for _ in range(6):
+        t += w.dt
+        st = w.states(t)
+        for r in runs:
+            r.step(w.dt, st, w.opts)
+    b = g.b
+    box = (b["x0"], b["y0"], b["z0"], b["x1"], b["y1"], b["z1"])
+    counts = []
+    for vs in (1.0, 1.5):
+        got, pts = g.read_deep(vs), o.deep_points()
+        want = pack_deep(pts, box, vs)
+        assert got["n"] == want["n"]
+        assert np.array_equal(got["pos"], want["pos"]) and np.array_equal(got["spd"], want["spd"])
+        counts.append(got["n"])
+    assert counts[0] == 200000 and 190000 < counts[1] < 200000
+    words, L = g.pack_live(1.2)
+    assert L["from_pos"] == 0 and L["n_deep"] == 200000
+    pos, _, _ = o.save_state()
+    sd = o.readSpray()
+    used = min(o.readStats()["spray_used"], o.sprayCap)
+    stride = max(1, -(-o.N // 300000))
+    assert stride == 7 and L["n_water"] == -(-o.N // stride)
+    want = pack_live(L, pos, stride, sd["p"], sd["v"], used, min(o.sprayCap, 200000), 3.0, o.deep_points(), box, 1.2)
+    assert words[1] == want[1] > 190000
+    assert np.array_equal(words, want)
+
+
+@pytest.mark.gpu
+def test_device_live_view_with_whitewater_matches_the_oracle():
+    """The live view of a tank full of whitewater (every kind): water, whitewater codes in the shader's f32 packSpray."""
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from oracle.frames import pack_live
+    g, o = _spray_scene()
+    b = g.b
+    box = (b["x0"], b["y0"], b["z0"], b["x1"], b["y1"], b["z1"])
+    words, L = g.pack_live(1.0)
+    assert L["from_pos"] == 0 and L["n_spray"] == 30000 and L["n_deep"] == 0
+    pos, _, _ = o.save_state()
+    sd = o.readSpray()
+    used = min(o.readStats()["spray_used"], o.sprayCap)
+    want = pack_live(L, pos, 1, sd["p"], sd["v"], used, 30000, 3.0, None, box, 1.0)
+    assert words[0] == want[0] > 1000
+    assert np.array_equal(words, want)
