@@ -2,7 +2,9 @@
 (writeCacheParts / parseCache2, src/shared.js:688-736).
 
 Frames come from st_flip_read_frame (packed on the device in id order) and the per-frame measurements from
-st_flip_bake_diag, so a frame costs 8 bytes per point of readback instead of a 16-byte float copy per point.
+st_flip_bake_diag, so a frame costs 8 bytes per point of readback instead of a 16-byte float copy per point. The
+whitewater part (packSprayFrame, st_flip_read_spray_frame) and, with the deep look on, the deep-water part (readDeep +
+packDeep, st_flip_read_deep) are packed on the device too.
 """
 import json
 import math
@@ -40,10 +42,14 @@ def pack_objs(states):
     return out
 
 
-def run_bake(sim, runner, states, par, fps, frames, substeps=1, cfl=1.5, max_sub=16, vmax0=2.0, scale=1.0, on_frame=None):
+def run_bake(sim, runner, states, par, fps, frames, substeps=1, cfl=1.5, max_sub=16, vmax0=2.0, scale=1.0, on_frame=None, nb_look=False):
     """runBakeFlipGpu's frame loop (src/flip/bake.js:101-131) for a filled simulator: substeps per frame adapt to the
     fastest particle of the last frame and the objects' own motion; every frame is read as a packed frame with its
-    measurements. states(t) gives the objects; par the step options. Returns the list of frames."""
+    measurements, plus its whitewater points (when the simulator has a pool) and deep-water points (nb_look).
+    states(t) gives the objects; par the step options. Returns the list of frames."""
+    if nb_look:
+        sim.setDeepLook(True)
+    foam_life = ((par.get("spr") or {}).get("ww") or {}).get("foamLife") or 3.0
     dtF = 1.0 / fps
     max_sub = max(substeps, max_sub)
     out = []
@@ -53,6 +59,14 @@ def run_bake(sim, runner, states, par, fps, frames, substeps=1, cfl=1.5, max_sub
         fr["objs"] = pack_objs(states(f * dtF))
         diag = sim.bake_diag(par.get("vmax", 14.0))
         diag.update(sub=sub, objectSpeed=objv)
+        if f > 0 and sim.sprayCap:
+            fr["sp"] = sim.read_spray_frame(200000, foam_life)
+            diag["sprayPoints"] = fr["sp"]["alive"]
+        if f > 0 and nb_look:
+            dp = sim.read_deep(scale)
+            if dp:
+                fr["dp"] = dp
+                diag["deepPoints"] = dp["n"]
         if on_frame:
             on_frame(fr, dict(f=f, F=frames, n=fr["n"], sub=sub, diag=diag))
         out.append((fr, diag))
@@ -77,13 +91,17 @@ def run_bake(sim, runner, states, par, fps, frames, substeps=1, cfl=1.5, max_sub
 
 def write_cache(frames, meta):
     """writeCacheParts (src/shared.js:688-705), version 2: 'SPLC', 2, the JSON block, padding, frame count, then per
-    frame: points, flags (1 = white-water bytes follow), object poses, positions, speeds, [white water], padding."""
+    frame: points, flags (1 = white-water bytes follow, 2 = whitewater points follow, 4 = deep-water points follow),
+    object poses, positions, speeds, [white water], padding, [whitewater: count, positions, padding, codes], [deep
+    water: count, positions, speeds, padding]."""
     mj = json.dumps(meta, separators=(",", ":")).encode()
     pad = lambda k: b"\0" * ((4 - k % 4) % 4)   # noqa: E731
     parts = [b"SPLC", struct.pack("<II", 2, len(mj)), mj, pad(len(mj)), struct.pack("<I", len(frames))]
     for fr in frames:
         n, fm = fr["n"], fr.get("fm")
-        parts.append(struct.pack("<II", n, 1 if fm is not None else 0))
+        sp = fr.get("sp") if fr.get("sp") and fr["sp"]["n"] else None
+        dp = fr.get("dp") if fr.get("dp") and fr["dp"]["n"] else None
+        parts.append(struct.pack("<II", n, (1 if fm is not None else 0) | (2 if sp else 0) | (4 if dp else 0)))
         parts.append(np.asarray(fr["objs"], np.float32).tobytes())
         parts.append(np.asarray(fr["pos"], np.uint16).tobytes())
         parts.append(np.asarray(fr["spd"], np.uint8).tobytes())
@@ -92,11 +110,17 @@ def write_cache(frames, meta):
             parts.append(np.asarray(fm, np.uint8).tobytes())
             nb += n
         parts.append(pad(nb))
+        if sp:
+            parts += [struct.pack("<I", sp["n"]), np.asarray(sp["pos"], np.uint16).tobytes(), pad(sp["n"] * 6),
+                      np.asarray(sp["pk"], np.uint32).tobytes()]
+        if dp:
+            parts += [struct.pack("<I", dp["n"]), np.asarray(dp["pos"], np.uint16).tobytes(), np.asarray(dp["spd"], np.uint8).tobytes(),
+                      pad(dp["n"] * 7)]
     return b"".join(parts)
 
 
 def parse_cache(buf):
-    """parseCache2 (src/shared.js:706-736) for water frames: (meta, frames)."""
+    """parseCache2 (src/shared.js:706-736): (meta, frames), frames with their whitewater (sp) and deep-water (dp) parts."""
     assert buf[:4] == b"SPLC" and struct.unpack_from("<I", buf, 4)[0] == 2
     ml = struct.unpack_from("<I", buf, 8)[0]
     o = 12
@@ -120,5 +144,22 @@ def parse_cache(buf):
             fm = np.frombuffer(buf, np.uint8, n, o)
             o += n
         o += (4 - (n * (8 if fl & 1 else 7)) % 4) % 4
-        frames.append(dict(n=n, pos=pos, spd=spd, fm=fm, objs=objs))
+        fr = dict(n=n, pos=pos, spd=spd, fm=fm, objs=objs)
+        if fl & 2:
+            ns = struct.unpack_from("<I", buf, o)[0]
+            o += 4
+            p2 = np.frombuffer(buf, np.uint16, ns * 3, o).reshape(ns, 3)
+            o += ns * 6 + (4 - ns * 6 % 4) % 4
+            pk = np.frombuffer(buf, np.uint32, ns, o)
+            o += ns * 4
+            fr["sp"] = dict(n=ns, pos=p2, pk=pk, alive=ns)
+        if fl & 4:
+            nd = struct.unpack_from("<I", buf, o)[0]
+            o += 4
+            p3 = np.frombuffer(buf, np.uint16, nd * 3, o).reshape(nd, 3)
+            o += nd * 6
+            s3 = np.frombuffer(buf, np.uint8, nd, o)
+            o += nd + (4 - nd * 7 % 4) % 4
+            fr["dp"] = dict(n=nd, pos=p3, spd=s3)
+        frames.append(fr)
     return meta, frames

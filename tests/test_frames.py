@@ -25,6 +25,28 @@ def test_cache_round_trip():
         assert np.array_equal(a["objs"], b["objs"])
 
 
+def test_cache_round_trip_with_whitewater_and_deep_water():
+    rng = np.random.default_rng(5)
+    frames = []
+    for k in range(3):
+        n, ns, nd = int(rng.integers(1, 40)), int(rng.integers(0, 9)), int(rng.integers(0, 7))
+        fr = dict(n=n, pos=rng.integers(0, 65536, (n, 3)).astype(np.uint16), spd=rng.integers(0, 256, n).astype(np.uint8), fm=None,
+                  objs=np.zeros(0, np.float32),
+                  sp=dict(n=ns, pos=rng.integers(0, 65536, (ns, 3)).astype(np.uint16), pk=rng.integers(0, 2 ** 32, ns, dtype=np.uint64).astype(np.uint32)),
+                  dp=dict(n=nd, pos=rng.integers(0, 65536, (nd, 3)).astype(np.uint16), spd=rng.integers(0, 192, nd).astype(np.uint8)))
+        frames.append(fr)
+    buf = bake.write_cache(frames, dict(ids=[]))
+    assert len(buf) % 4 == 0
+    _, f2 = bake.parse_cache(buf)
+    for a, b in zip(frames, f2):
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["spd"], b["spd"])
+        for part, keys in (("sp", ("pos", "pk")), ("dp", ("pos", "spd"))):
+            if a[part]["n"]:
+                assert b[part]["n"] == a[part]["n"] and all(np.array_equal(a[part][k], b[part][k]) for k in keys)
+            else:
+                assert part not in b
+
+
 def test_frame_checker_follows_the_javascript_arithmetic():
     from oracle.frames import pack_frame_buf
     box = (-0.5, 0.0, -0.5, 0.5, 1.0, 0.5)
@@ -87,6 +109,22 @@ def test_bake_loop_writes_a_cache():
     buf = bake.write_cache([f for f, _ in frames], dict(d=tank.d, fps=60, ids=[1, 2], engine="flip"))
     meta, back = bake.parse_cache(buf)
     assert len(back) == 5 and back[-1]["n"] == frames[-1][0]["n"] and np.array_equal(back[-1]["pos"], frames[-1][0]["pos"])
+
+
+@pytest.mark.gpu
+def test_bake_loop_stores_whitewater_and_deep_water():
+    """With a whitewater pool and the deep look (narrow band of 3 cells), every frame after the first carries the
+    whitewater and deep-water parts, and the cache keeps them."""
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    tank = scenes.WaveTank(32, steps=60, spray_cap=20000, band=3.0)
+    sim = tank.make(FlipSim)
+    frames = bake.run_bake(sim, SceneRunner(sim), tank.states, dict(tank.opts), fps=60, frames=3, substeps=2, nb_look=True)
+    last, diag = frames[-1]
+    assert last["dp"]["n"] > 100 and diag["deepPoints"] == last["dp"]["n"] and "sprayPoints" in diag
+    buf = bake.write_cache([f for f, _ in frames], dict(d=tank.d, fps=60, ids=[1, 2], engine="flip"))
+    _, back = bake.parse_cache(buf)
+    assert back[-1]["dp"]["n"] == last["dp"]["n"] and np.array_equal(back[-1]["dp"]["pos"], last["dp"]["pos"])
 
 
 def test_spray_codes_follow_the_javascript_arithmetic():
