@@ -217,6 +217,30 @@ st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims
  * position on the collider in its own frame, the collider number, the normal in its own frame and the wetness (1 in
  * water, falling to 0 over o.drip.dry seconds out of it). *n receives the count; at most cap are written. */
 st_status st_flip_read_drips(st_flip* s, float* out8, uint32_t cap, uint32_t* n);
+/* ---- mesh colliders: buildSDF (src/shared.js:98-181) on the device ---- */
+/* A closed mesh as the reference's {v, f}: vertex positions and polygon faces, fan-triangulated as meshTris
+ * (src/shared.js:45-49). */
+typedef struct st_mesh {
+  const double* v;      /* nv x 3 vertex positions */
+  uint32_t nv;
+  const uint32_t* idx;  /* the faces' vertex indices, face after face */
+  const uint32_t* len;  /* vertices of each face (3 or more) */
+  uint32_t nf;
+} st_mesh;
+/* in: cell (voxel size; 0 means 0.025) and margin (how far outside the mesh the grid reaches; the reference's default
+ * is 0.16); out: the voxel size used (grown by 1.25 until the grid has at most 2.6M voxels), dims and origin. With data
+ * null only the grid is computed; otherwise data (cap floats, x fastest) receives the signed distances: exact within
+ * 2.5 voxels of the surface, chamfer distances farther out, negative inside. Results equal the reference's double
+ * arithmetic into a Float32Array (Math.hypot taken as the square root of the sum of squares). */
+typedef struct st_sdf_build {
+  uint32_t size;        /* sizeof(st_sdf_build) */
+  uint32_t dims[3];
+  double cell, margin;
+  double origin[3];
+  float* data;
+  uint64_t cap;
+} st_sdf_build;
+st_status st_build_sdf(int device, const st_mesh* mesh, st_sdf_build* b);
 /* FlipSim.stats via readStats (src/flip/sim.js:160-168). Synchronises. */
 st_status st_flip_stats(st_flip* s, st_stats* out);
 /* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */

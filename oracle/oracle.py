@@ -18,7 +18,7 @@ _FUNCS = None
 
 def build():
     subprocess.run(["make", "-s", "-C", HERE, os.path.join(HERE, "liboracle_flip.so"), os.path.join(HERE, "liboracle_pbf.so"),
-                    os.path.join(HERE, "liboracle_poisson.so")], check=True)
+                    os.path.join(HERE, "liboracle_poisson.so"), os.path.join(HERE, "liboracle_sdf.so")], check=True)
 
 
 def funcs():
@@ -146,3 +146,21 @@ class OraclePoisson:
             self.lib.oracle_poisson_destroy(self.h)
         except Exception:
             pass
+
+
+_SDF = None
+
+
+def build_sdf(v, faces, cell=0.025, margin=0.16):
+    """The oracle's buildSDF (oracle/sdf_oracle.cpp), through the same wrapper as the device builder."""
+    global _SDF
+    if _SDF is None:
+        path = os.path.join(HERE, "liboracle_sdf.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        _SDF = lib.oracle_build_sdf
+        _SDF.argtypes = [C.POINTER(abi.Mesh), C.POINTER(abi.SdfBuild)]
+        _SDF.restype = C.c_int
+    from splashtank_b200.sdf import build_sdf as wrap
+    return wrap(v, faces, cell, margin, fn=_SDF)

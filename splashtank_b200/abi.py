@@ -127,6 +127,18 @@ class BakeDiag(C.Structure):
                 ("height_hist", C.c_uint32 * 16)]
 
 
+class Mesh(C.Structure):
+    _fields_ = [("v", C.POINTER(C.c_double)), ("nv", C.c_uint32), ("idx", u32p), ("len", u32p), ("nf", C.c_uint32)]
+
+
+class SdfBuild(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("dims", C.c_uint32 * 3), ("cell", C.c_double), ("margin", C.c_double), ("origin", C.c_double * 3),
+                ("data", f32p), ("cap", C.c_uint64)]
+
+
+SDF_FUNCS = [("build_sdf", C.c_int, [C.c_int, C.POINTER(Mesh), C.POINTER(SdfBuild)])]
+
+
 class LiveLayout(C.Structure):
     _fields_ = [("size", C.c_uint32), ("n_water", C.c_uint32), ("n_spray", C.c_uint32), ("n_deep", C.c_uint32), ("from_pos", C.c_uint32),
                 ("o_wp", C.c_uint32), ("o_ws", C.c_uint32), ("o_wf", C.c_uint32), ("o_sp", C.c_uint32), ("o_sk", C.c_uint32),

@@ -33,7 +33,8 @@ def test_cuda_library_exports_every_declared_symbol():
 def test_bindings_match_the_library():
     from splashtank_b200 import abi, build
     lib = C.CDLL(build.build())
-    lists = abi.FLIP_FUNCS + abi.CUDA_ONLY_FUNCS + abi.PBF_FUNCS + abi.POISSON_FUNCS + abi.NOALLOC_FUNCS + abi.BATCH_FUNCS + abi.DIFF_FUNCS
+    lists = (abi.FLIP_FUNCS + abi.CUDA_ONLY_FUNCS + abi.PBF_FUNCS + abi.POISSON_FUNCS + abi.NOALLOC_FUNCS + abi.BATCH_FUNCS + abi.DIFF_FUNCS +
+             abi.SDF_FUNCS)
     f = abi.bind(lib, "st_", lists)
     assert len(f) == len(lists)
 
@@ -50,8 +51,8 @@ def test_struct_sizes_match_the_header():
 int main(void) {
   printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(st_flip_desc), sizeof(st_step_opts), sizeof(st_collider), sizeof(st_sdf),
          sizeof(st_stats), sizeof(st_flip_grid), sizeof(st_stage_times), sizeof(st_pbf_desc), sizeof(st_pbf_opts));
-  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(st_poisson_desc), sizeof(st_poisson_opts), sizeof(st_poisson_result), sizeof(st_poisson_system),
-         sizeof(st_batch_desc), sizeof(st_diff_desc), sizeof(st_live_layout));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(st_poisson_desc), sizeof(st_poisson_opts), sizeof(st_poisson_result), sizeof(st_poisson_system),
+         sizeof(st_batch_desc), sizeof(st_diff_desc), sizeof(st_live_layout), sizeof(st_mesh), sizeof(st_sdf_build));
   return 0;
 }
 '''
@@ -63,7 +64,7 @@ int main(void) {
         got = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(x) for x in (abi.FlipDesc, abi.StepOpts, abi.Collider, abi.Sdf, abi.Stats, abi.Grid, abi.StageTimes, abi.PbfDesc, abi.PbfOpts,
                                   abi.PoissonDesc, abi.PoissonOpts, abi.PoissonResult, abi.PoissonSystem, abi.BatchDesc, abi.DiffDesc,
-                                  abi.LiveLayout)]
+                                  abi.LiveLayout, abi.Mesh, abi.SdfBuild)]
     assert got == want
 
 
