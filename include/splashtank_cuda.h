@@ -106,6 +106,18 @@ typedef struct st_step_opts {
   int32_t drip_on;      /* o.drip.on: wet colliders drip after they leave the water (needs spray_on) */
   float drip_rate;      /* o.drip.rate: drops a second from a fully wet surface sample */
   float drip_dry;       /* o.drip.dry: seconds a surface stays wet out of the water */
+  /* o.ocean (src/flip/sim.js:185-217, oceanWaves src/shared.js:760-780): 24 linear waves around the peak wavelength
+   * with a Pierson-Moskowitz shaped spectrum; a boundary layer of width `layer` at the side walls holds the water to
+   * them. Turns the narrow band on. */
+  int32_t ocean_on;
+  float ocean_level;    /* mean surface height */
+  float ocean_layer;    /* boundary width */
+  float ocean_length;   /* peak wavelength */
+  float ocean_height;   /* significant wave height */
+  float ocean_dir;      /* direction, degrees */
+  float ocean_spread;   /* directional spread, degrees */
+  int32_t ocean_seed;
+  float time;           /* o.time: scene time, the waves' phase */
 } st_step_opts;
 
 /* Counters read back after a step: FlipSim.stats (src/flip/sim.js:160-168). */
@@ -217,6 +229,10 @@ st_status st_flip_read_air(st_flip* s, float* vel4, uint32_t cap, uint32_t* dims
  * position on the collider in its own frame, the collider number, the normal in its own frame and the wetness (1 in
  * water, falling to 0 over o.drip.dry seconds out of it). *n receives the count; at most cap are written. */
 st_status st_flip_read_drips(st_flip* s, float* out8, uint32_t cap, uint32_t* n);
+/* oceanWaves (src/shared.js:760-780), host only: the ocean's 24 waves for o's ocean settings, gravity o->g and water
+ * depth `depth` (the mean level above the floor), 8 floats each (kx, kz, amplitude, angular frequency, phase,
+ * wavenumber, 0, 0) into w (room for 192 floats). Returns the number of waves. The viewer draws the same sums. */
+int st_ocean_waves(const st_step_opts* o, double depth, float* w);
 /* ---- mesh colliders: buildSDF (src/shared.js:98-181) on the device ---- */
 /* A closed mesh as the reference's {v, f}: vertex positions and polygon faces, fan-triangulated as meshTris
  * (src/shared.js:45-49). */

@@ -94,6 +94,8 @@ struct Params {
   float wwFoamLife, wwRise, wwCrest, wwImpact;
   uint32_t airOn, aNx, aNy, aNz; float airCouple, airDecay, airH, airBlur;   // words 72-76, 82
   uint32_t ndrip; float dripRate, dripDry;                                    // words 79-81
+  uint32_t ocean, nwave; float otime, olevel, olayer, oy0, odepth;            // words 57-61, 63, 66
+  float waves[24 * 8];                                                        // oceanWaves: 8 floats per wave
   float fills[16][4];
 };
 
@@ -287,6 +289,37 @@ struct Oracle {
   }
   V3 velGVec(V3 x) const { return v3(velGAxis(x, 0), velGAxis(x, 1), velGAxis(x, 2)); }
   bool calmV(V3 v) const { return length(v) < 9.0f * P.h; }
+  // ---- ocean (wgsl-core.js:201-226) ----
+  float oceanEta(float x, float z) const {
+    float e = 0.0f;
+    for (uint32_t k = 0; k < P.nwave; k++) {
+      const float* A = &P.waves[k * 8]; const float* Bw = A + 4;
+      float sn, cs; st_sincosf(A[0] * x + A[1] * z - A[3] * P.otime + Bw[0], &sn, &cs);
+      e += A[2] * cs;
+    }
+    return P.olevel + e;
+  }
+  V3 oceanVel(V3 p) const {
+    float D = fmax_(P.odepth, 1.0e-3f), eta = oceanEta(p.x, p.z);
+    float ys = clampf((p.y - P.oy0) * D / fmax_(D + eta - P.olevel, 0.1f * D), 0.0f, D);
+    V3 v = v3(0, 0, 0);
+    for (uint32_t k = 0; k < P.nwave; k++) {
+      const float* A = &P.waves[k * 8]; const float* Bw = A + 4;
+      float kk = fmax_(Bw[1], 1.0e-4f);
+      float th = A[0] * p.x + A[1] * p.z - A[3] * P.otime + Bw[0];
+      float e1 = st_expf(kk * (ys - D)), e2 = st_expf(-kk * (ys + D)), dn = fmax_(1.0f - st_expf(-2.0f * kk * D), 1.0e-4f);
+      float aw = A[2] * A[3];
+      float sn, cs; st_sincosf(th, &sn, &cs);
+      float hc = aw * (e1 + e2) / dn * cs / kk;
+      v = v + v3(hc * A[0], aw * (e1 - e2) / dn * sn, hc * A[1]);
+    }
+    return v;
+  }
+  float layerW(V3 p) const {
+    if (P.ocean == 0u) return 0.0f;
+    float dw = fmin_(fmin_(p.x - P.x0, P.x1 - p.x), fmin_(p.z - P.z0, P.z1 - p.z));
+    return clampf(1.0f - dw / fmax_(P.olayer, 1.0e-4f), 0.0f, 1.0f);
+  }
   float fillPhi(V3 x) const {
     float dd = 1.0e9f;
     for (uint32_t k = 0; k < P.nfill; k++) {
@@ -298,6 +331,7 @@ struct Oracle {
         dd = fmin_(dd, length(x - v3(A[1], A[2], A[3])) - B[0]);
       }
     }
+    if (P.ocean != 0u) dd = fmin_(dd, x.y - oceanEta(x.x, x.z));
     return dd * P.ih;
   }
   // markAround (wgsl-core.js:239-246)
@@ -436,8 +470,50 @@ struct Oracle {
     P.airOn = airo ? 1u : 0u; P.airCouple = airo ? o->air_couple : 0.0f; P.airDecay = airo ? o->air_decay : 0.0f;
     P.airH = airCells ? (float)airH : 1.0f; P.airBlur = airo ? o->air_blur : 0.0f;
     P.aNx = airCells ? aNx : 1u; P.aNy = airCells ? aNy : 1u; P.aNz = airCells ? aNz : 1u;
+    // ocean (sim.js:210-218; oceanWaves, shared.js:760-780)
+    bool oc = o->ocean_on != 0;
+    P.ocean = oc ? 1u : 0u; P.otime = o->time; P.olevel = oc ? o->ocean_level : 0.0f; P.olayer = oc ? o->ocean_layer : 0.0f;
+    P.oy0 = (float)by0; P.odepth = oc ? (float)std::max((double)o->ocean_level - by0, 1e-3) : 1.0f;
+    P.nwave = oc ? oceanWaves(o, (double)o->g, (double)o->ocean_level - by0, P.waves) : 0u;
     bool dr = sprOn && o->drip_on != 0;
     P.ndrip = dr ? ndrip : 0u; P.dripRate = dr ? o->drip_rate : 0.0f; P.dripDry = dr ? o->drip_dry : 1.0f;
+  }
+
+  // oceanWaves (shared.js:760-780): mulberry32 draws, Pierson-Moskowitz amplitudes, dispersion by fixed-point iteration
+  static uint32_t oceanWaves(const st_step_opts* o, double g, double depth, float* w) {
+    auto toI32 = [](double x) -> int32_t {
+      if (!std::isfinite(x)) return 0;
+      double m = std::fmod(std::trunc(x), 4294967296.0); if (m < 0) m += 4294967296.0;
+      return (int32_t)(uint32_t)m;
+    };
+    int32_t sd = toI32((double)o->ocean_seed); if (sd == 0) sd = 1;
+    uint32_t a = (uint32_t)toI32((double)sd * 7919.0 + 13.0);
+    auto rnd = [&]() {
+      a += 0x6D2B79F5u;
+      uint32_t t = (a ^ (a >> 15)) * (1u | a);
+      t = (t + (t ^ (t >> 7)) * (61u | t)) ^ t;
+      return (double)(t ^ (t >> 14)) / 4294967296.0;
+    };
+    const int N = 24; const double PI = 3.141592653589793;
+    double D = std::max(depth, 1e-3), G = std::max(g, 1e-4), lp = std::max((double)o->ocean_length, 1e-3);
+    double kp = 2 * PI / lp, wp = std::sqrt(G * kp * std::tanh(kp * D));
+    auto kOf = [&](double om) { double k = om * om / G; for (int i = 0; i < 40; i++) k = om * om / (G * std::tanh(std::max(k * D, 1e-6))); return k; };
+    double dir = o->ocean_dir == o->ocean_dir ? o->ocean_dir : 0.0, sp = o->ocean_spread == o->ocean_spread ? o->ocean_spread : 0.0;
+    double th0 = dir * PI / 180, spr = std::max(0.0, sp) * PI / 180;
+    double K[N], OM[N], S[N], TH[N], PH[N], sum = 0;
+    for (int i = 0; i < N; i++) {
+      double r = 0.6 + 1.6 * (i + rnd()) / N;
+      OM[i] = r * wp; K[i] = kOf(OM[i]); S[i] = std::pow(r, -5) * std::exp(-1.25 * std::pow(r, -4));
+      double r1 = rnd(), r2 = rnd(), r3 = rnd();
+      TH[i] = th0 + spr * (r1 + r2 + r3 - 1.5) / 1.5; PH[i] = rnd() * 2 * PI; sum += S[i];
+    }
+    double hs = o->ocean_height == o->ocean_height ? o->ocean_height : 0.0, m0 = std::pow(std::max(hs, 0.0) / 4, 2);
+    for (int i = 0; i < N; i++) {
+      double amp = std::min(std::sqrt(2 * m0 * S[i] / sum), 0.3 / K[i]);
+      double rec[8] = {K[i] * std::cos(TH[i]), K[i] * std::sin(TH[i]), amp, OM[i], PH[i], K[i], 0, 0};
+      for (int q = 0; q < 8; q++) w[i * 8 + q] = (float)rec[q];
+    }
+    return N;
   }
 
   // ---- drip samples (dripSamples, bake.js:19-40, in JavaScript doubles; dripUpdate, sim.js:352-363) ----
@@ -524,7 +600,12 @@ struct Oracle {
         if (!inDom(i, j, k)) ph = 8.0f;
         if (P.nbInit == 2u) ph = fmin_(ph, phiOf(c));
         phiPut(c, ph);
-        if (P.nbInit == 1u) { velG[c * 3] = 0.0f; velG[c * 3 + 1] = 0.0f; velG[c * 3 + 2] = 0.0f; }
+        if (P.nbInit == 1u)
+          for (int ax = 0; ax < 3; ax++) {
+            V3 fp = facePos(i, j, k, ax); float v = 0.0f;
+            if (P.ocean != 0u && fp.y < oceanEta(fp.x, fp.z)) v = comp(oceanVel(fp), ax);
+            velG[c * 3 + ax] = v;
+          }
       });
     }
   }
@@ -618,6 +699,7 @@ struct Oracle {
       V3 x = cellCenter(i, j, k);
       float phA = phiSample(x - velGVec(x) * P.dt);
       bool inside = cnt[c] > 0 || phA < -1.0f;
+      if (P.ocean != 0u && layerW(x) >= 0.5f) inside = x.y < oceanEta(x.x, x.z);
       rhs[c] = inside ? clampf(phA, -7.9f, -0.5f) : clampf(phA, 0.5f, 7.9f);
     });
     auto jacA = [&]() { forActive([&](uint32_t c, int i, int j, int k) { phiPut(c, jacNb(i, j, k, rhs[c], true)); }); };
@@ -637,6 +719,7 @@ struct Oracle {
       V3 cx = cellCenter(i, j, k);
       if (!inDom(i, j, k)) ty = 0;
       else if ((sb & 0xff00u) != 0u) ty = 2;
+      else if (P.ocean != 0u && layerW(cx) >= 0.5f) ty = cx.y < oceanEta(cx.x, cx.z) ? 2u : 0u;
       else if (P.nb != 0u && phiOf(c) < -1.0f && (phiOf(c) < -P.band || calmV(velGVec(cx)))) ty = 1;
       else if (n > 0) {
         ty = 1;
@@ -694,6 +777,7 @@ struct Oracle {
           if (ci < 0 && th == 2u) ci = colAtCell(i, j, k);
           V3 fp = facePos(i, j, k, axis);
           if (ci >= 0) sv = comp(colSurfVel((uint32_t)ci, fp), axis);
+          else if (P.ocean != 0u && ((tl == 2u && inDom(li, lj, lk)) || (th == 2u && inDom(i, j, k)))) sv = comp(oceanVel(fp), axis);
           v = sv; old = sv;
         }
         accW[f] = fbits(old); accV[f] = fbits(v);
@@ -803,6 +887,7 @@ struct Oracle {
       V3 vn = v0 - v3(0.0f, P.gravity * P.dt, 0.0f); V3 vo = v0;
       if (hasStorage(fi, fj, fk)) sampleBoth(p, vn, vo);
       V3 v = vmix(vn, v0 + (vn - vo), P.flip);
+      if (P.ocean != 0u) { float lw = layerW(p); if (lw > 0.0f) { float s = clampf(lw * 2.0f, 0.0f, 1.0f); v = vmix(v, oceanVel(p), s * s * (1.0f - st_expf(-8.0f * P.dt))); } }
       V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
       int bi = (int)bcf.x, bj = (int)bcf.y, bk = (int)bcf.z;
       float csum = 8.0f * P.rest;
@@ -829,6 +914,7 @@ struct Oracle {
       float tau = fmax_(P.q5, 0.05f) * mixf(1.0f, 0.35f, smoothstep(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
       float foam = vel[i * 4 + 3] * st_expf(-P.dt / tau);
       foam = fmax_(foam, fmax_(spray * 0.9f, fmax_(impact, turb * 0.8f)));
+      if (P.ocean != 0u) foam *= 1.0f - clampf(layerW(p) * 2.0f, 0.0f, 1.0f);
       V3 gust = v3(0, 0, 0);
       if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
         V3 gp = p * 0.55f; float tt = P.q8 * 0.6f;
@@ -999,6 +1085,7 @@ struct Oracle {
       V3 np = p + v * P.dt;
       if (np.x < P.x0 || np.x > P.x1 || np.y < P.y0 || np.y > P.y1 || np.z < P.z0 || np.z > P.z1) life = 0.0f;
       else if (P.ncols > 0u && colAt(np) >= 0) life = 0.0f;
+      else if (P.ocean != 0u && kind >= 2u && layerW(np) > 0.6f) life = 0.0f;
       sPos[j * 4] = np.x; sPos[j * 4 + 1] = np.y; sPos[j * 4 + 2] = np.z; sPos[j * 4 + 3] = life;
       sVel[j * 4] = v.x; sVel[j * 4 + 1] = v.y; sVel[j * 4 + 2] = v.z; sVel[j * 4 + 3] = (float)kind + 0.4f * tk / WWHOLD;
     }
@@ -1048,6 +1135,7 @@ struct Oracle {
     for (int64_t ii = 0; ii < (int64_t)P.n; ii++) {
       uint32_t i = (uint32_t)ii;
       if (pos[i * 4 + 1] < DEADY) continue;
+      if (P.ocean != 0u && layerW(ppos(i)) > 0.0f) continue;
       V3 q = ppos(i); V3 v = pvel(i); float foam = vel[i * 4 + 3]; float spd = length(v);
       float fast = clampf((spd * P.vs - P.sprMin) / (2.0f * P.sprMin), 0.0f, 1.0f);
       V3 bcf = vfloor((q - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
@@ -1099,8 +1187,9 @@ struct Oracle {
     forParticles([&](uint32_t i) {                       // nbKill
       if (pos[i * 4 + 1] < DEADY) return;
       V3 q = ppos(i);
-      bool kill = false;
-      if (P.nb != 0u && calmV(pvel(i))) {
+      float lw = layerW(q);
+      bool kill = lw >= 0.5f || (lw > 0.25f && q.y > oceanEta(q.x, q.z) + 0.5f * P.h);
+      if (!kill && P.nb != 0u && calmV(pvel(i))) {
         int ci, cj, ck; particleCell(q, ci, cj, ck);
         if (hasStorage(ci, cj, ck) && phiOf(cellIdx(ci, cj, ck)) < -P.band) kill = true;
       }
@@ -1113,9 +1202,13 @@ struct Oracle {
     for (uint32_t tile : active) for (uint32_t local = 0; local < 512; local++) {
       int i, j, k; tileCoord(tile, local, i, j, k); uint32_t c = tile * 512 + local;
       if (!inDom(i, j, k) || colBits(c) != 0u) continue;
-      V3 cx = cellCenter(i, j, k); float ph = phiOf(c);
-      if ((ctype[c] & 0xffu) != 1u || ph > -1.0f || ph < -P.band) continue;
-      if (!calmV(velGVec(cx))) continue;
+      V3 cx = cellCenter(i, j, k); float ph = phiOf(c); float lw = layerW(cx);
+      if (lw > 0.25f && lw < 0.5f) {
+        if (cx.y > oceanEta(cx.x, cx.z) - 0.25f * P.h || ph < -P.band) continue;
+      } else {
+        if ((ctype[c] & 0xffu) != 1u || ph > -1.0f || ph < -P.band) continue;
+        if (!calmV(velGVec(cx))) continue;
+      }
       uint32_t n = (uint32_t)std::max(cnt[c], 0);
       if ((float)n >= 0.55f * P.rest) continue;
       uint32_t nd = std::min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
@@ -1132,6 +1225,7 @@ struct Oracle {
         uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
         V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
         V3 v = velGVec(x);
+        if (layerW(x) > 0.25f) v = oceanVel(x);
         pos[i * 4] = x.x; pos[i * 4 + 1] = x.y; pos[i * 4 + 2] = x.z; pos[i * 4 + 3] = fmin_(length(v), 63.0f);
         vel[i * 4] = v.x; vel[i * 4 + 1] = v.y; vel[i * 4 + 2] = v.z; vel[i * 4 + 3] = 0.0f;
       }
@@ -1163,7 +1257,7 @@ struct Oracle {
   // ---- FlipSim.step (sim.js:179-241, stage list :245-310) ----
   st_status step(double dt, const st_step_opts* o) {
     if (N == 0) return ST_NOT_READY;
-    bool nbOn = o->nb_on != 0;
+    bool nbOn = o->nb_on != 0 || o->ocean_on != 0;
     if (nbOn && !velGOn) velGOn = true;
     uint32_t init = nbOn && nbInit ? nbInit : 0;
     packCols(o);
@@ -1255,6 +1349,7 @@ st_status oracle_flip_read_drips(void* h, float* out8, uint32_t cap, uint32_t* n
   if (out8 && m) memcpy(out8, s->drip.data(), (size_t)m * 32);
   return ST_OK;
 }
+int oracle_ocean_waves(const st_step_opts* o, double depth, float* w) { return (int)Oracle::oceanWaves(o, (double)o->g, depth, w); }
 st_status oracle_flip_set_deep_look(void* h, int on) { ((Oracle*)h)->deepOn = on != 0; return ST_OK; }
 // one deep pass when the deep look applies (deep look on, narrow band and kept velocities on at the last step), as
 // float4 points; *n receives the count (0 when it does not apply)

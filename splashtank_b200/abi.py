@@ -39,7 +39,10 @@ class StepOpts(C.Structure):
                 ("foam_sens", C.c_float), ("gust", C.c_float), ("tear", C.c_float), ("vs", C.c_float), ("iters", C.c_int32),
                 ("flags", C.c_uint32), ("ncols", C.c_uint32), ("cols", C.POINTER(Collider)), ("spray_on", C.c_int32),
                 ("spray", SprayOpts), ("nb_on", C.c_int32), ("nb_band", C.c_float), ("air_on", C.c_int32), ("air_couple", C.c_float), ("air_decay", C.c_float), ("air_blur", C.c_float),
-                ("drip_on", C.c_int32), ("drip_rate", C.c_float), ("drip_dry", C.c_float)]
+                ("drip_on", C.c_int32), ("drip_rate", C.c_float), ("drip_dry", C.c_float),
+                ("ocean_on", C.c_int32), ("ocean_level", C.c_float), ("ocean_layer", C.c_float), ("ocean_length", C.c_float),
+                ("ocean_height", C.c_float), ("ocean_dir", C.c_float), ("ocean_spread", C.c_float), ("ocean_seed", C.c_int32),
+                ("time", C.c_float)]
 
 
 class Stats(C.Structure):
@@ -137,6 +140,7 @@ class SdfBuild(C.Structure):
 
 
 SDF_FUNCS = [("build_sdf", C.c_int, [C.c_int, C.POINTER(Mesh), C.POINTER(SdfBuild)])]
+OCEAN_FUNCS = [("ocean_waves", C.c_int, [C.POINTER(StepOpts), C.c_double, f32p])]
 
 
 class LiveLayout(C.Structure):

@@ -8,7 +8,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = ["capi.cu", "flip_kernels.cu", "flip_extra.cu", "pbf.cu", "poisson.cu", "diff.cu", "frames.cu", "live.cu", "sdf_build.cu", "drips.cpp"]
+SRC = ["capi.cu", "flip_kernels.cu", "flip_extra.cu", "pbf.cu", "poisson.cu", "diff.cu", "frames.cu", "live.cu", "sdf_build.cu", "drips.cpp", "ocean.cpp"]
 OUT = os.path.join(HERE, "libsplashtank_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",

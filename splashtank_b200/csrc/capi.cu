@@ -60,10 +60,11 @@ struct st_flip {
   std::string sdfSig;
   size_t sdfCap = 0;
   FlipParams hp{};
+  float waves[32 * 8] = {};   // this step's ocean waves (oceanWaves)
   // per-step uploads (parameter block + collider records) come from a ring of pinned host blocks, so the copies are
   // asynchronous and a block is rewritten only after the copy that read it has run
   static constexpr int RING = 16;
-  struct Upload { FlipParams P; alignas(16) float cols[32 * 32]; };   // cols are read as float4
+  struct Upload { FlipParams P; alignas(16) float cols[32 * 32]; alignas(16) float waves[32 * 8]; };   // cols and waves: float4 reads
   Upload* ring_h = nullptr;
   cudaEvent_t ring_ev[RING] = {};
   int ring_i = 0;
@@ -139,6 +140,7 @@ struct st_flip {
     B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
     B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
+    B.waves = reinterpret_cast<const float4*>(dUp->waves);
     B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.drip = drip; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
@@ -453,6 +455,12 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
   P.airOn = airOn ? 1u : 0u; P.airCouple = airOn ? o->air_couple : 0.0f; P.airDecay = airOn ? o->air_decay : 0.0f;
   P.airH = s->airCells ? (float)s->airH : 1.0f; P.airBlur = airOn ? o->air_blur : 0.0f;
   P.aNx = s->airCells ? s->aNx : 1u; P.aNy = s->airCells ? s->aNy : 1u; P.aNz = s->airCells ? s->aNz : 1u;
+  // ocean (words 57-61, 63, 66 and the wave list, src/flip/sim.js:210-218)
+  const bool oc = o->ocean_on != 0;
+  P.ocean = oc ? 1u : 0u;
+  P.nwave = oc ? (uint32_t)ocean_waves(o, (double)o->g, (double)o->ocean_level - s->by0, s->waves) : 0u;
+  P.otime = o->time; P.olevel = oc ? o->ocean_level : 0.0f; P.olayer = oc ? o->ocean_layer : 0.0f; P.oy0 = (float)s->by0;
+  P.odepth = oc ? (float)std::max((double)o->ocean_level - s->by0, 1e-3) : 1.0f;
   // drips (words 79-81): on only with whitewater on this step
   const bool drOn = sprOn && o->drip_on != 0;
   P.ndrip = drOn ? s->ndrip : 0u; P.dripRate = drOn ? o->drip_rate : 0.0f; P.dripDry = drOn ? o->drip_dry : 1.0f;
@@ -492,16 +500,17 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(2);
   if (nbOn) nl += launch_nb_phi(B, gT4, q);
   mark(3);
-  nl += launch_classify(B, gT4, q);
+  const bool ocean = s->hp.ocean != 0;
+  nl += launch_classify(B, gT4, ocean, q);
   if (nbOn) nl += launch_nb_vel(B, gT4, q);
   mark(4);
-  nl += launch_norm_div(B, gT4, q);
+  nl += launch_norm_div(B, gT4, ocean, q);
   mark(5);
   nl += launch_sor_compact(B, s->tileGrid(s->gridSor), gT4, iters, q);
   mark(6);
   nl += launch_project(B, gT4, q);
   mark(7);
-  nl += launch_g2p(B, gT, q);
+  nl += launch_g2p(B, gT, ocean, q);
   mark(8);
   if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, s->hp.ndrip != 0, gT4, q);
   mark(9);
@@ -511,11 +520,12 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
 }
 
 // A step's kernels as a CUDA graph, keyed by everything that changes what is launched: the particle buffer parity,
-// the particle count (grid sizes), SOR iterations, narrow band, whitewater emission, the air field and stage timing. Stage markers are
-// external event-record nodes, pointed at the timing ring's events before each launch.
+// the particle count (grid sizes), SOR iterations, narrow band, whitewater emission, the air field, drips, the ocean
+// and stage timing. Stage markers are external event-record nodes, pointed at the timing ring's events before each
+// launch.
 static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, bool timing) {
   return (uint64_t)s->cur | ((uint64_t)s->parity << 1) | ((uint64_t)nbOn << 2) | ((uint64_t)sprOn << 3) | ((uint64_t)timing << 4) |
-         ((uint64_t)(s->hp.airOn != 0) << 5) | ((uint64_t)(s->hp.ndrip != 0) << 6) |
+         ((uint64_t)(s->hp.airOn != 0) << 5) | ((uint64_t)(s->hp.ndrip != 0) << 6) | ((uint64_t)(s->hp.ocean != 0) << 7) |
          ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24);
 }
 static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, bool timing, st_flip::Graph** out) {
@@ -577,7 +587,7 @@ static void drop_graphs(st_flip* s) {
 // The host half of a step: parameter block, collider records and counters, with the uploads enqueued on q.
 struct StepPrep { bool nbOn = false, sprOn = false; uint32_t init = 0; int iters = 1; };
 static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cudaStream_t q, StepPrep* pr) {
-  const bool nbOn = o->nb_on != 0;
+  const bool nbOn = o->nb_on != 0 || o->ocean_on != 0;   // the ocean keeps its water by depth: it turns the narrow band on
   if (nbOn) s->velGOn = true;
   const uint32_t init = nbOn && s->nbInit ? s->nbInit : 0;
   // the next pinned upload block: wait for the copy that last read it
@@ -609,6 +619,10 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   up->P = s->hp;
   CK(cudaMemcpyAsync(&s->dUp->P, &up->P, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
   if (nc) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
+  if (s->hp.nwave) {
+    memcpy(up->waves, s->waves, s->hp.nwave * 8 * sizeof(float));
+    CK(cudaMemcpyAsync(s->dUp->waves, up->waves, s->hp.nwave * 8 * sizeof(float), cudaMemcpyHostToDevice, q));
+  }
   CK(cudaEventRecord(upEv, q));
   pr->nbOn = nbOn; pr->sprOn = sprOn; pr->init = init; pr->iters = iters;
   return ST_OK;

@@ -37,7 +37,9 @@ struct FlipParams {
   float airCouple, airDecay, airH, airBlur;
   uint32_t ndrip;                         // drips (words 79-81)
   float dripRate, dripDry;
-  uint32_t padW;
+  uint32_t ocean, nwave;                  // ocean (words 57-61, 63, 66; the waves follow the collider records)
+  float otime, olevel, olayer, oy0, odepth;
+  uint32_t padW[2];
   float fills[16][4];
 };
 // the collider records follow the block in the upload buffer and are read as float4
@@ -114,6 +116,7 @@ struct Bufs {
   float4* air2;
   int32_t* airAcc;      // 4 per air cell: sum of v w 256 (x, y, z) and of w 256
   float4* drip;         // 2 per drip sample (dripSamples, src/flip/bake.js:19-40): local position + collider, local normal + wetness
+  const float4* waves;  // ocean: 2 per wave, (kx, kz, amplitude, angular frequency) and (phase, wavenumber, 0, 0)
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)
   const float* sdf;
@@ -247,6 +250,59 @@ __device__ __forceinline__ float velGAxis(const FlipParams& P, const float* __re
 }
 __device__ __forceinline__ V3 velGVec(const FlipParams& P, const float* __restrict__ velG, uint32_t nc, V3 x) {
   return v3(velGAxis(P, velG, nc, x, 0), velGAxis(P, velG, nc, x, 1), velGAxis(P, velG, nc, x, 2));
+}
+
+// ---- ocean (src/flip/wgsl-core.js:201-226): a sum of linear (Airy) waves ----
+// Out of line: inlined, the wave loops raise the register count of the kernels that call them.
+static __device__ __noinline__ float oceanEta(const FlipParams& P, const float4* __restrict__ W, float x, float z) {
+  float e = 0.0f;
+  for (uint32_t k = 0; k < P.nwave; k++) {
+    const float4 A = W[2 * k], Bw = W[2 * k + 1];
+    float sn, cs;
+    st_sincosf(A.x * x + A.y * z - A.w * P.otime + Bw.x, &sn, &cs);
+    e += A.z * cs;
+  }
+  return P.olevel + e;
+}
+// the water velocity under the waves over a floor at depth odepth, the height stretched so a crest gets the surface value
+static __device__ __noinline__ V3 oceanVel(const FlipParams& P, const float4* __restrict__ W, V3 p) {
+  const float D = fmx(P.odepth, 1.0e-3f), eta = oceanEta(P, W, p.x, p.z);
+  const float ys = clampf((p.y - P.oy0) * D / fmx(D + eta - P.olevel, 0.1f * D), 0.0f, D);
+  V3 v = v3(0.0f, 0.0f, 0.0f);
+  for (uint32_t k = 0; k < P.nwave; k++) {
+    const float4 A = W[2 * k], Bw = W[2 * k + 1];
+    const float kk = fmx(Bw.y, 1.0e-4f);
+    const float th = A.x * p.x + A.y * p.z - A.w * P.otime + Bw.x;
+    const float e1 = st_expf(kk * (ys - D)), e2 = st_expf(-kk * (ys + D)), dn = fmx(1.0f - st_expf(-2.0f * kk * D), 1.0e-4f);
+    const float aw = A.z * A.w;
+    float sn, cs;
+    st_sincosf(th, &sn, &cs);
+    const float hc = aw * (e1 + e2) / dn * cs / kk;
+    v = v + v3(hc * A.x, aw * (e1 - e2) / dn * sn, hc * A.y);
+  }
+  return v;
+}
+// 1 at the side walls, 0 a boundary width in from them: above 0.5 the ocean is prescribed, below it particles are nudged
+__device__ __forceinline__ float layerW(const FlipParams& P, V3 p) {
+  if (P.ocean == 0u) return 0.0f;
+  const float dw = fmn(fmn(p.x - P.x0, P.x1 - p.x), fmn(p.z - P.z0, P.z1 - p.z));
+  return clampf(1.0f - dw / fmx(P.olayer, 1.0e-4f), 0.0f, 1.0f);
+}
+// fillPhi (wgsl-core.js:227-238): signed distance in cells to the starting water, boxes, spheres and the ocean
+__device__ __forceinline__ float fillPhi(const FlipParams& P, const float4* __restrict__ W, V3 x) {
+  float d = 1.0e9f;
+  for (uint32_t k = 0; k < P.nfill; k++) {
+    const float* A = P.fills[k * 2];
+    const float* Bq = P.fills[k * 2 + 1];
+    if (A[0] < 1.5f) {
+      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
+      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
+    } else {
+      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
+    }
+  }
+  if (P.ocean != 0u) d = fmn(d, x.y - oceanEta(P, W, x.x, x.z));
+  return d * P.ih;
 }
 
 // ---- colliders (src/gpu.js:6-38, src/flip/wgsl-core.js:113-126) ----

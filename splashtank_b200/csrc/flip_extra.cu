@@ -10,21 +10,6 @@
 
 namespace st {
 
-__device__ __forceinline__ float fillPhiX(const FlipParams& P, V3 x) {
-  float d = 1.0e9f;
-  for (uint32_t k = 0; k < P.nfill; k++) {
-    const float* A = P.fills[k * 2];
-    const float* Bq = P.fills[k * 2 + 1];
-    if (A[0] < 1.5f) {
-      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
-      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
-    } else {
-      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
-    }
-  }
-  return d * P.ih;
-}
-
 // ---- phiInitAll (wgsl-narrowband.js:20-35) ----
 __global__ void __launch_bounds__(512) k_nb_init(Bufs B) {
   __shared__ FlipParams P;
@@ -34,13 +19,20 @@ __global__ void __launch_bounds__(512) k_nb_init(Bufs B) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
-    float ph = clampf(fillPhiX(P, cellCenter(P, i, j, k)), -7.9f, 7.9f);
+    float ph = clampf(fillPhi(P, B.waves, cellCenter(P, i, j, k)), -7.9f, 7.9f);
     if (ph < 0.0f) ph = fmn(ph, -1.5f);
     if (!inDom(P, i, j, k)) ph = 8.0f;
     const uint32_t ct = B.ctype[c];
     if (P.nbInit == 2u) ph = fmn(ph, phiOfBits(ct));
     B.ctype[c] = phiPutBits(ct, ph);
-    if (P.nbInit == 1u) { B.velG[c] = 0.0f; B.velG[nc + c] = 0.0f; B.velG[2 * nc + c] = 0.0f; }
+    if (P.nbInit == 1u) {   // the starting velocity: the waves' under the ocean's surface, else at rest
+      for (int ax = 0; ax < 3; ax++) {
+        const V3 fp = facePos(P, i, j, k, ax);
+        float v = 0.0f;
+        if (P.ocean != 0u && fp.y < oceanEta(P, B.waves, fp.x, fp.z)) v = comp3(oceanVel(P, B.waves, fp), ax);
+        B.velG[ax * nc + c] = v;
+      }
+    }
   }
 }
 
@@ -74,7 +66,8 @@ __global__ void __launch_bounds__(512) k_nb_phi(Bufs B) {
     if (((B.ctype[c] >> 8) & 0xffu) != 0u) { B.rhs[c] = 0.5f; continue; }
     const V3 x = cellCenter(P, i, j, k);
     const float phA = phiSampleX(P, B.ctype, x - velGVec(P, B.velG, nc, x) * P.dt);
-    const bool inside = B.cnt[c] > 0 || phA < -1.0f;
+    bool inside = B.cnt[c] > 0 || phA < -1.0f;
+    if (P.ocean != 0u && layerW(P, x) >= 0.5f) inside = x.y < oceanEta(P, B.waves, x.x, x.z);   // the ocean's boundary decides
     B.rhs[c] = inside ? clampf(phA, -7.9f, -0.5f) : clampf(phA, 0.5f, 7.9f);
   }
 }
@@ -186,8 +179,14 @@ __device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs&
   const uint32_t ct = B.ctype[c];
   if (((ct >> 8) & 0xffu) != 0u) return 0;
   const float ph = phiOfBits(ct);
-  if ((ct & 0xffu) != 1u || ph > -1.0f || ph < -P.band) return 0;
-  if (!(len3(velGVec(P, B.velG, B.ncell, cellCenter(P, i, j, k))) < 9.0f * P.h)) return 0;
+  const V3 cx = cellCenter(P, i, j, k);
+  const float lw = layerW(P, cx);
+  if (lw > 0.25f && lw < 0.5f) {   // the inner half of the ocean's boundary is full below the ocean's surface
+    if (cx.y > oceanEta(P, B.waves, cx.x, cx.z) - 0.25f * P.h || ph < -P.band) return 0;
+  } else {
+    if ((ct & 0xffu) != 1u || ph > -1.0f || ph < -P.band) return 0;
+    if (!(len3(velGVec(P, B.velG, B.ncell, cx)) < 9.0f * P.h)) return 0;
+  }
   const uint32_t n = (uint32_t)max(B.cnt[c], 0);
   if ((float)n >= 0.55f * P.rest) return 0;
   return min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
@@ -230,7 +229,7 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
       const uint32_t pi = deadSlot(B, kk, nKilled, nLive);
       const uint32_t hh = (e * 9781u + m * 6271u + 17u) ^ (P.seed * 2654435761u);
       const V3 x = v3(P.x0, P.y0, P.z0) + (cp + v3(hash1(hh + 1u), hash1(hh + 2u), hash1(hh + 3u))) * P.h;
-      const V3 v = velGVec(P, B.velG, nc, x);
+      const V3 v = layerW(P, x) > 0.25f ? oceanVel(P, B.waves, x) : velGVec(P, B.velG, nc, x);
       Part q;
       q.p = make_float4(x.x, x.y, x.z, fmn(len3(v), 63.0f));
       q.v = make_float4(v.x, v.y, v.z, 0.0f);
@@ -467,6 +466,7 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
     const V3 np = p + v * P.dt;
     if (np.x < P.x0 || np.x > P.x1 || np.y < P.y0 || np.y > P.y1 || np.z < P.z0 || np.z > P.z1) life = 0.0f;
     else if (P.ncols > 0u && colAt(P, B.cols, B.sdf, np) >= 0) life = 0.0f;
+    else if (P.ocean != 0u && kind >= 2u && layerW(P, np) > 0.6f) life = 0.0f;   // foam and bubbles end at the ocean's boundary
     B.sPos[j] = make_float4(np.x, np.y, np.z, life);
     B.sVel[j] = make_float4(v.x, v.y, v.z, (float)kind + 0.4f * tk / WWHOLD);
   }

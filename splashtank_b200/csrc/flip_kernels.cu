@@ -103,22 +103,6 @@ __global__ void __launch_bounds__(512) k_mark_phi(Bufs B) {
   }
 }
 
-// fillPhi (wgsl-core.js:228-238) for box and sphere fills
-__device__ __forceinline__ float fillPhi(const FlipParams& P, V3 x) {
-  float d = 1.0e9f;
-  for (uint32_t k = 0; k < P.nfill; k++) {
-    const float* A = P.fills[k * 2];
-    const float* Bq = P.fills[k * 2 + 1];
-    if (A[0] < 1.5f) {
-      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
-      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
-    } else {
-      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
-    }
-  }
-  return d * P.ih;
-}
-
 // tileMarkFill (wgsl-narrowband.js:12-18): on a restart every tile the starting water reaches
 __global__ void k_mark_fill(Bufs B) {
   __shared__ FlipParams P;
@@ -126,7 +110,7 @@ __global__ void k_mark_fill(Bufs B) {
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntiles; t += gridDim.x * blockDim.x) {
     uint32_t tt = t / P.tx;
     V3 tc = v3((float)(t % P.tx), (float)(tt % P.ty), (float)(tt / P.ty)) * 8.0f + v3(4.0f, 4.0f, 4.0f);
-    if (fillPhi(P, v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) B.need[t] = P.stamp;
+    if (fillPhi(P, B.waves, v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) B.need[t] = P.stamp;
   }
 }
 
@@ -333,6 +317,9 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
 }
 
 // ---- 6. collider bits (solidBuild, wgsl-solver.js:42-45) + classify (wgsl-solver.js:47-74) ----
+// OCEAN: compiled with the ocean's boundary (an ocean scene) or without it, so the other scenes' kernels carry none
+// of its code or registers
+template <bool OCEAN>
 __global__ void __launch_bounds__(512) k_classify(Bufs B) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
@@ -349,6 +336,8 @@ __global__ void __launch_bounds__(512) k_classify(Bufs B) {
     uint32_t ty = 0;
     if (!inDom(P, i, j, k)) ty = 0;
     else if ((sb & 0xff00u) != 0u) ty = 2;
+    else if (OCEAN && P.ocean != 0u && layerW(P, cx) >= 0.5f)   // the ocean's boundary: a wall moving with the waves
+      ty = cx.y < oceanEta(P, B.waves, cx.x, cx.z) ? 2u : 0u;
     else if (P.nb != 0u && phiOfBits(ct) < -1.0f &&
              (phiOfBits(ct) < -P.band || len3(velGVec(P, B.velG, nc, cx)) < 9.0f * P.h)) ty = 1;
     else if (n > 0) {
@@ -381,6 +370,7 @@ __device__ __forceinline__ int colAtCell(const FlipParams& P, const uint32_t* __
   if (!inDom(P, i, j, k)) return -1;
   return (int)((ctype[cellIdx(P, i, j, k)] >> 8) & 0xffu) - 1;
 }
+template <bool OCEAN>
 __device__ __forceinline__ void normBody(const FlipParams& P, const Bufs& B, int axis, int i, int j, int k, uint32_t c, float& vOut, float& oldOut) {
   int li = i, lj = j, lk = k;
   if (axis == 0) li -= 1; else if (axis == 1) lj -= 1; else lk -= 1;
@@ -395,12 +385,15 @@ __device__ __forceinline__ void normBody(const FlipParams& P, const Bufs& B, int
     if (tl == 2u) ci = colAtCell(P, B.ctype, li, lj, lk);
     if (ci < 0 && th == 2u) ci = colAtCell(P, B.ctype, i, j, k);
     if (ci >= 0) sv = comp3(colSurfVel(B.cols, (uint32_t)ci, facePos(P, i, j, k, axis)), axis);
+    else if (OCEAN && P.ocean != 0u && ((tl == 2u && inDom(P, li, lj, lk)) || (th == 2u && inDom(P, i, j, k))))
+      sv = comp3(oceanVel(P, B.waves, facePos(P, i, j, k, axis)), axis);
     v = sv;
     old = sv;
   }
   vOut = v;
   oldOut = old;
 }
+template <bool OCEAN>
 __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float svn[3][512];
@@ -413,7 +406,7 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
     tileCoord(P, t, threadIdx.x, i, j, k);
     for (int axis = 0; axis < 3; axis++) {
       float v, old;
-      normBody(P, B, axis, i, j, k, c, v, old);
+      normBody<OCEAN>(P, B, axis, i, j, k, c, v, old);
       B.vn[axis * nc + c] = v;
       B.vo[axis * nc + c] = old;
       svn[axis][threadIdx.x] = v;
@@ -431,9 +424,9 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
     } else {
       float d, o2;
       float vxp, vyp, vzp;
-      if (lx < 7) vxp = svn[0][threadIdx.x + 1]; else { normBody(P, B, 0, i + 1, j, k, cellIdx(P, i + 1, j, k), d, o2); vxp = d; }
-      if (ly < 7) vyp = svn[1][threadIdx.x + 8]; else { normBody(P, B, 1, i, j + 1, k, cellIdx(P, i, j + 1, k), d, o2); vyp = d; }
-      if (lz < 7) vzp = svn[2][threadIdx.x + 64]; else { normBody(P, B, 2, i, j, k + 1, cellIdx(P, i, j, k + 1), d, o2); vzp = d; }
+      if (lx < 7) vxp = svn[0][threadIdx.x + 1]; else { normBody<OCEAN>(P, B, 0, i + 1, j, k, cellIdx(P, i + 1, j, k), d, o2); vxp = d; }
+      if (ly < 7) vyp = svn[1][threadIdx.x + 8]; else { normBody<OCEAN>(P, B, 1, i, j + 1, k, cellIdx(P, i, j + 1, k), d, o2); vyp = d; }
+      if (lz < 7) vzp = svn[2][threadIdx.x + 64]; else { normBody<OCEAN>(P, B, 2, i, j, k + 1, cellIdx(P, i, j, k + 1), d, o2); vzp = d; }
       const float div = (vxp - svn[0][threadIdx.x] + vyp - svn[1][threadIdx.x] + vzp - svn[2][threadIdx.x]) * P.ih;
       bool interior = true;
       uint32_t mask = 0, nns = 0;
@@ -776,6 +769,7 @@ struct G2PUni {
 __device__ __forceinline__ G2PUni g2pUni(const FlipParams& P) {
   return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f};
 }
+template <bool OCEAN>
 __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q) {
   const V3 p = xyz(q.p), v0 = xyz(q.v);
   int fi, fj, fk;
@@ -783,6 +777,13 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   V3 vn, vo;
   sampleWin(P, W, p, vn, vo);    // the particle's own tile has storage: it marked it this step
   V3 v = vmix(vn, v0 + (vn - vo), P.flip);
+  if (OCEAN && P.ocean != 0u) {   // near the ocean's boundary, ease into the waves
+    const float lw = layerW(P, p);
+    if (lw > 0.0f) {
+      const float s = clampf(lw * 2.0f, 0.0f, 1.0f);
+      v = vmix(v, oceanVel(P, B.waves, p), s * s * (1.0f - st_expf(-8.0f * P.dt)));
+    }
+  }
   const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
   const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
   float csum = 8.0f * P.rest;
@@ -809,6 +810,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const float tau = U.tau0 * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
   float foam = q.v.w * st_expf(-P.dt / tau);
   foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
+  if (OCEAN && P.ocean != 0u) foam *= 1.0f - clampf(layerW(P, p) * 2.0f, 0.0f, 1.0f);   // easing into the waves is not churning
   V3 gust = v3(0.0f, 0.0f, 0.0f);
   if (P.q7 > 0.0f && P.q4 > 0.0f && (!fast || shield < 0.9f)) {
     const V3 gp = p * 0.55f;
@@ -842,6 +844,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
 // One CTA per tile with storage: the tile's particles are one contiguous sorted segment, and every face and count they
 // sample lies in the 10^3-cell window (the tile plus one cell around it), staged once in shared memory.
 constexpr int G2P_T = 256;
+template <bool OCEAN>
 __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
@@ -896,7 +899,7 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
     uint32_t emitSum = 0, deadSum = 0;
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
       Part q = B.pa[i];
-      g2pOne(P, B, W, gtab, U, q);
+      g2pOne<OCEAN>(P, B, W, gtab, U, q);
       // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
       const bool gone = q.p.y < DEADY;
@@ -904,7 +907,8 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
       // e is 0 (or NaN) unless the particle is fast enough for crest (speed over sprMin) or churn (over 0.5): the
       // common slow particle skips the eight wetness reads (kc stays 0 either way)
       const float xs = len3(xyz(q.v)) * P.vs;
-      if (!gone && needWet && U.settle != 0.0f && (xs - P.sprMin > 0.0f || xs > 0.5f)) {
+      const bool oceanSide = OCEAN && P.ocean != 0u && !gone && layerW(P, xyz(q.p)) > 0.0f;   // no whitewater from the ocean's boundary
+      if (!gone && needWet && !oceanSide && U.settle != 0.0f && (xs - P.sprMin > 0.0f || xs > 0.5f)) {
         float rho, fast, e;
         // the eight cells around the moved particle: from the window when it holds them
         const V3 bcf = vfloor((xyz(q.p) - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
@@ -917,7 +921,11 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
         }
       }
       bool kill = false;
-      if (!gone && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
+      if (oceanSide) {   // inside the ocean's boundary, or above the ocean's surface in its inner half
+        const float lw = layerW(P, xyz(q.p));
+        kill = lw >= 0.5f || (lw > 0.25f && q.p.y > oceanEta(P, B.waves, q.p.x, q.p.z) + 0.5f * P.h);
+      }
+      if (!kill && !gone && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
         int ci, cj, ck;
         particleCell(P, xyz(q.p), ci, cj, ck);
         if (W.has(ci, cj, ck)) kill = W.kill[W.idx(ci, cj, ck)] != 0;
@@ -982,8 +990,16 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
 int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
 int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<(B.nblk + CM_U - 1) / CM_U, PBLK, 0, s>>>(B); return 1; }
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
-int launch_classify(const Bufs& B, int grid, cudaStream_t s) { k_classify<<<grid, 512, 0, s>>>(B); return 1; }
-int launch_norm_div(const Bufs& B, int grid, cudaStream_t s) { k_norm_div<<<grid, 512, 0, s>>>(B); return 1; }
+int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
+  if (ocean) k_classify<true><<<grid, 512, 0, s>>>(B);
+  else k_classify<false><<<grid, 512, 0, s>>>(B);
+  return 1;
+}
+int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
+  if (ocean) k_norm_div<true><<<grid, 512, 0, s>>>(B);
+  else k_norm_div<false><<<grid, 512, 0, s>>>(B);
+  return 1;
+}
 int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s) {
   k_sor_slots<<<64, 256, 0, s>>>(B);
   k_sor_pack<<<grid4, 512, 0, s>>>(B);
@@ -992,8 +1008,9 @@ int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream
   return 2 * iters + 3;
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
-int launch_g2p(const Bufs& B, int grid, cudaStream_t s) {
-  k_g2p<<<grid, G2P_T, 0, s>>>(B);
+int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
+  if (ocean) k_g2p<true><<<grid, G2P_T, 0, s>>>(B);
+  else k_g2p<false><<<grid, G2P_T, 0, s>>>(B);
   return 1;
 }
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {

@@ -13,11 +13,12 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s);
 int launch_scan_counts(const Bufs& B, cudaStream_t s);
 int launch_scatter(const Bufs& B, cudaStream_t s);
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
-int launch_classify(const Bufs& B, int grid, cudaStream_t s);
-int launch_norm_div(const Bufs& B, int grid, cudaStream_t s);
+// ocean: the kernels compiled with the ocean's boundary (only an ocean scene needs them)
+int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s);
+int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s);
 int launch_project(const Bufs& B, int grid, cudaStream_t s);
-int launch_g2p(const Bufs& B, int grid, cudaStream_t s);
+int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);
 int launch_fill_f32(float* p, float v, size_t n, cudaStream_t s);
 int launch_iota(uint32_t* p, uint32_t n, cudaStream_t s);
@@ -31,6 +32,8 @@ int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, bool drip, int grid, cudaStream_t s);
 // drip samples of one collider's distance grid (drips.cpp), appended to out: 8 floats each
 void drip_samples(const st_sdf* sdf, double h, uint32_t k, std::vector<float>& out);
+// the ocean's wave list (ocean.cpp): 8 floats per wave into w (room for 24); returns the number of waves
+int ocean_waves(const st_step_opts* o, double g, double depth, float* w);
 // frames and bake measurements (frames.cu)
 struct FrameBox { double x0, y0, z0, kx, ky, kz, ks; };
 struct DiagBox { double x0, y0, z0, x1, y1, z1, hy, cap; };

@@ -129,7 +129,30 @@ def make_opts(o, opt=None, default=None):
     s.drip_on = 1 if (drip and drip.get("on")) else 0
     s.drip_rate = float((drip or {}).get("rate", 0.0))
     s.drip_dry = float((drip or {}).get("dry", 1.0))
+    oc = o.get("ocean")
+    s.ocean_on = 1 if (oc and oc.get("on")) else 0
+    if oc:
+        s.ocean_level = float(oc.get("level", 0.0))
+        s.ocean_layer = float(oc.get("layer", 0.0))
+        s.ocean_length = float(oc.get("length", 0.0))
+        s.ocean_height = float(oc.get("height", 0.0))
+        s.ocean_dir = float(oc.get("dir", 0.0))
+        s.ocean_spread = float(oc.get("spread", 0.0))
+        s.ocean_seed = int(oc.get("seed", 0))
+    s.time = float(o.get("time") or 0.0)
     return s, cols
+
+
+def ocean_waves(ocean, g=9.81, depth=None, y0=0.0):
+    """oceanWaves (src/shared.js:760-780) through st_ocean_waves: (24, 8) float32 rows kx, kz, amplitude, angular
+    frequency, phase, wavenumber, 0, 0. depth defaults to the mean level above y0."""
+    s, keep = make_opts(dict(g=g, ocean=dict(ocean, on=True)))
+    w = np.zeros(32 * 8, np.float32)
+    d = float(ocean["level"] - y0 if depth is None else depth)
+    f = abi.bind(load_library()[0], "st_", abi.OCEAN_FUNCS)
+    n = f["ocean_waves"](C.byref(s), d, w.ctypes.data_as(abi.f32p))
+    del keep
+    return w[:n * 8].reshape(n, 8)
 
 
 class FlipSim:

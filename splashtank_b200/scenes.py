@@ -37,6 +37,24 @@ def box_cells(n_xyz, pred):
     return np.stack([i[m], j[m], k[m]], 1)
 
 
+def ocean_tank(n=32, seed=5, level=0.3, layer=0.12, height=0.05, length=0.35, band=3.0, spray_cap=20000):
+    """An ocean scene: waves (24 linear waves, significant height `height`, peak wavelength `length`) at mean level
+    `level`, held to the side walls by a boundary layer `layer` wide; narrow band of `band` cells. The particles start
+    in the band under the mean level (8 per cell, seeded jitter, at rest) inside the boundary's inner half; the depth
+    field and the starting velocity come from the ocean itself (fillPhi and phiInitAll on a restart). Whitewater with
+    the app's settings, the air field and gusts."""
+    h = 1.0 / n
+    rng = np.random.default_rng(seed)
+    lw = lambda ci, ck: 1.0 - np.minimum(np.minimum(ci * h, 1.0 - ci * h), np.minimum(ck * h, 1.0 - ck * h)) / layer   # noqa: E731
+    cells = box_cells((n, n, n), lambda ci, cj, ck: (cj * h < level) & (cj * h > level - band * h) & (lw(ci, ck) < 0.5))
+    pos = seed_cells(cells, h, rng, -0.5, 0.0, -0.5)
+    ocean = dict(on=True, level=level, layer=layer, length=length, height=height, dir=30.0, spread=20.0, seed=3)
+    opts = dict(g=9.81, flip=0.95, comp=6.0, iters=30, vmax=50.0, drag=0.3, gust=1.0, tear=2.0, spr=dict(APP_SPRAY, min=0.25),
+                nb=dict(on=True, band=band), ocean=ocean, air=dict(on=True, couple=3.0, decay=0.6))
+    return dict(d=h / 2.0, ratio=2.0, size=(1.0, 1.0, 1.0), open=0, pos=pos, vel=np.zeros_like(pos), dt=1.0 / 240.0, opts=opts,
+                spray_cap=spray_cap, spare=len(pos) // 2 + 4000, name="ocean_tank_%d" % n)
+
+
 def dam_break(n=64, seed=1234, fx=0.4, fy=0.6):
     """Plain FLIP dam break: n^3 MAC grid (dx = 1/n) in 8^3 blocks, solid walls; fluid where the cell centre has
     x < fx and y < fy (all z); 8 particles per cell, seeded jitter. FLIP 0.97, gravity 9.81, dt 1/240, 50 red-black SOR

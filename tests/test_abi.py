@@ -34,7 +34,7 @@ def test_bindings_match_the_library():
     from splashtank_b200 import abi, build
     lib = C.CDLL(build.build())
     lists = (abi.FLIP_FUNCS + abi.CUDA_ONLY_FUNCS + abi.PBF_FUNCS + abi.POISSON_FUNCS + abi.NOALLOC_FUNCS + abi.BATCH_FUNCS + abi.DIFF_FUNCS +
-             abi.SDF_FUNCS)
+             abi.SDF_FUNCS + abi.OCEAN_FUNCS)
     f = abi.bind(lib, "st_", lists)
     assert len(f) == len(lists)
 
