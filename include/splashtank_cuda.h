@@ -208,6 +208,17 @@ typedef struct st_live_layout {
   uint32_t words;       /* words in all */
 } st_live_layout;
 st_status st_flip_pack_live(st_flip* s, float vs, uint32_t* words, uint64_t cap_words, st_live_layout* layout);
+/* FlipSim.readDeep (src/flip/sim.js:408-421): the deep-water points of the last step as float4 (x, y, z, 4096 +
+ * speed), compacted; *n = 0 when the deep look does not apply. At most cap are written (ST_OVERFLOW when more). */
+st_status st_flip_read_deep_points(st_flip* s, float* out4, uint32_t cap, uint32_t* n);
+/* FlipSim.setSprayCap (src/flip/sim.js:326-334): room for n whitewater points (0 turns whitewater off); the pool starts
+ * empty, the slot counter keeps counting. The first pool also brings the air field (airAlloc). */
+st_status st_flip_set_spray_cap(st_flip* s, uint32_t n);
+/* FlipSim.recycle (src/gpu.js:393): when on (the default), FlipSim.add reuses slots in a ring once the cap is reached. */
+st_status st_flip_set_recycle(st_flip* s, int on);
+/* FlipSim.memBytes (src/flip/sim.js:492-495): device memory this handle holds, in bytes (its own count of what it
+ * allocated, not the reference's estimate). */
+st_status st_flip_mem_bytes(st_flip* s, uint64_t* bytes);
 /* FlipSim.setDeepLook (src/flip/sim.js:406): show the narrow band's deep water (fluid cells with no particles). */
 st_status st_flip_set_deep_look(st_flip* s, int on);
 /* readDeep + packDeep (src/flip/sim.js:408-421, src/gpu.js:512-524): the deep-water points of the last step for a

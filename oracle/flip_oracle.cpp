@@ -1350,6 +1350,22 @@ st_status oracle_flip_read_drips(void* h, float* out8, uint32_t cap, uint32_t* n
   return ST_OK;
 }
 int oracle_ocean_waves(const st_step_opts* o, double depth, float* w) { return (int)Oracle::oceanWaves(o, (double)o->g, depth, w); }
+st_status oracle_flip_set_recycle(void* h, int on) { ((Oracle*)h)->recycle = on != 0; return ST_OK; }
+// FlipSim.setSprayCap (sim.js:326-334): a new empty pool; sctl keeps counting. The first pool also brings the air field.
+st_status oracle_flip_set_spray_cap(void* h, uint32_t n) {
+  Oracle* s = (Oracle*)h;
+  if (n == s->sprayCap) return ST_OK;
+  s->sprayCap = n;
+  s->sPos.assign((size_t)std::max(n, 1u) * 4, 0.0f); s->sVel = s->sPos; s->sAux = s->sPos;
+  if (n && !s->airCells) {
+    int r = std::max(2, (int)std::ceil(std::cbrt((double)s->nx * s->ny * s->nz / 260000.0)));
+    s->airH = s->h * r;
+    s->aNx = (uint32_t)((s->nx + r - 1) / r + 1); s->aNy = (uint32_t)((s->ny + r - 1) / r + 1); s->aNz = (uint32_t)((s->nz + r - 1) / r + 1);
+    s->airCells = s->aNx * s->aNy * s->aNz;
+    s->air.assign((size_t)s->airCells * 4, 0.0f); s->air2 = s->air; s->airAcc.assign((size_t)s->airCells * 4, 0);
+  }
+  return ST_OK;
+}
 st_status oracle_flip_set_deep_look(void* h, int on) { ((Oracle*)h)->deepOn = on != 0; return ST_OK; }
 // one deep pass when the deep look applies (deep look on, narrow band and kept velocities on at the last step), as
 // float4 points; *n receives the count (0 when it does not apply)

@@ -116,6 +116,8 @@ FLIP_FUNCS = [
     ("flip_read_air", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
     ("flip_read_drips", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
     ("flip_set_deep_look", C.c_int, [C.c_void_p, C.c_int]),
+    ("flip_set_spray_cap", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("flip_set_recycle", C.c_int, [C.c_void_p, C.c_int]),
     ("flip_stats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     ("flip_read_grid", C.c_int, [C.c_void_p, C.POINTER(Grid)]),
     ("flip_get_dims", C.c_int, [C.c_void_p, C.POINTER(Dims)]),
@@ -151,6 +153,8 @@ class LiveLayout(C.Structure):
 
 CUDA_ONLY_FUNCS = [
     ("flip_pack_live", C.c_int, [C.c_void_p, C.c_float, u32p, C.c_uint64, C.POINTER(LiveLayout)]),
+    ("flip_read_deep_points", C.c_int, [C.c_void_p, f32p, C.c_uint32, u32p]),
+    ("flip_mem_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("flip_read_deep", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, C.c_uint32, u32p]),
     ("flip_read_spray_frame", C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_uint16), u32p, C.c_uint32, u32p, u32p]),
     ("flip_read_frame", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, u8p, C.c_uint32, u32p, C.POINTER(C.c_int32)]),

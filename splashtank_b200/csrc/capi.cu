@@ -31,9 +31,13 @@ void set_err(const char* what, cudaError_t e) {
     }                                             \
   } while (0)
 
+thread_local size_t g_alloc_bytes = 0;   // bytes dalloc handed out on this thread (a handle's create sums its own)
 template <class T>
 cudaError_t dalloc(T** p, size_t count) {
-  return cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+  const size_t b = std::max<size_t>(count, 1) * sizeof(T);
+  const cudaError_t e = cudaMalloc((void**)p, b);
+  if (e == cudaSuccess) g_alloc_bytes += b;
+  return e;
 }
 
 }  // namespace
@@ -121,6 +125,7 @@ struct st_flip {
   size_t liveWords = 0;
   uint8_t* framePart = nullptr;    // packed whitewater or deep-water points of a frame
   size_t framePartBytes = 0;
+  size_t createBytes = 0;          // device bytes allocated by create
   cudaEvent_t ev[16] = {};
   int cur = 0;   // part[cur] holds this step's storage order
   uint64_t launches = 0;   // kernels launched by steps since create
@@ -221,6 +226,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   st_status st = ST_OK;
   auto A = [&](cudaError_t ee, const char* what) { if (ee != cudaSuccess && st == ST_OK) { set_err(what, ee); st = ee == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR; } };
   A(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  g_alloc_bytes = 0;
   A(dalloc(&s->dCtl, 1), "ctl"); A(cudaMallocHost((void**)&s->hCtl, sizeof(Ctl)), "ctl host");
   for (int b = 0; b < 2; b++) { A(dalloc(&s->part[b], M), "particles"); A(dalloc(&s->ids[b], M), "ids"); A(dalloc(&s->cnt[b], C), "cnt"); }
   A(dalloc(&s->key, M), "key"); A(dalloc(&s->rank, M), "rank"); A(dalloc(&s->srcIdx, M), "srcIdx"); A(dalloc(&s->spid, M), "spid");
@@ -248,6 +254,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(cudaMallocHost((void**)&s->ring_h, sizeof(st_flip::Upload) * st_flip::RING), "upload ring"); A(dalloc(&s->dUp, 1), "upload");
   for (auto& ev : s->ring_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "ring event");
   if (st != ST_OK) { st_flip_destroy(s); return st; }
+  s->createBytes = g_alloc_bytes;
   // every tile starts in the state the reference's spare slot reads as
   cudaStream_t q = s->stream;
   A(cudaMemsetAsync(s->dCtl, 0, sizeof(Ctl), q), "memset");
@@ -771,6 +778,79 @@ static st_status deep_pass(st_flip* s, uint32_t* n) {
   CK(cudaGetLastError());
   s->deepPrev = h[0];
   *n = std::min(h[1], st_flip::DEEP_MAX);
+  return ST_OK;
+}
+
+st_status st_flip_read_deep_points(st_flip* s, float* out4, uint32_t cap, uint32_t* n) {
+  if (!s || !n) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  *n = 0;
+  if (!deep_ready(s)) return ST_OK;
+  uint32_t nd = 0;
+  st_status st = deep_pass(s, &nd);
+  if (st != ST_OK) return st;
+  *n = nd;
+  const uint32_t m = std::min(nd, cap);
+  if (out4 && m) {
+    CK(cudaMemcpyAsync(out4, s->deepBuf, (size_t)m * sizeof(float4), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  }
+  return m < nd ? ST_OVERFLOW : ST_OK;
+}
+
+st_status st_flip_set_recycle(st_flip* s, int on) {
+  if (!s) return ST_BAD_ARG;
+  s->recycle = on != 0;
+  return ST_OK;
+}
+
+st_status st_flip_set_spray_cap(st_flip* s, uint32_t n) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (n == s->sprayCap) return ST_OK;
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graphs(s);   // captured steps hold the old pool
+  float4 *p = nullptr, *v = nullptr;
+  cudaError_t e = dalloc(&p, std::max<size_t>(n, 1));
+  if (e == cudaSuccess) e = dalloc(&v, std::max<size_t>(n, 1));
+  if (e != cudaSuccess) {
+    if (p) cudaFree(p);
+    set_err("spray pool", e);
+    return e == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR;
+  }
+  CK(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * 16, s->stream));
+  CK(cudaMemsetAsync(v, 0, std::max<size_t>(n, 1) * 16, s->stream));
+  if (n && !s->airCells) {   // the air field comes with the first pool (airAlloc, src/flip/sim.js:343-350)
+    const double cells = (double)s->nx * (double)s->ny * (double)s->nz;
+    const int r = std::max(2, (int)std::ceil(std::cbrt(cells / 260000.0)));
+    const uint32_t ax = (uint32_t)((s->nx + r - 1) / r + 1), ay = (uint32_t)((s->ny + r - 1) / r + 1), az = (uint32_t)((s->nz + r - 1) / r + 1);
+    const uint32_t na = ax * ay * az;
+    CK(dalloc(&s->air, na)); CK(dalloc(&s->air2, na)); CK(dalloc(&s->airAcc, 4 * (size_t)na));
+    CK(cudaMemsetAsync(s->air, 0, (size_t)na * 16, s->stream));
+    CK(cudaMemsetAsync(s->air2, 0, (size_t)na * 16, s->stream));
+    s->airH = s->h * r; s->aNx = ax; s->aNy = ay; s->aNz = az; s->airCells = na;
+    s->createBytes += (size_t)na * 48;
+  }
+  s->createBytes += 32 * std::max<size_t>(n, 1);
+  s->createBytes -= 32 * std::max<size_t>(s->sprayCap, 1);
+  CK(cudaStreamSynchronize(s->stream));
+  cudaFree(s->sPos);
+  cudaFree(s->sVel);
+  s->sPos = p;
+  s->sVel = v;
+  s->sprayCap = n;   // the ring counter keeps counting, as the reference's sctl does
+  return ST_OK;
+}
+
+st_status st_flip_mem_bytes(st_flip* s, uint64_t* bytes) {
+  if (!s || !bytes) return ST_BAD_ARG;
+  uint64_t b = s->createBytes;
+  b += (uint64_t)s->sdfCap * 4 - 64;                                     // distance grids beyond the first 16 floats
+  b += s->frame ? (uint64_t)s->maxN * 8 + 16 : 0;
+  b += s->diag ? sizeof(DiagAcc) : 0;
+  b += s->deepBuf ? (uint64_t)st_flip::DEEP_MAX * sizeof(float4) : 0;
+  b += (uint64_t)s->viewScratchN * 4 + (uint64_t)s->liveWords * 4 + s->framePartBytes + (uint64_t)s->dripCap * 32;
+  *bytes = b;
   return ST_OK;
 }
 

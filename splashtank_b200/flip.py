@@ -382,6 +382,58 @@ class FlipSim:
         self._check(self.f["flip_read_spray"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.sprayCap, C.byref(n)), "readSpray")
         return dict(n=n.value, p=p[: n.value], v=v[: n.value])
 
+    def setSprayCap(self, n):
+        """FlipSim.setSprayCap (src/flip/sim.js:326-334): room for n whitewater points (0 turns whitewater off)."""
+        self.flushRun()
+        self._check(self.f["flip_set_spray_cap"](self._h, int(n)), "setSprayCap")
+        self.sprayCap = int(n)
+
+    @property
+    def recycle(self):
+        """FlipSim.recycle: add() reuses slots in a ring once the cap is reached (default on)."""
+        return getattr(self, "_recycle", True)
+
+    @recycle.setter
+    def recycle(self, on):
+        self._check(self.f["flip_set_recycle"](self._h, 1 if on else 0), "recycle")
+        self._recycle = bool(on)
+
+    def prime(self, o=None):
+        """FlipSim.prime (src/flip/sim.js:170-178) sizes the reference's block pool for the starting water. Every tile
+        here has a fixed home in device memory, so there is no pool to size: nothing to do."""
+        return None
+
+    def memBytes(self):
+        """FlipSim.memBytes (src/flip/sim.js:492-495): device memory this simulator holds."""
+        b = C.c_uint64()
+        self._check(self.f["flip_mem_bytes"](self._h, C.byref(b)), "memBytes")
+        return b.value
+
+    def readDeep(self):
+        """FlipSim.readDeep (src/flip/sim.js:408-421): dict n, p ((n, 4) float32: x, y, z, 4096 + speed) of the deep
+        water of the last step, or None when the deep look does not apply."""
+        self.flushRun()
+        out = np.zeros((200000, 4), np.float32)
+        n = C.c_uint32()
+        self._check(self.f["flip_read_deep_points"](self._h, out.ctypes.data_as(abi.f32p), len(out), C.byref(n)), "readDeep")
+        return dict(n=n.value, p=out[:n.value]) if n.value else None
+
+    def pump(self, vs=1.0):
+        """FlipSim.pump + unpackLive (src/flip/sim.js:506-537): the live view packed on the device, read back and made
+        into this.outFrame (n, pos, spd, fm, b, and sp / dp when present); gen counts the frames made."""
+        words, L = self.pack_live(vs)
+        u8, u16 = words.view(np.uint8), words.view(np.uint16)
+        nW, nS, nD = L["n_water"], min(int(words[0]), L["n_spray"]), min(int(words[1]), L["n_deep"])
+        fr = dict(n=nW, pos=u16[L["o_wp"] * 2: L["o_wp"] * 2 + nW * 3].reshape(nW, 3).copy(), spd=u8[L["o_ws"] * 4: L["o_ws"] * 4 + nW].copy(),
+                  fm=u8[L["o_wf"] * 4: L["o_wf"] * 4 + nW].copy(), b=dict(self.b))
+        if nS:
+            fr["sp"] = dict(n=nS, pos=u16[L["o_sp"] * 2: L["o_sp"] * 2 + nS * 3].reshape(nS, 3).copy(), pk=words[L["o_sk"]: L["o_sk"] + nS].copy(), alive=nS)
+        if nD:
+            fr["dp"] = dict(n=nD, pos=u16[L["o_dp"] * 2: L["o_dp"] * 2 + nD * 3].reshape(nD, 3).copy(), spd=u8[L["o_ds"] * 4: L["o_ds"] * 4 + nD].copy())
+        self.outFrame = fr
+        self.gen = getattr(self, "gen", 0) + 1
+        return fr
+
     def setDeepLook(self, on):
         """FlipSim.setDeepLook (src/flip/sim.js:406): show the narrow band's deep water as points."""
         self._check(self.f["flip_set_deep_look"](self._h, 1 if on else 0), "setDeepLook")

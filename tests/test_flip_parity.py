@@ -249,3 +249,30 @@ def test_empty_and_bad_arguments():
     d.d = -1.0
     h = C.c_void_p()
     assert f["flip_create"](C.byref(d), C.byref(h)) == abi.ST_BAD_ARG
+
+
+def test_spray_pool_resized_mid_run_and_ring_recycling():
+    """setSprayCap between steps (a smaller pool, then none, then one again: the slot counter keeps counting, the pool
+    starts empty, the first pool brings the air field) and recycle off (add takes no more once the cap is reached)."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    sc = scenes.dam_break(32)
+    sc["vel"] = np.tile(np.array([[2.5, 0.5, 0.0]], np.float32), (len(sc["pos"]), 1))
+    opts = dict(sc["opts"], spr=dict(scenes.APP_SPRAY, min=0.5), air=dict(on=True, couple=3.0, decay=0.6), gust=1.0)
+    g, o = make_pair(sc, spray_cap=0)
+    for s in (g, o):
+        p, v, i = s.save_state()
+        s.load_state(p, v, i, t=0.6, seed=0)
+    for cap, steps in ((20000, 10), (3000, 10), (0, 3), (8000, 10)):
+        for s in (g, o):
+            s.setSprayCap(cap)
+        for _ in range(steps):
+            for s in (g, o):
+                s.step(sc["dt"], opts)
+        assert_same_state(g, o, spray=cap > 0)
+    assert g.readStats()["spray_used"] > 8000
+    for s in (g, o):
+        s.recycle = False
+        s.setCap(s.N)
+    extra = np.zeros((5, 3), np.float32)
+    assert g.add_many(extra) == o.add_many(extra) == 0

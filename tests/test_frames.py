@@ -244,3 +244,31 @@ def test_device_live_view_with_whitewater_matches_the_oracle():
     want = pack_live(L, pos, 1, sd["p"], sd["v"], used, 30000, 3.0, None, box, 1.0)
     assert words[0] == want[0] > 1000
     assert np.array_equal(words, want)
+
+
+@pytest.mark.gpu
+def test_read_deep_points_pump_and_mem_bytes():
+    """readDeep's raw points equal the oracle's deep pass; pump() unpacks the packed live view into outFrame; memBytes
+    counts what the handle holds, including the buffers its first frame and live view allocate."""
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    w = scenes.WaveTank(48, spray_cap=20000, band=3.0)
+    g, o = w.make(FlipSim), w.make(OracleFlipSim, threads=8)
+    m0 = g.memBytes()
+    assert m0 > 48 ** 3 * 40
+    for s in (g, o):
+        s.setDeepLook(True)
+    runs, t = [SceneRunner(s) for s in (g, o)], 0.0
+    for _ in range(4):
+        t += w.dt
+        for r in runs:
+            r.step(w.dt, w.states(t), w.opts)
+    d = g.readDeep()
+    want = o.deep_points()
+    assert d["n"] == len(want) > 1000 and np.array_equal(d["p"], want)
+    fr = g.pump(1.0)
+    assert g.gen == 1 and fr["n"] == g.N and fr["dp"]["n"] > 1000 and fr["pos"].shape == (g.N, 3)
+    assert g.memBytes() > m0
+    g.read_frame()
+    assert g.memBytes() >= m0 + g.MAXN * 8
