@@ -304,7 +304,9 @@ def run_pressure(a):
             dist.barrier()
         torch.cuda.synchronize()
 
-    ro = dict(tol=a.tol, omega=a.omega, inner_sweeps=a.inner, max_sweeps=200000)
+    # every solve checks its residual on the same schedule: blocks sized from the last block's reduction per iteration
+    # (at most a.inner iterations), so that no solver runs up to a block past the tolerance
+    ro = dict(tol=a.tol, omega=a.omega, inner_sweeps=a.inner, max_sweeps=200000, predict=True)
     for _ in range(a.warmup):
         s.solve(REFINE, **ro)
     clocks = Clocks(local)
@@ -321,15 +323,18 @@ def run_pressure(a):
     r_ref = res[-1]
     x_ref32 = s.read()
     # plain FP32 SOR to the same tolerance (residual checked as often as the refinement checks it), then FP64 SOR
-    r32 = s.solve(SOR32, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000))
+    r32 = s.solve(SOR32, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000), predict=True)
     x32 = s.read()
-    r64 = s.solve(SOR64, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000))
+    r64 = s.solve(SOR64, tol=a.tol, omega=a.omega, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000), predict=True)
     x64 = s.read()
+    # the same two with fixed blocks of a.inner iterations between checks
+    fixed = {k: s.solve(m, tol=a.tol, omega=a.omega, inner_sweeps=a.inner, check_every=a.inner, max_sweeps=max(4 * r_ref["sweeps"], 2000))
+             for k, m in (("refine", REFINE), ("fp32_sor", SOR32))}
     # a tighter target: FP32 SOR stops improving at its rounding floor, the refinement keeps going at FP32 sweep cost
     t9 = 1e-9
-    r9 = s.solve(REFINE, tol=t9, omega=a.omega, inner_sweeps=a.inner, max_sweeps=20000)
-    r9_32 = s.solve(SOR32, tol=t9, omega=a.omega, check_every=a.inner, max_sweeps=max(2 * r9["sweeps"], 2000))
-    r9_64 = s.solve(SOR64, tol=t9, omega=a.omega, check_every=a.inner, max_sweeps=max(2 * r9["sweeps"], 2000))
+    r9 = s.solve(REFINE, tol=t9, omega=a.omega, inner_sweeps=a.inner, max_sweeps=20000, predict=True)
+    r9_32 = s.solve(SOR32, tol=t9, omega=a.omega, check_every=a.inner, max_sweeps=max(2 * r9["sweeps"], 2000), predict=True)
+    r9_64 = s.solve(SOR64, tol=t9, omega=a.omega, check_every=a.inner, max_sweeps=max(2 * r9["sweeps"], 2000), predict=True)
     rgold = s.solve(SOR64, tol=1e-11, omega=a.omega, check_every=50, max_sweeps=400000)
     gold = s.read()
     gn, gmax = float(np.linalg.norm(gold)), float(np.abs(gold).max())
@@ -368,6 +373,9 @@ def run_pressure(a):
                 "fp64_reference": {"method": "FP64 SOR to 1e-11", "sweeps": rgold["sweeps"], "rel_residual": rgold["rel_residual"], "ms": rgold["ms"]},
                 "tol_1e-9": {k: {"ms": r["ms"], "sweeps": r["sweeps"], "rel_residual": r["rel_residual"], "converged": r["converged"]}
                              for k, r in (("refine", r9), ("fp32_sor", r9_32), ("fp64_sor", r9_64))},
+                "schedule": "checks after blocks sized from the last block's reduction per iteration (8 to %d iterations)" % a.inner,
+                "fixed_blocks": {k: {"ms": r["ms"], "sweeps": r["sweeps"], "refinements": r["refinements"], "rel_residual": r["rel_residual"]}
+                                 for k, r in fixed.items()},
                 "clocks": clk, "roofline": rl,
                 "e2e": {"value": e_ms, "unit": "ms", "h2d_bytes_per_step": int(ty.nbytes + rhs.nbytes), "d2h_bytes_per_step": int(gold.nbytes),
                         "note": "wall clock of set (host builds the tile index) + solve + read through the C ABI"}}

@@ -356,7 +356,11 @@ typedef struct st_poisson_opts {
   int32_t max_sweeps;   /* red + black iterations, all refinements together */
   int32_t inner_sweeps; /* iterations per refinement (mode 1) */
   int32_t check_every;  /* iterations between residual checks (modes 0 and 2) */
+  int32_t schedule;     /* ST_SCHEDULE_*: blocks of check_every / inner_sweeps iterations between checks, or blocks sized
+                           from the last block's measured reduction per iteration to end at the tolerance (at least 8
+                           iterations, at most check_every / inner_sweeps); the same rule for every mode */
 } st_poisson_opts;
+enum { ST_SCHEDULE_FIXED = 0, ST_SCHEDULE_PREDICT = 1 };
 typedef struct st_poisson_result {
   double rel_residual;
   int32_t sweeps;

@@ -88,7 +88,7 @@ class PoissonDesc(C.Structure):
 
 class PoissonOpts(C.Structure):
     _fields_ = [("size", C.c_uint32), ("mode", C.c_int32), ("tol", C.c_double), ("omega", C.c_float), ("max_sweeps", C.c_int32),
-                ("inner_sweeps", C.c_int32), ("check_every", C.c_int32)]
+                ("inner_sweeps", C.c_int32), ("check_every", C.c_int32), ("schedule", C.c_int32)]
 
 
 class PoissonResult(C.Structure):

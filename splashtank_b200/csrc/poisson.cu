@@ -124,6 +124,41 @@ __global__ void __launch_bounds__(512) k_ps_resid(uint32_t nT, const uint32_t* _
     __syncthreads();
   }
 }
+// One refinement step in one pass: the corrected solution x + e (xo), its FP64 residual (as k_ps_resid<double> computes
+// it from the corrected values: the same sums in the same order, the same per-tile tree), and the next inner
+// right-hand side rhs32 = (float) r. The corrected solution goes to a second buffer, since neighbours still read x and
+// e; the caller swaps the two and clears e.
+__global__ void __launch_bounds__(512) k_ps_refine(uint32_t nT, const uint32_t* __restrict__ nbs, const uint16_t* __restrict__ info,
+                                                   const double* __restrict__ x, const float* __restrict__ e, const double* __restrict__ b,
+                                                   double* __restrict__ xo, float* __restrict__ rhs32, double* __restrict__ tileR2) {
+  __shared__ double sr[512];
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
+    const uint32_t l = threadIdx.x, c = a * 512u + splitIdx(l);
+    const uint32_t in = info[c];
+    const double xc = x[c] + (double)e[c];
+    double rv = 0.0;
+    if (in & 0x8000u) {
+      const uint32_t nns = (in >> 8) & 7u;
+      double s = 0.0;
+      for (int q = 0; q < 6; q++)
+        if (in & (1u << q)) {
+          const uint32_t nb = nbIdx(nbs, a, l, q);
+          s += x[nb] + (double)e[nb];
+        }
+      rv = b[c] - ((double)nns * xc - s);
+    }
+    xo[c] = xc;
+    rhs32[c] = (float)rv;
+    sr[l] = rv * rv;
+    __syncthreads();
+    for (int w = 256; w > 0; w >>= 1) {
+      if ((int)l < w) sr[l] += sr[l + w];
+      __syncthreads();
+    }
+    if (l == 0) tileR2[a] = sr[0];
+    __syncthreads();
+  }
+}
 // sum of per-tile partials in tile order (one CTA, fixed tree): out[0] = sum tileR2, out[1] = sum tileB2
 __global__ void __launch_bounds__(1024) k_ps_norms(const double* __restrict__ tileR2, const double* __restrict__ tileB2, uint32_t nT, double* out) {
   __shared__ double s1[1024], s2[1024];
@@ -139,15 +174,12 @@ __global__ void __launch_bounds__(1024) k_ps_norms(const double* __restrict__ ti
   }
   if (threadIdx.x == 0) { out[0] = s1[0]; out[1] = s2[0]; }
 }
-// refinement helpers over all stored cells: inner right-hand side and zero start; correction x += e; FP32 -> FP64 copy
+// over all stored cells: the first inner right-hand side with a zero start; FP32 -> FP64 copy
 __global__ void k_ps_inner(size_t n, const double* __restrict__ r, float* __restrict__ rhs32, float* __restrict__ e) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     rhs32[i] = (float)r[i];
     e[i] = 0.0f;
   }
-}
-__global__ void k_ps_correct(size_t n, const float* __restrict__ e, double* __restrict__ x) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = x[i] + (double)e[i];
 }
 __global__ void k_ps_copy(size_t n, const float* __restrict__ p32, double* __restrict__ x) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = (double)p32[i];
@@ -168,6 +200,7 @@ struct st_poisson {
   uint16_t* info = nullptr;
   float *p32 = nullptr, *rhs32 = nullptr;
   double *x64 = nullptr, *b64 = nullptr, *r64 = nullptr, *tileR2 = nullptr, *tileB2 = nullptr, *norms = nullptr;
+  double* x64b = nullptr;   // the refinement's second solution buffer
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   size_t cells() const { return (size_t)nT * 512; }
 };
@@ -182,9 +215,9 @@ struct st_poisson {
   } while (0)
 
 static void poisson_free(st_poisson* s) {
-  void* ptrs[] = {s->nbs, s->info, s->p32, s->rhs32, s->x64, s->b64, s->r64, s->tileR2, s->tileB2};
+  void* ptrs[] = {s->nbs, s->info, s->p32, s->rhs32, s->x64, s->x64b, s->b64, s->r64, s->tileR2, s->tileB2};
   for (void* p : ptrs) if (p) cudaFree(p);
-  s->nbs = nullptr; s->info = nullptr; s->p32 = s->rhs32 = nullptr; s->x64 = s->b64 = s->r64 = s->tileR2 = s->tileB2 = nullptr;
+  s->nbs = nullptr; s->info = nullptr; s->p32 = s->rhs32 = nullptr; s->x64 = s->x64b = s->b64 = s->r64 = s->tileR2 = s->tileB2 = nullptr;
   s->capT = 0;
 }
 
@@ -285,6 +318,7 @@ st_status st_poisson_set(st_poisson* s, const uint8_t* type, const double* rhs) 
     SK(cudaMalloc((void**)&s->p32, m * 4));
     SK(cudaMalloc((void**)&s->rhs32, m * 4));
     SK(cudaMalloc((void**)&s->x64, m * 8));
+    SK(cudaMalloc((void**)&s->x64b, m * 8));
     SK(cudaMalloc((void**)&s->b64, m * 8));
     SK(cudaMalloc((void**)&s->r64, m * 8));
     SK(cudaMalloc((void**)&s->tileR2, (size_t)std::max(nT, 1u) * 8));
@@ -347,43 +381,61 @@ st_status st_poisson_solve(st_poisson* s, const st_poisson_opts* o, st_poisson_r
   SK(cudaEventRecord(s->e0, q));
   int it = 0, ref = 0;
   double rel = 1.0;
+  // iterations before the next residual check: fixed blocks, or (ST_SCHEDULE_PREDICT) the count the last block's
+  // reduction per iteration says reaches the tolerance, with 2% and one iteration to spare, between 8 and the block
+  double lastRel = 1.0;
+  int lastK = 0;
+  auto nextBlock = [&](int block) {
+    if (o->schedule != ST_SCHEDULE_PREDICT || lastK == 0 || !(rel < lastRel) || !(rel > 0.0)) return block;
+    const double rho = std::pow(rel / lastRel, 1.0 / lastK);
+    if (!(rho > 0.0 && rho < 1.0)) return block;
+    const double need = std::log(o->tol / rel) / std::log(rho);
+    return std::max(std::min(8, block), std::min(block, (int)std::ceil(need * 1.02) + 1));
+  };
+  auto checked = [&](double before, int k) { lastRel = before; lastK = k; };
   if (o->mode == 0) {
     k_ps_inner<<<gridE, 256, 0, q>>>(n, s->b64, s->rhs32, s->p32);
     while (it < maxIt) {
-      const int k = std::min(check, maxIt - it);
+      const int k = std::min(nextBlock(check), maxIt - it);
       sweeps32(s, grid, om, k);
       it += k;
       k_ps_resid<float><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->p32, s->b64, s->r64, s->tileR2, nullptr);
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
+      checked(rel, k);
       rel = std::sqrt(r2) / bn;
       if (rel <= o->tol) break;
     }
     k_ps_copy<<<gridE, 256, 0, q>>>(n, s->p32, s->x64);
   } else if (o->mode == 1) {
     const int inner = std::max(1, o->inner_sweeps);
+    k_ps_inner<<<gridE, 256, 0, q>>>(n, s->b64, s->rhs32, s->p32);   // x = 0: the first correction solves A e = b
     while (it < maxIt) {
-      k_ps_inner<<<gridE, 256, 0, q>>>(n, s->r64, s->rhs32, s->p32);
-      const int k = std::min(inner, maxIt - it);
+      const int k = std::min(nextBlock(inner), maxIt - it);
       sweeps32(s, grid, om, k);
       it += k;
-      k_ps_correct<<<gridE, 256, 0, q>>>(n, s->p32, s->x64);
-      k_ps_resid<double><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
+      k_ps_refine<<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->p32, s->b64, s->x64b, s->rhs32, s->tileR2);
+      std::swap(s->x64, s->x64b);
+      SK(cudaMemsetAsync(s->p32, 0, n * 4, q));
       ref++;
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
+      checked(rel, k);
       rel = std::sqrt(r2) / bn;
       if (rel <= o->tol) break;
     }
   } else if (o->mode == 2) {
     while (it < maxIt) {
-      for (int k = 0; k < check && it < maxIt; k++, it++) {
+      const int blk = nextBlock(check);
+      int k = 0;
+      for (; k < blk && it < maxIt; k++, it++) {
         k_ps_sor<double><<<grid, 256, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, (double)om, 0u);
         k_ps_sor<double><<<grid, 256, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, (double)om, 1u);
       }
       k_ps_resid<double><<<grid4, 512, 0, q>>>(s->nT, s->nbs, s->info, s->x64, s->b64, s->r64, s->tileR2, nullptr);
       st = norms(s, false, &r2, nullptr);
       if (st != ST_OK) return st;
+      checked(rel, k);
       rel = std::sqrt(r2) / bn;
       if (rel <= o->tol) break;
     }

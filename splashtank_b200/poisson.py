@@ -46,10 +46,13 @@ class PoissonSolver:
         self.n_tiles = int(occ.sum()) if occ is not None else None
         self.n_fluid = int((t == 1).sum())
 
-    def solve(self, mode, tol=1e-6, omega=1.9, max_sweeps=100000, inner_sweeps=50, check_every=10):
+    def solve(self, mode, tol=1e-6, omega=1.9, max_sweeps=100000, inner_sweeps=50, check_every=10, predict=False):
+        """predict: size each block of iterations between residual checks from the last block's reduction (the same
+        rule for every mode), instead of fixed blocks."""
         o = abi.PoissonOpts()
         o.size = C.sizeof(abi.PoissonOpts)
         o.mode, o.tol, o.omega, o.max_sweeps, o.inner_sweeps, o.check_every = int(mode), float(tol), float(omega), int(max_sweeps), int(inner_sweeps), int(check_every)
+        o.schedule = 1 if predict else 0
         r = abi.PoissonResult()
         self._check(self.f["poisson_solve"](self._h, C.byref(o), C.byref(r)), "solve")
         return dict(rel_residual=r.rel_residual, sweeps=r.sweeps, refinements=r.refinements, converged=bool(r.converged), ms=r.ms)

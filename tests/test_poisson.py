@@ -64,3 +64,24 @@ def test_refinement_reaches_1e6_and_matches_fp64():
     assert r64["converged"] and np.linalg.norm(x64 - ref) / np.linalg.norm(ref) < 1e-8
     r32 = g.solve(SOR32, tol=1e-6, omega=1.9, check_every=10, max_sweeps=4000)
     assert r32["rel_residual"] < 1e-3   # FP32 SOR gets close; whether it reaches 1e-6 depends on rounding
+
+
+@pytest.mark.gpu
+def test_predicted_check_schedule():
+    """Checks after blocks sized from the last block's reduction per iteration: every mode still stops at the tolerance
+    (checked in FP64 against the oracle's residual), and no later than with fixed blocks of the same maximum."""
+    from oracle.oracle import OraclePoisson
+    from splashtank_b200.poisson import REFINE, SOR32, SOR64, PoissonSolver
+    n = 64
+    ty, b = scenes.splash_blobs(n, seed=9)
+    g = PoissonSolver((n, n, n))
+    g.set(ty, b)
+    o = OraclePoisson((n, n, n), threads=8)
+    o.set(ty, b)
+    for mode in (REFINE, SOR64, SOR32):
+        kw = dict(tol=1e-6, omega=1.9, inner_sweeps=50, check_every=50, max_sweeps=20000)
+        fixed, pred = g.solve(mode, **kw), g.solve(mode, predict=True, **kw)
+        x = g.read()
+        assert pred["converged"] and pred["rel_residual"] <= 1e-6, (mode, pred)
+        assert abs(o.rel_residual(x) - pred["rel_residual"]) <= 1e-9 * pred["rel_residual"]
+        assert pred["sweeps"] <= fixed["sweeps"], (mode, pred["sweeps"], fixed["sweeps"])
