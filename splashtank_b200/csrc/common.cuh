@@ -252,6 +252,22 @@ __device__ __forceinline__ V3 velGVec(const FlipParams& P, const float* __restri
   return v3(velGAxis(P, velG, nc, x, 0), velGAxis(P, velG, nc, x, 1), velGAxis(P, velG, nc, x, 2));
 }
 
+// ---- value noise (wgsl-solver.js:198-207): the gusts of g2p and of the whitewater step ----
+__device__ __forceinline__ float hsh3(V3 p) {
+  V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f);
+  q = q - vfloor(q);
+  q = q * 17.0f;
+  const float r = q.x * q.y * q.z * (q.x + q.y + q.z);
+  return r - floorf(r);
+}
+static __device__ float vnz(V3 x) {
+  const V3 i = vfloor(x), fr = x - vfloor(x);
+  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
+  const float a = mixf(mixf(hsh3(i), hsh3(i + v3(1, 0, 0)), u.x), mixf(hsh3(i + v3(0, 1, 0)), hsh3(i + v3(1, 1, 0)), u.x), u.y);
+  const float b = mixf(mixf(hsh3(i + v3(0, 0, 1)), hsh3(i + v3(1, 0, 1)), u.x), mixf(hsh3(i + v3(0, 1, 1)), hsh3(i + v3(1, 1, 1)), u.x), u.y);
+  return mixf(a, b, u.z);
+}
+
 // ---- ocean (src/flip/wgsl-core.js:201-226): a sum of linear (Airy) waves ----
 // Out of line: inlined, the wave loops raise the register count of the kernels that call them.
 static __device__ __noinline__ float oceanEta(const FlipParams& P, const float4* __restrict__ W, float x, float z) {
@@ -422,6 +438,17 @@ __device__ __forceinline__ uint32_t blockExclusive(uint32_t v, uint32_t* smem, u
   if (total) *total = smem[32];
   __syncthreads();
   return r;
+}
+// exclusive scan of arr[0, n) in place by one CTA (contiguous chunks per thread), arr[n] and *total (when given) = sum
+__device__ __forceinline__ void scanOne(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
+  const uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
+  const uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
+  uint32_t s = 0;
+  for (uint32_t x = beg; x < end; x++) s += arr[x];
+  uint32_t tot;
+  uint32_t run = blockExclusive(s, sm, &tot);
+  for (uint32_t x = beg; x < end; x++) { const uint32_t v = arr[x]; arr[x] = run; run += v; }
+  if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
 }
 
 }  // namespace st

@@ -129,25 +129,15 @@ __global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
 }
 
 // ---- refill: nbDead (wgsl-narrowband.js:106-110), nbDeficit (:112-130), nbSpawn (:134-148); nbKill is in g2p ----
-__device__ void scanOneX(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
-  uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
-  uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
-  uint32_t s = 0;
-  for (uint32_t x = beg; x < end; x++) s += arr[x];
-  uint32_t tot;
-  uint32_t run = blockExclusive(s, sm, &tot);
-  for (uint32_t x = beg; x < end; x++) { uint32_t v = arr[x]; arr[x] = run; run += v; }
-  if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
-}
 // which: 0 particles killed per tile, 1 deficit (cells and need per tile), 2 whitewater points per tile
 __global__ void __launch_bounds__(1024) k_scan_x(Bufs B, int which) {
   __shared__ uint32_t sm[33];
   const uint32_t nA = B.ctl->nActive;
-  if (which == 0) scanOneX(B.tileDead, nA, &B.ctl->nKilled, sm);
+  if (which == 0) scanOne(B.tileDead, nA, &B.ctl->nKilled, sm);
   else if (which == 1) {
-    if (blockIdx.x == 0) scanOneX(B.tileAux, nA, &B.ctl->defCount, sm);
-    else scanOneX(B.tileAux2, nA, &B.ctl->defNeed, sm);
-  } else scanOneX(B.tileEmit, nA, &B.ctl->emitTried, sm);
+    if (blockIdx.x == 0) scanOne(B.tileAux, nA, &B.ctl->defCount, sm);
+    else scanOne(B.tileAux2, nA, &B.ctl->defNeed, sm);
+  } else scanOne(B.tileEmit, nA, &B.ctl->emitTried, sm);
 }
 // the dead slots, in ascending storage index: this step's kills inside the tiles' segments (listed here), then the slots
 // that were already dead when the step sorted them ([nLive, N), no list needed)
@@ -252,20 +242,6 @@ __device__ __forceinline__ float wetAt(const FlipParams& P, const Bufs& B, V3 p)
     if (w > 0.0f) s += w * wetCell(P, B, i0 + dx, j0 + dy, k0 + dz);
   }
   return s;
-}
-__device__ __forceinline__ float hsh3X(V3 p) {
-  V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f);
-  q = q - vfloor(q);
-  q = q * 17.0f;
-  const float r = q.x * q.y * q.z * (q.x + q.y + q.z);
-  return r - floorf(r);
-}
-__device__ __forceinline__ float vnzX(V3 x) {
-  const V3 i = vfloor(x), fr = x - vfloor(x);
-  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
-  const float a = mixf(mixf(hsh3X(i), hsh3X(i + v3(1, 0, 0)), u.x), mixf(hsh3X(i + v3(0, 1, 0)), hsh3X(i + v3(1, 1, 0)), u.x), u.y);
-  const float b = mixf(mixf(hsh3X(i + v3(0, 0, 1)), hsh3X(i + v3(1, 0, 1)), u.x), mixf(hsh3X(i + v3(0, 1, 1)), hsh3X(i + v3(1, 1, 1)), u.x), u.y);
-  return mixf(a, b, u.z);
 }
 // ---- air field (wgsl-whitewater.js:24-89): a coarse grid of air velocity at cell centres (cells P.airH wide from the
 // box's low corner) that water near the surface and flying spray drag along; spray and mist drift with it ----
@@ -448,7 +424,7 @@ __global__ void __launch_bounds__(256) k_ww_step(Bufs B) {
       if (P.q7 > 0.0f) {
         const V3 gp = p * 0.55f * P.vs;
         const float tt = P.q8 * 0.6f;
-        gust = v3(vnzX(gp + v3(tt, 0.0f, 0.0f)), vnzX(gp + v3(17.3f, tt, 4.1f)), vnzX(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
+        gust = v3(vnz(gp + v3(tt, 0.0f, 0.0f)), vnz(gp + v3(17.3f, tt, 4.1f)), vnz(gp + v3(5.7f, 9.2f, tt))) * 2.0f - v3(1.0f, 1.0f, 1.0f);
       }
       const V3 base = P.airOn != 0u ? airAt(P, B.air, p) : v3(P.q1, P.q2, P.q3);
       const V3 airv = base + gust * P.q7 * (mist ? 2.5f : 1.0f);

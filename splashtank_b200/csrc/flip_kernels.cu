@@ -182,16 +182,6 @@ __global__ void __launch_bounds__(512) k_tile_prep(Bufs B) {
 
 // Exclusive scan of up to a few hundred thousand counts by one CTA; block 0 scans the per-tile particle counts
 // (total = live particles), block 1 the per-block dead counts. arr[n] receives the total.
-__device__ void scanOne(uint32_t* arr, uint32_t n, uint32_t* total, uint32_t* sm) {
-  uint32_t chunk = (n + blockDim.x - 1) / blockDim.x;
-  uint32_t beg = min(threadIdx.x * chunk, n), end = min(beg + chunk, n);
-  uint32_t s = 0;
-  for (uint32_t x = beg; x < end; x++) s += arr[x];
-  uint32_t tot;
-  uint32_t run = blockExclusive(s, sm, &tot);
-  for (uint32_t x = beg; x < end; x++) { uint32_t v = arr[x]; arr[x] = run; run += v; }
-  if (threadIdx.x == 0) { arr[n] = tot; if (total) *total = tot; }
-}
 __global__ void __launch_bounds__(1024) k_scan_counts(Bufs B) {
   __shared__ uint32_t sm[33];
   if (blockIdx.x == 0) scanOne(B.tileCnt, B.ctl->nActive, &B.ctl->nLive, sm);
@@ -649,20 +639,6 @@ __device__ __forceinline__ V3 collideP(const FlipParams& P, const Bufs& B, V3 pi
   const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
   const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
   return vclamp(p, lo, hi);
-}
-__device__ __forceinline__ float hsh3(V3 p) {
-  V3 q = p * 0.3183099f + v3(0.1f, 0.2f, 0.3f);
-  q = q - vfloor(q);
-  q = q * 17.0f;
-  const float r = q.x * q.y * q.z * (q.x + q.y + q.z);
-  return r - floorf(r);
-}
-__device__ float vnz(V3 x) {   // value noise (wgsl-solver.js:202-207)
-  const V3 i = vfloor(x), fr = x - vfloor(x);
-  const V3 u = fr * fr * (v3(3.0f, 3.0f, 3.0f) - fr * 2.0f);
-  const float a = mixf(mixf(hsh3(i), hsh3(i + v3(1, 0, 0)), u.x), mixf(hsh3(i + v3(0, 1, 0)), hsh3(i + v3(1, 1, 0)), u.x), u.y);
-  const float b = mixf(mixf(hsh3(i + v3(0, 0, 1)), hsh3(i + v3(1, 0, 1)), u.x), mixf(hsh3(i + v3(0, 1, 1)), hsh3(i + v3(1, 1, 1)), u.x), u.y);
-  return mixf(a, b, u.z);
 }
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
