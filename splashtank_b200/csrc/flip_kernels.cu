@@ -254,12 +254,17 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
     if (staged) for (uint32_t u = s0 + threadIdx.x; u < s1; u += P2G_T) sid[u - s0] = B.spid[u];
     for (int r = threadIdx.x; r < 512; r += P2G_T) { soff[r] = B.cellOff[t * 512u + r]; scnt[r] = B.cnt[t * 512u + r]; }
     __syncthreads();
+    // lanes of a warp take particles 8 apart, so they fall in different cells and their shared atomics rarely collide;
+    // each thread gathers its next particle while it splats the current one
+    const uint32_t lanePos = (uint32_t)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
+    Part qNext;
+    if (s0 + lanePos < s1) qNext = B.pb[B.srcIdx[s0 + lanePos]];
     for (uint32_t base = s0; base < s1; base += P2G_T) {
-      // lanes of a warp take particles 8 apart, so they fall in different cells and their shared atomics rarely collide
-      const uint32_t s = base + (uint32_t)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
+      const uint32_t s = base + lanePos;
+      const Part q = qNext;
+      if (s + P2G_T < s1) qNext = B.pb[B.srcIdx[s + P2G_T]];
       if (s >= s1) continue;
-      const uint32_t src = B.srcIdx[s], myid = staged ? sid[s - s0] : B.spid[s];
-      const Part q = B.pb[src];
+      const uint32_t myid = staged ? sid[s - s0] : B.spid[s];
       const V3 p = xyz(q.p), v = xyz(q.v);
       int ci, cj, ck;
       particleCell(P, p, ci, cj, ck);
