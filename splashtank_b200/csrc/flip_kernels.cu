@@ -24,11 +24,15 @@ __device__ __forceinline__ void markAround(const FlipParams& P, uint32_t* __rest
 // One pass over the particles in storage order: mark tiles near live particles, count particles per cell with
 // warp-aggregated atomics (the returned base gives each particle a rank in its cell), count dead slots per block,
 // and the fastest speed (ctl[6], wgsl-solver.js:24).
-// A CTA takes CM_U consecutive blocks of PBLK particles and keeps all of them in flight (loads, then the atomics, then
-// the tile marks), so the latency of the dependent steps overlaps across blocks; dead slots are still counted per block.
-constexpr int CM_U = 4;
-__global__ void __launch_bounds__(PBLK, 1) k_count_mark(Bufs B) {
+// A CTA of CM_T threads takes one block of PBLK particles, CM_U per thread (a warp's lanes on consecutive particles),
+// and keeps all of them in flight (loads, then the atomics, then the tile marks); several CTAs per SM overlap the
+// dependent steps and barriers of one another.
+constexpr int CM_T = 256, CM_U = PBLK / CM_T;
+static_assert(CM_U == 4, "k_scatter packs the dead counts of four slices into two scans");
+__global__ void __launch_bounds__(CM_T, 4) k_count_mark(Bufs B) {
   __shared__ FlipParams P;
+  __shared__ float wmax[CM_T / 32];
+  __shared__ uint32_t wdead[CM_T / 32];
   loadParams(P, B.P);
   const int lane = threadIdx.x & 31;
   Part q[CM_U];
@@ -38,7 +42,7 @@ __global__ void __launch_bounds__(PBLK, 1) k_count_mark(Bufs B) {
   float sp = 0.0f;
 #pragma unroll
   for (int u = 0; u < CM_U; u++) {
-    idx[u] = (blockIdx.x * CM_U + u) * PBLK + threadIdx.x;
+    idx[u] = blockIdx.x * PBLK + u * CM_T + threadIdx.x;
     if (idx[u] < P.n) q[u] = B.pb[idx[u]];
   }
 #pragma unroll
@@ -72,21 +76,24 @@ __global__ void __launch_bounds__(PBLK, 1) k_count_mark(Bufs B) {
     const uint32_t b = __shfl_sync(0xffffffffu, base[u], __ffs(peers[u]) - 1);
     if (live[u]) B.rank[idx[u]] = b + __popc(peers[u] & ((1u << lane) - 1u));
   }
-  // fastest speed: lengths are non-negative, so their bit patterns order like the floats; one atomic per CTA
-  __shared__ float wmax[PBLK / 32];
+  // the block's dead slots, and the fastest speed: lengths are non-negative, so their bit patterns order like the
+  // floats; one atomic per CTA
+  uint32_t nd = 0;
+#pragma unroll
+  for (int u = 0; u < CM_U; u++) nd += (uint32_t)__popc(__ballot_sync(0xffffffffu, dead[u]));
   float m = sp;
   for (int o = 16; o > 0; o >>= 1) m = fmx(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) wmax[threadIdx.x >> 5] = m;
-#pragma unroll
-  for (int u = 0; u < CM_U; u++) {
-    const uint32_t nd = __syncthreads_count(dead[u]);
-    const uint32_t blk = blockIdx.x * CM_U + u;
-    if (threadIdx.x == 0 && blk < B.nblk) B.blkDead[blk] = nd;
-  }
+  if (lane == 0) { wmax[threadIdx.x >> 5] = m; wdead[threadIdx.x >> 5] = nd; }
+  __syncthreads();
   if (threadIdx.x < 32) {
-    float b = wmax[threadIdx.x];
+    float b = threadIdx.x < CM_T / 32 ? wmax[threadIdx.x] : 0.0f;
+    uint32_t d = threadIdx.x < CM_T / 32 ? wdead[threadIdx.x] : 0u;
     for (int o = 16; o > 0; o >>= 1) b = fmx(b, __shfl_xor_sync(0xffffffffu, b, o));
-    if (threadIdx.x == 0 && b > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(b));
+    d = __reduce_add_sync(0xffffffffu, d);
+    if (threadIdx.x == 0) {
+      B.blkDead[blockIdx.x] = d;
+      if (b > 0.0f) atomicMax(&B.ctl->vmaxBits, __float_as_uint(b));
+    }
   }
 }
 
@@ -191,7 +198,7 @@ __global__ void __launch_bounds__(1024) k_scan_counts(Bufs B) {
 // ---- 4. scatter: sorted position of every particle ----
 // Live: (tile offset + cell offset + rank from the atomic count); the order inside a cell is fixed to ascending id by
 // p2g. Dead: after all live ones, in storage order (a block scan keeps it stable); they are moved here directly.
-__global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
+__global__ void __launch_bounds__(CM_T, 4) k_scatter(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
@@ -199,7 +206,7 @@ __global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
   bool dead[CM_U];
 #pragma unroll
   for (int u = 0; u < CM_U; u++) {
-    idx[u] = (blockIdx.x * CM_U + u) * PBLK + threadIdx.x;
+    idx[u] = blockIdx.x * PBLK + u * CM_T + threadIdx.x;
     k[u] = idx[u] < P.n ? B.key[idx[u]] : 0u;
   }
 #pragma unroll
@@ -210,8 +217,14 @@ __global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
       if (!dead[u]) { a[u] = B.tileSlot[k[u] >> 9]; off[u] = B.cellOff[k[u]]; rk[u] = B.rank[idx[u]]; }
     }
   }
-#pragma unroll
-  for (int u = 0; u < CM_U; u++) r[u] = blockExclusive(dead[u] ? 1u : 0u, sm, nullptr);
+  // dead ranks in storage order (slice by slice): two slices per scan in 16-bit fields (a slice has at most CM_T)
+  uint32_t t01, t23;
+  const uint32_t e01 = blockExclusive((dead[0] ? 1u : 0u) | (dead[1] ? 0x10000u : 0u), sm, &t01);
+  const uint32_t e23 = blockExclusive((dead[2] ? 1u : 0u) | (dead[3] ? 0x10000u : 0u), sm, &t23);
+  r[0] = e01 & 0xffffu;
+  r[1] = (t01 & 0xffffu) + (e01 >> 16);
+  r[2] = (t01 & 0xffffu) + (t01 >> 16) + (e23 & 0xffffu);
+  r[3] = (t01 & 0xffffu) + (t01 >> 16) + (t23 & 0xffffu) + (e23 >> 16);
 #pragma unroll
   for (int u = 0; u < CM_U; u++) {
     if (idx[u] >= P.n) continue;
@@ -220,7 +233,7 @@ __global__ void __launch_bounds__(PBLK) k_scatter(Bufs B) {
       B.srcIdx[pos] = idx[u];
       B.spid[pos] = id[u];
     } else {
-      const uint32_t pos = B.ctl->nLive + B.blkDead[blockIdx.x * CM_U + u] + r[u];
+      const uint32_t pos = B.ctl->nLive + B.blkDead[blockIdx.x] + r[u];
       B.pa[pos] = B.pb[idx[u]];
       B.ida[pos] = id[u];
     }
@@ -958,7 +971,7 @@ __global__ void k_iota(uint32_t* p, uint32_t n) {
 }
 
 // ---- launchers: each returns how many kernels it launched ----
-int launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<(B.nblk + CM_U - 1) / CM_U, PBLK, 0, s>>>(B); return 1; }
+int launch_count_mark(const Bufs& B, cudaStream_t s) { k_count_mark<<<B.nblk, CM_T, 0, s>>>(B); return 1; }
 int launch_mark_phi(const Bufs& B, int grid, cudaStream_t s) { k_mark_phi<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_mark_fill(const Bufs& B, int grid, cudaStream_t s) { k_mark_fill<<<grid, 256, 0, s>>>(B); return 1; }
 int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
@@ -969,7 +982,7 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
   return 3;
 }
 int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
-int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<(B.nblk + CM_U - 1) / CM_U, PBLK, 0, s>>>(B); return 1; }
+int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, CM_T, 0, s>>>(B); return 1; }
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
 int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
   if (ocean) k_classify<true><<<grid, 512, 0, s>>>(B);
