@@ -175,10 +175,12 @@ __device__ __forceinline__ uint32_t deficitNeed(const FlipParams& P, const Bufs&
     if (cx.y > oceanEta(P, B.waves, cx.x, cx.z) - 0.25f * P.h || ph < -P.band) return 0;
   } else {
     if ((ct & 0xffu) != 1u || ph > -1.0f || ph < -P.band) return 0;
-    if (!(len3(velGVec(P, B.velG, B.ncell, cx)) < 9.0f * P.h)) return 0;
   }
+  // the count test before the calm test (both only ever return 0, so the order is free): a full cell skips the
+  // 24-corner velocity sample
   const uint32_t n = (uint32_t)max(B.cnt[c], 0);
   if ((float)n >= 0.55f * P.rest) return 0;
+  if (!(lw > 0.25f && lw < 0.5f) && !(len3(velGVec(P, B.velG, B.ncell, cx)) < 9.0f * P.h)) return 0;
   return min((uint32_t)rintf(0.85f * P.rest) - n, 64u);
 }
 __global__ void __launch_bounds__(512) k_def_count(Bufs B) {

@@ -402,12 +402,14 @@ __device__ __forceinline__ void normBody(const FlipParams& P, const Bufs& B, int
   oldOut = old;
 }
 template <bool OCEAN>
-__global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
+__global__ void __launch_bounds__(512, 3) k_norm_div(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float svn[3][512];
+  __shared__ float shi[3][64];   // the faces just past the tile's high side, per axis, (other two local coordinates)
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
+  const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
@@ -418,6 +420,15 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
       B.vn[axis * nc + c] = v;
       B.vo[axis * nc + c] = old;
       svn[axis][threadIdx.x] = v;
+    }
+    // the divergence of the tile's high layer needs the neighbour tiles' first faces: six whole warps compute them
+    // (a face outside the tile box is never read: fluid cells lie inside the domain, which the box exceeds by a cell)
+    if (threadIdx.x < 192) {
+      const int ax = threadIdx.x >> 6, f0 = threadIdx.x & 7, f1 = (threadIdx.x >> 3) & 7;
+      const int fi = i - lx + (ax == 0 ? 8 : f0), fj = j - ly + (ax == 0 ? f0 : ax == 1 ? 8 : f1), fk = k - lz + (ax == 2 ? 8 : f1);
+      float d = 0.0f, o2;
+      if (fi < NX && fj < NY && fk < NZ) normBody<OCEAN>(P, B, ax, fi, fj, fk, cellIdx(P, fi, fj, fk), d, o2);
+      shi[ax][threadIdx.x & 63] = d;
     }
     __syncthreads();
     const uint32_t ct = B.ctype[c];
@@ -430,11 +441,9 @@ __global__ void __launch_bounds__(512) k_norm_div(Bufs B) {
       B.rhs[c] = 0.0f;
       B.sorInfo[c] = 0;
     } else {
-      float d, o2;
-      float vxp, vyp, vzp;
-      if (lx < 7) vxp = svn[0][threadIdx.x + 1]; else { normBody<OCEAN>(P, B, 0, i + 1, j, k, cellIdx(P, i + 1, j, k), d, o2); vxp = d; }
-      if (ly < 7) vyp = svn[1][threadIdx.x + 8]; else { normBody<OCEAN>(P, B, 1, i, j + 1, k, cellIdx(P, i, j + 1, k), d, o2); vyp = d; }
-      if (lz < 7) vzp = svn[2][threadIdx.x + 64]; else { normBody<OCEAN>(P, B, 2, i, j, k + 1, cellIdx(P, i, j, k + 1), d, o2); vzp = d; }
+      const float vxp = lx < 7 ? svn[0][threadIdx.x + 1] : shi[0][ly + 8 * lz];
+      const float vyp = ly < 7 ? svn[1][threadIdx.x + 8] : shi[1][lx + 8 * lz];
+      const float vzp = lz < 7 ? svn[2][threadIdx.x + 64] : shi[2][lx + 8 * ly];
       const float div = (vxp - svn[0][threadIdx.x] + vyp - svn[1][threadIdx.x] + vzp - svn[2][threadIdx.x]) * P.ih;
       bool interior = true;
       uint32_t mask = 0, nns = 0;
