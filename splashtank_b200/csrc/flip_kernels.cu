@@ -848,7 +848,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
 // sample lies in the 10^3-cell window (the tile plus one cell around it), staged once in shared memory.
 constexpr int G2P_T = 256;
 template <bool OCEAN>
-__global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
+__global__ void __launch_bounds__(G2P_T, 2) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
@@ -900,8 +900,12 @@ __global__ void __launch_bounds__(G2P_T) k_g2p(Bufs B) {
     }
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
     uint32_t emitSum = 0, deadSum = 0;
+    // each thread loads its next particle while it updates the current one
+    Part qNext;
+    if (s0 + threadIdx.x < s1) qNext = B.pa[s0 + threadIdx.x];
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
-      Part q = B.pa[i];
+      Part q = qNext;
+      if (i + G2P_T < s1) qNext = B.pa[i + G2P_T];
       g2pOne<OCEAN>(P, B, W, gtab, U, q);
       // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
