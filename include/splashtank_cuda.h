@@ -389,6 +389,15 @@ void* st_poisson_stream(st_poisson* s);
  * min(cap, n) are written. vs: metres per scene unit (the bake's scale; 0 means 1). */
 st_status st_flip_read_frame(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap, uint32_t* n,
                              int32_t* any_foam);
+/* The same frame without waiting for it, as the reference's readback is a mapAsync that the bake awaits later
+ * (readbackInto, src/gpu.js:430-443, awaited by the bake loops, src/gpu.js:577-587 and src/flip/bake.js:103-115): the
+ * frame of the particles as they are now is packed on the step stream and copied to pos/spd/fm on a second stream
+ * while the caller goes on stepping. st_flip_frame_wait blocks until it has landed and gives *n and *any_foam as st_flip_read_frame would. The copy covers
+ * min(cap, slots) points whatever *n turns out to be (points from *n on are unspecified) and fm always (all zero when
+ * no point has white water). The host buffers must stay valid until the wait; pinned memory lets the copy overlap the
+ * steps. One frame is pending at a time: another frame call first waits for it. A wait with nothing pending gives 0. */
+st_status st_flip_read_frame_async(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap);
+st_status st_flip_frame_wait(st_flip* s, uint32_t* n, int32_t* any_foam);
 /* bakeDiag (src/flip/bake.js:60-83) of the current particles, on the device: the same counts; sums agree to rounding. */
 typedef struct st_bake_diag {
   uint32_t alive, gone, non_finite, outside_box, at_speed_limit, foamy;

@@ -97,6 +97,11 @@ struct st_flip {
   uint16_t* cinfo = nullptr;
   uint32_t *nbs = nullptr, *slotOf = nullptr;
   uint8_t* frame = nullptr;   // packed frame (allocated by the first st_flip_read_frame)
+  // an asynchronous frame (st_flip_read_frame_async): copied to the host on its own stream while later steps run
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t frameReady = nullptr, frameCopied = nullptr;
+  uint32_t* frameMeta = nullptr;   // pinned: the frame's point count and any-foam flag
+  bool framePending = false;
   DiagAcc* diag = nullptr;
   float* wet = nullptr;
   float* sdf = nullptr;
@@ -176,6 +181,7 @@ void st_flip_destroy(st_flip* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->copyStream) cudaStreamSynchronize(s->copyStream);
   drop_graphs(s);
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
@@ -188,6 +194,10 @@ void st_flip_destroy(st_flip* s) {
   for (auto& e : s->ring_ev) if (e) cudaEventDestroy(e);
   for (auto& row : s->tev) for (auto& e : row) if (e) cudaEventDestroy(e);
   for (auto& e : s->ev) if (e) cudaEventDestroy(e);
+  if (s->frameReady) cudaEventDestroy(s->frameReady);
+  if (s->frameCopied) cudaEventDestroy(s->frameCopied);
+  if (s->frameMeta) cudaFreeHost(s->frameMeta);
+  if (s->copyStream) cudaStreamDestroy(s->copyStream);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -954,6 +964,33 @@ st_status st_flip_pack_live(st_flip* s, float vs, uint32_t* words, uint64_t cap_
   return ST_OK;
 }
 
+// the frame unsorted into the spare particle buffer and packed into s->frame, on the step stream
+struct FramePtrs { uint32_t* meta; uint16_t* p16; uint8_t* sp; uint8_t* f8; };
+static st_status frame_pack(st_flip* s, float vs, FramePtrs* f) {
+  if (!s->frame) {   // packed frame: 6 + 1 + 1 bytes per slot, plus 2 counters
+    CK(cudaMalloc((void**)&s->frame, (size_t)s->maxN * 8 + 16));
+  }
+  f->meta = reinterpret_cast<uint32_t*>(s->frame);
+  f->p16 = reinterpret_cast<uint16_t*>(s->frame + 16);
+  f->sp = s->frame + 16 + (size_t)s->maxN * 6;
+  f->f8 = f->sp + s->maxN;
+  float4* tmp = reinterpret_cast<float4*>(s->part[s->cur ^ 1]);
+  launch_unsort(s->part[s->cur], s->ids[s->cur], s->N, tmp, nullptr, s->stream);
+  FrameBox F{s->bx0, s->by0, s->bz0, 65535.0 / (s->bx1 - s->bx0), 65535.0 / (s->by1 - s->by0), 65535.0 / (s->bz1 - s->bz0),
+             16.0 * (vs != 0.0f ? (double)vs : 1.0)};
+  CK(cudaMemsetAsync(f->meta, 0, 8, s->stream));
+  launch_pack_frame(tmp, s->N, F, f->p16, f->sp, f->f8, f->meta, s->stream);
+  CK(cudaGetLastError());
+  return ST_OK;
+}
+// the host has the pending asynchronous frame (s->frame is free again)
+static st_status frame_settle(st_flip* s) {
+  if (!s->framePending) return ST_OK;
+  s->framePending = false;
+  CK(cudaEventSynchronize(s->frameCopied));
+  return ST_OK;
+}
+
 st_status st_flip_read_frame(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap, uint32_t* n,
                              int32_t* any_foam) {
   if (!s || !n) return ST_BAD_ARG;
@@ -961,32 +998,64 @@ st_status st_flip_read_frame(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, 
   *n = 0;
   if (any_foam) *any_foam = 0;
   if (s->N == 0) return ST_OK;
-  if (!s->frame) {   // packed frame: 6 + 1 + 1 bytes per slot, plus 2 counters
-    CK(cudaMalloc((void**)&s->frame, (size_t)s->maxN * 8 + 16));
-  }
-  uint32_t* meta = reinterpret_cast<uint32_t*>(s->frame);
-  uint16_t* p16 = reinterpret_cast<uint16_t*>(s->frame + 16);
-  uint8_t* sp = s->frame + 16 + (size_t)s->maxN * 6;
-  uint8_t* f8 = sp + s->maxN;
-  float4* tmp = reinterpret_cast<float4*>(s->part[s->cur ^ 1]);
-  launch_unsort(s->part[s->cur], s->ids[s->cur], s->N, tmp, nullptr, s->stream);
-  FrameBox F{s->bx0, s->by0, s->bz0, 65535.0 / (s->bx1 - s->bx0), 65535.0 / (s->by1 - s->by0), 65535.0 / (s->bz1 - s->bz0),
-             16.0 * (vs != 0.0f ? (double)vs : 1.0)};
-  CK(cudaMemsetAsync(meta, 0, 8, s->stream));
-  launch_pack_frame(tmp, s->N, F, p16, sp, f8, meta, s->stream);
-  CK(cudaGetLastError());
+  st_status r = frame_settle(s);
+  if (r != ST_OK) return r;
+  FramePtrs f;
+  if ((r = frame_pack(s, vs, &f)) != ST_OK) return r;
   uint32_t h[2];
-  CK(cudaMemcpyAsync(h, meta, 8, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(h, f.meta, 8, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   *n = h[0];
   if (any_foam) *any_foam = (int32_t)h[1];
   const uint32_t m = std::min(cap, h[0]);
   if (m) {
-    if (pos) CK(cudaMemcpyAsync(pos, p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->stream));
-    if (spd) CK(cudaMemcpyAsync(spd, sp, m, cudaMemcpyDeviceToHost, s->stream));
-    if (fm && h[1]) CK(cudaMemcpyAsync(fm, f8, m, cudaMemcpyDeviceToHost, s->stream));
+    if (pos) CK(cudaMemcpyAsync(pos, f.p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->stream));
+    if (spd) CK(cudaMemcpyAsync(spd, f.sp, m, cudaMemcpyDeviceToHost, s->stream));
+    if (fm && h[1]) CK(cudaMemcpyAsync(fm, f.f8, m, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
   }
+  return ST_OK;
+}
+
+st_status st_flip_read_frame_async(st_flip* s, float vs, uint16_t* pos, uint8_t* spd, uint8_t* fm, uint32_t cap) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  st_status r = frame_settle(s);
+  if (r != ST_OK) return r;
+  if (!s->copyStream) {
+    CK(cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s->frameReady, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s->frameCopied, cudaEventDisableTiming));
+    CK(cudaHostAlloc((void**)&s->frameMeta, 16, cudaHostAllocDefault));
+  }
+  s->frameMeta[0] = s->frameMeta[1] = 0;
+  if (s->N == 0) return ST_OK;   // nothing pending: the wait gives 0 points
+  FramePtrs f;
+  if ((r = frame_pack(s, vs, &f)) != ST_OK) return r;
+  CK(cudaEventRecord(s->frameReady, s->stream));
+  CK(cudaStreamWaitEvent(s->copyStream, s->frameReady, 0));
+  CK(cudaMemcpyAsync(s->frameMeta, f.meta, 8, cudaMemcpyDeviceToHost, s->copyStream));
+  const uint32_t m = std::min(cap, s->N);   // the point count is not known yet: every slot the caller has room for
+  if (m) {
+    if (pos) CK(cudaMemcpyAsync(pos, f.p16, (size_t)m * 6, cudaMemcpyDeviceToHost, s->copyStream));
+    if (spd) CK(cudaMemcpyAsync(spd, f.sp, m, cudaMemcpyDeviceToHost, s->copyStream));
+    if (fm) CK(cudaMemcpyAsync(fm, f.f8, m, cudaMemcpyDeviceToHost, s->copyStream));
+  }
+  CK(cudaEventRecord(s->frameCopied, s->copyStream));
+  s->framePending = true;
+  return ST_OK;
+}
+
+st_status st_flip_frame_wait(st_flip* s, uint32_t* n, int32_t* any_foam) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  if (n) *n = 0;
+  if (any_foam) *any_foam = 0;
+  if (!s->framePending) return ST_OK;
+  st_status r = frame_settle(s);
+  if (r != ST_OK) return r;
+  if (n) *n = s->frameMeta[0];
+  if (any_foam) *any_foam = (int32_t)s->frameMeta[1];
   return ST_OK;
 }
 

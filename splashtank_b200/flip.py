@@ -305,6 +305,32 @@ class FlipSim:
         m = n.value
         return dict(n=m, pos=pos[:m], spd=spd[:m], fm=fm[:m] if foam.value else None)
 
+    def read_frame_async(self, vs=1.0, out=None):
+        """Starts the same frame and returns at once (readbackInto's mapAsync, src/gpu.js:430-443): it is packed on the
+        step stream and copied on a second stream while later steps run; frame_wait() gives it. out as in read_frame
+        (pinned host memory lets the copy overlap the steps); the arrays are held until the wait."""
+        self.flushRun()
+        cap = max(self.MAXN, 1)
+        if out is None:
+            out = (np.zeros((cap, 3), np.uint16), np.zeros(cap, np.uint8), np.zeros(cap, np.uint8))
+        pos, spd, fm = out
+        cap = min(cap, len(spd), len(fm), pos.size // 3)
+        self._frame_out = out
+        self._check(self.f["flip_read_frame_async"](self._h, float(vs), pos.ctypes.data_as(C.POINTER(C.c_uint16)),
+                                                    spd.ctypes.data_as(abi.u8p), fm.ctypes.data_as(abi.u8p), cap), "read_frame_async")
+
+    def frame_wait(self):
+        """The frame of the last read_frame_async once it has landed, as read_frame returns it (n = 0 when none is
+        pending)."""
+        n, foam = C.c_uint32(), C.c_int32()
+        self._check(self.f["flip_frame_wait"](self._h, C.byref(n), C.byref(foam)), "frame_wait")
+        out, self._frame_out = getattr(self, "_frame_out", None), None
+        m = n.value
+        if out is None:
+            return dict(n=0, pos=np.zeros((0, 3), np.uint16), spd=np.zeros(0, np.uint8), fm=None)
+        pos, spd, fm = out
+        return dict(n=m, pos=pos[:m], spd=spd[:m], fm=fm[:m] if foam.value else None)
+
     def bake_diag(self, vcap=14.0):
         """bakeDiag (src/flip/bake.js:60-83) computed on the device, with the reference's keys."""
         d = abi.BakeDiag()

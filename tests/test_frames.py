@@ -95,6 +95,48 @@ def test_device_frame_and_diag_match_the_reference_arithmetic():
 
 
 @pytest.mark.gpu
+def test_async_frame_matches_the_synchronous_one():
+    """st_flip_read_frame_async: the frame of the particles at the call lands while later steps run and equals the
+    synchronous frame taken at the same point; a second call first settles the pending one; a wait with nothing
+    pending gives no points."""
+    import torch
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    tank = scenes.WaveTank(32, steps=60, spray_cap=100_000)
+    sim = tank.make(FlipSim)
+    run = SceneRunner(sim)
+    t = [0.0]
+
+    def advance(k):
+        for _ in range(k):
+            t[0] += tank.dt
+            run.step(tank.dt, tank.states(t[0]), tank.opts)
+
+    def same(a, b):
+        assert a["n"] == b["n"] > 0
+        assert np.array_equal(a["pos"], b["pos"]) and np.array_equal(a["spd"], b["spd"])
+        assert (a["fm"] is None) == (b["fm"] is None)
+        assert a["fm"] is None or np.array_equal(a["fm"], b["fm"])
+
+    advance(30)
+    assert sim.frame_wait()["n"] == 0
+    cap = sim.MAXN
+    pin = torch.empty(cap * 8, dtype=torch.uint8, pin_memory=True).numpy()
+    out = (pin[:cap * 6].view(np.uint16).reshape(cap, 3), pin[cap * 6:cap * 7], pin[cap * 7:cap * 8])
+    want = sim.read_frame(1.3)
+    sim.read_frame_async(1.3, out=out)
+    advance(3)   # steps queued behind the frame's packing while its copy runs
+    same(sim.frame_wait(), want)
+    assert sim.frame_wait()["n"] == 0
+    want = sim.read_frame(1.0)
+    sim.read_frame_async(1.0)
+    sim.read_frame_async(1.0, out=out)
+    same(sim.frame_wait(), want)
+    advance(1)
+    assert not np.array_equal(sim.read_frame(1.0)["pos"], want["pos"])
+
+
+@pytest.mark.gpu
 def test_bake_loop_writes_a_cache():
     from splashtank_b200.flip import FlipSim
     from splashtank_b200.scene import SceneRunner
