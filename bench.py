@@ -735,10 +735,11 @@ def main():
     value = live_sum * a.steps / (ms_max * 1e-3)
 
     # ---- end to end through the C ABI with host buffers: every step the options and collider records go up from pinned
-    # host memory and the step's counters come back (readStats); every 4th step (a 60 Hz frame at dt 1/240) the
-    # particles come back as a cache frame (6 + 1 + 1 bytes per point, packed on the device) into pinned host memory, as
-    # a bake stores them: st_flip_read_frame_async, so the copy runs while the next steps compute, and
-    # st_flip_frame_wait before the next frame and at the end (inside the timed region)
+    # host memory and the step's counters come back (readStats as the reference issues it: queued behind the step,
+    # waited for once the next step is queued, so the device never idles while the host reads them); every 4th step (a
+    # 60 Hz frame at dt 1/240) the particles come back as a cache frame (6 + 1 + 1 bytes per point, packed on the device)
+    # into pinned host memory, as a bake stores them: st_flip_read_frame_async, so the copy runs while the next steps
+    # compute, and st_flip_frame_wait before the next frame and at the end (inside the timed region)
     n_all = st1["n"]
     cap = max(sim.MAXN, 1)
     pin = torch.empty(cap * 8, dtype=torch.uint8, pin_memory=True).numpy()
@@ -751,12 +752,18 @@ def main():
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
+    prev = None
     for k in range(a.e2e_steps):
         step()
-        sim.readStats()
+        tk = sim.readStatsAsync()
+        if prev is not None:
+            sim.statsWait(prev)
+        prev = tk
         if k % 4 == 3:
             sim.frame_wait()
             sim.read_frame_async(1.0, out=fbuf)
+    if prev is not None:
+        sim.statsWait(prev)
     sim.frame_wait()
     f1.record(stream)
     f1.synchronize()
@@ -779,7 +786,7 @@ def main():
                 "stage_ms_per_step": {k: round(v / max(nrec, 1), 4) for k, v in stages.items()},
                 "clocks": clk, "roofline": rl,
                 "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                        "steps": a.e2e_steps, "readback": "counters every step, a packed cache frame of all particles every 4th step, copied while the next steps run"}}
+                        "steps": a.e2e_steps, "readback": "counters every step (read once the next step is queued), a packed cache frame of all particles every 4th step, copied while the next steps run"}}
         if world == 1 and not a.no_cpu_baseline:
             del sim
             cb, _ = cpu_sample(a.workload)

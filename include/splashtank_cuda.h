@@ -270,6 +270,13 @@ typedef struct st_sdf_build {
 st_status st_build_sdf(int device, const st_mesh* mesh, st_sdf_build* b);
 /* FlipSim.stats via readStats (src/flip/sim.js:160-168). Synchronises. */
 st_status st_flip_stats(st_flip* s, st_stats* out);
+/* The counters without waiting, as the reference reads them (readStats, src/flip/sim.js:160-168: the copy is encoded
+ * into the step's submission and mapped later): st_flip_stats_async enqueues a copy of the counters as they will be
+ * after the work queued so far into pinned host memory and returns a ticket (1, 2, ...); st_flip_stats_wait blocks
+ * until that copy has landed and fills *out as st_flip_stats would have at that point. The last 4 tickets are held: a
+ * fifth call first waits for the oldest copy, and a ticket older than that gives ST_BAD_ARG. */
+st_status st_flip_stats_async(st_flip* s, uint64_t* ticket);
+st_status st_flip_stats_wait(st_flip* s, uint64_t ticket, st_stats* out);
 /* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */
 st_status st_flip_read_grid(st_flip* s, const st_flip_grid* g);
 st_status st_flip_get_dims(st_flip* s, st_flip_dims* out);

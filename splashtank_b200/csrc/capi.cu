@@ -102,6 +102,11 @@ struct st_flip {
   cudaEvent_t frameReady = nullptr, frameCopied = nullptr;
   uint32_t* frameMeta = nullptr;   // pinned: the frame's point count and any-foam flag
   bool framePending = false;
+  // counters read without waiting (st_flip_stats_async): a ring of pinned copies, each with its ticket and event
+  static constexpr int STAT_SLOTS = 4;
+  struct StatSlot { Ctl* h = nullptr; cudaEvent_t ev = nullptr; uint64_t ticket = 0, steps = 0, launches = 0; uint32_t n = 0; bool pending = false; };
+  StatSlot stat[STAT_SLOTS];
+  uint64_t statNext = 1;
   DiagAcc* diag = nullptr;
   float* wet = nullptr;
   float* sdf = nullptr;
@@ -197,6 +202,10 @@ void st_flip_destroy(st_flip* s) {
   if (s->frameReady) cudaEventDestroy(s->frameReady);
   if (s->frameCopied) cudaEventDestroy(s->frameCopied);
   if (s->frameMeta) cudaFreeHost(s->frameMeta);
+  for (auto& q : s->stat) {
+    if (q.ev) cudaEventDestroy(q.ev);
+    if (q.h) cudaFreeHost(q.h);
+  }
   if (s->copyStream) cudaStreamDestroy(s->copyStream);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -729,15 +738,52 @@ st_status st_flip_step_timed(st_flip* s, double dt, const st_step_opts* o, st_st
   return do_step(s, dt, o, t);
 }
 
+static void stats_fill(const Ctl& c, uint32_t n, uint64_t steps, uint64_t launches, st_stats* out) {
+  out->sc = c.nActive; out->ovf = 0; out->fluid = c.fluid;
+  uint32_t vb = c.vmaxBits; float vm; memcpy(&vm, &vb, 4); out->vmax = vm;
+  out->n = n; out->live = steps ? c.nLive : n; out->spray_used = c.sctl0; out->steps = steps;
+  out->launches = launches; out->spray_overflow = c.sprayOvf;
+}
+
 st_status st_flip_stats(st_flip* s, st_stats* out) {
   if (!s || !out) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));
   CK(cudaMemcpyAsync(s->hCtl, s->dCtl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
-  out->sc = s->hCtl->nActive; out->ovf = 0; out->fluid = s->hCtl->fluid;
-  uint32_t vb = s->hCtl->vmaxBits; float vm; memcpy(&vm, &vb, 4); out->vmax = vm;
-  out->n = s->N; out->live = s->steps ? s->hCtl->nLive : s->N; out->spray_used = s->hCtl->sctl0; out->steps = s->steps;
-  out->launches = s->launches; out->spray_overflow = s->hCtl->sprayOvf;
+  stats_fill(*s->hCtl, s->N, s->steps, s->launches, out);
+  return ST_OK;
+}
+
+st_status st_flip_stats_async(st_flip* s, uint64_t* ticket) {
+  if (!s || !ticket) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  st_flip::StatSlot& q = s->stat[s->statNext % st_flip::STAT_SLOTS];
+  if (q.pending) {   // the ring is full: the oldest copy has to land before its slot is reused
+    q.pending = false;
+    CK(cudaEventSynchronize(q.ev));
+  }
+  if (!q.h) {
+    CK(cudaHostAlloc((void**)&q.h, sizeof(Ctl), cudaHostAllocDefault));
+    CK(cudaEventCreateWithFlags(&q.ev, cudaEventDisableTiming));
+  }
+  CK(cudaMemcpyAsync(q.h, s->dCtl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaEventRecord(q.ev, s->stream));
+  q.ticket = s->statNext; q.n = s->N; q.steps = s->steps; q.launches = s->launches; q.pending = true;
+  *ticket = s->statNext++;
+  return ST_OK;
+}
+
+st_status st_flip_stats_wait(st_flip* s, uint64_t ticket, st_stats* out) {
+  if (!s || !out) return ST_BAD_ARG;
+  st_flip::StatSlot& q = s->stat[ticket % st_flip::STAT_SLOTS];
+  if (ticket == 0 || q.ticket != ticket) {   // never issued, or its slot has been reused since
+    st::set_error_text("st_flip_stats_wait: ticket not issued or no longer held");
+    return ST_BAD_ARG;
+  }
+  CK(cudaSetDevice(s->device));
+  CK(cudaEventSynchronize(q.ev));
+  q.pending = false;
+  stats_fill(*q.h, q.n, q.steps, q.launches, out);
   return ST_OK;
 }
 

@@ -372,9 +372,24 @@ class FlipSim:
     def readStats(self):
         s = abi.Stats()
         self._check(self.f["flip_stats"](self._h, C.byref(s)), "stats")
+        return self._set_stats(s)
+
+    def _set_stats(self, s):
         self.stats = dict(sc=s.sc, ovf=s.ovf, fluid=s.fluid, vmax=s.vmax, n=s.n, live=s.live, spray_used=s.spray_used, steps=s.steps,
                           spray_overflow=s.spray_overflow, launches=s.launches)
         return self.stats
+
+    def readStatsAsync(self):
+        """readStats as the reference issues it (src/flip/sim.js:160-168): the counters' copy is queued behind the work
+        so far and the call returns a ticket; statsWait(ticket) gives them once they have landed."""
+        t = C.c_uint64()
+        self._check(self.f["flip_stats_async"](self._h, C.byref(t)), "readStatsAsync")
+        return t.value
+
+    def statsWait(self, ticket):
+        s = abi.Stats()
+        self._check(self.f["flip_stats_wait"](self._h, C.c_uint64(ticket), C.byref(s)), "statsWait")
+        return self._set_stats(s)
 
     def activeCells(self):
         return self.readStats()["fluid"]

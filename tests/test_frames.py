@@ -137,6 +137,33 @@ def test_async_frame_matches_the_synchronous_one():
 
 
 @pytest.mark.gpu
+def test_async_stats_match_the_synchronous_ones():
+    """st_flip_stats_async / st_flip_stats_wait: the counters of each step, read later, equal those read right after it
+    on an identical tank; only the last four tickets are held."""
+    from splashtank_b200.flip import FlipSim, StError
+    from splashtank_b200.scene import SceneRunner
+    tank = scenes.WaveTank(32, steps=60, spray_cap=100_000)
+    a, b = tank.make(FlipSim), tank.make(FlipSim)
+    ra, rb = SceneRunner(a), SceneRunner(b)
+    want, tickets = [], []
+    t = 0.0
+    for _ in range(6):
+        t += tank.dt
+        ra.step(tank.dt, tank.states(t), tank.opts)
+        want.append(dict(a.readStats()))
+        rb.step(tank.dt, tank.states(t), tank.opts)
+        tickets.append(b.readStatsAsync())
+    assert tickets == [1, 2, 3, 4, 5, 6]
+    for k in range(2, 6):
+        assert b.statsWait(tickets[k]) == want[k], k
+    assert b.statsWait(tickets[5]) == want[5]   # a ticket can be read again while it is held
+    for k in (0, 1):
+        with pytest.raises(StError):
+            b.statsWait(tickets[k])
+    assert want[5]["steps"] == 6 and want[5]["live"] > 0
+
+
+@pytest.mark.gpu
 def test_bake_loop_writes_a_cache():
     from splashtank_b200.flip import FlipSim
     from splashtank_b200.scene import SceneRunner
