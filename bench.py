@@ -29,7 +29,7 @@ sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
-NCU_TRAFFIC = {"g2p": {"bytes": 180544768 + 102174464, "particles": 4669521},
+NCU_TRAFFIC = {"g2p": {"bytes": 180631296 + 105086464, "particles": 4669521},
                "p2g": {"bytes": 209715200 + 135951360, "particles": 4669521}}
 FALLBACK_HBM = 6650.0
 
