@@ -507,6 +507,9 @@ __global__ void __launch_bounds__(512) k_sor_pack(Bufs B) {
   }
 }
 __global__ void __launch_bounds__(256) k_sor_c(Bufs B, uint32_t color) {
+  // launched as a programmatic dependent of the previous sweep: its CTAs may become resident early, and wait here until
+  // that sweep has finished and its writes are visible
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const uint32_t nT = B.ctl->nFluidTiles;
   const float omega = B.P->omega;
   const uint32_t j = threadIdx.x, lz = j >> 5, ly = (j >> 2) & 7u;
@@ -1010,7 +1013,19 @@ int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
 int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s) {
   k_sor_slots<<<64, 256, 0, s>>>(B);
   k_sor_pack<<<grid4, 512, 0, s>>>(B);
-  for (int it = 0; it < iters; it++) { k_sor_c<<<grid, 256, 0, s>>>(B, 0u); k_sor_c<<<grid, 256, 0, s>>>(B, 1u); }
+  // each sweep is a programmatic dependent launch of the one before, so its launch overlaps the previous sweep's tail
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  for (int it = 0; it < iters; it++)
+    for (uint32_t color = 0; color < 2; color++) cudaLaunchKernelEx(&cfg, k_sor_c, B, color);
   k_sor_unpack<<<grid4, 512, 0, s>>>(B);
   return 2 * iters + 3;
 }
