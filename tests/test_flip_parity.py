@@ -176,6 +176,39 @@ def test_drips_from_a_rising_sphere():
     assert_same_state(g, o, spray=True)
 
 
+def test_ragged_box_open_face_collider_and_whitewater():
+    """A box whose cell counts are multiples of 8 on no axis (37 x 22 x 29 cells; tile box 5 x 3 x 4 with its padding
+    cells), open on +x, water thrown towards the open face past a moving sphere, whitewater with the air field, gusts,
+    sheet tearing and a 3-cell narrow band: 30 steps bit for bit."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    from splashtank_b200.scene import SceneRunner, sphere_sdf
+    h, n = 1.0 / 32, (37, 22, 29)
+    size = tuple(k * h for k in n)
+    rng = np.random.default_rng(21)
+    cells = scenes.box_cells(n, lambda ci, cj, ck: (ci < 20) & (cj < 14))
+    pos = scenes.seed_cells(cells, h, rng, -size[0] / 2, 0.0, -size[2] / 2)
+    vel = np.tile(np.array([[1.5, 0.3, 0.2]], np.float32), (len(pos), 1))
+    sc = dict(d=h / 2, ratio=2.0, size=size, open=2, pos=pos, vel=vel)
+    opts = dict(g=9.81, flip=0.95, comp=6.0, iters=30, vmax=14.0, drag=0.3, gust=1.0, tear=2.0,
+                spr=dict(scenes.APP_SPRAY, min=0.5), air=dict(on=True, couple=3.0, decay=0.6), nb=dict(on=True, band=3.0))
+    g, o = make_pair(sc, spray_cap=30000)
+    for s in (g, o):
+        assert (s.nx, s.ny, s.nz) == n
+        p, v, i = s.save_state()
+        s.load_state(p, v, i, t=0.6, seed=0)
+    sdf = sphere_sdf(0.08, h / 2, sid=7)
+    runs, t, dt = [SceneRunner(s) for s in (g, o)], 0.0, 1.0 / 240.0
+    for _ in range(30):
+        t += dt
+        st = [dict(id=1, sdf=sdf, x=0.1 + 0.5 * t, y=0.25, z=0.05)]
+        for r in runs:
+            r.step(dt, st, opts)
+    gs = g.readStats()
+    assert gs["live"] < gs["n"] and gs["spray_used"] > 0
+    assert_same_state(g, o, spray=True)
+
+
 def test_particle_state_round_trip():
     """save_state -> load_state -> save_state returns the same particles, ids and storage order."""
     from splashtank_b200 import scenes
