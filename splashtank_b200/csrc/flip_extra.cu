@@ -74,15 +74,26 @@ __global__ void __launch_bounds__(512) k_nb_phi(Bufs B) {
 __device__ __forceinline__ float jacNb(const FlipParams& P, const Bufs& B, int i, int j, int k, float cur, bool fromRhs) {
   if (!inDom(P, i, j, k)) return 8.0f;
   if (cur >= 0.0f) return cur;
-  float m = -8.0f;
+  // the six neighbours' words are loaded together from addresses that are always valid (a neighbour outside the domain
+  // reads the cell itself and is skipped below); the maximum then runs in the reference's order
+  uint32_t ct[6];
+  float rv[6];
+  bool in[6];
+  const uint32_t self = cellIdx(P, i, j, k);
+#pragma unroll
   for (int q = 0; q < 6; q++) {
     int a = i, b = j, c = k;
     if (q == 0) a -= 1; else if (q == 1) a += 1; else if (q == 2) b -= 1; else if (q == 3) b += 1; else if (q == 4) c -= 1; else c += 1;
-    if (!inDom(P, a, b, c)) continue;
-    const uint32_t cq = cellIdx(P, a, b, c);
-    const uint32_t ct = B.ctype[cq];
-    if (((ct >> 8) & 0xffu) != 0u) continue;
-    m = fmx(m, fromRhs ? B.rhs[cq] : phiOfBits(ct));
+    in[q] = inDom(P, a, b, c);
+    const uint32_t cq = in[q] ? cellIdx(P, a, b, c) : self;
+    ct[q] = B.ctype[cq];
+    rv[q] = fromRhs ? B.rhs[cq] : 0.0f;
+  }
+  float m = -8.0f;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    if (!in[q] || ((ct[q] >> 8) & 0xffu) != 0u) continue;
+    m = fmx(m, fromRhs ? rv[q] : phiOfBits(ct[q]));
   }
   return clampf(m - 1.0f, -7.9f, -0.5f);
 }
@@ -114,12 +125,20 @@ __global__ void __launch_bounds__(512) k_nb_vel(Bufs B) {
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
     if (!inDom(P, i, j, k) || (B.ctype[c] & 0xffu) != 1u) continue;
+    // the three lower neighbours' types and the three face weights, loaded together (a neighbour outside the domain
+    // reads the cell itself and is skipped)
+    uint32_t nt[3];
+    int32_t wsum[3];
+    bool in[3];
+#pragma unroll
     for (int ax = 0; ax < 3; ax++) {
-      int li = i, lj = j, lk = k;
-      if (ax == 0) li -= 1; else if (ax == 1) lj -= 1; else lk -= 1;
-      if (!inDom(P, li, lj, lk)) continue;
-      if ((B.ctype[cellIdx(P, li, lj, lk)] & 0xffu) != 1u) continue;
-      if (B.acc[(3 + ax) * nc + c] > 0) continue;
+      const int li = ax == 0 ? i - 1 : i, lj = ax == 1 ? j - 1 : j, lk = ax == 2 ? k - 1 : k;
+      in[ax] = inDom(P, li, lj, lk);
+      nt[ax] = B.ctype[in[ax] ? cellIdx(P, li, lj, lk) : c];
+      wsum[ax] = B.acc[(3 + ax) * nc + c];
+    }
+    for (int ax = 0; ax < 3; ax++) {
+      if (!in[ax] || (nt[ax] & 0xffu) != 1u || wsum[ax] > 0) continue;
       const V3 fp = facePos(P, i, j, k, ax);
       const float vc = velGAxis(P, B.velG, nc, fp - velGVec(P, B.velG, nc, fp) * P.dt, ax);
       B.acc[ax * nc + c] = (int32_t)rintf(vc * P.scale);
