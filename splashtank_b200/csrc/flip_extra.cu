@@ -212,10 +212,10 @@ __global__ void __launch_bounds__(512) k_def_count(Bufs B) {
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
     const uint32_t nd = deficitNeed(P, B, c, i, j, k);
-    uint32_t cells, needs;
-    blockExclusive(nd ? 1u : 0u, sm, &cells);
-    blockExclusive(nd, sm, &needs);
-    if (threadIdx.x == 0) { B.tileAux[a] = cells; B.tileAux2[a] = needs; }
+    // one scan of two 16-bit fields: cells asking (at most 512) and particles asked for (at most 64 a cell)
+    uint32_t tot;
+    blockExclusive((nd ? 1u : 0u) | (nd << 16), sm, &tot);
+    if (threadIdx.x == 0) { B.tileAux[a] = tot & 0xffffu; B.tileAux2[a] = tot >> 16; }
   }
 }
 __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
@@ -226,12 +226,13 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
   const uint32_t nKilled = B.ctl->nKilled, nLive = B.ctl->nLive;
   const uint32_t avail = min(nKilled + (P.n - nLive), P.lcap);
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+    if (B.tileAux2[a + 1] == B.tileAux2[a]) continue;   // no cell of this tile asks (the whole CTA skips it)
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
     const uint32_t nd = deficitNeed(P, B, c, i, j, k);
-    const uint32_t e = B.tileAux[a] + blockExclusive(nd ? 1u : 0u, sm, nullptr);
-    const uint32_t base = B.tileAux2[a] + blockExclusive(nd, sm, nullptr);
+    const uint32_t ex = blockExclusive((nd ? 1u : 0u) | (nd << 16), sm, nullptr);
+    const uint32_t e = B.tileAux[a] + (ex & 0xffffu), base = B.tileAux2[a] + (ex >> 16);
     if (!nd || e >= P.lcap / 2u) continue;
     const V3 cp = v3((float)i, (float)j, (float)k);
     for (uint32_t m = 0; m < nd; m++) {
