@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="wave_tank_256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=40)
+    ap.add_argument("--e2e-steps", type=int, default=80)
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--tol", type=float, default=1e-6, help="pressure workloads: relative residual to reach")
     ap.add_argument("--omega", type=float, default=1.9, help="pressure workloads: SOR factor")
@@ -749,22 +749,28 @@ def main():
     d2h = 64 + (8 * n_all) / 4.0
     if a.no_e2e:
         a.e2e_steps = 0
+
+    def e2e_run(steps):
+        prev = None
+        for k in range(steps):
+            step()
+            tk = sim.readStatsAsync()
+            if prev is not None:
+                sim.statsWait(prev)
+            prev = tk
+            if k % 4 == 3:
+                sim.frame_wait()
+                sim.read_frame_async(1.0, out=fbuf)
+        if prev is not None:
+            sim.statsWait(prev)
+        sim.frame_wait()
+
+    if a.e2e_steps:
+        e2e_run(8)   # untimed: the copy stream, the pinned frame buffer and the counter ring get their first use
     barrier()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    prev = None
-    for k in range(a.e2e_steps):
-        step()
-        tk = sim.readStatsAsync()
-        if prev is not None:
-            sim.statsWait(prev)
-        prev = tk
-        if k % 4 == 3:
-            sim.frame_wait()
-            sim.read_frame_async(1.0, out=fbuf)
-    if prev is not None:
-        sim.statsWait(prev)
-    sim.frame_wait()
+    e2e_run(a.e2e_steps)
     f1.record(stream)
     f1.synchronize()
     barrier()
