@@ -275,6 +275,11 @@ st_status st_flip_stats(st_flip* s, st_stats* out);
  * after the work queued so far into pinned host memory and returns a ticket (1, 2, ...); st_flip_stats_wait blocks
  * until that copy has landed and fills *out as st_flip_stats would have at that point. The last 4 tickets are held: a
  * fifth call first waits for the oldest copy, and a ticket older than that gives ST_BAD_ARG. */
+/* The step timer of the reference's FlipSim (track, src/gpu.js:444-454): *inflight = steps queued but not finished,
+ * *last_ms = the median device time of the last 31 finished steps (0 before the first), *slow_ms = the slowest step
+ * so far. Each step records an event before and after itself; this call reads those of the finished steps without
+ * waiting for the others. */
+st_status st_flip_track(st_flip* s, uint32_t* inflight, float* last_ms, float* slow_ms);
 st_status st_flip_stats_async(st_flip* s, uint64_t* ticket);
 st_status st_flip_stats_wait(st_flip* s, uint64_t ticket, st_stats* out);
 /* FlipSim.dbgColumn/dbgRow/activeCells (src/flip/sim.js:457-490), all cells at once. */

@@ -158,6 +158,7 @@ CUDA_ONLY_FUNCS = [
     ("flip_read_deep", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, C.c_uint32, u32p]),
     ("flip_read_spray_frame", C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.POINTER(C.c_uint16), u32p, C.c_uint32, u32p, u32p]),
     ("flip_read_frame", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, u8p, C.c_uint32, u32p, C.POINTER(C.c_int32)]),
+    ("flip_track", C.c_int, [C.c_void_p, u32p, f32p, f32p]),
     ("flip_stats_async", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("flip_stats_wait", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Stats)]),
     ("flip_read_frame_async", C.c_int, [C.c_void_p, C.c_float, C.POINTER(C.c_uint16), u8p, u8p, C.c_uint32]),

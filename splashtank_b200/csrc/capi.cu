@@ -102,6 +102,13 @@ struct st_flip {
   cudaEvent_t frameReady = nullptr, frameCopied = nullptr;
   uint32_t* frameMeta = nullptr;   // pinned: the frame's point count and any-foam flag
   bool framePending = false;
+  // step tracking (track, src/gpu.js:444-454): an event before and after each step, read once the step is done
+  static constexpr int TRK = 64;
+  cudaEvent_t trkStart[TRK] = {}, trkDone[TRK] = {};
+  uint64_t trkHead = 0, trkTail = 0;   // steps recorded, steps read back
+  float trkMs[31] = {};
+  int trkN = 0, trkPos = 0;
+  float lastMs = 0.0f, slowMs = 0.0f;
   // counters read without waiting (st_flip_stats_async): a ring of pinned copies, each with its ticket and event
   static constexpr int STAT_SLOTS = 4;
   struct StatSlot { Ctl* h = nullptr; cudaEvent_t ev = nullptr; uint64_t ticket = 0, steps = 0, launches = 0; uint32_t n = 0; bool pending = false; };
@@ -205,6 +212,10 @@ void st_flip_destroy(st_flip* s) {
   for (auto& q : s->stat) {
     if (q.ev) cudaEventDestroy(q.ev);
     if (q.h) cudaFreeHost(q.h);
+  }
+  for (int k = 0; k < st_flip::TRK; k++) {
+    if (s->trkStart[k]) cudaEventDestroy(s->trkStart[k]);
+    if (s->trkDone[k]) cudaEventDestroy(s->trkDone[k]);
   }
   if (s->copyStream) cudaStreamDestroy(s->copyStream);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -654,6 +665,36 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   return ST_OK;
 }
 
+// a finished step's device time joins the last 31 (the median is lastMs) and the slowest so far (slowMs)
+static void trk_take(st_flip* s) {
+  const int k = (int)(s->trkTail % st_flip::TRK);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, s->trkStart[k], s->trkDone[k]);
+  s->trkMs[s->trkPos] = ms;
+  s->trkPos = (s->trkPos + 1) % 31;
+  if (s->trkN < 31) s->trkN++;
+  float r[31];
+  for (int i = 0; i < s->trkN; i++) r[i] = s->trkMs[i];
+  std::sort(r, r + s->trkN);
+  s->lastMs = r[s->trkN >> 1];
+  s->slowMs = std::max(s->slowMs, ms);
+  s->trkTail++;
+}
+// read back every finished step, in order; wait for the oldest first when the ring is full
+static st_status trk_poll(st_flip* s, bool full) {
+  if (full && s->trkHead - s->trkTail == (uint64_t)st_flip::TRK) {
+    CK(cudaEventSynchronize(s->trkDone[s->trkTail % st_flip::TRK]));
+    trk_take(s);
+  }
+  while (s->trkTail < s->trkHead) {
+    const cudaError_t e = cudaEventQuery(s->trkDone[s->trkTail % st_flip::TRK]);
+    if (e == cudaErrorNotReady) break;
+    CK(e);
+    trk_take(s);
+  }
+  return ST_OK;
+}
+
 // one step; t (optional) receives device ms per stage
 static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_times* t) {
   if (!s || !o || o->size != sizeof(st_step_opts)) return ST_BAD_ARG;
@@ -672,6 +713,14 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
     if (s->tcount >= (uint32_t)st_flip::TSLOTS) CK(cudaEventSynchronize(s->tev[s->tcount % st_flip::TSLOTS][10]));
     tslot = s->tev[s->tcount % st_flip::TSLOTS];
   }
+  if (!s->trkStart[0])
+    for (int k = 0; k < st_flip::TRK; k++) {
+      CK(cudaEventCreate(&s->trkStart[k]));
+      CK(cudaEventCreate(&s->trkDone[k]));
+    }
+  if ((st = trk_poll(s, true)) != ST_OK) return st;
+  const int tk = (int)(s->trkHead % st_flip::TRK);
+  CK(cudaEventRecord(s->trkStart[tk], q));
   int nl = 0;
   if (s->use_graphs && !t && !init) {
     st_flip::Graph* g = nullptr;
@@ -689,6 +738,8 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   }
   s->launches += (uint64_t)nl;
   CK(cudaGetLastError());
+  CK(cudaEventRecord(s->trkDone[tk], q));
+  s->trkHead++;
   s->steps++;
   if (tslot) s->tcount++;
   if (t) {
@@ -751,6 +802,17 @@ st_status st_flip_stats(st_flip* s, st_stats* out) {
   CK(cudaMemcpyAsync(s->hCtl, s->dCtl, sizeof(Ctl), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   stats_fill(*s->hCtl, s->N, s->steps, s->launches, out);
+  return ST_OK;
+}
+
+st_status st_flip_track(st_flip* s, uint32_t* inflight, float* last_ms, float* slow_ms) {
+  if (!s) return ST_BAD_ARG;
+  CK(cudaSetDevice(s->device));
+  st_status st = trk_poll(s, false);
+  if (st != ST_OK) return st;
+  if (inflight) *inflight = (uint32_t)(s->trkHead - s->trkTail);
+  if (last_ms) *last_ms = s->lastMs;
+  if (slow_ms) *slow_ms = s->slowMs;
   return ST_OK;
 }
 

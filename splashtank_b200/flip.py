@@ -193,7 +193,9 @@ class FlipSim:
         self.sprayCap = int(spray_cap)
         self.opt = {"noFoam": False, "noCull": False, "fastAir": False, "iters": 0}
         self.stats = None
-        self.lastMs = 0.0
+        self.lastMs = 0.0     # track(): median device ms of the last 31 finished steps
+        self.slowMs = 0.0     # the slowest step so far
+        self.inflight = 0     # steps queued and not yet finished
         self._pend_p, self._pend_v = [], []
         self._n_host = 0
 
@@ -277,7 +279,17 @@ class FlipSim:
         st = self.f["flip_step"](self._h, float(dt), C.byref(s))
         self._check(st, "step")
         del keep
+        self.track()
         return min(len(o.get("cols") or []), 32)
+
+    def track(self):
+        """track (src/gpu.js:444-454): refresh lastMs (median device time of the last 31 finished steps), slowMs and
+        inflight from the steps that have finished, without waiting for the rest."""
+        if "flip_track" not in self.f:
+            return
+        n, last, slow = C.c_uint32(), C.c_float(), C.c_float()
+        self._check(self.f["flip_track"](self._h, C.byref(n), C.byref(last), C.byref(slow)), "track")
+        self.inflight, self.lastMs, self.slowMs = n.value, last.value, slow.value
 
     def stepTimed(self, dt, o):
         """FlipSim.stepTimed (src/flip/sim.js:312-331): device ms per stage."""

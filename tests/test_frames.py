@@ -164,6 +164,30 @@ def test_async_stats_match_the_synchronous_ones():
 
 
 @pytest.mark.gpu
+def test_track_reports_step_times():
+    """track (src/gpu.js:444-454): once the queued steps have finished none is in flight, lastMs is the median of the
+    recent step times and slowMs the largest, and the median is near the device time the stage timer measures."""
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    tank = scenes.WaveTank(32, steps=60, spray_cap=20_000)
+    sim = tank.make(FlipSim)
+    run = SceneRunner(sim)
+    sim.track()
+    assert sim.inflight == 0 and sim.lastMs == 0.0 and sim.slowMs == 0.0
+    t = 0.0
+    for _ in range(12):
+        t += tank.dt
+        run.step(tank.dt, tank.states(t), tank.opts)
+    sim.readStats()   # waits for the stream
+    sim.track()
+    assert sim.inflight == 0
+    assert 0.0 < sim.lastMs <= sim.slowMs < 1000.0
+    timed = sim.stepTimed(tank.dt, dict(tank.opts, cols=[]))
+    sim.track()
+    assert sim.inflight == 0 and sim.lastMs < 5.0 * max(timed["total"], 0.05)
+
+
+@pytest.mark.gpu
 def test_bake_loop_writes_a_cache():
     from splashtank_b200.flip import FlipSim
     from splashtank_b200.scene import SceneRunner
