@@ -300,9 +300,16 @@ st_status st_flip_load_state(st_flip* s, const float* pos4, const float* vel4, c
 st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size);
 st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size);
 /* Narrow band start (nbSeed's sim.nbFills, src/shared.js:849-851): boxes as {x0,y0,z0,x1,y1,z1} and spheres as
- * {x,y,z,r}; the next step initialises the depth field from them (nbInit = mode). */
+ * {x,y,z,r}; the next step initialises the depth field from them (nbInit = mode). mode 2 (water added to a running
+ * tank) adds to the fills given since the last restart step; other modes replace them. */
 st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const float* spheres4, uint32_t nsph,
                            uint32_t mode);
+/* The water meshes of the same start (sim.nbFillVols, src/shared.js:829-831, 849-850): each a collider-shaped record
+ * (distance grid, position, rotation; velocities are ignored) whose negative distance is water. The next restart step
+ * packs them after its colliders (FlipSim.step, src/flip/sim.js:189-190) for fillPhi (wgsl-core.js:235) and then drops
+ * them; the grids are copied at the call. mode as for st_flip_nb_fills. Fill volumes pending at a full checkpoint are
+ * not stored in it. */
+st_status st_flip_nb_fill_vols(st_flip* s, const st_collider* vols, uint32_t n, uint32_t mode);
 /* The CUDA stream the handle enqueues on (a cudaStream_t), for events and graph capture by the caller. */
 void* st_flip_stream(st_flip* s);
 

@@ -95,6 +95,7 @@ struct Params {
   uint32_t airOn, aNx, aNy, aNz; float airCouple, airDecay, airH, airBlur;   // words 72-76, 82
   uint32_t ndrip; float dripRate, dripDry;                                    // words 79-81
   uint32_t ocean, nwave; float otime, olevel, olayer, oy0, odepth;            // words 57-61, 63, 66
+  uint32_t nfv;                                                               // word 67: fill volumes after the colliders
   float waves[24 * 8];                                                        // oceanWaves: 8 floats per wave
   float fills[16][4];
 };
@@ -135,6 +136,10 @@ struct Oracle {
   bool velGOn = false;
   uint32_t nbInit = 0;
   std::vector<float> fillsPacked;  // 8 floats per fill
+  // water-mesh fill volumes of the next restart (sim.nbFillVols, src/shared.js:849-850): records with owned grids
+  struct FillVol { st_sdf sd; std::vector<float> data; st_collider c; };
+  std::vector<FillVol> fillVols;
+  uint32_t nfv = 0;
   // time and seed (sim.js:200, 207)
   double tm = 0;
   uint32_t seed = 0, steps = 0;
@@ -331,6 +336,7 @@ struct Oracle {
         dd = fmin_(dd, length(x - v3(A[1], A[2], A[3])) - B[0]);
       }
     }
+    for (uint32_t k = P.ncols; k < P.ncols + P.nfv; k++) { float phi; V3 wn; sdfEval(k, x, phi, wn); dd = fmin_(dd, phi); }
     if (P.ocean != 0u) dd = fmin_(dd, x.y - oceanEta(x.x, x.z));
     return dd * P.ih;
   }
@@ -389,7 +395,7 @@ struct Oracle {
   }
   // FlipSim.clear (sim.js:539-547, gpu.js:389)
   void clear() {
-    N = 0; ring = 0; tm = 0; nbInit = 1; fillsPacked.clear();
+    N = 0; ring = 0; tm = 0; nbInit = 1; fillsPacked.clear(); fillVols.clear();
     std::fill(sPos.begin(), sPos.end(), 0.0f); sctl0 = 0;
     std::fill(air.begin(), air.end(), 0.0f);
     dripSig.clear();   // drip samples come back dry
@@ -461,7 +467,7 @@ struct Oracle {
     P.mistFrac = sprOn ? sp.mist : 0.0f; P.sprDrag = sprOn ? sp.drag : 1.0f; P.mistDrag = sprOn ? sp.mdrag : 4.0f; P.vs = o->vs != 0.0f ? o->vs : 1.0f;
     P.smax = sprayCap; P.seed = seed;
     P.nb = nbOn ? 1u : 0u; P.band = std::max(2.0f, o->nb_band != 0.0f ? o->nb_band : 3.0f); P.nbInit = init;
-    uint32_t nf = init ? (uint32_t)std::min<size_t>(fillsPacked.size() / 8, 8) : 0u; P.nfill = nf;
+    uint32_t nf = init ? (uint32_t)std::min<size_t>(fillsPacked.size() / 8, 8) : 0u; P.nfill = nf; P.nfv = nfv;
     memset(P.fills, 0, sizeof(P.fills));
     for (uint32_t k = 0; k < nf; k++) memcpy(P.fills[k * 2], &fillsPacked[k * 8], 8 * sizeof(float));
     P.wwFoamLife = sp.foam_life != 0.0f ? sp.foam_life : 3.0f; P.wwRise = sp.rise != 0.0f ? sp.rise : 0.3f;
@@ -1260,14 +1266,28 @@ struct Oracle {
     bool nbOn = o->nb_on != 0 || o->ocean_on != 0;
     if (nbOn && !velGOn) velGOn = true;
     uint32_t init = nbOn && nbInit ? nbInit : 0;
-    packCols(o);
+    // a restart packs the fill volumes after the step's colliders (FlipSim.step, src/flip/sim.js:189-190)
+    const uint32_t ncStep = std::min(o->ncols, 32u);
+    nfv = 0;
+    if (init && !fillVols.empty()) {
+      std::vector<st_collider> all(o->cols, o->cols + ncStep);
+      for (auto& f : fillVols) { all.push_back(f.c); all.back().sdf = &f.sd; f.sd.data = f.data.data(); }
+      st_step_opts o2 = *o;
+      o2.cols = all.data();
+      o2.ncols = (uint32_t)all.size();
+      packCols(&o2);
+      nfv = ncols - std::min(ncStep, ncols);
+      ncols -= nfv;
+    } else {
+      packCols(o);
+    }
     bool sprOn = o->spray_on != 0 && sprayCap > 0;
     if (sprOn && o->drip_on != 0) dripUpdate(o, ncols);
     lastN = N; lastNb = nbOn;
     seed = seed + 1u;
     packParams(dt, o, init, nbOn, sprOn);
     tm = tm + dt;
-    if (init) { nbInit = 0; fillsPacked.clear(); }
+    if (init) { nbInit = 0; fillsPacked.clear(); fillVols.clear(); }
     int iters = std::max(1, o->iters);
     stageBlocks(nbOn, init);
     stageClear();
@@ -1429,7 +1449,7 @@ st_status oracle_flip_load_state(void* h, const float* pos4, const float* vel4, 
 }
 st_status oracle_flip_nb_fills(void* h, const float* boxes6, uint32_t nbox, const float* sph4, uint32_t nsph, uint32_t mode) {
   Oracle* s = (Oracle*)h;
-  s->fillsPacked.clear();
+  if (mode != 2) s->fillsPacked.clear();   // water added to a running tank adds to the fills (src/shared.js:849)
   for (uint32_t k = 0; k < nbox; k++) {
     const float* b = &boxes6[k * 6];
     float f[8] = {1, b[0], b[1], b[2], b[3], b[4], b[5], 0}; s->fillsPacked.insert(s->fillsPacked.end(), f, f + 8);
@@ -1437,6 +1457,24 @@ st_status oracle_flip_nb_fills(void* h, const float* boxes6, uint32_t nbox, cons
   for (uint32_t k = 0; k < nsph; k++) {
     const float* q = &sph4[k * 4];
     float f[8] = {2, q[0], q[1], q[2], q[3], 0, 0, 0}; s->fillsPacked.insert(s->fillsPacked.end(), f, f + 8);
+  }
+  s->nbInit = mode ? mode : 1;
+  return ST_OK;
+}
+// nbSeed's sim.nbFillVols (src/shared.js:849-850): water meshes whose distance grids start the depth field
+st_status oracle_flip_nb_fill_vols(void* h, const st_collider* vols, uint32_t n, uint32_t mode) {
+  Oracle* s = (Oracle*)h;
+  if (n && !vols) return ST_BAD_ARG;
+  for (uint32_t k = 0; k < n; k++)
+    if (!vols[k].sdf || !vols[k].sdf->data) return ST_BAD_ARG;
+  if (mode != 2) s->fillVols.clear();
+  for (uint32_t k = 0; k < n; k++) {
+    Oracle::FillVol f;
+    f.sd = *vols[k].sdf;
+    f.data.assign(vols[k].sdf->data, vols[k].sdf->data + (size_t)f.sd.dims[0] * f.sd.dims[1] * f.sd.dims[2]);
+    f.c = vols[k];
+    for (int a = 0; a < 3; a++) { f.c.vel[a] = 0.0f; f.c.ang[a] = 0.0f; }
+    s->fillVols.push_back(std::move(f));
   }
   s->nbInit = mode ? mode : 1;
   return ST_OK;

@@ -124,6 +124,7 @@ FLIP_FUNCS = [
     ("flip_save_state", C.c_int, [C.c_void_p, f32p, f32p, u32p, C.c_uint32, u32p]),
     ("flip_load_state", C.c_int, [C.c_void_p, f32p, f32p, u32p, C.c_uint32, C.c_double, C.c_uint32]),
     ("flip_nb_fills", C.c_int, [C.c_void_p, f32p, C.c_uint32, f32p, C.c_uint32, C.c_uint32]),
+    ("flip_nb_fill_vols", C.c_int, [C.c_void_p, C.POINTER(Collider), C.c_uint32, C.c_uint32]),
 ]
 class BakeDiag(C.Structure):
     _fields_ = [("alive", C.c_uint32), ("gone", C.c_uint32), ("non_finite", C.c_uint32), ("outside_box", C.c_uint32),

@@ -61,6 +61,9 @@ struct st_flip {
   bool velGOn = false;
   uint32_t nbInit = 0;
   std::vector<float> fills;
+  // water-mesh fill volumes of the next restart (sim.nbFillVols, src/shared.js:849-850): records with owned grids
+  struct FillVol { st_sdf sd; std::vector<float> data; st_collider c; };
+  std::vector<FillVol> fillVols;
   std::string sdfSig;
   size_t sdfCap = 0;
   FlipParams hp{};
@@ -322,7 +325,7 @@ void* st_flip_stream(st_flip* s) { return s ? (void*)s->stream : nullptr; }
 st_status st_flip_clear(st_flip* s) {
   if (!s) return ST_BAD_ARG;
   cudaSetDevice(s->device);
-  s->N = 0; s->ring = 0; s->tm = 0; s->nbInit = 1; s->fills.clear(); s->steps = 0;
+  s->N = 0; s->ring = 0; s->tm = 0; s->nbInit = 1; s->fills.clear(); s->fillVols.clear(); s->steps = 0;
   if (s->sprayCap) {
     CK(cudaMemsetAsync(s->sPos, 0, (size_t)s->sprayCap * 16, s->stream));
     CK(cudaMemsetAsync(&s->dCtl->sctl0, 0, 4, s->stream));
@@ -632,9 +635,29 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   cudaEvent_t upEv = s->ring_ev[s->ring_i];
   s->ring_i = (s->ring_i + 1) % st_flip::RING;
   CK(cudaEventSynchronize(upEv));
-  uint32_t nc = 0;
-  st_status st = pack_colliders(s, o, nc, up->cols, q);
-  if (st != ST_OK) return st;
+  uint32_t nc = 0, nfv = 0;
+  st_status st;
+  if (init && !s->fillVols.empty()) {   // a restart packs the fill volumes after the colliders (src/flip/sim.js:189-190)
+    const uint32_t ncStep = std::min(o->ncols, 32u);
+    if (ncStep && !o->cols) return ST_BAD_ARG;
+    std::vector<st_collider> all;
+    if (ncStep) all.assign(o->cols, o->cols + ncStep);
+    for (auto& f : s->fillVols) {
+      f.sd.data = f.data.data();
+      all.push_back(f.c);
+      all.back().sdf = &f.sd;
+    }
+    st_step_opts o2 = *o;
+    o2.cols = all.data();
+    o2.ncols = (uint32_t)all.size();
+    st = pack_colliders(s, &o2, nc, up->cols, q);
+    if (st != ST_OK) return st;
+    nfv = nc - std::min(ncStep, nc);
+    nc -= nfv;
+  } else {
+    st = pack_colliders(s, o, nc, up->cols, q);
+    if (st != ST_OK) return st;
+  }
   const bool sprOn = o->spray_on != 0 && s->sprayCap > 0;
   if (sprOn && o->drip_on) {
     st = drip_update(s, o, nc, q);
@@ -643,19 +666,20 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   s->seed = s->seed + 1u;
   s->stamp = s->stamp + 1u;
   pack_params(s, dt, o, nc, init, nbOn, sprOn);
+  s->hp.nfv = nfv;
   s->tm = s->tm + dt;
   // the live view's water sample (src/flip/sim.js:184): every stride-th particle, at most about DISP_MAX
   s->stride = std::max<uint32_t>(1u, (uint32_t)((s->N + st_flip::DISP_MAX - 1) / st_flip::DISP_MAX));
   s->lastN = s->N;
   s->lastNb = nbOn;
-  if (init) { s->nbInit = 0; s->fills.clear(); }
+  if (init) { s->nbInit = 0; s->fills.clear(); s->fillVols.clear(); }
   const int iters = std::max(1, o->iters);
   // this step's storage order goes into the other particle buffer; cell counts alternate buffers
   s->cur ^= 1;
   s->parity ^= 1;
   up->P = s->hp;
   CK(cudaMemcpyAsync(&s->dUp->P, &up->P, sizeof(FlipParams), cudaMemcpyHostToDevice, q));
-  if (nc) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, nc * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
+  if (nc + nfv) CK(cudaMemcpyAsync(s->dUp->cols, up->cols, (nc + nfv) * 32 * sizeof(float), cudaMemcpyHostToDevice, q));
   if (s->hp.nwave) {
     memcpy(up->waves, s->waves, s->hp.nwave * 8 * sizeof(float));
     CK(cudaMemcpyAsync(s->dUp->waves, up->waves, s->hp.nwave * 8 * sizeof(float), cudaMemcpyHostToDevice, q));
@@ -1315,7 +1339,7 @@ st_status st_flip_load_state(st_flip* s, const float* pos4, const float* vel4, c
 
 st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const float* sph4, uint32_t nsph, uint32_t mode) {
   if (!s || (nbox && !boxes6) || (nsph && !sph4)) return ST_BAD_ARG;
-  s->fills.clear();
+  if (mode != 2) s->fills.clear();   // water added to a running tank adds to the fills (src/shared.js:849)
   for (uint32_t k = 0; k < nbox; k++) {
     const float* b = &boxes6[k * 6];
     float f[8] = {1, b[0], b[1], b[2], b[3], b[4], b[5], 0};
@@ -1330,6 +1354,23 @@ st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const
   return ST_OK;
 }
 
+
+st_status st_flip_nb_fill_vols(st_flip* s, const st_collider* vols, uint32_t n, uint32_t mode) {
+  if (!s || (n && !vols)) return ST_BAD_ARG;
+  for (uint32_t k = 0; k < n; k++)
+    if (!vols[k].sdf || !vols[k].sdf->data) return ST_BAD_ARG;
+  if (mode != 2) s->fillVols.clear();
+  for (uint32_t k = 0; k < n; k++) {
+    st_flip::FillVol f;
+    f.sd = *vols[k].sdf;
+    f.data.assign(vols[k].sdf->data, vols[k].sdf->data + (size_t)f.sd.dims[0] * f.sd.dims[1] * f.sd.dims[2]);
+    f.c = vols[k];
+    for (int a = 0; a < 3; a++) { f.c.vel[a] = 0.0f; f.c.ang[a] = 0.0f; }
+    s->fillVols.push_back(std::move(f));
+  }
+  s->nbInit = mode ? mode : 1;
+  return ST_OK;
+}
 
 // ---- full checkpoint: every buffer a step reads before it writes, plus the host step state ----
 struct FullHdr {

@@ -39,7 +39,8 @@ struct FlipParams {
   float dripRate, dripDry;
   uint32_t ocean, nwave;                  // ocean (words 57-61, 63, 66; the waves follow the collider records)
   float otime, olevel, olayer, oy0, odepth;
-  uint32_t padW[2];
+  uint32_t nfv;                           // water-mesh fill volumes after the colliders (word 67), on a restart step
+  uint32_t padW[1];
   float fills[16][4];
 };
 // the collider records follow the block in the upload buffer and are read as float4
@@ -304,23 +305,6 @@ __device__ __forceinline__ float layerW(const FlipParams& P, V3 p) {
   const float dw = fmn(fmn(p.x - P.x0, P.x1 - p.x), fmn(p.z - P.z0, P.z1 - p.z));
   return clampf(1.0f - dw / fmx(P.olayer, 1.0e-4f), 0.0f, 1.0f);
 }
-// fillPhi (wgsl-core.js:227-238): signed distance in cells to the starting water, boxes, spheres and the ocean
-__device__ __forceinline__ float fillPhi(const FlipParams& P, const float4* __restrict__ W, V3 x) {
-  float d = 1.0e9f;
-  for (uint32_t k = 0; k < P.nfill; k++) {
-    const float* A = P.fills[k * 2];
-    const float* Bq = P.fills[k * 2 + 1];
-    if (A[0] < 1.5f) {
-      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
-      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
-    } else {
-      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
-    }
-  }
-  if (P.ocean != 0u) d = fmn(d, x.y - oceanEta(P, W, x.x, x.z));
-  return d * P.ih;
-}
-
 // ---- colliders (src/gpu.js:6-38, src/flip/wgsl-core.js:113-126) ----
 __device__ __forceinline__ void sdfEval(const float4* __restrict__ cols, const float* __restrict__ sdf, uint32_t k, V3 p,
                                         float& phi, V3& wn) {
@@ -354,6 +338,31 @@ __device__ __forceinline__ void sdfEval(const float4* __restrict__ cols, const f
   }
   wn = r0 * gl.x + r1 * gl.y + r2 * gl.z;
 }
+// fillPhi (wgsl-core.js:227-238): signed distance in cells to the starting water: boxes, spheres, water meshes (the
+// distance grids of the fill volumes, records ncols .. ncols + nfv - 1 after the colliders) and the ocean
+__device__ __forceinline__ float fillPhi(const FlipParams& P, const float4* __restrict__ W, const float4* __restrict__ cols,
+                                         const float* __restrict__ sdf, V3 x) {
+  float d = 1.0e9f;
+  for (uint32_t k = 0; k < P.nfill; k++) {
+    const float* A = P.fills[k * 2];
+    const float* Bq = P.fills[k * 2 + 1];
+    if (A[0] < 1.5f) {
+      V3 q = vmax(v3(A[1], A[2], A[3]) - x, x - v3(Bq[0], Bq[1], Bq[2]));
+      d = fmn(d, len3(vmax(q, v3(0.0f, 0.0f, 0.0f))) + fmn(fmx(q.x, fmx(q.y, q.z)), 0.0f));
+    } else {
+      d = fmn(d, len3(x - v3(A[1], A[2], A[3])) - Bq[0]);
+    }
+  }
+  for (uint32_t k = P.ncols; k < P.ncols + P.nfv; k++) {
+    float phi;
+    V3 wn;
+    sdfEval(cols, sdf, k, x, phi, wn);
+    d = fmn(d, phi);
+  }
+  if (P.ocean != 0u) d = fmn(d, x.y - oceanEta(P, W, x.x, x.z));
+  return d * P.ih;
+}
+
 __device__ __forceinline__ V3 colSurfVel(const float4* __restrict__ cols, uint32_t k, V3 p) {
   V3 c = xyz(cols[k * 8 + 5]);
   return xyz(cols[k * 8 + 6]) + cross3(xyz(cols[k * 8 + 7]), p - c);

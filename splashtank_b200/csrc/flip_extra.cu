@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(512) k_nb_init(Bufs B) {
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
-    float ph = clampf(fillPhi(P, B.waves, cellCenter(P, i, j, k)), -7.9f, 7.9f);
+    float ph = clampf(fillPhi(P, B.waves, B.cols, B.sdf, cellCenter(P, i, j, k)), -7.9f, 7.9f);
     if (ph < 0.0f) ph = fmn(ph, -1.5f);
     if (!inDom(P, i, j, k)) ph = 8.0f;
     const uint32_t ct = B.ctype[c];

@@ -117,7 +117,7 @@ __global__ void k_mark_fill(Bufs B) {
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < P.ntiles; t += gridDim.x * blockDim.x) {
     uint32_t tt = t / P.tx;
     V3 tc = v3((float)(t % P.tx), (float)(tt % P.ty), (float)(tt / P.ty)) * 8.0f + v3(4.0f, 4.0f, 4.0f);
-    if (fillPhi(P, B.waves, v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) B.need[t] = P.stamp;
+    if (fillPhi(P, B.waves, B.cols, B.sdf, v3(P.x0, P.y0, P.z0) + tc * P.h) < 9.0f) B.need[t] = P.stamp;
   }
 }
 

@@ -592,6 +592,12 @@ class FlipSim:
         s = np.ascontiguousarray(np.array(spheres, np.float32).reshape(-1, 4))
         self._check(self.f["flip_nb_fills"](self._h, b.ctypes.data_as(abi.f32p), len(b), s.ctypes.data_as(abi.f32p), len(s), int(mode)), "nb_fills")
 
+    def nb_fill_vols(self, vols=(), mode=1):
+        """Water meshes of the narrow band's start (sim.nbFillVols written by nbSeed, src/shared.js:829-831, 849-850):
+        collider-shaped dicts (sdf, x, y, z, R) whose negative distance is water; the next restart step reads them."""
+        pack = _ColliderPack(list(vols))
+        self._check(self.f["flip_nb_fill_vols"](self._h, C.cast(pack.arr, C.POINTER(abi.Collider)), pack.n, int(mode)), "nb_fill_vols")
+
     def stream(self):
         return self.f["flip_stream"](self._h)
 

@@ -209,6 +209,60 @@ def test_ragged_box_open_face_collider_and_whitewater():
     assert_same_state(g, o, spray=True)
 
 
+def test_fill_volume_restart_with_a_collider():
+    """A restart whose starting water is a water mesh (a fill volume's distance grid, packed after the colliders) and
+    a box fill, next to a moving sphere collider, narrow band of 3 cells: 6 steps bit for bit."""
+    from test_oracle import shell_drop
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner, sphere_sdf
+    r, c = 0.22, (0.0, 0.45, 0.0)
+    g, opts = shell_drop(FlipSim, r=r, c=c)
+    o, _ = shell_drop(OracleFlipSim, r=r, c=c, threads=8)
+    vol = dict(sdf=sphere_sdf(r, g.h / 2, sid=9), x=c[0], y=c[1], z=c[2])
+    col = sphere_sdf(0.08, g.h / 2, sid=5)
+    for s in (g, o):
+        s.nb_fill_vols([vol])
+        s.nb_fills(boxes=[(-0.5, 0.0, -0.5, 0.5, 0.06, 0.5)])
+    runs, t, dt = [SceneRunner(s) for s in (g, o)], 0.0, 1.0 / 240.0
+    for _ in range(6):
+        t += dt
+        st = [dict(id=1, sdf=col, x=0.3 - 0.5 * t, y=0.3, z=0.0)]
+        for rr in runs:
+            rr.step(dt, st, opts)
+    assert_same_state(g, o)
+
+
+def test_water_added_to_a_running_tank():
+    """nbSeed's mode 2 (water added to a running tank, src/shared.js:849): after 5 steps a second ball is added as a
+    fill volume and its band particles; the depth field keeps the old water and gains the new: 5 more steps bit for
+    bit."""
+    from test_oracle import shell_drop
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import sphere_sdf
+    r, c = 0.22, (0.0, 0.45, 0.0)
+    g, opts = shell_drop(FlipSim, r=r, c=c)
+    o, _ = shell_drop(OracleFlipSim, r=r, c=c, threads=8)
+    for s in (g, o):
+        s.nb_fills(spheres=[(c[0], c[1], c[2], r)])
+    dt = 1.0 / 240.0
+    for _ in range(5):
+        for s in (g, o):
+            s.step(dt, opts)
+    r2, c2 = 0.1, (-0.25, 0.75, 0.2)
+    add, _ = shell_drop(OracleFlipSim, r=r2, c=c2, band=2.0, seed=8)
+    p2 = add.save_state()[0][:, :3]
+    vol = dict(sdf=sphere_sdf(r2, g.h / 2, sid=11), x=c2[0], y=c2[1], z=c2[2])
+    for s in (g, o):
+        s.add_many(p2)
+        s.nb_fill_vols([vol], mode=2)
+    for _ in range(5):
+        for s in (g, o):
+            s.step(dt, opts)
+    assert_same_state(g, o)
+
+
 def test_particle_state_round_trip():
     """save_state -> load_state -> save_state returns the same particles, ids and storage order."""
     from splashtank_b200 import scenes

@@ -130,6 +130,43 @@ def test_narrow_band_full_depth_keeps_particles():
     assert (phi[deep] < 0.5).mean() > 0.9                     # water cells carry a negative depth
 
 
+def shell_drop(cls, n=24, r=0.22, c=(0.0, 0.45, 0.0), band=3.0, seed=4, **kw):
+    """A ball of water with particles only in the narrow band under its surface (nbSeed's 'vol' and sphere branches,
+    src/shared.js:806-847, with seeded jitter): the tank, the particles and the step options."""
+    h = 1.0 / n
+    rng = np.random.default_rng(seed)
+    cells = scenes.box_cells((n, n, n), lambda ci, cj, ck: np.abs(np.sqrt((ci * h - 0.5 - c[0]) ** 2 + (cj * h - c[1]) ** 2 +
+                                                                           (ck * h - 0.5 - c[2]) ** 2) - (r - 0.5 * band * h)) < 0.5 * band * h)
+    pos = scenes.seed_cells(cells, h, rng, -0.5, 0.0, -0.5)
+    s = cls(h / 2, len(pos) + 4000, size=(1.0, 1.0, 1.0), **kw)
+    s.add_many(pos)
+    opts = dict(g=9.81, flip=0.95, comp=6.0, iters=30, vmax=14.0, nb=dict(on=True, band=band))
+    return s, opts
+
+
+def test_fill_volume_starts_the_depth_field_like_its_shape():
+    """A water mesh given as a fill volume (its distance grid, fillPhi's loop over the records after the colliders,
+    wgsl-core.js:235) starts the depth field as the same ball given as a sphere fill does, to the grid's interpolation
+    error; a restart consumes the fills, so a second restart without new ones starts from air."""
+    from splashtank_b200.scene import sphere_sdf
+    r, c = 0.22, (0.0, 0.45, 0.0)
+    a, opts = shell_drop(OracleFlipSim, r=r, c=c, threads=4)
+    b, _ = shell_drop(OracleFlipSim, r=r, c=c, threads=4)
+    a.nb_fills(spheres=[(c[0], c[1], c[2], r)])
+    b.nb_fill_vols([dict(sdf=sphere_sdf(r, a.h / 2, sid=9), x=c[0], y=c[1], z=c[2])])
+    for s in (a, b):
+        s.step(1.0 / 240.0, opts)
+    phi = [8.0 - (s.grid()["ctype"] >> 16) / 4096.0 for s in (a, b)]
+    on = a.grid()["tile_on"].astype(bool)
+    assert np.array_equal(on, b.grid()["tile_on"].astype(bool))
+    near = phi[0] < 1.0   # inside the ball and a cell around it, where the distance grid reaches
+    assert near.sum() > 1000 and (phi[0][near] < 0).sum() > 500
+    assert np.max(np.abs(phi[0][near] - phi[1][near])) < 0.05
+    assert phi[1].min() < -4.0   # deeper than the particles alone make it (about -2.5 from a band of 3)
+    st = [s.readStats() for s in (a, b)]
+    assert st[0]["live"] == st[1]["live"] and st[0]["fluid"] > 0
+
+
 def test_air_field_settles_to_the_wind():
     """With no coupling, every air cell relaxes towards the wind by 1 - exp(-decay dt) a step (airUpdate,
     src/flip/wgsl-whitewater.js:67-86); a uniform field stays uniform under the blur. The grid is airAlloc's
