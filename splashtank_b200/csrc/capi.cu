@@ -166,7 +166,8 @@ struct st_flip {
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
     B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
     B.waves = reinterpret_cast<const float4*>(dUp->waves);
-    B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.drip = drip; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
+    B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.drip = drip; B.dripTmp = drip ? drip + 2 * (size_t)dripCap : nullptr;
+    B.dripCnt = drip ? reinterpret_cast<uint32_t*>(drip + 4 * (size_t)dripCap) : nullptr; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
     B.ncell = ncell; B.nblk = (N + PBLK - 1) / PBLK;
     return B;
   }
@@ -424,6 +425,9 @@ static st_status pack_colliders(st_flip* s, const st_step_opts* o, uint32_t& nc,
   return ST_OK;
 }
 
+// float4s of the drip buffer for n samples: the samples (2 each), the pass's scratch (2 each) and the chunk counts
+static size_t drip_words(uint32_t n) { return 4 * (size_t)n + ((size_t)n / DRIP_T + 4 + 3) / 4; }
+
 // dripUpdate (src/flip/sim.js:352-363): the samples of every collider's distance grid, rebuilt when the grids of the
 // colliders (in collider order) change; a rebuilt set starts dry
 static st_status drip_update(st_flip* s, const st_step_opts* o, uint32_t nc, cudaStream_t q) {
@@ -451,7 +455,7 @@ static st_status drip_update(st_flip* s, const st_step_opts* o, uint32_t nc, cud
     if (s->drip) cudaFree(s->drip);
     s->drip = nullptr;
     s->dripCap = 0;
-    CK(dalloc(&s->drip, 2 * (size_t)n));
+    CK(dalloc(&s->drip, drip_words(n)));
     s->dripCap = n;
   }
   if (n) {
@@ -552,7 +556,7 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(7);
   nl += launch_g2p(B, gT, ocean, q);
   mark(8);
-  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, s->hp.ndrip != 0, gT4, q);
+  if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, s->hp.ndrip != 0 ? s->dripCap : 0u, gT4, q);
   mark(9);
   if (nbOn) nl += launch_nb_reseed(B, gT4, q);
   mark(10);
@@ -991,7 +995,7 @@ st_status st_flip_mem_bytes(st_flip* s, uint64_t* bytes) {
   b += s->frame ? (uint64_t)s->maxN * 8 + 16 : 0;
   b += s->diag ? sizeof(DiagAcc) : 0;
   b += s->deepBuf ? (uint64_t)st_flip::DEEP_MAX * sizeof(float4) : 0;
-  b += (uint64_t)s->viewScratchN * 4 + (uint64_t)s->liveWords * 4 + s->framePartBytes + (uint64_t)s->dripCap * 32;
+  b += (uint64_t)s->viewScratchN * 4 + (uint64_t)s->liveWords * 4 + s->framePartBytes + (uint64_t)drip_words(s->dripCap) * 16;
   *bytes = b;
   return ST_OK;
 }
@@ -1441,7 +1445,7 @@ st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
     if (s->drip) cudaFree(s->drip);
     s->drip = nullptr;
     s->dripCap = 0;
-    CK(dalloc(&s->drip, 2 * (size_t)h.ndrip));
+    CK(dalloc(&s->drip, drip_words(h.ndrip)));
     s->dripCap = h.ndrip;
   }
   s->ndrip = h.ndrip;

@@ -117,6 +117,8 @@ struct Bufs {
   float4* air2;
   int32_t* airAcc;      // 4 per air cell: sum of v w 256 (x, y, z) and of w 256
   float4* drip;         // 2 per drip sample (dripSamples, src/flip/bake.js:19-40): local position + collider, local normal + wetness
+  float4* dripTmp;      // 2 per drip sample: the probe point (w: 1 when it drips this step) and the drop's velocity
+  uint32_t* dripCnt;    // drops per chunk of DRIP_T samples, then their exclusive offsets, the total and the ring start
   const float4* waves;  // ocean: 2 per wave, (kx, kz, amplitude, angular frequency) and (phase, wavenumber, 0, 0)
   // colliders
   const float4* cols;   // 8 per collider (src/gpu.js:3-4)

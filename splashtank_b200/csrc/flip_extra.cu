@@ -534,55 +534,75 @@ __global__ void k_emit_done(Bufs B) {
 // P.dripDry seconds out of it, letting go of drops while they dry. The reference hands out ring slots with an atomic in
 // arbitrary order; here one CTA walks the samples in ascending order and numbers the drops with block scans, so drop
 // r goes to slot (sctl[0] + r) % smax. Drops beyond smax in one pass are not written (their slots would repeat).
-__global__ void __launch_bounds__(1024) k_drip(Bufs B) {
+// Three passes so that every SM takes part: each CTA tests one chunk of DRIP_T samples and counts its drops, one CTA
+// turns the counts into offsets, then each chunk writes its drops into the ring in sample order (the order of the
+// reference's single loop, so the slots are the same).
+__global__ void __launch_bounds__(DRIP_T) k_drip_test(Bufs B) {
   __shared__ FlipParams P;
-  __shared__ uint32_t sm[33];
   loadParams(P, B.P);
-  const uint32_t nd = P.ndrip, s0ring = B.ctl->sctl0;
-  uint32_t base = 0;
-  for (uint32_t c0 = 0; c0 < nd; c0 += blockDim.x) {
-    const uint32_t s = c0 + threadIdx.x;
-    uint32_t want = 0;
-    V3 probe = v3(0.0f, 0.0f, 0.0f), nv = probe;
-    if (s < nd) {
-      const float4 a = B.drip[2 * s], b = B.drip[2 * s + 1];
-      const uint32_t k = u32f(a.w);
-      if (k < P.ncols) {
-        const V3 r0 = xyz(B.cols[k * 8 + 2]), r1 = xyz(B.cols[k * 8 + 3]), r2 = xyz(B.cols[k * 8 + 4]);
-        const V3 wp = xyz(B.cols[k * 8 + 5]) + r0 * a.x + r1 * a.y + r2 * a.z;
-        const V3 wr = r0 * b.x + r1 * b.y + r2 * b.z;
-        const V3 wn = wr / len3(wr);
-        probe = wp + wn * P.h * 0.75f;
-        const float here = wetAt(P, B, probe);
-        if (here > 0.4f) {
-          B.drip[2 * s + 1] = make_float4(b.x, b.y, b.z, 1.0f);
-        } else {
-          const float wetness = fmx(0.0f, b.w - P.dt / fmx(P.dripDry, 0.05f));
-          B.drip[2 * s + 1] = make_float4(b.x, b.y, b.z, wetness);
-          if (!(wetness <= 0.0f || here > 0.1f || P.smax == 0u || P.dripRate <= 0.0f)) {
-            const float down = clampf(-wn.y, 0.0f, 1.0f);
-            const float rate = P.dripRate * wetness * wetness * (0.15f + 0.85f * down);
-            const uint32_t h0 = s * 747796405u + P.seed * 2891336453u + 17u;
-            if (hash1(h0) < rate * P.dt) {
-              want = 1;
-              nv = colSurfVel(B.cols, k, wp) + wn * P.h * 2.0f * hash1(h0 + 1u);
-            }
+  const uint32_t nd = P.ndrip, s = blockIdx.x * DRIP_T + threadIdx.x;
+  if (blockIdx.x * DRIP_T >= nd) return;   // a chunk past the samples (the grid covers the buffer's capacity)
+  uint32_t want = 0;
+  V3 probe = v3(0.0f, 0.0f, 0.0f), nv = probe;
+  if (s < nd) {
+    const float4 a = B.drip[2 * s], b = B.drip[2 * s + 1];
+    const uint32_t k = u32f(a.w);
+    if (k < P.ncols) {
+      const V3 r0 = xyz(B.cols[k * 8 + 2]), r1 = xyz(B.cols[k * 8 + 3]), r2 = xyz(B.cols[k * 8 + 4]);
+      const V3 wp = xyz(B.cols[k * 8 + 5]) + r0 * a.x + r1 * a.y + r2 * a.z;
+      const V3 wr = r0 * b.x + r1 * b.y + r2 * b.z;
+      const V3 wn = wr / len3(wr);
+      probe = wp + wn * P.h * 0.75f;
+      const float here = wetAt(P, B, probe);
+      if (here > 0.4f) {
+        B.drip[2 * s + 1] = make_float4(b.x, b.y, b.z, 1.0f);
+      } else {
+        const float wetness = fmx(0.0f, b.w - P.dt / fmx(P.dripDry, 0.05f));
+        B.drip[2 * s + 1] = make_float4(b.x, b.y, b.z, wetness);
+        if (!(wetness <= 0.0f || here > 0.1f || P.smax == 0u || P.dripRate <= 0.0f)) {
+          const float down = clampf(-wn.y, 0.0f, 1.0f);
+          const float rate = P.dripRate * wetness * wetness * (0.15f + 0.85f * down);
+          const uint32_t h0 = s * 747796405u + P.seed * 2891336453u + 17u;
+          if (hash1(h0) < rate * P.dt) {
+            want = 1;
+            nv = colSurfVel(B.cols, k, wp) + wn * P.h * 2.0f * hash1(h0 + 1u);
           }
         }
       }
     }
-    uint32_t tot;
-    const uint32_t run = base + blockExclusive(want, sm, &tot);
-    base += tot;
-    if (want && run < P.smax) {
-      const uint32_t slot = (uint32_t)(((uint64_t)s0ring + run) % P.smax);
-      if (!(B.sPos[slot].w > 0.0f)) {
-        B.sPos[slot] = make_float4(probe.x, probe.y, probe.z, P.sprLife * 2.0f);
-        B.sVel[slot] = make_float4(nv.x, nv.y, nv.z, 0.0f);
-      }
+    B.dripTmp[2 * s] = make_float4(probe.x, probe.y, probe.z, want ? 1.0f : 0.0f);
+    B.dripTmp[2 * s + 1] = make_float4(nv.x, nv.y, nv.z, 0.0f);
+  }
+  const uint32_t cnt = (uint32_t)__syncthreads_count(want != 0u);
+  if (threadIdx.x == 0) B.dripCnt[blockIdx.x] = cnt;
+}
+__global__ void __launch_bounds__(1024) k_drip_scan(Bufs B) {
+  __shared__ uint32_t sm[33];
+  const uint32_t nd = B.P->ndrip, nch = (nd + DRIP_T - 1) / DRIP_T;
+  const uint32_t s0ring = B.ctl->sctl0;
+  scanOne(B.dripCnt, nch, nullptr, sm);   // dripCnt[nch] = the drops of this step
+  if (threadIdx.x == 0) {
+    B.dripCnt[nch + 1] = s0ring;
+    B.ctl->sctl0 = s0ring + B.dripCnt[nch];
+  }
+}
+__global__ void __launch_bounds__(DRIP_T) k_drip_write(Bufs B) {
+  __shared__ FlipParams P;
+  __shared__ uint32_t sm[33];
+  loadParams(P, B.P);
+  const uint32_t nd = P.ndrip, nch = (nd + DRIP_T - 1) / DRIP_T, s = blockIdx.x * DRIP_T + threadIdx.x;
+  if (blockIdx.x >= nch) return;
+  const float4 pr = s < nd ? B.dripTmp[2 * s] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const uint32_t want = pr.w > 0.5f ? 1u : 0u;
+  const uint32_t run = B.dripCnt[blockIdx.x] + blockExclusive(want, sm, nullptr);
+  if (want && run < P.smax) {
+    const uint32_t slot = (uint32_t)(((uint64_t)B.dripCnt[nch + 1] + run) % P.smax);
+    if (!(B.sPos[slot].w > 0.0f)) {
+      const float4 nv = B.dripTmp[2 * s + 1];
+      B.sPos[slot] = make_float4(pr.x, pr.y, pr.z, P.sprLife * 2.0f);
+      B.sVel[slot] = make_float4(nv.x, nv.y, nv.z, 0.0f);
     }
   }
-  if (threadIdx.x == 0) B.ctl->sctl0 = s0ring + base;
 }
 
 // ---- launchers: each returns how many kernels it launched ----
@@ -603,7 +623,7 @@ int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
   k_spawn<<<grid, 512, 0, s>>>(B);
   return 5;
 }
-int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, bool drip, int grid, cudaStream_t s) {
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, uint32_t dripCap, int grid, cudaStream_t s) {
   if (!smax) return 0;
   int nl = 0;
   if (airCells) {   // the air field first, so the whitewater moves with this step's air (src/flip/sim.js:297-301)
@@ -622,9 +642,12 @@ int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, boo
     k_emit_done<<<1, 1, 0, s>>>(B);
     nl += 3;
   }
-  if (drip) {
-    k_drip<<<1, 1024, 0, s>>>(B);
-    nl++;
+  if (dripCap) {
+    const int nch = (int)((dripCap + DRIP_T - 1) / DRIP_T);
+    k_drip_test<<<nch, DRIP_T, 0, s>>>(B);
+    k_drip_scan<<<1, 1024, 0, s>>>(B);
+    k_drip_write<<<nch, DRIP_T, 0, s>>>(B);
+    nl += 3;
   }
   return nl;
 }

@@ -29,7 +29,8 @@ int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s);
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s);
 // whitewater (flip_extra.cu)
 // airCells: air-field cells to step first (0 when the air field is off this step); drip: step the drip samples last
-int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, bool drip, int grid, cudaStream_t s);
+constexpr uint32_t DRIP_T = 1024;   // drip samples per chunk (one CTA)
+int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, uint32_t dripCap, int grid, cudaStream_t s);
 // drip samples of one collider's distance grid (drips.cpp), appended to out: 8 floats each
 void drip_samples(const st_sdf* sdf, double h, uint32_t k, std::vector<float>& out);
 // the ocean's wave list (ocean.cpp): 8 floats per wave into w (room for 24); returns the number of waves
