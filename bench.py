@@ -2,7 +2,7 @@
 """Benchmark of the B200 FLIP step: particle-steps/s on the full-feature 256^3 wave tank (one JSON line).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload wave_tank_256|dam_break_64|pressure_512|batch_64]
+                [--workload wave_tank_256|dam_break_64|pressure_512|batch_64|diff_128]
 
 One process per GPU (torchrun for N > 1, NCCL only for the barrier and the max/sum of the numbers). The FLIP step of
 one tank does not shard, so N GPUs run N independent replica tanks (weak scaling) and value is the total over them.
