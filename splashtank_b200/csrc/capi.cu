@@ -748,7 +748,6 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
     }
   if ((st = trk_poll(s, true)) != ST_OK) return st;
   const int tk = (int)(s->trkHead % st_flip::TRK);
-  CK(cudaEventRecord(s->trkStart[tk], q));
   int nl = 0;
   if (s->use_graphs && !t && !init) {
     st_flip::Graph* g = nullptr;
@@ -756,9 +755,11 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
     if (st != ST_OK) return st;
     if (tslot)
       for (int k = 0; k < st_flip::TEV; k++) CK(cudaGraphExecEventRecordNodeSetEvent(g->exec, g->evnode[k], tslot[k]));
+    CK(cudaEventRecord(s->trkStart[tk], q));   // after the host work, so a new graph's instantiation is not timed
     CK(cudaGraphLaunch(g->exec, q));
     nl = g->launches;
   } else {
+    CK(cudaEventRecord(s->trkStart[tk], q));
     nl = enqueue_step(s, B, q, nbOn, init, sprOn, iters, [&](int k) {
       if (t) cudaEventRecord(s->ev[k], q);
       if (tslot) cudaEventRecord(tslot[k], q);
