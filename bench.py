@@ -29,6 +29,9 @@ sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
+# what limits each kernel instead, from the same captures (profiles/flip_kernels_wave_tank_128.md)
+NCU_LIMITER = {"g2p": "instruction issue: 59% issue active at 16 warps per SM, 1,318 instructions per particle",
+               "p2g": "shared-memory atomics: L1 pipe 84% busy, 3.2 wavefronts per atomic"}
 NCU_TRAFFIC = {"g2p": {"bytes": 180631296 + 105086464, "particles": 4669521},
                "p2g": {"bytes": 209715200 + 135951360, "particles": 4669521}}
 FALLBACK_HBM = 6650.0
@@ -176,7 +179,7 @@ def roofline(stage_ms, nsteps, n, cells, fluid, iters, peak, peak_src):
     return {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src, "traffic": traffic,
             "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per_launch_ms, 5),
-            "stage_share": round(stage_ms[dom] / stage_ms["total"], 4)}
+            "stage_share": round(stage_ms[dom] / stage_ms["total"], 4), "limiter": NCU_LIMITER.get(dom)}
 
 
 def measured_peak():
