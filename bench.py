@@ -28,10 +28,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
-# what limits each kernel instead, from ncu captures of the same kernels on the 128^3 wave tank
+# what limits each kernel instead of DRAM bandwidth, from ncu captures of the same kernels on the 128^3 wave tank
 NCU_LIMITER = {"g2p": "instruction issue: 59% issue active at 16 warps per SM, 1,318 instructions per particle",
                "p2g": "shared-memory atomics: L1 pipe 84% busy, 3.2 wavefronts per atomic"}
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
 NCU_TRAFFIC = {"g2p": {"bytes": 180631296 + 105086464, "particles": 4669521},
                "p2g": {"bytes": 209715200 + 135951360, "particles": 4669521}}
 FALLBACK_HBM = 6650.0
