@@ -297,16 +297,18 @@ def test_deterministic_repeat():
         assert same(x, y)
 
 
-def test_large_tank_invariants():
-    """128^3 tank (about 4.7M particles), no oracle: properties that hold at any size."""
+@pytest.mark.parametrize("n,steps,cap", [(128, 20, 500_000), (256, 6, 4_000_000)])
+def test_large_tank_invariants(n, steps, cap):
+    """128^3 (about 4.7M particles) and the benchmark's 256^3 tank (about 38.6M) with the air field, drips, whitewater
+    and the narrow band at full depth, no oracle: properties that hold at any size."""
     from splashtank_b200 import scenes
     from splashtank_b200.flip import FlipSim
     from splashtank_b200.scene import SceneRunner
-    w = scenes.WaveTank(128, spray_cap=500000)
+    w = scenes.WaveTank(n, spray_cap=cap)
     s = w.make(FlipSim)
     r = SceneRunner(s)
     t = 0.0
-    for _ in range(20):
+    for _ in range(steps):
         t += w.dt
         r.step(w.dt, w.states(t), w.opts)
     st = s.readStats()
