@@ -29,7 +29,7 @@ __device__ __forceinline__ void markAround(const FlipParams& P, uint32_t* __rest
 // dependent steps and barriers of one another.
 constexpr int CM_T = 256, CM_U = PBLK / CM_T;
 static_assert(CM_U == 4, "k_scatter packs the dead counts of four slices into two scans");
-__global__ void __launch_bounds__(CM_T, 4) k_count_mark(Bufs B) {
+__global__ void __launch_bounds__(CM_T, 5) k_count_mark(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float wmax[CM_T / 32];
   __shared__ uint32_t wdead[CM_T / 32];
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(1024) k_scan_counts(Bufs B) {
 // ---- 4. scatter: sorted position of every particle ----
 // Live: (tile offset + cell offset + rank from the atomic count); the order inside a cell is fixed to ascending id by
 // p2g. Dead: after all live ones, in storage order (a block scan keeps it stable); they are moved here directly.
-__global__ void __launch_bounds__(CM_T, 4) k_scatter(Bufs B) {
+__global__ void __launch_bounds__(CM_T, 6) k_scatter(Bufs B) {
   __shared__ FlipParams P;
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
