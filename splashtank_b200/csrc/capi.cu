@@ -1378,30 +1378,41 @@ st_status st_flip_nb_fill_vols(st_flip* s, const st_collider* vols, uint32_t n, 
 }
 
 // ---- full checkpoint: every buffer a step reads before it writes, plus the host step state ----
+// Layout: header, pending fills (floats), drip-grid signature (padded to 4 bytes), pending fill volumes (per volume 20
+// words of record - id, dims, origin, cell, pos, R - then its grid), then the device buffers of full_parts in order.
 struct FullHdr {
   uint32_t magic, version, nx, ny, nz, ntiles, ncell, maxN, sprayCap;
-  uint32_t N, cap, ring, seed, steps, stamp, parity, cur, velGOn, nbInit, nfills, ndrip, nsig, pad[2];
+  uint32_t N, cap, ring, seed, steps, stamp, parity, cur, velGOn, nbInit, nfills, ndrip, nsig, airCells, nvols;
+  uint64_t volWords;
   double tm;
 };
 static constexpr uint32_t FULL_MAGIC = 0x53544650u;   // "PFTS"
-static constexpr uint32_t FULL_VERSION = 3;           // 3: the air field and the drip samples follow the whitewater pools
-static void full_parts(st_flip* s, std::vector<std::pair<void*, size_t>>& v) {
-  const size_t C = s->ncell, T = s->ntiles, SC = std::max<size_t>(s->sprayCap, 1), N = s->N;
-  v = {{s->dCtl, sizeof(Ctl)}, {s->part[s->cur], N * sizeof(Part)}, {s->ids[s->cur], N * 4}, {s->need, T * 4}, {s->on, T},
+static constexpr uint32_t FULL_VERSION = 4;           // 4: air-field size and the pending fill volumes in the header
+static constexpr uint32_t VOL_REC = 20;               // words of one fill volume's record
+// the device parts of a checkpoint for N particles, the current buffer cur and ndrip drip samples
+static void full_parts(st_flip* s, uint32_t N, int cur, uint32_t ndrip, std::vector<std::pair<void*, size_t>>& v) {
+  const size_t C = s->ncell, T = s->ntiles, SC = std::max<size_t>(s->sprayCap, 1);
+  v = {{s->dCtl, sizeof(Ctl)}, {s->part[cur], (size_t)N * sizeof(Part)}, {s->ids[cur], (size_t)N * 4}, {s->need, T * 4}, {s->on, T},
        {s->tstate, T}, {s->active, T * 4}, {s->cnt[0], C * 4}, {s->cnt[1], C * 4}, {s->ctype, C * 4}, {s->pres, C * 4},
        {s->rhs, C * 4}, {s->acc, 6 * C * 4}, {s->vn, 3 * C * 4}, {s->vo, 3 * C * 4}, {s->velG, 3 * C * 4}, {s->sorInfo, C * 2},
        {s->wet, C * 4}, {s->sPos, SC * 16}, {s->sVel, SC * 16}};
   if (s->airCells) v.push_back({s->air, (size_t)s->airCells * 16});
-  if (s->ndrip) v.push_back({s->drip, (size_t)s->ndrip * 32});
+  if (ndrip) v.push_back({s->drip, (size_t)ndrip * 32});
 }
 static size_t pad4(size_t n) { return (n + 3) & ~(size_t)3; }
+static uint64_t vol_words(const st_flip* s) {
+  uint64_t w = 0;
+  for (auto& f : s->fillVols) w += VOL_REC + f.data.size();
+  return w;
+}
 
 st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size) {
   if (!s || !size) return ST_BAD_ARG;
   CK(cudaSetDevice(s->device));
   std::vector<std::pair<void*, size_t>> parts;
-  full_parts(s, parts);
-  uint64_t need = sizeof(FullHdr) + s->fills.size() * sizeof(float) + pad4(s->dripSig.size());
+  full_parts(s, s->N, s->cur, s->ndrip, parts);
+  const uint64_t vw = vol_words(s);
+  uint64_t need = sizeof(FullHdr) + s->fills.size() * sizeof(float) + pad4(s->dripSig.size()) + vw * 4;
   for (auto& p : parts) need += p.second;
   *size = need;
   if (!buf) return ST_OK;
@@ -1411,7 +1422,8 @@ st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size)
   h.ncell = s->ncell; h.maxN = s->maxN; h.sprayCap = s->sprayCap; h.N = s->N; h.cap = s->cap; h.ring = s->ring; h.seed = s->seed;
   h.steps = s->steps; h.stamp = s->stamp; h.parity = s->parity; h.cur = (uint32_t)s->cur; h.velGOn = s->velGOn ? 1u : 0u;
   h.nbInit = s->nbInit; h.nfills = (uint32_t)s->fills.size(); h.tm = s->tm;
-  h.ndrip = s->ndrip; h.nsig = (uint32_t)s->dripSig.size();
+  h.ndrip = s->ndrip; h.nsig = (uint32_t)s->dripSig.size(); h.airCells = s->airCells;
+  h.nvols = (uint32_t)s->fillVols.size(); h.volWords = vw;
   char* out = static_cast<char*>(buf);
   memcpy(out, &h, sizeof(h));
   out += sizeof(h);
@@ -1419,6 +1431,15 @@ st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size)
   memset(out, 0, pad4(s->dripSig.size()));
   memcpy(out, s->dripSig.data(), s->dripSig.size());
   out += pad4(s->dripSig.size());
+  for (auto& f : s->fillVols) {
+    uint32_t rec[VOL_REC];
+    rec[0] = f.sd.id; rec[1] = f.sd.dims[0]; rec[2] = f.sd.dims[1]; rec[3] = f.sd.dims[2];
+    memcpy(&rec[4], f.sd.origin, 12); memcpy(&rec[7], &f.sd.cell, 4); memcpy(&rec[8], f.c.pos, 12); memcpy(&rec[11], f.c.R, 36);
+    memcpy(out, rec, sizeof(rec));
+    out += sizeof(rec);
+    memcpy(out, f.data.data(), f.data.size() * 4);
+    out += f.data.size() * 4;
+  }
   for (auto& p : parts) {
     if (p.second) CK(cudaMemcpyAsync(out, p.first, p.second, cudaMemcpyDeviceToHost, s->stream));
     out += p.second;
@@ -1427,50 +1448,93 @@ st_status st_flip_save_full(st_flip* s, void* buf, uint64_t cap, uint64_t* size)
   return ST_OK;
 }
 
+// Every header field and every length is checked against this handle and the blob's size before anything of the
+// handle changes, so a rejected blob leaves the tank as it was (and steppable).
 st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
   if (!s || !buf || size < sizeof(FullHdr)) return ST_BAD_ARG;
   FullHdr h;
   memcpy(&h, buf, sizeof(h));
   if (h.magic != FULL_MAGIC || h.version != FULL_VERSION || h.nx != (uint32_t)s->nx || h.ny != (uint32_t)s->ny || h.nz != (uint32_t)s->nz ||
-      h.ntiles != s->ntiles || h.ncell != s->ncell || h.maxN != s->maxN || h.sprayCap != s->sprayCap || h.N > s->maxN || h.cur > 1 ||
-      h.parity > 1) {
+      h.ntiles != s->ntiles || h.ncell != s->ncell || h.maxN != s->maxN || h.sprayCap != s->sprayCap || h.airCells != s->airCells) {
     snprintf(g_err, sizeof(g_err), "load_full: the checkpoint is not of a simulator with this geometry and capacity");
     return ST_BAD_ARG;
   }
-  CK(cudaSetDevice(s->device));
-  CK(cudaStreamSynchronize(s->stream));
-  s->N = h.N; s->cap = h.cap; s->ring = h.ring; s->seed = h.seed; s->steps = h.steps; s->stamp = h.stamp; s->parity = h.parity;
-  s->cur = (int)h.cur; s->velGOn = h.velGOn != 0; s->nbInit = h.nbInit; s->tm = h.tm;
-  if (h.ndrip > s->dripCap) {
-    drop_graphs(s);
-    if (s->drip) cudaFree(s->drip);
-    s->drip = nullptr;
-    s->dripCap = 0;
-    CK(dalloc(&s->drip, drip_words(h.ndrip)));
-    s->dripCap = h.ndrip;
-  }
-  s->ndrip = h.ndrip;
-  std::vector<std::pair<void*, size_t>> parts;
-  full_parts(s, parts);
-  uint64_t need = sizeof(FullHdr) + (uint64_t)h.nfills * sizeof(float) + pad4(h.nsig);
-  for (auto& p : parts) need += p.second;
-  if (size < need) {
-    snprintf(g_err, sizeof(g_err), "load_full: %llu bytes given, %llu needed", (unsigned long long)size, (unsigned long long)need);
+  if (h.cap > s->maxN || h.N > h.cap || (h.cap ? h.ring >= h.cap : h.ring != 0) || h.cur > 1 || h.parity > 1 || h.nbInit > 2 ||
+      h.nfills % 8 != 0 || h.nfills > (1u << 20) || h.nsig > (1u << 24) || h.ndrip > (1u << 26) || h.nvols > 4096) {
+    snprintf(g_err, sizeof(g_err), "load_full: the checkpoint's counters are out of range (N %u, cap %u, ring %u)", h.N, h.cap, h.ring);
     return ST_BAD_ARG;
   }
-  const char* in = static_cast<const char*>(buf) + sizeof(FullHdr);
-  s->fills.assign(reinterpret_cast<const float*>(in), reinterpret_cast<const float*>(in) + h.nfills);
-  in += (size_t)h.nfills * sizeof(float);
-  s->dripSig.assign(in, h.nsig);
-  in += pad4(h.nsig);
-  for (auto& p : parts) {
-    if (p.second) CK(cudaMemcpyAsync(p.first, in, p.second, cudaMemcpyHostToDevice, s->stream));
-    in += p.second;
+  // the sizes of every part from the header alone
+  const char* base = static_cast<const char*>(buf);
+  uint64_t off = sizeof(FullHdr) + (uint64_t)h.nfills * sizeof(float) + pad4(h.nsig);
+  if (off > size) goto short_blob;
+  {
+    // fill volumes: walk the records, checking each grid's length against what is left
+    const uint64_t volStart = off;
+    uint64_t words = 0;
+    for (uint32_t k = 0; k < h.nvols; k++) {
+      if (off + VOL_REC * 4 > size) goto short_blob;
+      uint32_t rec[VOL_REC];
+      memcpy(rec, base + off, sizeof(rec));
+      const uint64_t n = (uint64_t)rec[1] * rec[2] * rec[3];
+      if (!rec[1] || !rec[2] || !rec[3] || rec[1] > 4096 || rec[2] > 4096 || rec[3] > 4096 || off + VOL_REC * 4 + n * 4 > size) goto short_blob;
+      off += VOL_REC * 4 + n * 4;
+      words += VOL_REC + n;
+    }
+    if (words != h.volWords) goto short_blob;
+    std::vector<std::pair<void*, size_t>> parts;
+    full_parts(s, h.N, (int)h.cur, h.ndrip, parts);   // sizes only: the drip pointer may change below
+    uint64_t need = off;
+    for (auto& p : parts) need += p.second;
+    if (size < need) {
+      snprintf(g_err, sizeof(g_err), "load_full: %llu bytes given, %llu needed", (unsigned long long)size, (unsigned long long)need);
+      return ST_BAD_ARG;
+    }
+    // everything checked: commit
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    if (h.ndrip > s->dripCap) {
+      drop_graphs(s);
+      float4* nd = nullptr;
+      CK(dalloc(&nd, drip_words(h.ndrip)));
+      if (s->drip) cudaFree(s->drip);
+      s->drip = nd;
+      s->dripCap = h.ndrip;
+    }
+    s->N = h.N; s->cap = h.cap; s->ring = h.ring; s->seed = h.seed; s->steps = h.steps; s->stamp = h.stamp; s->parity = h.parity;
+    s->cur = (int)h.cur; s->velGOn = h.velGOn != 0; s->nbInit = h.nbInit; s->tm = h.tm;
+    s->ndrip = h.ndrip;
+    const char* in = base + sizeof(FullHdr);
+    s->fills.assign(reinterpret_cast<const float*>(in), reinterpret_cast<const float*>(in) + h.nfills);
+    in += (size_t)h.nfills * sizeof(float);
+    s->dripSig.assign(in, h.nsig);
+    in = base + volStart;
+    s->fillVols.clear();
+    for (uint32_t k = 0; k < h.nvols; k++) {
+      uint32_t rec[VOL_REC];
+      memcpy(rec, in, sizeof(rec));
+      in += sizeof(rec);
+      st_flip::FillVol f{};
+      f.sd.id = rec[0]; f.sd.dims[0] = rec[1]; f.sd.dims[1] = rec[2]; f.sd.dims[2] = rec[3];
+      memcpy(f.sd.origin, &rec[4], 12); memcpy(&f.sd.cell, &rec[7], 4); memcpy(f.c.pos, &rec[8], 12); memcpy(f.c.R, &rec[11], 36);
+      const size_t n = (size_t)rec[1] * rec[2] * rec[3];
+      f.data.assign(reinterpret_cast<const float*>(in), reinterpret_cast<const float*>(in) + n);
+      in += n * 4;
+      s->fillVols.push_back(std::move(f));
+    }
+    full_parts(s, s->N, s->cur, s->ndrip, parts);
+    for (auto& p : parts) {
+      if (p.second) CK(cudaMemcpyAsync(p.first, in, p.second, cudaMemcpyHostToDevice, s->stream));
+      in += p.second;
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    drop_graphs(s);
+    s->sdfSig.clear();   // the next step uploads its colliders' distance grids again
+    return ST_OK;
   }
-  CK(cudaStreamSynchronize(s->stream));
-  drop_graphs(s);
-  s->sdfSig.clear();   // the next step uploads its colliders' distance grids again
-  return ST_OK;
+short_blob:
+  snprintf(g_err, sizeof(g_err), "load_full: the checkpoint is truncated or its fill volumes are malformed");
+  return ST_BAD_ARG;
 }
 
 st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light_ctas_per_sm, int32_t sor_ctas_per_sm) {
