@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=80)
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the pressure study and the 3-cell band run after the step")
     ap.add_argument("--tol", type=float, default=1e-6, help="pressure workloads: relative residual to reach")
     ap.add_argument("--omega", type=float, default=1.9, help="pressure workloads: SOR factor")
     ap.add_argument("--inner", type=int, default=100, help="pressure workloads: FP32 iterations per refinement")
@@ -66,8 +67,11 @@ def parse():
 def workload(name):
     from splashtank_b200 import scenes
     if name.startswith("wave_tank"):
-        n = int(name.rsplit("_", 1)[1])
-        return scenes.WaveTank(n)
+        # wave_tank_<n> (narrow band at full depth) or wave_tank_<n>_band<b> (a narrow band of b cells)
+        parts = name.split("_")
+        n = int(parts[2])
+        band = float(parts[3][4:]) if len(parts) > 3 and parts[3].startswith("band") else 1e4
+        return scenes.WaveTank(n, band=band)
     if name.startswith("dam_break"):
         n = int(name.rsplit("_", 1)[1])
         sc = scenes.dam_break(n)
@@ -90,11 +94,13 @@ def workload(name):
 
 
 def config_of(name, w, n_live):
-    cfg = {"workload": name, "particles": int(n_live), "dt": w.dt, "steps_per_run": getattr(w, "steps", None),
+    cfg = {"workload": name, "particles": int(n_live), "dt": w.dt,
            "l2": "working set larger than L2 (126 MB): no flush", "parallelism": "replicas"}
     if name.startswith("wave_tank"):
-        cfg.update(grid=[w.n] * 3, tile="8^3", sor_iters=w.opts["iters"], narrow_band="full depth (band 1e4)",
-                   colliders="piston box 0.5 Hz amp 0.05 + sphere r 0.1 on a linear path", whitewater_cap=w.spray_cap,
+        cfg.update(grid=[w.n] * 3, tile="8^3", sor_iters=w.opts["iters"],
+                   narrow_band="full depth (band 1e4)" if w.band >= 1e4 else "%g cells" % w.band,
+                   colliders="piston box 0.5 Hz amp 0.05 + sphere r 0.1 on a linear path over %d steps" % w.steps,
+                   whitewater_cap=w.spray_cap,
                    pbf="not in this step")
     return cfg
 
@@ -182,6 +188,40 @@ def roofline(stage_ms, nsteps, n, cells, fluid, iters, peak, peak_src):
             "stage_share": round(stage_ms[dom] / stage_ms["total"], 4), "limiter": NCU_LIMITER.get(dom)}
 
 
+def step_bytes_model(n, cells, fluid, iters, nb_on, ww_slots, sort_every=16):
+    """Algorithmic HBM bytes of one whole step by the per-unit model of the reference's state layout: particles 112 B
+    (tile marking reads pos 16, P2G reads pos and vel 32, G2P reads 32 and writes 32) plus the sort's copies (pos, vel
+    and id in and out, 72 B) every sort_every steps (the reference sorts every 16th step; this library's sort is part of
+    P2G's gather every step and is not counted again); grid 168 B per cell with storage (P2G sums and count 28, classify
+    8, normFaces 48, divergence 24, project 32, G2P face reads 24, clear 4); the red-black SOR 16 B per fluid cell and
+    iteration; the narrow band 56 B per cell (four 8-byte passes and the kept velocity); whitewater 32 B per particle
+    (the emission read) and 64 B per handed-out point (its sample and step)."""
+    b = 112 * n + 72 * n / sort_every + 168 * cells + 16 * fluid * iters
+    if nb_on:
+        b += 56 * cells
+    if ww_slots is not None:
+        b += 32 * n + 64 * ww_slots
+    return int(b)
+
+
+def step_roofline(ms_per_step, n, cells, fluid, iters, nb_on, ww_slots, stage_ms, nrec, peak, peak_src):
+    """The whole step against the HBM roofline: algorithmic bytes of a step (step_bytes_model) over the device time of
+    a step, and beside it the sum of the per-kernel figures of stage_bytes over the stages that ran."""
+    b = step_bytes_model(n, cells, fluid, iters, nb_on, ww_slots)
+    ach = b / (ms_per_step * 1e-3) / 1e9
+    kb = 0
+    for k in stage_ms:
+        if k == "total" or stage_ms[k] <= 0:
+            continue
+        x, launches = stage_bytes(k, n, cells, fluid, iters)
+        kb += (x or 0) * launches
+    return {"step_bytes": b, "step_ms": round(ms_per_step, 4), "step_achieved": round(ach, 1), "step_frac": round(ach / peak, 4),
+            "kernel_bytes": int(kb), "kernel_frac": round(kb / (ms_per_step * 1e-3) / 1e9 / peak, 4),
+            "target_ms_at_60pct": round(b / (0.6 * peak * 1e9) * 1e3, 4), "peak": peak, "peak_source": peak_src,
+            "model": "112 B/particle + 72 B/particle sort copies + 168 B/cell + 16 B/fluid cell/iteration + 56 B/cell narrow band "
+                     "+ 32 B/particle + 64 B/point whitewater"}
+
+
 def measured_peak():
     try:
         p = json.load(open(PEAKS))
@@ -191,78 +231,66 @@ def measured_peak():
 
 
 # ---------------------------------------------------------------- CPU baseline (oracle)
-def cpu_sample(name, steps_cap=None, budget_s=20.0, threads=None):
-    """Time the CPU restatement (all host threads) on a bounded sample: the same scene at 96^3 (wave tank) or 64^3."""
+def cpu_sample(name, w=None, budget_s=20.0, threads=None, warm=1):
+    """Time the CPU restatement (all host threads) on a bounded sample of the same workload: `warm` untimed steps, then
+    steps until budget_s has passed (at least one). w: the workload object already built for the GPU run, if any."""
     from oracle.oracle import OracleFlipSim
     from splashtank_b200.scene import SceneRunner
-    sample = "wave_tank_96" if name.startswith("wave_tank") else name
-    w = workload(sample)
+    w = w or workload(name)
     th = threads or os.cpu_count() or 1
     sim = w.make(OracleFlipSim, threads=th)
     run = SceneRunner(sim)
-    t, k, t0 = 0.0, 0, time.perf_counter()
-    live = None
+    t = 0.0
+    for _ in range(warm):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    k, t0 = 0, time.perf_counter()
     while True:
         t += w.dt
         run.step(w.dt, w.states(t), w.opts)
         k += 1
-        if live is None:
-            live = sim.readStats()["live"]
         el = time.perf_counter() - t0
-        if (steps_cap and k >= steps_cap) or el > budget_s:
+        if el > budget_s:
             break
     live = sim.readStats()["live"]
+    sim.destroy()
     return {"value": live * k / el, "unit": "particle-steps/s", "cores": th, "kind": "port",
-            "sample": "%s (%d particles), %d steps, oracle with %d OpenMP threads" % (sample, live, k, th)}, el
+            "sample": "%s (%d live particles): %d steps after %d untimed, oracle with %d OpenMP threads (%.1f s)" % (name, live, k, warm, th, el)}, el
 
 
 def run_reference(a):
+    """The reference arm: the reference's FLIP step exists only as WGSL for a browser (no graphics stack here), so its
+    CPU restatement (the oracle, all host threads) steps the same workload; each timed step is a whole step of that
+    workload, and the timed steps are bounded (at most 10 after at most 1 untimed) so the arm ends within minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle.oracle import OracleFlipSim
     from splashtank_b200.scene import SceneRunner
-    sample = "wave_tank_96" if a.workload.startswith("wave_tank") else a.workload
-    w = workload(sample)
+    w = workload(a.workload)
     th = os.cpu_count() or 1
     sim = w.make(OracleFlipSim, threads=th)
     run = SceneRunner(sim)
+    warm, steps = min(a.warmup, 1), max(1, min(a.steps, 10))
     t = 0.0
-    for _ in range(a.warmup):
+    for _ in range(warm):
         t += w.dt
         run.step(w.dt, w.states(t), w.opts)
     t0 = time.perf_counter()
-    for _ in range(a.steps):
+    for _ in range(steps):
         t += w.dt
         run.step(w.dt, w.states(t), w.opts)
     el = time.perf_counter() - t0
     live = sim.readStats()["live"]
-    v = live * a.steps / el
+    v = live * steps / el
+    sample = ("%s (%d live particles): %d steps after %d untimed, the oracle with %d OpenMP threads; the reference's FLIP step runs "
+              "only as WGSL in a browser (no graphics stack here), so its CPU restatement stands in" % (a.workload, live, steps, warm, th))
     line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "impl": "reference", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": el * 1e3 / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config_of(a.workload, workload_meta(a.workload), live),
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": th, "kind": "port",
-                             "sample": "%s (%d particles) per step, oracle with %d OpenMP threads: the reference's FLIP step runs only "
-                                       "as WGSL in a browser (no graphics stack here), so its CPU restatement stands in" % (sample, live, th)},
+            "steps": steps, "warmup": warm, "ms_per_step": el * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config_of(a.workload, w, live),
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": th, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def workload_meta(name):
-    class M:
-        pass
-    m = M()
-    if name.startswith("wave_tank"):
-        from splashtank_b200 import scenes
-        m.n = int(name.rsplit("_", 1)[1])
-        m.dt = 1.0 / 240.0
-        m.steps = 200
-        m.opts = dict(iters=30)
-        m.spray_cap = 4_000_000
-    else:
-        m.dt = 1.0 / 240.0
-        m.steps = 100
-    return m
 
 
 # ---------------------------------------------------------------- pressure solve precision study
@@ -419,6 +447,77 @@ def run_pressure_reference(a):
             "config": {"workload": a.workload, "grid": [n] * 3, "tol": a.tol, "omega": a.omega},
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def pressure_summary(local, tol=1e-6, omega=1.9, inner=100, repeats=3, n=512):
+    """The metric's pressure half, run after the FLIP step's timed region: ms per solve of the 512^3 splash system to
+    `tol` relative residual, FP32 SOR inside FP64 refinement against plain FP32 SOR (the median of `repeats` solves each,
+    the same predicted check schedule for both), each solution's error against an FP64 SOR solve to 1e-11, and the same
+    comparison at 1e-9, where FP32 SOR stalls at its rounding floor."""
+    from splashtank_b200.poisson import REFINE, SOR32, SOR64, PoissonSolver
+    ty, rhs = pressure_scene("pressure_%d" % n)[1:]
+    s = PoissonSolver((n, n, n), device=local)
+    s.set(ty, rhs)
+    nt, nf = s.stats()
+    ro = dict(tol=tol, omega=omega, inner_sweeps=inner, max_sweeps=200000, predict=True)
+    s.solve(REFINE, **ro)   # warm-up
+    out = {}
+    for key, mode in (("refine", REFINE), ("fp32_sor", SOR32)):
+        runs = []
+        for _ in range(repeats):
+            kw = dict(ro) if mode == REFINE else dict(tol=tol, omega=omega, check_every=inner, max_sweeps=20000, predict=True)
+            runs.append(s.solve(mode, **kw))
+        runs.sort(key=lambda r: r["ms"])
+        r = runs[len(runs) // 2]
+        out[key] = {"ms": r["ms"], "ms_runs": [round(x["ms"], 3) for x in runs], "sweeps": r["sweeps"], "refinements": r["refinements"],
+                    "rel_residual": r["rel_residual"], "converged": r["converged"], "x": s.read()}
+    r9 = {"refine": s.solve(REFINE, tol=1e-9, omega=omega, inner_sweeps=inner, max_sweeps=20000, predict=True)}
+    r9["fp32_sor"] = s.solve(SOR32, tol=1e-9, omega=omega, check_every=inner, max_sweeps=2 * r9["refine"]["sweeps"], predict=True)
+    rgold = s.solve(SOR64, tol=1e-11, omega=omega, check_every=50, max_sweeps=400000)
+    gold = s.read()
+    s.destroy()
+    gn, gmax = float(np.linalg.norm(gold)), float(np.abs(gold).max())
+    for k in out:
+        d = out[k].pop("x") - gold
+        out[k]["error_vs_fp64"] = {"rel_l2": float(np.linalg.norm(d)) / gn, "max_abs_over_max": float(np.abs(d).max()) / gmax}
+    out.update(workload="pressure_%d" % n, tol=tol, omega=omega, active_tiles=nt, fluid_cells=nf,
+               refine_vs_fp32_speedup=round(out["fp32_sor"]["ms"] / out["refine"]["ms"], 4),
+               fp64_reference={"method": "FP64 SOR to 1e-11", "sweeps": rgold["sweeps"], "rel_residual": rgold["rel_residual"]},
+               tol_1e9={k: {"ms": r["ms"], "sweeps": r["sweeps"], "rel_residual": r["rel_residual"], "converged": r["converged"]}
+                        for k, r in r9.items()},
+               scene="seeded Gaussian blobs (120, sigma 0.025-0.07 of the box) above 0.5 inside solid walls; rhs = divergence of a "
+                     "seeded uniform(-1,1) face field", unit="ms per solve, CUDA events on the solver's stream")
+    return out
+
+
+def band_summary(local, name="wave_tank_256_band3", warm=8, steps=20):
+    """The wave tank with the reference's narrow band of 3 cells (particles only in the band under the surface after
+    the first steps trim the deep water), device-timed like the headline run."""
+    import torch
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    w = workload(name)
+    sim = w.make(FlipSim, device=local)
+    run = SceneRunner(sim)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    t = 0.0
+    for _ in range(warm):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = sim.readStats()
+    sim.destroy()
+    return {"workload": name, "value": st["live"] * steps / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms / steps,
+            "live_particles": st["live"], "seeded_particles": len(w.pos), "tiles_with_storage": st["sc"], "fluid_cells": st["fluid"],
+            "steps": steps, "warmup": warm, "narrow_band": "3 cells (deep calm particles trimmed, thin band cells refilled)"}
 
 
 # ---------------------------------------------------------------- many tanks per step
@@ -699,9 +798,13 @@ def main():
         t += w.dt
         run.step(w.dt, w.states(t), w.opts)
 
+    # the stage timer is on from the first warm-up step, so the timed steps' graph (with its event nodes) is captured
+    # and instantiated before the timed region; the warm-up's stage times are read and discarded
+    sim.set_timing(True)
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
+    sim.read_timing()
     st0 = sim.readStats()
 
     def barrier():
@@ -710,7 +813,6 @@ def main():
         torch.cuda.synchronize()
 
     # ---- device-timed region
-    sim.set_timing(True)
     clocks = Clocks(local)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -787,7 +889,13 @@ def main():
     if rank == 0:
         peak, src = measured_peak()
         cells = st1["sc"] * 512
-        rl = roofline(stages, nrec, live, cells, st1["fluid"], w.opts.get("iters", 30), peak, src)
+        iters = w.opts.get("iters", 30)
+        rl = roofline(stages, nrec, live, cells, st1["fluid"], iters, peak, src)
+        nb_on = bool(w.opts.get("nb", {}).get("on"))
+        ww = min(st1["spray_used"], w.spray_cap) if w.spray_cap else None
+        srl = step_roofline(ms / a.steps, live, cells, st1["fluid"], iters, nb_on, ww, stages, nrec, peak, src)
+        if rl is not None:
+            rl.update(srl)
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded jitter, 8 particles per cell)",
@@ -796,10 +904,16 @@ def main():
                 "clocks": clk, "roofline": rl,
                 "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                         "steps": a.e2e_steps, "readback": "counters every step (read once the next step is queued), a packed cache frame of all particles every 4th step, copied while the next steps run"}}
-        if world == 1 and not a.no_cpu_baseline:
+        if world == 1:
+            sim.destroy()
             del sim
-            cb, _ = cpu_sample(a.workload)
-            line["cpu_baseline"] = cb
+            if not a.no_extras and a.workload.startswith("wave_tank"):
+                # the metric's pressure half and the reference's narrow band of 3 cells, after the timed regions
+                line["pressure"] = pressure_summary(local)
+                line["band3"] = band_summary(local, a.workload + "_band3")
+            if not a.no_cpu_baseline:
+                cb, _ = cpu_sample(a.workload, w)
+                line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

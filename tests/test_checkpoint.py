@@ -12,7 +12,7 @@ def _state(sim):
     p = np.zeros((max(n, 1), 4), np.float32)
     v = np.zeros((max(n, 1), 4), np.float32)
     sim.readbackInto(p, v)
-    sp = sim.readSpray()
+    sp = sim.readSpray() or {"p": np.zeros((0, 4), np.float32), "v": np.zeros((0, 4), np.float32)}   # None without a pool
     st = sim.readStats()
     return p[:n].copy(), v[:n].copy(), sp["p"].copy(), sp["v"].copy(), (st["live"], st["fluid"], st["sc"], st["spray_used"])
 

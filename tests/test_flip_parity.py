@@ -322,6 +322,46 @@ def test_large_tank_invariants(n, steps, cap):
     assert (g["ctype"] & 255 == 1).sum() == st["fluid"]
 
 
+def test_dam_break_64_as_benchmarked():
+    """The plain dam break exactly as its configuration states it: 64^3 MAC grid (dx 1/64) in 8^3 blocks, solid walls,
+    fluid where x < 0.4 and y < 0.6, 8 particles per cell with seeded jitter (505,856 particles), FLIP 0.97, gravity
+    9.81, dt 1/240, 50 red-black SOR iterations at omega 1.7, 100 steps: bit for bit with the oracle."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    sc = scenes.dam_break(64)
+    assert len(sc["pos"]) == 505_856 and sc["opts"]["iters"] == 50 and sc["opts"]["omega"] == 1.7 and sc["steps"] == 100
+    g, o = make_pair(sc, extra=0)
+    o.set_threads(os.cpu_count() or 8)
+    for _ in range(sc["steps"]):
+        for s in (g, o):
+            s.step(sc["dt"], sc["opts"])
+    assert_same_state(g, o)
+
+
+def _big_tank_pair(n, spray_cap):
+    from oracle.oracle import OracleFlipSim
+    from splashtank_b200 import scenes
+    from splashtank_b200.flip import FlipSim
+    w = scenes.WaveTank(n, spray_cap=spray_cap)
+    g = w.make(FlipSim)
+    o = w.make(OracleFlipSim, threads=os.cpu_count() or 8)
+    return w, g, o
+
+
+@pytest.mark.parametrize("n,steps,cap", [(128, 10, 500_000), (256, 3, 4_000_000)])
+def test_wave_tank_at_benchmark_sizes(n, steps, cap):
+    """The full-feature wave tank at 128^3 (about 4.7M particles, 10 steps) and at the benchmark's 256^3 (about 38.6M
+    particles, 3 steps): piston and sphere colliders, narrow band at full depth with refills, whitewater, air field,
+    drips, gusts and sheet tearing, every field bit for bit with the oracle (tile counts and particle indices at the
+    benchmark's scale)."""
+    w, g, o = _big_tank_pair(n, cap)
+    _run_tank(w, (g, o), steps)
+    assert g.readStats()["live"] > 0.9 * len(w.pos)
+    assert_same_state(g, o, spray=True)
+    g.destroy()
+    o.destroy()
+
+
 def test_empty_and_bad_arguments():
     import ctypes as C
     from splashtank_b200 import abi
