@@ -245,78 +245,126 @@ __global__ void __launch_bounds__(CM_T, 6) k_scatter(Bufs B) {
 // written to their final place (ascending id inside each cell) and splatted into a 10^3-cell shared-memory window
 // (the tile plus one cell around it) in the reference's fixed point: i32(round(w * v * 65536)) and i32(round(w * 65536)).
 // Integer sums do not depend on order, so the window is flushed to HBM with plain atomic adds.
-// The tile's ids (when at most P2G_IDS), cell offsets and counts are staged in shared memory first: the in-cell rank
-// (ids below this particle's in its cell) then reads shared memory instead of issuing a global load per neighbour.
+// The tile's cell offsets and counts are staged in shared memory first; the in-cell rank is the number of ids below
+// the particle's in its cell. A particle whose corner faces need no clamping (the usual case) splats with window offsets
+// fixed at compile time. Chunks of 256 particles go through two phases. The move (gather from the previous order, in-cell rank, write to the
+// final place) runs with a warp's lanes on consecutive particles, so its global loads and stores are coalesced and
+// the lanes of one cell read the same ids (L1 broadcasts); it leaves each particle's position and velocity in shared
+// memory. The splat then takes them back with a warp's lanes 8 particles apart (different cells, so the window atomics
+// rarely collide), from a layout padded by one word per 32 so those reads hit 32 different banks. Four CTAs share an
+// SM (64 registers, 34 KB of shared memory each); staging the tile's ids in shared memory, a second staging buffer,
+// five or six CTAs per SM and window strides padded against bank conflicts (24 / 256 words) all measured slower.
 constexpr int P2G_T = 256;
-constexpr uint32_t P2G_IDS = 4608;
-__global__ void __launch_bounds__(P2G_T) k_p2g(Bufs B) {
+constexpr int P2G_SW = P2G_T + P2G_T / 32;
+struct P2GSmem {
+  int32_t win[6][1000];
+  uint32_t soff[512];
+  int32_t scnt[512];
+  float stg[6][P2G_SW];
+};
+__device__ __forceinline__ int p2gSlot(uint32_t r) { return (int)(r + (r >> 5)); }
+// The 8 corners of one axis for a particle whose corner faces all lie in the window without clamping (the tile is at
+// least a cell away from every wall, and corner (0,0,0) has window coordinates in [0, 8]): window offsets are
+// compile-time constants from the base, weights are the reference's ((wx * wy) * wz) with the xy products shared, and
+// each sum is i32(round(w * v * 65536)) / i32(round(w * 65536)) as in the general path.
+__device__ __forceinline__ void splatAxisFast(int32_t* __restrict__ pv, int32_t* __restrict__ pw, V3 fr, float vc, float scale) {
+  const float wx0 = 1.0f - fr.x, wx1 = fr.x, wy0 = 1.0f - fr.y, wy1 = fr.y, wz0 = 1.0f - fr.z, wz1 = fr.z;
+  const float wxy[4] = {wx0 * wy0, wx1 * wy0, wx0 * wy1, wx1 * wy1};
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int off = (c & 1) + 10 * ((c >> 1) & 1) + 100 * (c >> 2);
+    const float w = wxy[c & 3] * ((c & 4) ? wz1 : wz0);
+    if (!(w <= 0.0f)) {
+      atomicAdd(pv + off, __float2int_rn(w * vc * scale));
+      atomicAdd(pw + off, __float2int_rn(w * scale));
+    }
+  }
+}
+__device__ __forceinline__ void p2gSplat(const FlipParams& P, P2GSmem& S, V3 p, V3 v, int ox, int oy, int oz, bool inner) {
+  for (int axis = 0; axis < 3; axis++) {
+    V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
+    if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
+    const V3 f0 = vfloor(g), fr = g - f0;
+    const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
+    const float vc = comp3(v, axis);
+    const int bx = i0 - ox + 1, by = j0 - oy + 1, bz = k0 - oz + 1;
+    if (inner && (unsigned)bx <= 8u && (unsigned)by <= 8u && (unsigned)bz <= 8u) {
+      const int wb = bx + 10 * (by + 10 * bz);
+      splatAxisFast(&S.win[axis][wb], &S.win[3 + axis][wb], fr, vc, P.scale);
+      continue;
+    }
+    for (int c = 0; c < 8; c++) {
+      const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+      const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
+      if (w <= 0.0f) continue;
+      int fi = i0 + dx, fj = j0 + dy, fk = k0 + dz;   // the face's cell, clamped as faceIndex does
+      if (axis == 0) { fi = clampi(fi, 0, (int)P.nx); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz - 1); }
+      else if (axis == 1) { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny); fk = clampi(fk, 0, (int)P.nz - 1); }
+      else { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz); }
+      const int widx = (fi - ox + 1) + 10 * ((fj - oy + 1) + 10 * (fk - oz + 1));
+      atomicAdd(&S.win[axis][widx], (int32_t)rintf(w * vc * P.scale));
+      atomicAdd(&S.win[3 + axis][widx], (int32_t)rintf(w * P.scale));
+    }
+  }
+}
+__global__ void __launch_bounds__(P2G_T, 4) k_p2g(Bufs B) {
+  extern __shared__ __align__(16) unsigned char p2gRaw[];
+  P2GSmem& S = *reinterpret_cast<P2GSmem*>(p2gRaw);
   __shared__ FlipParams P;
-  __shared__ int32_t win[6][1000];
-  __shared__ uint32_t sid[P2G_IDS];
-  __shared__ uint32_t soff[512];
-  __shared__ int32_t scnt[512];
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
+  const uint32_t tid = threadIdx.x, splatPos = (tid & 31) * 8 + (tid >> 5);
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a];
     const uint32_t tt = t / P.tx;
     const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
-    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
-    const bool staged = s1 - s0 <= P2G_IDS;
-    for (int r = threadIdx.x; r < 6000; r += P2G_T) (&win[0][0])[r] = 0;
-    if (staged) for (uint32_t u = s0 + threadIdx.x; u < s1; u += P2G_T) sid[u - s0] = B.spid[u];
-    for (int r = threadIdx.x; r < 512; r += P2G_T) { soff[r] = B.cellOff[t * 512u + r]; scnt[r] = B.cnt[t * 512u + r]; }
+    const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1], n = s1 - s0;
+    // clamping of face indices (faceIndex) is the identity for every corner of this tile's particles
+    const bool inner = ox >= 1 && oy >= 1 && oz >= 1 && ox + 9 <= (int)P.nx && oy + 9 <= (int)P.ny && oz + 9 <= (int)P.nz;
+    for (int r = tid; r < 6000; r += P2G_T) (&S.win[0][0])[r] = 0;
+    for (int r = tid; r < 512; r += P2G_T) { S.soff[r] = B.cellOff[t * 512u + r]; S.scnt[r] = B.cnt[t * 512u + r]; }
     __syncthreads();
-    // lanes of a warp take particles 8 apart, so they fall in different cells and their shared atomics rarely collide;
-    // each thread gathers its next particle while it splats the current one
-    const uint32_t lanePos = (uint32_t)((threadIdx.x & 31) * 8 + (threadIdx.x >> 5));
-    Part qNext;
-    if (s0 + lanePos < s1) qNext = B.pb[B.srcIdx[s0 + lanePos]];
-    for (uint32_t base = s0; base < s1; base += P2G_T) {
-      const uint32_t s = base + lanePos;
-      const Part q = qNext;
-      if (s + P2G_T < s1) qNext = B.pb[B.srcIdx[s + P2G_T]];
-      if (s >= s1) continue;
-      const uint32_t myid = staged ? sid[s - s0] : B.spid[s];
-      const V3 p = xyz(q.p), v = xyz(q.v);
+    // the move of one chunk: particle s = s0 + chunk * 256 + tid, already loaded into q
+    auto move = [&](uint32_t ch, const Part& q) {
+      const uint32_t s = s0 + ch * P2G_T + tid;
+      if (s >= s1) return;
+      const uint32_t myid = B.spid[s];
       int ci, cj, ck;
-      particleCell(P, p, ci, cj, ck);
+      particleCell(P, xyz(q.p), ci, cj, ck);
       const uint32_t key = cellIdx(P, ci, cj, ck), lk = key - t * 512u;
       uint32_t cs, ce;
-      if (lk < 512u) { cs = s0 + soff[lk]; ce = cs + (uint32_t)scnt[lk]; }
+      if (lk < 512u) { cs = s0 + S.soff[lk]; ce = cs + (uint32_t)S.scnt[lk]; }
       else { cs = s0 + B.cellOff[key]; ce = cs + (uint32_t)B.cnt[key]; }
       uint32_t rk = 0;
-      if (staged && cs >= s0 && ce <= s1) { for (uint32_t u = cs - s0; u < ce - s0; u++) rk += sid[u] < myid ? 1u : 0u; }
-      else { for (uint32_t u = cs; u < ce; u++) rk += B.spid[u] < myid ? 1u : 0u; }
+      for (uint32_t u = cs; u < ce; u++) rk += B.spid[u] < myid ? 1u : 0u;
       B.pa[cs + rk] = q;
       B.ida[cs + rk] = myid;
-      for (int axis = 0; axis < 3; axis++) {
-        V3 g = (p - v3(P.x0, P.y0, P.z0)) * P.ih;
-        if (axis == 0) { g.y -= 0.5f; g.z -= 0.5f; } else if (axis == 1) { g.x -= 0.5f; g.z -= 0.5f; } else { g.x -= 0.5f; g.y -= 0.5f; }
-        const V3 f0 = vfloor(g), fr = g - f0;
-        const int i0 = gidx(f0.x), j0 = gidx(f0.y), k0 = gidx(f0.z);
-        const float vc = comp3(v, axis);
-        for (int c = 0; c < 8; c++) {
-          const int dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
-          const float w = (dx == 1 ? fr.x : 1.0f - fr.x) * (dy == 1 ? fr.y : 1.0f - fr.y) * (dz == 1 ? fr.z : 1.0f - fr.z);
-          if (w <= 0.0f) continue;
-          int fi = i0 + dx, fj = j0 + dy, fk = k0 + dz;   // the face's cell, clamped as faceIndex does
-          if (axis == 0) { fi = clampi(fi, 0, (int)P.nx); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz - 1); }
-          else if (axis == 1) { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny); fk = clampi(fk, 0, (int)P.nz - 1); }
-          else { fi = clampi(fi, 0, (int)P.nx - 1); fj = clampi(fj, 0, (int)P.ny - 1); fk = clampi(fk, 0, (int)P.nz); }
-          const int widx = (fi - ox + 1) + 10 * ((fj - oy + 1) + 10 * (fk - oz + 1));
-          atomicAdd(&win[axis][widx], (int32_t)rintf(w * vc * P.scale));
-          atomicAdd(&win[3 + axis][widx], (int32_t)rintf(w * P.scale));
-        }
+      const int k = p2gSlot(tid);
+      S.stg[0][k] = q.p.x; S.stg[1][k] = q.p.y; S.stg[2][k] = q.p.z;
+      S.stg[3][k] = q.v.x; S.stg[4][k] = q.v.y; S.stg[5][k] = q.v.z;
+    };
+    const uint32_t nch = (n + P2G_T - 1) / P2G_T;
+    // the next chunk's particle is loaded while this chunk is splatted
+    Part qn;
+    if (tid < n) qn = B.pb[B.srcIdx[s0 + tid]];
+    for (uint32_t ch = 0; ch < nch; ch++) {
+      move(ch, qn);
+      if ((ch + 1) * P2G_T + tid < n) qn = B.pb[B.srcIdx[s0 + (ch + 1) * P2G_T + tid]];
+      __syncthreads();
+      if (ch * P2G_T + splatPos < n) {
+        const int k = p2gSlot(splatPos);
+        const V3 p = v3(S.stg[0][k], S.stg[1][k], S.stg[2][k]);
+        const V3 v = v3(S.stg[3][k], S.stg[4][k], S.stg[5][k]);
+        p2gSplat(P, S, p, v, ox, oy, oz, inner);
       }
+      __syncthreads();
     }
-    __syncthreads();
-    for (int r = threadIdx.x; r < 1000; r += P2G_T) {
+    for (int r = tid; r < 1000; r += P2G_T) {
       const int gi = ox + (r % 10) - 1, gj = oy + (r / 10) % 10 - 1, gk = oz + r / 100 - 1;
       if (gi < 0 || gj < 0 || gk < 0 || gi >= (int)P.tx * 8 || gj >= (int)P.ty * 8 || gk >= (int)P.tz * 8) continue;
       const uint32_t c = cellIdx(P, gi, gj, gk);
       for (int pl = 0; pl < 6; pl++) {
-        const int32_t v = win[pl][r];
+        const int32_t v = S.win[pl][r];
         if (v != 0) atomicAdd(&B.acc[pl * nc + c], v);
       }
     }
@@ -999,7 +1047,12 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
 }
 int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
 int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, CM_T, 0, s>>>(B); return 1; }
-int launch_p2g(const Bufs& B, int grid, cudaStream_t s) { k_p2g<<<grid, P2G_T, 0, s>>>(B); return 1; }
+int launch_p2g(const Bufs& B, int grid, cudaStream_t s) {
+  // the window, ids, offsets and staging buffers take more than the 48 KB of static shared memory
+  cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(P2GSmem));
+  k_p2g<<<grid, P2G_T, sizeof(P2GSmem), s>>>(B);
+  return 1;
+}
 int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
   if (ocean) k_classify<true><<<grid, 512, 0, s>>>(B);
   else k_classify<false><<<grid, 512, 0, s>>>(B);
