@@ -118,6 +118,11 @@ typedef struct st_step_opts {
   float ocean_spread;   /* directional spread, degrees */
   int32_t ocean_seed;
   float time;           /* o.time: scene time, the waves' phase */
+  /* PBF density constraints on the FLIP particles at the end of the step, after the whitewater and narrow-band
+   * stages (no counterpart in the reference's FLIP step; the constraint is GpuSim's, src/gpu.js:208-292): iterations
+   * of lambda + delta with kernel radius 2.2 d, the boundary density of the walls and colliders, FLIP's collider
+   * response after each correction, and the particle velocity changed by the correction over dt. 0: off. */
+  int32_t pbf_iters;
 } st_step_opts;
 
 /* Counters read back after a step: FlipSim.stats (src/flip/sim.js:160-168). */
@@ -154,9 +159,9 @@ typedef struct st_flip_dims {
 } st_flip_dims;
 
 /* Per-stage device milliseconds of the last step (FlipSim.stepTimed, src/flip/sim.js:312-331). Stage
- * names as in src/app/14-bench.js:17. */
+ * names as in src/app/14-bench.js:17; pbf is the density stage of st_step_opts.pbf_iters (0 when off). */
 typedef struct st_stage_times {
-  float sort, blocks, clear, p2g, narrow_band, classify, norm_faces, divergence, pressure, project, g2p, spray, reseed, total;
+  float sort, blocks, clear, p2g, narrow_band, classify, norm_faces, divergence, pressure, project, g2p, pbf, spray, reseed, total;
 } st_stage_times;
 
 /* ---- FLIP ---- */
@@ -308,50 +313,53 @@ st_status st_flip_nb_fills(st_flip* s, const float* boxes6, uint32_t nbox, const
  * (distance grid, position, rotation; velocities are ignored) whose negative distance is water. The next restart step
  * packs them after its colliders (FlipSim.step, src/flip/sim.js:189-190) for fillPhi (wgsl-core.js:235) and then drops
  * them; the grids are copied at the call. mode as for st_flip_nb_fills. Fill volumes pending at a full checkpoint are
- * not stored in it. */
+ * stored in it. */
 st_status st_flip_nb_fill_vols(st_flip* s, const st_collider* vols, uint32_t n, uint32_t mode);
 /* The CUDA stream the handle enqueues on (a cudaStream_t), for events and graph capture by the caller. */
 void* st_flip_stream(st_flip* s);
 
-/* ---- PBF (GpuSim, src/gpu.js:357-428) ---- */
+/* ---- PBF (GpuSim, src/gpu.js:357-476) ----
+ * The app's WebGPU position-based fluid engine: constants of FluidSim (src/shared.js:220-270), colliders as signed
+ * distance grids (the same st_collider records as the FLIP step), open faces, dead particles (y below -1e5) kept in
+ * place, particles in index order. The order inside a grid cell, which the reference leaves to an atomic counter, is
+ * ascending particle index here. */
 
 typedef struct st_pbf st_pbf;
 
+/* new GpuSim(device, {d, maxN, size, open}) (src/gpu.js:357-380) */
 typedef struct st_pbf_desc {
   uint32_t size;        /* sizeof(st_pbf_desc) */
   double d;             /* particle spacing; kernel radius h = 2.2 d */
   double box[3];        /* zeros mean (3, 2.6, 3) */
-  uint32_t open;
+  uint32_t open;        /* ST_OPEN_* bits */
   uint32_t max_n;
   int32_t device;
-  double eps_k;         /* 0 means 0.64 (src/shared.js:259) */
-  double wall_k;        /* 0 means 1.8 (src/shared.js:268) */
+  double eps_k;         /* FluidSim opt.epsK; 0 means 0.64 (src/shared.js:259) */
+  double wall_k;        /* FluidSim opt.wallK; 0 means 1.8 (src/shared.js:268) */
 } st_pbf_desc;
 
-/* Analytic collider of the native baker (native/splash.cpp:22): kind 0 sphere (r), kind 1 box (half
- * extents, rotated by yaw about y). */
-typedef struct st_pbf_col {
-  int32_t kind;
-  float x, y, z, r, hx, hy, hz, yaw;
-} st_pbf_col;
-
+/* GpuSim.step's options o (src/gpu.js:409-416): gravity, XSPH viscosity, solver iterations (at least 1), colliders */
 typedef struct st_pbf_opts {
-  uint32_t size;
+  uint32_t size;        /* sizeof(st_pbf_opts) */
   float g;
   float visc;
   int32_t iters;
-  uint32_t ncols;
-  const st_pbf_col* cols;
+  uint32_t ncols;       /* at most 32 are used */
+  const st_collider* cols;
 } st_pbf_opts;
 
-/* new FluidSim/GpuSim constants (src/shared.js:220-271, native/splash.cpp:50-71). */
 st_status st_pbf_create(const st_pbf_desc* desc, st_pbf** out);
 void st_pbf_destroy(st_pbf* s);
-/* Sim::add / fillBox (native/splash.cpp:78-89): n particles. */
+/* GpuSim.add (src/gpu.js:390-402) for n particles (vel3 may be NULL: at rest); the ring overwrites slots once the cap is
+ * reached while recycling is on. *added: how many were taken. */
 st_status st_pbf_add(st_pbf* s, const float* pos3, const float* vel3, uint32_t n, uint32_t* added);
-/* Sim::step (native/splash.cpp:212-247), GpuSim.step (src/gpu.js:409-428). */
+/* GpuSim.setCap / clear / recycle (src/gpu.js:387-389) */
+st_status st_pbf_set_cap(st_pbf* s, uint32_t cap);
+st_status st_pbf_clear(st_pbf* s);
+st_status st_pbf_set_recycle(st_pbf* s, int32_t on);
+/* GpuSim.step (src/gpu.js:409-428): predict, grid, iters x (lambda, delta, applyDelta), finalize, viscosity. Enqueues. */
 st_status st_pbf_step(st_pbf* s, double dt, const st_pbf_opts* o);
-/* positions (xyz, speed in w) and velocities in id order. */
+/* readbackInto (src/gpu.js:430-443): positions (xyz, speed in w) and velocities of the N slots in index order. */
 st_status st_pbf_read(st_pbf* s, float* pos4, float* vel4, uint32_t cap, uint32_t* n);
 void* st_pbf_stream(st_pbf* s);
 

@@ -31,47 +31,11 @@
 
 #include "../include/splashtank_cuda.h"
 #include "../include/st_math.h"
+#include "oracle_math.h"
+#include "pbf_core.h"
 
 namespace {
 
-struct V3 { float x, y, z; };
-inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
-inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-inline V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-inline V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
-inline V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
-inline V3 operator/(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
-inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline float length(V3 a) { return sqrtf(dot(a, a)); }
-inline float fmin_(float a, float b) { return a < b ? a : b; }
-inline float fmax_(float a, float b) { return a > b ? a : b; }
-inline float clampf(float x, float lo, float hi) { return fmin_(fmax_(x, lo), hi); }
-inline V3 vmin(V3 a, V3 b) { return v3(fmin_(a.x, b.x), fmin_(a.y, b.y), fmin_(a.z, b.z)); }
-inline V3 vmax(V3 a, V3 b) { return v3(fmax_(a.x, b.x), fmax_(a.y, b.y), fmax_(a.z, b.z)); }
-inline V3 vclamp(V3 a, V3 lo, V3 hi) { return vmin(vmax(a, lo), hi); }
-inline V3 vfloor(V3 a) { return v3(floorf(a.x), floorf(a.y), floorf(a.z)); }
-inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
-inline V3 vmix(V3 a, V3 b, float t) { return v3(mixf(a.x, b.x, t), mixf(a.y, b.y, t), mixf(a.z, b.z, t)); }
-inline V3 cross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-inline float smoothstep(float e0, float e1, float x) { float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f); return t * t * (3.0f - 2.0f * t); }
-inline float comp(V3 a, int ax) { return ax == 0 ? a.x : (ax == 1 ? a.y : a.z); }
-inline void setc(V3& a, int ax, float v) { if (ax == 0) a.x = v; else if (ax == 1) a.y = v; else a.z = v; }
-inline float bitsf(int32_t i) { float f; memcpy(&f, &i, 4); return f; }
-inline int32_t fbits(float f) { int32_t i; memcpy(&i, &f, 4); return i; }
-// WGSL u32(f): truncation, saturating at 0 for negative values
-inline uint32_t u32f(float f) { return f <= 0.0f ? 0u : (uint32_t)f; }
-// WGSL i32(f): truncation, saturating at the ends of the range; NaN gives 0
-inline int32_t i32f(float f) {
-  if (!(f == f)) return 0;
-  if (f >= 2147483648.0f) return 2147483647;
-  if (f <= -2147483648.0f) return (int32_t)0x80000000u;
-  return (int32_t)f;
-}
-// a floored coordinate as an index, held in [-2, 2^24] so that index + 1 cannot overflow (in-range values unchanged)
-inline int i32idx(float f) { return std::min(std::max(i32f(f), -2), 1 << 24); }
-
-const float DEADY = -1.0e5f;
 const uint32_t NONE = 0xffffffffu;
 const float WWHOLD = 0.2f;
 
@@ -197,35 +161,7 @@ struct Oracle {
 
   // ---- colliders (gpu.js:6-38, wgsl-core.js:113-131) ----
   const float* col(uint32_t k, int m) const { return &cols[(size_t)k * 32 + (size_t)m * 4]; }
-  void sdfEval(uint32_t k, V3 p, float& phi, V3& wn) const {
-    const float* a = col(k, 0); const float* b = col(k, 1);
-    V3 r0 = v3(col(k, 2)[0], col(k, 2)[1], col(k, 2)[2]);
-    V3 r1 = v3(col(k, 3)[0], col(k, 3)[1], col(k, 3)[2]);
-    V3 r2 = v3(col(k, 4)[0], col(k, 4)[1], col(k, 4)[2]);
-    V3 d_ = p - v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]);
-    V3 lp = v3(dot(r0, d_), dot(r1, d_), dot(r2, d_));
-    V3 g = (lp - v3(b[0], b[1], b[2])) / b[3];
-    V3 dims = v3(a[1], a[2], a[3]);
-    V3 gc = vclamp(g, v3(0, 0, 0), dims - v3(1.0001f, 1.0001f, 1.0001f));
-    V3 fl = vfloor(gc); V3 f = gc - fl;
-    uint32_t nx_ = u32f(a[1]), ny_ = u32f(a[2]);
-    uint32_t base = u32f(a[0]) + u32f(fl.x) + nx_ * (u32f(fl.y) + ny_ * u32f(fl.z));
-    uint32_t s = nx_ * ny_;
-    const float* sd = sdf.data();
-    float v000 = sd[base], v100 = sd[base + 1], v010 = sd[base + nx_], v110 = sd[base + nx_ + 1];
-    float v001 = sd[base + s], v101 = sd[base + s + 1], v011 = sd[base + s + nx_], v111 = sd[base + s + nx_ + 1];
-    float c00 = mixf(v000, v100, f.x), c10 = mixf(v010, v110, f.x), c01 = mixf(v001, v101, f.x), c11 = mixf(v011, v111, f.x);
-    float c0 = mixf(c00, c10, f.y), c1 = mixf(c01, c11, f.y);
-    phi = mixf(c0, c1, f.z);
-    V3 out = g - gc; V3 gl;
-    if (dot(out, out) > 0.0f) {
-      float l = length(out); phi += l * b[3]; gl = out / l;
-    } else {
-      gl = v3(mixf(mixf(v100 - v000, v110 - v010, f.y), mixf(v101 - v001, v111 - v011, f.y), f.z), mixf(c10 - c00, c11 - c01, f.z), c1 - c0);
-      float l = length(gl); gl = gl / fmax_(l, 1e-9f);
-    }
-    wn = r0 * gl.x + r1 * gl.y + r2 * gl.z;
-  }
+  void sdfEval(uint32_t k, V3 p, float& phi, V3& wn) const { sdfEvalRec(cols.data(), sdf.data(), k, p, phi, wn); }
   V3 colSurfVel(uint32_t k, V3 p) const {
     V3 c = v3(col(k, 5)[0], col(k, 5)[1], col(k, 5)[2]);
     return v3(col(k, 6)[0], col(k, 6)[1], col(k, 6)[2]) + cross(v3(col(k, 7)[0], col(k, 7)[1], col(k, 7)[2]), p - c);
@@ -1038,6 +974,34 @@ struct Oracle {
     std::copy(air2.begin(), air2.begin() + (size_t)na * 4, air.begin());        // airCopy
   }
 
+  // PBF density constraints on the particles at the end of the step (st_step_opts.pbf_iters; the reference's FLIP step
+  // has none): GpuSim's grid, lambda and delta (src/gpu.js:162-292, restated in pbf_core.h) with kernel radius 2.2 d,
+  // the walls' and colliders' boundary density, collideP after each correction; then v += (x - p) / dt, pos.w again
+  void stagePbf(double dt, int iters) {
+    const PbfConsts pc = pbfConsts(d, 0.0, 0.0);
+    const double lo[3] = {bx0, by0, bz0}, hi[3] = {bx1, by1, bz1};
+    const PbfP Q = pbfParams(pc, d, lo, hi, dt, 0.0, 0.0, N, P.ncols, open);
+    std::vector<float> prd((size_t)N * 4), lam, bgr, dlt;
+    for (size_t i = 0; i < (size_t)N; i++) {
+      prd[i * 4] = pos[i * 4]; prd[i * 4 + 1] = pos[i * 4 + 1]; prd[i * 4 + 2] = pos[i * 4 + 2]; prd[i * 4 + 3] = 0.0f;
+    }
+    PbfGrid G;
+    pbfBuildGrid(Q, prd.data(), 4, N, G);
+    auto sdfOf = [&](uint32_t k, V3 x, float& phi, V3& wn) { sdfEval(k, x, phi, wn); };
+    auto col = [&](V3 p) { return collideP(p); };
+    for (int it = 0; it < iters; it++) pbfIteration(Q, sdfOf, P.ncols, col, G, prd.data(), N, lam, bgr, dlt, nthreads);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t ii = 0; ii < (int64_t)N; ii++) {
+      const size_t i = (size_t)ii;
+      if (G.cid[i] == PBF_DEADC) continue;
+      const V3 x = v3(prd[i * 4], prd[i * 4 + 1], prd[i * 4 + 2]);
+      const V3 v = pvel((uint32_t)i) + (x - ppos((uint32_t)i)) / Q.dt;
+      const float foam = vel[i * 4 + 3];
+      pos[i * 4] = x.x; pos[i * 4 + 1] = x.y; pos[i * 4 + 2] = x.z; pos[i * 4 + 3] = fmin_(length(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f);
+      vel[i * 4] = v.x; vel[i * 4 + 1] = v.y; vel[i * 4 + 2] = v.z;
+    }
+  }
+
   void stageSpray(bool emit) {
     if (P.airOn != 0u) stageAir();   // the air field first, so the whitewater moves with this step's air (sim.js:297-301)
     uint32_t m = std::min(sctl0, P.smax);
@@ -1303,6 +1267,7 @@ struct Oracle {
     stageG2P();
     if (sprayCap > 0) stageSpray(sprOn);
     if (nbOn) stageReseed();
+    if (o->pbf_iters > 0) stagePbf(dt, std::min(o->pbf_iters, 64));
     steps++;
     return ST_OK;
   }

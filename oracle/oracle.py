@@ -63,22 +63,21 @@ class OracleFlipSim(FlipSim):
 
 
 _PBF = None
+_BAKER = None
 
 
 def pbf_funcs():
+    """oracle_pbf_*: the GpuSim restatement, bound with st_pbf_*'s signatures."""
     global _PBF
     if _PBF is None:
         path = os.path.join(HERE, "liboracle_pbf.so")
         if not os.path.exists(path):
             build()
         lib = C.CDLL(path)
-        f = abi.bind(lib, "oracle_", abi.PBF_FUNCS[:5])
+        f = abi.bind(lib, "oracle_", abi.PBF_FUNCS)
         f["set_threads"] = lib.oracle_pbf_set_threads
         f["set_threads"].argtypes = [C.c_void_p, C.c_int]
         f["set_threads"].restype = None
-        f["fill_box"] = lib.oracle_pbf_fill_box
-        f["fill_box"].argtypes = [C.c_void_p] + [C.c_float] * 6
-        f["fill_box"].restype = C.c_uint32
         _PBF = f
     return _PBF
 
@@ -87,17 +86,103 @@ from splashtank_b200.pbf import PbfSim  # noqa: E402
 
 
 class OraclePbfSim(PbfSim):
-    """The CPU restatement of native/splash.cpp's Sim behind PbfSim's methods."""
+    """The CPU restatement of GpuSim (oracle/pbf_oracle.cpp) behind PbfSim's methods."""
 
     def __init__(self, *a, threads=1, **k):
         super().__init__(*a, _funcs=pbf_funcs(), **k)
         self.f["set_threads"](self._h, int(threads))
+
+
+class BakerDesc(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("d", C.c_double), ("box", C.c_double * 3), ("max_n", C.c_uint32)]
+
+
+class BakerCol(C.Structure):
+    _fields_ = [("kind", C.c_int32)] + [(n, C.c_float) for n in ("x", "y", "z", "r", "hx", "hy", "hz", "yaw")]
+
+
+class BakerOpts(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("g", C.c_float), ("visc", C.c_float), ("iters", C.c_int32), ("ncols", C.c_uint32),
+                ("cols", C.POINTER(BakerCol))]
+
+
+def baker_funcs():
+    global _BAKER
+    if _BAKER is None:
+        path = os.path.join(HERE, "liboracle_baker.so")
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        sig = {"create": (C.c_int, [C.POINTER(BakerDesc), C.POINTER(C.c_void_p)]), "destroy": (None, [C.c_void_p]),
+               "set_threads": (None, [C.c_void_p, C.c_int]), "add": (C.c_int, [C.c_void_p, abi.f32p, abi.f32p, C.c_uint32, abi.u32p]),
+               "fill_box": (C.c_uint32, [C.c_void_p] + [C.c_float] * 6), "step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(BakerOpts)]),
+               "read": (C.c_int, [C.c_void_p, abi.f32p, abi.f32p, C.c_uint32, abi.u32p])}
+        f = {}
+        for k, (res, args) in sig.items():
+            fn = getattr(lib, "oracle_baker_" + k)
+            fn.restype, fn.argtypes = res, args
+            f[k] = fn
+        _BAKER = f
+    return _BAKER
+
+
+class OracleBakerSim:
+    """The CPU restatement of native/splash.cpp's Sim (oracle/baker_oracle.cpp): analytic sphere and yawed box colliders
+    {"kind": "sphere", x, y, z, r} / {"kind": "box", x, y, z, hx, hy, hz, yaw}, a 48-neighbour cap, closed walls."""
+
+    def __init__(self, d, maxN, size=None, threads=1):
+        self.f = baker_funcs()
+        desc = BakerDesc()
+        desc.size = C.sizeof(BakerDesc)
+        desc.d = float(d)
+        desc.box[:] = [float(x) for x in (size or (3.0, 2.6, 3.0))]
+        desc.max_n = int(maxN)
+        h = C.c_void_p()
+        if self.f["create"](C.byref(desc), C.byref(h)) != abi.ST_OK:
+            raise RuntimeError("baker oracle create failed")
+        self._h = h
+        self.f["set_threads"](self._h, int(threads))
+        self.n = 0
 
     def fill_box_baker(self, x0, x1, y0, y1, z0, z1):
         """The baker's own fillBox (native/splash.cpp:85-89): lattice plus jitter from mt19937 seeded 12345."""
         n = self.f["fill_box"](self._h, x0, x1, y0, y1, z0, z1)
         self.n += n
         return n
+
+    def add_many(self, pos3, vel3=None):
+        p = np.ascontiguousarray(pos3, np.float32).reshape(-1, 3)
+        v = None if vel3 is None else np.ascontiguousarray(vel3, np.float32).reshape(-1, 3)
+        got = C.c_uint32()
+        self.f["add"](self._h, p.ctypes.data_as(abi.f32p), None if v is None else v.ctypes.data_as(abi.f32p), len(p), C.byref(got))
+        self.n += got.value
+        return got.value
+
+    def step(self, dt, o):
+        cols = o.get("cols") or []
+        arr = (BakerCol * max(len(cols), 1))()
+        for k, c in enumerate(cols):
+            arr[k].kind = 1 if c.get("kind") == "box" else 0
+            for f in ("x", "y", "z", "r", "hx", "hy", "hz", "yaw"):
+                setattr(arr[k], f, float(c.get(f, 0.0)))
+        op = BakerOpts()
+        op.size = C.sizeof(BakerOpts)
+        op.g, op.visc, op.iters, op.ncols = float(o.get("g", 9.8)), float(o.get("visc", 0.0)), int(o.get("iters", 3)), len(cols)
+        op.cols = C.cast(arr, C.POINTER(BakerCol))
+        self.f["step"](self._h, float(dt), C.byref(op))
+
+    def particles(self):
+        p = np.zeros((max(self.n, 1), 4), np.float32)
+        v = np.zeros((max(self.n, 1), 4), np.float32)
+        got = C.c_uint32()
+        self.f["read"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p), self.n, C.byref(got))
+        return p[:got.value], v[:got.value]
+
+    def __del__(self):
+        try:
+            self.f["destroy"](self._h)
+        except Exception:
+            pass
 
 
 class OraclePoisson:

@@ -42,7 +42,7 @@ class StepOpts(C.Structure):
                 ("drip_on", C.c_int32), ("drip_rate", C.c_float), ("drip_dry", C.c_float),
                 ("ocean_on", C.c_int32), ("ocean_level", C.c_float), ("ocean_layer", C.c_float), ("ocean_length", C.c_float),
                 ("ocean_height", C.c_float), ("ocean_dir", C.c_float), ("ocean_spread", C.c_float), ("ocean_seed", C.c_int32),
-                ("time", C.c_float)]
+                ("time", C.c_float), ("pbf_iters", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -61,7 +61,7 @@ class Dims(C.Structure):
 
 
 STAGES = ("sort", "blocks", "clear", "p2g", "narrow_band", "classify", "norm_faces", "divergence", "pressure", "project", "g2p",
-          "spray", "reseed", "total")
+          "pbf", "spray", "reseed", "total")
 
 
 class StageTimes(C.Structure):
@@ -73,13 +73,9 @@ class PbfDesc(C.Structure):
                 ("device", C.c_int32), ("eps_k", C.c_double), ("wall_k", C.c_double)]
 
 
-class PbfCol(C.Structure):
-    _fields_ = [("kind", C.c_int32)] + [(n, C.c_float) for n in ("x", "y", "z", "r", "hx", "hy", "hz", "yaw")]
-
-
 class PbfOpts(C.Structure):
     _fields_ = [("size", C.c_uint32), ("g", C.c_float), ("visc", C.c_float), ("iters", C.c_int32), ("ncols", C.c_uint32),
-                ("cols", C.POINTER(PbfCol))]
+                ("cols", C.POINTER(Collider))]
 
 
 class PoissonDesc(C.Structure):
@@ -221,6 +217,9 @@ PBF_FUNCS = [
     ("pbf_add", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
     ("pbf_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(PbfOpts)]),
     ("pbf_read", C.c_int, [C.c_void_p, f32p, f32p, C.c_uint32, u32p]),
+    ("pbf_set_cap", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("pbf_clear", C.c_int, [C.c_void_p]),
+    ("pbf_set_recycle", C.c_int, [C.c_void_p, C.c_int32]),
     ("pbf_stream", C.c_void_p, [C.c_void_p]),
 ]
 

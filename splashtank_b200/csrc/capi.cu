@@ -11,6 +11,7 @@
 #include "../../include/splashtank_cuda.h"
 #include "common.cuh"
 #include "kernels.h"
+#include "pbf_core.cuh"
 
 using namespace st;
 
@@ -71,12 +72,13 @@ struct st_flip {
   // per-step uploads (parameter block + collider records) come from a ring of pinned host blocks, so the copies are
   // asynchronous and a block is rewritten only after the copy that read it has run
   static constexpr int RING = 16;
-  struct Upload { FlipParams P; alignas(16) float cols[32 * 32]; alignas(16) float waves[32 * 8]; };   // cols and waves: float4 reads
+  // cols and waves: float4 reads; pbf: the density stage's block (st_step_opts.pbf_iters)
+  struct Upload { FlipParams P; alignas(16) float cols[32 * 32]; alignas(16) float waves[32 * 8]; alignas(16) PbfParams pbf; };
   Upload* ring_h = nullptr;
   cudaEvent_t ring_ev[RING] = {};
   int ring_i = 0;
   // stage timing without stalls: each step records its stage events into a ring; st_flip_read_timing sums them
-  static constexpr int TSLOTS = 256, TEV = 11;
+  static constexpr int TSLOTS = 256, TEV = 12;
   bool timing = false;
   cudaEvent_t tev[TSLOTS][TEV] = {};
   uint32_t tcount = 0;
@@ -149,8 +151,12 @@ struct st_flip {
   cudaEvent_t ev[16] = {};
   int cur = 0;   // part[cur] holds this step's storage order
   uint64_t launches = 0;   // kernels launched by steps since create
-  struct Graph { uint64_t key = 0; cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t evnode[11] = {}; int launches = 0; };
+  struct Graph { uint64_t key = 0; cudaGraph_t graph = nullptr; cudaGraphExec_t exec = nullptr; cudaGraphNode_t evnode[TEV] = {}; int launches = 0; };
   std::vector<Graph> graphs;
+  // the PBF density stage's buffers, made on the first step that asks for it
+  PbfDev pbf{};
+  PbfHostConsts pbfc{};
+  uint32_t pbfCells = 0;
   bool use_graphs = true;
   // CTAs per SM of the per-tile kernels (heavy: p2g, g2p; light: the rest) and of the pressure sweeps
   int gridT = 8, gridT4 = 4, gridSor = 8;
@@ -207,6 +213,7 @@ void st_flip_destroy(st_flip* s) {
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
   if (s->dUp) cudaFree(s->dUp);
+  if (s->pbf.key) { s->pbf.P = nullptr; pbf_dev_free(s->pbf); }   // P points into the upload buffer
   for (auto& e : s->ring_ev) if (e) cudaEventDestroy(e);
   for (auto& row : s->tev) for (auto& e : row) if (e) cudaEventDestroy(e);
   for (auto& e : s->ev) if (e) cudaEventDestroy(e);
@@ -518,13 +525,14 @@ static void pack_params(st_flip* s, double dt, const st_step_opts* o, uint32_t n
 static void stage_fill(st_stage_times* t, const float* ms, float total) {
   t->sort = 0.0f; t->blocks = ms[0]; t->clear = 0.0f; t->p2g = ms[1]; t->narrow_band = ms[2]; t->classify = ms[3];
   t->norm_faces = ms[4]; t->divergence = 0.0f; t->pressure = ms[5]; t->project = ms[6]; t->g2p = ms[7]; t->spray = ms[8];
-  t->reseed = ms[9]; t->total = total;
+  t->reseed = ms[9]; t->pbf = ms[10]; t->total = total;
 }
 
 // The device work of one step after the uploads: counters reset, then the stages in the reference's order
-// (src/flip/sim.js:253-309). mark(k) is called at the 11 stage boundaries. Returns the kernels launched.
+// (src/flip/sim.js:253-309), then the PBF density stage when pbfIters > 0. mark(k) is called at the 12 stage
+// boundaries. Returns the kernels launched.
 template <class Mark>
-static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, bool sprOn, int iters, Mark mark) {
+static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, bool sprOn, int iters, int pbfIters, Mark mark) {
   cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q);        // fluid, vmaxBits, nLive (nActive is kept)
   cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q);
   cudaMemsetAsync(&s->dCtl->emitTried, 0, 2 * sizeof(uint32_t), q);     // emitTried, nFluidTiles
@@ -560,6 +568,10 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(9);
   if (nbOn) nl += launch_nb_reseed(B, gT4, q);
   mark(10);
+  // the density stage last: the whitewater, the air field and the narrow band's trim and refill above all see the
+  // particles g2p moved (their emission counts and trim tests are fused into g2p)
+  if (pbfIters > 0) nl += launch_flip_pbf(B, s->pbf, pbfIters, std::max(1, std::min<int>(s->sms * 8, (int)((s->N + PBF_T - 1) / PBF_T))), q);
+  mark(11);
   return nl;
 }
 
@@ -567,13 +579,13 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
 // the particle count (grid sizes), SOR iterations, narrow band, whitewater emission, the air field, drips, the ocean
 // and stage timing. Stage markers are external event-record nodes, pointed at the timing ring's events before each
 // launch.
-static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, bool timing) {
+static uint64_t graph_key(const st_flip* s, bool nbOn, bool sprOn, int iters, int pbfIters, bool timing) {
   return (uint64_t)s->cur | ((uint64_t)s->parity << 1) | ((uint64_t)nbOn << 2) | ((uint64_t)sprOn << 3) | ((uint64_t)timing << 4) |
          ((uint64_t)(s->hp.airOn != 0) << 5) | ((uint64_t)(s->hp.ndrip != 0) << 6) | ((uint64_t)(s->hp.ocean != 0) << 7) |
-         ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24);
+         ((uint64_t)(iters & 0xffff) << 8) | ((uint64_t)s->N << 24) | ((uint64_t)(pbfIters & 0xff) << 56);
 }
-static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, bool timing, st_flip::Graph** out) {
-  const uint64_t key = graph_key(s, nbOn, sprOn, iters, timing);
+static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int iters, int pbfIters, bool timing, st_flip::Graph** out) {
+  const uint64_t key = graph_key(s, nbOn, sprOn, iters, pbfIters, timing);
   for (auto& g : s->graphs) if (g.exec && g.key == key) { *out = &g; return ST_OK; }
   if (s->graphs.size() >= 8) {   // a small cache: drop the oldest
     if (s->graphs.front().exec) cudaGraphExecDestroy(s->graphs.front().exec);
@@ -583,7 +595,7 @@ static st_status get_graph(st_flip* s, const Bufs& B, bool nbOn, bool sprOn, int
   cudaStream_t q = s->stream;
   cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(q, cudaStreamCaptureModeThreadLocal));
-  int nl = enqueue_step(s, B, q, nbOn, 0, sprOn, iters, [&](int k) {
+  int nl = enqueue_step(s, B, q, nbOn, 0, sprOn, iters, pbfIters, [&](int k) {
     if (timing) cudaEventRecordWithFlags(s->tev[0][k], q, cudaEventRecordExternal);
   });
   cudaError_t e = cudaStreamEndCapture(q, &graph);
@@ -629,7 +641,7 @@ static void drop_graphs(st_flip* s) {
 }
 
 // The host half of a step: parameter block, collider records and counters, with the uploads enqueued on q.
-struct StepPrep { bool nbOn = false, sprOn = false; uint32_t init = 0; int iters = 1; };
+struct StepPrep { bool nbOn = false, sprOn = false; uint32_t init = 0; int iters = 1, pbfIters = 0; };
 static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cudaStream_t q, StepPrep* pr) {
   const bool nbOn = o->nb_on != 0 || o->ocean_on != 0;   // the ocean keeps its water by depth: it turns the narrow band on
   if (nbOn) s->velGOn = true;
@@ -678,6 +690,23 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
   s->lastNb = nbOn;
   if (init) { s->nbInit = 0; s->fills.clear(); s->fillVols.clear(); }
   const int iters = std::max(1, o->iters);
+  // the PBF density stage: its block (FluidSim's constants for this spacing, the tank's box and walls, this step's dt
+  // and colliders) and, on first use, its buffers (outside any graph capture)
+  const int pbfIters = std::min(std::max(o->pbf_iters, 0), 64);
+  if (pbfIters > 0) {
+    if (!s->pbf.key) {
+      s->pbfc = pbf_consts(s->d, 0.0, 0.0);
+      const double lo[3] = {s->bx0, s->by0, s->bz0}, hi[3] = {s->bx1, s->by1, s->bz1};
+      const PbfParams P0 = pbf_params(s->pbfc, s->d, lo, hi, dt, 0.0, 0.0, 0, 0, s->open);
+      s->pbfCells = P0.ncell;
+      cudaError_t e = pbf_dev_alloc(s->pbf, s->maxN, s->pbfCells);
+      if (e != cudaSuccess) { pbf_dev_free(s->pbf); set_err("pbf stage buffers", e); return e == cudaErrorMemoryAllocation ? ST_OOM : ST_DEVICE_ERROR; }
+      cudaFree(s->pbf.P);   // the block lives in the upload buffer
+    }
+    s->pbf.P = &s->dUp->pbf;
+    const double lo[3] = {s->bx0, s->by0, s->bz0}, hi[3] = {s->bx1, s->by1, s->bz1};
+    up->pbf = pbf_params(s->pbfc, s->d, lo, hi, dt, 0.0, 0.0, s->N, nc, s->open);
+  }
   // this step's storage order goes into the other particle buffer; cell counts alternate buffers
   s->cur ^= 1;
   s->parity ^= 1;
@@ -688,8 +717,9 @@ static st_status prepare_step(st_flip* s, double dt, const st_step_opts* o, cuda
     memcpy(up->waves, s->waves, s->hp.nwave * 8 * sizeof(float));
     CK(cudaMemcpyAsync(s->dUp->waves, up->waves, s->hp.nwave * 8 * sizeof(float), cudaMemcpyHostToDevice, q));
   }
+  if (pbfIters > 0) CK(cudaMemcpyAsync(&s->dUp->pbf, &up->pbf, sizeof(PbfParams), cudaMemcpyHostToDevice, q));
   CK(cudaEventRecord(upEv, q));
-  pr->nbOn = nbOn; pr->sprOn = sprOn; pr->init = init; pr->iters = iters;
+  pr->nbOn = nbOn; pr->sprOn = sprOn; pr->init = init; pr->iters = iters; pr->pbfIters = pbfIters;
   return ST_OK;
 }
 
@@ -738,7 +768,7 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   const Bufs B = s->bufs();
   cudaEvent_t* tslot = nullptr;
   if (s->timing) {
-    if (s->tcount >= (uint32_t)st_flip::TSLOTS) CK(cudaEventSynchronize(s->tev[s->tcount % st_flip::TSLOTS][10]));
+    if (s->tcount >= (uint32_t)st_flip::TSLOTS) CK(cudaEventSynchronize(s->tev[s->tcount % st_flip::TSLOTS][st_flip::TEV - 1]));
     tslot = s->tev[s->tcount % st_flip::TSLOTS];
   }
   if (!s->trkStart[0])
@@ -751,7 +781,7 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   int nl = 0;
   if (s->use_graphs && !t && !init) {
     st_flip::Graph* g = nullptr;
-    st = get_graph(s, B, nbOn, sprOn, iters, tslot != nullptr, &g);
+    st = get_graph(s, B, nbOn, sprOn, iters, pr.pbfIters, tslot != nullptr, &g);
     if (st != ST_OK) return st;
     if (tslot)
       for (int k = 0; k < st_flip::TEV; k++) CK(cudaGraphExecEventRecordNodeSetEvent(g->exec, g->evnode[k], tslot[k]));
@@ -760,7 +790,7 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
     nl = g->launches;
   } else {
     CK(cudaEventRecord(s->trkStart[tk], q));
-    nl = enqueue_step(s, B, q, nbOn, init, sprOn, iters, [&](int k) {
+    nl = enqueue_step(s, B, q, nbOn, init, sprOn, iters, pr.pbfIters, [&](int k) {
       if (t) cudaEventRecord(s->ev[k], q);
       if (tslot) cudaEventRecord(tslot[k], q);
     });
@@ -772,11 +802,12 @@ static st_status do_step(st_flip* s, double dt, const st_step_opts* o, st_stage_
   s->steps++;
   if (tslot) s->tcount++;
   if (t) {
-    CK(cudaEventSynchronize(s->ev[10]));
-    float ms[10];
-    for (int k = 0; k < 10; k++) cudaEventElapsedTime(&ms[k], s->ev[k], s->ev[k + 1]);
+    constexpr int L = st_flip::TEV - 1;
+    CK(cudaEventSynchronize(s->ev[L]));
+    float ms[L];
+    for (int k = 0; k < L; k++) cudaEventElapsedTime(&ms[k], s->ev[k], s->ev[k + 1]);
     float tot = 0.0f;
-    cudaEventElapsedTime(&tot, s->ev[0], s->ev[10]);
+    cudaEventElapsedTime(&tot, s->ev[0], s->ev[L]);
     stage_fill(t, ms, tot);
   }
   return ST_OK;
@@ -802,11 +833,12 @@ st_status st_flip_read_timing(st_flip* s, st_stage_times* sum, uint32_t* nsteps)
   memset(sum, 0, sizeof(*sum));
   uint32_t n = std::min<uint32_t>(s->tcount, st_flip::TSLOTS);
   if (n) CK(cudaStreamSynchronize(s->stream));
-  float acc[10] = {0}, tot = 0.0f;
+  constexpr int L = st_flip::TEV - 1;
+  float acc[L] = {0}, tot = 0.0f;
   for (uint32_t k = 0; k < n; k++) {
     cudaEvent_t* e = s->tev[(s->tcount - 1 - k) % st_flip::TSLOTS];
-    for (int j = 0; j < 10; j++) { float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[j], e[j + 1])); acc[j] += ms; }
-    float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[0], e[10])); tot += ms;
+    for (int j = 0; j < L; j++) { float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[j], e[j + 1])); acc[j] += ms; }
+    float ms = 0.0f; CK(cudaEventElapsedTime(&ms, e[0], e[L])); tot += ms;
   }
   stage_fill(sum, acc, tot);
   if (nsteps) *nsteps = n;
@@ -1650,10 +1682,10 @@ st_status st_batch_step(st_batch* b, double dt, const st_step_opts* const* opts)
     const Bufs B = s->bufs();
     int nl = 0;
     if (pr.init || !s->use_graphs) {
-      nl = enqueue_step(s, B, q, pr.nbOn, pr.init, pr.sprOn, pr.iters, [](int) {});
+      nl = enqueue_step(s, B, q, pr.nbOn, pr.init, pr.sprOn, pr.iters, pr.pbfIters, [](int) {});
     } else {
       st_flip::Graph* g = nullptr;
-      st = get_graph(s, B, pr.nbOn, pr.sprOn, pr.iters, false, &g);
+      st = get_graph(s, B, pr.nbOn, pr.sprOn, pr.iters, pr.pbfIters, false, &g);
       if (st != ST_OK) return st;
       nl = g->launches;
       if (b->mode == ST_BATCH_SEQUENTIAL) {

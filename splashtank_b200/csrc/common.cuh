@@ -389,6 +389,21 @@ __device__ __forceinline__ int colAt(const FlipParams& P, const float4* __restri
   return -1;
 }
 
+// collideP (src/flip/wgsl-solver.js:185-197): out of every collider near p by q0, then the walls less the margin
+__device__ __forceinline__ V3 collideP(const FlipParams& P, const float4* __restrict__ cols, const float* __restrict__ sdf, V3 pin) {
+  V3 p = pin;
+  const float m = P.margin;
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    if (!colNear(P, cols, k, p)) continue;
+    float phi; V3 wn;
+    sdfEval(cols, sdf, k, p, phi, wn);
+    if (phi < P.q0) p = p + wn * (P.q0 - phi);
+  }
+  const float big = 1.0e9f;
+  const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
+  const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
+  return vclamp(p, lo, hi);
+}
 // ---- whitewater emission terms (sprayEmit, src/flip/wgsl-whitewater.js:101-117), shared by g2p and the emit pass ----
 constexpr uint8_t EMIT_KILL = 0x80;   // emitK flag: the narrow band trims this particle once its points are written
 __device__ __forceinline__ float wetCellAt(const FlipParams& P, const float* __restrict__ wet, int i, int j, int k) {

@@ -704,20 +704,6 @@ __device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, cons
   const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
   return vclamp(p, lo, hi);
 }
-__device__ __forceinline__ V3 collideP(const FlipParams& P, const Bufs& B, V3 pin) {
-  V3 p = pin;
-  const float m = P.margin;
-  for (uint32_t k = 0; k < P.ncols; k++) {
-    if (!colNear(P, B.cols, k, p)) continue;
-    float phi; V3 wn;
-    sdfEval(B.cols, B.sdf, k, p, phi, wn);
-    if (phi < P.q0) p = p + wn * (P.q0 - phi);
-  }
-  const float big = 1.0e9f;
-  const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
-  const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
-  return vclamp(p, lo, hi);
-}
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
   const float2* v;   // [3][1000]: (vn, vo) of each face, one 64-bit load per corner

@@ -1,0 +1,214 @@
+// pbf_core.cuh - position-based fluid passes on sm_100a with the semantics of GpuSim (src/gpu.js:102-353), shared by
+// the PBF engine (st_pbf_*) and the density stage of the FLIP step, whose kernels are in pbf.cu.
+//
+// Design: every step sorts the live particles by uniform-grid cell (cell size h = 2.2 d) into a cell-sorted copy of
+// their positions, so each solver pass is one thread per sorted slot and the 27-cell neighbour loops read contiguous
+// runs of that copy: the lanes of a warp sit in one or two cells and read the same neighbours (L1 broadcasts), instead
+// of the reference's gathers through an index list. Inside a cell the order is ascending particle index (the
+// reference's atomic scatter leaves it open), fixed by a rank pass after the scatter, so every float sum is
+// reproducible and equal to the oracle's. delta and applyDelta are one kernel writing a second position buffer (the
+// neighbours' positions of the same iteration stay intact), so an iteration is two launches.
+// Arithmetic: f32 in the reference's source order, no contraction (-fmad=false), inverseSqrt as 1 / sqrt.
+#pragma once
+#include "common.cuh"
+
+namespace st {
+
+// GpuSim's uniform block (struct Params, src/gpu.js:73-82), plus 1 / h and 1 / rho0 (computed in f32 by the shaders)
+struct PbfParams {
+  uint32_t n, nx, ny, nz, ncols, open, ncell, pad;
+  float dt, h, h2, d, rho0, poly, spiky, W0, eps, c0, Gh, margin, gravity, visc, rest, relax;
+  float bx0, bx1, by0, by1, bz0, bz1, maxD, vmax, inv, irho;
+};
+constexpr uint32_t PBF_DEAD = 0xffffffffu;
+// the uniform block into the CTA's shared copy (every thread calls it; it ends with a barrier)
+__device__ __forceinline__ void loadPbf(PbfParams& s, const PbfParams* g) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
+  for (int i = threadIdx.x; i < (int)(sizeof(PbfParams) / 4); i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+constexpr int PBF_T = 256;
+constexpr int PBF_SCAN = 2048;   // cells per block of the grid scan
+
+// Gf (src/gpu.js:116-121)
+__device__ __forceinline__ float pbfGf(const PbfParams& P, float s) {
+  const float h2 = P.h2, h4 = h2 * h2, h6 = h4 * h2, h8 = h4 * h4;
+  const float s2 = s * s, s3 = s2 * s, s5 = s3 * s2, s7 = s5 * s2, s9 = s7 * s2;
+  return h8 * s - (4.0f / 3.0f) * h6 * s3 + (6.0f / 5.0f) * h4 * s5 - (4.0f / 7.0f) * h2 * s7 + s9 / 9.0f;
+}
+// surf (src/gpu.js:123-128)
+__device__ __forceinline__ void pbfSurf(const PbfParams& P, float phi0, float& rho, float& drho) {
+  const float p = fmx(phi0, 0.0f);
+  const float t = P.h2 - p * p;
+  const float t2 = t * t;
+  rho = P.c0 * (P.Gh - pbfGf(P, p));
+  drho = -P.c0 * t2 * t2;
+}
+// bnd (src/gpu.js:129-148): boundary density and its gradient from the closed walls and every collider's grid
+__device__ __forceinline__ void pbfBnd(const PbfParams& P, const float4* __restrict__ cols, const float* __restrict__ sdf, V3 x, float& rho, V3& g) {
+  const float h = P.h;
+  rho = 0.0f;
+  g = v3(0.0f, 0.0f, 0.0f);
+  float r, dr;
+  float ph = x.x - P.bx0; if ((P.open & 1u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.x += dr; }
+  ph = P.bx1 - x.x; if ((P.open & 2u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.x -= dr; }
+  ph = x.y - P.by0; if ((P.open & 4u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.y += dr; }
+  ph = P.by1 - x.y; if ((P.open & 8u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.y -= dr; }
+  ph = x.z - P.bz0; if ((P.open & 16u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.z += dr; }
+  ph = P.bz1 - x.z; if ((P.open & 32u) == 0u && ph < h) { pbfSurf(P, ph, r, dr); rho += r; g.z -= dr; }
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    float phi; V3 wn;
+    sdfEval(cols, sdf, k, x, phi, wn);
+    if (phi >= h) continue;
+    pbfSurf(P, phi, r, dr);
+    rho += r;
+    g = g + wn * dr;
+  }
+}
+// collide (src/gpu.js:102-114): out of every collider by the margin, then the closed walls
+__device__ __forceinline__ V3 pbfCollide(const PbfParams& P, const float4* __restrict__ cols, const float* __restrict__ sdf, V3 pin) {
+  V3 p = pin;
+  const float m = P.margin;
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    float phi; V3 wn;
+    sdfEval(cols, sdf, k, p, phi, wn);
+    if (phi < m) p = p + wn * (m - phi);
+  }
+  const float big = 1.0e9f;
+  const V3 lo = v3((P.open & 1u) ? -big : P.bx0 + m, (P.open & 4u) ? -big : P.by0 + m, (P.open & 16u) ? -big : P.bz0 + m);
+  const V3 hi = v3((P.open & 2u) ? big : P.bx1 - m, (P.open & 8u) ? big : P.by1 - m, (P.open & 32u) ? big : P.bz1 - m);
+  return vclamp(p, lo, hi);
+}
+// WGSL i32(f) (truncation, saturating) clamped into [0, n - 1]
+__device__ __forceinline__ int pbfAxisCell(float f, uint32_t n) {
+  int c = (f == f) ? (f >= 2147483648.0f ? 2147483647 : (f <= -2147483648.0f ? (int)0x80000000 : (int)f)) : 0;
+  return c < 0 ? 0 : (c > (int)n - 1 ? (int)n - 1 : c);
+}
+// cellOf (src/gpu.js:149-155)
+__device__ __forceinline__ uint32_t pbfCellOf(const PbfParams& P, V3 p) {
+  const int cx = pbfAxisCell((p.x - P.bx0) * P.inv, P.nx), cy = pbfAxisCell((p.y - P.by0) * P.inv, P.ny);
+  const int cz = pbfAxisCell((p.z - P.bz0) * P.inv, P.nz);
+  return (uint32_t)cx + P.nx * ((uint32_t)cy + P.ny * (uint32_t)cz);
+}
+// the 27-cell neighbourhood as 9 runs of sorted slots (three x-adjacent cells are contiguous), z outer, y inner: the
+// loop order of lambda, delta and viscosity (src/gpu.js:220-224). Use:
+//   PbfRows R(P, c); for (int r = 0; r < R.nrows; r++) for (uint32_t s = R.begin(P, start, r), e = R.end(P, start, r); s < e; s++)
+struct PbfRows {
+  int z0, y0, ny;
+  uint32_t xa, xb;
+  int nrows;
+  __device__ __forceinline__ PbfRows(const PbfParams& P, uint32_t c) {
+    const int cx = (int)(c % P.nx);
+    const uint32_t t = c / P.nx;
+    const int cy = (int)(t % P.ny), cz = (int)(t / P.ny);
+    xa = (uint32_t)max(cx - 1, 0);
+    xb = (uint32_t)min(cx + 1, (int)P.nx - 1);
+    z0 = max(cz - 1, 0);
+    y0 = max(cy - 1, 0);
+    ny = min(cy + 1, (int)P.ny - 1) - y0 + 1;
+    nrows = (min(cz + 1, (int)P.nz - 1) - z0 + 1) * ny;
+  }
+  __device__ __forceinline__ uint32_t row(const PbfParams& P, int r) const {
+    const int z = z0 + r / ny, y = y0 + r % ny;
+    return P.nx * (uint32_t)(y + (int)P.ny * z);
+  }
+  __device__ __forceinline__ uint32_t begin(const PbfParams& P, const uint32_t* __restrict__ start, int r) const { return start[row(P, r) + xa]; }
+  __device__ __forceinline__ uint32_t end(const PbfParams& P, const uint32_t* __restrict__ start, int r) const { return start[row(P, r) + xb + 1u]; }
+};
+
+// ---- the grid of one step: count (warp-aggregated atomics), scan, scatter, canonical order ----
+// One particle per lane: its cell (or PBF_DEAD), and a provisional rank in the cell from the count's atomic.
+// Every lane of the warp must call it (the aggregation is warp-wide).
+__device__ __forceinline__ void pbfCount(uint32_t key, bool valid, uint32_t* __restrict__ cnt, uint32_t& rank) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t peers = __match_any_sync(0xffffffffu, valid && key != PBF_DEAD ? key : PBF_DEAD);
+  const uint32_t lead = (uint32_t)__ffs(peers) - 1u;
+  uint32_t base = 0;
+  if (valid && key != PBF_DEAD && lane == lead) base = atomicAdd(&cnt[key], (uint32_t)__popc(peers));
+  base = __shfl_sync(0xffffffffu, base, lead);
+  rank = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+}
+// ---- one solver iteration in sorted space ----
+// lambda (src/gpu.js:208-251) for sorted slot t
+__device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
+                                             uint32_t t, const float4* __restrict__ cols, const float* __restrict__ sdf, float& lam, V3& bgr) {
+  const V3 qi = xyz(xs[t]);
+  const float irho = P.irho;
+  float rho = P.W0, sg = 0.0f;
+  V3 g = v3(0.0f, 0.0f, 0.0f);
+  const PbfRows R(P, c);
+  for (int rr = 0; rr < R.nrows; rr++)
+    for (uint32_t s = R.begin(P, start, rr), e = R.end(P, start, rr); s < e; s++) {
+      if (s == t) continue;
+      const V3 dd = qi - xyz(xs[s]);
+      const float r2 = dot3(dd, dd);
+      if (r2 >= P.h2) continue;
+      const float tt = P.h2 - r2;
+      rho += P.poly * tt * tt * tt;
+      const float r = sqrtf(r2);
+      if (r < 1e-7f) continue;
+      const float hr = P.h - r;
+      const float f = P.spiky * hr * hr / r * irho;
+      const V3 fv = dd * f;
+      g = g + fv;
+      sg += dot3(fv, fv);
+    }
+  float br; V3 bg;
+  pbfBnd(P, cols, sdf, qi, br, bg);
+  rho += br;
+  bg = bg * irho;
+  bgr = bg;
+  g = g + bg;
+  sg += dot3(bg, bg);
+  const float C = rho * irho - 1.0f;
+  lam = C > 0.0f ? -C / (sg + dot3(g, g) + P.eps) : 0.0f;
+}
+// delta (src/gpu.js:253-286) for sorted slot t: the clamped correction
+__device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
+                                          uint32_t t, const float* __restrict__ lamS, const float4* __restrict__ bgrS) {
+  const V3 qi = xyz(xs[t]);
+  const float irho = P.irho, li = lamS[t];
+  V3 s = xyz(bgrS[t]) * li;
+  const PbfRows R(P, c);
+  for (int rr = 0; rr < R.nrows; rr++)
+    for (uint32_t q = R.begin(P, start, rr), e = R.end(P, start, rr); q < e; q++) {
+      if (q == t) continue;
+      const float sj = li + lamS[q];
+      if (sj == 0.0f) continue;
+      const V3 dd = qi - xyz(xs[q]);
+      const float r2 = dot3(dd, dd);
+      if (r2 >= P.h2) continue;
+      const float r = sqrtf(r2);
+      if (r < 1e-7f) continue;
+      const float hr = P.h - r;
+      s = s + dd * (P.spiky * hr * hr / r * irho * sj);
+    }
+  s = s * P.relax;
+  const float m2 = dot3(s, s);
+  if (m2 > P.maxD * P.maxD) s = s * (P.maxD * (1.0f / sqrtf(m2)));
+  return s;
+}
+
+// Device buffers of one solver (the engine's, or the FLIP step's density stage)
+struct PbfDev {
+  PbfParams* P = nullptr;                   // the uniform block, uploaded each step
+  uint32_t *key = nullptr, *rank = nullptr, *tmp = nullptr, *sidx = nullptr, *cellS = nullptr;   // per particle / slot
+  float4* xs[2] = {nullptr, nullptr};       // sorted positions, two iteration buffers
+  float4* bgrS = nullptr;                   // boundary gradient / rho0 per slot
+  float* lamS = nullptr;                    // lambda per slot
+  uint32_t *cnt = nullptr, *start = nullptr, *bsum = nullptr;   // per cell; scan blocks
+  uint32_t ncell = 0;
+};
+// FluidSim's constants in double (src/shared.js:236-270)
+struct PbfHostConsts { double h, h2, poly, spiky, W0, rho0, eps, c0, Gh, margin; };
+PbfHostConsts pbf_consts(double d, double epsK, double wallK);
+PbfParams pbf_params(const PbfHostConsts& c, double d, const double lo[3], const double hi[3], double dt, double g, double visc, uint32_t n,
+                     uint32_t ncols, uint32_t open);
+cudaError_t pbf_dev_alloc(PbfDev& D, uint32_t maxN, uint32_t ncell);
+void pbf_dev_free(PbfDev& D);
+size_t pbf_dev_bytes(uint32_t maxN, uint32_t ncell);
+// the FLIP step's density stage on the particles of B.pa (D.P->n slots): grid, iters x (lambda, delta + collideP), write back
+int launch_flip_pbf(const Bufs& B, const PbfDev& D, int iters, int grid, cudaStream_t s);
+
+}  // namespace st

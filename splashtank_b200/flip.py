@@ -140,6 +140,9 @@ def make_opts(o, opt=None, default=None):
         s.ocean_spread = float(oc.get("spread", 0.0))
         s.ocean_seed = int(oc.get("seed", 0))
     s.time = float(o.get("time") or 0.0)
+    # PBF density constraints on the particles after g2p: o.pbf = iterations, or {"iters": n}
+    pb = o.get("pbf")
+    s.pbf_iters = int((pb.get("iters", 0) if isinstance(pb, dict) else pb) or 0)
     return s, cols
 
 

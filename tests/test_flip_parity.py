@@ -322,6 +322,34 @@ def test_large_tank_invariants(n, steps, cap):
     assert (g["ctype"] & 255 == 1).sum() == st["fluid"]
 
 
+@pytest.mark.parametrize("scene", ["dam", "tank"])
+def test_pbf_density_stage(scene):
+    """PBF density constraints (4 iterations) on the FLIP particles at the end of every step: a dam break thrown at a
+    moving sphere (collider response after each correction, the sphere's boundary density), and the wave tank with
+    whitewater, the air field and a 3-cell narrow band (refilled particles join the constraint): 20 steps bit for bit."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    from splashtank_b200.scene import SceneRunner, sphere_sdf
+    if scene == "dam":
+        sc = scenes.dam_break(32)
+        sc["vel"] = np.tile(np.array([[1.5, 0.0, 0.0]], np.float32), (len(sc["pos"]), 1))
+        g, o = make_pair(sc)
+        sdf = sphere_sdf(0.12, 1 / 64, sid=3)
+        opts = dict(sc["opts"], pbf=4)
+        runs, t = [SceneRunner(s) for s in (g, o)], 0.0
+        for _ in range(20):
+            t += sc["dt"]
+            st = [dict(id=1, sdf=sdf, x=0.1 - 0.5 * t, y=0.15, z=0.0)]
+            for r in runs:
+                r.step(sc["dt"], st, opts)
+        assert_same_state(g, o)
+    else:
+        w, g, o = _tank_pair(32, 3.0)
+        w.opts = dict(w.opts, pbf=dict(iters=4))
+        _run_tank(w, (g, o), 20)
+        assert_same_state(g, o, spray=True)
+
+
 def test_dam_break_64_as_benchmarked():
     """The plain dam break exactly as its configuration states it: 64^3 MAC grid (dx 1/64) in 8^3 blocks, solid walls,
     fluid where x < 0.4 and y < 0.6, 8 particles per cell with seeded jitter (505,856 particles), FLIP 0.97, gravity
