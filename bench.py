@@ -2,7 +2,7 @@
 """Benchmark of the B200 FLIP step: particle-steps/s on the full-feature 256^3 wave tank (one JSON line).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload wave_tank_256|dam_break_64|pressure_512|batch_64|diff_128]
+                [--workload wave_tank_256|wave_tank_256_band3|dam_break_64|pressure_512|batch_64|diff_128|pbf_dam]
 
 One process per GPU (torchrun for N > 1, NCCL only for the barrier and the max/sum of the numbers). The FLIP step of
 one tank does not shard, so N GPUs run N independent replica tanks (weak scaling) and value is the total over them.
@@ -60,6 +60,8 @@ def parse():
         a.steps = 100
     if a.workload.startswith("diff_") and "--steps" not in sys.argv:
         a.steps, a.warmup = 3, 1
+    if a.workload.startswith("pbf_") and "--steps" not in sys.argv:
+        a.steps, a.warmup = 30, 3
     return a
 
 
@@ -101,7 +103,7 @@ def config_of(name, w, n_live):
                    narrow_band="full depth (band 1e4)" if w.band >= 1e4 else "%g cells" % w.band,
                    colliders="piston box 0.5 Hz amp 0.05 + sphere r 0.1 on a linear path over %d steps" % w.steps,
                    whitewater_cap=w.spray_cap,
-                   pbf="not in this step")
+                   pbf="not in this step (the 4-iteration PBF density stage is timed in the pbf4 sub-object)")
     return cfg
 
 
@@ -520,6 +522,164 @@ def band_summary(local, name="wave_tank_256_band3", warm=8, steps=20):
             "steps": steps, "warmup": warm, "narrow_band": "3 cells (deep calm particles trimmed, thin band cells refilled)"}
 
 
+def pbf4_summary(local, name="wave_tank_256", iters=4, warm=3, steps=8):
+    """The headline tank with the PBF density stage of 4 iterations at the end of every step (st_step_opts.pbf_iters):
+    the configuration's "PBF density constraints with 4 iterations", device-timed like the headline run."""
+    import torch
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    w = workload(name)
+    w.opts = dict(w.opts, pbf=iters)
+    sim = w.make(FlipSim, device=local)
+    run = SceneRunner(sim)
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    t = 0.0
+    sim.set_timing(True)
+    for _ in range(warm):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    torch.cuda.synchronize()
+    sim.read_timing()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        t += w.dt
+        run.step(w.dt, w.states(t), w.opts)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    stages, nrec = sim.read_timing()
+    st = sim.readStats()
+    sim.destroy()
+    return {"workload": name, "pbf": "%d iterations (GpuSim's density constraint, kernel radius 2.2 d)" % iters,
+            "value": st["live"] * steps / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms / steps,
+            "pbf_stage_ms": stages["pbf"] / max(nrec, 1), "flip_stages_ms": (stages["total"] - stages["pbf"]) / max(nrec, 1),
+            "particles": st["live"], "steps": steps, "warmup": warm}
+
+
+# ---------------------------------------------------------------- the PBF engine (GpuSim)
+def pbf_scene(name):
+    """pbf_dam: GpuSim's dam break in the app's default box (3 x 2.6 x 3): water where x < 0 and y < 1.3 on FluidSim's
+    lattice at spacing d = 0.0125 with its jitter (seeded): 2,995,200 particles; a sphere collider of radius 0.3 as a
+    distance grid; gravity 9.81, XSPH viscosity 0.02, 4 solver iterations, dt 1/120."""
+    from splashtank_b200.scene import sphere_sdf
+    d = 0.0125
+    rng = np.random.default_rng(9)
+    j = 0.01 * d / 0.12
+    ys, xs, zs = np.arange(d / 2, 1.3, d), np.arange(-1.5 + d / 2, 0.0, d), np.arange(-1.5 + d / 2, 1.5, d)
+    Y, X, Z = np.meshgrid(ys, xs, zs, indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    pos = (pos + (rng.random(pos.shape) - 0.5) * j).astype(np.float32)
+    sph = sphere_sdf(0.3, 0.02, sid=1)
+    opts = dict(g=9.81, iters=4, visc=0.02, cols=[dict(sdf=sph, x=0.6, y=0.3, z=0.0)])
+    return dict(d=d, pos=pos, opts=opts, dt=1.0 / 120.0)
+
+
+def pbf_bytes(n, iters):
+    """Algorithmic HBM bytes of one PBF step by the per-unit model (8 + 2 iters) x 32 B per particle: the particle state
+    read and written by predict, finalize and viscosity, and twice per iteration the sorted positions and multipliers;
+    neighbour reads are served from the caches and not counted."""
+    return (8 + 2 * iters) * 32 * n
+
+
+def run_pbf(a):
+    """particle-steps/s of the PBF engine (st_pbf_step, GpuSim's semantics) on pbf_dam; the GpuSim restatement (the
+    oracle, all host threads) on a bounded sample of steps of the same scene beside it."""
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    from splashtank_b200.pbf import PbfSim
+    sc = pbf_scene(a.workload)
+    n = len(sc["pos"])
+    s = PbfSim(sc["d"], n, device=local)
+    s.add_many(sc["pos"])
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    for _ in range(a.warmup):
+        s.step(sc["dt"], sc["opts"])
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        s.step(sc["dt"], sc["opts"])
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    # end to end: parameters and collider records up, every particle (position and velocity) back each step
+    pin = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True).numpy()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, a.steps // 2)
+    import ctypes as C
+    from splashtank_b200 import abi
+    pp = pin[:n * 16].view(np.float32)
+    vv = pin[n * 16:].view(np.float32)
+    got = C.c_uint32()
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        s.step(sc["dt"], sc["opts"])
+        s.f["pbf_read"](s._h, pp.ctypes.data_as(abi.f32p), vv.ctypes.data_as(abi.f32p), n, C.byref(got))
+    f1.record(stream)
+    f1.synchronize()
+    ems = f0.elapsed_time(f1)
+    s.destroy()
+    if rank == 0:
+        peak, src = measured_peak()
+        per = ms / a.steps
+        b = pbf_bytes(n, sc["opts"]["iters"])
+        line = {"metric": "particle-steps/s", "value": n * a.steps / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": 1, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": per, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded lattice jitter)",
+                "config": {"workload": a.workload, "particles": n, "d": sc["d"], "iters": sc["opts"]["iters"], "visc": sc["opts"]["visc"],
+                           "dt": sc["dt"], "colliders": "sphere r 0.3 (distance grid)", "box": [3.0, 2.6, 3.0],
+                           "l2": "working set larger than L2: no flush", "parallelism": "replicas"},
+                "gpu_launches": int(a.steps * (6 + 2 * sc["opts"]["iters"] + 2)), "clocks": clk,
+                "roofline": {"kernel": "whole PBF step", "bound": "hbm", "achieved": round(b / (per * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(b / (per * 1e-3) / 1e9 / peak, 4), "peak_source": src, "traffic": None,
+                             "algorithmic_bytes_per_launch": int(b), "launch_ms": round(per, 4),
+                             "limiter": "the 27-cell neighbour loops (about 290 candidates per particle per pass): issue and L1 latency"},
+                "e2e": {"value": n * e2e_steps / (ems * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": 64 + 128,
+                        "d2h_bytes_per_step": n * 32, "steps": e2e_steps, "readback": "every particle's position and velocity each step"}}
+        if not a.no_cpu_baseline:
+            line["cpu_baseline"] = pbf_cpu(sc)
+        print(json.dumps(line), flush=True)
+
+
+def pbf_cpu(sc, budget_s=20.0, steps=None):
+    """The GpuSim restatement (all host threads) on the same scene: steps until budget_s has passed (at least one)."""
+    from oracle.oracle import OraclePbfSim
+    th = os.cpu_count() or 1
+    n = len(sc["pos"])
+    o = OraclePbfSim(sc["d"], n, threads=th)
+    o.add_many(sc["pos"])
+    o.step(sc["dt"], sc["opts"])
+    k, t0 = 0, time.perf_counter()
+    while True:
+        o.step(sc["dt"], sc["opts"])
+        k += 1
+        el = time.perf_counter() - t0
+        if (steps and k >= steps) or (not steps and el > budget_s):
+            break
+    o.destroy()
+    return {"value": n * k / el, "unit": "particle-steps/s", "cores": th, "kind": "port",
+            "sample": "pbf_dam (%d particles): %d steps after 1 untimed, the GpuSim restatement with %d OpenMP threads (%.1f s)" % (n, k, th, el)}
+
+
+def run_pbf_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = pbf_scene(a.workload)
+    cb = pbf_cpu(sc, steps=max(1, min(a.steps, 10)))
+    line = {"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s", "impl": "reference", "n_gpus": a.gpus,
+            "steps": max(1, min(a.steps, 10)), "warmup": 1, "ms_per_step": len(sc["pos"]) / cb["value"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice jitter)",
+            "config": {"workload": a.workload, "particles": len(sc["pos"])}, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- many tanks per step
 def batch_bytes(stats, iters):
     """Algorithmic HBM bytes of one step of every tank (the stage_bytes figures of the main stages, summed)."""
@@ -767,6 +927,8 @@ def main():
         return run_pressure_reference(a) if a.impl == "reference" else run_pressure(a)
     if a.workload.startswith("batch_"):
         return run_batch_reference(a) if a.impl == "reference" else run_batch(a)
+    if a.workload.startswith("pbf_"):
+        return run_pbf_reference(a) if a.impl == "reference" else run_pbf(a)
     if a.workload.startswith("diff_"):
         if a.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no differentiable rollout"}), flush=True)
@@ -911,6 +1073,7 @@ def main():
                 # the metric's pressure half and the reference's narrow band of 3 cells, after the timed regions
                 line["pressure"] = pressure_summary(local)
                 line["band3"] = band_summary(local, a.workload + "_band3")
+                line["pbf4"] = pbf4_summary(local, a.workload)
             if not a.no_cpu_baseline:
                 cb, _ = cpu_sample(a.workload, w)
                 line["cpu_baseline"] = cb
