@@ -709,7 +709,7 @@ def run_batch(a):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
     from splashtank_b200 import scenes
-    from splashtank_b200.batch import TankBatch, autotune, lpt_partition
+    from splashtank_b200.batch import TankBatch, autotune, lpt_partition, tune_schedule
     from splashtank_b200.flip import FlipSim
     from splashtank_b200.scene import SceneRunner
     count = int(a.workload.rsplit("_", 1)[1])
@@ -758,6 +758,9 @@ def run_batch(a):
     third = max(1, len(order) // 3)
     classes = [order[:third], order[third:2 * third], order[2 * third:]]
     choice, trials = autotune(batch, sims, classes, step, timer) if not a.no_autotune else ([(8, 4, 8)] * 3, {})
+    # the pressure-sweep schedule: per-tank chains in graph branches, the shared pool swept by one launch per colour, or
+    # one persistent cooperative launch
+    sched, sched_ms = tune_schedule(batch, step, timer) if not a.no_autotune else (("graph", 8), {})
     for _ in range(a.warmup):
         step()
     barrier()
@@ -779,7 +782,13 @@ def run_batch(a):
         step()
     barrier()
     ms_seq = max_over_ranks(timer(lambda: [step() for _ in range(a.steps)]))
+    # every tank's step graph as a parallel branch of one launch (the per-tank sweep chains), for comparison
     batch.set_mode("graph")
+    for _ in range(2):
+        step()
+    barrier()
+    ms_branch = max_over_ranks(timer(lambda: [step() for _ in range(a.steps)]))
+    batch.set_mode(sched[0])
     # end to end: every step the options and collider records go up and every tank's counters come back
     barrier()
     e_steps = max(1, a.e2e_steps // 4)
@@ -797,12 +806,20 @@ def run_batch(a):
                 "config": {"workload": a.workload, "tanks": count, "tanks_rank0": ntanks, "particles": int(live_all),
                            "edges": "uniform from %s per axis, cell 1/64" % (scenes.TANK_EDGES,), "fill": "20-60%",
                            "collider": "one static SDF sphere per tank", "sor_iters": iters, "dt": spec.dt,
-                           "mode": "one graph launch per step (tank step graphs as parallel branches)",
+                           "mode": {"graph": "one graph launch per step (tank step graphs as parallel branches)",
+                                    "pooled": "one graph per step: tank branches, then every tank's fluid tiles in one shared pool swept by "
+                                              "one launch per colour, then tank branches",
+                                    "persistent": "tank branches, one persistent cooperative launch for all sweeps of all tanks (bounded "
+                                                  "grid-barrier waits), tank branches"}[sched[0]],
+                           "sweep_schedule": {"mode": sched[0], "ctas_per_sm": sched[1]},
                            "launch_shape_per_class": choice, "parallelism": "tanks split over ranks (LPT)",
                            "l2": "working set larger than L2: no flush"},
                 "gpu_launches": int(launches),
                 "sequential": {"ms_per_step": ms_seq / a.steps, "value": live_all * a.steps / (ms_seq * 1e-3),
                                "mode": "the same step graphs launched one after another on one stream"},
+                "graph_branches": {"ms_per_step": ms_branch / a.steps, "value": live_all * a.steps / (ms_branch * 1e-3),
+                                   "mode": "every tank's step graph as a parallel branch of one launch"},
+                "schedule_ms": {"%s:%d" % k: round(v, 3) for k, v in sched_ms.items()},
                 "autotune_ms": {"%d:%s" % (k, "x".join(map(str, c))): round(v, 3) for (k, c), v in trials.items()},
                 "clocks": clk,
                 "roofline": {"kernel": "whole batch step (all kernels of all tanks)", "bound": "hbm", "achieved": round(achieved, 1),

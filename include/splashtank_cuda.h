@@ -445,11 +445,19 @@ st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light
 
 /* ---- many independent tanks stepped together (no reference counterpart; the reference steps one tank) ----
  * The tanks are st_flip handles on one device, created and owned by the caller. st_batch_step does each tank's
- * st_flip_step (same options, same result) and runs all their step graphs either as parallel branches of one CUDA
- * graph launch (ST_BATCH_GRAPH) or one after another on the batch stream (ST_BATCH_SEQUENTIAL). The batch's work is
- * ordered after each tank's earlier work and before its later work. */
+ * st_flip_step (same options, same result, bit for bit) in one of four ways:
+ *  ST_BATCH_GRAPH       every tank's step graph as a parallel branch of one CUDA graph launch;
+ *  ST_BATCH_SEQUENTIAL  the step graphs one after another on the batch stream;
+ *  ST_BATCH_POOLED      one graph: parallel tank branches up to the pressure sweeps, then every tank's fluid tiles
+ *                       in one shared pool (tank order, tiles ascending; the reference's slot pool,
+ *                       src/flip/wgsl-blocks.js:16-35, shared by all tanks) swept by one launch per colour for all
+ *                       tanks, then parallel tank branches to the end of the step;
+ *  ST_BATCH_PERSISTENT  as POOLED, with all sweeps of the step in one persistent cooperative launch whose grid-barrier
+ *                       waits are bounded: a wait that runs out makes the next st_batch_step return ST_TIMEOUT.
+ * The pooled modes need the same SOR iteration count on every tank; a step where a tank restarts its narrow band
+ * runs as ST_BATCH_GRAPH. The batch's work is ordered after each tank's earlier work and before its later work. */
 typedef struct st_batch st_batch;
-enum { ST_BATCH_GRAPH = 0, ST_BATCH_SEQUENTIAL = 1 };
+enum { ST_BATCH_GRAPH = 0, ST_BATCH_SEQUENTIAL = 1, ST_BATCH_POOLED = 2, ST_BATCH_PERSISTENT = 3 };
 typedef struct st_batch_desc {
   uint32_t size;   /* sizeof(st_batch_desc) */
   int32_t mode;    /* ST_BATCH_* */
@@ -462,6 +470,12 @@ st_status st_batch_set_mode(st_batch* b, int32_t mode);
 void* st_batch_stream(st_batch* b);
 /* kernels launched by batch steps so far */
 uint64_t st_batch_launches(st_batch* b);
+/* the pooled modes' sweeps: CTAs per SM (capped by residency in ST_BATCH_PERSISTENT) and the limit of each grid-barrier
+ * wait in microseconds (default 1,000,000) */
+st_status st_batch_set_sweeps(st_batch* b, int32_t ctas_per_sm, uint32_t wait_limit_us);
+/* The persistent sweep's bounded grid barrier on its own, expecting `missing` more CTAs than it launches, so every wait
+ * runs out after about limit_us: *timed_out = 1 when the kernel reported it and returned (the check of the bound). */
+st_status st_batch_barrier_test(int32_t device, uint32_t missing, uint32_t limit_us, uint32_t* timed_out);
 
 /* ---- differentiable rollout and its adjoint (no reference counterpart: the reference has no gradients) ----
  * A FLIP rollout on a dense n^3 MAC grid over the unit box (P2G, gravity, collider and wall face velocities, pressure
@@ -486,6 +500,11 @@ typedef struct st_diff_desc {
   float box_half[3];      /* collider half extents */
   uint32_t cg_maxit;
   float cg_tol;           /* relative residual of the pressure solves */
+  /* 1: the collider is the box's signed distance grid (nodes grid_cell apart, 3 cells of margin) sampled as sdfEval
+   * does (src/gpu.js:6-33: trilinear distance, the normalised trilinear gradient as the normal), and the adjoint
+   * differentiates that response (the trilinear gradient and Hessian); 0: the analytic box */
+  int32_t collider_grid;
+  float grid_cell;
 } st_diff_desc;
 /* pos3: initial particle positions; target: n^3 densities, x fastest */
 st_status st_diff_create(const st_diff_desc* d, const float* pos3, uint32_t np, const float* target, st_diff** out);
@@ -493,6 +512,8 @@ void st_diff_destroy(st_diff* s);
 st_status st_diff_forward(st_diff* s, const double* params, int32_t record, double* loss);
 /* gradient of the loss at the parameters of the last recording forward pass */
 st_status st_diff_backward(st_diff* s, double* grad);
+/* the particles after the last forward pass (positions, then velocities when vel3 is not NULL), np x 3 floats each */
+st_status st_diff_read_state(st_diff* s, float* pos3, float* vel3);
 /* device bytes held; conjugate-gradient iterations of the last forward or backward call */
 st_status st_diff_stats(st_diff* s, uint64_t* device_bytes, int32_t* cg_iters);
 void* st_diff_stream(st_diff* s);

@@ -184,7 +184,7 @@ class BatchDesc(C.Structure):
     _fields_ = [("size", C.c_uint32), ("mode", C.c_int32)]
 
 
-ST_BATCH_GRAPH, ST_BATCH_SEQUENTIAL = 0, 1
+ST_BATCH_GRAPH, ST_BATCH_SEQUENTIAL, ST_BATCH_POOLED, ST_BATCH_PERSISTENT = 0, 1, 2, 3
 BATCH_FUNCS = [
     ("batch_create", C.c_int, [C.POINTER(BatchDesc), C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]),
     ("batch_destroy", None, [C.c_void_p]),
@@ -192,11 +192,14 @@ BATCH_FUNCS = [
     ("batch_set_mode", C.c_int, [C.c_void_p, C.c_int32]),
     ("batch_stream", C.c_void_p, [C.c_void_p]),
     ("batch_launches", C.c_uint64, [C.c_void_p]),
+    ("batch_set_sweeps", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32]),
+    ("batch_barrier_test", C.c_int, [C.c_int32, C.c_uint32, C.c_uint32, u32p]),
 ]
 class DiffDesc(C.Structure):
     _fields_ = [("size", C.c_uint32), ("n", C.c_uint32), ("steps", C.c_uint32), ("ckpt_every", C.c_uint32), ("fp64", C.c_int32),
                 ("device", C.c_int32), ("dt", C.c_float), ("flip", C.c_float), ("g", C.c_float), ("q0", C.c_float), ("margin", C.c_float),
-                ("box_half", C.c_float * 3), ("cg_maxit", C.c_uint32), ("cg_tol", C.c_float)]
+                ("box_half", C.c_float * 3), ("cg_maxit", C.c_uint32), ("cg_tol", C.c_float), ("collider_grid", C.c_int32),
+                ("grid_cell", C.c_float)]
 
 
 DIFF_FUNCS = [
@@ -205,6 +208,7 @@ DIFF_FUNCS = [
     ("diff_forward", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double)]),
     ("diff_backward", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("diff_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
+    ("diff_read_state", C.c_int, [C.c_void_p, f32p, f32p]),
     ("diff_stream", C.c_void_p, [C.c_void_p]),
 ]
 NOALLOC_FUNCS = [

@@ -1,8 +1,10 @@
 """Many independent tanks stepped together (st_batch_*), the split of tanks over GPUs, and the launch-shape autotuner.
 
 A batch step does every tank's FlipSim.step (src/flip/sim.js:179-241) with that tank's own options; the tanks' captured
-step graphs run as parallel branches of one CUDA graph launch ("graph") or one after another ("sequential"). Each tank
-gets exactly the result of stepping it alone. Compute runs in libsplashtank_cuda.so.
+step graphs run as parallel branches of one CUDA graph launch ("graph") or one after another ("sequential"), or the tanks
+share one pool of fluid tiles for the pressure sweeps, swept for all tanks by one launch per colour ("pooled") or by one
+persistent cooperative launch with bounded grid-barrier waits ("persistent"). Each tank gets exactly the result of
+stepping it alone. Compute runs in libsplashtank_cuda.so.
 """
 import ctypes as C
 import time
@@ -20,7 +22,8 @@ def funcs():
     return _B
 
 
-MODES = {"graph": abi.ST_BATCH_GRAPH, "sequential": abi.ST_BATCH_SEQUENTIAL}
+MODES = {"graph": abi.ST_BATCH_GRAPH, "sequential": abi.ST_BATCH_SEQUENTIAL, "pooled": abi.ST_BATCH_POOLED,
+         "persistent": abi.ST_BATCH_PERSISTENT}
 
 
 class TankBatch:
@@ -56,6 +59,12 @@ class TankBatch:
         if st != abi.ST_OK:
             raise status_error("batch step", st)
         del packs
+
+    def set_sweeps(self, ctas_per_sm=8, wait_limit_us=1_000_000):
+        """CTAs per SM of the pooled modes' sweeps, and the limit of each grid-barrier wait of the persistent one."""
+        st = self.f["batch_set_sweeps"](self._h, int(ctas_per_sm), int(wait_limit_us))
+        if st != abi.ST_OK:
+            raise status_error("batch set_sweeps", st)
 
     def stream(self):
         return self.f["batch_stream"](self._h)
@@ -120,6 +129,36 @@ def autotune(batch, sims, classes, run_step, timer, candidates=CANDIDATES, steps
         choice[k] = best[1]
     apply()
     return choice, trials
+
+
+SCHEDULES = [("graph", 8), ("pooled", 8), ("pooled", 4), ("pooled", 16), ("persistent", 4), ("persistent", 2)]
+
+
+def tune_schedule(batch, run_step, timer, schedules=SCHEDULES, steps=3):
+    """The pressure-sweep schedule of a batch: each tank's own chained sweeps in its graph branch ("graph"), one pooled
+    sweep launch per colour for all tanks ("pooled") or one persistent launch ("persistent"), at a number of CTAs per
+    SM. Each is timed over `steps` batch steps after one that captures its graphs; the fastest is kept. Results do not
+    depend on it. Returns (best (mode, ctas), {(mode, ctas): ms})."""
+    trials = {}
+    for mode, ctas in schedules:
+        batch.set_mode(mode)
+        batch.set_sweeps(ctas)
+        run_step()
+        trials[(mode, ctas)] = timer(lambda: [run_step() for _ in range(steps)]) / steps
+    best = min(trials, key=lambda k: trials[k])
+    batch.set_mode(best[0])
+    batch.set_sweeps(best[1])
+    return best, trials
+
+
+def barrier_test(device=0, missing=1, limit_us=200_000):
+    """The persistent sweep's bounded grid barrier with `missing` CTAs that never arrive: True when every wait ran out
+    and the kernel returned with its error flag set (st_batch_barrier_test)."""
+    out = C.c_uint32()
+    st = funcs()["batch_barrier_test"](int(device), int(missing), int(limit_us), C.byref(out))
+    if st != abi.ST_OK:
+        raise status_error("batch barrier_test", st)
+    return bool(out.value)
 
 
 def wall_ms(fn, sync):

@@ -101,6 +101,8 @@ struct st_flip {
   float *cp = nullptr, *crhs = nullptr;
   uint16_t* cinfo = nullptr;
   uint32_t *nbs = nullptr, *slotOf = nullptr;
+  uint32_t* poolZero = nullptr;   // offset 0 of a tank alone in its own compact copy
+  float* pomega = nullptr;        // SOR factor of each copied tile
   uint8_t* frame = nullptr;   // packed frame (allocated by the first st_flip_read_frame)
   // an asynchronous frame (st_flip_read_frame_async): copied to the host on its own stream while later steps run
   cudaStream_t copyStream = nullptr;
@@ -170,7 +172,7 @@ struct st_flip {
     B.need = need; B.on = on; B.tstate = tstate; B.blkTiles = blkTiles; B.active = active; B.prevActive = nullptr;
     B.tileSlot = tileSlot; B.dropped = dropped; B.fluidTiles = fluidTiles; B.wet = wet; B.tileCnt = tileCnt; B.tileAux = tileAux; B.tileAux2 = tileAux2; B.tileEmit = tileEmit; B.tileDead = tileDead; B.deadF = deadF;
     B.cnt = cnt[parity]; B.cntOther = cnt[parity ^ 1]; B.cellOff = cellOff; B.ctype = ctype; B.pres = pres; B.rhs = rhs;
-    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
+    B.acc = acc; B.vn = vn; B.vo = vo; B.velG = velG; B.sorInfo = sorInfo; B.cp = cp; B.crhs = crhs; B.cinfo = cinfo; B.nbs = nbs; B.slotOf = slotOf; B.poolOff = poolZero; B.pomega = pomega; B.cols = reinterpret_cast<const float4*>(dUp->cols); B.sdf = sdf;
     B.waves = reinterpret_cast<const float4*>(dUp->waves);
     B.sPos = sPos; B.sVel = sVel; B.air = air; B.air2 = air2; B.airAcc = airAcc; B.drip = drip; B.dripTmp = drip ? drip + 2 * (size_t)dripCap : nullptr;
     B.dripCnt = drip ? reinterpret_cast<uint32_t*>(drip + 4 * (size_t)dripCap) : nullptr; B.emitK = emitK; B.blkEmit = blkEmit; B.deadList = deadList;
@@ -208,7 +210,7 @@ void st_flip_destroy(st_flip* s) {
   void* ptrs[] = {s->dCtl, s->part[0], s->part[1], s->ids[0], s->ids[1], s->key, s->rank, s->srcIdx, s->spid, s->blkDead,
                   s->need, s->blkTiles, s->active, s->tileSlot, s->dropped, s->fluidTiles, s->wet, s->tileCnt, s->tileAux, s->tileAux2, s->tileEmit, s->tileDead, s->deadF, s->on, s->tstate,
                   s->cnt[0], s->cnt[1], s->cellOff, s->ctype, s->pres, s->rhs, s->vn, s->vo, s->velG, s->acc, s->sorInfo,
-                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->drip, s->deepBuf, s->viewScratch, s->liveOut, s->framePart, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag};
+                  s->sdf, s->sPos, s->sVel, s->air, s->air2, s->airAcc, s->drip, s->deepBuf, s->viewScratch, s->liveOut, s->framePart, s->emitK, s->blkEmit, s->deadList, s->cp, s->crhs, s->cinfo, s->nbs, s->slotOf, s->frame, s->diag, s->poolZero, s->pomega};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (s->hCtl) cudaFreeHost(s->hCtl);
   if (s->ring_h) cudaFreeHost(s->ring_h);
@@ -281,7 +283,8 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(dalloc(&s->acc, 6 * C), "acc"); A(dalloc(&s->vn, 3 * C), "vn"); A(dalloc(&s->vo, 3 * C), "vo"); A(dalloc(&s->velG, 3 * C), "velG");
   A(dalloc(&s->sorInfo, C), "sorInfo");
   A(dalloc(&s->cp, C), "sweep p"); A(dalloc(&s->crhs, C), "sweep rhs"); A(dalloc(&s->cinfo, C), "sweep info");
-  A(dalloc(&s->nbs, 6 * T), "sweep neighbours"); A(dalloc(&s->slotOf, T), "sweep slots"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
+  A(dalloc(&s->nbs, 6 * T), "sweep neighbours"); A(dalloc(&s->slotOf, T), "sweep slots");
+  A(dalloc(&s->poolZero, 1), "pool offset"); A(dalloc(&s->pomega, T), "sweep omega"); A(dalloc(&s->sdf, 16), "sdf"); s->sdfCap = 16;
   A(dalloc(&s->sPos, std::max<size_t>(s->sprayCap, 1)), "sPos"); A(dalloc(&s->sVel, std::max<size_t>(s->sprayCap, 1)), "sVel");
   if (s->sprayCap) {   // the air field exists only with whitewater: it is stepped in the whitewater stage
     const double cells = (double)s->nx * (double)s->ny * (double)s->nz;
@@ -307,6 +310,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   A(cudaMemsetAsync(s->vo, 0, 3 * C * 4, q), "memset"); A(cudaMemsetAsync(s->velG, 0, 3 * C * 4, q), "memset");
   A(cudaMemsetAsync(s->sorInfo, 0, C * 2, q), "memset");
   A(cudaMemsetAsync(s->slotOf, 0xff, T * 4, q), "memset");
+  A(cudaMemsetAsync(s->poolZero, 0, 4, q), "memset");
   A(cudaMemsetAsync(s->wet, 0, C * 4, q), "memset");
   A(cudaMemsetAsync(s->sPos, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
   A(cudaMemsetAsync(s->sVel, 0, std::max<size_t>(s->sprayCap, 1) * 16, q), "memset");
@@ -530,9 +534,10 @@ static void stage_fill(st_stage_times* t, const float* ms, float total) {
 
 // The device work of one step after the uploads: counters reset, then the stages in the reference's order
 // (src/flip/sim.js:253-309), then the PBF density stage when pbfIters > 0. mark(k) is called at the 12 stage
-// boundaries. Returns the kernels launched.
+// boundaries. The front half runs up to the pressure sweeps, the back half from the projection on; a pooled batch
+// runs its tanks' sweeps between the two. Each returns the kernels it launched.
 template <class Mark>
-static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, bool sprOn, int iters, int pbfIters, Mark mark) {
+static int enqueue_front(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, Mark mark) {
   cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q);        // fluid, vmaxBits, nLive (nActive is kept)
   cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q);
   cudaMemsetAsync(&s->dCtl->emitTried, 0, 2 * sizeof(uint32_t), q);     // emitTried, nFluidTiles
@@ -558,7 +563,13 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   mark(4);
   nl += launch_norm_div(B, gT4, ocean, q);
   mark(5);
-  nl += launch_sor_compact(B, s->tileGrid(s->gridSor), gT4, iters, q);
+  return nl;
+}
+template <class Mark>
+static int enqueue_back(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, bool sprOn, int pbfIters, Mark mark) {
+  const int gT = s->tileGrid(s->gridT), gT4 = s->tileGrid(s->gridT4);
+  const bool ocean = s->hp.ocean != 0;
+  int nl = 0;
   mark(6);
   nl += launch_project(B, gT4, q);
   mark(7);
@@ -573,6 +584,12 @@ static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, ui
   if (pbfIters > 0) nl += launch_flip_pbf(B, s->pbf, pbfIters, std::max(1, std::min<int>(s->sms * 8, (int)((s->N + PBF_T - 1) / PBF_T))), q);
   mark(11);
   return nl;
+}
+template <class Mark>
+static int enqueue_step(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, uint32_t init, bool sprOn, int iters, int pbfIters, Mark mark) {
+  int nl = enqueue_front(s, B, q, nbOn, init, mark);
+  nl += launch_sor_compact(B, s->tileGrid(s->gridSor), s->tileGrid(s->gridT4), iters, q);
+  return nl + enqueue_back(s, B, q, nbOn, sprOn, pbfIters, mark);
 }
 
 // A step's kernels as a CUDA graph, keyed by everything that changes what is launched: the particle buffer parity,
@@ -1602,6 +1619,21 @@ struct st_batch {
   };
   std::vector<Combined> cache;
   uint64_t launches = 0, graph_launches = 0;
+  // pooled modes: one compact copy of every tank's fluid tiles, swept by one launch per colour (ST_BATCH_POOLED) or
+  // by one persistent cooperative launch (ST_BATCH_PERSISTENT)
+  PoolBufs pool{};
+  const Ctl** dCtls = nullptr;     // device: each tank's counters
+  unsigned int* hErr = nullptr;    // pinned: the persistent sweep's error word after its launch
+  bool errPending = false;
+  int poolGrid = 8;                // CTAs per SM of the pooled sweeps
+  uint64_t limitNs = 1000000000ull;
+  struct Pooled {
+    std::vector<uint64_t> key;
+    cudaGraph_t g[2] = {nullptr, nullptr};
+    cudaGraphExec_t x[2] = {nullptr, nullptr};
+    int launches = 0;
+  };
+  std::vector<Pooled> pcache;
 };
 
 static void batch_drop(st_batch* b) {
@@ -1610,6 +1642,141 @@ static void batch_drop(st_batch* b) {
     if (c.graph) cudaGraphDestroy(c.graph);
   }
   b->cache.clear();
+  for (auto& c : b->pcache)
+    for (int k = 0; k < 2; k++) {
+      if (c.x[k]) cudaGraphExecDestroy(c.x[k]);
+      if (c.g[k]) cudaGraphDestroy(c.g[k]);
+    }
+  b->pcache.clear();
+}
+static void pool_free(st_batch* b) {
+  void* ps[] = {b->pool.cp, b->pool.crhs, b->pool.cinfo, b->pool.nbs, b->pool.pomega, b->pool.off, b->pool.total, b->pool.bar, b->pool.err,
+                (void*)b->dCtls};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  b->pool = PoolBufs{};
+  b->dCtls = nullptr;
+}
+// the pool holds every tile of every tank (an upper bound on their fluid tiles)
+static cudaError_t pool_alloc(st_batch* b) {
+  size_t T = 0;
+  for (auto* s : b->tanks) T += s->ntiles;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  A(dalloc(&b->pool.cp, T * 512)); A(dalloc(&b->pool.crhs, T * 512)); A(dalloc(&b->pool.cinfo, T * 512)); A(dalloc(&b->pool.nbs, T * 6));
+  A(dalloc(&b->pool.pomega, T)); A(dalloc(&b->pool.off, b->tanks.size())); A(dalloc(&b->pool.total, 1)); A(dalloc(&b->pool.bar, 1));
+  A(dalloc(&b->pool.err, 1)); A(dalloc(&b->dCtls, b->tanks.size()));
+  if (e == cudaSuccess) {
+    std::vector<const Ctl*> h(b->tanks.size());
+    for (size_t i = 0; i < h.size(); i++) h[i] = b->tanks[i]->dCtl;
+    e = cudaMemcpy((void*)b->dCtls, h.data(), h.size() * sizeof(Ctl*), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMemset(b->pool.err, 0, 4);
+  return e;
+}
+// a tank's buffers with its compact copy in the pool, at the offset the plan kernel writes
+static Bufs pooled_bufs(const st_batch* b, size_t i) {
+  Bufs B = b->tanks[i]->bufs();
+  B.cp = b->pool.cp; B.crhs = b->pool.crhs; B.cinfo = b->pool.cinfo; B.nbs = b->pool.nbs; B.pomega = b->pool.pomega;
+  B.poolOff = b->pool.off + i;
+  return B;
+}
+
+// One pooled batch step after every tank's host half: a graph of parallel per-tank branches up to the pressure
+// sweeps, the plan of pool offsets, every tank's copy into the pool (parallel), then the sweeps over the whole pool, then
+// parallel per-tank branches unpacking and finishing the step. ST_BATCH_POOLED captures the sweeps into the graph as
+// chained launches; ST_BATCH_PERSISTENT runs them as one cooperative launch between two graphs (its grid barrier waits
+// are bounded; a wait that ran out is reported as ST_TIMEOUT by the next batch call).
+static st_status batch_pooled(st_batch* b, const std::vector<StepPrep>& prs) {
+  const size_t n = b->tanks.size();
+  cudaStream_t q = b->stream;
+  const bool persist = b->mode == ST_BATCH_PERSISTENT;
+  int sms = b->tanks[0]->sms;
+  const int iters = prs[0].iters;
+  int grid = sms * b->poolGrid;
+  if (persist) grid = sms * std::max(1, std::min(b->poolGrid, persistent_ctas_per_sm()));
+  std::vector<uint64_t> key;
+  for (size_t i = 0; i < n; i++) {
+    st_flip* s = b->tanks[i];
+    key.push_back(graph_key(s, prs[i].nbOn, prs[i].sprOn, prs[i].iters, prs[i].pbfIters, false));
+    key.push_back(s->gen);
+  }
+  key.push_back((uint64_t)b->mode | ((uint64_t)grid << 8));
+  st_batch::Pooled* c = nullptr;
+  for (auto& x : b->pcache) if (x.key == key) c = &x;
+  if (!c) {
+    if (b->pcache.size() >= 4) {
+      auto& f = b->pcache.front();
+      for (int k = 0; k < 2; k++) { if (f.x[k]) cudaGraphExecDestroy(f.x[k]); if (f.g[k]) cudaGraphDestroy(f.g[k]); }
+      b->pcache.erase(b->pcache.begin());
+    }
+    st_batch::Pooled nc;
+    nc.key = key;
+    int nl = 0;
+    auto fork = [&](auto&& body) -> cudaError_t {   // body(i, stream) on every tank's stream, joined back into q
+      cudaError_t e = cudaEventRecord(b->evOut, q);
+      for (size_t i = 0; i < n && e == cudaSuccess; i++) {
+        st_flip* s = b->tanks[i];
+        e = cudaStreamWaitEvent(s->stream, b->evOut, 0);
+        if (e == cudaSuccess) nl += body(i, s->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->tankEv[i], s->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(q, b->tankEv[i], 0);
+      }
+      return e;
+    };
+    auto sweeps = [&]() { nl += launch_pool_sweeps(b->pool, grid, iters, q); };
+    for (int part = 0; part < (persist ? 2 : 1); part++) {
+      cudaError_t e = cudaStreamBeginCapture(q, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess && part == 0) {
+        e = fork([&](size_t i, cudaStream_t sq) {
+          st_flip* s = b->tanks[i];
+          return enqueue_front(s, pooled_bufs(b, i), sq, prs[i].nbOn, 0u, [](int) {});
+        });
+        if (e == cudaSuccess) nl += launch_pool_plan(b->pool, b->dCtls, (uint32_t)n, q);
+        if (e == cudaSuccess)
+          e = fork([&](size_t i, cudaStream_t sq) { return launch_sor_pack(pooled_bufs(b, i), b->tanks[i]->tileGrid(b->tanks[i]->gridT4), sq); });
+        if (e == cudaSuccess && !persist) sweeps();
+      }
+      if (e == cudaSuccess && (part == 1 || !persist)) {
+        e = fork([&](size_t i, cudaStream_t sq) {
+          st_flip* s = b->tanks[i];
+          const Bufs B = pooled_bufs(b, i);
+          return launch_sor_unpack(B, s->tileGrid(s->gridT4), sq) + enqueue_back(s, B, sq, prs[i].nbOn, prs[i].sprOn, prs[i].pbfIters, [](int) {});
+        });
+      }
+      cudaGraph_t g = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(q, &g);
+      if (e == cudaSuccess) e = e2;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&nc.x[part], g, 0);
+      nc.g[part] = g;
+      if (e != cudaSuccess) {
+        set_err("pooled batch graph", e);
+        for (int k = 0; k < 2; k++) { if (nc.x[k]) cudaGraphExecDestroy(nc.x[k]); if (nc.g[k]) cudaGraphDestroy(nc.g[k]); }
+        return ST_DEVICE_ERROR;
+      }
+    }
+    nc.launches = nl + (persist ? 1 : 0);
+    b->pcache.push_back(nc);
+    c = &b->pcache.back();
+  }
+  CK(cudaGraphLaunch(c->x[0], q));
+  b->graph_launches++;
+  if (persist) {
+    CK(launch_pool_persistent(b->pool, grid, iters, b->limitNs, q));
+    CK(cudaMemcpyAsync(b->hErr, b->pool.err, 4, cudaMemcpyDeviceToHost, q));
+    b->errPending = true;
+    CK(cudaGraphLaunch(c->x[1], q));
+    b->graph_launches++;
+  }
+  for (size_t i = 0; i < n; i++) {
+    b->tanks[i]->launches += (uint64_t)(c->launches / std::max<size_t>(n, 1));
+    b->tanks[i]->steps++;
+  }
+  b->launches += (uint64_t)c->launches;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b->evOut, q));
+  for (size_t i = 0; i < n; i++) CK(cudaStreamWaitEvent(b->tanks[i]->stream, b->evOut, 0));
+  return ST_OK;
 }
 
 extern "C" {
@@ -1619,6 +1786,8 @@ void st_batch_destroy(st_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop(b);
+  pool_free(b);
+  if (b->hErr) cudaFreeHost(b->hErr);
   for (auto e : b->tankEv) if (e) cudaEventDestroy(e);
   if (b->evOut) cudaEventDestroy(b->evOut);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -1626,7 +1795,7 @@ void st_batch_destroy(st_batch* b) {
 }
 
 st_status st_batch_create(const st_batch_desc* d, st_flip* const* tanks, uint32_t n, st_batch** out) {
-  if (!d || !out || d->size != sizeof(st_batch_desc) || !tanks || !n || (d->mode != ST_BATCH_GRAPH && d->mode != ST_BATCH_SEQUENTIAL))
+  if (!d || !out || d->size != sizeof(st_batch_desc) || !tanks || !n || d->mode < ST_BATCH_GRAPH || d->mode > ST_BATCH_PERSISTENT)
     return ST_BAD_ARG;
   *out = nullptr;
   for (uint32_t i = 0; i < n; i++)
@@ -1640,6 +1809,9 @@ st_status st_batch_create(const st_batch_desc* d, st_flip* const* tanks, uint32_
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evOut, cudaEventDisableTiming);
   for (uint32_t i = 0; i < n && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&b->tankEv[i], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = pool_alloc(b);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->hErr, 4);
+  if (e == cudaSuccess) *b->hErr = 0u;
   if (e != cudaSuccess) {
     set_err("batch create", e);
     st_batch_destroy(b);
@@ -1650,8 +1822,41 @@ st_status st_batch_create(const st_batch_desc* d, st_flip* const* tanks, uint32_
 }
 
 st_status st_batch_set_mode(st_batch* b, int32_t mode) {
-  if (!b || (mode != ST_BATCH_GRAPH && mode != ST_BATCH_SEQUENTIAL)) return ST_BAD_ARG;
+  if (!b || mode < ST_BATCH_GRAPH || mode > ST_BATCH_PERSISTENT) return ST_BAD_ARG;
   b->mode = mode;
+  return ST_OK;
+}
+
+st_status st_batch_set_sweeps(st_batch* b, int32_t ctas_per_sm, uint32_t wait_limit_us) {
+  if (!b || ctas_per_sm < 1 || ctas_per_sm > 64 || wait_limit_us == 0) return ST_BAD_ARG;
+  if (b->poolGrid != ctas_per_sm) {
+    CK(cudaSetDevice(b->device));
+    CK(cudaStreamSynchronize(b->stream));
+    batch_drop(b);
+  }
+  b->poolGrid = ctas_per_sm;
+  b->limitNs = (uint64_t)wait_limit_us * 1000ull;
+  return ST_OK;
+}
+
+// The bounded grid barrier of the persistent sweep, run on its own with more arrivals expected than the launch has
+// (missing > 0): every CTA's wait must run out within about limit_us and report it. *timed_out = 1 when it did.
+st_status st_batch_barrier_test(int32_t device, uint32_t missing, uint32_t limit_us, uint32_t* timed_out) {
+  if (!timed_out || limit_us == 0 || limit_us > 10000000u) return ST_BAD_ARG;
+  CK(cudaSetDevice(device));
+  int sms = 148;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  unsigned int* w = nullptr;
+  CK(cudaMalloc((void**)&w, 8));
+  cudaError_t e = cudaMemset(w, 0, 8);
+  const int grid = sms;   // one CTA per SM: all resident
+  if (e == cudaSuccess) e = launch_barrier_test(w, w + 1, grid, (unsigned int)grid + missing, (uint64_t)limit_us * 1000ull, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  unsigned int h[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(h, w, 8, cudaMemcpyDeviceToHost);
+  cudaFree(w);
+  CK(e);
+  *timed_out = h[1] != 0u ? 1u : 0u;
   return ST_OK;
 }
 
@@ -1671,13 +1876,38 @@ st_status st_batch_step(st_batch* b, double dt, const st_step_opts* const* opts)
     CK(cudaEventRecord(b->tankEv[i], b->tanks[i]->stream));
     CK(cudaStreamWaitEvent(q, b->tankEv[i], 0));
   }
+  if (b->errPending) {   // the last persistent sweep's error word has landed by now (this call waited above)
+    CK(cudaStreamSynchronize(q));
+    b->errPending = false;
+    if (*b->hErr) {
+      *b->hErr = 0u;
+      CK(cudaMemsetAsync(b->pool.err, 0, 4, q));
+      snprintf(g_err, sizeof(g_err), "batch: a grid barrier of the persistent pressure sweeps ran out of time");
+      return ST_TIMEOUT;
+    }
+  }
+  std::vector<StepPrep> prs(n);
+  bool pooled = b->mode == ST_BATCH_POOLED || b->mode == ST_BATCH_PERSISTENT;
+  if (pooled) {
+    // every tank's host half first; a tank that restarts this step (or cannot use graphs) sends the step down the
+    // branch path below, as do differing iteration counts
+    for (size_t i = 0; i < n; i++) {
+      st_flip* s = b->tanks[i];
+      if (s->N == 0) { pooled = false; continue; }
+      st_status st = prepare_step(s, dt, opts[i], q, &prs[i]);
+      if (st != ST_OK) return st;
+      if (prs[i].init || !s->use_graphs || prs[i].iters != prs[0].iters) pooled = false;
+    }
+    if (pooled) return batch_pooled(b, prs);
+  }
   std::vector<cudaGraph_t> kids;
   std::vector<uint64_t> key;
+  const bool prepared = b->mode == ST_BATCH_POOLED || b->mode == ST_BATCH_PERSISTENT;
   for (size_t i = 0; i < n; i++) {
     st_flip* s = b->tanks[i];
     if (s->N == 0) continue;
-    StepPrep pr;
-    st_status st = prepare_step(s, dt, opts[i], q, &pr);
+    StepPrep pr = prs[i];
+    st_status st = prepared ? ST_OK : prepare_step(s, dt, opts[i], q, &pr);
     if (st != ST_OK) return st;
     const Bufs B = s->bufs();
     int nl = 0;

@@ -111,6 +111,10 @@ struct Bufs {
   uint16_t* cinfo;
   uint32_t* nbs;
   uint32_t* slotOf;     // per tile: position in fluidTiles, or 0xffffffff
+  // where this tank's fluid tiles start in the compact copy (0 for a tank alone; a tank of a pooled batch shares one
+  // copy with the others, at the offset the batch's plan kernel writes); pomega: the SOR factor of each copied tile
+  const uint32_t* poolOff;
+  float* pomega;
   float* wet;           // per cell: how much water (wetCell, src/flip/wgsl-whitewater.js:7-12), 0 outside the domain
   // air field (src/flip/wgsl-whitewater.js:24-89): velocity at air-cell centres, its next value, fixed-point pushes
   float4* air;
@@ -138,6 +142,20 @@ struct Bufs {
 };
 
 constexpr int PBLK = 1024;     // particles per block in the order-defining passes (count, scatter, dead lists)
+
+// The compact copy shared by the tanks of a pooled batch (capi.cu's ST_BATCH_POOLED): every tank's fluid tiles one after
+// another in tank order, with their SOR factors; the offsets and total come from the plan kernel each step.
+struct PoolBufs {
+  float* cp;
+  float* crhs;
+  uint16_t* cinfo;
+  uint32_t* nbs;
+  float* pomega;
+  uint32_t* off;          // per tank
+  uint32_t* total;
+  unsigned int* bar;      // the persistent sweep's grid barrier
+  unsigned int* err;      // set when a barrier wait ran out
+};
 
 // the parameter block into a CTA's shared copy (every thread of the CTA calls it; it ends with a barrier)
 __device__ __forceinline__ void loadParams(FlipParams& s, const FlipParams* g) {

@@ -4,7 +4,8 @@
 // :107-123, relax/project :124-180, g2p/collideP :181-275) on a dense n^3 MAC grid over the unit box, with the parts that
 // have a derivative: P2G as float sums (mass-weighted face velocity), gravity, collider and wall face velocities, the
 // pressure projection (the Poisson system of the step, solved by Jacobi-preconditioned conjugate gradients), FLIP/PIC
-// G2P, advection, the push-out of an analytic box collider and the wall clamp. Its discrete decisions (cell types,
+// G2P, advection, the push-out of a box collider (analytic, or its distance grid sampled as sdfEval does) and the wall
+// clamp. Its discrete decisions (cell types,
 // which faces carry mass, which particles touch the collider or a wall, which piece of the box's distance field each
 // particle is on) are recorded by a forward pass and then held
 // fixed: the adjoint differentiates the step with those decisions as constants, and a frozen forward pass evaluates
@@ -123,6 +124,72 @@ __device__ __forceinline__ void boxSdf(const T* q, const T* hb, uint8_t* regime,
   }
 }
 
+// The collider's distance grid (collider_grid = 1): nodes `cell` apart from `origin` (relative to the collider centre),
+// dims nodes per axis, the box's exact distance at each node.
+struct DGrid {
+  int mode;            // 0 analytic box, 1 its distance grid
+  int dims[3];
+  double origin[3], cell;
+  const float* data;
+};
+// The collider at q = x - centre: distance phi, unit normal n, d phi / dq (dphi) and d n / dq (J, row major). The
+// analytic box gives dphi = n and J = its Hessian. The grid follows sdfEval (src/gpu.js:6-33): the trilinear distance at
+// the clamped grid coordinate plus the distance outside the grid, the normal the normalised trilinear gradient (in grid
+// units, raw = d phi / d f), so dphi = raw / cell and J = (I - n n^T) H_f / (|raw| cell) with H_f the trilinear Hessian
+// (zero diagonal). Outside the grid the normal points out of it and J is left 0: the grid's margin exceeds q0, so no
+// contact happens there.
+template <class T>
+__device__ __forceinline__ void colEval(const DGrid& Gd, const T* q, const T* hb, uint8_t* regime, int record, T& phi, T* n, T* dphi, T* J) {
+  if (Gd.mode == 0) {
+    boxSdf<T>(q, hb, regime, record, phi, n, J);
+    for (int k = 0; k < 3; k++) dphi[k] = n[k];
+    return;
+  }
+  if (record) *regime = 0;
+  T g[3], gc[3], f[3];
+  int fl[3];
+  T out2 = (T)0;
+  for (int d = 0; d < 3; d++) {
+    g[d] = (q[d] - (T)Gd.origin[d]) / (T)Gd.cell;
+    gc[d] = fmin(fmax(g[d], (T)0), (T)Gd.dims[d] - (T)1.0001);
+    const T fv = floor(gc[d]);
+    fl[d] = (int)fv;
+    f[d] = gc[d] - fv;
+    out2 += (g[d] - gc[d]) * (g[d] - gc[d]);
+  }
+  const int nx = Gd.dims[0], nxy = Gd.dims[0] * Gd.dims[1];
+  const size_t b0 = (size_t)fl[0] + (size_t)nx * fl[1] + (size_t)nxy * fl[2];
+  const T v000 = (T)Gd.data[b0], v100 = (T)Gd.data[b0 + 1], v010 = (T)Gd.data[b0 + nx], v110 = (T)Gd.data[b0 + nx + 1];
+  const T v001 = (T)Gd.data[b0 + nxy], v101 = (T)Gd.data[b0 + nxy + 1], v011 = (T)Gd.data[b0 + nxy + nx], v111 = (T)Gd.data[b0 + nxy + nx + 1];
+  auto mix = [](T a, T b, T t) { return a * ((T)1 - t) + b * t; };
+  const T c00 = mix(v000, v100, f[0]), c10 = mix(v010, v110, f[0]), c01 = mix(v001, v101, f[0]), c11 = mix(v011, v111, f[0]);
+  const T c0 = mix(c00, c10, f[1]), c1 = mix(c01, c11, f[1]);
+  phi = mix(c0, c1, f[2]);
+  for (int k = 0; k < 9; k++) J[k] = (T)0;
+  if (out2 > (T)0) {
+    const T l = sqrt(out2);
+    phi += l * (T)Gd.cell;
+    for (int d = 0; d < 3; d++) { n[d] = (g[d] - gc[d]) / l; dphi[d] = n[d]; }
+    return;
+  }
+  const T ax0 = v100 - v000, ax1 = v110 - v010, ax2 = v101 - v001, ax3 = v111 - v011;
+  const T raw[3] = {mix(mix(ax0, ax1, f[1]), mix(ax2, ax3, f[1]), f[2]), mix(c10 - c00, c11 - c01, f[2]), c1 - c0};
+  const T l = sqrt(raw[0] * raw[0] + raw[1] * raw[1] + raw[2] * raw[2]);
+  const T il = (T)1 / fmax(l, (T)1e-9);
+  for (int d = 0; d < 3; d++) { n[d] = raw[d] * il; dphi[d] = raw[d] / (T)Gd.cell; }
+  // trilinear Hessian in grid units (symmetric, zero diagonal)
+  const T hxy = mix(ax1 - ax0, ax3 - ax2, f[2]);
+  const T hxz = mix(ax2, ax3, f[1]) - mix(ax0, ax1, f[1]);
+  const T hyz = (c11 - c01) - (c10 - c00);
+  const T Hf[9] = {(T)0, hxy, hxz, hxy, (T)0, hyz, hxz, hyz, (T)0};
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) {
+      T acc = (T)0;
+      for (int m = 0; m < 3; m++) acc += (((r == m) ? (T)1 : (T)0) - n[r] * n[m]) * Hf[m * 3 + c];
+      J[r * 3 + c] = acc * il / (T)Gd.cell;
+    }
+}
+
 // ---- forward kernels ----
 template <class T>
 __global__ void k_d_p2g(DGeo G, size_t np, const T* __restrict__ x, const T* __restrict__ v, T* mom, T* mass, int* count) {
@@ -148,13 +215,20 @@ __global__ void k_d_p2g(DGeo G, size_t np, const T* __restrict__ x, const T* __r
 // cell types: outside the box nothing (walls are handled by the neighbour logic); collider cells solid; cells with a
 // particle fluid
 template <class T>
-__global__ void k_d_types(DGeo G, const int* __restrict__ count, const T* c, const T* hb, uint8_t* types) {
+__global__ void k_d_types(DGeo G, const int* __restrict__ count, const T* c, const T* hb, DGrid Gd, uint8_t* types) {
   const size_t nc = G.cells();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc; i += (size_t)gridDim.x * blockDim.x) {
     const int ci = (int)(i % G.n), cj = (int)((i / G.n) % G.n), ck = (int)(i / ((size_t)G.n * G.n));
     const T q[3] = {((T)ci + (T)0.5) * (T)G.h - c[0], ((T)cj + (T)0.5) * (T)G.h - c[1], ((T)ck + (T)0.5) * (T)G.h - c[2]};
     bool inside = true;
-    for (int k = 0; k < 3; k++) inside = inside && fabs(q[k]) < hb[k];
+    if (Gd.mode == 0) {
+      for (int k = 0; k < 3; k++) inside = inside && fabs(q[k]) < hb[k];
+    } else {
+      T phi, n[3], dphi[3], J[9];
+      uint8_t rg = 0;
+      colEval<T>(Gd, q, hb, &rg, 1, phi, n, dphi, J);
+      inside = phi < (T)0;
+    }
     types[i] = inside ? T_SOLID : (count[i] > 0 ? T_FLUID : T_AIR);
   }
 }
@@ -272,7 +346,7 @@ __global__ void k_d_project(DGeo G, const uint8_t* __restrict__ types, const T* 
 // collider, bit 1 its velocity pointed into it, bits 2-7 the position was clamped on (x lo, x hi, y lo, ...).
 template <class T>
 __global__ void k_d_g2p(DGeo G, size_t np, const T* __restrict__ x, const T* __restrict__ v, const T* __restrict__ u2,
-                        const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, T q0, T lo, T hi, uint8_t* flags,
+                        const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, DGrid Gd, T q0, T lo, T hi, uint8_t* flags,
                         uint8_t* regimes, int record, T* xo, T* vo) {
   const size_t nf = G.nf(0);
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < np; p += (size_t)gridDim.x * blockDim.x) {
@@ -289,9 +363,9 @@ __global__ void k_d_g2p(DGeo G, size_t np, const T* __restrict__ x, const T* __r
     T xa[3];
     for (int a = 0; a < 3; a++) xa[a] = xp[a] + vn[a] * dt;
     uint8_t fl = record ? 0 : flags[p];
-    T q[3] = {xa[0] - c[0], xa[1] - c[1], xa[2] - c[2]}, phi, n[3], H[9];
+    T q[3] = {xa[0] - c[0], xa[1] - c[1], xa[2] - c[2]}, phi, n[3], dphi[3], J[9];
     uint8_t rg = regimes[p];
-    boxSdf<T>(q, hb, &rg, record, phi, n, H);
+    colEval<T>(Gd, q, hb, &rg, record, phi, n, dphi, J);
     if (record) regimes[p] = rg;
     if (record && phi < q0) fl |= 1;
     if (fl & 1) {
@@ -359,7 +433,7 @@ __global__ void k_d_splat_b(DGeo G, size_t np, const T* __restrict__ x, const T*
 // inputs (in place), face adjoints of u2 and u0 (atomics), the collider centre's adjoint (atomics into gc[3]).
 template <class T>
 __global__ void k_d_g2p_b(DGeo G, size_t np, const T* __restrict__ x, const T* __restrict__ v, const T* __restrict__ u2,
-                          const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, T q0, const uint8_t* __restrict__ flags,
+                          const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, DGrid Gd, T q0, const uint8_t* __restrict__ flags,
                           const uint8_t* __restrict__ regimes, T* gx, T* gv, T* gu2, T* gu0, double* gc) {
   const size_t nf = G.nf(0);
   T gcx = 0, gcy = 0, gcz = 0;
@@ -377,9 +451,9 @@ __global__ void k_d_g2p_b(DGeo G, size_t np, const T* __restrict__ x, const T* _
     T xa[3];
     for (int a = 0; a < 3; a++) xa[a] = xp[a] + vn[a] * dt;
     const uint8_t fl = flags[p];
-    T q[3] = {xa[0] - c[0], xa[1] - c[1], xa[2] - c[2]}, phi, n[3], H[9];
+    T q[3] = {xa[0] - c[0], xa[1] - c[1], xa[2] - c[2]}, phi, n[3], dphi[3], J[9];
     uint8_t rg = regimes[p];
-    boxSdf<T>(q, hb, &rg, 0, phi, n, H);
+    colEval<T>(Gd, q, hb, &rg, 0, phi, n, dphi, J);
     T gxo[3] = {gx[3 * p], gx[3 * p + 1], gx[3 * p + 2]}, gvo[3] = {gv[3 * p], gv[3 * p + 1], gv[3 * p + 2]};
     // wall clamp: a clamped coordinate is constant
     for (int a = 0; a < 3; a++) if (fl & (12u << (2 * a))) gxo[a] = (T)0;
@@ -396,9 +470,9 @@ __global__ void k_d_g2p_b(DGeo G, size_t np, const T* __restrict__ x, const T* _
           gn[a] += -(ng * vn[a] + vd * gvo[a]);
         }
       }
-      // phi and n are functions of q = x_a - c: d phi = n . dq, d n = H dq
+      // phi and n are functions of q = x_a - c: d phi = dphi . dq, d n = J dq
       T gq[3];
-      for (int r = 0; r < 3; r++) gq[r] = gphi * n[r] + H[r * 3] * gn[0] + H[r * 3 + 1] * gn[1] + H[r * 3 + 2] * gn[2];
+      for (int r = 0; r < 3; r++) gq[r] = gphi * dphi[r] + J[r] * gn[0] + J[3 + r] * gn[1] + J[6 + r] * gn[2];
       for (int a = 0; a < 3; a++) gxa[a] += gq[a];
       gcx -= gq[0]; gcy -= gq[1]; gcz -= gq[2];
     }
@@ -544,6 +618,9 @@ struct st_diff {
   void *tx = nullptr, *tv = nullptr, *tu0 = nullptr, *tmass = nullptr, *tu2 = nullptr, *tp = nullptr;
   void *ckx = nullptr, *ckv = nullptr;   // checkpoints: particles at every segment start
   int cgIters = 0;
+  DGrid col{};                  // the collider's distance grid (mode 1), or mode 0
+  float* gridData = nullptr;
+  DGrid grid_() const { return col; }
 };
 
 static size_t esz(const st_diff* s) { return s->fp64 ? 8 : 4; }
@@ -665,7 +742,7 @@ static st_status step_fwd(st_diff* s, int k, bool record, const double* cs, cons
   DK(cudaMemsetAsync(s->mass, 0, 3 * nf * sizeof(T), q));
   if (record) DK(cudaMemsetAsync(s->count, 0, nc * sizeof(int), q));
   k_d_p2g<T><<<gr, 256, 0, q>>>(G, s->np, P<T>(s->x), P<T>(s->v), P<T>(s->mom), P<T>(s->mass), record ? s->count : nullptr);
-  if (record) k_d_types<T><<<gr, 256, 0, q>>>(G, s->count, cb, cb + 6, types);
+  if (record) k_d_types<T><<<gr, 256, 0, q>>>(G, s->count, cb, cb + 6, s->grid_(), types);
   T* u0 = tapeSlot >= 0 ? P<T>(s->tu0) + (size_t)tapeSlot * 3 * nf : P<T>(s->u0);
   T* u2 = tapeSlot >= 0 ? P<T>(s->tu2) + (size_t)tapeSlot * 3 * nf : P<T>(s->u2);
   T* pp = tapeSlot >= 0 ? P<T>(s->tp) + (size_t)tapeSlot * nc : P<T>(s->p);
@@ -676,7 +753,7 @@ static st_status step_fwd(st_diff* s, int k, bool record, const double* cs, cons
   if (st != ST_OK) return st;
   k_d_project<T><<<gr, 256, 0, q>>>(G, types, pp, P<T>(s->u1), (T)(s->d.dt / G.h), u2);
   const T lo = (T)s->d.margin, hi = (T)(1.0 - s->d.margin);
-  k_d_g2p<T><<<gr, 256, 0, q>>>(G, s->np, P<T>(s->x), P<T>(s->v), u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, (T)s->d.q0, lo, hi,
+  k_d_g2p<T><<<gr, 256, 0, q>>>(G, s->np, P<T>(s->x), P<T>(s->v), u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, s->grid_(), (T)s->d.q0, lo, hi,
                                 flags, regimes, record ? 1 : 0, P<T>(s->xn), P<T>(s->vn));
   std::swap(s->x, s->xn);
   std::swap(s->v, s->vn);
@@ -761,7 +838,7 @@ static st_status backward(st_diff* s, double* grad) {
       DK(cudaMemsetAsync(s->gu2, 0, 3 * nf * sizeof(T), q));
       DK(cudaMemsetAsync(s->gu0, 0, 3 * nf * sizeof(T), q));
       DK(cudaMemsetAsync(s->cred, 0, 8 * sizeof(double), q));
-      k_d_g2p_b<T><<<gr, 256, 0, q>>>(G, np, tx, tv, u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, (T)s->d.q0, flags,
+      k_d_g2p_b<T><<<gr, 256, 0, q>>>(G, np, tx, tv, u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, s->grid_(), (T)s->d.q0, flags,
                                       regimes, P<T>(s->gx), P<T>(s->gv), P<T>(s->gu2), P<T>(s->gu0), s->cred);
       k_d_project_b<T><<<gr, 256, 0, q>>>(G, types, P<T>(s->gu2), (T)(s->d.dt / G.h), P<T>(s->gp));
       st_status st = pcg<T>(s, types, P<T>(s->gp), P<T>(s->gb));   // A is symmetric: the adjoint solve uses it again
@@ -806,6 +883,7 @@ void st_diff_destroy(st_diff* s) {
   cudaSetDevice(s->d.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->mem) cudaFree(s->mem);
+  if (s->gridData) cudaFree(s->gridData);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -853,6 +931,34 @@ st_status st_diff_create(const st_diff_desc* d, const float* pos3, uint32_t np, 
     }
   }
   if (e == cudaSuccess) e = cudaMemcpy(s->tgt, target, nc * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && d->collider_grid) {
+    // the box's exact signed distance at grid nodes, 3 cells of margin around it (as a mesh collider's grid is built)
+    const double cell = d->grid_cell > 0.0f ? (double)d->grid_cell : 0.5 / d->n, m = 3.0 * cell;
+    DGrid& Gd = s->col;
+    Gd.mode = 1;
+    Gd.cell = cell;
+    for (int k = 0; k < 3; k++) {
+      Gd.origin[k] = -((double)d->box_half[k] + m);
+      Gd.dims[k] = (int)std::floor(2.0 * ((double)d->box_half[k] + m) / cell + 1e-9) + 1;
+    }
+    const size_t ng = (size_t)Gd.dims[0] * Gd.dims[1] * Gd.dims[2];
+    std::vector<float> h(ng);
+    for (int k = 0; k < Gd.dims[2]; k++)
+      for (int j = 0; j < Gd.dims[1]; j++)
+        for (int i = 0; i < Gd.dims[0]; i++) {
+          const double x[3] = {Gd.origin[0] + i * cell, Gd.origin[1] + j * cell, Gd.origin[2] + k * cell};
+          double o2 = 0.0, in = -1e30;
+          for (int a = 0; a < 3; a++) {
+            const double qd = std::fabs(x[a]) - d->box_half[a];
+            o2 += std::max(qd, 0.0) * std::max(qd, 0.0);
+            in = std::max(in, qd);
+          }
+          h[(size_t)i + (size_t)Gd.dims[0] * ((size_t)j + (size_t)Gd.dims[1] * k)] = (float)(std::sqrt(o2) + std::min(in, 0.0));
+        }
+    e = cudaMalloc((void**)&s->gridData, ng * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(s->gridData, h.data(), ng * 4, cudaMemcpyHostToDevice);
+    Gd.data = s->gridData;
+  }
   if (e != cudaSuccess) {
     snprintf(g_derr, sizeof(g_derr), "diff create: %s", cudaGetErrorString(e));
     st::set_error_text(g_derr);
@@ -891,6 +997,26 @@ st_status st_diff_backward(st_diff* s, double* grad) {
 }
 
 void* st_diff_stream(st_diff* s) { return s ? (void*)s->stream : nullptr; }
+
+st_status st_diff_read_state(st_diff* s, float* pos3, float* vel3) {
+  if (!s || !pos3) return ST_BAD_ARG;
+  DK(cudaSetDevice(s->d.device));
+  DK(cudaStreamSynchronize(s->stream));
+  const size_t n = s->np * 3;
+  for (int w = 0; w < 2; w++) {
+    float* out = w == 0 ? pos3 : vel3;
+    if (!out) continue;
+    const void* src = w == 0 ? s->x : s->v;
+    if (s->fp64) {
+      std::vector<double> h(n);
+      DK(cudaMemcpy(h.data(), src, n * 8, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < n; i++) out[i] = (float)h[i];
+    } else {
+      DK(cudaMemcpy(out, src, n * 4, cudaMemcpyDeviceToHost));
+    }
+  }
+  return ST_OK;
+}
 
 st_status st_diff_stats(st_diff* s, uint64_t* device_bytes, int32_t* cg_iters) {
   if (!s) return ST_BAD_ARG;

@@ -533,12 +533,13 @@ __device__ __forceinline__ uint32_t splitIdx(uint32_t local) {
 __global__ void __launch_bounds__(512) k_sor_pack(Bufs B) {
   __shared__ FlipParams P;
   loadParams(P, B.P);
-  const uint32_t nT = B.ctl->nFluidTiles;
+  const uint32_t nT = B.ctl->nFluidTiles, O = *B.poolOff;
   for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t t = B.fluidTiles[a], c = t * 512u + threadIdx.x, d = a * 512u + splitIdx(threadIdx.x);
+    const uint32_t t = B.fluidTiles[a], c = t * 512u + threadIdx.x, d = (O + a) * 512u + splitIdx(threadIdx.x);
     B.cp[d] = B.pres[c];
     B.crhs[d] = B.rhs[c];
     B.cinfo[d] = B.sorInfo[c];
+    if (threadIdx.x == 6) B.pomega[O + a] = P.omega;
     if (threadIdx.x < 6) {
       const uint32_t tt = t / P.tx, ti = t % P.tx, tj = tt % P.ty, tk = tt / P.ty;
       const int dir = threadIdx.x;
@@ -550,52 +551,115 @@ __global__ void __launch_bounds__(512) k_sor_pack(Bufs B) {
       if (dir == 4 && tk > 0) n = t - P.tx * P.ty;
       if (dir == 5 && tk + 1 < P.tz) n = t + P.tx * P.ty;
       const uint32_t sl = n != 0xffffffffu ? B.slotOf[n] : 0xffffffffu;
-      B.nbs[a * 6u + dir] = sl != 0xffffffffu ? sl : a;   // no fluid there: never summed, so any valid cell will do
+      B.nbs[(O + a) * 6u + dir] = O + (sl != 0xffffffffu ? sl : a);   // no fluid there: never summed, any valid cell will do
     }
   }
+}
+// one colour of one red-black iteration on the copied tile at position a (neighbour positions in nbs are absolute)
+__device__ __forceinline__ void sorTile(float* cp, const float* __restrict__ crhs, const uint16_t* __restrict__ cinfo,
+                                        const uint32_t* __restrict__ nbs, uint32_t a, float omega, uint32_t color, uint32_t j) {
+  const uint32_t lz = j >> 5, ly = (j >> 2) & 7u;
+  const uint32_t lx = 2u * (j & 3u) + ((ly + lz + color) & 1u), row = j & ~3u;
+  const uint32_t own = color * 256u + j, oth = (color ^ 1u) * 256u;
+  const uint32_t* nb = nbs + a * 6u;
+  const uint32_t base = a * 512u + oth;
+  const uint32_t ixm = lx > 0 ? base + row + ((lx - 1u) >> 1) : nb[0] * 512u + oth + row + 3u;
+  const uint32_t ixp = lx < 7 ? base + row + ((lx + 1u) >> 1) : nb[1] * 512u + oth + row;
+  const uint32_t iym = ly > 0 ? base + j - 4u : nb[2] * 512u + oth + j + 28u;
+  const uint32_t iyp = ly < 7 ? base + j + 4u : nb[3] * 512u + oth + j - 28u;
+  const uint32_t izm = lz > 0 ? base + j - 32u : nb[4] * 512u + oth + j + 224u;
+  const uint32_t izp = lz < 7 ? base + j + 32u : nb[5] * 512u + oth + j - 224u;
+  const uint32_t c = a * 512u + own;
+  const uint32_t info = cinfo[c];
+  const float p0 = cp[c], r0 = crhs[c];
+  const float pxm = cp[ixm], pxp = cp[ixp], pym = cp[iym], pyp = cp[iyp], pzm = cp[izm], pzp = cp[izp];
+  if (!(info & 0x8000u)) return;
+  const uint32_t nns = (info >> 8) & 7u;
+  if (nns == 0u) { cp[c] = 0.0f; return; }
+  float sum = 0.0f;
+  if (info & 1u) sum += pxm;
+  if (info & 2u) sum += pxp;
+  if (info & 4u) sum += pym;
+  if (info & 8u) sum += pyp;
+  if (info & 16u) sum += pzm;
+  if (info & 32u) sum += pzp;
+  const float pg = (r0 + sum) / (float)nns;
+  cp[c] = p0 + omega * (pg - p0);
 }
 __global__ void __launch_bounds__(256) k_sor_c(Bufs B, uint32_t color) {
   // launched as a programmatic dependent of the previous sweep: its CTAs may become resident early, and wait here until
   // that sweep has finished and its writes are visible
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const uint32_t nT = B.ctl->nFluidTiles;
+  const uint32_t nT = B.ctl->nFluidTiles, O = *B.poolOff;
   const float omega = B.P->omega;
-  const uint32_t j = threadIdx.x, lz = j >> 5, ly = (j >> 2) & 7u;
-  const uint32_t lx = 2u * (j & 3u) + ((ly + lz + color) & 1u), row = j & ~3u;
-  const uint32_t own = color * 256u + j, oth = (color ^ 1u) * 256u;
-  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
-    const uint32_t* nb = B.nbs + a * 6u;
-    const uint32_t base = a * 512u + oth;
-    const uint32_t ixm = lx > 0 ? base + row + ((lx - 1u) >> 1) : nb[0] * 512u + oth + row + 3u;
-    const uint32_t ixp = lx < 7 ? base + row + ((lx + 1u) >> 1) : nb[1] * 512u + oth + row;
-    const uint32_t iym = ly > 0 ? base + j - 4u : nb[2] * 512u + oth + j + 28u;
-    const uint32_t iyp = ly < 7 ? base + j + 4u : nb[3] * 512u + oth + j - 28u;
-    const uint32_t izm = lz > 0 ? base + j - 32u : nb[4] * 512u + oth + j + 224u;
-    const uint32_t izp = lz < 7 ? base + j + 32u : nb[5] * 512u + oth + j - 224u;
-    const uint32_t c = a * 512u + own;
-    const uint32_t info = B.cinfo[c];
-    const float p0 = B.cp[c], r0 = B.crhs[c];
-    const float pxm = B.cp[ixm], pxp = B.cp[ixp], pym = B.cp[iym], pyp = B.cp[iyp], pzm = B.cp[izm], pzp = B.cp[izp];
-    if (!(info & 0x8000u)) continue;
-    const uint32_t nns = (info >> 8) & 7u;
-    if (nns == 0u) { B.cp[c] = 0.0f; continue; }
-    float sum = 0.0f;
-    if (info & 1u) sum += pxm;
-    if (info & 2u) sum += pxp;
-    if (info & 4u) sum += pym;
-    if (info & 8u) sum += pyp;
-    if (info & 16u) sum += pzm;
-    if (info & 32u) sum += pzp;
-    const float pg = (r0 + sum) / (float)nns;
-    B.cp[c] = p0 + omega * (pg - p0);
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) sorTile(B.cp, B.crhs, B.cinfo, B.nbs, O + a, omega, color, threadIdx.x);
+}
+// the sweeps of a pooled batch: every tank's copied tiles in one launch, each with its own tank's SOR factor
+__global__ void __launch_bounds__(256) k_sor_pool(const PoolBufs Q, uint32_t color) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const uint32_t nT = *Q.total;
+  for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) sorTile(Q.cp, Q.crhs, Q.cinfo, Q.nbs, a, Q.pomega[a], color, threadIdx.x);
+}
+// The same sweeps as one persistent cooperative launch: every CTA walks its share of the pool, then waits for all CTAs
+// at a grid barrier between colours. Each wait is bounded (limit_ns of the global timer): a barrier that runs out sets
+// Q.err and every CTA returns after its current sweep, so the host gets ST_TIMEOUT and the context stays usable.
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool gridBarrier(unsigned int* bar, unsigned int expect, unsigned int& gen, unsigned int* err, uint64_t limit_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    gen++;
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const uint64_t t0 = gtimer();
+    while (true) {
+      unsigned int v;
+      asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= gen * expect) break;
+      if (*(volatile unsigned int*)err) break;
+      if (gtimer() - t0 > limit_ns) { atomicOr(err, 1u); break; }
+      __nanosleep(64);
+    }
+    __threadfence();
   }
+  __syncthreads();
+  return *(volatile unsigned int*)err == 0u;
+}
+__global__ void __launch_bounds__(256) k_sor_persist(const PoolBufs Q, int iters, unsigned int expect, uint64_t limit_ns) {
+  const uint32_t nT = *Q.total;
+  unsigned int gen = 0;
+  for (int it = 0; it < iters; it++)
+    for (uint32_t color = 0; color < 2; color++) {
+      for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) sorTile(Q.cp, Q.crhs, Q.cinfo, Q.nbs, a, Q.pomega[a], color, threadIdx.x);
+      __threadfence();
+      if (!gridBarrier(Q.bar, expect, gen, Q.err, limit_ns)) return;
+    }
+}
+// offsets of every tank's copied tiles in the pool (ascending tank order) and the pool's total; the barrier word cleared
+__global__ void k_pool_plan(const PoolBufs Q, const Ctl* const* ctls, uint32_t ntanks) {
+  if (threadIdx.x != 0) return;
+  uint32_t o = 0;
+  for (uint32_t k = 0; k < ntanks; k++) {
+    Q.off[k] = o;
+    o += ctls[k]->nFluidTiles;
+  }
+  *Q.total = o;
+  *Q.bar = 0u;
+}
+// a barrier that expects more arrivals than the launch has: every wait runs out (the test of the bounded wait)
+__global__ void __launch_bounds__(256) k_barrier_test(unsigned int* bar, unsigned int* err, unsigned int expect, uint64_t limit_ns) {
+  unsigned int gen = 0;
+  gridBarrier(bar, expect, gen, err, limit_ns);
 }
 // back into the grid; the slot map goes back to empty for the next step
 __global__ void __launch_bounds__(512) k_sor_unpack(Bufs B) {
-  const uint32_t nT = B.ctl->nFluidTiles;
+  const uint32_t nT = B.ctl->nFluidTiles, O = *B.poolOff;
   for (uint32_t a = blockIdx.x; a < nT; a += gridDim.x) {
     const uint32_t t = B.fluidTiles[a];
-    B.pres[t * 512u + threadIdx.x] = B.cp[a * 512u + splitIdx(threadIdx.x)];
+    B.pres[t * 512u + threadIdx.x] = B.cp[(O + a) * 512u + splitIdx(threadIdx.x)];
     if (threadIdx.x == 0) B.slotOf[t] = 0xffffffffu;
   }
 }
@@ -1049,10 +1113,15 @@ int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
   else k_norm_div<false><<<grid, 512, 0, s>>>(B);
   return 1;
 }
-int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s) {
+int launch_sor_pack(const Bufs& B, int grid4, cudaStream_t s) {
   k_sor_slots<<<64, 256, 0, s>>>(B);
   k_sor_pack<<<grid4, 512, 0, s>>>(B);
-  // each sweep is a programmatic dependent launch of the one before, so its launch overlaps the previous sweep's tail
+  return 2;
+}
+// iters red-black iterations, each colour a programmatic dependent launch of the one before (its launch overlaps the
+// previous sweep's tail); the kernel is either a tank's own sweep or a pooled batch's
+template <class Arg>
+static int launch_sweeps(void (*kern)(Arg, uint32_t), const Arg& A, int grid, int iters, cudaStream_t s) {
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
@@ -1064,9 +1133,37 @@ int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream
   cfg.attrs = at;
   cfg.numAttrs = 1;
   for (int it = 0; it < iters; it++)
-    for (uint32_t color = 0; color < 2; color++) cudaLaunchKernelEx(&cfg, k_sor_c, B, color);
+    for (uint32_t color = 0; color < 2; color++) cudaLaunchKernelEx(&cfg, kern, A, color);
+  return 2 * iters;
+}
+int launch_sor_unpack(const Bufs& B, int grid4, cudaStream_t s) {
   k_sor_unpack<<<grid4, 512, 0, s>>>(B);
-  return 2 * iters + 3;
+  return 1;
+}
+int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s) {
+  int nl = launch_sor_pack(B, grid4, s);
+  nl += launch_sweeps(k_sor_c, B, grid, iters, s);
+  return nl + launch_sor_unpack(B, grid4, s);
+}
+int launch_pool_plan(const PoolBufs& Q, const Ctl* const* ctls, uint32_t ntanks, cudaStream_t s) {
+  k_pool_plan<<<1, 32, 0, s>>>(Q, ctls, ntanks);
+  return 1;
+}
+int launch_pool_sweeps(const PoolBufs& Q, int grid, int iters, cudaStream_t s) { return launch_sweeps(k_sor_pool, Q, grid, iters, s); }
+cudaError_t launch_pool_persistent(const PoolBufs& Q, int grid, int iters, uint64_t limit_ns, cudaStream_t s) {
+  unsigned int expect = (unsigned int)grid;
+  int it = iters;
+  void* args[] = {(void*)&Q, (void*)&it, (void*)&expect, (void*)&limit_ns};
+  return cudaLaunchCooperativeKernel((const void*)k_sor_persist, dim3((unsigned)grid), dim3(256), args, 0, s);
+}
+int persistent_ctas_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sor_persist, 256, 0);
+  return n;
+}
+cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, unsigned int expect, uint64_t limit_ns, cudaStream_t s) {
+  void* args[] = {(void*)&bar, (void*)&err, (void*)&expect, (void*)&limit_ns};
+  return cudaLaunchCooperativeKernel((const void*)k_barrier_test, dim3((unsigned)grid), dim3(256), args, 0, s);
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {

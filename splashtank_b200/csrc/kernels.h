@@ -17,6 +17,15 @@ int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
 int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_sor_compact(const Bufs& B, int grid, int grid4, int iters, cudaStream_t s);
+int launch_sor_pack(const Bufs& B, int grid4, cudaStream_t s);
+int launch_sor_unpack(const Bufs& B, int grid4, cudaStream_t s);
+// a pooled batch's pressure sweeps (capi.cu's ST_BATCH_POOLED): the plan of offsets, then the sweeps over every tank's
+// copied tiles, as launches chained by programmatic dependence or as one persistent cooperative launch
+int launch_pool_plan(const PoolBufs& Q, const Ctl* const* ctls, uint32_t ntanks, cudaStream_t s);
+int launch_pool_sweeps(const PoolBufs& Q, int grid, int iters, cudaStream_t s);
+cudaError_t launch_pool_persistent(const PoolBufs& Q, int grid, int iters, uint64_t limit_ns, cudaStream_t s);
+int persistent_ctas_per_sm();
+cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, unsigned int expect, uint64_t limit_ns, cudaStream_t s);
 int launch_project(const Bufs& B, int grid, cudaStream_t s);
 int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);

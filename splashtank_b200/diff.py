@@ -20,7 +20,9 @@ def funcs():
 
 class DiffRollout:
     def __init__(self, n, pos, target, steps, ckpt_every=8, fp64=False, dt=1.0 / 240.0, flip=0.95, g=9.81, q0=None,
-                 margin=None, box_half=(0.06, 0.12, 0.25), cg_maxit=None, cg_tol=None, device=0):
+                 margin=None, box_half=(0.06, 0.12, 0.25), cg_maxit=None, cg_tol=None, device=0, collider="box", grid_cell=None):
+        """collider: "box" (analytic signed distance) or "grid" (the box's distance grid with nodes grid_cell apart,
+        default half a cell, sampled and differentiated as sdfEval samples a collider grid)."""
         self.f = funcs()
         d = abi.DiffDesc()
         d.size = C.sizeof(abi.DiffDesc)
@@ -32,6 +34,8 @@ class DiffRollout:
         d.box_half[:] = [float(x) for x in box_half]
         d.cg_maxit = int(cg_maxit if cg_maxit is not None else (4000 if fp64 else 1000))
         d.cg_tol = float(cg_tol if cg_tol is not None else (1e-12 if fp64 else 1e-5))
+        d.collider_grid = 1 if collider == "grid" else 0
+        d.grid_cell = float(grid_cell if grid_cell is not None else 0.5 * h)
         p = np.ascontiguousarray(pos, np.float32)
         t = np.ascontiguousarray(target, np.float32)
         assert t.size == n ** 3
@@ -57,6 +61,15 @@ class DiffRollout:
         if st != abi.ST_OK:
             raise status_error("diff backward", st)
         return g
+
+    def state(self):
+        """(positions, velocities) of the particles after the last forward pass, (np, 3) float32 each."""
+        p = np.zeros((self.np, 3), np.float32)
+        v = np.zeros((self.np, 3), np.float32)
+        st = self.f["diff_read_state"](self._h, p.ctypes.data_as(abi.f32p), v.ctypes.data_as(abi.f32p))
+        if st != abi.ST_OK:
+            raise status_error("diff read_state", st)
+        return p, v
 
     def stream(self):
         return self.f["diff_stream"](self._h)

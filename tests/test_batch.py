@@ -86,13 +86,15 @@ def test_batch_step_matches_single_tank_steps():
     from splashtank_b200.scene import SceneRunner
     spec = scenes.BatchTanks(count=4, seed=9, edges=(32, 48))
     runs = {}
-    for mode in ("graph", "sequential", "single"):
+    for mode in ("graph", "sequential", "pooled", "persistent", "single"):
         made = [spec.make(k, FlipSim) for k in range(4)]
         sims = [m[0] for m in made]
         runners = [SceneRunner(s) for s in sims]
-        if mode == "graph":
+        if mode in ("graph", "pooled"):
             sims[1].set_launch(2, 1, 2)   # launch shapes differ per tank; results must not
         batch = TankBatch(sims, mode) if mode != "single" else None
+        if mode == "persistent":
+            batch.set_sweeps(2)
         for _ in range(6):
             opts = [spec.step_opts(k, sims[k], runners[k]) for k in range(4)]
             if batch:
@@ -112,5 +114,28 @@ def test_batch_step_matches_single_tank_steps():
         for s in sims:
             s.destroy()
     for k in range(4):
-        assert np.array_equal(runs["graph"][k].view(np.uint32), runs["single"][k].view(np.uint32)), k
-        assert np.array_equal(runs["sequential"][k].view(np.uint32), runs["single"][k].view(np.uint32)), k
+        for mode in ("graph", "sequential", "pooled", "persistent"):
+            assert np.array_equal(runs[mode][k].view(np.uint32), runs["single"][k].view(np.uint32)), (mode, k)
+
+
+@pytest.mark.gpu
+def test_persistent_sweep_barrier_wait_is_bounded():
+    """The persistent sweep's grid barrier with one CTA that never arrives: every wait runs out after its limit, the
+    kernel sets its error flag and returns, and the device stays usable (a batch step runs right after)."""
+    import time
+    from splashtank_b200.batch import TankBatch, barrier_test
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    t0 = time.perf_counter()
+    assert barrier_test(missing=1, limit_us=200_000)
+    assert time.perf_counter() - t0 < 20.0
+    spec = scenes.BatchTanks(count=2, seed=3, edges=(32,))
+    sims = [spec.make(k, FlipSim)[0] for k in range(2)]
+    runners = [SceneRunner(s) for s in sims]
+    b = TankBatch(sims, "persistent")
+    for _ in range(3):
+        b.step(spec.dt, [spec.step_opts(k, sims[k], runners[k]) for k in range(2)])
+    assert all(s.readStats()["steps"] == 3 for s in sims)
+    b.destroy()
+    for s in sims:
+        s.destroy()
