@@ -917,6 +917,32 @@ def run_diff(a):
         fd.append((s64.forward(p0 + e, record=False) - s64.forward(p0 - e, record=False)) / 2e-3)
     fd = np.array(fd)
     s64.destroy()
+    # the collider as the box's distance grid (sdfEval's trilinear sampling, its gradient and Hessian in the adjoint):
+    # the FP32 gradient against the FP64 one, and its time
+    g32g = g64g = None
+    sg = d.make(collider="grid", device=local)
+    ms_grid = timed(lambda: (sg.forward(p0), sg.backward()), 1)
+    sg.forward(p0)
+    g32g = sg.backward()
+    sg.destroy()
+    sg64 = d.make(fp64=True, collider="grid", device=local)
+    sg64.forward(p0)
+    g64g = sg64.backward()
+    sg64.destroy()
+    # the rollout against the FLIP step on the same scene (the particles' displacements and the final density splat)
+    from splashtank_b200.diff import flip_rollout
+    sv = d.make(collider="grid", margin=0.15 / n, cg_tol=1e-6, device=local)
+    sv.forward(p0)
+    xd, _ = sv.state()
+    sv.destroy()
+    xf = flip_rollout(d, p0, device=local)
+    disp_d, disp_f = xd - d.pos, xf - d.pos
+    rho_d, rho_f = scenes.splat_density(xd, n), scenes.splat_density(np.clip(xf, 0.0, 1.0), n)
+    vs_flip = {"displacement_rel_l2": float(np.linalg.norm(disp_d - disp_f) / np.linalg.norm(disp_f)),
+               "density_rel_l2": float(np.linalg.norm(rho_d - rho_f) / np.linalg.norm(rho_f)),
+               "displacement_rms": float(np.sqrt((disp_f ** 2).sum(1).mean())),
+               "flip_step": "st_flip_step on the same particles, the box's distance grid on the same keyframe path, SOR 400 "
+                            "iterations, no density correction"}
     ps = d.pos.shape[0] * d.steps
     if rank == 0:
         line = {"metric": "gradient particle-steps/s (forward + adjoint)", "value": ps / (ms_grad * 1e-3), "unit": "particle-steps/s",
@@ -930,6 +956,9 @@ def run_diff(a):
                 "grad_check": {"f32_vs_f64_adjoint_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
                                "f64_adjoint_vs_fd_max_rel": float(np.max(np.abs(g64[idx] - fd)) / max(np.max(np.abs(fd)), 1e-300)),
                                "params_checked": idx, "fd_eps": 1e-3},
+                "grid_collider": {"gradient_ms": ms_grid,
+                                  "f32_vs_f64_adjoint_rel_l2": float(np.linalg.norm(g32g - g64g) / np.linalg.norm(g64g))},
+                "vs_flip_step": vs_flip,
                 "clocks": clk, "roofline": None, "gpu_launches": None,
                 "e2e": {"value": ps / (ms_grad * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": 27 * 8, "d2h_bytes_per_step": 27 * 8,
                         "note": "parameters up and gradient back through the C ABI are inside the timed calls"},

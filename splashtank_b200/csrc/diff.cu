@@ -212,10 +212,10 @@ __global__ void k_d_p2g(DGeo G, size_t np, const T* __restrict__ x, const T* __r
     }
   }
 }
-// cell types: outside the box nothing (walls are handled by the neighbour logic); collider cells solid; cells with a
-// particle fluid
+// cell types: outside the box nothing (walls are handled by the neighbour logic); collider cells solid (inside the
+// analytic box, or a distance below q0 at the centre for the grid, as colAt decides); cells with a particle fluid
 template <class T>
-__global__ void k_d_types(DGeo G, const int* __restrict__ count, const T* c, const T* hb, DGrid Gd, uint8_t* types) {
+__global__ void k_d_types(DGeo G, const int* __restrict__ count, const T* c, const T* hb, DGrid Gd, T q0, uint8_t* types) {
   const size_t nc = G.cells();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nc; i += (size_t)gridDim.x * blockDim.x) {
     const int ci = (int)(i % G.n), cj = (int)((i / G.n) % G.n), ck = (int)(i / ((size_t)G.n * G.n));
@@ -227,7 +227,7 @@ __global__ void k_d_types(DGeo G, const int* __restrict__ count, const T* c, con
       T phi, n[3], dphi[3], J[9];
       uint8_t rg = 0;
       colEval<T>(Gd, q, hb, &rg, 1, phi, n, dphi, J);
-      inside = phi < (T)0;
+      inside = phi < q0;   // colAt's test (src/flip/wgsl-core.js:127-131), as the step classifies collider cells
     }
     types[i] = inside ? T_SOLID : (count[i] > 0 ? T_FLUID : T_AIR);
   }
@@ -244,7 +244,8 @@ __device__ __forceinline__ void faceCells(const DGeo& G, int a, size_t f, long& 
   hi = hi3[a] >= G.n ? -1 : (long)G.cell(hi3[0], hi3[1], hi3[2]);
 }
 // face velocity: mass-weighted mean (recorded or frozen: which faces carry mass), gravity on y, collider velocity on
-// faces touching a collider cell, 0 on wall faces
+// faces touching a collider cell, 0 on wall faces; the old velocity u0 (the FLIP term's) is the mean, or the boundary's
+// velocity on those faces (normFaces, src/flip/wgsl-solver.js:75-105)
 template <class T>
 __global__ void k_d_norm(DGeo G, const T* __restrict__ mom, const T* __restrict__ mass, uint8_t* mask, int record,
                          const uint8_t* __restrict__ types, const T* vc, T gdt, T* u0, T* u1) {
@@ -254,12 +255,12 @@ __global__ void k_d_norm(DGeo G, const T* __restrict__ mom, const T* __restrict_
     const size_t f = t % nf;
     if (record) mask[t] = mass[t] > (T)0 ? 1 : 0;
     const T u = (mask[t] && mass[t] > (T)0) ? mom[t] / mass[t] : (T)0;
-    u0[t] = u;
     long lo, hi;
     faceCells(G, a, f, lo, hi);
-    T r = u - (a == 1 ? gdt : (T)0);
-    if (lo < 0 || hi < 0) r = (T)0;
-    else if (types[lo] == T_SOLID || types[hi] == T_SOLID) r = vc[a];
+    T r = u - (a == 1 ? gdt : (T)0), old = u;
+    if (lo < 0 || hi < 0) r = old = (T)0;                                                   // a wall
+    else if (types[lo] == T_SOLID || types[hi] == T_SOLID) r = old = vc[a];                // the collider's velocity
+    u0[t] = old;   // the step's old face velocity (vo): on a boundary face the boundary's, as normFaces sets it
     u1[t] = r;
   }
 }
@@ -342,8 +343,11 @@ __global__ void k_d_project(DGeo G, const uint8_t* __restrict__ types, const T* 
     u2[t] = r;
   }
 }
-// G2P + advection + collider push-out + wall clamp. flags (recorded or frozen) per particle: bit 0 touches the
-// collider, bit 1 its velocity pointed into it, bits 2-7 the position was clamped on (x lo, x hi, y lo, ...).
+// G2P + advection + collider push-out + wall clamp, then the step's velocity response (g2p after collideP,
+// src/flip/wgsl-solver.js:259-265): the displacement dsp = x_out - x_a of the push-out and the clamp together, and when
+// it is not negligible the velocity's component into it removed (v -= nrm min(v . nrm, 0), nrm = dsp / |dsp|).
+// flags (recorded or frozen) per particle: bit 0 touches the collider, bit 1 the velocity response applies (moved and
+// v . nrm < 0), bits 2-7 the position was clamped on (x lo, x hi, y lo, ...).
 template <class T>
 __global__ void k_d_g2p(DGeo G, size_t np, const T* __restrict__ x, const T* __restrict__ v, const T* __restrict__ u2,
                         const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, DGrid Gd, T q0, T lo, T hi, uint8_t* flags,
@@ -368,17 +372,34 @@ __global__ void k_d_g2p(DGeo G, size_t np, const T* __restrict__ x, const T* __r
     colEval<T>(Gd, q, hb, &rg, record, phi, n, dphi, J);
     if (record) regimes[p] = rg;
     if (record && phi < q0) fl |= 1;
-    if (fl & 1) {
-      for (int a = 0; a < 3; a++) xa[a] += n[a] * (q0 - phi);
-      const T vd = vn[0] * n[0] + vn[1] * n[1] + vn[2] * n[2];
-      if (record && vd < (T)0) fl |= 2;
-      if (fl & 2) for (int a = 0; a < 3; a++) vn[a] -= n[a] * vd;
+    T xc[3] = {xa[0], xa[1], xa[2]}, dsp[3] = {(T)0, (T)0, (T)0};
+    if (fl & 1)
+      for (int a = 0; a < 3; a++) {
+        xc[a] += n[a] * (q0 - phi);
+        dsp[a] = n[a] * fabs(q0 - phi);   // = the push where it was recorded (phi < q0); a frozen pass that no longer
+                                          // reaches q0 keeps the normal's side, so the response does not flip
+      }
+    for (int a = 0; a < 3; a++) {
+      if (record) { if (xc[a] < lo) fl |= (uint8_t)(4u << (2 * a)); else if (xc[a] > hi) fl |= (uint8_t)(8u << (2 * a)); }
+      const T before = xc[a];
+      if (fl & (4u << (2 * a))) xc[a] = lo;
+      else if (fl & (8u << (2 * a))) xc[a] = hi;
+      dsp[a] += xc[a] - before;
+    }
+    const T d2 = dsp[0] * dsp[0] + dsp[1] * dsp[1] + dsp[2] * dsp[2];
+    if (record && d2 > (T)1e-12) {
+      const T il = (T)1 / sqrt(d2);
+      const T vd = (vn[0] * dsp[0] + vn[1] * dsp[1] + vn[2] * dsp[2]) * il;
+      if (vd < (T)0) fl |= 2;
+    }
+    if (fl & 2) {
+      const T il = (T)1 / sqrt(d2);
+      const T nr[3] = {dsp[0] * il, dsp[1] * il, dsp[2] * il};
+      const T vd = vn[0] * nr[0] + vn[1] * nr[1] + vn[2] * nr[2];
+      for (int a = 0; a < 3; a++) vn[a] -= nr[a] * vd;
     }
     for (int a = 0; a < 3; a++) {
-      if (record) { if (xa[a] < lo) fl |= (uint8_t)(4u << (2 * a)); else if (xa[a] > hi) fl |= (uint8_t)(8u << (2 * a)); }
-      if (fl & (4u << (2 * a))) xa[a] = lo;
-      else if (fl & (8u << (2 * a))) xa[a] = hi;
-      xo[3 * p + a] = xa[a];
+      xo[3 * p + a] = xc[a];
       vo[3 * p + a] = vn[a];
     }
     if (record) flags[p] = fl;
@@ -433,7 +454,8 @@ __global__ void k_d_splat_b(DGeo G, size_t np, const T* __restrict__ x, const T*
 // inputs (in place), face adjoints of u2 and u0 (atomics), the collider centre's adjoint (atomics into gc[3]).
 template <class T>
 __global__ void k_d_g2p_b(DGeo G, size_t np, const T* __restrict__ x, const T* __restrict__ v, const T* __restrict__ u2,
-                          const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, DGrid Gd, T q0, const uint8_t* __restrict__ flags,
+                          const T* __restrict__ u0, T beta, T dt, const T* c, const T* hb, DGrid Gd, T q0, T lo, T hi,
+                          const uint8_t* __restrict__ flags,
                           const uint8_t* __restrict__ regimes, T* gx, T* gv, T* gu2, T* gu0, double* gc) {
   const size_t nf = G.nf(0);
   T gcx = 0, gcy = 0, gcz = 0;
@@ -455,21 +477,41 @@ __global__ void k_d_g2p_b(DGeo G, size_t np, const T* __restrict__ x, const T* _
     uint8_t rg = regimes[p];
     colEval<T>(Gd, q, hb, &rg, 0, phi, n, dphi, J);
     T gxo[3] = {gx[3 * p], gx[3 * p + 1], gx[3 * p + 2]}, gvo[3] = {gv[3 * p], gv[3 * p + 1], gv[3 * p + 2]};
+    // the forward's output position again: push-out, then the clamp
+    T xc[3] = {xa[0], xa[1], xa[2]};
+    if (fl & 1)
+      for (int a = 0; a < 3; a++) xc[a] += n[a] * (q0 - phi);
+    for (int a = 0; a < 3; a++) {
+      if (fl & (4u << (2 * a))) xc[a] = lo;
+      else if (fl & (8u << (2 * a))) xc[a] = hi;
+    }
+    // velocity response: v_out = v' - nrm (v' . nrm), nrm = dsp / |dsp|, dsp = x_out - x_a
+    T gvp[3] = {gvo[0], gvo[1], gvo[2]}, gxa[3] = {(T)0, (T)0, (T)0};
+    if (fl & 2) {
+      const T dsp[3] = {xc[0] - xa[0], xc[1] - xa[1], xc[2] - xa[2]};
+      const T l = sqrt(dsp[0] * dsp[0] + dsp[1] * dsp[1] + dsp[2] * dsp[2]);
+      const T nr[3] = {dsp[0] / l, dsp[1] / l, dsp[2] / l};
+      const T vd = vn[0] * nr[0] + vn[1] * nr[1] + vn[2] * nr[2];
+      const T ng = nr[0] * gvo[0] + nr[1] * gvo[1] + nr[2] * gvo[2];
+      T gnr[3];
+      for (int a = 0; a < 3; a++) {
+        gvp[a] = gvo[a] - nr[a] * ng;
+        gnr[a] = -(vd * gvo[a] + ng * vn[a]);
+      }
+      const T nd = nr[0] * gnr[0] + nr[1] * gnr[1] + nr[2] * gnr[2];
+      for (int a = 0; a < 3; a++) {
+        const T gd = (gnr[a] - nr[a] * nd) / l;   // through nrm = dsp / |dsp|
+        gxo[a] += gd;                            // dsp = x_out - x_a
+        gxa[a] -= gd;
+      }
+    }
     // wall clamp: a clamped coordinate is constant
     for (int a = 0; a < 3; a++) if (fl & (12u << (2 * a))) gxo[a] = (T)0;
-    // collider: x_c = x_a + n (q0 - phi); v_c = v' - n (v'.n) when bit 1
-    T gxa[3] = {gxo[0], gxo[1], gxo[2]}, gvp[3] = {gvo[0], gvo[1], gvo[2]};
+    // collider: x_c = x_a + n (q0 - phi)
+    for (int a = 0; a < 3; a++) gxa[a] += gxo[a];
     if (fl & 1) {
       T gn[3] = {gxo[0] * (q0 - phi), gxo[1] * (q0 - phi), gxo[2] * (q0 - phi)};
       T gphi = -(gxo[0] * n[0] + gxo[1] * n[1] + gxo[2] * n[2]);
-      if (fl & 2) {
-        const T vd = vn[0] * n[0] + vn[1] * n[1] + vn[2] * n[2];
-        const T ng = n[0] * gvo[0] + n[1] * gvo[1] + n[2] * gvo[2];
-        for (int a = 0; a < 3; a++) {
-          gvp[a] = gvo[a] - n[a] * ng;
-          gn[a] += -(ng * vn[a] + vd * gvo[a]);
-        }
-      }
       // phi and n are functions of q = x_a - c: d phi = dphi . dq, d n = J dq
       T gq[3];
       for (int r = 0; r < 3; r++) gq[r] = gphi * dphi[r] + J[r] * gn[0] + J[3 + r] * gn[1] + J[6 + r] * gn[2];
@@ -537,11 +579,13 @@ __global__ void k_d_norm_b(DGeo G, const uint8_t* __restrict__ types, const T* _
     // b_c = -(h/dt) (u1[c's high face] - u1[c's low face]) for fluid c
     if (lo >= 0 && types[lo] == T_FLUID) g += -hdt * gb[lo];
     if (hi >= 0 && types[hi] == T_FLUID) g -= -hdt * gb[hi];
+    // the G2P's FLIP term reads u0 directly: on a boundary face u0 is the boundary's velocity like u1
     T g0 = (T)0;
     if (lo < 0 || hi < 0) g0 = (T)0;
-    else if (types[lo] == T_SOLID || types[hi] == T_SOLID) { if (a == 0) gva += g; else if (a == 1) gvb += g; else gvcz += g; }
-    else g0 = g;
-    g0 += gu0[t];   // the G2P's FLIP term reads u0 directly
+    else if (types[lo] == T_SOLID || types[hi] == T_SOLID) {
+      const T gb2 = g + gu0[t];
+      if (a == 0) gva += gb2; else if (a == 1) gvb += gb2; else gvcz += gb2;
+    } else g0 = g + gu0[t];
     const bool m = mask[t] && mass[t] > (T)0;
     gmom[t] = m ? g0 / mass[t] : (T)0;
     gmass[t] = m ? -g0 * u0[t] / mass[t] : (T)0;
@@ -742,7 +786,7 @@ static st_status step_fwd(st_diff* s, int k, bool record, const double* cs, cons
   DK(cudaMemsetAsync(s->mass, 0, 3 * nf * sizeof(T), q));
   if (record) DK(cudaMemsetAsync(s->count, 0, nc * sizeof(int), q));
   k_d_p2g<T><<<gr, 256, 0, q>>>(G, s->np, P<T>(s->x), P<T>(s->v), P<T>(s->mom), P<T>(s->mass), record ? s->count : nullptr);
-  if (record) k_d_types<T><<<gr, 256, 0, q>>>(G, s->count, cb, cb + 6, s->grid_(), types);
+  if (record) k_d_types<T><<<gr, 256, 0, q>>>(G, s->count, cb, cb + 6, s->grid_(), (T)s->d.q0, types);
   T* u0 = tapeSlot >= 0 ? P<T>(s->tu0) + (size_t)tapeSlot * 3 * nf : P<T>(s->u0);
   T* u2 = tapeSlot >= 0 ? P<T>(s->tu2) + (size_t)tapeSlot * 3 * nf : P<T>(s->u2);
   T* pp = tapeSlot >= 0 ? P<T>(s->tp) + (size_t)tapeSlot * nc : P<T>(s->p);
@@ -838,7 +882,8 @@ static st_status backward(st_diff* s, double* grad) {
       DK(cudaMemsetAsync(s->gu2, 0, 3 * nf * sizeof(T), q));
       DK(cudaMemsetAsync(s->gu0, 0, 3 * nf * sizeof(T), q));
       DK(cudaMemsetAsync(s->cred, 0, 8 * sizeof(double), q));
-      k_d_g2p_b<T><<<gr, 256, 0, q>>>(G, np, tx, tv, u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, s->grid_(), (T)s->d.q0, flags,
+      k_d_g2p_b<T><<<gr, 256, 0, q>>>(G, np, tx, tv, u2, u0, (T)s->d.flip, (T)s->d.dt, cb, cb + 6, s->grid_(), (T)s->d.q0,
+                                      (T)s->d.margin, (T)(1.0 - s->d.margin), flags,
                                       regimes, P<T>(s->gx), P<T>(s->gv), P<T>(s->gu2), P<T>(s->gu0), s->cred);
       k_d_project_b<T><<<gr, 256, 0, q>>>(G, types, P<T>(s->gu2), (T)(s->d.dt / G.h), P<T>(s->gp));
       st_status st = pcg<T>(s, types, P<T>(s->gp), P<T>(s->gb));   // A is symmetric: the adjoint solve uses it again

@@ -89,3 +89,41 @@ class DiffRollout:
             self.destroy()
         except Exception:
             pass
+
+
+def flip_rollout(dam, params, box_half=(0.06, 0.12, 0.25), iters=400, omega=1.9, device=0):
+    """The same rollout through the FLIP step itself (st_flip_step): dam's particles (unit box, shifted into the
+    reference box) with the initial velocity params[24:27], the box collider as its distance grid (half a cell apart)
+    moving along the keyframe path params[:24] (linear, keyframes evenly over the rollout, the collider's velocity from
+    consecutive poses as SceneRunner gives it), FLIP 0.95, gravity 9.81, no density correction, no sheet tearing, the
+    SOR run for `iters` iterations. Returns the particles' final positions in the unit box, in the input order."""
+    from .flip import FlipSim
+    from .scene import SceneRunner, box_sdf
+    n, steps = dam.n, dam.steps
+    h = 1.0 / n
+    sim = FlipSim(h / 2, len(dam.pos), size=(1.0, 1.0, 1.0), device=device)
+    p0 = dam.pos.astype(np.float32).copy()
+    p0[:, 0] -= 0.5
+    p0[:, 2] -= 0.5
+    sim.add_many(p0, np.tile(np.asarray(params[24:27], np.float32)[None, :], (len(p0), 1)))
+    sdf = box_sdf(*box_half, h / 2, sid=1)
+    K = np.asarray(params[:24], np.float64).reshape(8, 3)
+    T = steps / 240.0
+
+    def centre(t):
+        u = t / T * 7.0
+        i = min(6, max(0, int(np.floor(u))))
+        a = u - i
+        return (1 - a) * K[i] + a * K[i + 1]
+    run = SceneRunner(sim)
+    opts = dict(g=9.81, flip=0.95, comp=0.0, iters=iters, omega=omega, vmax=100.0, tear=0.0)
+    for k in range(steps):
+        c = centre((k + 1) / 240.0)
+        run.step(1 / 240.0, [dict(id=1, sdf=sdf, x=c[0] - 0.5, y=c[1], z=c[2] - 0.5)], opts)
+    out = np.zeros((len(p0), 4), np.float32)
+    sim.readbackInto(out)
+    sim.destroy()
+    x = out[:, :3].copy()
+    x[:, 0] += 0.5
+    x[:, 2] += 0.5
+    return x
