@@ -1032,10 +1032,12 @@ st_status st_diff_backward(st_diff* s, double* grad) {
     return ST_BAD_ARG;
   }
   DK(cudaSetDevice(s->d.device));
-  // the final state of the recorded pass: recompute it (a frozen pass may have run since)
+  // the final state of the recorded pass: recompute it (a frozen pass may have run since) as a frozen pass, so the
+  // decisions stay those of the recording (recording again could flip one whose test sits at rounding level, such as
+  // the sign of v.n of a particle sliding along the collider, since the FP64 sums are atomic)
   double loss;
   std::vector<double> prm = s->params;
-  st_status st = s->fp64 ? forward<double>(s, prm.data(), true, &loss) : forward<float>(s, prm.data(), true, &loss);
+  st_status st = s->fp64 ? forward<double>(s, prm.data(), false, &loss) : forward<float>(s, prm.data(), false, &loss);
   if (st != ST_OK) return st;
   s->cgIters = 0;
   return s->fp64 ? backward<double>(s, grad) : backward<float>(s, grad);

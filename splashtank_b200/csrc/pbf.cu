@@ -193,16 +193,14 @@ __global__ void __launch_bounds__(PBF_T, 4) k_pbf_visc(const PbfParams* __restri
     const float irho = P.irho;
     V3 a = v3(0.0f, 0.0f, 0.0f);
     if (P.visc > 0.0f) {
-      const PbfRows R(P, cellS[t]);
-      for (int rr = 0; rr < R.nrows; rr++)
-        for (uint32_t s = R.begin(P, start, rr), e = R.end(P, start, rr); s < e; s++) {
-          if (s == t) continue;
-          const V3 dd = pi - xyz(posF[s]);
-          const float r2 = dot3(dd, dd);
-          if (r2 >= P.h2) continue;
-          const float tt = P.h2 - r2;
-          a = a + (xyz(vel2S[s]) - vi) * (P.poly * tt * tt * tt * irho);
-        }
+      pbfNear(P, posF, start, cellS[t], pi, [&](uint32_t s) {
+        if (s == t) return;
+        const V3 dd = pi - xyz(posF[s]);
+        const float r2 = dot3(dd, dd);
+        if (r2 >= P.h2) return;
+        const float tt = P.h2 - r2;
+        a = a + (xyz(vel2S[s]) - vi) * (P.poly * tt * tt * tt * irho);
+      });
     }
     const V3 nv = vi + a * P.visc;
     vel[i] = make_float4(nv.x, nv.y, nv.z, 0.0f);
@@ -362,7 +360,7 @@ cudaError_t pbf_dev_alloc(PbfDev& D, uint32_t maxN, uint32_t ncell) {
   const size_t N = std::max<uint32_t>(maxN, 1);
   A((void**)&D.P, sizeof(PbfParams));
   A((void**)&D.key, N * 4); A((void**)&D.rank, N * 4); A((void**)&D.tmp, N * 4); A((void**)&D.sidx, N * 4); A((void**)&D.cellS, N * 4);
-  A((void**)&D.xs[0], N * 16); A((void**)&D.xs[1], N * 16); A((void**)&D.bgrS, N * 16); A((void**)&D.lamS, N * 4);
+  A((void**)&D.xs[0], (N + PBF_PAD) * 16); A((void**)&D.xs[1], (N + PBF_PAD) * 16); A((void**)&D.bgrS, N * 16); A((void**)&D.lamS, N * 4);
   A((void**)&D.cnt, (size_t)ncell * 4); A((void**)&D.start, ((size_t)ncell + 1) * 4); A((void**)&D.bsum, ((size_t)nb + 1) * 4);
   return e;
 }
@@ -374,7 +372,7 @@ void pbf_dev_free(PbfDev& D) {
 }
 size_t pbf_dev_bytes(uint32_t maxN, uint32_t ncell) {
   const size_t N = std::max<uint32_t>(maxN, 1);
-  return N * (5 * 4 + 3 * 16 + 4) + (size_t)ncell * 8 + ((size_t)ncell / PBF_SCAN + 2) * 4 + sizeof(PbfParams);
+  return N * (5 * 4 + 3 * 16 + 4) + 2 * PBF_PAD * 16 + (size_t)ncell * 8 + ((size_t)ncell / PBF_SCAN + 2) * 4 + sizeof(PbfParams);
 }
 
 }  // namespace st
@@ -443,8 +441,8 @@ st_status st_pbf_create(const st_pbf_desc* ds, st_pbf** out) {
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
   const size_t N = s->maxN;
-  for (float4** p : {&s->pos, &s->vel, &s->prd, &s->posF, &s->vel2S})
-    if ((e = cudaMalloc((void**)p, N * 16)) != cudaSuccess) return fail("particles", e);
+  for (float4** p : {&s->pos, &s->vel, &s->prd, &s->posF, &s->vel2S})   // posF is walked by the viscosity pass: padded
+    if ((e = cudaMalloc((void**)p, (p == &s->posF ? N + PBF_PAD : N) * 16)) != cudaSuccess) return fail("particles", e);
   if ((e = cudaMemsetAsync(s->pos, 0, N * 16, s->stream)) != cudaSuccess) return fail("memset", e);
   if ((e = cudaMemsetAsync(s->vel, 0, N * 16, s->stream)) != cudaSuccess) return fail("memset", e);
   if ((e = pbf_dev_alloc(s->D, s->maxN, s->ncell)) != cudaSuccess) return fail("solver buffers", e);

@@ -91,31 +91,79 @@ __device__ __forceinline__ uint32_t pbfCellOf(const PbfParams& P, V3 p) {
   const int cz = pbfAxisCell((p.z - P.bz0) * P.inv, P.nz);
   return (uint32_t)cx + P.nx * ((uint32_t)cy + P.ny * (uint32_t)cz);
 }
-// the 27-cell neighbourhood as 9 runs of sorted slots (three x-adjacent cells are contiguous), z outer, y inner: the
-// loop order of lambda, delta and viscosity (src/gpu.js:220-224). Use:
-//   PbfRows R(P, c); for (int r = 0; r < R.nrows; r++) for (uint32_t s = R.begin(P, start, r), e = R.end(P, start, r); s < e; s++)
-struct PbfRows {
-  int z0, y0, ny;
-  uint32_t xa, xb;
-  int nrows;
-  __device__ __forceinline__ PbfRows(const PbfParams& P, uint32_t c) {
-    const int cx = (int)(c % P.nx);
-    const uint32_t t = c / P.nx;
-    const int cy = (int)(t % P.ny), cz = (int)(t / P.ny);
-    xa = (uint32_t)max(cx - 1, 0);
-    xb = (uint32_t)min(cx + 1, (int)P.nx - 1);
-    z0 = max(cz - 1, 0);
-    y0 = max(cy - 1, 0);
-    ny = min(cy + 1, (int)P.ny - 1) - y0 + 1;
-    nrows = (min(cz + 1, (int)P.nz - 1) - z0 + 1) * ny;
-  }
-  __device__ __forceinline__ uint32_t row(const PbfParams& P, int r) const {
-    const int z = z0 + r / ny, y = y0 + r % ny;
-    return P.nx * (uint32_t)(y + (int)P.ny * z);
-  }
-  __device__ __forceinline__ uint32_t begin(const PbfParams& P, const uint32_t* __restrict__ start, int r) const { return start[row(P, r) + xa]; }
-  __device__ __forceinline__ uint32_t end(const PbfParams& P, const uint32_t* __restrict__ start, int r) const { return start[row(P, r) + xb + 1u]; }
-};
+// Slots past the last one that the neighbour walk may read (and then ignores): the sorted-position arrays it walks are
+// allocated with them.
+constexpr uint32_t PBF_PAD = 8;
+// The candidates of a particle in cell c that may lie inside the kernel radius, handed to f in the loop order of lambda,
+// delta and viscosity (src/gpu.js:220-224): the 27-cell neighbourhood as 9 rows of three x-adjacent cells, which are
+// contiguous runs of the sorted slots, z outer, y inner, slots ascending. Two phases: the lane first tests every slot of
+// its rows in groups of eight (independent loads, a bit per slot at a fixed position) into 64-slot masks kept in shared
+// memory (PBF_ENT per thread), then walks all set bits of all masks in one loop, calling f for each. A warp thus runs
+// the per-neighbour work (square root, division) once per neighbour of its busiest lane over the whole neighbourhood,
+// instead of once per slot where any lane has a neighbour (about 45 of the 290 slots of a 27-cell neighbourhood are
+// within h); a lane whose masks fill the buffer walks them before it tests on. The test is a superset: the fused r2
+// stays within a few units of rounding of the unfused one and the bound is h2 (1 + 2^-20), so every slot that the
+// reference's loop does not skip reaches f (a NaN distance too). f makes that loop's own tests (the slot itself, the
+// unfused r2 against h2) before its sums, so every sum gets the same terms in the same order. Blocks of PBF_T threads.
+constexpr int PBF_ENT = 12;
+template <class F>
+__device__ __forceinline__ void pbfNear(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
+                                        V3 qi, F&& f) {
+  __shared__ uint32_t entBase[PBF_ENT][PBF_T];
+  __shared__ uint2 entMask[PBF_ENT][PBF_T];
+  const uint32_t tid = threadIdx.x;
+  int nent = 0;
+  auto walk = [&]() {
+    int j = 0;
+    unsigned long long m = 0ull;
+    uint32_t base = 0;
+    while (true) {
+      while (m == 0ull && j < nent) {
+        const uint2 mm = entMask[j][tid];
+        m = ((unsigned long long)mm.y << 32) | mm.x;
+        base = entBase[j][tid];
+        j++;
+      }
+      if (m == 0ull) break;
+      const uint32_t k = (uint32_t)__ffsll((long long)m) - 1u;
+      m &= m - 1ull;
+      f(base + k);
+    }
+    nent = 0;
+  };
+  const int cx = (int)(c % P.nx);
+  const uint32_t cq = c / P.nx;
+  const int cy = (int)(cq % P.ny), cz = (int)(cq / P.ny);
+  const uint32_t xa = (uint32_t)max(cx - 1, 0), xe = (uint32_t)min(cx + 1, (int)P.nx - 1) + 1u;
+  const int ya = max(cy - 1, 0), yb = min(cy + 1, (int)P.ny - 1), za = max(cz - 1, 0), zb = min(cz + 1, (int)P.nz - 1);
+  const float lim = P.h2 * (1.0f + 1.0f / 1048576.0f);
+  for (int z = za; z <= zb; z++)
+    for (int y = ya; y <= yb; y++) {
+      const uint32_t row = P.nx * (uint32_t)(y + (int)P.ny * z);
+      const uint32_t e = start[row + xe];
+      for (uint32_t s = start[row + xa]; s < e; s += 64u) {
+        const uint32_t n = min(e - s, 64u);
+        unsigned long long m = 0ull;
+        for (uint32_t g = 0; g < n; g += 8u) {
+          uint32_t gm = 0;
+#pragma unroll
+          for (uint32_t k = 0; k < 8u; k++) {
+            const float4 x = xs[s + g + k];
+            const float dx = qi.x - x.x, dy = qi.y - x.y, dz = qi.z - x.z;
+            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+            if (!(r2 >= lim)) gm |= 1u << k;
+          }
+          m |= (unsigned long long)gm << g;
+        }
+        if (n < 64u) m &= (1ull << n) - 1ull;
+        if (m == 0ull) continue;
+        entBase[nent][tid] = s;
+        entMask[nent][tid] = make_uint2((uint32_t)m, (uint32_t)(m >> 32));
+        if (++nent == PBF_ENT) walk();
+      }
+    }
+  walk();
+}
 
 // ---- the grid of one step: count (warp-aggregated atomics), scan, scatter, canonical order ----
 // One particle per lane: its cell (or PBF_DEAD), and a provisional rank in the cell from the count's atomic.
@@ -137,23 +185,21 @@ __device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const float4* _
   const float irho = P.irho;
   float rho = P.W0, sg = 0.0f;
   V3 g = v3(0.0f, 0.0f, 0.0f);
-  const PbfRows R(P, c);
-  for (int rr = 0; rr < R.nrows; rr++)
-    for (uint32_t s = R.begin(P, start, rr), e = R.end(P, start, rr); s < e; s++) {
-      if (s == t) continue;
-      const V3 dd = qi - xyz(xs[s]);
-      const float r2 = dot3(dd, dd);
-      if (r2 >= P.h2) continue;
-      const float tt = P.h2 - r2;
-      rho += P.poly * tt * tt * tt;
-      const float r = sqrtf(r2);
-      if (r < 1e-7f) continue;
-      const float hr = P.h - r;
-      const float f = P.spiky * hr * hr / r * irho;
-      const V3 fv = dd * f;
-      g = g + fv;
-      sg += dot3(fv, fv);
-    }
+  pbfNear(P, xs, start, c, qi, [&](uint32_t s) {
+    if (s == t) return;
+    const V3 dd = qi - xyz(xs[s]);
+    const float r2 = dot3(dd, dd);
+    if (r2 >= P.h2) return;
+    const float tt = P.h2 - r2;
+    rho += P.poly * tt * tt * tt;
+    const float r = sqrtf(r2);
+    if (r < 1e-7f) return;
+    const float hr = P.h - r;
+    const float f = P.spiky * hr * hr / r * irho;
+    const V3 fv = dd * f;
+    g = g + fv;
+    sg += dot3(fv, fv);
+  });
   float br; V3 bg;
   pbfBnd(P, cols, sdf, qi, br, bg);
   rho += br;
@@ -170,20 +216,18 @@ __device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const float4* __re
   const V3 qi = xyz(xs[t]);
   const float irho = P.irho, li = lamS[t];
   V3 s = xyz(bgrS[t]) * li;
-  const PbfRows R(P, c);
-  for (int rr = 0; rr < R.nrows; rr++)
-    for (uint32_t q = R.begin(P, start, rr), e = R.end(P, start, rr); q < e; q++) {
-      if (q == t) continue;
-      const float sj = li + lamS[q];
-      if (sj == 0.0f) continue;
-      const V3 dd = qi - xyz(xs[q]);
-      const float r2 = dot3(dd, dd);
-      if (r2 >= P.h2) continue;
-      const float r = sqrtf(r2);
-      if (r < 1e-7f) continue;
-      const float hr = P.h - r;
-      s = s + dd * (P.spiky * hr * hr / r * irho * sj);
-    }
+  pbfNear(P, xs, start, c, qi, [&](uint32_t q) {
+    if (q == t) return;
+    const float sj = li + lamS[q];
+    if (sj == 0.0f) return;
+    const V3 dd = qi - xyz(xs[q]);
+    const float r2 = dot3(dd, dd);
+    if (r2 >= P.h2) return;
+    const float r = sqrtf(r2);
+    if (r < 1e-7f) return;
+    const float hr = P.h - r;
+    s = s + dd * (P.spiky * hr * hr / r * irho * sj);
+  });
   s = s * P.relax;
   const float m2 = dot3(s, s);
   if (m2 > P.maxD * P.maxD) s = s * (P.maxD * (1.0f / sqrtf(m2)));
