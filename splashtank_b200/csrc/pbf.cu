@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(PBF_T, 4) k_pbf_visc(const PbfParams* __restri
     const float irho = P.irho;
     V3 a = v3(0.0f, 0.0f, 0.0f);
     if (P.visc > 0.0f) {
-      pbfNear(P, posF, start, cellS[t], pi, [&](uint32_t s) {
+      pbfNear(P, posF, start, cellS[t], pi, [&](uint32_t s, float4 pfS) {
         if (s == t) return;
-        const V3 dd = pi - xyz(posF[s]);
+        const V3 dd = pi - xyz(pfS);
         const float r2 = dot3(dd, dd);
         if (r2 >= P.h2) return;
         const float tt = P.h2 - r2;

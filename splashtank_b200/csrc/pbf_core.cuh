@@ -101,7 +101,7 @@ constexpr uint32_t PBF_PAD = 8;
 // memory (PBF_ENT per thread), then walks all set bits of all masks in one loop, calling f for each. A warp thus runs
 // the per-neighbour work (square root, division) once per neighbour of its busiest lane over the whole neighbourhood,
 // instead of once per slot where any lane has a neighbour (about 45 of the 290 slots of a 27-cell neighbourhood are
-// within h); a lane whose masks fill the buffer walks them before it tests on. The test is a superset: the fused r2
+// within h); a lane whose masks fill the buffer walks them before it tests on. f gets the slot and its position. The test is a superset: the fused r2
 // stays within a few units of rounding of the unfused one and the bound is h2 (1 + 2^-20), so every slot that the
 // reference's loop does not skip reaches f (a NaN distance too). f makes that loop's own tests (the slot itself, the
 // unfused r2 against h2) before its sums, so every sum gets the same terms in the same order. Blocks of PBF_T threads.
@@ -113,21 +113,36 @@ __device__ __forceinline__ void pbfNear(const PbfParams& P, const float4* __rest
   __shared__ uint2 entMask[PBF_ENT][PBF_T];
   const uint32_t tid = threadIdx.x;
   int nent = 0;
+  // the bits of all masks in order; the next neighbour's position is loaded before f works on the current one
   auto walk = [&]() {
     int j = 0;
     unsigned long long m = 0ull;
     uint32_t base = 0;
-    while (true) {
+    auto next = [&](uint32_t& slot) {
       while (m == 0ull && j < nent) {
         const uint2 mm = entMask[j][tid];
         m = ((unsigned long long)mm.y << 32) | mm.x;
         base = entBase[j][tid];
         j++;
       }
-      if (m == 0ull) break;
-      const uint32_t k = (uint32_t)__ffsll((long long)m) - 1u;
+      if (m == 0ull) return false;
+      slot = base + (uint32_t)__ffsll((long long)m) - 1u;
       m &= m - 1ull;
-      f(base + k);
+      return true;
+    };
+    uint32_t cur;
+    if (next(cur)) {
+      float4 xc = xs[cur];
+      while (true) {
+        uint32_t nx;
+        const bool more = next(nx);
+        float4 xn;
+        if (more) xn = xs[nx];
+        f(cur, xc);
+        if (!more) break;
+        cur = nx;
+        xc = xn;
+      }
     }
     nent = 0;
   };
@@ -185,9 +200,9 @@ __device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const float4* _
   const float irho = P.irho;
   float rho = P.W0, sg = 0.0f;
   V3 g = v3(0.0f, 0.0f, 0.0f);
-  pbfNear(P, xs, start, c, qi, [&](uint32_t s) {
+  pbfNear(P, xs, start, c, qi, [&](uint32_t s, float4 xsS) {
     if (s == t) return;
-    const V3 dd = qi - xyz(xs[s]);
+    const V3 dd = qi - xyz(xsS);
     const float r2 = dot3(dd, dd);
     if (r2 >= P.h2) return;
     const float tt = P.h2 - r2;
@@ -216,11 +231,11 @@ __device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const float4* __re
   const V3 qi = xyz(xs[t]);
   const float irho = P.irho, li = lamS[t];
   V3 s = xyz(bgrS[t]) * li;
-  pbfNear(P, xs, start, c, qi, [&](uint32_t q) {
+  pbfNear(P, xs, start, c, qi, [&](uint32_t q, float4 xsQ) {
     if (q == t) return;
     const float sj = li + lamS[q];
     if (sj == 0.0f) return;
-    const V3 dd = qi - xyz(xs[q]);
+    const V3 dd = qi - xyz(xsQ);
     const float r2 = dot3(dd, dd);
     if (r2 >= P.h2) return;
     const float r = sqrtf(r2);
