@@ -29,11 +29,12 @@ sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # what limits each kernel instead of DRAM bandwidth, from ncu captures of the same kernels on the 128^3 wave tank
-NCU_LIMITER = {"g2p": "instruction issue: 59% issue active at 16 warps per SM, 1,318 instructions per particle",
-               "p2g": "shared-memory atomics: L1 pipe 84% busy, 3.2 wavefronts per atomic"}
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of the 128^3 wave tank (4,669,521 particles)
-NCU_TRAFFIC = {"g2p": {"bytes": 180631296 + 105086464, "particles": 4669521},
-               "p2g": {"bytes": 209715200 + 135951360, "particles": 4669521}}
+NCU_LIMITER = {"g2p": "instruction issue: 73% issue active at 24 warps per SM (80 registers), 1,370 instructions per particle",
+               "p2g": "shared-memory atomics: L1 pipe 74% busy, 3.1 wavefronts per atomic (two thirds bank-conflict replays)"}
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch in a one-pass ncu capture of the 256^3 wave tank itself
+# (the third step of `bench.py --steps 2 --warmup 1`, 37,847,049 live particles), scaled by the live particles
+NCU_TRAFFIC = {"g2p": {"bytes": 1554359040 + 1229789952, "particles": 37847049},
+               "p2g": {"bytes": 1720653824 + 1469603072, "particles": 37847049}}
 FALLBACK_HBM = 6650.0
 
 
@@ -181,7 +182,7 @@ def roofline(stage_ms, nsteps, n, cells, fluid, iters, peak, peak_src):
         return None
     per_launch_ms = stage_ms[dom] / (nsteps * launches)
     achieved = b / (per_launch_ms * 1e-3) / 1e9
-    # DRAM bytes of one launch from an ncu capture of a smaller tank, scaled by particles (traffic grows with them)
+    # DRAM bytes of one launch from an ncu capture of the same tank, scaled by the live particles of this run
     ent = NCU_TRAFFIC.get(dom)
     traffic = int(ent["bytes"] * n / ent["particles"]) if ent else None
     return {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
