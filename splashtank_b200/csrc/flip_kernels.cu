@@ -394,21 +394,28 @@ __global__ void __launch_bounds__(512) k_classify(Bufs B) {
     else if ((sb & 0xff00u) != 0u) ty = 2;
     else if (OCEAN && P.ocean != 0u && layerW(P, cx) >= 0.5f)   // the ocean's boundary: a wall moving with the waves
       ty = cx.y < oceanEta(P, B.waves, cx.x, cx.z) ? 2u : 0u;
-    else if (P.nb != 0u && phiOfBits(ct) < -1.0f &&
-             (phiOfBits(ct) < -P.band || len3(velGVec(P, B.velG, nc, cx)) < 9.0f * P.h)) ty = 1;
-    else if (n > 0) {
-      ty = 1;
-      if ((float)n < P.sheetMin) {
-        const int32_t dth = (int32_t)ceilf(0.6f * P.rest);
-        bool dense = false;
-        for (int q = 0; q < 6; q++) {
-          int qi = i, qj = j, qk = k;
-          if (q == 0) qi -= 1; else if (q == 1) qi += 1; else if (q == 2) qj -= 1; else if (q == 3) qj += 1; else if (q == 4) qk -= 1; else qk += 1;
-          if (!inDom(P, qi, qj, qk)) continue;
-          if (B.cnt[cellIdx(P, qi, qj, qk)] >= dth) dense = true;
+    else {
+      // fluid when the narrow band holds deep water here (deeper than the band, or calm) or when particles are here
+      // and the sheet does not tear. Either makes the cell fluid, so the particle test runs first: the calm test's 24
+      // kept-velocity loads are only needed for a cell that the particles leave air (in a full-depth band, few).
+      bool fl = false;
+      if (n > 0) {
+        fl = true;
+        if ((float)n < P.sheetMin) {
+          const int32_t dth = (int32_t)ceilf(0.6f * P.rest);
+          bool dense = false;
+          for (int q = 0; q < 6; q++) {
+            int qi = i, qj = j, qk = k;
+            if (q == 0) qi -= 1; else if (q == 1) qi += 1; else if (q == 2) qj -= 1; else if (q == 3) qj += 1; else if (q == 4) qk -= 1; else qk += 1;
+            if (!inDom(P, qi, qj, qk)) continue;
+            if (B.cnt[cellIdx(P, qi, qj, qk)] >= dth) dense = true;
+          }
+          fl = dense;
         }
-        if (!dense) ty = 0;
       }
+      if (!fl && P.nb != 0u && phiOfBits(ct) < -1.0f &&
+          (phiOfBits(ct) < -P.band || len3(velGVec(P, B.velG, nc, cx)) < 9.0f * P.h)) fl = true;
+      ty = fl ? 1u : 0u;
     }
     B.ctype[c] = ty | sb;
     if (ty != 1u) B.pres[c] = 0.0f;
