@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(PBF_T) k_pbf_scatter(const PbfParams* __restri
 // position (x: float4 records `stride` float4 apart) goes to the sorted copy
 __global__ void __launch_bounds__(PBF_T) k_pbf_order(const PbfParams* __restrict__ Pg, const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ key,
                                                      const uint32_t* __restrict__ start, const float4* __restrict__ x, uint32_t stride,
-                                                     uint32_t* __restrict__ sidx, uint32_t* __restrict__ cellS, float4* __restrict__ xs) {
+                                                     uint32_t* __restrict__ sidx, uint32_t* __restrict__ cellS, PbfPos xs) {
   const uint32_t nLive = start[Pg->ncell];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nLive; t += gridDim.x * blockDim.x) {
     const uint32_t i = tmp[t], c = key[i];
@@ -73,11 +73,11 @@ __global__ void __launch_bounds__(PBF_T) k_pbf_order(const PbfParams* __restrict
     const float4 q = x[(size_t)i * stride];
     sidx[a + r] = i;
     cellS[a + r] = c;
-    xs[a + r] = make_float4(q.x, q.y, q.z, 0.0f);
+    pbfPut(xs, a + r, q.x, q.y, q.z);
   }
 }
 
-__global__ void __launch_bounds__(PBF_T, 4) k_pbf_lambda(const PbfParams* __restrict__ Pg, const float4* __restrict__ xs, const uint32_t* __restrict__ cellS,
+__global__ void __launch_bounds__(PBF_T, 4) k_pbf_lambda(const PbfParams* __restrict__ Pg, const PbfPos xs, const uint32_t* __restrict__ cellS,
                                                       const uint32_t* __restrict__ start, const float4* __restrict__ cols, const float* __restrict__ sdf,
                                                       float* __restrict__ lamS, float4* __restrict__ bgrS) {
   __shared__ PbfParams P;
@@ -125,23 +125,23 @@ __global__ void __launch_bounds__(PBF_T) k_pbf_predict(const PbfParams* __restri
   }
 }
 // delta (src/gpu.js:253-286) + applyDelta (:288-292): the corrected, collided position into the other buffer
-__global__ void __launch_bounds__(PBF_T, 4) k_pbf_delta(const PbfParams* __restrict__ Pg, const float4* __restrict__ xs, const uint32_t* __restrict__ cellS,
+__global__ void __launch_bounds__(PBF_T, 4) k_pbf_delta(const PbfParams* __restrict__ Pg, const PbfPos xs, const uint32_t* __restrict__ cellS,
                                                      const uint32_t* __restrict__ start, const float* __restrict__ lamS, const float4* __restrict__ bgrS,
-                                                     const float4* __restrict__ cols, const float* __restrict__ sdf, float4* __restrict__ xsOut) {
+                                                     const float4* __restrict__ cols, const float* __restrict__ sdf, const PbfPos xsOut) {
   __shared__ PbfParams P;
   loadPbf(P, Pg);
   const uint32_t nLive = start[P.ncell];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nLive; t += gridDim.x * blockDim.x) {
     const V3 s = pbfDeltaOne(P, xs, start, cellS[t], t, lamS, bgrS);
-    const V3 q = pbfCollide(P, cols, sdf, xyz(xs[t]) + s);
-    xsOut[t] = make_float4(q.x, q.y, q.z, 0.0f);
+    const V3 q = pbfCollide(P, cols, sdf, xyz(xs.v[t]) + s);
+    pbfPut(xsOut, t, q.x, q.y, q.z);
   }
 }
 // finalize (src/gpu.js:293-322) in sorted space: the velocity of the move, restitution where the boundary pushes,
 // the speed limit of 12, and open faces; the result goes to the sorted final positions and velocities
 __global__ void __launch_bounds__(PBF_T) k_pbf_finalize(const PbfParams* __restrict__ Pg, const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                         const uint32_t* __restrict__ sidx, const float4* __restrict__ xs, const float4* __restrict__ bgrS,
-                                                        const uint32_t* __restrict__ start, float4* __restrict__ posF, float4* __restrict__ vel2S) {
+                                                        const uint32_t* __restrict__ start, const PbfPos posF, float4* __restrict__ vel2S) {
   __shared__ PbfParams P;
   loadPbf(P, Pg);
   const uint32_t nLive = start[P.ncell];
@@ -165,10 +165,10 @@ __global__ void __launch_bounds__(PBF_T) k_pbf_finalize(const PbfParams* __restr
     const uint32_t o = P.open;
     if (o != 0u && (((o & 1u) && q.x < P.bx0) || ((o & 2u) && q.x > P.bx1) || ((o & 4u) && q.y < P.by0) || ((o & 8u) && q.y > P.by1) ||
                     ((o & 16u) && q.z < P.bz0) || ((o & 32u) && q.z > P.bz1))) {
-      posF[t] = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
+      pbfPut(posF, t, 0.0f, -1.0e6f, 0.0f);
       vel2S[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     } else {
-      posF[t] = make_float4(q.x, q.y, q.z, 0.0f);
+      pbfPut(posF, t, q.x, q.y, q.z);
       vel2S[t] = make_float4(v.x, v.y, v.z, 0.0f);
     }
   }
@@ -176,14 +176,14 @@ __global__ void __launch_bounds__(PBF_T) k_pbf_finalize(const PbfParams* __restr
 // viscosity (src/gpu.js:323-353): XSPH over the neighbours found through the step's grid, at the final positions;
 // written back to index order with the speed in pos.w
 __global__ void __launch_bounds__(PBF_T, 4) k_pbf_visc(const PbfParams* __restrict__ Pg, const uint32_t* __restrict__ sidx, const uint32_t* __restrict__ cellS,
-                                                    const uint32_t* __restrict__ start, const float4* __restrict__ posF, const float4* __restrict__ vel2S,
+                                                    const uint32_t* __restrict__ start, const PbfPos posF, const float4* __restrict__ vel2S,
                                                     float4* __restrict__ pos, float4* __restrict__ vel) {
   __shared__ PbfParams P;
   loadPbf(P, Pg);
   const uint32_t nLive = start[P.ncell];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nLive; t += gridDim.x * blockDim.x) {
     const uint32_t i = sidx[t];
-    const float4 pf = posF[t];
+    const float4 pf = posF.v[t];
     if (pf.y < DEADY) {
       pos[i] = pf;
       vel[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -229,9 +229,9 @@ __global__ void __launch_bounds__(PBF_T) k_fpbf_count(const PbfParams* __restric
   }
 }
 // delta + the FLIP step's collideP (src/flip/wgsl-solver.js:185-197) as the projection after each correction
-__global__ void __launch_bounds__(PBF_T, 4) k_fpbf_delta(const PbfParams* __restrict__ Pg, Bufs B, const float4* __restrict__ xs, const uint32_t* __restrict__ cellS,
+__global__ void __launch_bounds__(PBF_T, 4) k_fpbf_delta(const PbfParams* __restrict__ Pg, Bufs B, const PbfPos xs, const uint32_t* __restrict__ cellS,
                                                       const uint32_t* __restrict__ start, const float* __restrict__ lamS, const float4* __restrict__ bgrS,
-                                                      float4* __restrict__ xsOut) {
+                                                      const PbfPos xsOut) {
   __shared__ FlipParams FP;
   loadParams(FP, B.P);
   __shared__ PbfParams P;
@@ -239,8 +239,8 @@ __global__ void __launch_bounds__(PBF_T, 4) k_fpbf_delta(const PbfParams* __rest
   const uint32_t nLive = start[P.ncell];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nLive; t += gridDim.x * blockDim.x) {
     const V3 s = pbfDeltaOne(P, xs, start, cellS[t], t, lamS, bgrS);
-    const V3 q = collideP(FP, B.cols, B.sdf, xyz(xs[t]) + s);
-    xsOut[t] = make_float4(q.x, q.y, q.z, 0.0f);
+    const V3 q = collideP(FP, B.cols, B.sdf, xyz(xs.v[t]) + s);
+    pbfPut(xsOut, t, q.x, q.y, q.z);
   }
 }
 // back to the FLIP particles: position q, velocity v + (q - p) / dt, pos.w from the new speed and the foam level (the
@@ -285,7 +285,7 @@ int launch_flip_pbf(const Bufs& B, const PbfDev& D, int iters, int grid, cudaStr
     cur ^= 1;
     nl += 2;
   }
-  k_fpbf_write<<<grid, PBF_T, 0, s>>>(D.P, D.sidx, D.xs[cur], D.start, B.pa);
+  k_fpbf_write<<<grid, PBF_T, 0, s>>>(D.P, D.sidx, D.xs[cur].v, D.start, B.pa);
   return nl + 1;
 }
 
@@ -352,6 +352,24 @@ PbfParams pbf_params(const PbfHostConsts& c, double d, const double lo[3], const
   return P;
 }
 
+// a sorted-position buffer of n slots (and PBF_PAD more) in one allocation: the float4 records, then x, y and z, each
+// array an even number of floats long so every even slot starts an aligned pair
+static size_t pbf_pos_slots(size_t n) { return (n + PBF_PAD + 1) & ~(size_t)1; }
+static cudaError_t pbf_pos_alloc(PbfPos& b, size_t n) {
+  const size_t np = pbf_pos_slots(n);
+  char* m = nullptr;
+  const cudaError_t e = cudaMalloc((void**)&m, np * 28);
+  if (e != cudaSuccess) return e;
+  b.v = reinterpret_cast<float4*>(m);
+  b.x = reinterpret_cast<float*>(m + np * 16);
+  b.y = b.x + np;
+  b.z = b.y + np;
+  return cudaSuccess;
+}
+static void pbf_pos_free(PbfPos& b) {
+  if (b.v) cudaFree(b.v);
+  b = PbfPos{};
+}
 cudaError_t pbf_dev_alloc(PbfDev& D, uint32_t maxN, uint32_t ncell) {
   D.ncell = ncell;
   const uint32_t nb = (ncell + PBF_SCAN - 1) / PBF_SCAN;
@@ -360,19 +378,22 @@ cudaError_t pbf_dev_alloc(PbfDev& D, uint32_t maxN, uint32_t ncell) {
   const size_t N = std::max<uint32_t>(maxN, 1);
   A((void**)&D.P, sizeof(PbfParams));
   A((void**)&D.key, N * 4); A((void**)&D.rank, N * 4); A((void**)&D.tmp, N * 4); A((void**)&D.sidx, N * 4); A((void**)&D.cellS, N * 4);
-  A((void**)&D.xs[0], (N + PBF_PAD) * 16); A((void**)&D.xs[1], (N + PBF_PAD) * 16); A((void**)&D.bgrS, N * 16); A((void**)&D.lamS, N * 4);
+  for (PbfPos& b : D.xs)
+    if (e == cudaSuccess) e = pbf_pos_alloc(b, N);
+  A((void**)&D.bgrS, N * 16); A((void**)&D.lamS, N * 4);
   A((void**)&D.cnt, (size_t)ncell * 4); A((void**)&D.start, ((size_t)ncell + 1) * 4); A((void**)&D.bsum, ((size_t)nb + 1) * 4);
   return e;
 }
 void pbf_dev_free(PbfDev& D) {
-  void* ps[] = {D.P, D.key, D.rank, D.tmp, D.sidx, D.cellS, D.xs[0], D.xs[1], D.bgrS, D.lamS, D.cnt, D.start, D.bsum};
+  for (PbfPos& b : D.xs) pbf_pos_free(b);
+  void* ps[] = {D.P, D.key, D.rank, D.tmp, D.sidx, D.cellS, D.bgrS, D.lamS, D.cnt, D.start, D.bsum};
   for (void* p : ps)
     if (p) cudaFree(p);
   D = PbfDev{};
 }
 size_t pbf_dev_bytes(uint32_t maxN, uint32_t ncell) {
   const size_t N = std::max<uint32_t>(maxN, 1);
-  return N * (5 * 4 + 3 * 16 + 4) + 2 * PBF_PAD * 16 + (size_t)ncell * 8 + ((size_t)ncell / PBF_SCAN + 2) * 4 + sizeof(PbfParams);
+  return N * (5 * 4 + 16 + 4) + 2 * pbf_pos_slots(N) * 28 + (size_t)ncell * 8 + ((size_t)ncell / PBF_SCAN + 2) * 4 + sizeof(PbfParams);
 }
 
 }  // namespace st
@@ -388,7 +409,8 @@ struct st_pbf {
   PbfHostConsts c{};
   uint32_t open = 0, maxN = 0, cap = 0, N = 0, ring = 0, ncell = 0;
   bool recycle = true;
-  float4 *pos = nullptr, *vel = nullptr, *prd = nullptr, *posF = nullptr, *vel2S = nullptr;
+  float4 *pos = nullptr, *vel = nullptr, *prd = nullptr, *vel2S = nullptr;
+  PbfPos posF{};             // the final sorted positions, walked by the viscosity pass
   PbfDev D{};
   float4* cols = nullptr;    // 8 float4 per collider (packColliders, src/gpu.js:57-67)
   float* sdf = nullptr;
@@ -405,7 +427,8 @@ void st_pbf_destroy(st_pbf* s) {
   if (!s) return;
   cudaSetDevice(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
-  void* ps[] = {s->pos, s->vel, s->prd, s->posF, s->vel2S, s->cols, s->sdf};
+  pbf_pos_free(s->posF);
+  void* ps[] = {s->pos, s->vel, s->prd, s->vel2S, s->cols, s->sdf};
   for (void* p : ps)
     if (p) cudaFree(p);
   pbf_dev_free(s->D);
@@ -441,8 +464,9 @@ st_status st_pbf_create(const st_pbf_desc* ds, st_pbf** out) {
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
   const size_t N = s->maxN;
-  for (float4** p : {&s->pos, &s->vel, &s->prd, &s->posF, &s->vel2S})   // posF is walked by the viscosity pass: padded
-    if ((e = cudaMalloc((void**)p, (p == &s->posF ? N + PBF_PAD : N) * 16)) != cudaSuccess) return fail("particles", e);
+  for (float4** p : {&s->pos, &s->vel, &s->prd, &s->vel2S})
+    if ((e = cudaMalloc((void**)p, N * 16)) != cudaSuccess) return fail("particles", e);
+  if ((e = pbf_pos_alloc(s->posF, N)) != cudaSuccess) return fail("particles", e);
   if ((e = cudaMemsetAsync(s->pos, 0, N * 16, s->stream)) != cudaSuccess) return fail("memset", e);
   if ((e = cudaMemsetAsync(s->vel, 0, N * 16, s->stream)) != cudaSuccess) return fail("memset", e);
   if ((e = pbf_dev_alloc(s->D, s->maxN, s->ncell)) != cudaSuccess) return fail("solver buffers", e);
@@ -578,7 +602,7 @@ st_status st_pbf_step(st_pbf* s, double dt, const st_pbf_opts* o) {
     k_pbf_delta<<<grid, PBF_T, 0, q>>>(s->D.P, s->D.xs[cur], s->D.cellS, s->D.start, s->D.lamS, s->D.bgrS, s->cols, s->sdf, s->D.xs[cur ^ 1]);
     cur ^= 1;
   }
-  k_pbf_finalize<<<grid, PBF_T, 0, q>>>(s->D.P, s->pos, s->vel, s->D.sidx, s->D.xs[cur], s->D.bgrS, s->D.start, s->posF, s->vel2S);
+  k_pbf_finalize<<<grid, PBF_T, 0, q>>>(s->D.P, s->pos, s->vel, s->D.sidx, s->D.xs[cur].v, s->D.bgrS, s->D.start, s->posF, s->vel2S);
   k_pbf_visc<<<grid, PBF_T, 0, q>>>(s->D.P, s->D.sidx, s->D.cellS, s->D.start, s->posF, s->vel2S, s->pos, s->vel);
   PK(cudaGetLastError());
   return ST_OK;

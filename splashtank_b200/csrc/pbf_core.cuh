@@ -94,21 +94,34 @@ __device__ __forceinline__ uint32_t pbfCellOf(const PbfParams& P, V3 p) {
 // Slots past the last one that the neighbour walk may read (and then ignores): the sorted-position arrays it walks are
 // allocated with them.
 constexpr uint32_t PBF_PAD = 8;
+// A buffer of sorted positions: float4 records (each neighbour's own read and every other pass) and the same positions
+// split into x, y and z arrays (the neighbour walk's test reads two slots per 8-byte load). Each holds PBF_PAD more slots.
+struct PbfPos {
+  float4* v;
+  float *x, *y, *z;
+};
+__device__ __forceinline__ void pbfPut(const PbfPos& b, uint32_t t, float qx, float qy, float qz) {
+  b.v[t] = make_float4(qx, qy, qz, 0.0f);
+  b.x[t] = qx;
+  b.y[t] = qy;
+  b.z[t] = qz;
+}
 // The candidates of a particle in cell c that may lie inside the kernel radius, handed to f in the loop order of lambda,
 // delta and viscosity (src/gpu.js:220-224): the 27-cell neighbourhood as 9 rows of three x-adjacent cells, which are
 // contiguous runs of the sorted slots, z outer, y inner, slots ascending. Two phases: the lane first tests every slot of
-// its rows in groups of eight (independent loads, a bit per slot at a fixed position) into 64-slot masks kept in shared
-// memory (PBF_ENT per thread), then walks all set bits of all masks in one loop, calling f for each. A warp thus runs
-// the per-neighbour work (square root, division) once per neighbour of its busiest lane over the whole neighbourhood,
+// its rows (two slots per paired f32 operation on the split x, y, z arrays, in groups of eight with a bit per slot at a
+// fixed position) into 64-slot masks kept in shared memory (PBF_ENT per thread), then walks all set bits of all masks
+// in one loop, calling f with the slot and its position (loaded one neighbour ahead). A warp thus runs the
+// per-neighbour work (square root, division) once per neighbour of its busiest lane over the whole neighbourhood,
 // instead of once per slot where any lane has a neighbour (about 45 of the 290 slots of a 27-cell neighbourhood are
-// within h); a lane whose masks fill the buffer walks them before it tests on. f gets the slot and its position. The test is a superset: the fused r2
+// within h); a lane whose masks fill the buffer walks them before it tests on. The test is a superset: its fused r2
 // stays within a few units of rounding of the unfused one and the bound is h2 (1 + 2^-20), so every slot that the
 // reference's loop does not skip reaches f (a NaN distance too). f makes that loop's own tests (the slot itself, the
 // unfused r2 against h2) before its sums, so every sum gets the same terms in the same order. Blocks of PBF_T threads.
 constexpr int PBF_ENT = 12;
 template <class F>
-__device__ __forceinline__ void pbfNear(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
-                                        V3 qi, F&& f) {
+__device__ __forceinline__ void pbfNear(const PbfParams& P, const PbfPos& xs, const uint32_t* __restrict__ start, uint32_t c, V3 qi,
+                                        F&& f) {
   __shared__ uint32_t entBase[PBF_ENT][PBF_T];
   __shared__ uint2 entMask[PBF_ENT][PBF_T];
   const uint32_t tid = threadIdx.x;
@@ -132,12 +145,12 @@ __device__ __forceinline__ void pbfNear(const PbfParams& P, const float4* __rest
     };
     uint32_t cur;
     if (next(cur)) {
-      float4 xc = xs[cur];
+      float4 xc = xs.v[cur];
       while (true) {
         uint32_t nx;
         const bool more = next(nx);
         float4 xn;
-        if (more) xn = xs[nx];
+        if (more) xn = xs.v[nx];
         f(cur, xc);
         if (!more) break;
         cur = nx;
@@ -152,25 +165,35 @@ __device__ __forceinline__ void pbfNear(const PbfParams& P, const float4* __rest
   const uint32_t xa = (uint32_t)max(cx - 1, 0), xe = (uint32_t)min(cx + 1, (int)P.nx - 1) + 1u;
   const int ya = max(cy - 1, 0), yb = min(cy + 1, (int)P.ny - 1), za = max(cz - 1, 0), zb = min(cz + 1, (int)P.nz - 1);
   const float lim = P.h2 * (1.0f + 1.0f / 1048576.0f);
+  const float2 nqx = make_float2(-qi.x, -qi.x), nqy = make_float2(-qi.y, -qi.y), nqz = make_float2(-qi.z, -qi.z);
+  const float* __restrict__ sx = xs.x;
+  const float* __restrict__ sy = xs.y;
+  const float* __restrict__ sz = xs.z;
   for (int z = za; z <= zb; z++)
     for (int y = ya; y <= yb; y++) {
       const uint32_t row = P.nx * (uint32_t)(y + (int)P.ny * z);
-      const uint32_t e = start[row + xe];
-      for (uint32_t s = start[row + xa]; s < e; s += 64u) {
+      const uint32_t sb = start[row + xa], e = start[row + xe];
+      // runs start at even slots, so each pair of slots is one aligned 8-byte load per axis (paired f32 arithmetic);
+      // a slot before the row's start is masked off below
+      for (uint32_t s = sb & ~1u; s < e; s += 64u) {
         const uint32_t n = min(e - s, 64u);
         unsigned long long m = 0ull;
         for (uint32_t g = 0; g < n; g += 8u) {
           uint32_t gm = 0;
 #pragma unroll
-          for (uint32_t k = 0; k < 8u; k++) {
-            const float4 x = xs[s + g + k];
-            const float dx = qi.x - x.x, dy = qi.y - x.y, dz = qi.z - x.z;
-            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
-            if (!(r2 >= lim)) gm |= 1u << k;
+          for (uint32_t k = 0; k < 8u; k += 2u) {
+            const uint32_t i = s + g + k;
+            const float2 dx = __fadd2_rn(*reinterpret_cast<const float2*>(sx + i), nqx);
+            const float2 dy = __fadd2_rn(*reinterpret_cast<const float2*>(sy + i), nqy);
+            const float2 dz = __fadd2_rn(*reinterpret_cast<const float2*>(sz + i), nqz);
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            if (!(r2.x >= lim)) gm |= 1u << k;
+            if (!(r2.y >= lim)) gm |= 2u << k;
           }
           m |= (unsigned long long)gm << g;
         }
         if (n < 64u) m &= (1ull << n) - 1ull;
+        if (s < sb) m &= ~1ull;
         if (m == 0ull) continue;
         entBase[nent][tid] = s;
         entMask[nent][tid] = make_uint2((uint32_t)m, (uint32_t)(m >> 32));
@@ -194,9 +217,9 @@ __device__ __forceinline__ void pbfCount(uint32_t key, bool valid, uint32_t* __r
 }
 // ---- one solver iteration in sorted space ----
 // lambda (src/gpu.js:208-251) for sorted slot t
-__device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
+__device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const PbfPos& xs, const uint32_t* __restrict__ start, uint32_t c,
                                              uint32_t t, const float4* __restrict__ cols, const float* __restrict__ sdf, float& lam, V3& bgr) {
-  const V3 qi = xyz(xs[t]);
+  const V3 qi = xyz(xs.v[t]);
   const float irho = P.irho;
   float rho = P.W0, sg = 0.0f;
   V3 g = v3(0.0f, 0.0f, 0.0f);
@@ -226,9 +249,9 @@ __device__ __forceinline__ void pbfLambdaOne(const PbfParams& P, const float4* _
   lam = C > 0.0f ? -C / (sg + dot3(g, g) + P.eps) : 0.0f;
 }
 // delta (src/gpu.js:253-286) for sorted slot t: the clamped correction
-__device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t c,
+__device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const PbfPos& xs, const uint32_t* __restrict__ start, uint32_t c,
                                           uint32_t t, const float* __restrict__ lamS, const float4* __restrict__ bgrS) {
-  const V3 qi = xyz(xs[t]);
+  const V3 qi = xyz(xs.v[t]);
   const float irho = P.irho, li = lamS[t];
   V3 s = xyz(bgrS[t]) * li;
   pbfNear(P, xs, start, c, qi, [&](uint32_t q, float4 xsQ) {
@@ -253,7 +276,7 @@ __device__ __forceinline__ V3 pbfDeltaOne(const PbfParams& P, const float4* __re
 struct PbfDev {
   PbfParams* P = nullptr;                   // the uniform block, uploaded each step
   uint32_t *key = nullptr, *rank = nullptr, *tmp = nullptr, *sidx = nullptr, *cellS = nullptr;   // per particle / slot
-  float4* xs[2] = {nullptr, nullptr};       // sorted positions, two iteration buffers
+  PbfPos xs[2] = {};                        // sorted positions, two iteration buffers
   float4* bgrS = nullptr;                   // boundary gradient / rho0 per slot
   float* lamS = nullptr;                    // lambda per slot
   uint32_t *cnt = nullptr, *start = nullptr, *bsum = nullptr;   // per cell; scan blocks
