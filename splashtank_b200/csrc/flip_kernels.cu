@@ -778,7 +778,7 @@ __device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, cons
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
   const float2* v;   // [3][1000]: (vn, vo) of each face, one 64-bit load per corner
-  const float* csum;     // [9][9][9]: g2p's summed counts of the 2 x 2 x 2 cells from (ox - 1, oy - 1, oz - 1) + (x, y, z)
+  const float4* foam;    // [9][9][9]: foamCell of the summed counts of the 2 x 2 x 2 cells from (ox - 1, oy - 1, oz - 1) + (x, y, z)
   const int32_t* cnt;
   const float* wet;      // wetCellAt of each window cell (0 outside the domain)
   const uint8_t* kill;   // the narrow band's trim test of each window cell
@@ -886,6 +886,20 @@ struct G2PUni {
 __device__ __forceinline__ G2PUni g2pUni(const FlipParams& P) {
   return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f};
 }
+// The terms of g2p's particle update that depend only on the local density rho = csum / (8 rest) of the particle's
+// 2 x 2 x 2 count sum (wgsl-solver.js:222-240): air, the foam decay exp(-dt / tau), the drag factor
+// 1 - exp(-kd dt) and shield, in the reference's operations. In the default mode every particle of a tile takes its
+// count sum from one of 729 corner cells, so g2p evaluates them once per corner cell into a shared-memory table instead
+// of once per particle (two exp and five divisions).
+__device__ __forceinline__ float4 foamCell(const FlipParams& P, const G2PUni& U, float csum) {
+  const float rho = csum / (8.0f * P.rest);
+  const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
+  const float shield = smoothstepf(0.1f, 0.65f, rho);
+  const float exposure = 1.0f - 0.97f * shield;
+  const float tau = U.tau0 * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
+  const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
+  return make_float4(air, st_expf(-P.dt / tau), 1.0f - st_expf(-kd * P.dt), shield);
+}
 template <bool OCEAN>
 __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q) {
   const V3 p = xyz(q.p), v0 = xyz(q.v);
@@ -903,20 +917,18 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   }
   const V3 bcf = vfloor((p - v3(P.x0, P.y0, P.z0)) * P.ih - v3(0.5f, 0.5f, 0.5f));
   const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
-  float csum = 8.0f * P.rest;
   const bool fast = P.q12 > 0.5f;
-  if (P.q9 < 0.5f && fast) csum = 8.0f * (float)W.cnt[W.idx(fi, fj, fk)];
-  else if (P.q9 < 0.5f) {
+  float4 fc;
+  if (P.q9 < 0.5f && !fast) {
     // the sum depends on the corner only through its clamp into [-1, n - 1], which the tile's particles keep within
     // the staged 9^3 block (the outer clamp only keeps the shared-memory index in bounds)
     const int x = clampi(clampi(bi, -1, (int)P.nx - 1) - (W.ox - 1), 0, 8), y = clampi(clampi(bj, -1, (int)P.ny - 1) - (W.oy - 1), 0, 8);
     const int z = clampi(clampi(bk, -1, (int)P.nz - 1) - (W.oz - 1), 0, 8);
-    csum = W.csum[x + 9 * (y + 9 * z)];
+    fc = W.foam[x + 9 * (y + 9 * z)];
+  } else {
+    fc = foamCell(P, U, P.q9 < 0.5f ? 8.0f * (float)W.cnt[W.idx(fi, fj, fk)] : 8.0f * P.rest);
   }
-  const float rho = csum / (8.0f * P.rest);
-  const float air = 1.0f - smoothstepf(0.008f, 0.1f, rho);
-  const float shield = smoothstepf(0.1f, 0.65f, rho);
-  const float exposure = 1.0f - 0.97f * shield;
+  const float air = fc.x, shield = fc.w;
   const float spd0 = len3(v);
   const float sens = U.sens;
   const float pacc = len3(vn - vo) / P.dt;
@@ -924,8 +936,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
   const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
   const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
-  const float tau = U.tau0 * mixf(1.0f, 0.35f, smoothstepf(0.7f, 1.0f, rho)) * mixf(1.0f, 2.5f, air);
-  float foam = q.v.w * st_expf(-P.dt / tau);
+  float foam = q.v.w * fc.y;
   foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
   if (OCEAN && P.ocean != 0u) foam *= 1.0f - clampf(layerW(P, p) * 2.0f, 0.0f, 1.0f);   // easing into the waves is not churning
   V3 gust = v3(0.0f, 0.0f, 0.0f);
@@ -934,9 +945,8 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     const float tt = U.tt;
     gust = gustAt(T, gp, tt) * 2.0f - v3(1.0f, 1.0f, 1.0f);
   }
-  const float kd = P.q4 * (0.04f + 1.5f * exposure * exposure);
   const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
-  v = v + (airv - v) * (1.0f - st_expf(-kd * P.dt));
+  v = v + (airv - v) * fc.z;
   const float sp = len3(v);
   if (sp > P.vmax) v = v * (P.vmax / sp);
   const V3 pt = p + v * P.dt;
@@ -965,7 +975,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
-  __shared__ float wcsum[729];
+  extern __shared__ __align__(16) float4 wfoam[];   // 729 entries (dynamic: the static arrays fill the 48 KB limit)
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
   __shared__ ColPre cpre[32];
@@ -978,7 +988,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wv, wcsum, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wv, wfoam, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
     const G2PUni U = g2pUni(P);
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
@@ -996,7 +1006,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
     }
     __syncthreads();
     // the local density's count sums (g2p's foam terms, wgsl-solver.js:222-229) of every corner a particle of this tile
-    // can have: integer-valued floats, so the sum is exact in any order
+    // can have (integer-valued floats, so the sum is exact in any order), and the terms that follow from each
     if (P.q9 < 0.5f && !(P.q12 > 0.5f)) {
       for (int r = threadIdx.x; r < 729; r += G2P_T) {
         const int bi = W.ox - 1 + r % 9, bj = W.oy - 1 + (r / 9) % 9, bk = W.oz - 1 + r / 81;
@@ -1007,7 +1017,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
         for (int dz = 0; dz <= 1; dz++)
           for (int dy = 0; dy <= 1; dy++)
             for (int dx = 0; dx <= 1; dx++) cs += (float)wcnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
-        wcsum[r] = cs;
+        wfoam[r] = foamCell(P, U, cs);
       }
       __syncthreads();
     }
@@ -1179,8 +1189,14 @@ cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, 
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
-  if (ocean) k_g2p<true><<<grid, G2P_T, 0, s>>>(B);
-  else k_g2p<false><<<grid, G2P_T, 0, s>>>(B);
+  const int dyn = 729 * (int)sizeof(float4);
+  if (ocean) {
+    cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    k_g2p<true><<<grid, G2P_T, dyn, s>>>(B);
+  } else {
+    cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    k_g2p<false><<<grid, G2P_T, dyn, s>>>(B);
+  }
   return 1;
 }
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {
