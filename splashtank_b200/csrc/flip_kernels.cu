@@ -881,10 +881,12 @@ __device__ __noinline__ V3 gustAt(const GustTab& T, V3 gp, float tt) {
 }
 // values of the particle update that depend only on the parameters, computed once per thread
 struct G2PUni {
-  float sens, settle, tau0, tt;
+  float sens, settle, tau0, tt, v2lo;
 };
 __device__ __forceinline__ G2PUni g2pUni(const FlipParams& P) {
-  return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f};
+  // v2lo: below it |v|^2 cannot round to a speed above vmax (vmax^2 (1 - 2^-20) leaves room for both roundings)
+  return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f,
+                P.vmax * P.vmax * (1.0f - 1.0f / 1048576.0f)};
 }
 // The terms of g2p's particle update that depend only on the local density rho = csum / (8 rest) of the particle's
 // 2 x 2 x 2 count sum (wgsl-solver.js:222-240): air, the foam decay exp(-dt / tau), the drag factor
@@ -947,8 +949,11 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   }
   const V3 airv = v3(P.q1, P.q2, P.q3) + gust * P.q7;
   v = v + (airv - v) * fc.z;
-  const float sp = len3(v);
-  if (sp > P.vmax) v = v * (P.vmax / sp);
+  const float sp2 = dot3(v, v);
+  if (!(sp2 < U.v2lo)) {   // the speed limit; the common slow particle skips its square root
+    const float sp = sqrtf(sp2);
+    if (sp > P.vmax) v = v * (P.vmax / sp);
+  }
   const V3 pt = p + v * P.dt;
   const V3 pc = collidePB(P, B, W.cpre, pt);
   const V3 dsp = pc - pt;
