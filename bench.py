@@ -29,12 +29,12 @@ sys.path.insert(0, ROOT)
 
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # what limits each kernel instead of DRAM bandwidth, from ncu captures of the same kernels on the 128^3 wave tank
-NCU_LIMITER = {"g2p": "instruction issue: 73% issue active at 24 warps per SM (80 registers), 1,370 instructions per particle",
+NCU_LIMITER = {"g2p": "instruction issue: 72% issue active at 24 warps per SM (80 registers), 1,216 instructions per particle",
                "p2g": "shared-memory atomics: L1 pipe 74% busy, 3.1 wavefronts per atomic (two thirds bank-conflict replays)"}
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch in a one-pass ncu capture of the 256^3 wave tank itself
 # (the third step of `bench.py --steps 2 --warmup 1`, 37,847,049 live particles), scaled by the live particles
-NCU_TRAFFIC = {"g2p": {"bytes": 1554359040 + 1229789952, "particles": 37847049},
-               "p2g": {"bytes": 1720653824 + 1469603072, "particles": 37847049}}
+NCU_TRAFFIC = {"g2p": {"bytes": 1558394880 + 1230945536, "particles": 37847049},
+               "p2g": {"bytes": 1722830592 + 1471039232, "particles": 37847049}}
 FALLBACK_HBM = 6650.0
 
 
@@ -556,6 +556,93 @@ def pbf4_summary(local, name="wave_tank_256", iters=4, warm=3, steps=8):
             "value": st["live"] * steps / (ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms / steps,
             "pbf_stage_ms": stages["pbf"] / max(nrec, 1), "flip_stages_ms": (stages["total"] - stages["pbf"]) / max(nrec, 1),
             "particles": st["live"], "steps": steps, "warmup": warm}
+
+
+def batch_summary(local, count=64, warm=2, steps=10):
+    """Config 5 after the headline's timed region: the 64 uneven tanks stepped together with the sweep schedule picked
+    by the autotuner (graph branches, or the shared pool swept by one launch per colour or one persistent launch),
+    against the same step graphs as parallel branches and launched one after another; device-timed, 1 GPU."""
+    import torch
+    from splashtank_b200 import scenes
+    from splashtank_b200.batch import TankBatch, tune_schedule
+    from splashtank_b200.flip import FlipSim
+    from splashtank_b200.scene import SceneRunner
+    spec = scenes.BatchTanks(count=count)
+    made = [spec.make(k, FlipSim, device=local) for k in range(count)]
+    sims = [m[0] for m in made]
+    runners = [SceneRunner(s) for s in sims]
+    batch = TankBatch(sims, "graph")
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+
+    def step():
+        batch.step(spec.dt, [spec.step_opts(k, s, r) for k, s, r in zip(range(count), sims, runners)])
+
+    def timer(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(warm):
+        step()
+    sched, trials = tune_schedule(batch, step, timer)
+    out = {}
+    for name, mode in (("tuned", sched[0]), ("graph_branches", "graph"), ("sequential", "sequential")):
+        batch.set_mode(mode)
+        for _ in range(warm):
+            step()
+        ms = timer(lambda: [step() for _ in range(steps)]) / steps
+        out[name] = ms
+    live = sum(s.readStats()["live"] for s in sims)
+    batch.destroy()
+    for s in sims:
+        s.destroy()
+    return {"workload": "batch_%d" % count, "tanks": count, "particles": int(live), "unit": "particle-steps/s",
+            "value": live / (out["tuned"] * 1e-3), "ms_per_step": out["tuned"],
+            "sweep_schedule": {"mode": sched[0], "ctas_per_sm": sched[1]},
+            "schedule_trials_ms": {"%s:%d" % k: round(v, 3) for k, v in trials.items()},
+            "graph_branches_ms_per_step": out["graph_branches"], "sequential_ms_per_step": out["sequential"],
+            "speedup_vs_sequential": round(out["sequential"] / out["tuned"], 3), "steps": steps, "warmup": warm,
+            "launch_shape": "default (the full autotune of launch shapes runs in --workload batch_64)"}
+
+
+def diff_summary(local, n=128):
+    """Config 4 after the headline's timed region: one FP32 gradient of the 32-step rollout (forward with checkpoints,
+    recompute, adjoint) and the forward alone, with the distance-grid box collider, and the FP32 gradient against the
+    FP64 one."""
+    import torch
+    from splashtank_b200 import scenes
+    d = scenes.DiffDam(n=n)
+    p0 = d.params
+    s32 = d.make(collider="grid", device=local)
+    stream = torch.cuda.ExternalStream(s32.stream(), device=local)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    s32.forward(p0)
+    s32.backward()
+    ms_grad = timed(lambda: (s32.forward(p0), s32.backward()))
+    ms_fwd = timed(lambda: s32.forward(p0))
+    s32.forward(p0)
+    g32 = s32.backward()
+    s32.destroy()
+    s64 = d.make(fp64=True, collider="grid", device=local)
+    s64.forward(p0)
+    g64 = s64.backward()
+    s64.destroy()
+    ps = d.pos.shape[0] * d.steps
+    return {"workload": "diff_%d" % n, "particles": int(d.pos.shape[0]), "rollout_steps": d.steps, "checkpoint_every": d.ckpt,
+            "collider": "the box's distance grid (sdfEval's trilinear gradient and Hessian in the adjoint)",
+            "gradient_ms": ms_grad, "forward_ms": ms_fwd, "value": ps / (ms_grad * 1e-3), "unit": "gradient particle-steps/s",
+            "f32_vs_f64_adjoint_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))}
 
 
 # ---------------------------------------------------------------- the PBF engine (GpuSim)
@@ -1117,10 +1204,13 @@ def main():
             sim.destroy()
             del sim
             if not a.no_extras and a.workload.startswith("wave_tank"):
-                # the metric's pressure half and the reference's narrow band of 3 cells, after the timed regions
+                # the metric's pressure half, the reference's narrow band of 3 cells, config 2 with its PBF stage, and the
+                # batching and differentiation configurations, after the timed regions
                 line["pressure"] = pressure_summary(local)
                 line["band3"] = band_summary(local, a.workload + "_band3")
                 line["pbf4"] = pbf4_summary(local, a.workload)
+                line["batch64"] = batch_summary(local)
+                line["diff128"] = diff_summary(local)
             if not a.no_cpu_baseline:
                 cb, _ = cpu_sample(a.workload, w)
                 line["cpu_baseline"] = cb
