@@ -905,8 +905,6 @@ __device__ __forceinline__ float4 foamCell(const FlipParams& P, const G2PUni& U,
 template <bool OCEAN>
 __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q) {
   const V3 p = xyz(q.p), v0 = xyz(q.v);
-  int fi, fj, fk;
-  particleCell(P, p, fi, fj, fk);
   V3 vn, vo;
   sampleWin(P, W, p, vn, vo);    // the particle's own tile has storage: it marked it this step
   V3 v = vmix(vn, v0 + (vn - vo), P.flip);
@@ -928,6 +926,8 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     const int z = clampi(clampi(bk, -1, (int)P.nz - 1) - (W.oz - 1), 0, 8);
     fc = W.foam[x + 9 * (y + 9 * z)];
   } else {
+    int fi, fj, fk;
+    particleCell(P, p, fi, fj, fk);
     fc = foamCell(P, U, P.q9 < 0.5f ? 8.0f * (float)W.cnt[W.idx(fi, fj, fk)] : 8.0f * P.rest);
   }
   const float air = fc.x, shield = fc.w;
