@@ -97,8 +97,13 @@ def workload(name):
 
 
 def config_of(name, w, n_live):
-    cfg = {"workload": name, "particles": int(n_live), "dt": w.dt,
-           "l2": "working set larger than L2 (126 MB): no flush", "parallelism": "replicas"}
+    # particles (two 32-byte buffers) and the tile box's cells (about 94 bytes each) against the 126 MB L2
+    n = getattr(w, "n", None) or int(round(1.0 / (2.0 * w.d)))
+    ws = 64 * len(w.pos) + 94 * (math.ceil((n + 1) / 8.0) * 8) ** 3
+    l2 = ("working set larger than L2 (126 MB): no flush" if ws > 126e6 else
+          "working set (about %d MB) fits in L2: steps run back to back without a flush, each reading the state the one "
+          "before left, as a running simulation does" % (ws // 1000000))
+    cfg = {"workload": name, "particles": int(n_live), "dt": w.dt, "l2": l2, "parallelism": "replicas"}
     if name.startswith("wave_tank"):
         cfg.update(grid=[w.n] * 3, tile="8^3", sor_iters=w.opts["iters"],
                    narrow_band="full depth (band 1e4)" if w.band >= 1e4 else "%g cells" % w.band,
