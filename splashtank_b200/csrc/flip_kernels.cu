@@ -728,9 +728,12 @@ __device__ __forceinline__ void sampleBoth(const FlipParams& P, const Bufs& B, V
 // unchanged. s: a world-space sphere around the near box (xyz centre, w radius^2; w = +inf when the rows are not a
 // rotation): in exact arithmetic colNear(p) puts the local point inside the box centre cL +- half extents h, so
 // |p - (pos + R^T cL)| < |h|. lo/hi: the near box in local coordinates, before colNear's division by the voxel size.
-// Both carry slack (1% and one voxel) that covers rounding. on = 0 when colNear always holds.
+// Both carry slack (1% and one voxel) that covers rounding; wlo/whi bound the near box in world space and go first,
+// six compares that reject most particles of a tank near a long collider such as a wall piston, whose sphere covers
+// them. on = 0 when colNear always holds.
 struct ColPre {
   float4 s, r0, r1, r2, pos, lo, hi;
+  float4 wlo, whi;   // the near box's world-space bounding box (a tenth of a percent and 1e-5 wider), +-inf when unused
   int on;
 };
 __device__ ColPre colPre(const FlipParams& P, const float4* __restrict__ cols, uint32_t k) {
@@ -750,6 +753,21 @@ __device__ ColPre colPre(const FlipParams& P, const float4* __restrict__ cols, u
   const V3 c = pos + r0 * cL.x + r1 * cL.y + r2 * cL.z;
   const float rad = len3(h) * 1.01f + hw;
   X.s = (X.on && rot) ? make_float4(c.x, c.y, c.z, rad * rad) : make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0x7f800000));
+  // world bounds of the local box [lo, hi]: the rows are orthonormal to 1e-4, so pos + R^T lp covers it up to that
+  // relative error, far inside the box's voxel of slack; widened once more against the bounds' own rounding
+  const float inf = __int_as_float(0x7f800000);
+  X.wlo = make_float4(-inf, -inf, -inf, 0.0f);
+  X.whi = make_float4(inf, inf, inf, 0.0f);
+  if (X.on && rot) {
+    const V3 cl = v3((X.lo.x + X.hi.x) * 0.5f, (X.lo.y + X.hi.y) * 0.5f, (X.lo.z + X.hi.z) * 0.5f);
+    const V3 hl = v3((X.hi.x - X.lo.x) * 0.5f, (X.hi.y - X.lo.y) * 0.5f, (X.hi.z - X.lo.z) * 0.5f);
+    const V3 wc = pos + r0 * cl.x + r1 * cl.y + r2 * cl.z;
+    const V3 wh = v3(fabsf(r0.x) * hl.x + fabsf(r1.x) * hl.y + fabsf(r2.x) * hl.z, fabsf(r0.y) * hl.x + fabsf(r1.y) * hl.y + fabsf(r2.y) * hl.z,
+                     fabsf(r0.z) * hl.x + fabsf(r1.z) * hl.y + fabsf(r2.z) * hl.z);
+    const float e = 1.0e-5f * (1.0f + fabsf(wc.x) + fabsf(wc.y) + fabsf(wc.z) + len3(hl));
+    X.wlo = make_float4(wc.x - wh.x * 1.001f - e, wc.y - wh.y * 1.001f - e, wc.z - wh.z * 1.001f - e, 0.0f);
+    X.whi = make_float4(wc.x + wh.x * 1.001f + e, wc.y + wh.y * 1.001f + e, wc.z + wh.z * 1.001f + e, 0.0f);
+  }
   return X;
 }
 // collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first
@@ -758,6 +776,7 @@ __device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, cons
   const float m = P.margin;
   for (uint32_t k = 0; k < P.ncols; k++) {
     const ColPre& X = pre[k];
+    if (p.x < X.wlo.x || p.y < X.wlo.y || p.z < X.wlo.z || p.x > X.whi.x || p.y > X.whi.y || p.z > X.whi.z) continue;
     const V3 d0 = p - xyz(X.s);
     if (dot3(d0, d0) > X.s.w) continue;
     if (X.on) {
