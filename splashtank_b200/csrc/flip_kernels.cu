@@ -900,12 +900,15 @@ __device__ __noinline__ V3 gustAt(const GustTab& T, V3 gp, float tt) {
 }
 // values of the particle update that depend only on the parameters, computed once per thread
 struct G2PUni {
-  float sens, settle, tau0, tt, v2lo;
+  float sens, settle, tau0, tt, v2lo, imp2lo, trb2lo;
 };
 __device__ __forceinline__ G2PUni g2pUni(const FlipParams& P) {
-  // v2lo: below it |v|^2 cannot round to a speed above vmax (vmax^2 (1 - 2^-20) leaves room for both roundings)
-  return G2PUni{fmx(P.q6, 0.05f), smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f,
-                P.vmax * P.vmax * (1.0f - 1.0f / 1048576.0f)};
+  // v2lo: below it |v|^2 cannot round to a speed above vmax (vmax^2 (1 - 2^-20) leaves room for both roundings).
+  // imp2lo, trb2lo: below them |vn - vo|^2 and |v0 - vo|^2 cannot round to an impact or turbulence term above 0 (their
+  // clamped ramps start at 15 sens / dt and 0.35 sens; the factor 1 - 2^-16 leaves room for every rounding on the way)
+  const float sens = fmx(P.q6, 0.05f), a = 15.0f * sens * P.dt, b = 0.35f * sens;
+  return G2PUni{sens, smoothstepf(0.1f, 0.5f, P.q8), fmx(P.q5, 0.05f), P.q8 * 0.6f, P.vmax * P.vmax * (1.0f - 1.0f / 1048576.0f),
+                a * a * (1.0f - 1.0f / 65536.0f), b * b * (1.0f - 1.0f / 65536.0f)};
 }
 // The terms of g2p's particle update that depend only on the local density rho = csum / (8 rest) of the particle's
 // 2 x 2 x 2 count sum (wgsl-solver.js:222-240): air, the foam decay exp(-dt / tau), the drag factor
@@ -952,10 +955,17 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const float air = fc.x, shield = fc.w;
   const float spd0 = len3(v);
   const float sens = U.sens;
-  const float pacc = len3(vn - vo) / P.dt;
   const float settle = U.settle;
-  const float impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
-  const float turb = clampf((len3(v0 - vo) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
+  // impact and turbulence are 0 unless |vn - vo| / dt and |v0 - vo| reach their ramps: the common calm particle skips
+  // their square roots and divisions
+  const V3 dvn = vn - vo, dv0 = v0 - vo;
+  const float dvn2 = dot3(dvn, dvn), dv02 = dot3(dv0, dv0);
+  float impact = 0.0f, turb = 0.0f;
+  if (!(dvn2 < U.imp2lo)) {
+    const float pacc = sqrtf(dvn2) / P.dt;
+    impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
+  }
+  if (!(dv02 < U.trb2lo)) turb = clampf((sqrtf(dv02) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
   const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
   float foam = q.v.w * fc.y;
   foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
