@@ -953,7 +953,6 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     fc = foamCell(P, U, P.q9 < 0.5f ? 8.0f * (float)W.cnt[W.idx(fi, fj, fk)] : 8.0f * P.rest);
   }
   const float air = fc.x, shield = fc.w;
-  const float spd0 = len3(v);
   const float sens = U.sens;
   const float settle = U.settle;
   // impact and turbulence are 0 unless |vn - vo| / dt and |v0 - vo| reach their ramps: the common calm particle skips
@@ -966,7 +965,8 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     impact = clampf((pacc / sens - 15.0f) / 80.0f, 0.0f, 1.0f) * settle;
   }
   if (!(dv02 < U.trb2lo)) turb = clampf((sqrtf(dv02) / sens - 0.35f) / 1.5f, 0.0f, 1.0f) * settle;
-  const float spray = air * (0.25f + 0.75f * clampf(spd0 / 4.0f, 0.0f, 1.0f));
+  // with no air around (air 0, the deep water) the spray term is 0 whatever the speed: its square root is skipped
+  const float spray = air == 0.0f ? 0.0f : air * (0.25f + 0.75f * clampf(len3(v) / 4.0f, 0.0f, 1.0f));
   float foam = q.v.w * fc.y;
   foam = fmx(foam, fmx(spray * 0.9f, fmx(impact, turb * 0.8f)));
   if (OCEAN && P.ocean != 0u) foam *= 1.0f - clampf(layerW(P, p) * 2.0f, 0.0f, 1.0f);   // easing into the waves is not churning
@@ -1023,7 +1023,9 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
     G2PWin W{wv, wfoam, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
-    const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u;
+    // the trim (depth below the band) needs a band shallower than the deepest depth a cell word holds (8 - 65535 / 4096):
+    // at full depth (band 1e4) no particle is ever trimmed and the test is left out
+    const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u && P.band < 8.0f;
     const G2PUni U = g2pUni(P);
     for (int r = threadIdx.x; r < 1000; r += G2P_T) {
       const int gi = W.ox + r % 10 - 1, gj = W.oy + (r / 10) % 10 - 1, gk = W.oz + r / 100 - 1;
@@ -1089,7 +1091,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
         const float lw = layerW(P, xyz(q.p));
         kill = lw >= 0.5f || (lw > 0.25f && q.p.y > oceanEta(P, B.waves, q.p.x, q.p.z) + 0.5f * P.h);
       }
-      if (!kill && !gone && P.nb != 0u && len3(xyz(q.v)) < 9.0f * P.h) {
+      if (!kill && !gone && needKill && len3(xyz(q.v)) < 9.0f * P.h) {
         int ci, cj, ck;
         particleCell(P, xyz(q.p), ci, cj, ck);
         if (W.has(ci, cj, ck)) kill = W.kill[W.idx(ci, cj, ck)] != 0;
