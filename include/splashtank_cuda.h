@@ -528,7 +528,9 @@ void* st_diff_stream(st_diff* s);
  * library, one per device: 2 x ST_NOALLOC_MAX_TILES + 4 doubles (1 MiB), holding per-tile partial sums.
  *  - n_tiles above ST_NOALLOC_MAX_TILES is rejected with ST_BAD_ARG and a message in st_last_error().
  *  - The first call on each device, made with that device current, looks up the scratch address
- *    (cudaGetSymbolAddress); make that first call before any stream capture on the device.
+ *    (cudaGetSymbolAddress).
+ *  - Every call synchronises `stream` and copies the result into host memory, so no call can be captured into a
+ *    graph: do not call it while `stream` (or, under global capture mode, any stream on the device) is capturing.
  *  - The scratch's error word must start at zero: each call clears it on `stream` before its kernels. The partial sums
  *    need no clearing; each call writes every one it reads.
  *  - Calls on one device share the scratch: calls that overlap in time (on other streams or host threads) race and
