@@ -770,10 +770,9 @@ __device__ ColPre colPre(const FlipParams& P, const float4* __restrict__ cols, u
   }
   return X;
 }
-// collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first
-__device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, const ColPre* pre, V3 pin) {
+// collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first; wall[0], wall[1]: the clamp box (wallBox)
+__device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, const ColPre* pre, const float4* wall, V3 pin) {
   V3 p = pin;
-  const float m = P.margin;
   for (uint32_t k = 0; k < P.ncols; k++) {
     const ColPre& X = pre[k];
     if (p.x < X.wlo.x || p.y < X.wlo.y || p.z < X.wlo.z || p.x > X.whi.x || p.y > X.whi.y || p.z > X.whi.z) continue;
@@ -789,10 +788,14 @@ __device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, cons
     sdfEval(B.cols, B.sdf, k, p, phi, wn);
     if (phi < P.q0) p = p + wn * (P.q0 - phi);
   }
-  const float big = 1.0e9f;
-  const V3 lo = v3((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m);
-  const V3 hi = v3((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m);
-  return vclamp(p, lo, hi);
+  const float4 lo = wall[0], hi = wall[1];
+  return vclamp(p, xyz(lo), xyz(hi));
+}
+// collideP's wall clamp box, the same for every particle: faces left open do not clamp
+__device__ __forceinline__ void wallBox(const FlipParams& P, float4* wall) {
+  const float big = 1.0e9f, m = P.margin;
+  wall[0] = make_float4((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m, 0.0f);
+  wall[1] = make_float4((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m, 0.0f);
 }
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
@@ -802,6 +805,7 @@ struct G2PWin {
   const float* wet;      // wetCellAt of each window cell (0 outside the domain)
   const uint8_t* kill;   // the narrow band's trim test of each window cell
   const ColPre* cpre;    // collider pre-tests (colPre)
+  const float4* wall;    // collideP's wall clamp box (wallBox)
   int ox, oy, oz;
   __device__ __forceinline__ int idx(int i, int j, int k) const { return (i - ox + 1) + 10 * ((j - oy + 1) + 10 * (k - oz + 1)); }
   __device__ __forceinline__ bool has(int i, int j, int k) const {
@@ -925,7 +929,8 @@ __device__ __forceinline__ float4 foamCell(const FlipParams& P, const G2PUni& U,
   return make_float4(air, st_expf(-P.dt / tau), 1.0f - st_expf(-kd * P.dt), shield);
 }
 template <bool OCEAN>
-__device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q) {
+__device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const G2PWin& W, const GustTab& T, const G2PUni& U, Part& q,
+                                       float& speed) {
   const V3 p = xyz(q.p), v0 = xyz(q.v);
   V3 vn, vo;
   sampleWin(P, W, p, vn, vo);    // the particle's own tile has storage: it marked it this step
@@ -984,7 +989,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     if (sp > P.vmax) v = v * (P.vmax / sp);
   }
   const V3 pt = p + v * P.dt;
-  const V3 pc = collidePB(P, B, W.cpre, pt);
+  const V3 pc = collidePB(P, B, W.cpre, W.wall, pt);
   const V3 dsp = pc - pt;
   if (dot3(dsp, dsp) > 1.0e-12f) {
     const V3 nrm = dsp / len3(dsp);
@@ -996,8 +1001,10 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
                   ((o & 8u) && pc.y > P.y1) || ((o & 16u) && pc.z < P.z0) || ((o & 32u) && pc.z > P.z1))) {
     q.p = make_float4(0.0f, -1.0e6f, 0.0f, 0.0f);
     q.v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    speed = 0.0f;
   } else {
-    q.p = make_float4(pc.x, pc.y, pc.z, fmn(len3(v), 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f));
+    speed = len3(v);   // |q.v.xyz|, also for the emission and trim tests after the update
+    q.p = make_float4(pc.x, pc.y, pc.z, fmn(speed, 63.0f) + 64.0f * floorf(foam * 15.0f + 0.5f));
     q.v = make_float4(v.x, v.y, v.z, foam);
   }
 }
@@ -1013,16 +1020,18 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
   __shared__ ColPre cpre[32];
+  __shared__ float4 wall[2];
   __shared__ GustTab gtab;
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
   if (threadIdx.x < P.ncols) cpre[threadIdx.x] = colPre(P, B.cols, threadIdx.x);
-  buildGust(P, gtab);   // its barriers also publish cpre
+  if (threadIdx.x == 0) wallBox(P, wall);
+  buildGust(P, gtab);   // its barriers also publish cpre and wall
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wv, wfoam, wcnt, wwet, wkill, cpre, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wv, wfoam, wcnt, wwet, wkill, cpre, wall, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     // the trim (depth below the band) needs a band shallower than the deepest depth a cell word holds (8 - 65535 / 4096):
     // at full depth (band 1e4) no particle is ever trimmed and the test is left out
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u && P.band < 8.0f;
@@ -1065,14 +1074,15 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
       Part q = qNext;
       if (i + G2P_T < s1) qNext = B.pa[i + G2P_T];
-      g2pOne<OCEAN>(P, B, W, gtab, U, q);
+      float speed;
+      g2pOne<OCEAN>(P, B, W, gtab, U, q, speed);
       // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
       // trim of deep calm particles (nbKill, wgsl-narrowband.js:93-102), both from the moved particle
       const bool gone = q.p.y < DEADY;
       uint32_t kc = 0;
       // e is 0 (or NaN) unless the particle is fast enough for crest (speed over sprMin) or churn (over 0.5): the
       // common slow particle skips the eight wetness reads (kc stays 0 either way)
-      const float xs = len3(xyz(q.v)) * P.vs;
+      const float xs = speed * P.vs;
       const bool oceanSide = OCEAN && P.ocean != 0u && !gone && layerW(P, xyz(q.p)) > 0.0f;   // no whitewater from the ocean's boundary
       if (!gone && needWet && !oceanSide && U.settle != 0.0f && (xs - P.sprMin > 0.0f || xs > 0.5f)) {
         float rho, fast, e;
@@ -1091,7 +1101,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
         const float lw = layerW(P, xyz(q.p));
         kill = lw >= 0.5f || (lw > 0.25f && q.p.y > oceanEta(P, B.waves, q.p.x, q.p.z) + 0.5f * P.h);
       }
-      if (!kill && !gone && needKill && len3(xyz(q.v)) < 9.0f * P.h) {
+      if (!kill && !gone && needKill && speed < 9.0f * P.h) {
         int ci, cj, ck;
         particleCell(P, xyz(q.p), ci, cj, ck);
         if (W.has(ci, cj, ck)) kill = W.kill[W.idx(ci, cj, ck)] != 0;
