@@ -1011,12 +1011,26 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
 // One CTA per tile with storage: the tile's particles are one contiguous sorted segment, and every face and count they
 // sample lies in the 10^3-cell window (the tile plus one cell around it), staged once in shared memory.
 constexpr int G2P_T = 256;
+constexpr int G2P_DYN = 729 * 16 + 2 * G2P_T * 32;   // the foam table, then two particle slots per thread
+// 16-byte asynchronous copies from global to shared memory (cp.async): the data lands without passing through
+// registers, and the issuing thread waits for it with cpAsyncWait before reading the slot
+__device__ __forceinline__ void cpAsync16(void* smem, const void* gmem) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncPart(Part* slot, const Part* src) {
+  cpAsync16(&slot->p, &src->p);
+  cpAsync16(&slot->v, &src->v);
+}
 template <bool OCEAN>
 __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
-  extern __shared__ __align__(16) float4 wfoam[];   // 729 entries (dynamic: the static arrays fill the 48 KB limit)
+  extern __shared__ __align__(16) float4 wfoam[];   // 729 entries, then pslot (dynamic: the static arrays fill 48 KB)
+  Part* const pslot = reinterpret_cast<Part*>(wfoam + 729);   // [2][G2P_T]: this thread's next particles
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
   __shared__ ColPre cpre[32];
@@ -1068,12 +1082,17 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
     }
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
     uint32_t emitSum = 0, deadSum = 0;
-    // each thread loads its next particle while it updates the current one
-    Part qNext;
-    if (s0 + threadIdx.x < s1) qNext = B.pa[s0 + threadIdx.x];
+    // each thread's next particle is copied into its shared-memory slot while it updates the current one (no registers
+    // held for it); two slots, so a copy never lands in the slot being read
+    if (s0 + threadIdx.x < s1) cpAsyncPart(&pslot[threadIdx.x], &B.pa[s0 + threadIdx.x]);
+    cpAsyncCommit();
+    uint32_t slot = 0;
     for (uint32_t i = s0 + threadIdx.x; i < s1; i += G2P_T) {
-      Part q = qNext;
-      if (i + G2P_T < s1) qNext = B.pa[i + G2P_T];
+      cpAsyncWait();
+      Part q = pslot[slot * G2P_T + threadIdx.x];
+      slot ^= 1u;
+      if (i + G2P_T < s1) cpAsyncPart(&pslot[slot * G2P_T + threadIdx.x], &B.pa[i + G2P_T]);
+      cpAsyncCommit();
       float speed;
       g2pOne<OCEAN>(P, B, W, gtab, U, q, speed);
       // the whitewater each particle will throw off (sprayEmit's count, wgsl-whitewater.js:101-117) and the narrow band
@@ -1235,12 +1254,15 @@ cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, 
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
-  const int dyn = 729 * (int)sizeof(float4);
+  // three CTAs of about 73 KB each share an SM: ask for the largest shared-memory carveout
+  const int dyn = G2P_DYN;
   if (ocean) {
     cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     k_g2p<true><<<grid, G2P_T, dyn, s>>>(B);
   } else {
     cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     k_g2p<false><<<grid, G2P_T, dyn, s>>>(B);
   }
   return 1;
