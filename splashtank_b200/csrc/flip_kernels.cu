@@ -797,10 +797,17 @@ __device__ __forceinline__ void wallBox(const FlipParams& P, float4* wall) {
   wall[0] = make_float4((P.open & 1u) ? -big : P.x0 + m, (P.open & 4u) ? -big : P.y0 + m, (P.open & 16u) ? -big : P.z0 + m, 0.0f);
   wall[1] = make_float4((P.open & 2u) ? big : P.x1 - m, (P.open & 8u) ? big : P.y1 - m, (P.open & 32u) ? big : P.z1 - m, 0.0f);
 }
+constexpr int G2P_T = 256;
+// dynamic shared memory: the foam terms of count sums 0 .. G2P_LUT - 1 (float4), the tile's 729 count sums (int, padded
+// to 16 bytes), then two particle slots per thread
+constexpr int G2P_LUT = G2P_T;
+constexpr int G2P_CSUM_OFF = G2P_LUT * 16, G2P_SLOT_OFF = G2P_CSUM_OFF + 2928;
+constexpr int G2P_DYN = G2P_SLOT_OFF + 2 * G2P_T * 32;
 // The particle update of g2p: p, v0 in; vn/vo and the counts come from the tile's shared-memory window.
 struct G2PWin {
   const float2* v;   // [3][1000]: (vn, vo) of each face, one 64-bit load per corner
-  const float4* foam;    // [9][9][9]: foamCell of the summed counts of the 2 x 2 x 2 cells from (ox - 1, oy - 1, oz - 1) + (x, y, z)
+  const int32_t* csum;   // [9][9][9]: the summed counts of the 2 x 2 x 2 cells from (ox - 1, oy - 1, oz - 1) + (x, y, z)
+  const float4* lut;     // [G2P_LUT]: foamCell of the count sums 0 .. G2P_LUT - 1
   const int32_t* cnt;
   const float* wet;      // wetCellAt of each window cell (0 outside the domain)
   const uint8_t* kill;   // the narrow band's trim test of each window cell
@@ -946,17 +953,22 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
   const int bi = gidx(bcf.x), bj = gidx(bcf.y), bk = gidx(bcf.z);
   const bool fast = P.q12 > 0.5f;
   float4 fc;
+  float csum;
+  bool direct = true;
   if (P.q9 < 0.5f && !fast) {
     // the sum depends on the corner only through its clamp into [-1, n - 1], which the tile's particles keep within
     // the staged 9^3 block (the outer clamp only keeps the shared-memory index in bounds)
     const int x = clampi(clampi(bi, -1, (int)P.nx - 1) - (W.ox - 1), 0, 8), y = clampi(clampi(bj, -1, (int)P.ny - 1) - (W.oy - 1), 0, 8);
     const int z = clampi(clampi(bk, -1, (int)P.nz - 1) - (W.oz - 1), 0, 8);
-    fc = W.foam[x + 9 * (y + 9 * z)];
+    const int32_t cs = W.csum[x + 9 * (y + 9 * z)];
+    if ((uint32_t)cs < (uint32_t)G2P_LUT) { fc = W.lut[cs]; direct = false; }
+    else csum = (float)cs;
   } else {
     int fi, fj, fk;
     particleCell(P, p, fi, fj, fk);
-    fc = foamCell(P, U, P.q9 < 0.5f ? 8.0f * (float)W.cnt[W.idx(fi, fj, fk)] : 8.0f * P.rest);
+    csum = P.q9 < 0.5f ? 8.0f * (float)W.cnt[W.idx(fi, fj, fk)] : 8.0f * P.rest;
   }
+  if (direct) fc = foamCell(P, U, csum);
   const float air = fc.x, shield = fc.w;
   const float sens = U.sens;
   const float settle = U.settle;
@@ -1010,8 +1022,6 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
 }
 // One CTA per tile with storage: the tile's particles are one contiguous sorted segment, and every face and count they
 // sample lies in the 10^3-cell window (the tile plus one cell around it), staged once in shared memory.
-constexpr int G2P_T = 256;
-constexpr int G2P_DYN = 729 * 16 + 2 * G2P_T * 32;   // the foam table, then two particle slots per thread
 // 16-byte asynchronous copies from global to shared memory (cp.async): the data lands without passing through
 // registers, and the issuing thread waits for it with cpAsyncWait before reading the slot
 __device__ __forceinline__ void cpAsync16(void* smem, const void* gmem) {
@@ -1029,8 +1039,10 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   __shared__ FlipParams P;
   __shared__ float2 wv[3 * 1000];
   __shared__ int32_t wcnt[1000];
-  extern __shared__ __align__(16) float4 wfoam[];   // 729 entries, then pslot (dynamic: the static arrays fill 48 KB)
-  Part* const pslot = reinterpret_cast<Part*>(wfoam + 729);   // [2][G2P_T]: this thread's next particles
+  extern __shared__ __align__(16) unsigned char g2pDyn[];   // dynamic: the static arrays fill the 48 KB
+  float4* const wlut = reinterpret_cast<float4*>(g2pDyn);
+  int32_t* const wcsum = reinterpret_cast<int32_t*>(g2pDyn + G2P_CSUM_OFF);
+  Part* const pslot = reinterpret_cast<Part*>(g2pDyn + G2P_SLOT_OFF);   // [2][G2P_T]: this thread's next particles
   __shared__ float wwet[1000];
   __shared__ uint8_t wkill[1000];
   __shared__ ColPre cpre[32];
@@ -1040,12 +1052,18 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   loadParams(P, B.P);
   if (threadIdx.x < P.ncols) cpre[threadIdx.x] = colPre(P, B.cols, threadIdx.x);
   if (threadIdx.x == 0) wallBox(P, wall);
-  buildGust(P, gtab);   // its barriers also publish cpre and wall
+  // g2p's density terms depend on the local density only through the integer count sum of the particle's 2 x 2 x 2
+  // corner cells: evaluated once per CTA for the sums below G2P_LUT, in the reference's operations (the same values)
+  if (P.q9 < 0.5f && !(P.q12 > 0.5f)) {
+    const G2PUni U0 = g2pUni(P);
+    for (int r = threadIdx.x; r < G2P_LUT; r += G2P_T) wlut[r] = foamCell(P, U0, (float)r);
+  }
+  buildGust(P, gtab);   // its barriers also publish cpre, wall and wlut
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wv, wfoam, wcnt, wwet, wkill, cpre, wall, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    G2PWin W{wv, wcsum, wlut, wcnt, wwet, wkill, cpre, wall, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
     // the trim (depth below the band) needs a band shallower than the deepest depth a cell word holds (8 - 65535 / 4096):
     // at full depth (band 1e4) no particle is ever trimmed and the test is left out
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u && P.band < 8.0f;
@@ -1065,18 +1083,18 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
     }
     __syncthreads();
     // the local density's count sums (g2p's foam terms, wgsl-solver.js:222-229) of every corner a particle of this tile
-    // can have (integer-valued floats, so the sum is exact in any order), and the terms that follow from each
+    // can have (integers; the reference sums them as floats, exactly, so the float of this sum is its value)
     if (P.q9 < 0.5f && !(P.q12 > 0.5f)) {
       for (int r = threadIdx.x; r < 729; r += G2P_T) {
         const int bi = W.ox - 1 + r % 9, bj = W.oy - 1 + (r / 9) % 9, bk = W.oz - 1 + r / 81;
         const int xa = clampi(bi, 0, (int)P.nx - 1), xb = clampi(bi + 1, 0, (int)P.nx - 1);
         const int ya = clampi(bj, 0, (int)P.ny - 1), yb = clampi(bj + 1, 0, (int)P.ny - 1);
         const int za = clampi(bk, 0, (int)P.nz - 1), zb = clampi(bk + 1, 0, (int)P.nz - 1);
-        float cs = 0.0f;
+        int32_t cs = 0;
         for (int dz = 0; dz <= 1; dz++)
           for (int dy = 0; dy <= 1; dy++)
-            for (int dx = 0; dx <= 1; dx++) cs += (float)wcnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
-        wfoam[r] = foamCell(P, U, cs);
+            for (int dx = 0; dx <= 1; dx++) cs += wcnt[W.idx(dx ? xb : xa, dy ? yb : ya, dz ? zb : za)];
+        wcsum[r] = cs;
       }
       __syncthreads();
     }
