@@ -770,10 +770,15 @@ __device__ ColPre colPre(const FlipParams& P, const float4* __restrict__ cols, u
   }
   return X;
 }
-// collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first; wall[0], wall[1]: the clamp box (wallBox)
-__device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, const ColPre* pre, const float4* wall, V3 pin) {
+// collideP (src/flip/wgsl-solver.js:185-197) with the cheap tests first; wall[0], wall[1]: the clamp box (wallBox).
+// cmask: the colliders whose near box the tile's particles can reach (tileColliders); the others are skipped until a
+// push-out has moved the particle, after which every later collider is tested as the reference tests it.
+__device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, const ColPre* pre, const float4* wall, uint32_t cmask,
+                                        V3 pin) {
   V3 p = pin;
-  for (uint32_t k = 0; k < P.ncols; k++) {
+  bool moved = false;
+  for (uint32_t k = 0; cmask != 0u && k < P.ncols; k++) {
+    if (!moved && !((cmask >> k) & 1u)) continue;
     const ColPre& X = pre[k];
     if (p.x < X.wlo.x || p.y < X.wlo.y || p.z < X.wlo.z || p.x > X.whi.x || p.y > X.whi.y || p.z > X.whi.z) continue;
     const V3 d0 = p - xyz(X.s);
@@ -786,10 +791,25 @@ __device__ __forceinline__ V3 collidePB(const FlipParams& P, const Bufs& B, cons
     if (!colNear(P, B.cols, k, p)) continue;
     float phi; V3 wn;
     sdfEval(B.cols, B.sdf, k, p, phi, wn);
-    if (phi < P.q0) p = p + wn * (P.q0 - phi);
+    if (phi < P.q0) { p = p + wn * (P.q0 - phi); moved = true; }
   }
   const float4 lo = wall[0], hi = wall[1];
   return vclamp(p, xyz(lo), xyz(hi));
+}
+// The colliders a particle of the tile at cell (ox, oy, oz) can reach before a push-out moves it: their near boxes'
+// world bounds (ColPre wlo/whi) against the tile's cells grown by a cell (particleCell's rounding) and by the furthest
+// a particle moves in a step (vmax dt: the speed is limited before the move), with slack for the bounds' rounding.
+__device__ __forceinline__ uint32_t tileColliders(const FlipParams& P, const ColPre* pre, int ox, int oy, int oz) {
+  const float pad = P.h * 1.01f + fabsf(P.vmax) * P.dt * 1.01f +
+                    1.0e-5f * (1.0f + fabsf(P.x0) + fabsf(P.y0) + fabsf(P.z0) + fabsf(P.x1) + fabsf(P.y1) + fabsf(P.z1));
+  const V3 lo = v3(P.x0 + (float)ox * P.h - pad, P.y0 + (float)oy * P.h - pad, P.z0 + (float)oz * P.h - pad);
+  const V3 hi = v3(P.x0 + (float)(ox + 8) * P.h + pad, P.y0 + (float)(oy + 8) * P.h + pad, P.z0 + (float)(oz + 8) * P.h + pad);
+  uint32_t m = 0;
+  for (uint32_t k = 0; k < P.ncols; k++) {
+    const ColPre& X = pre[k];
+    if (!(hi.x < X.wlo.x || hi.y < X.wlo.y || hi.z < X.wlo.z || lo.x > X.whi.x || lo.y > X.whi.y || lo.z > X.whi.z)) m |= 1u << k;
+  }
+  return m;
 }
 // collideP's wall clamp box, the same for every particle: faces left open do not clamp
 __device__ __forceinline__ void wallBox(const FlipParams& P, float4* wall) {
@@ -813,6 +833,7 @@ struct G2PWin {
   const uint8_t* kill;   // the narrow band's trim test of each window cell
   const ColPre* cpre;    // collider pre-tests (colPre)
   const float4* wall;    // collideP's wall clamp box (wallBox)
+  uint32_t cmask;        // the colliders this tile's particles can reach (tileColliders)
   int ox, oy, oz;
   __device__ __forceinline__ int idx(int i, int j, int k) const { return (i - ox + 1) + 10 * ((j - oy + 1) + 10 * (k - oz + 1)); }
   __device__ __forceinline__ bool has(int i, int j, int k) const {
@@ -1001,7 +1022,7 @@ __device__ __forceinline__ void g2pOne(const FlipParams& P, const Bufs& B, const
     if (sp > P.vmax) v = v * (P.vmax / sp);
   }
   const V3 pt = p + v * P.dt;
-  const V3 pc = collidePB(P, B, W.cpre, W.wall, pt);
+  const V3 pc = collidePB(P, B, W.cpre, W.wall, W.cmask, pt);
   const V3 dsp = pc - pt;
   if (dot3(dsp, dsp) > 1.0e-12f) {
     const V3 nrm = dsp / len3(dsp);
@@ -1063,7 +1084,8 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
   for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
     const uint32_t t = B.active[a], tt = t / P.tx;
-    G2PWin W{wv, wcsum, wlut, wcnt, wwet, wkill, cpre, wall, (int)((t % P.tx) * 8u), (int)((tt % P.ty) * 8u), (int)((tt / P.ty) * 8u)};
+    const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
+    G2PWin W{wv, wcsum, wlut, wcnt, wwet, wkill, cpre, wall, tileColliders(P, cpre, ox, oy, oz), ox, oy, oz};
     // the trim (depth below the band) needs a band shallower than the deepest depth a cell word holds (8 - 65535 / 4096):
     // at full depth (band 1e4) no particle is ever trimmed and the test is left out
     const bool needWet = P.sprayOn != 0u && P.smax != 0u && P.sprRate > 0.0f, needKill = P.nb != 0u && P.band < 8.0f;

@@ -153,6 +153,32 @@ def test_air_field_with_whitewater(spray_cap):
     assert_same_state(g, o, spray=True)
 
 
+@pytest.mark.parametrize("mode", ["noFoam", "fastAir", None])
+def test_density_terms_modes_and_a_packed_clump(mode):
+    """g2p's local-density terms (air, shield, the foam decay and the drag factor) in each of the reference's modes: from
+    the 2 x 2 x 2 corner count sum (the default: a per-CTA table of the sums below 256 and a direct evaluation above),
+    from the particle's own cell (fastAir, with the gust skipped under shield) and at rest density (noFoam). Drag 0.3
+    with gusts and a steady wind; a clump of 2,400 extra particles packed into 2 x 2 x 2 cells makes corner sums far
+    above 256 in the first steps. 20 steps bit for bit."""
+    from flip_compare import make_pair
+    from splashtank_b200 import scenes
+    sc = scenes.dam_break(32)
+    rng = np.random.default_rng(11)
+    clump = (np.array([0.125, 0.3125, 0.0]) + rng.random((2400, 3)) * (2.0 / 32)).astype(np.float32)   # 2^3 cells in the air
+    sc["pos"] = np.concatenate([sc["pos"], clump]).astype(np.float32)
+    sc["vel"] = np.zeros_like(sc["pos"])
+    opts = dict(sc["opts"], drag=0.3, gust=1.0, wind=(1.5, 0.0, -0.5))
+    g, o = make_pair(sc)
+    for s in (g, o):
+        if mode:
+            s.opt[mode] = True
+    for _ in range(20):
+        for s in (g, o):
+            s.step(sc["dt"], opts)
+    assert g.readStats()["live"] == len(sc["pos"])
+    assert_same_state(g, o)
+
+
 def test_rotating_box_collider():
     """A box collider (its distance grid) turning about two axes while it sweeps through a dam break: the solid cells,
     the faces' collider velocity with the spin, and g2p's collider response (its world-space, sphere and local-space
