@@ -248,6 +248,8 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   cudaError_t e = cudaSetDevice(s->device);
   if (e != cudaSuccess) { set_err("cudaSetDevice", e); delete s; return ST_DEVICE_ERROR; }
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
+  // the resident-CTA counts of the dynamic-tile kernels, queried once here rather than first inside a graph capture
+  (void)p2g_ctas_per_sm(); (void)g2p_ctas_per_sm(false); (void)g2p_ctas_per_sm(true);
   s->d = desc->d;
   double r = desc->ratio != 0 ? desc->ratio : 2.0;
   s->ratio = std::max(1.4, std::min(4.0, r));
@@ -541,7 +543,7 @@ static int enqueue_front(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, u
   cudaMemsetAsync(&s->dCtl->fluid, 0, 3 * sizeof(uint32_t), q);        // fluid, vmaxBits, nLive (nActive is kept)
   cudaMemsetAsync(&s->dCtl->nDropped, 0, sizeof(uint32_t), q);
   cudaMemsetAsync(&s->dCtl->emitTried, 0, 2 * sizeof(uint32_t), q);     // emitTried, nFluidTiles
-  const int gT = s->tileGrid(s->gridT), gT4 = s->tileGrid(s->gridT4);
+  const int gT4 = s->tileGrid(s->gridT4);
   int nl = 0;
   mark(0);
   // blocks + sort: mark and count, activate tiles, offsets, scatter (the sort is part of the blocks stage)
@@ -553,7 +555,7 @@ static int enqueue_front(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, u
   nl += launch_scan_counts(B, q);
   nl += launch_scatter(B, q);
   mark(1);
-  nl += launch_p2g(B, gT, q);
+  nl += launch_p2g(B, s->tileGrid(std::min(s->gridT, p2g_ctas_per_sm())), q);   // dynamic tiles: resident CTAs only
   mark(2);
   if (nbOn) nl += launch_nb_phi(B, gT4, q);
   mark(3);
@@ -567,13 +569,13 @@ static int enqueue_front(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, u
 }
 template <class Mark>
 static int enqueue_back(st_flip* s, const Bufs& B, cudaStream_t q, bool nbOn, bool sprOn, int pbfIters, Mark mark) {
-  const int gT = s->tileGrid(s->gridT), gT4 = s->tileGrid(s->gridT4);
+  const int gT4 = s->tileGrid(s->gridT4);
   const bool ocean = s->hp.ocean != 0;
   int nl = 0;
   mark(6);
   nl += launch_project(B, gT4, q);
   mark(7);
-  nl += launch_g2p(B, gT, ocean, q);
+  nl += launch_g2p(B, s->tileGrid(std::min(s->gridT, g2p_ctas_per_sm(ocean))), ocean, q);   // dynamic tiles: resident CTAs only
   mark(8);
   if (s->sprayCap > 0) nl += launch_spray(B, s->sprayCap, sprOn, s->hp.airOn ? s->airCells : 0u, s->hp.ndrip != 0 ? s->dripCap : 0u, gT4, q);
   mark(9);

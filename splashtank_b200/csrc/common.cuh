@@ -61,8 +61,30 @@ struct Ctl {
   uint32_t emitTried;   // whitewater points tried this step
   uint32_t nFluidTiles; // tiles holding at least one fluid cell
   uint32_t nKilled;     // particles g2p killed this step (open faces, narrow band trim)
-  uint32_t pad[3];
+  uint32_t tileNext;    // p2g / g2p: the next tile a CTA takes (nextTile), 0 between launches
+  uint32_t tileDone;    // p2g / g2p: CTAs that have run out of tiles, 0 between launches
+  uint32_t pad;
 };
+// Dynamic tile assignment for the per-tile kernels whose tiles differ widely in work (p2g, g2p): a CTA takes the next
+// tile of the list when it has finished one, so the SMs that drew light tiles take more of them (a fixed stride left
+// SMs idle for the last sixth of g2p). Launch these kernels with only as many CTAs as can be resident. The call is a
+// barrier of the CTA; `slot` is a shared word.
+__device__ __forceinline__ uint32_t nextTile(Ctl* ctl, uint32_t* slot) {
+  if (threadIdx.x == 0) *slot = atomicAdd(&ctl->tileNext, 1u);
+  __syncthreads();
+  return *slot;
+}
+// After a CTA's last nextTile: the last CTA to leave puts the counters back to 0 for the next launch on the stream
+// (every other CTA has taken its last tile by then: each one's fetch is fenced before it counts itself out).
+__device__ __forceinline__ void tilesDone(Ctl* ctl) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctl->tileDone, 1u) == gridDim.x - 1u) {
+      ctl->tileNext = 0u;
+      ctl->tileDone = 0u;
+    }
+  }
+}
 
 struct Part { float4 p, v; };   // one particle: position (w: speed + 64 x foam level), velocity (w: foam)
 

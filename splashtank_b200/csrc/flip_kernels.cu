@@ -314,7 +314,10 @@ __global__ void __launch_bounds__(P2G_T, 4) k_p2g(Bufs B) {
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const uint32_t tid = threadIdx.x, splatPos = (tid & 31) * 8 + (tid >> 5);
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t tileSlot;
+  for (;;) {
+    const uint32_t a = nextTile(B.ctl, &tileSlot);
+    if (a >= nA) break;
     const uint32_t t = B.active[a];
     const uint32_t tt = t / P.tx;
     const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
@@ -370,6 +373,7 @@ __global__ void __launch_bounds__(P2G_T, 4) k_p2g(Bufs B) {
     }
     __syncthreads();
   }
+  tilesDone(B.ctl);
 }
 
 // ---- 6. collider bits (solidBuild, wgsl-solver.js:42-45) + classify (wgsl-solver.js:47-74) ----
@@ -1082,7 +1086,10 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
   buildGust(P, gtab);   // its barriers also publish cpre, wall and wlut
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t tileSlot;
+  for (;;) {
+    const uint32_t a = nextTile(B.ctl, &tileSlot);
+    if (a >= nA) break;
     const uint32_t t = B.active[a], tt = t / P.tx;
     const int ox = (int)((t % P.tx) * 8u), oy = (int)((tt % P.ty) * 8u), oz = (int)((tt / P.ty) * 8u);
     G2PWin W{wv, wcsum, wlut, wcnt, wwet, wkill, cpre, wall, tileColliders(P, cpre, ox, oy, oz), ox, oy, oz};
@@ -1190,6 +1197,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Bufs B) {
     }
     __syncthreads();
   }
+  tilesDone(B.ctl);
 }
 
 // unsort for readback (wgsl-blocks.js:97-99): id order into dst (pos and vel)
@@ -1224,8 +1232,19 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s) {
 }
 int launch_scan_counts(const Bufs& B, cudaStream_t s) { k_scan_counts<<<2, 1024, 0, s>>>(B); return 1; }
 int launch_scatter(const Bufs& B, cudaStream_t s) { k_scatter<<<B.nblk, CM_T, 0, s>>>(B); return 1; }
-int launch_p2g(const Bufs& B, int grid, cudaStream_t s) {
+// CTAs of a kernel that fit on one SM at once (the dynamic-tile kernels are launched with no more than these)
+static int residentPerSm(const void* fn, int threads, size_t dyn) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, dyn) != cudaSuccess || n < 1) n = 1;
+  return n;
+}
+int p2g_ctas_per_sm() {
   // the window, ids, offsets and staging buffers take more than the 48 KB of static shared memory
+  cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(P2GSmem));
+  static const int n = residentPerSm((const void*)k_p2g, P2G_T, sizeof(P2GSmem));
+  return n;
+}
+int launch_p2g(const Bufs& B, int grid, cudaStream_t s) {
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(P2GSmem));
   k_p2g<<<grid, P2G_T, sizeof(P2GSmem), s>>>(B);
   return 1;
@@ -1293,18 +1312,29 @@ cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, 
   return cudaLaunchCooperativeKernel((const void*)k_barrier_test, dim3((unsigned)grid), dim3(256), args, 0, s);
 }
 int launch_project(const Bufs& B, int grid, cudaStream_t s) { k_project<<<grid, 512, 0, s>>>(B); return 1; }
-int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
-  // three CTAs of about 73 KB each share an SM: ask for the largest shared-memory carveout
-  const int dyn = G2P_DYN;
+static void g2pAttributes(bool ocean) {
+  // three CTAs of about 68 KB each share an SM: ask for the largest shared-memory carveout
   if (ocean) {
-    cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, G2P_DYN);
     cudaFuncSetAttribute(k_g2p<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    k_g2p<true><<<grid, G2P_T, dyn, s>>>(B);
   } else {
-    cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, G2P_DYN);
     cudaFuncSetAttribute(k_g2p<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    k_g2p<false><<<grid, G2P_T, dyn, s>>>(B);
   }
+}
+int g2p_ctas_per_sm(bool ocean) {
+  g2pAttributes(ocean);
+  if (ocean) {
+    static const int n = residentPerSm((const void*)k_g2p<true>, G2P_T, G2P_DYN);
+    return n;
+  }
+  static const int n = residentPerSm((const void*)k_g2p<false>, G2P_T, G2P_DYN);
+  return n;
+}
+int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
+  g2pAttributes(ocean);
+  if (ocean) k_g2p<true><<<grid, G2P_T, G2P_DYN, s>>>(B);
+  else k_g2p<false><<<grid, G2P_T, G2P_DYN, s>>>(B);
   return 1;
 }
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s) {

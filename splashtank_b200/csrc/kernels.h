@@ -13,6 +13,7 @@ int launch_tiles(const Bufs& B, uint32_t ntiles, int grid, cudaStream_t s);
 int launch_scan_counts(const Bufs& B, cudaStream_t s);
 int launch_scatter(const Bufs& B, cudaStream_t s);
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
+int p2g_ctas_per_sm();   // CTAs of k_p2g resident on one SM (its launches use no more)
 // ocean: the kernels compiled with the ocean's boundary (only an ocean scene needs them)
 int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s);
@@ -28,6 +29,7 @@ int persistent_ctas_per_sm();
 cudaError_t launch_barrier_test(unsigned int* bar, unsigned int* err, int grid, unsigned int expect, uint64_t limit_ns, cudaStream_t s);
 int launch_project(const Bufs& B, int grid, cudaStream_t s);
 int launch_g2p(const Bufs& B, int grid, bool ocean, cudaStream_t s);
+int g2p_ctas_per_sm(bool ocean);   // CTAs of k_g2p resident on one SM (its launches use no more)
 int launch_unsort(const Part* src, const uint32_t* ids, uint32_t n, float4* pos, float4* vel, cudaStream_t s);
 int launch_fill_f32(float* p, float v, size_t n, cudaStream_t s);
 int launch_iota(uint32_t* p, uint32_t n, cudaStream_t s);
