@@ -250,6 +250,7 @@ st_status st_flip_create(const st_flip_desc* desc, st_flip** out) {
   cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device);
   // the resident-CTA counts of the dynamic-tile kernels, queried once here rather than first inside a graph capture
   (void)p2g_ctas_per_sm(); (void)g2p_ctas_per_sm(false); (void)g2p_ctas_per_sm(true);
+  warm_walk_grids_flip(); warm_walk_grids_extra();
   s->d = desc->d;
   double r = desc->ratio != 0 ? desc->ratio : 2.0;
   s->ratio = std::max(1.4, std::min(4.0, r));

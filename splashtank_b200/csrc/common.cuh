@@ -74,6 +74,26 @@ __device__ __forceinline__ uint32_t nextTile(Ctl* ctl, uint32_t* slot) {
   __syncthreads();
   return *slot;
 }
+// The same assignment for kernels whose tiles are short: the index of the next tile is fetched when the CTA starts a
+// tile, so its latency hides behind the tile's work, and handed over at a barrier that ends the tile (two shared
+// words, so a slow warp still reading the current index is never overwritten).
+//   TileWalk w{B.ctl, words};
+//   for (uint32_t a = w.begin(); a < nA; a = w.next()) { w.fetch(); ...the tile... }
+//   w.done();
+struct TileWalk {
+  Ctl* ctl;
+  uint32_t* slot;
+  uint32_t k = 0, pre = 0;
+  __device__ __forceinline__ uint32_t begin() { return nextTile(ctl, slot); }
+  __device__ __forceinline__ void fetch() { if (threadIdx.x == 0) pre = atomicAdd(&ctl->tileNext, 1u); }
+  __device__ __forceinline__ uint32_t next() {
+    k ^= 1u;
+    if (threadIdx.x == 0) slot[k] = pre;
+    __syncthreads();
+    return slot[k];
+  }
+  __device__ __forceinline__ void done();
+};
 // After a CTA's last nextTile: the last CTA to leave puts the counters back to 0 for the next launch on the stream
 // (every other CTA has taken its last tile by then: each one's fetch is fenced before it counts itself out).
 __device__ __forceinline__ void tilesDone(Ctl* ctl) {
@@ -85,6 +105,7 @@ __device__ __forceinline__ void tilesDone(Ctl* ctl) {
     }
   }
 }
+__device__ __forceinline__ void TileWalk::done() { tilesDone(ctl); }
 
 struct Part { float4 p, v; };   // one particle: position (w: speed + 64 x foam level), velocity (w: foam)
 

@@ -165,7 +165,10 @@ __global__ void __launch_bounds__(512) k_killed_list(Bufs B) {
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive;
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t walk[2];
+  TileWalk w{B.ctl, walk};
+  for (uint32_t a = w.begin(); a < nA; a = w.next()) {
+    w.fetch();
     if (B.tileDead[a + 1] == B.tileDead[a]) continue;   // uniform per block: no kills in this tile
     const uint32_t s0 = B.tileCnt[a], s1 = B.tileCnt[a + 1];
     uint32_t base = B.tileDead[a];
@@ -178,6 +181,7 @@ __global__ void __launch_bounds__(512) k_killed_list(Bufs B) {
       base += tot;
     }
   }
+  w.done();
 }
 __device__ __forceinline__ uint32_t deadSlot(const Bufs& B, uint32_t k, uint32_t nKilled, uint32_t nLive) {
   return k < nKilled ? B.deadList[k] : nLive + (k - nKilled);
@@ -209,7 +213,10 @@ __global__ void __launch_bounds__(512, 3) k_def_count(Bufs B) {
   __shared__ uint32_t sm[33];
   loadParams(P, B.P);
   const uint32_t nA = B.ctl->nActive;
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t walk[2];
+  TileWalk w{B.ctl, walk};
+  for (uint32_t a = w.begin(); a < nA; a = w.next()) {
+    w.fetch();
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
@@ -219,6 +226,7 @@ __global__ void __launch_bounds__(512, 3) k_def_count(Bufs B) {
     blockExclusive((nd ? 1u : 0u) | (nd << 16), sm, &tot);
     if (threadIdx.x == 0) { B.tileAux[a] = tot & 0xffffu; B.tileAux2[a] = tot >> 16; }
   }
+  w.done();
 }
 __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
   __shared__ FlipParams P;
@@ -227,7 +235,10 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const uint32_t nKilled = B.ctl->nKilled, nLive = B.ctl->nLive;
   const uint32_t avail = min(nKilled + (P.n - nLive), P.lcap);
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t walk[2];
+  TileWalk w{B.ctl, walk};
+  for (uint32_t a = w.begin(); a < nA; a = w.next()) {
+    w.fetch();
     if (B.tileAux2[a + 1] == B.tileAux2[a]) continue;   // no cell of this tile asks (the whole CTA skips it)
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
@@ -250,6 +261,7 @@ __global__ void __launch_bounds__(512) k_spawn(Bufs B) {
       B.pa[pi] = q;
     }
   }
+  w.done();
 }
 
 // ---- whitewater: wetCell / wetAt (wgsl-whitewater.js:7-23) ----
@@ -619,11 +631,16 @@ int launch_nb_phi(const Bufs& B, int grid, cudaStream_t s) {
 int launch_nb_vel(const Bufs& B, int grid, cudaStream_t s) { k_nb_vel<<<grid, 512, 0, s>>>(B); return 1; }
 int launch_nb_reseed(const Bufs& B, int grid, cudaStream_t s) {
   k_scan_x<<<1, 1024, 0, s>>>(B, 0);
-  k_killed_list<<<grid, 512, 0, s>>>(B);
-  k_def_count<<<grid, 512, 0, s>>>(B);
+  k_killed_list<<<walk_grid((const void*)k_killed_list, 512, grid), 512, 0, s>>>(B);
+  k_def_count<<<walk_grid((const void*)k_def_count, 512, grid), 512, 0, s>>>(B);
   k_scan_x<<<2, 1024, 0, s>>>(B, 1);
-  k_spawn<<<grid, 512, 0, s>>>(B);
+  k_spawn<<<walk_grid((const void*)k_spawn, 512, grid), 512, 0, s>>>(B);
   return 5;
+}
+void warm_walk_grids_extra() {
+  walk_grid((const void*)k_killed_list, 512, 1);
+  walk_grid((const void*)k_def_count, 512, 1);
+  walk_grid((const void*)k_spawn, 512, 1);
 }
 int launch_spray(const Bufs& B, uint32_t smax, bool emit, uint32_t airCells, uint32_t dripCap, int grid, cudaStream_t s) {
   if (!smax) return 0;

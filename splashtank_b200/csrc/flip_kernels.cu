@@ -3,6 +3,10 @@
 //
 // Every kernel is either one thread per particle (storage order) or one CTA per tile with storage, striding over
 // device-side counts, so a step needs no host round trip. Citations name the WGSL kernel each one restates.
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -469,7 +473,10 @@ __global__ void __launch_bounds__(512, 3) k_norm_div(Bufs B) {
   const uint32_t nA = B.ctl->nActive, nc = B.ncell;
   const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
   const int NX = (int)P.tx * 8, NY = (int)P.ty * 8, NZ = (int)P.tz * 8;
-  for (uint32_t a = blockIdx.x; a < nA; a += gridDim.x) {
+  __shared__ uint32_t walk[2];
+  TileWalk w{B.ctl, walk};
+  for (uint32_t a = w.begin(); a < nA; a = w.next()) {
+    w.fetch();
     const uint32_t t = B.active[a], c = t * 512u + threadIdx.x;
     int i, j, k;
     tileCoord(P, t, threadIdx.x, i, j, k);
@@ -520,8 +527,8 @@ __global__ void __launch_bounds__(512, 3) k_norm_div(Bufs B) {
       B.rhs[c] = (tgt - div) * P.h * P.h / P.dt;
       B.sorInfo[c] = (uint16_t)(0x8000u | (nns << 8) | mask);
     }
-    __syncthreads();
   }
+  w.done();
 }
 
 // ---- 8. red-black SOR (relax, wgsl-solver.js:124-140; rbRed/rbBlack :162-164) ----
@@ -1238,6 +1245,27 @@ static int residentPerSm(const void* fn, int threads, size_t dyn) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, dyn) != cudaSuccess || n < 1) n = 1;
   return n;
 }
+// The grid of a kernel that walks the tile list dynamically (TileWalk): no more CTAs than fit on the SMs at once (a CTA
+// that starts after the list is taken only loads its parameters and leaves). Resident counts are cached per kernel.
+static std::mutex g_walk_mu;
+static std::unordered_map<const void*, int> g_walk_res;
+int walk_grid(const void* fn, int threads, int grid) {
+  int res;
+  {
+    std::lock_guard<std::mutex> lk(g_walk_mu);
+    auto it = g_walk_res.find(fn);
+    if (it == g_walk_res.end()) res = g_walk_res[fn] = residentPerSm(fn, threads, 0);
+    else res = it->second;
+  }
+  int dev = 0, sms = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(1, std::min(grid, sms * res));
+}
+void warm_walk_grids_flip() {
+  walk_grid((const void*)k_norm_div<false>, 512, 1);
+  walk_grid((const void*)k_norm_div<true>, 512, 1);
+}
 int p2g_ctas_per_sm() {
   // the window, ids, offsets and staging buffers take more than the 48 KB of static shared memory
   cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(P2GSmem));
@@ -1255,8 +1283,8 @@ int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
   return 1;
 }
 int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s) {
-  if (ocean) k_norm_div<true><<<grid, 512, 0, s>>>(B);
-  else k_norm_div<false><<<grid, 512, 0, s>>>(B);
+  if (ocean) k_norm_div<true><<<walk_grid((const void*)k_norm_div<true>, 512, grid), 512, 0, s>>>(B);
+  else k_norm_div<false><<<walk_grid((const void*)k_norm_div<false>, 512, grid), 512, 0, s>>>(B);
   return 1;
 }
 int launch_sor_pack(const Bufs& B, int grid4, cudaStream_t s) {

@@ -14,6 +14,10 @@ int launch_scan_counts(const Bufs& B, cudaStream_t s);
 int launch_scatter(const Bufs& B, cudaStream_t s);
 int launch_p2g(const Bufs& B, int grid, cudaStream_t s);
 int p2g_ctas_per_sm();   // CTAs of k_p2g resident on one SM (its launches use no more)
+// the grid of a kernel that walks the tile list dynamically: at most its resident CTAs (cached per kernel)
+int walk_grid(const void* fn, int threads, int grid);
+void warm_walk_grids_flip();    // fill that cache for the kernels of flip_kernels.cu / flip_extra.cu (outside any
+void warm_walk_grids_extra();   // graph capture)
 // ocean: the kernels compiled with the ocean's boundary (only an ocean scene needs them)
 int launch_classify(const Bufs& B, int grid, bool ocean, cudaStream_t s);
 int launch_norm_div(const Bufs& B, int grid, bool ocean, cudaStream_t s);
