@@ -439,8 +439,9 @@ st_status st_flip_bake_diag(st_flip* s, float vcap, st_bake_diag* out);
 
 /* ---- launch shape of a tank's kernels (no reference counterpart: WebGPU picks no grid sizes) ----
  * CTAs per SM of the per-tile kernels: heavy (p2g, g2p; default 8), light (classify, normalise, project, narrow band;
- * default 4) and the pressure sweeps (default 8), each capped at the tile count. Results do not depend on them; an
- * autotuner picks them for many tanks sharing one GPU. */
+ * default 4) and the pressure sweeps (default 8), each capped at the tile count. The kernels that take their tiles from
+ * a counter (p2g, g2p, normalise + divergence, the narrow band's refill) are also capped at the CTAs that fit on the
+ * SMs at once. Results do not depend on them; an autotuner picks them for many tanks sharing one GPU. */
 st_status st_flip_set_launch(st_flip* s, int32_t tile_ctas_per_sm, int32_t light_ctas_per_sm, int32_t sor_ctas_per_sm);
 
 /* ---- many independent tanks stepped together (no reference counterpart; the reference steps one tank) ----
