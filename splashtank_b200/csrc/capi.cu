@@ -1579,6 +1579,8 @@ st_status st_flip_load_full(st_flip* s, const void* buf, uint64_t size) {
       if (p.second) CK(cudaMemcpyAsync(p.first, in, p.second, cudaMemcpyHostToDevice, s->stream));
       in += p.second;
     }
+    // the dynamic-tile counters are 0 between launches; a checkpoint cannot change that
+    CK(cudaMemsetAsync(&s->dCtl->tileNext, 0, 2 * sizeof(uint32_t), s->stream));
     CK(cudaStreamSynchronize(s->stream));
     drop_graphs(s);
     s->sdfSig.clear();   // the next step uploads its colliders' distance grids again
