@@ -255,9 +255,10 @@ __global__ void __launch_bounds__(CM_T, 6) k_scatter(Bufs B) {
 // final place) runs with a warp's lanes on consecutive particles, so its global loads and stores are coalesced and
 // the lanes of one cell read the same ids (L1 broadcasts); it leaves each particle's position and velocity in shared
 // memory. The splat then takes them back with a warp's lanes 8 particles apart (different cells, so the window atomics
-// rarely collide), from a layout padded by one word per 32 so those reads hit 32 different banks. Four CTAs share an
-// SM (64 registers, 34 KB of shared memory each); staging the tile's ids in shared memory, a second staging buffer,
-// five or six CTAs per SM and window strides padded against bank conflicts (24 / 256 words) all measured slower.
+// rarely collide), from a layout padded by one word per 32 so those reads hit 32 different banks. Five CTAs share an
+// SM (48 registers, 34 KB of shared memory each; with the tiles taken dynamically five beat four, 1.42 -> 1.37 ms at
+// 256^3, and six spill); staging the tile's ids in shared memory, a second staging buffer and window strides padded
+// against bank conflicts (24 / 256 words) all measured slower.
 constexpr int P2G_T = 256;
 constexpr int P2G_SW = P2G_T + P2G_T / 32;
 struct P2GSmem {
@@ -311,7 +312,7 @@ __device__ __forceinline__ void p2gSplat(const FlipParams& P, P2GSmem& S, V3 p, 
     }
   }
 }
-__global__ void __launch_bounds__(P2G_T, 4) k_p2g(Bufs B) {
+__global__ void __launch_bounds__(P2G_T, 5) k_p2g(Bufs B) {
   extern __shared__ __align__(16) unsigned char p2gRaw[];
   P2GSmem& S = *reinterpret_cast<P2GSmem*>(p2gRaw);
   __shared__ FlipParams P;
