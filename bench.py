@@ -1214,6 +1214,8 @@ def main():
                 line["pressure"] = pressure_summary(local)
                 line["band3"] = band_summary(local, a.workload + "_band3")
                 line["pbf4"] = pbf4_summary(local, a.workload)
+                # config 2 with everything it names at once: the 3-cell narrow band and the 4-iteration PBF stage
+                line["band3_pbf4"] = pbf4_summary(local, a.workload + "_band3", warm=8, steps=20)
                 line["batch64"] = batch_summary(local)
                 line["diff128"] = diff_summary(local)
             if not a.no_cpu_baseline:
