@@ -109,7 +109,7 @@ def config_of(name, w, n_live):
                    narrow_band="full depth (band 1e4)" if w.band >= 1e4 else "%g cells" % w.band,
                    colliders="piston box 0.5 Hz amp 0.05 + sphere r 0.1 on a linear path over %d steps" % w.steps,
                    whitewater_cap=w.spray_cap,
-                   pbf="not in this step (the 4-iteration PBF density stage is timed in the pbf4 sub-object)")
+                   pbf="not in this step (the 4-iteration PBF density stage is timed in the pbf4 and band3_pbf4 sub-objects)")
     return cfg
 
 
