@@ -30,11 +30,11 @@ sys.path.insert(0, ROOT)
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # what limits each kernel instead of DRAM bandwidth, from ncu captures of the same kernels on the 128^3 wave tank
 NCU_LIMITER = {"g2p": "instruction issue: 71% issue active at 24 warps per SM (80 registers), 998 instructions per particle",
-               "p2g": "shared-memory atomics: L1 pipe 75% busy, 3.1 wavefronts per atomic (two thirds bank-conflict replays)"}
+               "p2g": "shared-memory atomics: L1 pipe 78% busy, 3.1 wavefronts per atomic (two thirds bank-conflict replays)"}
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch in a one-pass ncu capture of the 256^3 wave tank itself
 # (the third step of `bench.py --steps 2 --warmup 1`, 37,847,049 live particles), scaled by the live particles
-NCU_TRAFFIC = {"g2p": {"bytes": 1406323712 + 1227884032, "particles": 37847049},
-               "p2g": {"bytes": 1686296064 + 1440514560, "particles": 37847049}}
+NCU_TRAFFIC = {"g2p": {"bytes": 1405361152 + 1227728640, "particles": 37847049},
+               "p2g": {"bytes": 1697710848 + 1451466496, "particles": 37847049}}
 FALLBACK_HBM = 6650.0
 
 
